@@ -1,0 +1,75 @@
+"""ctypes binding of libhdsdp_b200.so (the in-tree CUDA build).
+
+The library has no CPU path: loading fails loudly when the shared object is
+missing, and HDSDPCreate refuses to create a solver without a CUDA device.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libhdsdp_b200.so")
+
+# Every entry point declared in include/hdsdp.h, include/hdsdp_user_data.h and
+# include/hdsdp_b200.h.
+EXPORTS = [
+    "HDSDPCreate", "HDSDPInit", "HDSDPSetCone", "HDSDPSetDualObjective", "HDSDPOptimize",
+    "HDSDPSetIntParam", "HDSDPSetDblParam", "HDSDPGetRowDual", "HDSDPGetConeValues",
+    "HDSDPCheckSolution", "HDSDPClear", "HDSDPDestroy",
+    "HUserDataCreate", "HUserDataSetConeData", "HUserDataChooseCone", "HUserDataClear",
+    "HUserDataDestroy",
+    "HDSDPGetStatus", "HDSDPGetIterCount", "HDSDPSetPrimalRefinement", "HDSDPSetPrecision",
+    "HDSDPGetIterLog", "HDSDPGetTimers",
+    "hdsdpb_schur_probe", "hdsdpb_ratio_probe", "hdsdpb_cholesky", "hdsdpb_inverse", "hdsdpb_gemm",
+]
+
+_lib = None
+
+
+def load():
+    """Load the CUDA library, raising if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError("libhdsdp_b200.so is missing: run __graft_entry__.build() "
+                           "(this library has no CPU fallback)")
+    L = C.CDLL(LIB_PATH)
+    vp, ip, dp, i, d = C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_double), C.c_int, C.c_double
+    sig = {
+        "HDSDPCreate": ([C.POINTER(vp)], i),
+        "HDSDPInit": ([vp, i, i], i),
+        "HDSDPSetCone": ([vp, i, vp], i),
+        "HDSDPSetDualObjective": ([vp, dp], None),
+        "HDSDPOptimize": ([vp, i], i),
+        "HDSDPSetIntParam": ([vp, i, i], None),
+        "HDSDPSetDblParam": ([vp, i, d], None),
+        "HDSDPGetRowDual": ([vp, dp, dp, dp], i),
+        "HDSDPGetConeValues": ([vp, i, dp, dp, dp], None),
+        "HDSDPCheckSolution": ([vp, dp], i),
+        "HDSDPClear": ([vp], None),
+        "HDSDPDestroy": ([C.POINTER(vp)], None),
+        "HUserDataCreate": ([C.POINTER(vp)], i),
+        "HUserDataSetConeData": ([vp, i, i, i, ip, ip, dp], None),
+        "HUserDataChooseCone": ([vp], i),
+        "HUserDataClear": ([vp], None),
+        "HUserDataDestroy": ([C.POINTER(vp)], None),
+        "HDSDPGetStatus": ([vp], i),
+        "HDSDPGetIterCount": ([vp], i),
+        "HDSDPSetPrimalRefinement": ([vp, i], None),
+        "HDSDPSetPrecision": ([vp, i], None),
+        "HDSDPGetIterLog": ([vp, i, dp, dp, dp, dp, dp, ip], i),
+        "HDSDPGetTimers": ([vp, dp], None),
+        "hdsdpb_schur_probe": ([i, i, ip, ip, dp, dp, d, i, dp, dp, dp, dp], i),
+        "hdsdpb_ratio_probe": ([i, i, ip, ip, dp, dp, d, dp, d, dp, dp], i),
+        "hdsdpb_cholesky": ([i, dp, dp, dp], i),
+        "hdsdpb_inverse": ([i, dp, dp], i),
+        "hdsdpb_gemm": ([i, i, i, d, dp, i, i, dp, i, i, d, dp, i], i),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = res
+    _lib = L
+    return L

@@ -1,0 +1,1020 @@
+// Dense SDP cone, scalar bound cone, Schur (KKT) system and Lanczos step
+// estimator of the B200 HDSDP solver.
+#include "solver.h"
+#include <cmath>
+#include <cstring>
+#include <cstdlib>
+#include <algorithm>
+#include <chrono>
+
+namespace hb {
+
+static double wall() {
+    using namespace std::chrono;
+    return duration<double>(steady_clock::now().time_since_epoch()).count();
+}
+
+// ======================================================================================
+// Presolve: coefficient types and rank-one extraction
+// ======================================================================================
+namespace {
+
+// Packed lower-triangle index -> (row, col) (interface/hdsdp_utils.h:49).
+inline void unpack(int n, long p, int &i, int &j) {
+    // column j starts at j*(2n - j + 1)/2
+    long lo = 0, hi = n - 1;
+    while (lo < hi) {
+        long mid = (lo + hi + 1) / 2;
+        long start = mid * (2L * n - mid + 1) / 2;
+        if (start <= p) lo = mid;
+        else hi = mid - 1;
+    }
+    j = (int) lo;
+    i = (int) (p - ((2L * n - lo - 1) * lo) / 2);
+}
+
+// Rank-one test of a sparse lower triplet matrix, following the acceptance rules of
+// tsp_r1_extract (linalg/sparse_opts.c:151-214): the first stored entry must be
+// diagonal, its column defines a, the entry count must be that of a's outer product,
+// and the reconstruction error in the 1-norm must not exceed 1e-10.
+bool sparse_rank_one(int n, const std::vector<int> &r, const std::vector<int> &c, const std::vector<double> &v,
+                     double &sgn, std::vector<double> &a) {
+    const int nnz = (int) v.size();
+    if (nnz == 0) return false;
+    a.assign(n, 0.0);
+    const int i0 = r[0];
+    if (r[0] != c[0]) return false;
+    if (nnz == 1) {
+        sgn = v[0];
+        a[i0] = 1.0;
+        return true;
+    }
+    const double s = (v[0] > 0) ? 1.0 : -1.0;
+    const double root = std::sqrt(std::fabs(v[0]));
+    int k = 0, anz = 0;
+    for (k = 0; k < nnz; ++k) {
+        if (c[k] > i0) break;
+        a[r[k]] = v[k] / root;
+        anz += 1;
+    }
+    if (nnz != anz * (anz + 1) / 2) return false;
+    if (k == n) return false;
+    double eps = 0.0;
+    for (int e = 0; e < nnz; ++e) eps += std::fabs(v[e] - s * a[r[e]] * a[c[e]]);
+    if (eps > 1e-10) return false;
+    sgn = s;
+    return true;
+}
+
+// Rank-one test of a dense packed matrix (pds_r1_extract, linalg/dense_opts.c:174-230):
+// a is read from the column of the first nonzero diagonal entry.
+bool dense_rank_one(int n, const std::vector<double> &P, double &sgn, std::vector<double> &a) {
+    long k = 0;
+    int i;
+    for (i = 0; i < n; ++i) {
+        if (P[k] != 0) break;
+        k += n - i;
+    }
+    if (i == n) return false;
+    const double s = (P[k] > 0) ? 1.0 : -1.0;
+    const double root = std::sqrt(std::fabs(P[k]));
+    a.assign(n, 0.0);
+    const long colStart = ((2L * n - i - 1) * i) / 2;
+    for (int q = 0; q < n; ++q) a[q] = P[colStart + q] / root;
+    double eps = 0.0;
+    long id = 0;
+    for (int col = 0; col < n; ++col) {
+        for (int j = 0; j < n - col; ++j) eps += std::fabs(P[id + j] - s * a[col] * a[col + j]);
+        id += n - col;
+        if (eps > 1e-10) return false;
+    }
+    sgn = s;
+    return true;
+}
+
+// Normalise a = a / ||a||, sign *= ||a||^2 (linalg/hdsdp_sdpdata.c:880-899).
+void normalize_r1(HostCoeff &h) {
+    double nrm = 0.0;
+    for (double x : h.aval) nrm += x * x;
+    nrm = std::sqrt(nrm);
+    h.sign *= nrm * nrm;
+    for (double &x : h.aval) x /= nrm;
+}
+
+}  // namespace
+
+hdsdp_retcode SdpCone::proc_data(int nRow, int nCol, const int *Ap, const int *Ai, const double *Ax) {
+    n = nCol;
+    m = nRow;
+    A.assign(m, HostCoeff());
+    refType.assign(m, REF_ZERO);
+    for (int k = 0; k < 5; ++k) stats[k] = 0;
+    const long npack = (long) n * (n + 1) / 2;
+    auto load = [&](int col, HostCoeff &h, int &type) -> hdsdp_retcode {
+        const int s0 = Ap[col], s1 = Ap[col + 1];
+        std::vector<std::pair<long, double>> ent;
+        ent.reserve(s1 - s0);
+        for (int e = s0; e < s1; ++e) {
+            if (Ai[e] < 0 || Ai[e] >= npack) return HDSDP_RETCODE_FAILED;
+            ent.push_back({(long) Ai[e], Ax[e]});
+        }
+        std::stable_sort(ent.begin(), ent.end(), [](auto &x, auto &y) { return x.first < y.first; });
+        const int nnz = (int) ent.size();
+        h.r.resize(nnz);
+        h.c.resize(nnz);
+        h.v.resize(nnz);
+        for (int e = 0; e < nnz; ++e) {
+            unpack(n, ent[e].first, h.r[e], h.c[e]);
+            h.v[e] = ent[e].second;
+        }
+        // sdpDataMatSetData (linalg/hdsdp_sdpdata.c:2262-2286)
+        if (nnz == 0) type = REF_ZERO;
+        else if (nnz > 0.3 * npack) {
+            type = REF_DENSE;
+            h.dense_packed = true;
+            h.packed.assign(npack, 0.0);
+            for (auto &p : ent) h.packed[p.first] = p.second;
+        } else type = REF_SPARSE;
+        return HDSDP_RETCODE_OK;
+    };
+    if (load(0, C, refTypeC) != HDSDP_RETCODE_OK) return HDSDP_RETCODE_FAILED;
+    stats[refTypeC] += 1;
+    for (int i = 0; i < m; ++i) {
+        if (load(i + 1, A[i], refType[i]) != HDSDP_RETCODE_OK) return HDSDP_RETCODE_FAILED;
+        stats[refType[i]] += 1;
+    }
+    return HDSDP_RETCODE_OK;
+}
+
+// sdpDenseConePresolveImpl (interface/hdsdp_conic_sdp.c:1486-1514): rank-one detection.
+hdsdp_retcode SdpCone::presolve() {
+    auto eig = [&](HostCoeff &h, int &type) {
+        double sgn = 0.0;
+        std::vector<double> a;
+        bool r1 = false;
+        if (type == REF_SPARSE) r1 = sparse_rank_one(n, h.r, h.c, h.v, sgn, a);
+        else if (type == REF_DENSE) r1 = dense_rank_one(n, h.packed, sgn, a);
+        if (!r1) return;
+        int nz = 0;
+        for (int q = 0; q < n; ++q)
+            if (std::fabs(a[q]) > 1e-10) nz += 1;
+        h.sign = sgn;
+        h.aidx.clear();
+        h.aval.clear();
+        if (nz > 0.5 * n) {
+            type = REF_DSR1;
+            for (int q = 0; q < n; ++q) {
+                h.aidx.push_back(q);
+                h.aval.push_back(a[q]);
+            }
+        } else {
+            type = REF_SPR1;
+            for (int q = 0; q < n; ++q)
+                if (std::fabs(a[q]) > 1e-10) {
+                    h.aidx.push_back(q);
+                    h.aval.push_back(a[q]);
+                }
+        }
+        normalize_r1(h);
+    };
+    eig(C, refTypeC);
+    for (int i = 0; i < m; ++i) {
+        stats[refType[i]] -= 1;
+        eig(A[i], refType[i]);
+        stats[refType[i]] += 1;
+    }
+    // device class per row
+    for (int i = 0; i < m; ++i) {
+        HostCoeff &h = A[i];
+        switch (refType[i]) {
+            case REF_ZERO: h.cls = CLS_ZERO; break;
+            case REF_SPARSE: h.cls = ((int) h.r.size() <= kSpMax) ? CLS_SP : CLS_DR; break;
+            case REF_DENSE: h.cls = CLS_DR; break;
+            case REF_SPR1: h.cls = ((int) h.aidx.size() <= kR1SmallMax) ? CLS_R1S : CLS_R1D; break;
+            case REF_DSR1: h.cls = CLS_R1D; break;
+        }
+    }
+    return HDSDP_RETCODE_OK;
+}
+
+static double coeff_norm_of(const HostCoeff &h, int type, int which) {
+    double nrm = 0.0;
+    if (type == REF_ZERO) return 0.0;
+    if (type == REF_SPARSE || type == REF_DENSE) {
+        for (size_t e = 0; e < h.v.size(); ++e) {
+            const bool diag = h.r[e] == h.c[e];
+            if (which == FRO_NORM) nrm += diag ? h.v[e] * h.v[e] : 2.0 * h.v[e] * h.v[e];
+            else nrm += diag ? std::fabs(h.v[e]) : 2.0 * std::fabs(h.v[e]);
+        }
+        return which == FRO_NORM ? std::sqrt(nrm) : nrm;
+    }
+    // rank one: |sign| * ||a||_2^2 or |sign| * ||a||_1^2 (hdsdp_sdpdata.c:272-309)
+    double s2 = 0.0, s1 = 0.0;
+    for (double x : h.aval) {
+        s2 += x * x;
+        s1 += std::fabs(x);
+    }
+    return which == FRO_NORM ? s2 * std::fabs(h.sign) : s1 * s1 * std::fabs(h.sign);
+}
+
+double SdpCone::obj_norm(int type) const { return coeff_norm_of(C, refTypeC, type); }
+
+double SdpCone::coeff_norm(int type) const {
+    double nrm = 0.0;
+    for (int i = 0; i < m; ++i) {
+        double t = coeff_norm_of(A[i], refType[i], type);
+        nrm += (type == ABS_NORM) ? t : t * t;
+    }
+    return (type == ABS_NORM) ? nrm : std::sqrt(nrm);
+}
+
+void SdpCone::scal(double a) {
+    objScal *= a;
+    if (refTypeC == REF_SPR1 || refTypeC == REF_DSR1) C.sign *= a;
+}
+
+// sdpDenseConeFeatureDetectImpl (interface/hdsdp_conic_sdp.c:2560-2654)
+void SdpCone::detect_feature(const double *rowRHS, int intF[20], double dblF[20]) const {
+    intF[15] = stats[REF_ZERO];
+    intF[17] = stats[REF_DENSE];
+    intF[16] = stats[REF_SPARSE];
+    intF[18] = stats[REF_SPR1];
+    intF[19] = stats[REF_DSR1];
+    auto rank = [&](int i) {
+        if (refType[i] == REF_ZERO) return 0;
+        if (refType[i] == REF_SPR1 || refType[i] == REF_DSR1) return 1;
+        return n;
+    };
+    bool noPrimalInterior = false;
+    for (int i = 0; i < m; ++i)
+        if (rank(i) == 1 && std::fabs(rowRHS[i]) < 1e-03 * coeff_norm_of(A[i], refType[i], FRO_NORM))
+            noPrimalInterior = true;
+    if (noPrimalInterior) intF[2] = 1;
+
+    bool impliedTrace = false;
+    double traceX = 0.0;
+    for (int i = 0; i < m; ++i) {
+        if (refType[i] != REF_SPARSE) continue;
+        const HostCoeff &h = A[i];
+        if ((int) h.v.size() != n) continue;
+        bool eye = true;
+        const double d = h.v[0];
+        for (size_t e = 0; e < h.v.size(); ++e)
+            if (h.r[e] != h.c[e] || h.v[e] != d) { eye = false; break; }
+        if (eye && rowRHS[i] / d > 0.0) {
+            impliedTrace = true;
+            traceX = rowRHS[i] / d;
+            break;
+        }
+    }
+    // The reference resets the estimate here before storing it (conic_sdp.c:2622).
+    traceX = 0.0;
+    std::vector<int> unitCol(std::max(m, n), 0);
+    if (!impliedTrace) {
+        for (int i = 0; i < m; ++i) {
+            const HostCoeff &h = A[i];
+            if (refType[i] == REF_SPR1 && h.aidx.size() == 1 && h.aval[0] == 1.0 && h.sign == 1.0 &&
+                !unitCol[h.aidx[0]]) {
+                unitCol[h.aidx[0]] = 1;
+                traceX += rowRHS[i];
+            }
+        }
+    }
+    int nSumUnit = 0;
+    for (int i = 0; i < m; ++i) nSumUnit += unitCol[i];
+    if (nSumUnit == n) impliedTrace = true;
+    if (impliedTrace) {
+        intF[5] = 1;
+        dblF[11] = traceX;
+    }
+    if (stats[REF_DENSE] >= 0.7 * m) intF[4] = 1;
+}
+
+hdsdp_retcode SdpCone::setup_device(cudaStream_t stream, Timers *t) {
+    s = stream;
+    tm = t;
+    ld = pad_ld(n);
+    // device copy of the (scaled) objective from its lower triplets
+    HostCoeff Cdev = C;
+    for (double &v : Cdev.v) v *= objScal;
+    dev.upload(n, m, Cdev, A, s);
+    HB_CUDA(cudaMalloc(&Svar, sizeof(double) * ld * n));
+    HB_CUDA(cudaMalloc(&Scheck, sizeof(double) * ld * n));
+    HB_CUDA(cudaMalloc(&dS, sizeof(double) * ld * n));
+    HB_CUDA(cudaMalloc(&W, sizeof(double) * ld * n));
+    HB_CUDA(cudaMemsetAsync(Svar, 0, sizeof(double) * ld * n, s));
+    HB_CUDA(cudaMemsetAsync(Scheck, 0, sizeof(double) * ld * n, s));
+    HB_CUDA(cudaMemsetAsync(dS, 0, sizeof(double) * ld * n, s));
+    Fvar.alloc(n);
+    Fcheck.alloc(n);
+    lz.init(n, s);
+    HB_CUDA(cudaMalloc(&d_y, sizeof(double) * std::max(m, 1)));
+    HB_CUDA(cudaMalloc(&d_vec, sizeof(double) * std::max(m, 1)));
+    HB_CUDA(cudaMallocHost(&h_vec, sizeof(double) * std::max(m, 1)));
+    HB_CUDA(cudaMalloc(&d_scal, sizeof(double) * 8));
+    HB_CUDA(cudaMallocHost(&h_scal, sizeof(double) * 8));
+    HB_CUDA(cudaStreamSynchronize(s));
+    return device_error_flag() ? HDSDP_RETCODE_MEMORY : HDSDP_RETCODE_OK;
+}
+
+void SdpCone::release() {
+    dev.release();
+    auto f = [](void *p) { if (p) cudaFree(p); };
+    f(Svar); f(Scheck); f(dS); f(W); f(d_y); f(d_vec); f(d_scal);
+    if (h_vec) cudaFreeHost(h_vec);
+    if (h_scal) cudaFreeHost(h_scal);
+    Svar = Scheck = dS = W = d_y = d_vec = d_scal = h_vec = h_scal = nullptr;
+    Fvar.release();
+    Fcheck.release();
+    lz.release();
+}
+
+// target = dC*C + dAs*sum_i y_i A_i + (dEye [+ perturbation])*I
+// (sdpDenseConeIUpdateBuffer, interface/hdsdp_conic_sdp.c:343-402)
+void SdpCone::update_buffer(double dC, double dAs, const double *y, double dEye, int which) {
+    double t0 = wall();
+    double *target = (which == BUFFER_DUALVAR) ? Svar : (which == BUFFER_DUALCHECK) ? Scheck : dS;
+    if (which != BUFFER_DUALSTEP) dEye += dualPerturb;
+    std::memcpy(h_vec, y, sizeof(double) * m);
+    HB_CUDA(cudaMemcpyAsync(d_y, h_vec, sizeof(double) * m, cudaMemcpyHostToDevice, s));
+    dev.assemble(dC, dAs, d_y, dEye, target, ld);
+    if (tm) tm->assemble += wall() - t0;
+}
+
+hdsdp_retcode SdpCone::update(double tau, const double *y) {
+    update_buffer(tau, -1.0, y, -dualResidual, BUFFER_DUALVAR);
+    return HDSDP_RETCODE_OK;
+}
+
+static bool timed_factor(cudaStream_t s, DenseFactor &F, const double *S, long ld, Timers *tm) {
+    double t0 = wall();
+    bool ok = factorize(s, F, S, ld);
+    if (tm) {
+        tm->s_factor += wall() - t0;
+        tm->n_sfactor += 1;
+    }
+    return ok;
+}
+
+hdsdp_retcode SdpCone::ratio_test(double dtau, const double *dy, double ada, int which, double *step) {
+    update_buffer(dtau, -1.0, dy, ada * dualResidual, BUFFER_DUALSTEP);
+    DenseFactor &F = (which == BUFFER_DUALVAR) ? Fvar : Fcheck;
+    if (n == 1) {
+        double vals[2];
+        HB_CUDA(cudaMemcpyAsync(&vals[0], dS, sizeof(double), cudaMemcpyDeviceToHost, s));
+        HB_CUDA(cudaMemcpyAsync(&vals[1], (which == BUFFER_DUALVAR) ? Svar : Scheck, sizeof(double),
+                                cudaMemcpyDeviceToHost, s));
+        HB_CUDA(cudaStreamSynchronize(s));
+        *step = (vals[0] > 0.0) ? HDSDP_INFINITY : (-vals[1] / vals[0]);
+        return HDSDP_RETCODE_OK;
+    }
+    return lz.solve(F, dS, ld, step, tm);
+}
+
+hdsdp_retcode SdpCone::interior_check(double tau, const double *y, int *interior) {
+    update(tau, y);
+    *interior = timed_factor(s, Fvar, Svar, ld, tm) ? 1 : 0;
+    return device_error_flag() ? HDSDP_RETCODE_FAILED : HDSDP_RETCODE_OK;
+}
+
+hdsdp_retcode SdpCone::interior_check_expert(double dC, double dAs, const double *y, double dEye, int which,
+                                             int *interior) {
+    update_buffer(dC, dAs, y, dEye, which);
+    if (which == BUFFER_DUALVAR) *interior = timed_factor(s, Fvar, Svar, ld, tm) ? 1 : 0;
+    else *interior = timed_factor(s, Fcheck, Scheck, ld, tm) ? 1 : 0;
+    return device_error_flag() ? HDSDP_RETCODE_FAILED : HDSDP_RETCODE_OK;
+}
+
+hdsdp_retcode SdpCone::get_barrier(double tau, const double *y, int which, double *logdet) {
+    DenseFactor &F = (which == BUFFER_DUALVAR) ? Fvar : Fcheck;
+    if (y) {
+        update(tau, y);
+        if (!timed_factor(s, Fvar, Svar, ld, tm)) return HDSDP_RETCODE_FAILED;
+    }
+    log_diag_sum(s, F, d_scal);
+    HB_CUDA(cudaMemcpyAsync(h_scal, d_scal, sizeof(double), cudaMemcpyDeviceToHost, s));
+    HB_CUDA(cudaStreamSynchronize(s));
+    *logdet = 2.0 * h_scal[0];
+    return HDSDP_RETCODE_OK;
+}
+
+hdsdp_retcode SdpCone::add_step_and_check(double step, int which, int *interior) {
+    if (which == BUFFER_DUALVAR) {
+        axpy(s, (int) (ld * n), step, dS, Svar);
+        *interior = timed_factor(s, Fvar, Svar, ld, tm) ? 1 : 0;
+    } else {
+        HB_CUDA(cudaMemcpyAsync(Scheck, Svar, sizeof(double) * ld * n, cudaMemcpyDeviceToDevice, s));
+        axpy(s, (int) (ld * n), step, dS, Scheck);
+        *interior = timed_factor(s, Fcheck, Scheck, ld, tm) ? 1 : 0;
+    }
+    return device_error_flag() ? HDSDP_RETCODE_FAILED : HDSDP_RETCODE_OK;
+}
+
+// X = mu * (S^-1 + S^-1 (A^* dy) S^-1) at S = C - A^T y (+ perturbation), computed as
+// mu * K^T (K dS K^T + I) K with K = L^-1 (sdpDenseConeGetPrimal, conic_sdp.c:2328-2379).
+void SdpCone::get_primal(double mu, const double *y, const double *dy, double *X) {
+    double t0 = wall();
+    int interior = 0;
+    interior_check_expert(1.0, -1.0, y, 0.0, BUFFER_DUALCHECK, &interior);
+    if (!interior) {
+        printf("Recovery step is infeasible\n");
+        return;
+    }
+    update_buffer(0.0, 1.0, dy, 0.0, BUFFER_DUALSTEP);
+    compute_inverse_factor(s, Fcheck);
+    double *T1 = dev.T1, *T2 = dev.T2;
+    const double *K = Fcheck.K;
+    gemm(s, n, n, n, 1.0, K, ld, 0, dS, ld, 0, 0.0, T1, ld, GEMM_A_LOWER);                    // K dS
+    gemm(s, n, n, n, 1.0, T1, ld, 0, K, ld, 1, 0.0, T2, ld, GEMM_B_UPPER);                    // (K dS) K^T
+    add_diag(s, n, T2, ld, 1.0);
+    symmetrize_avg(s, n, T2, ld);
+    gemm(s, n, n, n, 1.0, T2, ld, 0, K, ld, 0, 0.0, T1, ld, GEMM_B_LOWER);                    // T2 K
+    gemm(s, n, n, n, mu, K, ld, 1, T1, ld, 0, 0.0, X, ld, GEMM_A_UPPER);                      // K^T T2 K
+    symmetrize_avg(s, n, X, ld);
+    HB_CUDA(cudaStreamSynchronize(s));
+    if (tm) tm->primal += wall() - t0;
+}
+
+void SdpCone::get_dual(double *S) {
+    HB_CUDA(cudaMemcpyAsync(S, Svar, sizeof(double) * ld * n, cudaMemcpyDeviceToDevice, s));
+}
+
+void SdpCone::atimesx(const double *X, double *out) {
+    dev.inner_all(X, ld, d_vec);
+    HB_CUDA(cudaMemcpyAsync(h_vec, d_vec, sizeof(double) * m, cudaMemcpyDeviceToHost, s));
+    HB_CUDA(cudaStreamSynchronize(s));
+    std::memcpy(out, h_vec, sizeof(double) * m);
+}
+
+double SdpCone::trace_cx(const double *X) { return dev.c_inner(X, ld); }
+
+// ======================================================================================
+// Scalar bound cone (interface/hdsdp_conic_bound.c)
+// ======================================================================================
+void BoundCone::proc(int m_, double l, double u) {
+    m = m_;
+    lo = l;
+    up = u;
+    for (auto *v : {&dl, &du, &dlInv, &duInv, &dlStep, &duStep, &dlChk, &duChk}) v->assign(m, 0.0);
+}
+
+void BoundCone::update_buffer(double dC, double dAs, const double *y, int which) {
+    std::vector<double> &L = (which == BUFFER_DUALVAR) ? dl : (which == BUFFER_DUALCHECK) ? dlChk : dlStep;
+    std::vector<double> &U = (which == BUFFER_DUALVAR) ? du : (which == BUFFER_DUALCHECK) ? duChk : duStep;
+    for (int i = 0; i < m; ++i) {
+        U[i] = dC * up + dAs * y[i];
+        L[i] = -dC * lo - dAs * y[i];
+    }
+}
+
+double BoundCone::ratio_test(double dtau, const double *dy, int which) {
+    update_buffer(dtau, -1.0, dy, BUFFER_DUALSTEP);
+    const std::vector<double> &L = (which == BUFFER_DUALVAR) ? dl : dlChk;
+    const std::vector<double> &U = (which == BUFFER_DUALVAR) ? du : duChk;
+    double mx = 0.0;
+    for (int i = 0; i < m; ++i) {
+        mx = std::min(mx, dlStep[i] / L[i]);
+        mx = std::min(mx, duStep[i] / U[i]);
+    }
+    mx = 1.0 / mx;
+    return (mx > 0.0) ? 100.0 : -mx;
+}
+
+int BoundCone::interior_check(double tau, const double *y) {
+    update(tau, y);
+    for (int i = 0; i < m; ++i)
+        if (dl[i] <= 0.0) return 0;
+    for (int i = 0; i < m; ++i)
+        if (du[i] <= 0.0) return 0;
+    return 1;
+}
+
+int BoundCone::interior_check_expert(double dC, double dAs, const double *y, int which) {
+    update_buffer(dC, dAs, y, which);
+    const std::vector<double> &L = (which == BUFFER_DUALVAR) ? dl : dlChk;
+    const std::vector<double> &U = (which == BUFFER_DUALVAR) ? du : duChk;
+    for (int i = 0; i < m; ++i)
+        if (L[i] <= 0.0) return 0;
+    for (int i = 0; i < m; ++i)
+        if (U[i] <= 0.0) return 0;
+    return 1;
+}
+
+hdsdp_retcode BoundCone::get_barrier(double tau, const double *y, int which, double *logdet) {
+    const std::vector<double> &L = (which == BUFFER_DUALVAR) ? dl : dlChk;
+    const std::vector<double> &U = (which == BUFFER_DUALVAR) ? du : duChk;
+    if (y) update(tau, y);
+    double ld = 0.0;
+    for (int i = 0; i < m; ++i) ld += std::log(L[i]) + std::log(U[i]);
+    if (ld != ld) {
+        printf("Bound constraint is violated\n");
+        return HDSDP_RETCODE_FAILED;
+    }
+    *logdet = ld;
+    return HDSDP_RETCODE_OK;
+}
+
+int BoundCone::add_step_and_check(double step, int which) {
+    std::vector<double> &L = (which == BUFFER_DUALVAR) ? dl : dlChk;
+    std::vector<double> &U = (which == BUFFER_DUALVAR) ? du : duChk;
+    if (which != BUFFER_DUALVAR) {
+        dlChk = dl;
+        duChk = du;
+    }
+    for (int i = 0; i < m; ++i) {
+        L[i] += step * dlStep[i];
+        U[i] += step * duStep[i];
+        if (L[i] <= 0.0 || U[i] <= 0.0) return 0;
+    }
+    return 1;
+}
+
+void BoundCone::get_primal(double mu, const double *y, const double *dy, double *lower, double *upper) const {
+    for (int i = 0; i < m; ++i) {
+        const double st = -dy[i];
+        const double su = up - y[i];
+        const double sl = y[i] - lo;
+        lower[i] = mu * (1.0 / sl - st / (sl * sl));
+        upper[i] = mu * (1.0 / su + st / (su * su));
+    }
+}
+
+// ======================================================================================
+// Schur complement system
+// ======================================================================================
+void KKT::init(int m_, cudaStream_t stream, Timers *t) {
+    m = m_;
+    s = stream;
+    tm = t;
+    ldm = pad_ld(m);
+    HB_CUDA(cudaMalloc(&M, sizeof(double) * ldm * m));
+    HB_CUDA(cudaMemsetAsync(M, 0, sizeof(double) * ldm * m, s));
+    F.alloc(m);
+    asinv.assign(m, 0.0);
+    asinvrd.assign(m, 0.0);
+    asinvcs.assign(m, 0.0);
+    diag_add.assign(m, 0.0);
+    for (double **p : {&d_rhs, &d_x, &d_r, &d_t, &d_diag}) HB_CUDA(cudaMalloc(p, sizeof(double) * m));
+    HB_CUDA(cudaMallocHost(&h_buf, sizeof(double) * m));
+}
+
+void KKT::release() {
+    if (M) cudaFree(M);
+    M = nullptr;
+    F.release();
+    for (double **p : {&d_rhs, &d_x, &d_r, &d_t, &d_diag}) {
+        if (*p) cudaFree(*p);
+        *p = nullptr;
+    }
+    if (h_buf) cudaFreeHost(h_buf);
+    h_buf = nullptr;
+}
+
+void KKT::clean(int type) {
+    std::fill(asinv.begin(), asinv.end(), 0.0);
+    std::fill(asinvrd.begin(), asinvrd.end(), 0.0);
+    if (type == KKT_TYPE_HOMOGENEOUS) {
+        std::fill(asinvcs.begin(), asinvcs.end(), 0.0);
+        dCSinv = dCSinvCSinv = dCSinvRdSinv = 0.0;
+    }
+    dTraceSinv = 0.0;
+}
+
+static void add_host(std::vector<double> &dst, const double *d_src, double *h_buf, int m, double scale,
+                     cudaStream_t s) {
+    HB_CUDA(cudaMemcpyAsync(h_buf, d_src, sizeof(double) * m, cudaMemcpyDeviceToHost, s));
+    HB_CUDA(cudaStreamSynchronize(s));
+    for (int i = 0; i < m; ++i) dst[i] += scale * h_buf[i];
+}
+
+// sdpDenseConeGetKKT / GetKKTByFixedStrategy (interface/hdsdp_conic_sdp.c:1722-1872)
+hdsdp_retcode KKT::build(SdpCone &cone, int type) {
+    double t0 = wall();
+    clean(type);
+    const int n = cone.n;
+    const long ld = cone.ld;
+    const double r = cone.dualResidual;
+    const double *Wp = nullptr;
+    if (type == KKT_TYPE_PRIMAL) {
+        if (!primalX) return HDSDP_RETCODE_FAILED;
+        Wp = primalX;
+    } else {
+        double ti = wall();
+        compute_inverse(s, cone.Fvar, cone.W, ld);
+        if (tm) {
+            HB_CUDA(cudaStreamSynchronize(s));
+            tm->s_inverse += wall() - ti;
+        }
+        Wp = cone.W;
+    }
+    SdpDevice &dev = cone.dev;
+    if (type == KKT_TYPE_CORRECTOR) {
+        dev.inner_all(Wp, ld, cone.d_vec);
+        add_host(asinv, cone.d_vec, h_buf, m, 1.0, s);
+        if (r != 0.0) {
+            dev.inner_all_sq(Wp, ld, cone.d_vec);
+            add_host(asinvrd, cone.d_vec, h_buf, m, r, s);
+        }
+        if (tm) tm->schur += wall() - t0;
+        return device_error_flag() ? HDSDP_RETCODE_FAILED : HDSDP_RETCODE_OK;
+    }
+    if (r != 0.0) {
+        trace(s, n, Wp, ld, cone.d_scal);
+        HB_CUDA(cudaMemcpyAsync(cone.h_scal, cone.d_scal, sizeof(double), cudaMemcpyDeviceToHost, s));
+        HB_CUDA(cudaStreamSynchronize(s));
+        dTraceSinv += cone.h_scal[0];
+    }
+    dev.schur_matrix(Wp, ld, M, ldm);
+    dev.inner_all(Wp, ld, cone.d_vec);
+    add_host(asinv, cone.d_vec, h_buf, m, 1.0, s);
+    if (r != 0.0) {
+        dev.inner_all_sq(Wp, ld, cone.d_vec);
+        add_host(asinvrd, cone.d_vec, h_buf, m, r, s);
+    }
+    if (type == KKT_TYPE_HOMOGENEOUS) {
+        // B = W C W; <A_i, B>, <C, W>, <C, B>, r * tr(B)
+        gemm(s, n, n, n, 1.0, dev.Cfull, dev.ld, 0, Wp, ld, 0, 0.0, dev.T1, dev.ld, 0);
+        gemm(s, n, n, n, 1.0, Wp, ld, 0, dev.T1, dev.ld, 0, 0.0, dev.T2, dev.ld, 0);
+        symmetrize_avg(s, n, dev.T2, dev.ld);
+        dev.inner_all(dev.T2, dev.ld, cone.d_vec);
+        add_host(asinvcs, cone.d_vec, h_buf, m, 1.0, s);
+        dCSinv += dev.c_inner(Wp, ld);
+        dCSinvCSinv += dev.c_inner(dev.T2, dev.ld);
+        if (r != 0.0) {
+            trace(s, n, dev.T2, dev.ld, cone.d_scal);
+            HB_CUDA(cudaMemcpyAsync(cone.h_scal, cone.d_scal, sizeof(double), cudaMemcpyDeviceToHost, s));
+            HB_CUDA(cudaStreamSynchronize(s));
+            dCSinvRdSinv += r * cone.h_scal[0];
+        }
+    }
+    HB_CUDA(cudaStreamSynchronize(s));
+    if (tm) {
+        tm->schur += wall() - t0;
+        tm->n_schur += 1;
+    }
+    return device_error_flag() ? HDSDP_RETCODE_FAILED : HDSDP_RETCODE_OK;
+}
+
+// sBoundConeGetKKT (interface/hdsdp_conic_bound.c:199-241)
+void KKT::add_bound(BoundCone &b, int type) {
+    for (int i = 0; i < b.m; ++i) {
+        b.dlInv[i] = 1.0 / b.dl[i];
+        b.duInv[i] = 1.0 / b.du[i];
+    }
+    for (int i = 0; i < m; ++i) {
+        asinv[i] -= b.dlInv[i];
+        asinv[i] += b.duInv[i];
+    }
+    if (type == KKT_TYPE_CORRECTOR) return;
+    for (int i = 0; i < b.m; ++i) h_buf[i] = b.dlInv[i] * b.dlInv[i] + b.duInv[i] * b.duInv[i];
+    HB_CUDA(cudaMemcpyAsync(d_diag, h_buf, sizeof(double) * m, cudaMemcpyHostToDevice, s));
+    add_diag_vec(s, m, M, ldm, d_diag);
+    HB_CUDA(cudaStreamSynchronize(s));
+    if (type == KKT_TYPE_HOMOGENEOUS) {
+        for (int i = 0; i < b.m; ++i) {
+            dCSinv += b.up * b.duInv[i];
+            double sq = b.duInv[i] * b.duInv[i];
+            asinvcs[i] += b.up * sq;
+            dCSinvCSinv += b.up * b.up * sq;
+            dCSinv -= b.lo * b.dlInv[i];
+            sq = b.dlInv[i] * b.dlInv[i];
+            asinvcs[i] += b.lo * sq;
+            dCSinvCSinv += b.lo * b.lo * sq;
+        }
+    }
+}
+
+// HKKTRegularize (interface/hdsdp_schur.c:348-373)
+void KKT::regularize(double reg) {
+    copy_matrix(s, 1, m, M, ldm + 1, d_t, 1);
+    HB_CUDA(cudaMemcpyAsync(h_buf, d_t, sizeof(double) * m, cudaMemcpyDeviceToHost, s));
+    HB_CUDA(cudaStreamSynchronize(s));
+    double mn = HDSDP_INFINITY;
+    for (int i = 0; i < m; ++i) mn = std::min(mn, h_buf[i]);
+    reg = reg * mn;
+    reg = std::min(reg, 1e-05);
+    if (reg < 1e-14) reg = 0.0;
+    if (reg != 0.0) add_diag(s, m, M, ldm, reg);
+}
+
+hdsdp_retcode KKT::factorize() {
+    double t0 = wall();
+    symmetrize_lower(s, m, M, ldm);
+    shift = 0.0;
+    bool ok = hb::factorize(s, F, M, ldm);
+    if (!ok) {
+        // The reference switches to an LDL^T factorisation here (linsolver.c:1373-1377);
+        // this build retries the Cholesky with a small diagonal shift instead.
+        copy_matrix(s, 1, m, M, ldm + 1, d_t, 1);
+        HB_CUDA(cudaMemcpyAsync(h_buf, d_t, sizeof(double) * m, cudaMemcpyDeviceToHost, s));
+        HB_CUDA(cudaStreamSynchronize(s));
+        double mx = 0.0;
+        for (int i = 0; i < m; ++i) mx = std::max(mx, std::fabs(h_buf[i]));
+        for (double eps = 1e-14; eps <= 1e-6 && !ok; eps *= 100.0) {
+            add_diag(s, m, M, ldm, eps * std::max(mx, 1.0));
+            shift += eps * std::max(mx, 1.0);
+            ok = hb::factorize(s, F, M, ldm);
+        }
+        if (ok) printf("KKT system is almost indefinite. Using a shifted Cholesky factor. \n");
+    }
+    if (ok) compute_inverse_factor(s, F);
+    HB_CUDA(cudaStreamSynchronize(s));
+    if (tm) tm->schur_factor += wall() - t0;
+    return ok && !device_error_flag() ? HDSDP_RETCODE_OK : HDSDP_RETCODE_FAILED;
+}
+
+// x = M^-1 b with one step of iterative refinement on the FP64 residual.
+hdsdp_retcode KKT::solve(const double *rhs, double *lhs) {
+    double t0 = wall();
+    std::memcpy(h_buf, rhs, sizeof(double) * m);
+    HB_CUDA(cudaMemcpyAsync(d_rhs, h_buf, sizeof(double) * m, cudaMemcpyHostToDevice, s));
+    coldot(s, m, m, F.KT, F.ld, d_rhs, d_t, 1.0, 0.0, 2);   // t = K b
+    coldot(s, m, m, F.K, F.ld, d_t, d_x, 1.0, 0.0, 1);      // x = K^T t
+    HB_CUDA(cudaMemcpyAsync(d_r, d_rhs, sizeof(double) * m, cudaMemcpyDeviceToDevice, s));
+    coldot(s, m, m, M, ldm, d_x, d_r, -1.0, 1.0, 0);        // r = b - M x
+    if (shift != 0.0) axpy(s, m, shift, d_x, d_r);          // residual of the unshifted system
+    coldot(s, m, m, F.KT, F.ld, d_r, d_t, 1.0, 0.0, 2);
+    coldot(s, m, m, F.K, F.ld, d_t, d_r, 1.0, 0.0, 1);
+    axpy(s, m, 1.0, d_r, d_x);
+    HB_CUDA(cudaMemcpyAsync(h_buf, d_x, sizeof(double) * m, cudaMemcpyDeviceToHost, s));
+    HB_CUDA(cudaStreamSynchronize(s));
+    std::memcpy(lhs, h_buf, sizeof(double) * m);
+    if (tm) {
+        tm->schur_solve += wall() - t0;
+        tm->n_schur_solve += 1;
+    }
+    return device_error_flag() ? HDSDP_RETCODE_FAILED : HDSDP_RETCODE_OK;
+}
+
+// ======================================================================================
+// Lanczos (linalg/hdsdp_lanczos.c:161-292)
+// ======================================================================================
+namespace {
+__device__ double bsum(double v) {
+    __shared__ double red[32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) red[w] = v;
+    __syncthreads();
+    const int nw = (blockDim.x + 31) >> 5;
+    v = (threadIdx.x < nw) ? red[threadIdx.x] : 0.0;
+    if (w == 0) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (threadIdx.x == 0) red[0] = v;
+    }
+    __syncthreads();
+    v = red[0];
+    __syncthreads();
+    return v;
+}
+
+// One Lanczos orthogonalisation step; single block.
+__global__ void lanczos_orth_kernel(int n, double *V, long ldv, int k, double *w, double *ab, int maxdim) {
+    const double *vk = V + (size_t) k * ldv;
+    if (k > 0) {
+        const double h = ab[maxdim + k - 1];
+        const double *vp = V + (size_t) (k - 1) * ldv;
+        for (int i = threadIdx.x; i < n; i += blockDim.x) w[i] -= h * vp[i];
+        __syncthreads();
+    }
+    double acc = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) acc += w[i] * vk[i];
+    const double alp = bsum(acc);
+    acc = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const double x = w[i] - alp * vk[i];
+        w[i] = x;
+        acc += x * x;
+    }
+    const double nrm = sqrt(bsum(acc));
+    if (threadIdx.x == 0) ab[k] = alp;
+    if (nrm > 0.0) {
+        double *vn = V + (size_t) (k + 1) * ldv;
+        for (int i = threadIdx.x; i < n; i += blockDim.x) vn[i] = w[i] / nrm;
+        if (threadIdx.x == 0) ab[maxdim + k] = nrm;
+    }
+}
+
+// v = (a ? a : 0) + b, then normalise into V[:,0]; single block.
+__global__ void lanczos_start_kernel(int n, const double *a, const double *b, double *V) {
+    double acc = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const double x = (a ? a[i] : 0.0) + b[i];
+        V[i] = x;
+        acc += x * x;
+    }
+    const double nrm = sqrt(bsum(acc));
+    for (int i = threadIdx.x; i < n; i += blockDim.x) V[i] = (nrm > 0.0) ? V[i] / nrm : 0.0;
+}
+
+// z = V[:, 0..k] * y
+__global__ void lanczos_combine_kernel(int n, const double *V, long ldv, int kp1, const double *y, double *z) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double acc = 0.0;
+        for (int j = 0; j < kp1; ++j) acc += V[(size_t) i + (size_t) j * ldv] * y[j];
+        z[i] = acc;
+    }
+}
+
+// z -= lam * x; out = ||z||; single block
+__global__ void lanczos_resid_kernel(int n, double *z, const double *x, double lam, double *out) {
+    double acc = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const double t = z[i] - lam * x[i];
+        z[i] = t;
+        acc += t * t;
+    }
+    const double v = sqrt(bsum(acc));
+    if (threadIdx.x == 0) *out = v;
+}
+
+// Eigen-decomposition of a small symmetric matrix by cyclic Jacobi rotations.
+void jacobi_eig(int n, std::vector<double> &A, std::vector<double> &evals, std::vector<double> &evecs) {
+    evecs.assign((size_t) n * n, 0.0);
+    for (int i = 0; i < n; ++i) evecs[(size_t) i * n + i] = 1.0;
+    auto a = [&](int i, int j) -> double & { return A[(size_t) i + (size_t) j * n]; };
+    auto v = [&](int i, int j) -> double & { return evecs[(size_t) i + (size_t) j * n]; };
+    for (int sweep = 0; sweep < 100; ++sweep) {
+        double off = 0.0, tot = 0.0;
+        for (int i = 0; i < n; ++i)
+            for (int j = 0; j < n; ++j) {
+                tot += a(i, j) * a(i, j);
+                if (i != j) off += a(i, j) * a(i, j);
+            }
+        if (off <= 1e-32 * tot || off == 0.0) break;
+        for (int p = 0; p < n - 1; ++p)
+            for (int q = p + 1; q < n; ++q) {
+                const double apq = a(p, q);
+                if (apq == 0.0) continue;
+                const double theta = (a(q, q) - a(p, p)) / (2.0 * apq);
+                const double t = (theta >= 0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
+                const double c = 1.0 / std::sqrt(t * t + 1.0), sn = t * c;
+                for (int k = 0; k < n; ++k) {
+                    const double akp = a(k, p), akq = a(k, q);
+                    a(k, p) = c * akp - sn * akq;
+                    a(k, q) = sn * akp + c * akq;
+                }
+                for (int k = 0; k < n; ++k) {
+                    const double apk = a(p, k), aqk = a(q, k);
+                    a(p, k) = c * apk - sn * aqk;
+                    a(q, k) = sn * apk + c * aqk;
+                }
+                for (int k = 0; k < n; ++k) {
+                    const double vkp = v(k, p), vkq = v(k, q);
+                    v(k, p) = c * vkp - sn * vkq;
+                    v(k, q) = sn * vkp + c * vkq;
+                }
+            }
+    }
+    evals.resize(n);
+    for (int i = 0; i < n; ++i) evals[i] = a(i, i);
+}
+}  // namespace
+
+void Lanczos::init(int n_, cudaStream_t s_) {
+    n = n_;
+    s = s_;
+    ld = pad_ld(n);
+    HB_CUDA(cudaMalloc(&V, sizeof(double) * ld * (maxdim + 1)));
+    for (double **p : {&w, &z1, &z2, &t1, &warm, &init_vec, &pert_vec}) HB_CUDA(cudaMalloc(p, sizeof(double) * ld));
+    HB_CUDA(cudaMalloc(&d_ab, sizeof(double) * (2 * maxdim + 2)));
+    HB_CUDA(cudaMallocHost(&h_ab, sizeof(double) * (2 * maxdim + 2)));
+    HB_CUDA(cudaMalloc(&d_y, sizeof(double) * 2 * (maxdim + 1)));
+    HB_CUDA(cudaMalloc(&d_scal, sizeof(double) * 4));
+    HB_CUDA(cudaMallocHost(&h_scal, sizeof(double) * 4));
+    // Deterministic start and perturbation vectors: srand(n) then, per entry,
+    // srand(rand()) and sqrt(sqrt(rand() % 1627)) * (rand() % 2 - 0.5)
+    // (HLanczosIPrepare / HLanczosIPerturb, linalg/hdsdp_lanczos.c:33-53).
+    std::vector<double> h(n);
+    srand(n);
+    for (int i = 0; i < n; ++i) {
+        srand(rand());
+        const int r1 = rand() % 1627;
+        const int r2 = rand() % 2;
+        h[i] = std::sqrt(std::sqrt((double) r1)) * (r2 - 0.5);
+    }
+    HB_CUDA(cudaMemcpy(init_vec, h.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+    srand(n);
+    for (int i = 0; i < n; ++i) {
+        srand(rand());
+        const int r1 = rand() % 1627;
+        const int r2 = rand() % 2;
+        h[i] = 1e-03 * std::sqrt(std::sqrt((double) r1)) * (r2 - 0.5);
+    }
+    HB_CUDA(cudaMemcpy(pert_vec, h.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+    nComputed = 0;
+}
+
+void Lanczos::release() {
+    for (double **p : {&V, &w, &z1, &z2, &t1, &warm, &init_vec, &pert_vec, &d_ab, &d_y, &d_scal}) {
+        if (*p) cudaFree(*p);
+        *p = nullptr;
+    }
+    if (h_ab) cudaFreeHost(h_ab);
+    if (h_scal) cudaFreeHost(h_scal);
+    h_ab = h_scal = nullptr;
+}
+
+hdsdp_retcode Lanczos::solve(DenseFactor &F, const double *D, long ldD, double *maxStep, Timers *tm) {
+    double t0 = wall();
+    compute_inverse_factor(s, F);
+    // buffers: V columns, w (Mv), t1 / z1 / z2 temporaries
+    double *u = nullptr;
+    HB_CUDA(cudaMallocAsync(&u, sizeof(double) * ld, s));
+    auto mv = [&](const double *x, double *y) {
+        coldot(s, n, n, F.K, F.ld, x, t1, 1.0, 0.0, 1);   // t1 = L^-T x
+        coldot(s, n, n, D, ldD, t1, u, -1.0, 0.0, 0);     // u  = -D t1
+        coldot(s, n, n, F.KT, F.ld, u, y, 1.0, 0.0, 2);   // y  = L^-1 u
+        if (tm) tm->n_lanczos_mv += 1;
+    };
+    HB_CUDA(cudaMemsetAsync(V, 0, sizeof(double) * ld * (maxdim + 1), s));
+    HB_CUDA(cudaMemsetAsync(d_ab, 0, sizeof(double) * (2 * maxdim + 2), s));
+    if (nComputed == 0) lanczos_start_kernel<<<1, 1024, 0, s>>>(n, nullptr, init_vec, V);
+    else lanczos_start_kernel<<<1, 1024, 0, s>>>(n, warm, pert_vec, V);
+
+    hdsdp_retcode ret = HDSDP_RETCODE_OK;
+    bool done = false;
+    int lastChecked = -1;
+    const int freq = std::min(maxdim / 5, 3);
+    std::vector<double> T, ev, evec;
+    for (int k = 0; k < maxdim && !done; ++k) {
+        mv(V + (size_t) k * ld, w);
+        lanczos_orth_kernel<<<1, 1024, 0, s>>>(n, V, ld, k, w, d_ab, maxdim);
+        const bool sched = ((k + 1) % freq == 0) || k >= maxdim - 1;
+        if (!sched) continue;
+        HB_CUDA(cudaMemcpyAsync(h_ab, d_ab, sizeof(double) * (2 * maxdim + 2), cudaMemcpyDeviceToHost, s));
+        HB_CUDA(cudaStreamSynchronize(s));
+        // The reference also checks as soon as a step breaks down (zero norm).
+        int kc = k;
+        for (int q = lastChecked + 1; q <= k; ++q)
+            if (h_ab[maxdim + q] == 0.0) { kc = q; break; }
+        lastChecked = k;
+        const int kp1 = kc + 1;
+        if (kp1 < 2) {  // two eigenpairs cannot be extracted from a 1 x 1 problem
+            ret = HDSDP_RETCODE_FAILED;
+            break;
+        }
+        T.assign((size_t) kp1 * kp1, 0.0);
+        for (int i = 0; i < kp1; ++i) {
+            T[(size_t) i + (size_t) i * kp1] = h_ab[i];
+            if (i + 1 < kp1) T[(size_t) (i + 1) + (size_t) i * kp1] = T[(size_t) i + (size_t) (i + 1) * kp1] = h_ab[maxdim + i];
+        }
+        jacobi_eig(kp1, T, ev, evec);
+        int i1 = 0, i2 = 0;  // largest, second largest
+        for (int i = 1; i < kp1; ++i)
+            if (ev[i] > ev[i1]) i1 = i;
+        i2 = (i1 == 0) ? 1 : 0;
+        for (int i = 0; i < kp1; ++i)
+            if (i != i1 && ev[i] > ev[i2]) i2 = i;
+        const double betak = h_ab[maxdim + kc];
+        const double resiVal = std::fabs(betak * evec[(size_t) kc + (size_t) i1 * kp1]);
+        if (!(resiVal < 1e-04 || kc >= maxdim - 1)) {
+            if (kc != k) { done = true; }  // unreachable for a breakdown (resiVal == 0)
+            continue;
+        }
+        const double eigMin1 = ev[i1], eigMin2 = ev[i2];
+        std::vector<double> yy(2 * kp1);
+        for (int i = 0; i < kp1; ++i) {
+            yy[i] = evec[(size_t) i + (size_t) i1 * kp1];
+            yy[kp1 + i] = evec[(size_t) i + (size_t) i2 * kp1];
+        }
+        HB_CUDA(cudaMemcpyAsync(d_y, yy.data(), sizeof(double) * 2 * kp1, cudaMemcpyHostToDevice, s));
+        lanczos_combine_kernel<<<(n + 255) / 256, 256, 0, s>>>(n, V, ld, kp1, d_y, z1);
+        mv(z1, z2);
+        HB_CUDA(cudaMemcpyAsync(warm, z2, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+        lanczos_resid_kernel<<<1, 1024, 0, s>>>(n, z2, z1, eigMin1, d_scal);
+        lanczos_combine_kernel<<<(n + 255) / 256, 256, 0, s>>>(n, V, ld, kp1, d_y + kp1, z2);
+        mv(z2, z1);
+        lanczos_resid_kernel<<<1, 1024, 0, s>>>(n, z1, z2, eigMin1, d_scal + 1);
+        HB_CUDA(cudaMemcpyAsync(h_scal, d_scal, sizeof(double) * 2, cudaMemcpyDeviceToHost, s));
+        HB_CUDA(cudaStreamSynchronize(s));
+        const double resiVal1 = h_scal[0], resiVal2 = h_scal[1];
+        const double resiDiff = eigMin1 - eigMin2 - resiVal2;
+        double valGamma = (resiDiff > 0) ? resiDiff : 1e-16;
+        const double sq = resiVal1 * resiVal1 / valGamma;
+        valGamma = std::min(resiVal1, sq);
+        if (valGamma < 1e-03 || valGamma + eigMin1 <= 0.5) {
+            *maxStep = (valGamma + eigMin1 <= 0.0) ? HDSDP_INFINITY : 1.0 / (valGamma + eigMin1);
+            done = true;
+        } else {
+            if (betak == 0.0) {
+                ret = HDSDP_RETCODE_FAILED;
+                break;
+            }
+            *maxStep = 1.0 / (valGamma + eigMin1);
+            if (kc != k) done = true;
+        }
+    }
+    HB_CUDA(cudaFreeAsync(u, s));
+    HB_CUDA(cudaStreamSynchronize(s));
+    if (ret == HDSDP_RETCODE_OK) nComputed += 1;
+    if (tm) {
+        tm->lanczos += wall() - t0;
+        tm->n_lanczos += 1;
+    }
+    return ret;
+}
+
+}  // namespace hb

@@ -1,0 +1,185 @@
+// Extension entry points of the B200 HDSDP library (include/hdsdp_b200.h).
+#include "solver.h"
+#include "../../include/hdsdp_b200.h"
+#include <cstring>
+#include <cmath>
+#include <vector>
+
+using namespace hb;
+
+extern "C" {
+
+int HDSDPGetStatus(hdsdp *h) { return (int) h->HStatus; }
+int HDSDPGetIterCount(hdsdp *h) { return h->nIterCount; }
+void HDSDPSetPrimalRefinement(hdsdp *h, int on) { h->HIntParams[INT_PARAM_PSDP] = on ? 1 : 0; }
+void HDSDPSetPrecision(hdsdp *h, int mode) { h->precision = mode; }
+
+int HDSDPGetIterLog(hdsdp *h, int maxLen, double *t, double *pObj, double *dObj, double *mu, double *gap,
+                    int *phase) {
+    const int n = (int) h->log.size();
+    for (int i = 0; i < n && i < maxLen; ++i) {
+        const IterRecord &r = h->log[i];
+        if (t) t[i] = r.t;
+        if (pObj) pObj[i] = r.pobj;
+        if (dObj) dObj[i] = r.dobj;
+        if (mu) mu[i] = r.mu;
+        if (gap) gap[i] = r.gap;
+        if (phase) phase[i] = r.phase;
+    }
+    return n;
+}
+
+void HDSDPGetTimers(hdsdp *h, double out[14]) {
+    const Timers &t = h->timers;
+    const double v[14] = {t.schur, t.schur_factor, t.schur_solve, t.s_factor, t.s_inverse, t.lanczos, t.assemble,
+                          t.primal, t.total, (double) t.n_schur, (double) t.n_sfactor, (double) t.n_lanczos,
+                          (double) t.n_lanczos_mv, (double) t.n_schur_solve};
+    std::memcpy(out, v, sizeof(v));
+}
+
+static int probe_setup(SdpCone &c, cudaStream_t s, int m, int n, const int *Ap, const int *Ai, const double *Ax,
+                       int precision) {
+    if (c.proc_data(m, n, Ap, Ai, Ax) != HDSDP_RETCODE_OK) return -1;
+    if (c.presolve() != HDSDP_RETCODE_OK) return -1;
+    c.precision = precision;
+    if (c.setup_device(s, nullptr) != HDSDP_RETCODE_OK) return -1;
+    return 0;
+}
+
+int hdsdpb_schur_probe(int m, int n, const int *Ap, const int *Ai, const double *Ax, const double *y, double resi,
+                       int precision, double *M, double *asinv, double *asinvrd, double *traceSinv) {
+    cudaStream_t s;
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return -1;
+    SdpCone c;
+    KKT k;
+    int ret = probe_setup(c, s, m, n, Ap, Ai, Ax, precision);
+    if (ret == 0) {
+        c.set_start(resi);
+        int interior = 0;
+        c.interior_check(1.0, y, &interior);
+        if (!interior) ret = 1;
+    }
+    if (ret == 0) {
+        k.init(m, s, nullptr);
+        if (k.build(c, KKT_TYPE_INFEASIBLE) != HDSDP_RETCODE_OK) ret = -1;
+        if (ret == 0) {
+            if (M) {
+                std::vector<double> h((size_t) k.ldm * m);
+                cudaMemcpy(h.data(), k.M, sizeof(double) * k.ldm * m, cudaMemcpyDeviceToHost);
+                for (int j = 0; j < m; ++j)
+                    for (int i = 0; i < m; ++i) M[(size_t) j * m + i] = (i >= j) ? h[(size_t) j * k.ldm + i] : 0.0;
+            }
+            std::memcpy(asinv, k.asinv.data(), sizeof(double) * m);
+            std::memcpy(asinvrd, k.asinvrd.data(), sizeof(double) * m);
+            if (traceSinv) *traceSinv = k.dTraceSinv;
+        }
+        k.release();
+    }
+    c.release();
+    cudaStreamDestroy(s);
+    return device_error_flag() ? -1 : ret;
+}
+
+int hdsdpb_ratio_probe(int m, int n, const int *Ap, const int *Ai, const double *Ax, const double *y, double resi,
+                       const double *dy, double ada, double *step, double *logdet) {
+    cudaStream_t s;
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return -1;
+    SdpCone c;
+    int ret = probe_setup(c, s, m, n, Ap, Ai, Ax, 0);
+    if (ret == 0) {
+        c.set_start(resi);
+        int interior = 0;
+        c.interior_check(1.0, y, &interior);
+        if (!interior) ret = 1;
+    }
+    if (ret == 0) {
+        if (c.get_barrier(0.0, nullptr, BUFFER_DUALVAR, logdet) != HDSDP_RETCODE_OK) ret = -1;
+        if (ret == 0 && c.ratio_test(0.0, dy, ada, BUFFER_DUALVAR, step) != HDSDP_RETCODE_OK) ret = -1;
+    }
+    c.release();
+    cudaStreamDestroy(s);
+    return device_error_flag() ? -1 : ret;
+}
+
+int hdsdpb_cholesky(int n, const double *S, double *L, double *logdiag) {
+    cudaStream_t s;
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return -1;
+    const long ld = pad_ld(n);
+    double *dS = nullptr, *dl = nullptr;
+    cudaMalloc(&dS, sizeof(double) * ld * n);
+    cudaMalloc(&dl, sizeof(double));
+    cudaMemcpy2D(dS, sizeof(double) * ld, S, sizeof(double) * n, sizeof(double) * n, n, cudaMemcpyHostToDevice);
+    DenseFactor F;
+    F.alloc(n);
+    const bool ok = factorize(s, F, dS, ld);
+    if (ok) {
+        log_diag_sum(s, F, dl);
+        if (logdiag) cudaMemcpyAsync(logdiag, dl, sizeof(double), cudaMemcpyDeviceToHost, s);
+        if (L) {
+            std::vector<double> h((size_t) ld * n);
+            cudaMemcpyAsync(h.data(), F.L, sizeof(double) * ld * n, cudaMemcpyDeviceToHost, s);
+            cudaStreamSynchronize(s);
+            for (int j = 0; j < n; ++j)
+                for (int i = 0; i < n; ++i) L[(size_t) j * n + i] = (i >= j) ? h[(size_t) j * ld + i] : 0.0;
+        }
+    }
+    cudaStreamSynchronize(s);
+    F.release();
+    cudaFree(dS);
+    cudaFree(dl);
+    cudaStreamDestroy(s);
+    if (device_error_flag()) return -1;
+    return ok ? 0 : 1;
+}
+
+int hdsdpb_inverse(int n, const double *S, double *Sinv) {
+    cudaStream_t s;
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return -1;
+    const long ld = pad_ld(n);
+    double *dS = nullptr, *dW = nullptr;
+    cudaMalloc(&dS, sizeof(double) * ld * n);
+    cudaMalloc(&dW, sizeof(double) * ld * n);
+    cudaMemcpy2D(dS, sizeof(double) * ld, S, sizeof(double) * n, sizeof(double) * n, n, cudaMemcpyHostToDevice);
+    DenseFactor F;
+    F.alloc(n);
+    const bool ok = factorize(s, F, dS, ld);
+    if (ok) {
+        compute_inverse(s, F, dW, ld);
+        cudaMemcpy2DAsync(Sinv, sizeof(double) * n, dW, sizeof(double) * ld, sizeof(double) * n, n,
+                          cudaMemcpyDeviceToHost, s);
+    }
+    cudaStreamSynchronize(s);
+    F.release();
+    cudaFree(dS);
+    cudaFree(dW);
+    cudaStreamDestroy(s);
+    if (device_error_flag()) return -1;
+    return ok ? 0 : 1;
+}
+
+int hdsdpb_gemm(int M, int N, int K, double alpha, const double *A, int lda, int transA, const double *B, int ldb,
+                int transB, double beta, double *C, int ldc) {
+    cudaStream_t s;
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return -1;
+    const int ar = transA ? K : M, ac = transA ? M : K;
+    const int br = transB ? N : K, bc = transB ? K : N;
+    double *dA = nullptr, *dB = nullptr, *dC = nullptr;
+    cudaMalloc(&dA, sizeof(double) * (size_t) lda * ac);
+    cudaMalloc(&dB, sizeof(double) * (size_t) ldb * bc);
+    cudaMalloc(&dC, sizeof(double) * (size_t) ldc * N);
+    cudaMemcpy(dA, A, sizeof(double) * (size_t) lda * ac, cudaMemcpyHostToDevice);
+    cudaMemcpy(dB, B, sizeof(double) * (size_t) ldb * bc, cudaMemcpyHostToDevice);
+    cudaMemcpy(dC, C, sizeof(double) * (size_t) ldc * N, cudaMemcpyHostToDevice);
+    (void) ar;
+    (void) br;
+    gemm(s, M, N, K, alpha, dA, lda, transA, dB, ldb, transB, beta, dC, ldc, 0);
+    cudaMemcpyAsync(C, dC, sizeof(double) * (size_t) ldc * N, cudaMemcpyDeviceToHost, s);
+    cudaStreamSynchronize(s);
+    cudaFree(dA);
+    cudaFree(dB);
+    cudaFree(dC);
+    cudaStreamDestroy(s);
+    return device_error_flag() ? -1 : 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,677 @@
+// Dense FP64 linear algebra kernels for sm_100a.
+//
+// The GEMM issues FP64 tensor-core MMAs (mma.sync m8n8k4 .f64, the DMMA
+// path); Blackwell's tcgen05 has no f64 kind, so this is the FP64 tensor
+// instruction on B200. Every factorisation routine below reduces to this
+// GEMM plus small 64 x 64 kernels.
+#include "la.h"
+#include <cmath>
+#include <algorithm>
+
+namespace hb {
+
+int &device_error_flag() {
+    static int flag = 0;
+    return flag;
+}
+
+// ------------------------------------------------------------------------------------
+// GEMM: 64 x 64 x 16 CTA tile, 4 warps (2 x 2), 32 x 32 warp tile of 8 x 8 DMMA tiles.
+// ------------------------------------------------------------------------------------
+namespace {
+constexpr int BM = 64, BN = 64, BK = 16, GT = 128;
+
+struct GemmP {
+    int M, N, K;
+    double alpha, beta;
+    const double *A;
+    long lda;
+    int ta;
+    const double *B;
+    long ldb;
+    int tb;
+    double *C;
+    long ldc;
+    int flags;
+    const int *abort_flag;
+};
+
+__device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
+__device__ __forceinline__ double load_a(const GemmP &p, int m, int k) {
+    if (m >= p.M || k >= p.K) return 0.0;
+    if ((p.flags & GEMM_A_LOWER) && k > m) return 0.0;
+    if ((p.flags & GEMM_A_UPPER) && k < m) return 0.0;
+    return p.ta ? p.A[(size_t) k + (size_t) m * p.lda] : p.A[(size_t) m + (size_t) k * p.lda];
+}
+
+__device__ __forceinline__ double load_b(const GemmP &p, int k, int n) {
+    if (n >= p.N || k >= p.K) return 0.0;
+    if ((p.flags & GEMM_B_LOWER) && k < n) return 0.0;
+    if ((p.flags & GEMM_B_UPPER) && k > n) return 0.0;
+    return p.tb ? p.B[(size_t) n + (size_t) k * p.ldb] : p.B[(size_t) k + (size_t) n * p.ldb];
+}
+
+__global__ void __launch_bounds__(GT) gemm_kernel(GemmP p) {
+    const int m0 = blockIdx.x * BM;
+    const int n0 = blockIdx.y * BN;
+    if ((p.flags & GEMM_C_LOWER) && m0 + BM - 1 < n0) return;
+    if (p.abort_flag && *p.abort_flag) return;
+
+    int kmin = 0, kmax = p.K;
+    if (p.flags & GEMM_A_LOWER) kmax = min(kmax, m0 + BM);
+    if (p.flags & GEMM_A_UPPER) kmin = max(kmin, m0);
+    if (p.flags & GEMM_B_LOWER) kmin = max(kmin, n0);
+    if (p.flags & GEMM_B_UPPER) kmax = min(kmax, n0 + BN);
+    kmin = (kmin / BK) * BK;
+
+    __shared__ double As[2][BK][BM + 4];
+    __shared__ double Bs[2][BK][BN + 4];
+
+    const int t = threadIdx.x;
+    const int lane = t & 31;
+    const int w = t >> 5;
+    const int wm = (w & 1) * 32;
+    const int wn = (w >> 1) * 32;
+
+    double acc[4][4][2];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+
+    double ra[8], rb[8];
+    auto gload = [&](int k0) {
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            int r, kk;
+            if (!p.ta) { r = t & 63; kk = (t >> 6) + 2 * i; }
+            else { kk = t & 15; r = (t >> 4) + 8 * i; }
+            ra[i] = load_a(p, m0 + r, k0 + kk);
+            int c, kb;
+            if (!p.tb) { kb = t & 15; c = (t >> 4) + 8 * i; }
+            else { c = t & 63; kb = (t >> 6) + 2 * i; }
+            rb[i] = load_b(p, k0 + kb, n0 + c);
+        }
+    };
+    auto sstore = [&](int buf) {
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            int r, kk;
+            if (!p.ta) { r = t & 63; kk = (t >> 6) + 2 * i; }
+            else { kk = t & 15; r = (t >> 4) + 8 * i; }
+            As[buf][kk][r] = ra[i];
+            int c, kb;
+            if (!p.tb) { kb = t & 15; c = (t >> 4) + 8 * i; }
+            else { c = t & 63; kb = (t >> 6) + 2 * i; }
+            Bs[buf][kb][c] = rb[i];
+        }
+    };
+
+    if (kmin < kmax) {
+        gload(kmin);
+        sstore(0);
+        __syncthreads();
+        int buf = 0;
+        for (int k0 = kmin; k0 < kmax; k0 += BK) {
+            const bool more = (k0 + BK) < kmax;
+            if (more) gload(k0 + BK);
+#pragma unroll
+            for (int ks = 0; ks < BK; ks += 4) {
+                double a[4], b[4];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) a[i] = As[buf][ks + (lane & 3)][wm + i * 8 + (lane >> 2)];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) b[j] = Bs[buf][ks + (lane & 3)][wn + j * 8 + (lane >> 2)];
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) dmma(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+            }
+            if (more) sstore(buf ^ 1);
+            __syncthreads();
+            buf ^= 1;
+        }
+    }
+
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int row = m0 + wm + i * 8 + (lane >> 2);
+        if (row >= p.M) continue;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+                const int col = n0 + wn + j * 8 + (lane & 3) * 2 + e;
+                if (col >= p.N) continue;
+                if ((p.flags & GEMM_C_LOWER) && row < col) continue;
+                double *cp = p.C + (size_t) row + (size_t) col * p.ldc;
+                double v = p.alpha * acc[i][j][e];
+                if (p.beta != 0.0) v += p.beta * (*cp);
+                *cp = v;
+            }
+        }
+    }
+}
+}  // namespace
+
+void gemm(cudaStream_t s, int M, int N, int K, double alpha, const double *A, long lda, int transA,
+          const double *B, long ldb, int transB, double beta, double *C, long ldc, int flags,
+          const int *abort_flag) {
+    if (M <= 0 || N <= 0) return;
+    GemmP p{M, N, K, alpha, beta, A, lda, transA, B, ldb, transB, C, ldc, flags, abort_flag};
+    dim3 grid((M + BM - 1) / BM, (N + BN - 1) / BN);
+    gemm_kernel<<<grid, GT, 0, s>>>(p);
+    HB_CUDA(cudaGetLastError());
+}
+
+// ------------------------------------------------------------------------------------
+// Column-dot matrix-vector product (one warp per output entry).
+// ------------------------------------------------------------------------------------
+namespace {
+__global__ void coldot_kernel(int nrows, int ncols, const double *__restrict__ A, long lda,
+                              const double *__restrict__ x, double *out, double alpha, double beta,
+                              int mode) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= ncols) return;
+    const int i = warp;
+    int lo = 0, hi = nrows;
+    if (mode == 1) lo = i;
+    else if (mode == 2) hi = min(nrows, i + 1);
+    const double *col = A + (size_t) i * lda;
+    double acc = 0.0;
+    int k = lo + lane;
+    for (; k + 96 < hi; k += 128) {
+        acc += col[k] * x[k] + col[k + 32] * x[k + 32] + col[k + 64] * x[k + 64] + col[k + 96] * x[k + 96];
+    }
+    for (; k < hi; k += 32) acc += col[k] * x[k];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) {
+        double v = alpha * acc;
+        if (beta != 0.0) v += beta * out[i];
+        out[i] = v;
+    }
+}
+}  // namespace
+
+void coldot(cudaStream_t s, int nrows, int ncols, const double *A, long lda, const double *x,
+            double *out, double alpha, double beta, int mode) {
+    if (ncols <= 0) return;
+    const int threads = 256;
+    const long warps = ncols;
+    const int blocks = (int) ((warps * 32 + threads - 1) / threads);
+    coldot_kernel<<<blocks, threads, 0, s>>>(nrows, ncols, A, lda, x, out, alpha, beta, mode);
+    HB_CUDA(cudaGetLastError());
+}
+
+// ------------------------------------------------------------------------------------
+// Cholesky: 64 x 64 diagonal-block factorisation + inverse, panel solve, SYRK update.
+// ------------------------------------------------------------------------------------
+namespace {
+constexpr int NB = 64;
+
+// Factorise the nb x nb diagonal block at (j0, j0) in shared memory, write it back,
+// and store its triangular inverse in Dinv rows [j0, j0 + nb), columns [0, nb).
+__global__ void __launch_bounds__(256) potf2_kernel(double *A, long lda, int nb, int j0, double *Dinv,
+                                                    long ldd, int *info) {
+    if (*info) return;
+    extern __shared__ double sm[];
+    double *T = sm;                 // T[r + c * 65]
+    double *Ti = sm + 65 * 64;      // inverse
+    __shared__ int fail;
+    const int tid = threadIdx.x;
+    for (int idx = tid; idx < nb * nb; idx += blockDim.x) {
+        int r = idx % nb, c = idx / nb;
+        T[r + c * 65] = (r >= c) ? A[(size_t) (j0 + r) + (size_t) (j0 + c) * lda] : 0.0;
+    }
+    if (tid == 0) fail = 0;
+    __syncthreads();
+    for (int c = 0; c < nb; ++c) {
+        if (tid == 0) {
+            double d = T[c + c * 65];
+            if (!(d > 0.0)) fail = c + 1;
+            else T[c + c * 65] = sqrt(d);
+        }
+        __syncthreads();
+        if (fail) break;
+        const double piv = T[c + c * 65];
+        for (int r = c + 1 + tid; r < nb; r += blockDim.x) T[r + c * 65] /= piv;
+        __syncthreads();
+        const int rem = nb - c - 1;
+        for (int idx = tid; idx < rem * rem; idx += blockDim.x) {
+            int r = c + 1 + idx % rem, q = c + 1 + idx / rem;
+            if (r >= q) T[r + q * 65] -= T[r + c * 65] * T[q + c * 65];
+        }
+        __syncthreads();
+    }
+    if (fail) {
+        if (tid == 0) *info = j0 + fail;
+        return;
+    }
+    for (int idx = tid; idx < nb * nb; idx += blockDim.x) {
+        int r = idx % nb, c = idx / nb;
+        if (r >= c) A[(size_t) (j0 + r) + (size_t) (j0 + c) * lda] = T[r + c * 65];
+    }
+    // Triangular inverse, one column per thread (forward substitution on e_c).
+    if (tid < nb) {
+        const int c = tid;
+        for (int r = 0; r < c; ++r) Ti[r + c * 65] = 0.0;
+        Ti[c + c * 65] = 1.0 / T[c + c * 65];
+        for (int r = c + 1; r < nb; ++r) {
+            double acc = 0.0;
+            for (int k = c; k < r; ++k) acc += T[r + k * 65] * Ti[k + c * 65];
+            Ti[r + c * 65] = -acc / T[r + r * 65];
+        }
+    }
+    __syncthreads();
+    for (int idx = tid; idx < NB * NB; idx += blockDim.x) {
+        int r = idx % NB, c = idx / NB;
+        double v = (r < nb && c < nb) ? Ti[r + c * 65] : 0.0;
+        if (r < nb) Dinv[(size_t) (j0 + r) + (size_t) c * ldd] = v;
+    }
+}
+
+// P (rows x nb, in place) <- P * Tinv^T for the panel below a diagonal block.
+__global__ void __launch_bounds__(256) trsm_panel_kernel(double *P, long ldp, int rows, int nb,
+                                                         const double *Tinv, long ldt, const int *info) {
+    if (*info) return;
+    extern __shared__ double sm[];
+    double *X = sm;             // 64 x nb, X[r + c*65]
+    double *T = sm + 65 * 64;   // nb x nb, T[r + c*65]
+    const int r0 = blockIdx.x * 64;
+    const int tid = threadIdx.x;
+    const int nr = min(64, rows - r0);
+    for (int idx = tid; idx < 64 * nb; idx += blockDim.x) {
+        int r = idx % 64, c = idx / 64;
+        X[r + c * 65] = (r < nr) ? P[(size_t) (r0 + r) + (size_t) c * ldp] : 0.0;
+    }
+    for (int idx = tid; idx < nb * nb; idx += blockDim.x) {
+        int r = idx % nb, c = idx / nb;
+        T[r + c * 65] = Tinv[(size_t) r + (size_t) c * ldt];
+    }
+    __syncthreads();
+    // out(r, c) = sum_{k <= c} X(r, k) * T(c, k)
+    for (int idx = tid; idx < 64 * nb; idx += blockDim.x) {
+        int r = idx % 64, c = idx / 64;
+        if (r >= nr) continue;
+        double acc = 0.0;
+        for (int k = 0; k <= c; ++k) acc += X[r + k * 65] * T[c + k * 65];
+        P[(size_t) (r0 + r) + (size_t) c * ldp] = acc;
+    }
+}
+
+// X row block (nb x cols, in place) <- Tinv * X, Tinv lower nb x nb.
+__global__ void __launch_bounds__(256) tri_left_kernel(double *X, long ldx, int nb, int cols,
+                                                       const double *Tinv, long ldt) {
+    extern __shared__ double sm[];
+    double *Xs = sm;             // nb x 64
+    double *T = sm + 65 * 64;
+    const int c0 = blockIdx.x * 64;
+    const int nc = min(64, cols - c0);
+    const int tid = threadIdx.x;
+    for (int idx = tid; idx < nb * 64; idx += blockDim.x) {
+        int r = idx % nb, c = idx / nb;
+        Xs[r + c * 65] = (c < nc) ? X[(size_t) r + (size_t) (c0 + c) * ldx] : 0.0;
+    }
+    for (int idx = tid; idx < nb * nb; idx += blockDim.x) {
+        int r = idx % nb, c = idx / nb;
+        T[r + c * 65] = Tinv[(size_t) r + (size_t) c * ldt];
+    }
+    __syncthreads();
+    for (int idx = tid; idx < nb * 64; idx += blockDim.x) {
+        int r = idx % nb, c = idx / nb;
+        if (c >= nc) continue;
+        double acc = 0.0;
+        for (int k = 0; k <= r; ++k) acc += T[r + k * 65] * Xs[k + c * 65];
+        X[(size_t) r + (size_t) (c0 + c) * ldx] = acc;
+    }
+}
+
+__global__ void copy_lower_kernel(int n, const double *S, long lds, double *L, long ldl) {
+    const long total = (long) n * n;
+    for (long idx = blockIdx.x * (long) blockDim.x + threadIdx.x; idx < total; idx += (long) gridDim.x * blockDim.x) {
+        int r = (int) (idx % n), c = (int) (idx / n);
+        L[(size_t) r + (size_t) c * ldl] = (r >= c) ? S[(size_t) r + (size_t) c * lds] : 0.0;
+    }
+}
+
+__global__ void set_identity_kernel(int n, double *A, long lda) {
+    const long total = (long) n * n;
+    for (long idx = blockIdx.x * (long) blockDim.x + threadIdx.x; idx < total; idx += (long) gridDim.x * blockDim.x) {
+        int r = (int) (idx % n), c = (int) (idx / n);
+        A[(size_t) r + (size_t) c * lda] = (r == c) ? 1.0 : 0.0;
+    }
+}
+
+__global__ void zero_int_kernel(int *p) { *p = 0; }
+
+int grid_for(long total, int threads = 256) {
+    long b = (total + threads - 1) / threads;
+    return (int) std::min<long>(std::max<long>(b, 1), 148L * 16);
+}
+}  // namespace
+
+void DenseFactor::alloc(int n_) {
+    n = n_;
+    ld = pad_ld(n);
+    HB_CUDA(cudaMalloc(&L, sizeof(double) * ld * n));
+    HB_CUDA(cudaMalloc(&Dinv, sizeof(double) * ld * NB));
+    HB_CUDA(cudaMalloc(&d_info, sizeof(int)));
+    HB_CUDA(cudaMallocHost(&h_info, sizeof(int)));
+    *h_info = 0;
+    HB_CUDA(cudaMemset(L, 0, sizeof(double) * ld * n));
+    HB_CUDA(cudaMemset(Dinv, 0, sizeof(double) * ld * NB));
+}
+
+void DenseFactor::release() {
+    if (L) cudaFree(L);
+    if (Dinv) cudaFree(Dinv);
+    if (K) cudaFree(K);
+    if (KT) cudaFree(KT);
+    if (d_info) cudaFree(d_info);
+    if (h_info) cudaFreeHost(h_info);
+    L = Dinv = K = KT = nullptr;
+    d_info = nullptr;
+    h_info = nullptr;
+    factored = ok = k_valid = false;
+}
+
+static void set_smem(const void *fn, int bytes) {
+    HB_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+}
+
+static int smem_bytes() { return 2 * 65 * 64 * (int) sizeof(double); }
+
+static void ensure_attrs() {
+    static bool init = false;
+    if (init) return;
+    set_smem((const void *) potf2_kernel, smem_bytes());
+    set_smem((const void *) trsm_panel_kernel, smem_bytes());
+    set_smem((const void *) tri_left_kernel, smem_bytes());
+    init = true;
+}
+
+void factorize_async(cudaStream_t s, DenseFactor &F, const double *S, long ldS) {
+    ensure_attrs();
+    const int n = F.n;
+    F.k_valid = false;
+    F.factored = true;
+    zero_int_kernel<<<1, 1, 0, s>>>(F.d_info);
+    copy_lower_kernel<<<grid_for((long) n * n), 256, 0, s>>>(n, S, ldS, F.L, F.ld);
+    for (int j0 = 0; j0 < n; j0 += NB) {
+        const int nb = std::min(NB, n - j0);
+        potf2_kernel<<<1, 256, smem_bytes(), s>>>(F.L, F.ld, nb, j0, F.Dinv, F.ld, F.d_info);
+        const int rows = n - j0 - nb;
+        if (rows > 0) {
+            double *P = F.L + (size_t) (j0 + nb) + (size_t) j0 * F.ld;
+            trsm_panel_kernel<<<(rows + 63) / 64, 256, smem_bytes(), s>>>(P, F.ld, rows, nb,
+                                                                         F.Dinv + j0, F.ld, F.d_info);
+            double *A22 = F.L + (size_t) (j0 + nb) + (size_t) (j0 + nb) * F.ld;
+            gemm(s, rows, rows, nb, -1.0, P, F.ld, 0, P, F.ld, 1, 1.0, A22, F.ld, GEMM_C_LOWER, F.d_info);
+        }
+    }
+    HB_CUDA(cudaMemcpyAsync(F.h_info, F.d_info, sizeof(int), cudaMemcpyDeviceToHost, s));
+    HB_CUDA(cudaGetLastError());
+}
+
+bool factor_status(cudaStream_t s, DenseFactor &F) {
+    HB_CUDA(cudaStreamSynchronize(s));
+    F.ok = (*F.h_info == 0);
+    return F.ok;
+}
+
+bool factorize(cudaStream_t s, DenseFactor &F, const double *S, long ldS) {
+    factorize_async(s, F, S, ldS);
+    return factor_status(s, F);
+}
+
+void compute_inverse_factor(cudaStream_t s, DenseFactor &F) {
+    ensure_attrs();
+    if (F.k_valid) return;
+    const int n = F.n;
+    if (!F.K) HB_CUDA(cudaMalloc(&F.K, sizeof(double) * F.ld * n));
+    if (!F.KT) HB_CUDA(cudaMalloc(&F.KT, sizeof(double) * F.ld * n));
+    set_identity_kernel<<<grid_for((long) n * n), 256, 0, s>>>(n, F.K, F.ld);
+    for (int i0 = 0; i0 < n; i0 += NB) {
+        const int nb = std::min(NB, n - i0);
+        const int cend = i0 + nb;
+        tri_left_kernel<<<(cend + 63) / 64, 256, smem_bytes(), s>>>(F.K + i0, F.ld, nb, cend, F.Dinv + i0, F.ld);
+        const int rows = n - cend;
+        if (rows > 0) {
+            gemm(s, rows, cend, nb, -1.0, F.L + (size_t) cend + (size_t) i0 * F.ld, F.ld, 0, F.K + i0, F.ld, 0,
+                 1.0, F.K + cend, F.ld, 0);
+        }
+    }
+    transpose(s, n, F.K, F.ld, F.KT, F.ld);
+    F.k_valid = true;
+}
+
+void compute_inverse(cudaStream_t s, DenseFactor &F, double *W, long ldW) {
+    compute_inverse_factor(s, F);
+    const int n = F.n;
+    gemm(s, n, n, n, 1.0, F.K, F.ld, 1, F.K, F.ld, 0, 0.0, W, ldW, GEMM_C_LOWER | GEMM_A_UPPER | GEMM_B_LOWER);
+    symmetrize_lower(s, n, W, ldW);
+}
+
+// ------------------------------------------------------------------------------------
+// Small reductions and elementwise helpers.
+// ------------------------------------------------------------------------------------
+namespace {
+__device__ double block_sum(double v) {
+    __shared__ double red[32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) red[w] = v;
+    __syncthreads();
+    const int nw = (blockDim.x + 31) >> 5;
+    v = (threadIdx.x < nw) ? red[threadIdx.x] : 0.0;
+    if (w == 0) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    }
+    __syncthreads();
+    return v;
+}
+
+__global__ void logdiag_kernel(int n, const double *L, long ld, double *out) {
+    double acc = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) acc += log(L[(size_t) i + (size_t) i * ld]);
+    acc = block_sum(acc);
+    if (threadIdx.x == 0) *out = acc;
+}
+
+__global__ void copydiag_kernel(int n, const double *L, long ld, double *out) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        out[i] = L[(size_t) i + (size_t) i * ld];
+}
+
+__global__ void fill_kernel(double *x, double v, size_t n) {
+    for (size_t i = blockIdx.x * (size_t) blockDim.x + threadIdx.x; i < n; i += (size_t) gridDim.x * blockDim.x) x[i] = v;
+}
+
+__global__ void axpy_kernel(int n, double a, const double *x, double *y) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) y[i] += a * x[i];
+}
+
+__global__ void symlower_kernel(int n, double *A, long lda) {
+    const long total = (long) n * n;
+    for (long idx = blockIdx.x * (long) blockDim.x + threadIdx.x; idx < total; idx += (long) gridDim.x * blockDim.x) {
+        int r = (int) (idx % n), c = (int) (idx / n);
+        if (r < c) A[(size_t) r + (size_t) c * lda] = A[(size_t) c + (size_t) r * lda];
+    }
+}
+
+__global__ void symavg_kernel(int n, double *A, long lda) {
+    const long total = (long) n * n;
+    for (long idx = blockIdx.x * (long) blockDim.x + threadIdx.x; idx < total; idx += (long) gridDim.x * blockDim.x) {
+        int r = (int) (idx % n), c = (int) (idx / n);
+        if (r > c) {
+            double a = A[(size_t) r + (size_t) c * lda], b = A[(size_t) c + (size_t) r * lda];
+            double v = 0.5 * (a + b);
+            A[(size_t) r + (size_t) c * lda] = v;
+            A[(size_t) c + (size_t) r * lda] = v;
+        }
+    }
+}
+
+__global__ void adddiag_kernel(int n, double *A, long lda, double v) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        A[(size_t) i + (size_t) i * lda] += v;
+}
+
+__global__ void adddiagvec_kernel(int n, double *A, long lda, const double *d) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        A[(size_t) i + (size_t) i * lda] += d[i];
+}
+
+__global__ void copymat_kernel(int rows, int cols, const double *A, long lda, double *B, long ldb) {
+    const long total = (long) rows * cols;
+    for (long idx = blockIdx.x * (long) blockDim.x + threadIdx.x; idx < total; idx += (long) gridDim.x * blockDim.x) {
+        int r = (int) (idx % rows), c = (int) (idx / rows);
+        B[(size_t) r + (size_t) c * ldb] = A[(size_t) r + (size_t) c * lda];
+    }
+}
+
+__global__ void transpose_kernel(int n, const double *A, long lda, double *B, long ldb) {
+    __shared__ double tile[32][33];
+    const int bx = blockIdx.x * 32, by = blockIdx.y * 32;
+    for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+        int r = bx + threadIdx.x, c = by + j;
+        if (r < n && c < n) tile[j][threadIdx.x] = A[(size_t) r + (size_t) c * lda];
+    }
+    __syncthreads();
+    for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+        int r = by + threadIdx.x, c = bx + j;
+        if (r < n && c < n) B[(size_t) r + (size_t) c * ldb] = tile[threadIdx.x][j];
+    }
+}
+
+__global__ void scalemat_kernel(int rows, int cols, double *A, long lda, double a) {
+    const long total = (long) rows * cols;
+    for (long idx = blockIdx.x * (long) blockDim.x + threadIdx.x; idx < total; idx += (long) gridDim.x * blockDim.x) {
+        int r = (int) (idx % rows), c = (int) (idx / rows);
+        A[(size_t) r + (size_t) c * lda] *= a;
+    }
+}
+
+__global__ void scalecols_kernel(int rows, int cols, const double *A, long lda, const double *d, double *B, long ldb) {
+    const long total = (long) rows * cols;
+    for (long idx = blockIdx.x * (long) blockDim.x + threadIdx.x; idx < total; idx += (long) gridDim.x * blockDim.x) {
+        int r = (int) (idx % rows), c = (int) (idx / rows);
+        B[(size_t) r + (size_t) c * ldb] = A[(size_t) r + (size_t) c * lda] * d[c];
+    }
+}
+
+// Deterministic two-level reduction: each block reduces a fixed slice, then block 0
+// of a second launch sums the partials.
+__global__ void frob_partial_kernel(int n, const double *A, long lda, const double *B, long ldb, double *part) {
+    double acc = 0.0;
+    const long total = (long) n * n;
+    for (long idx = blockIdx.x * (long) blockDim.x + threadIdx.x; idx < total; idx += (long) gridDim.x * blockDim.x) {
+        int r = (int) (idx % n), c = (int) (idx / n);
+        acc += A[(size_t) r + (size_t) c * lda] * B[(size_t) r + (size_t) c * ldb];
+    }
+    acc = block_sum(acc);
+    if (threadIdx.x == 0) part[blockIdx.x] = acc;
+}
+
+__global__ void sum_partials_kernel(int np, const double *part, double *out) {
+    double acc = 0.0;
+    for (int i = threadIdx.x; i < np; i += blockDim.x) acc += part[i];
+    acc = block_sum(acc);
+    if (threadIdx.x == 0) *out = acc;
+}
+
+__global__ void trace_kernel(int n, const double *A, long lda, double *out) {
+    double acc = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) acc += A[(size_t) i + (size_t) i * lda];
+    acc = block_sum(acc);
+    if (threadIdx.x == 0) *out = acc;
+}
+
+__global__ void dot_kernel(int n, const double *x, const double *y, double *out) {
+    double acc = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) acc += x[i] * y[i];
+    acc = block_sum(acc);
+    if (threadIdx.x == 0) *out = acc;
+}
+}  // namespace
+
+void log_diag_sum(cudaStream_t s, const DenseFactor &F, double *d_out) {
+    logdiag_kernel<<<1, 1024, 0, s>>>(F.n, F.L, F.ld, d_out);
+    HB_CUDA(cudaGetLastError());
+}
+
+void copy_diag(cudaStream_t s, const DenseFactor &F, double *d_out) {
+    copydiag_kernel<<<grid_for(F.n), 256, 0, s>>>(F.n, F.L, F.ld, d_out);
+}
+
+void fill(cudaStream_t s, double *x, double v, size_t n) {
+    if (!n) return;
+    fill_kernel<<<grid_for((long) n), 256, 0, s>>>(x, v, n);
+}
+
+void axpy(cudaStream_t s, int n, double a, const double *x, double *y) {
+    if (n <= 0) return;
+    axpy_kernel<<<grid_for(n), 256, 0, s>>>(n, a, x, y);
+}
+
+void symmetrize_lower(cudaStream_t s, int n, double *A, long lda) {
+    symlower_kernel<<<grid_for((long) n * n), 256, 0, s>>>(n, A, lda);
+}
+
+void symmetrize_avg(cudaStream_t s, int n, double *A, long lda) {
+    symavg_kernel<<<grid_for((long) n * n), 256, 0, s>>>(n, A, lda);
+}
+
+void add_diag(cudaStream_t s, int n, double *A, long lda, double v) {
+    adddiag_kernel<<<grid_for(n), 256, 0, s>>>(n, A, lda, v);
+}
+
+void add_diag_vec(cudaStream_t s, int n, double *A, long lda, const double *d) {
+    adddiagvec_kernel<<<grid_for(n), 256, 0, s>>>(n, A, lda, d);
+}
+
+void copy_matrix(cudaStream_t s, int rows, int cols, const double *A, long lda, double *B, long ldb) {
+    if (rows <= 0 || cols <= 0) return;
+    copymat_kernel<<<grid_for((long) rows * cols), 256, 0, s>>>(rows, cols, A, lda, B, ldb);
+}
+
+void transpose(cudaStream_t s, int n, const double *A, long lda, double *B, long ldb) {
+    dim3 grid((n + 31) / 32, (n + 31) / 32), block(32, 8);
+    transpose_kernel<<<grid, block, 0, s>>>(n, A, lda, B, ldb);
+}
+
+void scale_matrix(cudaStream_t s, int rows, int cols, double *A, long lda, double a) {
+    scalemat_kernel<<<grid_for((long) rows * cols), 256, 0, s>>>(rows, cols, A, lda, a);
+}
+
+void scale_columns(cudaStream_t s, int rows, int cols, const double *A, long lda, const double *d,
+                   double *B, long ldb) {
+    scalecols_kernel<<<grid_for((long) rows * cols), 256, 0, s>>>(rows, cols, A, lda, d, B, ldb);
+}
+
+void frob_dot(cudaStream_t s, int n, const double *A, long lda, const double *B, long ldb, double *d_out) {
+    static double *part = nullptr;
+    const int np = 296;
+    if (!part) HB_CUDA(cudaMalloc(&part, sizeof(double) * np));
+    frob_partial_kernel<<<np, 256, 0, s>>>(n, A, lda, B, ldb, part);
+    sum_partials_kernel<<<1, 512, 0, s>>>(np, part, d_out);
+}
+
+void trace(cudaStream_t s, int n, const double *A, long lda, double *d_out) {
+    trace_kernel<<<1, 1024, 0, s>>>(n, A, lda, d_out);
+}
+
+void dot(cudaStream_t s, int n, const double *x, const double *y, double *d_out) {
+    dot_kernel<<<1, 1024, 0, s>>>(n, x, y, d_out);
+}
+
+}  // namespace hb

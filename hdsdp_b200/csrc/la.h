@@ -1,0 +1,89 @@
+// Dense FP64 linear algebra on the B200: GEMM on the DMMA (FP64 tensor-core)
+// path, blocked Cholesky with a positive-definiteness flag, triangular
+// inverse, column-dot matrix-vector products and small reductions.
+//
+// All matrices are column-major FP64 with an explicit leading dimension.
+// Symmetric matrices are stored full (both triangles) unless a routine says
+// it reads only the lower triangle.
+#pragma once
+#include <cuda_runtime.h>
+#include "dev.cuh"
+
+namespace hb {
+
+enum GemmFlags : int {
+    GEMM_C_LOWER = 1,      // compute / write only entries with row >= col
+    GEMM_A_LOWER = 2,      // op(A)(i,k) == 0 for k > i  (read as zero)
+    GEMM_A_UPPER = 4,      // op(A)(i,k) == 0 for k < i
+    GEMM_B_LOWER = 8,      // op(B)(k,j) == 0 for k < j
+    GEMM_B_UPPER = 16,     // op(B)(k,j) == 0 for k > j
+};
+
+// C = alpha * op(A) * op(B) + beta * C   (op = transpose when trans != 0).
+// If abort_flag is non-null and *abort_flag != 0 when a tile starts, the tile is skipped.
+void gemm(cudaStream_t s, int M, int N, int K, double alpha, const double *A, long lda, int transA,
+          const double *B, long ldb, int transB, double beta, double *C, long ldc, int flags = 0,
+          const int *abort_flag = nullptr);
+
+// Column-dot matrix-vector product:
+//   out[i] = alpha * sum_{k in R(i)} A[k + i*lda] * x[k] + beta * out[i],  i < ncols
+// with R(i) = [0, nrows) (mode 0), [i, nrows) (mode 1), [0, i] (mode 2).
+void coldot(cudaStream_t s, int nrows, int ncols, const double *A, long lda, const double *x,
+            double *out, double alpha, double beta, int mode);
+
+// Factor object for an n x n symmetric positive definite matrix.
+// L holds the lower Cholesky factor, Dinv the inverses of its 64 x 64
+// diagonal blocks, K = L^-1 and KT = L^-T (computed on demand).
+struct DenseFactor {
+    int n = 0;
+    long ld = 0;
+    double *L = nullptr;
+    double *Dinv = nullptr;   // n x 64 (block b at rows [64b, 64b+64))
+    double *K = nullptr;
+    double *KT = nullptr;
+    int *d_info = nullptr;    // device: 0 = success, k > 0 = pivot k failed
+    int *h_info = nullptr;    // pinned host mirror
+    bool factored = false;
+    bool ok = false;
+    bool k_valid = false;
+    void alloc(int n_);
+    void release();
+};
+
+// Copy the lower triangle of S (n x n, ldS) into F.L and factorise it.
+// Returns true if S is positive definite (dpotrf semantics: fails on a
+// non-positive or NaN pivot). Synchronises the stream.
+bool factorize(cudaStream_t s, DenseFactor &F, const double *S, long ldS);
+// Enqueue the factorisation without synchronising; call factor_status() later.
+void factorize_async(cudaStream_t s, DenseFactor &F, const double *S, long ldS);
+bool factor_status(cudaStream_t s, DenseFactor &F);
+// K = L^-1 and KT = K^T (lower / upper triangular). Requires a successful factor.
+void compute_inverse_factor(cudaStream_t s, DenseFactor &F);
+// W = S^-1 = K^T K, full symmetric, into W (ldW).
+void compute_inverse(cudaStream_t s, DenseFactor &F, double *W, long ldW);
+// sum_i log L_ii (device scalar out).
+void log_diag_sum(cudaStream_t s, const DenseFactor &F, double *d_out);
+// Copy the diagonal of L into out (n).
+void copy_diag(cudaStream_t s, const DenseFactor &F, double *d_out);
+
+// Small vector / matrix helpers
+void fill(cudaStream_t s, double *x, double v, size_t n);
+void axpy(cudaStream_t s, int n, double a, const double *x, double *y);
+void symmetrize_lower(cudaStream_t s, int n, double *A, long lda);   // A(j,i) = A(i,j), i > j
+void symmetrize_avg(cudaStream_t s, int n, double *A, long lda);     // A = (A + A^T)/2
+void add_diag(cudaStream_t s, int n, double *A, long lda, double v);
+void add_diag_vec(cudaStream_t s, int n, double *A, long lda, const double *d);
+void copy_matrix(cudaStream_t s, int rows, int cols, const double *A, long lda, double *B, long ldb);
+void transpose(cudaStream_t s, int n, const double *A, long lda, double *B, long ldb);
+void scale_matrix(cudaStream_t s, int rows, int cols, double *A, long lda, double a);
+// d_out[0] = sum_ij A_ij * B_ij over the full n x n matrices
+void frob_dot(cudaStream_t s, int n, const double *A, long lda, const double *B, long ldb, double *d_out);
+// d_out[0] = trace(A)
+void trace(cudaStream_t s, int n, const double *A, long lda, double *d_out);
+// d_out = x . y
+void dot(cudaStream_t s, int n, const double *x, const double *y, double *d_out);
+// Column j of A scaled by d[j]
+void scale_columns(cudaStream_t s, int rows, int cols, const double *A, long lda, const double *d,
+                   double *B, long ldb);
+
+}  // namespace hb

@@ -1,0 +1,522 @@
+// Kernels on the coefficient matrices of one dense SDP block.
+//
+// Reference formulas (interface/hdsdp_conic_sdp.c, linalg/hdsdp_sdpdata.c):
+//   dual slack        S = dC*C + dA*sum_j w_j A_j + dEye*I   (sdpDenseConeIUpdateBuffer :343-402)
+//   Schur matrix      M_ij = <A_i, W A_j W>                    (KKT2-KKT5 :683-981)
+//   vectors           <A_j, W>, <A_j, W^2>                     (ASinv, ASinvRdSinv)
+// For a symmetric sparse A = sum_e v_e (E_rc + E_cr) (diagonal entries once):
+//   <A, Z>        = sum_e v_e * (r != c ? 2 Z_rc : Z_rr)
+//   <A, W B W>    = sum_e sum_f v_e u_f * pair(e, f)       (pair below)
+#include "sdp.h"
+#include <unordered_map>
+#include <algorithm>
+#include <cstring>
+
+namespace hb {
+
+namespace {
+
+template <typename T>
+T *upload_vec(const std::vector<T> &h, cudaStream_t s) {
+    if (h.empty()) return nullptr;
+    T *d = nullptr;
+    HB_CUDA(cudaMalloc(&d, sizeof(T) * h.size()));
+    HB_CUDA(cudaMemcpyAsync(d, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice, s));
+    return d;
+}
+
+int grid1(long total, int threads = 256) {
+    long b = (total + threads - 1) / threads;
+    return (int) std::min<long>(std::max<long>(b, 1), 148L * 16);
+}
+
+// tr(E_ab' W E_cd' W) summed over the symmetric expansions of (a,b) and (c,d).
+__device__ __forceinline__ double pair_term(const double *W, long ld, int a, int b, int c, int d) {
+    auto w = [&](int i, int j) { return W[(size_t) i + (size_t) j * ld]; };
+    if (a != b && c != d) return 2.0 * (w(b, c) * w(a, d) + w(b, d) * w(a, c));
+    if (a == b && c != d) return 2.0 * w(a, c) * w(a, d);
+    if (a != b && c == d) return 2.0 * w(a, c) * w(b, c);
+    double x = w(a, c);
+    return x * x;
+}
+
+__global__ void scatter_sym_kernel(int nnz, const int *r, const int *c, const double *v, double *A, long lda) {
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nnz; e += gridDim.x * blockDim.x) {
+        A[(size_t) r[e] + (size_t) c[e] * lda] = v[e];
+        A[(size_t) c[e] + (size_t) r[e] * lda] = v[e];
+    }
+}
+
+__global__ void s_init_kernel(int n, const double *C, long ldc, double dC, double dEye, double *S, long lds) {
+    const long total = (long) n * n;
+    for (long idx = blockIdx.x * (long) blockDim.x + threadIdx.x; idx < total; idx += (long) gridDim.x * blockDim.x) {
+        int r = (int) (idx % n), c = (int) (idx / n);
+        double v = (dC != 0.0) ? dC * C[(size_t) r + (size_t) c * ldc] : 0.0;
+        if (r == c) v += dEye;
+        S[(size_t) r + (size_t) c * lds] = v;
+    }
+}
+
+__global__ void s_gather_kernel(int npos, const int *pr, const int *pc, const int *ptr, const int *ej,
+                                const double *ev, const double *w, double dA, double *S, long lds) {
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npos; p += gridDim.x * blockDim.x) {
+        double acc = 0.0;
+        for (int e = ptr[p]; e < ptr[p + 1]; ++e) acc += ev[e] * w[ej[e]];
+        acc *= dA;
+        const int r = pr[p], c = pc[p];
+        S[(size_t) r + (size_t) c * lds] += acc;
+        if (r != c) S[(size_t) c + (size_t) r * lds] += acc;
+    }
+}
+
+__global__ void r1d_weights_kernel(int k, const int *id, const double *sign, const double *w, double dA, double *d) {
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < k; a += gridDim.x * blockDim.x) d[a] = dA * sign[a] * w[id[a]];
+}
+
+__global__ void axpy_mat_devscale_kernel(int n, const double *A, long lda, const double *w, int j, double dA,
+                                         double *S, long lds) {
+    const double a = dA * w[j];
+    if (a == 0.0) return;
+    const long total = (long) n * n;
+    for (long idx = blockIdx.x * (long) blockDim.x + threadIdx.x; idx < total; idx += (long) gridDim.x * blockDim.x) {
+        int r = (int) (idx % n), c = (int) (idx / n);
+        S[(size_t) r + (size_t) c * lds] += a * A[(size_t) r + (size_t) c * lda];
+    }
+}
+
+// ---- Schur pair kernels -------------------------------------------------------------
+__global__ void schur_spsp_kernel(int nsp, const int *id, const int *ptr, const int *rr, const int *cc,
+                                  const double *vv, const double *W, long ldw, double *M, long ldm) {
+    const int a = blockIdx.y * blockDim.y + threadIdx.y;
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= nsp || b > a) return;
+    double acc = 0.0;
+    for (int e = ptr[a]; e < ptr[a + 1]; ++e)
+        for (int f = ptr[b]; f < ptr[b + 1]; ++f) acc += vv[e] * vv[f] * pair_term(W, ldw, rr[e], cc[e], rr[f], cc[f]);
+    M[(size_t) id[a] + (size_t) id[b] * ldm] = acc;
+}
+
+__global__ void schur_r1s_kernel(int k, const int *id, const int *ptr, const int *pp, const double *aa,
+                                 const double *sg, const double *W, long ldw, double *M, long ldm) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    const int a = blockIdx.y * blockDim.y + threadIdx.y;
+    if (a >= k || b > a) return;
+    double g = 0.0;
+    for (int t = ptr[a]; t < ptr[a + 1]; ++t) {
+        double gt = 0.0;
+        for (int u = ptr[b]; u < ptr[b + 1]; ++u) gt += aa[u] * W[(size_t) pp[t] + (size_t) pp[u] * ldw];
+        g += aa[t] * gt;
+    }
+    M[(size_t) id[a] + (size_t) id[b] * ldm] = sg[a] * sg[b] * g * g;
+}
+
+__global__ void schur_hadamard_kernel(int k, const int *id, const double *sg, const double *G, long ldg,
+                                      double *M, long ldm) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    const int a = blockIdx.y * blockDim.y + threadIdx.y;
+    if (a >= k || b > a) return;
+    const double g = G[(size_t) a + (size_t) b * ldg];
+    M[(size_t) id[a] + (size_t) id[b] * ldm] = sg[a] * sg[b] * g * g;
+}
+
+// (a in R1D with column V[:,a]) x (b in R1S): (a_b^T v_a)^2 s_a s_b
+__global__ void schur_r1d_r1s_kernel(int kd, const int *idd, const double *sgd, const double *V, long ldv,
+                                     int ks, const int *ids, const int *ptr, const int *pp, const double *aa,
+                                     const double *sgs, double *M, long ldm) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    const int a = blockIdx.y * blockDim.y + threadIdx.y;
+    if (a >= kd || b >= ks) return;
+    double g = 0.0;
+    for (int u = ptr[b]; u < ptr[b + 1]; ++u) g += aa[u] * V[(size_t) pp[u] + (size_t) a * ldv];
+    const int i = idd[a], j = ids[b];
+    const int hi = max(i, j), lo = min(i, j);
+    M[(size_t) hi + (size_t) lo * ldm] = sgd[a] * sgs[b] * g * g;
+}
+
+// V[:, b] = sum_t a_t W[:, p_t] for R1S constraints
+__global__ void r1s_build_v_kernel(int n, int ks, const int *ptr, const int *pp, const double *aa,
+                                   const double *W, long ldw, double *V, long ldv) {
+    const int b = blockIdx.y;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        double acc = 0.0;
+        for (int t = ptr[b]; t < ptr[b + 1]; ++t) acc += aa[t] * W[(size_t) k + (size_t) pp[t] * ldw];
+        V[(size_t) k + (size_t) b * ldv] = acc;
+    }
+}
+
+// (a: rank one with column V[:,a], sign sg) x (b in SP): s_a * v^T A_b v
+__global__ void schur_r1_sp_kernel(int kr, const int *idr, const double *sgr, const double *V, long ldv,
+                                   int nsp, const int *ids, const int *ptr, const int *rr, const int *cc,
+                                   const double *vv, double *M, long ldm) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    const int a = blockIdx.y * blockDim.y + threadIdx.y;
+    if (a >= kr || b >= nsp) return;
+    const double *v = V + (size_t) a * ldv;
+    double acc = 0.0;
+    for (int f = ptr[b]; f < ptr[b + 1]; ++f) {
+        const int r = rr[f], c = cc[f];
+        acc += vv[f] * ((r != c) ? 2.0 * v[r] * v[c] : v[r] * v[r]);
+    }
+    const int i = idr[a], j = ids[b];
+    const int hi = max(i, j), lo = min(i, j);
+    M[(size_t) hi + (size_t) lo * ldm] = sgr[a] * acc;
+}
+
+__global__ void scatter_row_kernel(int m, int i, const double *t, double *M, long ldm) {
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < m; j += gridDim.x * blockDim.x) {
+        const int hi = max(i, j), lo = min(i, j);
+        M[(size_t) hi + (size_t) lo * ldm] = t[j];
+    }
+}
+
+// ---- inner products -------------------------------------------------------------------
+__global__ void inner_sp_kernel(int nsp, const int *id, const int *ptr, const int *rr, const int *cc,
+                                const double *vv, const double *Z, long ldz, double *out) {
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nsp; a += gridDim.x * blockDim.x) {
+        double acc = 0.0;
+        for (int e = ptr[a]; e < ptr[a + 1]; ++e) {
+            const int r = rr[e], c = cc[e];
+            const double z = Z[(size_t) r + (size_t) c * ldz];
+            acc += vv[e] * ((r != c) ? 2.0 * z : z);
+        }
+        out[id[a]] = acc;
+    }
+}
+
+__global__ void inner_r1s_kernel(int k, const int *id, const int *ptr, const int *pp, const double *aa,
+                                 const double *sg, const double *Z, long ldz, double *out) {
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < k; a += gridDim.x * blockDim.x) {
+        double acc = 0.0;
+        for (int t = ptr[a]; t < ptr[a + 1]; ++t) {
+            double at = 0.0;
+            for (int u = ptr[a]; u < ptr[a + 1]; ++u) at += aa[u] * Z[(size_t) pp[t] + (size_t) pp[u] * ldz];
+            acc += aa[t] * at;
+        }
+        out[id[a]] = sg[a] * acc;
+    }
+}
+
+// out[id[a]] = sg[a] * sum_k X[k,a] * Y[k,a]   (warp per column)
+__global__ void coldot_pair_kernel(int n, int k, const int *id, const double *sg, const double *X, long ldx,
+                                   const double *Y, long ldy, double *out) {
+    const int a = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (a >= k) return;
+    const double *x = X + (size_t) a * ldx;
+    const double *y = Y + (size_t) a * ldy;
+    double acc = 0.0;
+    for (int r = lane; r < n; r += 32) acc += x[r] * y[r];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) out[id[a]] = sg[a] * acc;
+}
+
+// <A_a, W^2> for SP: sum_e v_e (r != c ? 2 : 1) * W[:,r].W[:,c]   (warp per constraint)
+__global__ void innersq_sp_kernel(int n, int nsp, const int *id, const int *ptr, const int *rr, const int *cc,
+                                  const double *vv, const double *W, long ldw, double *out) {
+    const int a = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (a >= nsp) return;
+    double acc = 0.0;
+    for (int e = ptr[a]; e < ptr[a + 1]; ++e) {
+        const int r = rr[e], c = cc[e];
+        const double *wr = W + (size_t) r * ldw;
+        const double *wc = W + (size_t) c * ldw;
+        double d = 0.0;
+        for (int k = lane; k < n; k += 32) d += wr[k] * wc[k];
+        acc += vv[e] * ((r != c) ? 2.0 : 1.0) * d;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) out[id[a]] = acc;
+}
+
+// <A_a, W^2> for R1S: s * || sum_t a_t W[:, p_t] ||^2   (warp per constraint)
+__global__ void innersq_r1s_kernel(int n, int k, const int *id, const int *ptr, const int *pp, const double *aa,
+                                   const double *sg, const double *W, long ldw, double *out) {
+    const int a = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (a >= k) return;
+    double acc = 0.0;
+    for (int r = lane; r < n; r += 32) {
+        double v = 0.0;
+        for (int t = ptr[a]; t < ptr[a + 1]; ++t) v += aa[t] * W[(size_t) r + (size_t) pp[t] * ldw];
+        acc += v * v;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) out[id[a]] = sg[a] * acc;
+}
+
+}  // namespace
+
+void SdpDevice::upload(int n_, int m_, const HostCoeff &C, const std::vector<HostCoeff> &A, cudaStream_t s) {
+    n = n_;
+    m = m_;
+    ld = pad_ld(n);
+    stream = s;
+    HB_CUDA(cudaMalloc(&Cfull, sizeof(double) * ld * n));
+    HB_CUDA(cudaMemsetAsync(Cfull, 0, sizeof(double) * ld * n, s));
+    if (!C.r.empty()) {
+        int *dr = upload_vec(C.r, s), *dc = upload_vec(C.c, s);
+        double *dv = upload_vec(C.v, s);
+        scatter_sym_kernel<<<grid1((long) C.r.size()), 256, 0, s>>>((int) C.r.size(), dr, dc, dv, Cfull, ld);
+        HB_CUDA(cudaStreamSynchronize(s));
+        cudaFree(dr);
+        cudaFree(dc);
+        cudaFree(dv);
+    }
+
+    std::vector<int> spid, spptr{0}, spr, spc;
+    std::vector<double> spv;
+    std::vector<int> r1sid, r1sptr{0}, r1sp;
+    std::vector<double> r1sa, r1ssg;
+    std::vector<int> r1did;
+    std::vector<double> r1dsg;
+    std::vector<std::pair<int, int>> r1d_src;  // (constraint, unused)
+    // gather map: key = r * n + c
+    std::unordered_map<long long, std::vector<std::pair<int, double>>> posmap;
+    std::vector<long long> posorder;
+    auto addpos = [&](int r, int c, int j, double v) {
+        long long key = (long long) r * n + c;
+        auto it = posmap.find(key);
+        if (it == posmap.end()) {
+            posorder.push_back(key);
+            posmap[key].push_back({j, v});
+        } else {
+            it->second.push_back({j, v});
+        }
+    };
+
+    for (int j = 0; j < m; ++j) {
+        const HostCoeff &a = A[j];
+        if (a.cls == CLS_SP) {
+            spid.push_back(j);
+            for (size_t e = 0; e < a.r.size(); ++e) {
+                spr.push_back(a.r[e]);
+                spc.push_back(a.c[e]);
+                spv.push_back(a.v[e]);
+                addpos(a.r[e], a.c[e], j, a.v[e]);
+            }
+            spptr.push_back((int) spr.size());
+        } else if (a.cls == CLS_R1S) {
+            r1sid.push_back(j);
+            r1ssg.push_back(a.sign);
+            for (size_t t = 0; t < a.aidx.size(); ++t) {
+                r1sp.push_back(a.aidx[t]);
+                r1sa.push_back(a.aval[t]);
+            }
+            r1sptr.push_back((int) r1sp.size());
+            for (size_t t = 0; t < a.aidx.size(); ++t)
+                for (size_t u = 0; u <= t; ++u)
+                    addpos(a.aidx[t], a.aidx[u], j, a.sign * a.aval[t] * a.aval[u]);
+        } else if (a.cls == CLS_R1D) {
+            r1did.push_back(j);
+            r1dsg.push_back(a.sign);
+        } else if (a.cls == CLS_DR) {
+            dr_id.push_back(j);
+        }
+    }
+
+    nsp = (int) spid.size();
+    sp_id = upload_vec(spid, s);
+    sp_ptr = upload_vec(spptr, s);
+    sp_r = upload_vec(spr, s);
+    sp_c = upload_vec(spc, s);
+    sp_v = upload_vec(spv, s);
+
+    nr1s = (int) r1sid.size();
+    r1s_id = upload_vec(r1sid, s);
+    r1s_ptr = upload_vec(r1sptr, s);
+    r1s_p = upload_vec(r1sp, s);
+    r1s_a = upload_vec(r1sa, s);
+    r1s_sign = upload_vec(r1ssg, s);
+
+    nr1d = (int) r1did.size();
+    r1d_id = upload_vec(r1did, s);
+    r1d_sign = upload_vec(r1dsg, s);
+    if (nr1d > 0) {
+        std::vector<double> hA1((size_t) ld * nr1d, 0.0);
+        for (int a = 0; a < nr1d; ++a) {
+            const HostCoeff &c = A[r1did[a]];
+            for (size_t t = 0; t < c.aidx.size(); ++t) hA1[(size_t) a * ld + c.aidx[t]] = c.aval[t];
+        }
+        A1 = upload_vec(hA1, s);
+        HB_CUDA(cudaMalloc(&G, sizeof(double) * pad_ld(nr1d) * nr1d));
+    }
+    const int vcols = std::max(std::max(nr1d, nr1s), 1);
+    HB_CUDA(cudaMalloc(&V, sizeof(double) * ld * vcols));
+
+    ndr = (int) dr_id.size();
+    for (int i = 0; i < ndr; ++i) {
+        const HostCoeff &c = A[dr_id[i]];
+        double *mat = nullptr;
+        HB_CUDA(cudaMalloc(&mat, sizeof(double) * ld * n));
+        HB_CUDA(cudaMemsetAsync(mat, 0, sizeof(double) * ld * n, s));
+        int *dr = upload_vec(c.r, s), *dc = upload_vec(c.c, s);
+        double *dv = upload_vec(c.v, s);
+        if (!c.r.empty())
+            scatter_sym_kernel<<<grid1((long) c.r.size()), 256, 0, s>>>((int) c.r.size(), dr, dc, dv, mat, ld);
+        HB_CUDA(cudaStreamSynchronize(s));
+        cudaFree(dr);
+        cudaFree(dc);
+        cudaFree(dv);
+        dr_mat.push_back(mat);
+    }
+
+    // S-assembly gather map
+    std::vector<int> pr, pc, pptr{0}, ej;
+    std::vector<double> ev;
+    pr.reserve(posorder.size());
+    for (long long key : posorder) {
+        pr.push_back((int) (key / n));
+        pc.push_back((int) (key % n));
+        for (auto &e : posmap[key]) {
+            ej.push_back(e.first);
+            ev.push_back(e.second);
+        }
+        pptr.push_back((int) ej.size());
+    }
+    npos = (int) pr.size();
+    pos_r = upload_vec(pr, s);
+    pos_c = upload_vec(pc, s);
+    pos_ptr = upload_vec(pptr, s);
+    ent_j = upload_vec(ej, s);
+    ent_v = upload_vec(ev, s);
+
+    HB_CUDA(cudaMalloc(&T1, sizeof(double) * ld * n));
+    HB_CUDA(cudaMalloc(&T2, sizeof(double) * ld * n));
+    HB_CUDA(cudaMalloc(&vecbuf, sizeof(double) * std::max(m, 1)));
+    HB_CUDA(cudaMalloc(&d_w, sizeof(double) * (std::max(m, nr1d) + 1)));
+    HB_CUDA(cudaMalloc(&d_scal, sizeof(double) * 16));
+    HB_CUDA(cudaMallocHost(&h_scal, sizeof(double) * 16));
+    HB_CUDA(cudaStreamSynchronize(s));
+}
+
+void SdpDevice::release() {
+    auto f = [](void *p) { if (p) cudaFree(p); };
+    f(Cfull);
+    f(sp_id); f(sp_ptr); f(sp_r); f(sp_c); f(sp_v);
+    f(r1s_id); f(r1s_ptr); f(r1s_p); f(r1s_a); f(r1s_sign);
+    f(r1d_id); f(r1d_sign); f(A1); f(G); f(V);
+    for (double *p : dr_mat) f(p);
+    dr_mat.clear();
+    f(pos_r); f(pos_c); f(pos_ptr); f(ent_j); f(ent_v);
+    f(T1); f(T2); f(vecbuf); f(d_w); f(d_scal);
+    if (h_scal) cudaFreeHost(h_scal);
+    h_scal = nullptr;
+}
+
+void SdpDevice::assemble(double dC, double dA, const double *d_wvec, double dEye, double *S, long ldS) {
+    cudaStream_t s = stream;
+    s_init_kernel<<<grid1((long) n * n), 256, 0, s>>>(n, Cfull, ld, dC, dEye, S, ldS);
+    if (dA != 0.0) {
+        if (npos > 0)
+            s_gather_kernel<<<grid1(npos), 256, 0, s>>>(npos, pos_r, pos_c, pos_ptr, ent_j, ent_v, d_wvec, dA, S, ldS);
+        if (nr1d > 0) {
+            r1d_weights_kernel<<<grid1(nr1d), 256, 0, s>>>(nr1d, r1d_id, r1d_sign, d_wvec, dA, d_w);
+            scale_columns(s, n, nr1d, A1, ld, d_w, V, ld);
+            gemm(s, n, n, nr1d, 1.0, V, ld, 0, A1, ld, 1, 1.0, S, ldS, 0);
+        }
+        for (int i = 0; i < ndr; ++i)
+            axpy_mat_devscale_kernel<<<grid1((long) n * n), 256, 0, s>>>(n, dr_mat[i], ld, d_wvec, dr_id[i], dA, S, ldS);
+    }
+    HB_CUDA(cudaGetLastError());
+}
+
+void SdpDevice::schur_matrix(const double *W, long ldW, double *M, long ldM) {
+    cudaStream_t s = stream;
+    HB_CUDA(cudaMemsetAsync(M, 0, sizeof(double) * ldM * m, s));
+    dim3 blk(16, 16);
+    if (nsp > 0) {
+        dim3 grd((nsp + 15) / 16, (nsp + 15) / 16);
+        schur_spsp_kernel<<<grd, blk, 0, s>>>(nsp, sp_id, sp_ptr, sp_r, sp_c, sp_v, W, ldW, M, ldM);
+    }
+    if (nr1s > 0) {
+        dim3 grd((nr1s + 15) / 16, (nr1s + 15) / 16);
+        schur_r1s_kernel<<<grd, blk, 0, s>>>(nr1s, r1s_id, r1s_ptr, r1s_p, r1s_a, r1s_sign, W, ldW, M, ldM);
+    }
+    if (nr1d > 0) {
+        // V = W * A1,  G = A1^T V (lower),  M = (s s^T) o G o G
+        gemm(s, n, nr1d, n, 1.0, W, ldW, 0, A1, ld, 0, 0.0, V, ld, 0);
+        const long ldg = pad_ld(nr1d);
+        gemm(s, nr1d, nr1d, n, 1.0, A1, ld, 1, V, ld, 0, 0.0, G, ldg, GEMM_C_LOWER);
+        dim3 grd((nr1d + 15) / 16, (nr1d + 15) / 16);
+        schur_hadamard_kernel<<<grd, blk, 0, s>>>(nr1d, r1d_id, r1d_sign, G, ldg, M, ldM);
+        if (nr1s > 0) {
+            dim3 g2((nr1s + 15) / 16, (nr1d + 15) / 16);
+            schur_r1d_r1s_kernel<<<g2, blk, 0, s>>>(nr1d, r1d_id, r1d_sign, V, ld, nr1s, r1s_id, r1s_ptr, r1s_p,
+                                                    r1s_a, r1s_sign, M, ldM);
+        }
+        if (nsp > 0) {
+            dim3 g3((nsp + 15) / 16, (nr1d + 15) / 16);
+            schur_r1_sp_kernel<<<g3, blk, 0, s>>>(nr1d, r1d_id, r1d_sign, V, ld, nsp, sp_id, sp_ptr, sp_r, sp_c,
+                                                  sp_v, M, ldM);
+        }
+    }
+    if (nr1s > 0 && nsp > 0) {
+        double *Vs = nullptr;
+        HB_CUDA(cudaMallocAsync(&Vs, sizeof(double) * ld * nr1s, s));
+        dim3 gv(grid1(n) > 64 ? 64 : grid1(n), nr1s);
+        r1s_build_v_kernel<<<gv, 256, 0, s>>>(n, nr1s, r1s_ptr, r1s_p, r1s_a, W, ldW, Vs, ld);
+        dim3 g3((nsp + 15) / 16, (nr1s + 15) / 16);
+        schur_r1_sp_kernel<<<g3, blk, 0, s>>>(nr1s, r1s_id, r1s_sign, Vs, ld, nsp, sp_id, sp_ptr, sp_r, sp_c, sp_v,
+                                              M, ldM);
+        HB_CUDA(cudaFreeAsync(Vs, s));
+    }
+    for (int i = 0; i < ndr; ++i) {
+        // B_i = W A_i W, then M_ij = <A_j, B_i>
+        gemm(s, n, n, n, 1.0, dr_mat[i], ld, 0, W, ldW, 0, 0.0, T1, ld, 0);
+        gemm(s, n, n, n, 1.0, W, ldW, 0, T1, ld, 0, 0.0, T2, ld, 0);
+        symmetrize_avg(s, n, T2, ld);
+        inner_all(T2, ld, vecbuf);
+        scatter_row_kernel<<<grid1(m), 256, 0, s>>>(m, dr_id[i], vecbuf, M, ldM);
+    }
+    HB_CUDA(cudaGetLastError());
+}
+
+void SdpDevice::inner_all(const double *Z, long ldZ, double *out) {
+    cudaStream_t s = stream;
+    if (nsp > 0) inner_sp_kernel<<<grid1(nsp), 256, 0, s>>>(nsp, sp_id, sp_ptr, sp_r, sp_c, sp_v, Z, ldZ, out);
+    if (nr1s > 0)
+        inner_r1s_kernel<<<grid1(nr1s), 256, 0, s>>>(nr1s, r1s_id, r1s_ptr, r1s_p, r1s_a, r1s_sign, Z, ldZ, out);
+    if (nr1d > 0) {
+        double *Vt = nullptr;
+        HB_CUDA(cudaMallocAsync(&Vt, sizeof(double) * ld * nr1d, s));
+        gemm(s, n, nr1d, n, 1.0, Z, ldZ, 0, A1, ld, 0, 0.0, Vt, ld, 0);
+        coldot_pair_kernel<<<(nr1d * 32 + 255) / 256, 256, 0, s>>>(n, nr1d, r1d_id, r1d_sign, A1, ld, Vt, ld, out);
+        HB_CUDA(cudaFreeAsync(Vt, s));
+    }
+    for (int i = 0; i < ndr; ++i) frob_dot(s, n, dr_mat[i], ld, Z, ldZ, out + dr_id[i]);
+    HB_CUDA(cudaGetLastError());
+}
+
+void SdpDevice::inner_all_sq(const double *W, long ldW, double *out) {
+    cudaStream_t s = stream;
+    if (nsp > 0)
+        innersq_sp_kernel<<<(nsp * 32 + 255) / 256, 256, 0, s>>>(n, nsp, sp_id, sp_ptr, sp_r, sp_c, sp_v, W, ldW, out);
+    if (nr1s > 0)
+        innersq_r1s_kernel<<<(nr1s * 32 + 255) / 256, 256, 0, s>>>(n, nr1s, r1s_id, r1s_ptr, r1s_p, r1s_a, r1s_sign,
+                                                                   W, ldW, out);
+    if (nr1d > 0) {
+        double *Vt = nullptr;
+        HB_CUDA(cudaMallocAsync(&Vt, sizeof(double) * ld * nr1d, s));
+        gemm(s, n, nr1d, n, 1.0, W, ldW, 0, A1, ld, 0, 0.0, Vt, ld, 0);
+        coldot_pair_kernel<<<(nr1d * 32 + 255) / 256, 256, 0, s>>>(n, nr1d, r1d_id, r1d_sign, Vt, ld, Vt, ld, out);
+        HB_CUDA(cudaFreeAsync(Vt, s));
+    }
+    for (int i = 0; i < ndr; ++i) {
+        gemm(s, n, n, n, 1.0, dr_mat[i], ld, 0, W, ldW, 0, 0.0, T1, ld, 0);
+        frob_dot(s, n, T1, ld, W, ldW, out + dr_id[i]);
+    }
+    HB_CUDA(cudaGetLastError());
+}
+
+double SdpDevice::c_inner(const double *Z, long ldZ) {
+    frob_dot(stream, n, Cfull, ld, Z, ldZ, d_scal);
+    HB_CUDA(cudaMemcpyAsync(h_scal, d_scal, sizeof(double), cudaMemcpyDeviceToHost, stream));
+    HB_CUDA(cudaStreamSynchronize(stream));
+    return h_scal[0];
+}
+
+}  // namespace hb

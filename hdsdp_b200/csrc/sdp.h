@@ -1,0 +1,98 @@
+// Device representation of one dense SDP block and the kernels that touch
+// its coefficient matrices: dual-slack assembly S = dC*C + dA*sum_j w_j A_j +
+// dEye*I, Schur-complement assembly M_ij = <A_i, W A_j W> for a symmetric
+// W (S^-1 in the dual method, X in primal refinement), and the inner-product
+// vectors <A_j, Z> and <A_j, W^2>.
+//
+// Constraint classes (chosen at presolve, every class pair is covered):
+//   SP   sparse triplets, at most kSpMax lower-triangle entries  -> gathers from W
+//   R1S  rank one s*a*a^T with at most kR1SmallMax nonzeros      -> gathers from W
+//   R1D  rank one with a denser factor                            -> GEMMs V = W*A1, G = A1^T*V
+//   DR   dense or heavily populated coefficient                   -> B = W*A*W by GEMM, then gathers
+//   ZERO no contribution
+// Reference: interface/hdsdp_conic_sdp.c:683-981 (strategies M2-M5, which all
+// compute the same M, cross-checked by HUtilKKTCheck at interface/hdsdp_utils.c:293-464).
+#pragma once
+#include <vector>
+#include <cuda_runtime.h>
+#include "la.h"
+
+namespace hb {
+
+constexpr int kSpMax = 16;
+constexpr int kR1SmallMax = 8;
+
+enum CoeffClass { CLS_ZERO = 0, CLS_SP = 1, CLS_R1S = 2, CLS_R1D = 3, CLS_DR = 4 };
+
+// Host-side description of one coefficient matrix after presolve.
+struct HostCoeff {
+    int cls = CLS_ZERO;
+    // SP / DR sparse source: lower-triangle triplets (row >= col)
+    std::vector<int> r, c;
+    std::vector<double> v;
+    // rank one: sign * a a^T, a stored sparse (idx ascending)
+    double sign = 0.0;
+    std::vector<int> aidx;
+    std::vector<double> aval;
+    // DR from a dense packed column: full lower packed values (n(n+1)/2) or triplets above
+    bool dense_packed = false;
+    std::vector<double> packed;
+};
+
+struct SdpDevice {
+    int n = 0, m = 0;
+    long ld = 0;
+    cudaStream_t stream = nullptr;
+
+    // Objective, full symmetric n x n
+    double *Cfull = nullptr;
+
+    // SP class
+    int nsp = 0;
+    int *sp_id = nullptr, *sp_ptr = nullptr, *sp_r = nullptr, *sp_c = nullptr;
+    double *sp_v = nullptr;
+    // R1S class
+    int nr1s = 0;
+    int *r1s_id = nullptr, *r1s_ptr = nullptr, *r1s_p = nullptr;
+    double *r1s_a = nullptr, *r1s_sign = nullptr;
+    // R1D class: A1 is n x nr1d dense
+    int nr1d = 0;
+    int *r1d_id = nullptr;
+    double *r1d_sign = nullptr;
+    double *A1 = nullptr;
+    // DR class: full n x n matrices
+    int ndr = 0;
+    std::vector<int> dr_id;
+    std::vector<double *> dr_mat;
+    // S assembly gather map over SP and R1S lower entries
+    int npos = 0;
+    int *pos_r = nullptr, *pos_c = nullptr, *pos_ptr = nullptr, *ent_j = nullptr;
+    double *ent_v = nullptr;
+
+    // scratch
+    double *V = nullptr;       // n x max(nr1d, nr1s) (W * A_r1)
+    double *G = nullptr;       // nr1d x nr1d
+    double *T1 = nullptr;      // n x n
+    double *T2 = nullptr;      // n x n
+    double *vecbuf = nullptr;  // m
+    double *d_w = nullptr;     // m + 1 weights
+    double *d_scal = nullptr;  // small scalars
+    double *h_scal = nullptr;  // pinned mirror
+
+    void upload(int n_, int m_, const HostCoeff &C, const std::vector<HostCoeff> &A, cudaStream_t s);
+    void release();
+
+    // S = dC*C + dA*sum_j w_j A_j + dEye*I (full symmetric), w on device (length m)
+    void assemble(double dC, double dA, const double *d_wvec, double dEye, double *S, long ldS);
+
+    // Schur complement M (m x m, lower triangle written) from symmetric W.
+    void schur_matrix(const double *W, long ldW, double *M, long ldM);
+    // out[j] = <A_j, Z> for all j (Z full symmetric)
+    void inner_all(const double *Z, long ldZ, double *out);
+    // out[j] = <A_j, W^2> for all j
+    void inner_all_sq(const double *W, long ldW, double *out);
+    // <C, Z>
+    double c_inner(const double *Z, long ldZ);
+};
+
+}  // namespace hb

@@ -1,0 +1,193 @@
+// Internal structures of the B200 HDSDP solver.
+//
+// The host side holds the interior-point control flow and all m-vectors
+// (y, dy, Schur right-hand sides); n x n and m x m matrices live on the GPU.
+// Every cone / KKT operation mirrors one hook of the reference's conic
+// callback interface (interface/def_hdsdp_conic.h:56-104) and KKT manager
+// (interface/hdsdp_schur.h:10-21) with the same buffer semantics:
+// BUFFER_DUALVAR (S and its factor), BUFFER_DUALCHECK (trial S and its
+// factor), BUFFER_DUALSTEP (dS).
+#pragma once
+#include <vector>
+#include <string>
+#include <cuda_runtime.h>
+#include "la.h"
+#include "sdp.h"
+#include "../../include/hdsdp.h"
+#include "../../include/hdsdp_user_data.h"
+
+struct hdsdp_user_data {
+    cone_type cone;
+    int nConicRow;
+    int nConicCol;
+    int *coneMatBeg;
+    int *coneMatIdx;
+    double *coneMatElem;
+};
+
+namespace hb {
+
+enum { BUFFER_DUALVAR = 0, BUFFER_DUALCHECK = 1, BUFFER_DUALSTEP = 2 };
+enum { KKT_TYPE_INFEASIBLE = 0, KKT_TYPE_CORRECTOR = 1, KKT_TYPE_HOMOGENEOUS = 2, KKT_TYPE_PRIMAL = 3 };
+enum { REF_ZERO = 0, REF_SPARSE = 1, REF_DENSE = 2, REF_SPR1 = 3, REF_DSR1 = 4 };
+enum { ABS_NORM = 1, FRO_NORM = 2 };
+
+// Per-solve timing split (seconds, device-synchronised at each phase edge).
+struct Timers {
+    double schur = 0, schur_factor = 0, schur_solve = 0, s_factor = 0, s_inverse = 0, lanczos = 0,
+           assemble = 0, primal = 0, total = 0;
+    long n_schur = 0, n_sfactor = 0, n_lanczos = 0, n_lanczos_mv = 0, n_schur_solve = 0;
+};
+
+// Lanczos maximum-step estimator (linalg/hdsdp_lanczos.c:161-292) on the GPU.
+struct Lanczos {
+    int n = 0, maxdim = 30;
+    long ld = 0;
+    cudaStream_t s = nullptr;
+    double *V = nullptr, *w = nullptr, *z1 = nullptr, *z2 = nullptr, *t1 = nullptr, *warm = nullptr;
+    double *d_ab = nullptr;   // alpha[0..maxdim), beta[maxdim..2*maxdim+1)
+    double *h_ab = nullptr;   // pinned
+    double *d_y = nullptr;    // 2 * (maxdim + 1)
+    double *d_scal = nullptr, *h_scal = nullptr;
+    double *init_vec = nullptr, *pert_vec = nullptr;  // device, deterministic per n
+    int nComputed = 0;
+    void init(int n_, cudaStream_t s_);
+    void release();
+    // Max alpha with  I + alpha * K (-D) K^T  psd, where K = L^-1 of the factor.
+    hdsdp_retcode solve(DenseFactor &F, const double *D, long ldD, double *maxStep, Timers *tm);
+};
+
+// Dense SDP cone on the device (interface/hdsdp_conic_sdp.c dense half).
+struct SdpCone {
+    int n = 0, m = 0;
+    long ld = 0;
+    cudaStream_t s = nullptr;
+    SdpDevice dev;
+    HostCoeff C;
+    std::vector<HostCoeff> A;
+    std::vector<int> refType;    // reference coefficient type per row after presolve
+    int refTypeC = REF_ZERO;
+    int stats[5] = {0, 0, 0, 0, 0};
+    double *Svar = nullptr, *Scheck = nullptr, *dS = nullptr, *W = nullptr;
+    DenseFactor Fvar, Fcheck;
+    Lanczos lz;
+    double dualResidual = 0.0, dualPerturb = 0.0;
+    double *d_y = nullptr;       // device copy of the current coefficient vector
+    double *d_vec = nullptr;     // device m scratch
+    double *h_vec = nullptr;     // pinned m scratch
+    double *d_scal = nullptr, *h_scal = nullptr;
+    double objScal = 1.0;
+    Timers *tm = nullptr;
+    int precision = 0;
+
+    hdsdp_retcode proc_data(int nRow, int nCol, const int *Ap, const int *Ai, const double *Ax);
+    hdsdp_retcode presolve();
+    hdsdp_retcode setup_device(cudaStream_t stream, Timers *t);
+    void release();
+
+    double obj_norm(int type) const;
+    double coeff_norm(int type) const;
+    void scal(double a);
+    void detect_feature(const double *rowRHS, int intF[20], double dblF[20]) const;
+
+    void update_buffer(double dC, double dAs, const double *y, double dEye, int which);
+    void set_start(double r) { dualResidual = r; }
+    void reduce_resi(double r) { dualResidual = r; }
+    void set_perturb(double p) { dualPerturb = p; }
+    hdsdp_retcode update(double tau, const double *y);
+    hdsdp_retcode ratio_test(double dtau, const double *dy, double ada, int which, double *step);
+    hdsdp_retcode interior_check(double tau, const double *y, int *interior);
+    hdsdp_retcode interior_check_expert(double dC, double dAs, const double *y, double dEye, int which, int *interior);
+    hdsdp_retcode get_barrier(double tau, const double *y, int which, double *logdet);
+    hdsdp_retcode add_step_and_check(double step, int which, int *interior);
+    void get_primal(double mu, const double *y, const double *dy, double *X);   // device X (ld)
+    void get_dual(double *S);                                                  // device S (ld)
+    void atimesx(const double *X, double *out);                                // host out (m), overwritten
+    double trace_cx(const double *X);
+};
+
+// Scalar dual box l <= y <= u (interface/hdsdp_conic_bound.c), host-side O(m).
+struct BoundCone {
+    int m = 0;
+    double lo = -1e7, up = 1e7;
+    std::vector<double> dl, du, dlInv, duInv, dlStep, duStep, dlChk, duChk;
+    void proc(int m_, double l, double u);
+    void update_buffer(double dC, double dAs, const double *y, int which);
+    void update(double tau, const double *y) { update_buffer(tau, -1.0, y, BUFFER_DUALVAR); }
+    double ratio_test(double dtau, const double *dy, int which);
+    int interior_check(double tau, const double *y);
+    int interior_check_expert(double dC, double dAs, const double *y, int which);
+    hdsdp_retcode get_barrier(double tau, const double *y, int which, double *logdet);
+    int add_step_and_check(double step, int which);
+    void get_primal(double mu, const double *y, const double *dy, double *lower, double *upper) const;
+};
+
+// Schur complement system (interface/hdsdp_schur.c).
+struct KKT {
+    int m = 0;
+    long ldm = 0;
+    cudaStream_t s = nullptr;
+    double *M = nullptr;          // device m x m
+    DenseFactor F;
+    std::vector<double> asinv, asinvrd, asinvcs;
+    double dCSinv = 0, dCSinvCSinv = 0, dCSinvRdSinv = 0, dTraceSinv = 0;
+    double *d_rhs = nullptr, *d_x = nullptr, *d_r = nullptr, *d_t = nullptr, *d_diag = nullptr;
+    double *h_buf = nullptr;
+    std::vector<double> diag_add;     // bound-cone diagonal accumulated before factorisation
+    double shift = 0.0;               // diagonal shift applied if the Cholesky of M failed
+    const double *primalX = nullptr;  // device X for KKT_TYPE_PRIMAL
+    Timers *tm = nullptr;
+    void init(int m_, cudaStream_t stream, Timers *t);
+    void release();
+    void clean(int type);
+    hdsdp_retcode build(SdpCone &cone, int type);
+    void add_bound(BoundCone &b, int type);
+    void regularize(double reg);
+    hdsdp_retcode factorize();
+    hdsdp_retcode solve(const double *rhs, double *lhs);   // host vectors; lhs may alias rhs
+};
+
+// Per-iteration record for time-to-gap reporting.
+struct IterRecord {
+    double t, pobj, dobj, mu, gap;
+    int phase;
+};
+
+}  // namespace hb
+
+struct hdsdp_solver_internal {
+    int nRows = 0;
+    int nCones = 0;
+    std::vector<double> rowRHS;
+    hb::SdpCone *cone = nullptr;
+    user_data *usr = nullptr;
+    hb::BoundCone bnd;
+    hb::KKT kkt;
+    cudaStream_t stream = nullptr;
+    hb::Timers timers;
+
+    std::vector<double> y, dy, d1, d2, d3, d4, aux1, aux2, pInfUp, pInfLow;
+    std::vector<double> accY, accDy, inaccY, inaccDy;
+    double tau = 1.0, dtau = 0.0;
+    double dTraceSinv = 0.0;
+    int whichMethod = 0;
+    int nIterCount = 0;
+    int nSmallStep = 0;
+    double mu = 1e10, proxNorm = 0, potentialVal = 0, barrierVal = 0, dStep = 0, resi = 0, perturb = 0;
+    double allConeDims = 0;
+    double pObjVal = 0, dObjVal = 0, pObjInternal = 0, dObjInternal = 0, dObjImprove = 0;
+    double pInfeas = 0, dInfeas = 0, comp = HDSDP_INFINITY;
+    double accMu = -1.0, inaccMu = -1.0;
+    double timeBegin = 0;
+    hdsdp_status HStatus = HDSDP_UNKNOWN;
+    int HIntParams[20] = {0};
+    double HDblParams[20] = {0};
+    int HIntFeatures[20] = {0};
+    double HDblFeatures[20] = {0};
+    double dErrs[6] = {0};
+    bool optimized = false;
+    int precision = 0;
+    int verbose = 0;
+    std::vector<hb::IterRecord> log;
+    std::string modelFeatures;
+};

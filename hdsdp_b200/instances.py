@@ -1,0 +1,213 @@
+"""Seeded synthetic SDP instances in HDSDP's user-data layout.
+
+An SDP block is handed to ``HUserDataSetConeData`` as a CSC matrix with
+``n(n+1)/2`` rows and ``m+1`` columns (interface/def_hdsdp_user_data.h:11-21):
+column 0 holds the objective C, column i the constraint matrix A_i, and the
+row index of the lower-triangle entry (i, j), i >= j, is
+``PACK_IDX(n, i, j) = (2n - j - 1) j / 2 + i`` (interface/hdsdp_utils.h:49).
+An off-diagonal packed entry stands for the symmetric pair (i, j) and (j, i).
+
+The problem solved is ``min <C, X>  s.t.  <A_i, X> = b_i,  X psd``.
+
+Each generator follows one workload of the benchmark suite; they are seeded
+stand-ins for public instances (no benchmark data is shipped).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+
+def pack_idx(n: int, i, j):
+    """Packed lower-triangle row index of entry (i, j) with i >= j."""
+    i = np.asarray(i, dtype=np.int64)
+    j = np.asarray(j, dtype=np.int64)
+    return ((2 * n - j - 1) * j) // 2 + i
+
+
+@dataclass
+class SDPInstance:
+    """One dense SDP block plus the right-hand side, in the reference layout."""
+
+    name: str
+    n: int
+    m: int
+    Ap: np.ndarray  # int32, m + 2
+    Ai: np.ndarray  # int32, nnz
+    Ax: np.ndarray  # float64, nnz
+    b: np.ndarray   # float64, m
+    meta: dict = field(default_factory=dict)
+
+    def column(self, k: int):
+        """(packed row indices, values) of column k (0 = C, k = A_k)."""
+        s, e = int(self.Ap[k]), int(self.Ap[k + 1])
+        return self.Ai[s:e], self.Ax[s:e]
+
+    def dense(self, k: int) -> np.ndarray:
+        """Column k expanded to a full symmetric n x n matrix (small n only)."""
+        n = self.n
+        rows, vals = self.column(k)
+        # invert PACK_IDX column by column
+        M = np.zeros((n, n))
+        starts = pack_idx(n, np.arange(n), np.arange(n))
+        j = np.searchsorted(starts, rows, side="right") - 1
+        i = rows - starts[j] + j
+        M[i, j] = vals
+        M[j, i] = vals
+        return M
+
+
+def _assemble(name, n, cols, b, meta=None) -> SDPInstance:
+    """cols: list of (packed_idx, values) for C, A_1..A_m."""
+    m = len(cols) - 1
+    Ap = np.zeros(m + 2, dtype=np.int64)
+    idx_parts, val_parts = [], []
+    for k, (idx, val) in enumerate(cols):
+        idx = np.asarray(idx, dtype=np.int64)
+        val = np.asarray(val, dtype=np.float64)
+        order = np.argsort(idx, kind="stable")
+        idx, val = idx[order], val[order]
+        if idx.size > 1 and np.any(np.diff(idx) == 0):
+            raise ValueError("duplicate packed entries in column %d" % k)
+        idx_parts.append(idx)
+        val_parts.append(val)
+        Ap[k + 1] = Ap[k] + idx.size
+    Ai = np.concatenate(idx_parts) if idx_parts else np.zeros(0, np.int64)
+    Ax = np.concatenate(val_parts) if val_parts else np.zeros(0)
+    if Ai.size and Ai.max() >= n * (n + 1) // 2:
+        raise ValueError("packed index out of range")
+    return SDPInstance(name, n, m, Ap.astype(np.int32), Ai.astype(np.int32),
+                       Ax.astype(np.float64), np.asarray(b, dtype=np.float64), meta or {})
+
+
+def _laplacian_objective(n, ei, ej, w):
+    """C = -L/4 for the weighted graph (ei > ej), packed lower triangle."""
+    deg = np.zeros(n)
+    np.add.at(deg, ei, w)
+    np.add.at(deg, ej, w)
+    diag_idx = pack_idx(n, np.arange(n), np.arange(n))
+    keep = deg != 0
+    idx = np.concatenate([diag_idx[keep], pack_idx(n, ei, ej)])
+    val = np.concatenate([-deg[keep] / 4.0, w / 4.0])
+    return idx, val
+
+
+def _erdos_renyi_edges(n, p, rng):
+    iu = np.tril_indices(n, -1)
+    mask = rng.random(iu[0].size) < p
+    return iu[0][mask].astype(np.int64), iu[1][mask].astype(np.int64)
+
+
+def maxcut(n: int = 200, p: float = 0.05, seed: int = 1, n_edges: int | None = None,
+           weights: tuple | None = None) -> SDPInstance:
+    """MaxCut SDP relaxation: min <-L/4, X> s.t. diag(X) = 1.
+
+    With ``n_edges`` set, that many distinct edges are drawn uniformly (the
+    large sparse case); otherwise G(n, p). Weights are 1, or U(lo, hi).
+    """
+    rng = np.random.default_rng(seed)
+    if n_edges is None:
+        ei, ej = _erdos_renyi_edges(n, p, rng)
+    else:
+        picks = set()
+        while len(picks) < n_edges:
+            u = rng.integers(0, n, size=2 * (n_edges - len(picks)) + 16)
+            v = rng.integers(0, n, size=u.size)
+            for a, c in zip(u.tolist(), v.tolist()):
+                if a == c:
+                    continue
+                picks.add((max(a, c), min(a, c)))
+                if len(picks) == n_edges:
+                    break
+        pairs = np.array(sorted(picks), dtype=np.int64)
+        ei, ej = pairs[:, 0], pairs[:, 1]
+    if weights is None:
+        w = np.ones(ei.size)
+    else:
+        w = rng.uniform(weights[0], weights[1], size=ei.size)
+    cols = [_laplacian_objective(n, ei, ej, w)]
+    for i in range(n):
+        cols.append(([pack_idx(n, i, i)], [1.0]))
+    b = np.ones(n)
+    return _assemble("maxcut", n, cols, b, {"edges": int(ei.size), "seed": seed})
+
+
+def lovasz_theta(n: int = 300, p: float = 0.1, seed: int = 2) -> SDPInstance:
+    """Lovasz theta SDP: min <-J, X> s.t. tr(X) = 1, X_ij = 0 for edges ij."""
+    rng = np.random.default_rng(seed)
+    ei, ej = _erdos_renyi_edges(n, p, rng)
+    npack = n * (n + 1) // 2
+    cols = [(np.arange(npack), -np.ones(npack))]
+    cols.append((pack_idx(n, np.arange(n), np.arange(n)), np.ones(n)))
+    for a, c in zip(ei.tolist(), ej.tolist()):
+        cols.append(([pack_idx(n, a, c)], [1.0]))
+    b = np.zeros(1 + ei.size)
+    b[0] = 1.0
+    return _assemble("theta", n, cols, b, {"edges": int(ei.size), "seed": seed})
+
+
+def rank_one(n: int = 1000, m: int = 2000, density: float = 0.1, seed: int = 3) -> SDPInstance:
+    """Random rank-one SDP: A_i = a_i a_i^T with a fixed support size.
+
+    X0 = I + G G^T / n (G is n x 20) is primal feasible, b_i = a_i^T X0 a_i,
+    and C = I + R with R symmetric, 1% of off-diagonal pairs U(-0.1, 0.1),
+    so the dual is strictly feasible.
+    """
+    rng = np.random.default_rng(seed)
+    k = max(1, int(round(density * n)))
+    G = rng.standard_normal((n, 20))
+    cols = []
+    # objective
+    iu = np.tril_indices(n, -1)
+    mask = rng.random(iu[0].size) < 0.01
+    ri, rj = iu[0][mask], iu[1][mask]
+    rv = rng.uniform(-0.1, 0.1, size=ri.size)
+    cidx = np.concatenate([pack_idx(n, np.arange(n), np.arange(n)), pack_idx(n, ri, rj)])
+    cval = np.concatenate([np.ones(n), rv])
+    cols.append((cidx, cval))
+    b = np.zeros(m)
+    for t in range(m):
+        supp = np.sort(rng.choice(n, size=k, replace=False))
+        a = rng.standard_normal(k)
+        # lower triangle of a a^T on the support
+        I, J = np.tril_indices(k)
+        cols.append((pack_idx(n, supp[I], supp[J]), a[I] * a[J]))
+        Ga = G[supp].T @ a
+        b[t] = a @ a + Ga @ Ga / n
+    return _assemble("rank_one", n, cols, b, {"support": k, "seed": seed})
+
+
+def theta_adjoint(n: int = 200, p: float = 0.1, zero_frac: float = 0.2, seed: int = 5) -> SDPInstance:
+    """Theta-style SDP for the differentiable layer.
+
+    min <-W, X> s.t. tr(X) = 1 and X_ij = 0 on a seeded ``zero_frac`` subset of
+    the non-edges; W symmetric on the edge support with U(0, 1) entries.
+    """
+    rng = np.random.default_rng(seed)
+    ei, ej = _erdos_renyi_edges(n, p, rng)
+    w = rng.uniform(0.0, 1.0, size=ei.size)
+    edge = np.zeros((n, n), dtype=bool)
+    edge[ei, ej] = True
+    iu = np.tril_indices(n, -1)
+    non = ~edge[iu]
+    ni, nj = iu[0][non], iu[1][non]
+    pick = rng.random(ni.size) < zero_frac
+    zi, zj = ni[pick], nj[pick]
+    cols = [(pack_idx(n, ei, ej), -w)]
+    cols.append((pack_idx(n, np.arange(n), np.arange(n)), np.ones(n)))
+    for a, c in zip(zi.tolist(), zj.tolist()):
+        cols.append(([pack_idx(n, a, c)], [1.0]))
+    b = np.zeros(1 + zi.size)
+    b[0] = 1.0
+    return _assemble("theta_adjoint", n, cols, b,
+                     {"edges": int(ei.size), "zeros": int(zi.size), "seed": seed})
+
+
+WORKLOADS = {
+    "maxcut_n200": lambda: maxcut(200, 0.05, seed=1),
+    "theta_n300": lambda: lovasz_theta(300, 0.1, seed=2),
+    "rank1_n1000_m2000": lambda: rank_one(1000, 2000, 0.1, seed=3),
+    "maxcut_n8000": lambda: maxcut(8000, seed=4, n_edges=40000, weights=(0.5, 1.5)),
+    "theta_adjoint_n200": lambda: theta_adjoint(200, 0.1, 0.2, seed=5),
+}

@@ -1,0 +1,86 @@
+/*
+ * hdsdp_b200.h -- entry points that the B200 library adds next to the
+ * reference API of hdsdp.h. None of these has a counterpart in the reference
+ * interface; each comment names the reference code whose behaviour it
+ * exposes.
+ */
+#ifndef HDSDP_B200_EXT_H
+#define HDSDP_B200_EXT_H
+
+#include "hdsdp.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Solver status and iteration count: the reference keeps these in its private
+   solver struct (interface/def_hdsdp.h:111, :122) and has no getter. */
+extern int HDSDPGetStatus( hdsdp *HSolver );
+extern int HDSDPGetIterCount( hdsdp *HSolver );
+
+/* Enable / disable the five-step primal refinement run when Phase B reaches a
+   10% gap (interface/hdsdp_algo.c:1803-1810). The reference's setter refuses
+   index INT_PARAM_PSDP (interface/hdsdp.c:598). With it off, Phase B runs to
+   its own convergence test (interface/hdsdp_algo.c:1797-1801). */
+extern void HDSDPSetPrimalRefinement( hdsdp *HSolver, int on );
+
+/* Schur-assembly arithmetic: 0 = FP64 throughout (default); 1 = split
+   precision (rank-one Schur GEMMs as BF16x3 products with FP32
+   accumulation on the tensor cores, FP64 everywhere else). */
+extern void HDSDPSetPrecision( hdsdp *HSolver, int mode );
+
+/* Per-iteration record of the last solve: elapsed seconds, primal and dual
+   objective, barrier parameter, relative gap (p - d) / (1 + |p| + |d|) and
+   phase (0 infeasible, 1 embedding, 2 potential reduction, 3 refinement),
+   as printed by the reference's iteration log (interface/hdsdp_algo.c:151-193).
+   Returns the number of records (arrays may be NULL to query it). */
+extern int HDSDPGetIterLog( hdsdp *HSolver, int maxLen, double *t, double *pObj, double *dObj,
+                            double *mu, double *gap, int *phase );
+
+/* Wall-clock split of the last solve in seconds:
+   [0] Schur assembly  [1] Schur factorisation  [2] Schur solves  [3] S factorisations
+   [4] S inverse       [5] Lanczos              [6] S assembly    [7] primal recovery
+   [8] total           [9] #Schur builds       [10] #S factorisations
+   [11] #Lanczos runs  [12] #Lanczos matvecs    [13] #Schur solves */
+extern void HDSDPGetTimers( hdsdp *HSolver, double out[14] );
+
+/* ---- Kernel-level entry points (host buffers in, host buffers out) ---------------- */
+
+/* Schur complement of one SDP block given in the user-data CSC layout, at
+   S = C - sum_i y_i A_i - resi * I: the GPU counterpart of the reference's
+   HKKTBuildUp(KKT_TYPE_INFEASIBLE) (interface/hdsdp_schur.c:256-268).
+   Writes M (m x m, lower triangle, column-major), ASinv_i = <A_i, S^-1>,
+   ASinvRdSinv_i = resi <A_i, S^-2> and trace(S^-1).
+   Returns 0 on success, 1 if S is not positive definite, -1 on error. */
+extern int hdsdpb_schur_probe( int m, int n, const int *Ap, const int *Ai, const double *Ax,
+                               const double *y, double resi, int precision, double *M,
+                               double *asinv, double *asinvrd, double *traceSinv );
+
+/* First Lanczos ratio test on S = C - A^T y - resi I along dS = -A^T dy + ada * resi * I
+   (interface/hdsdp_conic_sdp.c:1638-1682), plus log det S.
+   Returns 0 on success, 1 if S is not positive definite, -1 on error. */
+extern int hdsdpb_ratio_probe( int m, int n, const int *Ap, const int *Ai, const double *Ax,
+                               const double *y, double resi, const double *dy, double ada,
+                               double *step, double *logdet );
+
+/* Cholesky factorisation of a symmetric n x n matrix (lower triangle read),
+   with the positive-definiteness test of the reference's dual checks
+   (linalg/hdsdp_linsolver.c:521-553). Writes L (lower, full n x n storage,
+   upper part zero) and sum(log L_ii). Returns 0 if positive definite, 1 if not. */
+extern int hdsdpb_cholesky( int n, const double *S, double *L, double *logdiag );
+
+/* Inverse of a symmetric positive definite n x n matrix through its Cholesky
+   factor (the reference's dpotri use, linalg/hdsdp_linsolver.c:647-669).
+   Returns 0 on success, 1 if not positive definite. */
+extern int hdsdpb_inverse( int n, const double *S, double *Sinv );
+
+/* FP64 GEMM on the tensor-core path: C = alpha op(A) op(B) + beta C with
+   column-major host buffers (op = transpose when trans != 0). */
+extern int hdsdpb_gemm( int M, int N, int K, double alpha, const double *A, int lda, int transA,
+                        const double *B, int ldb, int transB, double beta, double *C, int ldc );
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HDSDP_B200_EXT_H */

@@ -1,0 +1,206 @@
+"""ctypes driver for the reference HDSDP solver built by oracle/Makefile.
+
+TEST INFRASTRUCTURE ONLY. Imported by tests/ (parity checks, golden vectors)
+and by bench.py's reference / CPU-baseline arm; never by the product package.
+
+It feeds an ``SDPInstance`` through the reference's public C API
+(interface/hdsdp.h:105-116, interface/hdsdp_user_data.h:18-23) exactly as a C
+caller would, and reads status / iteration count through oracle/ref_probe.c.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_ref", "libhdsdp_ref.so")
+
+CONETYPE_DENSE_SDP = 4  # interface/def_hdsdp_conic.h:22-32
+
+_lib = None
+
+
+def available() -> bool:
+    return os.path.exists(LIB_PATH)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not available():
+            raise RuntimeError("reference oracle not built: run `make -C oracle` where the reference tree exists")
+        L = C.CDLL(LIB_PATH)
+        vp = C.c_void_p
+        L.HDSDPCreate.argtypes = [C.POINTER(vp)]
+        L.HDSDPInit.argtypes = [vp, C.c_int, C.c_int]
+        L.HDSDPSetCone.argtypes = [vp, C.c_int, vp]
+        L.HDSDPSetDualObjective.argtypes = [vp, C.POINTER(C.c_double)]
+        L.HDSDPOptimize.argtypes = [vp, C.c_int]
+        L.HDSDPSetIntParam.argtypes = [vp, C.c_int, C.c_int]
+        L.HDSDPSetDblParam.argtypes = [vp, C.c_int, C.c_double]
+        L.HDSDPGetRowDual.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        L.HDSDPGetConeValues.argtypes = [vp, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        L.HDSDPCheckSolution.argtypes = [vp, C.POINTER(C.c_double)]
+        L.HDSDPDestroy.argtypes = [C.POINTER(vp)]
+        L.HUserDataCreate.argtypes = [C.POINTER(vp)]
+        L.HUserDataSetConeData.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int),
+                                           C.POINTER(C.c_int), C.POINTER(C.c_double)]
+        L.HUserDataDestroy.argtypes = [C.POINTER(vp)]
+        L.oracle_status.argtypes = [vp]
+        L.oracle_iters.argtypes = [vp]
+        L.oracle_perturb.argtypes = [vp]
+        L.oracle_perturb.restype = C.c_double
+        L.oracle_mu.argtypes = [vp]
+        L.oracle_mu.restype = C.c_double
+        L.oracle_int_param.argtypes = [vp, C.c_int]
+        L.oracle_dbl_param.argtypes = [vp, C.c_int]
+        L.oracle_set_int_param.argtypes = [vp, C.c_int, C.c_int]
+        L.oracle_dbl_param.restype = C.c_double
+        L.oracle_schur_probe.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                         C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_double,
+                                         C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                         C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                         C.POINTER(C.c_double)]
+        L.oracle_ratio_probe.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                         C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_double,
+                                         C.POINTER(C.c_double), C.c_double, C.POINTER(C.c_double),
+                                         C.POINTER(C.c_double)]
+        _lib = L
+    return _lib
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _ip(a):
+    return a.ctypes.data_as(C.POINTER(C.c_int))
+
+
+def set_threads(n: int):
+    """Thread count of the BLAS under the reference (MKL stand-in)."""
+    try:
+        L = C.CDLL(LIB_PATH)
+        L.MKL_Set_Num_Threads(int(n))
+    except OSError:
+        pass
+
+
+def solve(inst, want_x: bool = True, params: dict | None = None, quiet: bool = True) -> dict:
+    """Run HDSDPOptimize on ``inst``; return y, objectives, status, X, S, errors, time."""
+    L = lib()
+    Ap = np.ascontiguousarray(inst.Ap, dtype=np.int32)
+    Ai = np.ascontiguousarray(inst.Ai, dtype=np.int32)
+    Ax = np.ascontiguousarray(inst.Ax, dtype=np.float64)
+    b = np.ascontiguousarray(inst.b, dtype=np.float64)
+    h = C.c_void_p()
+    ud = C.c_void_p()
+    assert L.HDSDPCreate(C.byref(h)) == 0
+    assert L.HUserDataCreate(C.byref(ud)) == 0
+    L.HUserDataSetConeData(ud, CONETYPE_DENSE_SDP, inst.m, inst.n, _ip(Ap), _ip(Ai), _dp(Ax))
+    assert L.HDSDPInit(h, inst.m, 1) == 0
+    assert L.HDSDPSetCone(h, 0, ud) == 0
+    L.HDSDPSetDualObjective(h, _dp(b))
+    for k, v in (params or {}).items():
+        if isinstance(v, int):
+            if k >= 3:
+                L.oracle_set_int_param(h, k, v)
+            else:
+                L.HDSDPSetIntParam(h, k, v)
+        else:
+            L.HDSDPSetDblParam(h, k, float(v))
+    saved = None
+    if quiet:
+        saved = os.dup(1)
+        devnull = os.open(os.devnull, os.O_WRONLY)
+        os.dup2(devnull, 1)
+        os.close(devnull)
+    try:
+        t0 = time.perf_counter()
+        ret = L.HDSDPOptimize(h, 0)
+        t1 = time.perf_counter()
+        y = np.zeros(inst.m)
+        po, do = C.c_double(), C.c_double()
+        L.HDSDPGetRowDual(h, C.byref(po), C.byref(do), _dp(y))
+        out = {"retcode": int(ret), "time": t1 - t0, "y": y, "pobj": po.value, "dobj": do.value,
+               "status": int(L.oracle_status(h)), "iters": int(L.oracle_iters(h)),
+               "perturb": float(L.oracle_perturb(h))}
+        if want_x:
+            n = inst.n
+            X = np.zeros(n * n)
+            S = np.zeros(n * n)
+            aux = np.zeros(n * n)
+            L.HDSDPGetConeValues(h, 0, _dp(X), _dp(S), _dp(aux))
+            out["X"] = X.reshape(n, n, order="F")
+            out["S"] = S.reshape(n, n, order="F")
+        errs = np.zeros(6)
+        L.HDSDPCheckSolution(h, _dp(errs))
+        out["errs"] = errs
+        out["status_after_check"] = int(L.oracle_status(h))
+    finally:
+        if quiet:
+            import sys
+            sys.stdout.flush()
+            os.dup2(saved, 1)
+            os.close(saved)
+    L.HUserDataDestroy(C.byref(ud))
+    L.HDSDPDestroy(C.byref(h))
+    return out
+
+
+def schur_probe(inst, y, resi, type_kkt: int = 0):
+    """Reference Schur complement at (y, resi): returns dict(M lower, asinv, asinvrd, ...)."""
+    L = lib()
+    m, n = inst.m, inst.n
+    Ap = np.ascontiguousarray(inst.Ap, dtype=np.int32)
+    Ai = np.ascontiguousarray(inst.Ai, dtype=np.int32)
+    Ax = np.ascontiguousarray(inst.Ax, dtype=np.float64)
+    y = np.ascontiguousarray(y, dtype=np.float64)
+    M = np.zeros(m * m)
+    asinv = np.zeros(m)
+    asinvrd = np.zeros(m)
+    asinvcs = np.zeros(m)
+    scal = np.zeros(4)
+    saved = os.dup(1)
+    devnull = os.open(os.devnull, os.O_WRONLY)
+    os.dup2(devnull, 1)
+    os.close(devnull)
+    try:
+        r = L.oracle_schur_probe(m, n, _ip(Ap), _ip(Ai), _dp(Ax), _dp(y), float(resi), int(type_kkt),
+                                 _dp(M), _dp(asinv), _dp(asinvrd), _dp(asinvcs), _dp(scal))
+    finally:
+        os.dup2(saved, 1)
+        os.close(saved)
+    if r != 0:
+        raise RuntimeError("schur probe failed (%d)" % r)
+    return {"M": M.reshape(m, m, order="F"), "asinv": asinv, "asinvrd": asinvrd,
+            "asinvcs": asinvcs, "csinv": scal[0], "csinvcsinv": scal[1], "csinvrd": scal[2],
+            "tracesinv": scal[3]}
+
+
+def ratio_probe(inst, y, resi, dy, ada):
+    """Reference Lanczos step bound for S(y) + alpha dS(dy) (first call of a fresh cone)."""
+    L = lib()
+    Ap = np.ascontiguousarray(inst.Ap, dtype=np.int32)
+    Ai = np.ascontiguousarray(inst.Ai, dtype=np.int32)
+    Ax = np.ascontiguousarray(inst.Ax, dtype=np.float64)
+    y = np.ascontiguousarray(y, dtype=np.float64)
+    dy = np.ascontiguousarray(dy, dtype=np.float64)
+    step = C.c_double()
+    logdet = C.c_double()
+    saved = os.dup(1)
+    devnull = os.open(os.devnull, os.O_WRONLY)
+    os.dup2(devnull, 1)
+    os.close(devnull)
+    try:
+        r = L.oracle_ratio_probe(inst.m, inst.n, _ip(Ap), _ip(Ai), _dp(Ax), _dp(y), float(resi),
+                                 _dp(dy), float(ada), C.byref(step), C.byref(logdet))
+    finally:
+        os.dup2(saved, 1)
+        os.close(saved)
+    if r != 0:
+        raise RuntimeError("ratio probe failed (%d)" % r)
+    return step.value, logdet.value
