@@ -183,3 +183,69 @@ int hdsdpb_gemm(int M, int N, int K, double alpha, const double *A, int lda, int
 }
 
 }  // extern "C"
+
+// ---- device-resident kernel timing (CUDA events on the launching stream) ----
+namespace {
+__global__ void fill_spd_kernel(int n, double *A, long ld, unsigned seed) {
+    const long total = (long) n * n;
+    for (long idx = blockIdx.x * (long) blockDim.x + threadIdx.x; idx < total; idx += (long) gridDim.x * blockDim.x) {
+        const int r = (int) (idx % n), c = (int) (idx / n);
+        const int lo = min(r, c), hi = max(r, c);
+        unsigned h = (unsigned) (lo * 2654435761u) ^ (unsigned) (hi * 40503u) ^ seed;
+        h ^= h >> 13; h *= 0x5bd1e995u; h ^= h >> 15;
+        double v = ((double) (h & 0xffffff) / 16777216.0 - 0.5) / n;
+        if (r == c) v += 1.0;
+        A[(size_t) r + (size_t) c * ld] = v;
+    }
+}
+}  // namespace
+
+extern "C" int hdsdpb_kernel_timing(int which, int n, int reps, double *ms) {
+    cudaStream_t s;
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return -1;
+    const long ld = pad_ld(n);
+    double *A = nullptr, *B = nullptr, *Cm = nullptr, *x = nullptr, *y = nullptr;
+    cudaMalloc(&A, sizeof(double) * ld * n);
+    cudaMalloc(&B, sizeof(double) * ld * n);
+    cudaMalloc(&Cm, sizeof(double) * ld * n);
+    cudaMalloc(&x, sizeof(double) * ld);
+    cudaMalloc(&y, sizeof(double) * ld);
+    fill_spd_kernel<<<1024, 256, 0, s>>>(n, A, ld, 1u);
+    fill_spd_kernel<<<1024, 256, 0, s>>>(n, B, ld, 7u);
+    fill(s, x, 1.0, n);
+    DenseFactor F;
+    F.alloc(n);
+    Lanczos lz;
+    if (which == 5) lz.init(n, s);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    auto once = [&]() {
+        switch (which) {
+            case 0: gemm(s, n, n, n, 1.0, A, ld, 0, B, ld, 0, 0.0, Cm, ld, 0); break;
+            case 1: gemm(s, n, n, n, 1.0, A, ld, 1, B, ld, 0, 0.0, Cm, ld, GEMM_C_LOWER); break;
+            case 2: factorize_async(s, F, A, ld); break;
+            case 3: F.k_valid = false; compute_inverse_factor(s, F); break;
+            case 4: coldot(s, n, n, A, ld, x, y, 1.0, 0.0, 0); break;
+            case 5: { double st; lz.solve(F, B, ld, &st, nullptr); } break;
+            case 6: gemm(s, n, n, 64, -1.0, A, ld, 0, B, ld, 1, 1.0, Cm, ld, GEMM_C_LOWER); break;
+        }
+    };
+    if (which == 3 || which == 5) factorize(s, F, A, ld);
+    for (int i = 0; i < 2; ++i) once();
+    cudaStreamSynchronize(s);
+    cudaEventRecord(e0, s);
+    for (int i = 0; i < reps; ++i) once();
+    cudaEventRecord(e1, s);
+    cudaEventSynchronize(e1);
+    float t = 0.f;
+    cudaEventElapsedTime(&t, e0, e1);
+    *ms = t / reps;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (which == 5) lz.release();
+    F.release();
+    for (double *p : {A, B, Cm, x, y}) cudaFree(p);
+    cudaStreamDestroy(s);
+    return device_error_flag() ? -1 : 0;
+}

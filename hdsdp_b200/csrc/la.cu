@@ -159,13 +159,170 @@ __global__ void __launch_bounds__(GT) gemm_kernel(GemmP p) {
 }
 }  // namespace
 
+// ------------------------------------------------------------------------------------
+// Large-tile GEMM: 128 x 128 x 16 CTA tile, 8 warps (4 along M x 2 along N), warp tile
+// 32 x 64 = 4 x 8 DMMA fragments, 3-stage cp.async pipeline with zero-fill predicates.
+// Shared-memory layout per operand follows its global contiguity so the loads stay
+// coalesced; row pitches of 132 / 20 doubles make the fragment reads conflict-free.
+// ------------------------------------------------------------------------------------
+namespace {
+constexpr int L_BM = 128, L_BN = 128, L_BK = 16, L_T = 256, L_ST = 3;
+constexpr int L_PK = L_BM + 4;   // pitch of a k-major tile row (128 contiguous elements)
+constexpr int L_PM = L_BK + 4;   // pitch of an m/n-major tile row (16 contiguous k)
+constexpr int L_STAGE = 2560;    // doubles per operand per stage (max of 16*132, 128*20)
+
+__device__ __forceinline__ void cp_async8(double *sdst, const double *gsrc, bool pred) {
+    const unsigned saddr = (unsigned) __cvta_generic_to_shared(sdst);
+    const int bytes = pred ? 8 : 0;
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(saddr), "l"(gsrc), "r"(bytes));
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+template <int TA, int TB>
+__global__ void __launch_bounds__(L_T) gemm_large_kernel(GemmP p) {
+    const int m0 = blockIdx.x * L_BM;
+    const int n0 = blockIdx.y * L_BN;
+    if ((p.flags & GEMM_C_LOWER) && m0 + L_BM - 1 < n0) return;
+    if (p.abort_flag && *p.abort_flag) return;
+    int kmin = 0, kmax = p.K;
+    if (p.flags & GEMM_A_LOWER) kmax = min(kmax, m0 + L_BM);
+    if (p.flags & GEMM_A_UPPER) kmin = max(kmin, m0);
+    if (p.flags & GEMM_B_LOWER) kmin = max(kmin, n0);
+    if (p.flags & GEMM_B_UPPER) kmax = min(kmax, n0 + L_BN);
+    kmin = (kmin / L_BK) * L_BK;
+    const int nk = (kmax > kmin) ? (kmax - kmin + L_BK - 1) / L_BK : 0;
+
+    extern __shared__ double smem[];
+    double *As = smem;
+    double *Bs = smem + L_ST * L_STAGE;
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    const int wm = (w & 3) * 32, wn = (w >> 2) * 64;
+
+    auto issue = [&](int kt, int stage) {
+        const int k0 = kmin + kt * L_BK;
+        double *as = As + stage * L_STAGE;
+        double *bs = Bs + stage * L_STAGE;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            int m, k;
+            if (!TA) { m = t & 127; k = (t >> 7) + 2 * i; }
+            else { k = t & 15; m = (t >> 4) + 16 * i; }
+            const int gm = m0 + m, gk = k0 + k;
+            bool ok = gm < p.M && gk < p.K;
+            if ((p.flags & GEMM_A_LOWER) && gk > gm) ok = false;
+            if ((p.flags & GEMM_A_UPPER) && gk < gm) ok = false;
+            const double *src = ok ? (TA ? p.A + (size_t) gk + (size_t) gm * p.lda : p.A + (size_t) gm + (size_t) gk * p.lda) : p.A;
+            double *dst = TA ? as + m * L_PM + k : as + k * L_PK + m;
+            cp_async8(dst, src, ok);
+        }
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            int n, k;
+            if (!TB) { k = t & 15; n = (t >> 4) + 16 * i; }
+            else { n = t & 127; k = (t >> 7) + 2 * i; }
+            const int gn = n0 + n, gk = k0 + k;
+            bool ok = gn < p.N && gk < p.K;
+            if ((p.flags & GEMM_B_LOWER) && gk < gn) ok = false;
+            if ((p.flags & GEMM_B_UPPER) && gk > gn) ok = false;
+            const double *src = ok ? (TB ? p.B + (size_t) gn + (size_t) gk * p.ldb : p.B + (size_t) gk + (size_t) gn * p.ldb) : p.B;
+            double *dst = TB ? bs + k * L_PK + n : bs + n * L_PM + k;
+            cp_async8(dst, src, ok);
+        }
+    };
+
+    double acc[4][8][2];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+
+#pragma unroll
+    for (int st = 0; st < L_ST - 1; ++st) {
+        if (st < nk) issue(st, st);
+        cp_commit();
+    }
+    for (int kt = 0; kt < nk; ++kt) {
+        cp_wait<L_ST - 2>();
+        __syncthreads();
+        const int nxt = kt + L_ST - 1;
+        if (nxt < nk) issue(nxt, nxt % L_ST);
+        cp_commit();
+        const double *as = As + (kt % L_ST) * L_STAGE;
+        const double *bs = Bs + (kt % L_ST) * L_STAGE;
+#pragma unroll
+        for (int ks = 0; ks < L_BK; ks += 4) {
+            const int kk = ks + (lane & 3);
+            double a[4], b[8];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const int m = wm + i * 8 + (lane >> 2);
+                a[i] = TA ? as[m * L_PM + kk] : as[kk * L_PK + m];
+            }
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const int n = wn + j * 8 + (lane >> 2);
+                b[j] = TB ? bs[kk * L_PK + n] : bs[n * L_PM + kk];
+            }
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 8; ++j) dmma(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+        }
+    }
+    cp_wait<0>();
+
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int row = m0 + wm + i * 8 + (lane >> 2);
+        if (row >= p.M) continue;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+                const int col = n0 + wn + j * 8 + (lane & 3) * 2 + e;
+                if (col >= p.N) continue;
+                if ((p.flags & GEMM_C_LOWER) && row < col) continue;
+                double *cp = p.C + (size_t) row + (size_t) col * p.ldc;
+                double v = p.alpha * acc[i][j][e];
+                if (p.beta != 0.0) v += p.beta * (*cp);
+                *cp = v;
+            }
+        }
+    }
+}
+
+constexpr int L_SMEM = 2 * L_ST * L_STAGE * (int) sizeof(double);
+
+template <int TA, int TB>
+void launch_large(const GemmP &p, cudaStream_t s) {
+    static bool init = false;
+    if (!init) {
+        HB_CUDA(cudaFuncSetAttribute(gemm_large_kernel<TA, TB>, cudaFuncAttributeMaxDynamicSharedMemorySize, L_SMEM));
+        init = true;
+    }
+    dim3 grid((p.M + L_BM - 1) / L_BM, (p.N + L_BN - 1) / L_BN);
+    gemm_large_kernel<TA, TB><<<grid, L_T, L_SMEM, s>>>(p);
+}
+}  // namespace
+
 void gemm(cudaStream_t s, int M, int N, int K, double alpha, const double *A, long lda, int transA,
           const double *B, long ldb, int transB, double beta, double *C, long ldc, int flags,
           const int *abort_flag) {
     if (M <= 0 || N <= 0) return;
     GemmP p{M, N, K, alpha, beta, A, lda, transA, B, ldb, transB, C, ldc, flags, abort_flag};
-    dim3 grid((M + BM - 1) / BM, (N + BN - 1) / BN);
-    gemm_kernel<<<grid, GT, 0, s>>>(p);
+    // Large tiles once the 128 x 128 grid fills the machine; 64 x 64 tiles otherwise.
+    const long tiles = (long) ((M + L_BM - 1) / L_BM) * ((N + L_BN - 1) / L_BN);
+    if (tiles >= 96 && K >= 64) {
+        if (!transA && !transB) launch_large<0, 0>(p, s);
+        else if (transA && !transB) launch_large<1, 0>(p, s);
+        else if (!transA && transB) launch_large<0, 1>(p, s);
+        else launch_large<1, 1>(p, s);
+    } else {
+        dim3 grid((M + BM - 1) / BM, (N + BN - 1) / BN);
+        gemm_kernel<<<grid, GT, 0, s>>>(p);
+    }
     HB_CUDA(cudaGetLastError());
 }
 

@@ -87,8 +87,8 @@ __global__ void axpy_mat_devscale_kernel(int n, const double *A, long lda, const
 // ---- Schur pair kernels -------------------------------------------------------------
 __global__ void schur_spsp_kernel(int nsp, const int *id, const int *ptr, const int *rr, const int *cc,
                                   const double *vv, const double *W, long ldw, double *M, long ldm) {
-    const int a = blockIdx.y * blockDim.y + threadIdx.y;
-    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    const int b = blockIdx.y * blockDim.y + threadIdx.y;
     if (a >= nsp || b > a) return;
     double acc = 0.0;
     for (int e = ptr[a]; e < ptr[a + 1]; ++e)
@@ -98,8 +98,8 @@ __global__ void schur_spsp_kernel(int nsp, const int *id, const int *ptr, const 
 
 __global__ void schur_r1s_kernel(int k, const int *id, const int *ptr, const int *pp, const double *aa,
                                  const double *sg, const double *W, long ldw, double *M, long ldm) {
-    const int b = blockIdx.x * blockDim.x + threadIdx.x;
-    const int a = blockIdx.y * blockDim.y + threadIdx.y;
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    const int b = blockIdx.y * blockDim.y + threadIdx.y;
     if (a >= k || b > a) return;
     double g = 0.0;
     for (int t = ptr[a]; t < ptr[a + 1]; ++t) {
@@ -112,8 +112,8 @@ __global__ void schur_r1s_kernel(int k, const int *id, const int *ptr, const int
 
 __global__ void schur_hadamard_kernel(int k, const int *id, const double *sg, const double *G, long ldg,
                                       double *M, long ldm) {
-    const int b = blockIdx.x * blockDim.x + threadIdx.x;
-    const int a = blockIdx.y * blockDim.y + threadIdx.y;
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    const int b = blockIdx.y * blockDim.y + threadIdx.y;
     if (a >= k || b > a) return;
     const double g = G[(size_t) a + (size_t) b * ldg];
     M[(size_t) id[a] + (size_t) id[b] * ldm] = sg[a] * sg[b] * g * g;
@@ -427,13 +427,13 @@ void SdpDevice::assemble(double dC, double dA, const double *d_wvec, double dEye
 void SdpDevice::schur_matrix(const double *W, long ldW, double *M, long ldM) {
     cudaStream_t s = stream;
     HB_CUDA(cudaMemsetAsync(M, 0, sizeof(double) * ldM * m, s));
-    dim3 blk(16, 16);
+    dim3 blk(32, 8);
     if (nsp > 0) {
-        dim3 grd((nsp + 15) / 16, (nsp + 15) / 16);
+        dim3 grd((nsp + 31) / 32, (nsp + 7) / 8);
         schur_spsp_kernel<<<grd, blk, 0, s>>>(nsp, sp_id, sp_ptr, sp_r, sp_c, sp_v, W, ldW, M, ldM);
     }
     if (nr1s > 0) {
-        dim3 grd((nr1s + 15) / 16, (nr1s + 15) / 16);
+        dim3 grd((nr1s + 31) / 32, (nr1s + 7) / 8);
         schur_r1s_kernel<<<grd, blk, 0, s>>>(nr1s, r1s_id, r1s_ptr, r1s_p, r1s_a, r1s_sign, W, ldW, M, ldM);
     }
     if (nr1d > 0) {
@@ -441,15 +441,15 @@ void SdpDevice::schur_matrix(const double *W, long ldW, double *M, long ldM) {
         gemm(s, n, nr1d, n, 1.0, W, ldW, 0, A1, ld, 0, 0.0, V, ld, 0);
         const long ldg = pad_ld(nr1d);
         gemm(s, nr1d, nr1d, n, 1.0, A1, ld, 1, V, ld, 0, 0.0, G, ldg, GEMM_C_LOWER);
-        dim3 grd((nr1d + 15) / 16, (nr1d + 15) / 16);
+        dim3 grd((nr1d + 31) / 32, (nr1d + 7) / 8);
         schur_hadamard_kernel<<<grd, blk, 0, s>>>(nr1d, r1d_id, r1d_sign, G, ldg, M, ldM);
         if (nr1s > 0) {
-            dim3 g2((nr1s + 15) / 16, (nr1d + 15) / 16);
+            dim3 g2((nr1s + 31) / 32, (nr1d + 7) / 8);
             schur_r1d_r1s_kernel<<<g2, blk, 0, s>>>(nr1d, r1d_id, r1d_sign, V, ld, nr1s, r1s_id, r1s_ptr, r1s_p,
                                                     r1s_a, r1s_sign, M, ldM);
         }
         if (nsp > 0) {
-            dim3 g3((nsp + 15) / 16, (nr1d + 15) / 16);
+            dim3 g3((nsp + 31) / 32, (nr1d + 7) / 8);
             schur_r1_sp_kernel<<<g3, blk, 0, s>>>(nr1d, r1d_id, r1d_sign, V, ld, nsp, sp_id, sp_ptr, sp_r, sp_c,
                                                   sp_v, M, ldM);
         }
@@ -459,7 +459,7 @@ void SdpDevice::schur_matrix(const double *W, long ldW, double *M, long ldM) {
         HB_CUDA(cudaMallocAsync(&Vs, sizeof(double) * ld * nr1s, s));
         dim3 gv(grid1(n) > 64 ? 64 : grid1(n), nr1s);
         r1s_build_v_kernel<<<gv, 256, 0, s>>>(n, nr1s, r1s_ptr, r1s_p, r1s_a, W, ldW, Vs, ld);
-        dim3 g3((nsp + 15) / 16, (nr1s + 15) / 16);
+        dim3 g3((nsp + 31) / 32, (nr1s + 7) / 8);
         schur_r1_sp_kernel<<<g3, blk, 0, s>>>(nr1s, r1s_id, r1s_sign, Vs, ld, nsp, sp_id, sp_ptr, sp_r, sp_c, sp_v,
                                               M, ldM);
         HB_CUDA(cudaFreeAsync(Vs, s));

@@ -79,6 +79,12 @@ extern int hdsdpb_inverse( int n, const double *S, double *Sinv );
 extern int hdsdpb_gemm( int M, int N, int K, double alpha, const double *A, int lda, int transA,
                         const double *B, int ldb, int transB, double beta, double *C, int ldc );
 
+/* Device-resident timing of one kernel family on an n x n problem (CUDA events
+   on the launching stream, 2 warm-up calls): 0 GEMM NN, 1 GEMM TN lower,
+   2 Cholesky, 3 triangular inverse L^-1, 4 matrix-vector product,
+   5 Lanczos step bound, 6 rank-64 SYRK update. Writes milliseconds per call. */
+extern int hdsdpb_kernel_timing( int which, int n, int reps, double *ms );
+
 #ifdef __cplusplus
 }
 #endif
