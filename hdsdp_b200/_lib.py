@@ -22,7 +22,7 @@ EXPORTS = [
     "HDSDPGetStatus", "HDSDPGetIterCount", "HDSDPSetPrimalRefinement", "HDSDPSetPrecision",
     "HDSDPGetIterLog", "HDSDPGetTimers",
     "hdsdpb_schur_probe", "hdsdpb_ratio_probe", "hdsdpb_cholesky", "hdsdpb_inverse", "hdsdpb_gemm",
-    "hdsdpb_kernel_timing",
+    "hdsdpb_kernel_timing", "hdsdpb_gridsync_probe",
 ]
 
 _lib = None
@@ -68,6 +68,7 @@ def load():
         "hdsdpb_inverse": ([i, dp, dp], i),
         "hdsdpb_gemm": ([i, i, i, d, dp, i, i, dp, i, i, d, dp, i], i),
         "hdsdpb_kernel_timing": ([i, i, i, dp], i),
+        "hdsdpb_gridsync_probe": ([i, i, dp], i),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

@@ -110,10 +110,11 @@ class Solver:
         return arr
 
     def timers(self):
-        t = np.zeros(14)
+        t = np.zeros(20)
         self.L.HDSDPGetTimers(self.h, _dp(t))
         keys = ["schur", "schur_factor", "schur_solve", "s_factor", "s_inverse", "lanczos", "assemble",
-                "primal", "total", "n_schur", "n_sfactor", "n_lanczos", "n_lanczos_mv", "n_schur_solve"]
+                "primal", "total", "n_schur", "n_sfactor", "n_lanczos", "n_lanczos_mv", "n_schur_solve",
+                "lz_inverse", "lz_host", "lz_wait", "sch_matrix", "sch_inner", "sch_innersq"]
         return dict(zip(keys, t.tolist()))
 
     def close(self):

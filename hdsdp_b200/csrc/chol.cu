@@ -1,0 +1,476 @@
+// Persistent cooperative Cholesky factorisation and triangular inverse.
+//
+// One cooperative launch covers the whole factorisation: for every 64-column
+// panel, block 0 factors the diagonal block (and inverts it), the grid
+// synchronises, all blocks solve the panel rows, synchronise, then update the
+// trailing lower triangle tile by tile on the DMMA path, and synchronise
+// again. A failed pivot (non-positive or NaN, the dpotrf test used by the
+// reference's positive-definiteness checks, linalg/hdsdp_linsolver.c:521-553)
+// is published in *info and every block leaves at the next grid barrier.
+//
+// The triangular inverse K = L^-1 uses the same structure on block rows:
+// X_i <- Dinv_i X_i, then X_below -= L_below,i X_i.
+#include "la.h"
+#include <cooperative_groups.h>
+#include <algorithm>
+#include <vector>
+
+namespace cg = cooperative_groups;
+
+namespace hb {
+
+// Optional per-phase timestamps of the factorisation (null in normal runs).
+__device__ unsigned long long *g_chol_stamps = nullptr;
+
+namespace {
+constexpr int NB = 64;
+
+__device__ __forceinline__ void stamp(int slot) {
+    if (g_chol_stamps && threadIdx.x == 0 && slot < 4096) {
+        unsigned long long t;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+        g_chol_stamps[slot] = t;
+    }
+}
+constexpr int TP = 68;                         // tile pitch (conflict-free DMMA fragment reads)
+constexpr int SM_DOUBLES = 3 * 64 * TP;        // three 64 x 68 tiles
+constexpr int COOP_THREADS = 256;
+
+__device__ __forceinline__ void cpa8(double *sdst, const double *gsrc, bool pred) {
+    const unsigned saddr = (unsigned) __cvta_generic_to_shared(sdst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(saddr), "l"(gsrc), "r"(pred ? 8 : 0));
+}
+__device__ __forceinline__ void cpa_wait_all() {
+    asm volatile("cp.async.commit_group;\n" ::);
+    asm volatile("cp.async.wait_group 0;\n" ::);
+}
+
+__device__ __forceinline__ void dmma_c(double &d0, double &d1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
+
+// Inverse of the 64 x 64 lower-triangular T (pitch TP, entries beyond nb padded with the
+// identity) into Ti, in shared memory: four warps invert the 16 x 16 diagonal blocks in
+// registers, then off-diagonal blocks follow in three block-parallel stages
+// Ti_ij = -Ti_ii * sum_{k=j}^{i-1} T_ik Ti_kj.
+__device__ void trinv64_dev(double *T, double *Ti, double *Pt, int nb) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int r = nb + tid; r < 64; r += blockDim.x) T[r + r * TP] = 1.0;
+    __syncthreads();
+    if (warp < 4 && lane < 16) {
+        const int b0 = warp * 16, c = lane;
+        double x[16];
+#pragma unroll
+        for (int r = 0; r < 16; ++r) {
+            if (r < c) x[r] = 0.0;
+            else if (r == c) x[r] = 1.0 / T[(b0 + r) + (b0 + r) * TP];
+            else {
+                double acc = 0.0;
+#pragma unroll
+                for (int k = 0; k < 16; ++k)
+                    if (k >= c && k < r) acc += T[(b0 + r) + (b0 + k) * TP] * x[k];
+                x[r] = -acc / T[(b0 + r) + (b0 + r) * TP];
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < 16; ++r) Ti[(b0 + r) + (b0 + c) * TP] = x[r];
+    }
+    for (int idx = tid; idx < 64 * 64; idx += blockDim.x) {
+        const int r = idx & 63, c = idx >> 6;
+        if ((r >> 4) < (c >> 4)) Ti[r + c * TP] = 0.0;
+    }
+    __syncthreads();
+    for (int d = 1; d < 4; ++d) {
+        const int nblk = 4 - d;
+        for (int e = tid; e < nblk * 256; e += blockDim.x) {
+            const int j = e >> 8, i = j + d, rr = (e & 255) >> 4, cc = e & 15;
+            double acc = 0.0;
+            for (int k = j; k < i; ++k)
+#pragma unroll
+                for (int t = 0; t < 16; ++t) acc += T[(16 * i + rr) + (16 * k + t) * TP] * Ti[(16 * k + t) + (16 * j + cc) * TP];
+            Pt[(j << 8) + (rr << 4) + cc] = acc;
+        }
+        __syncthreads();
+        for (int e = tid; e < nblk * 256; e += blockDim.x) {
+            const int j = e >> 8, i = j + d, rr = (e & 255) >> 4, cc = e & 15;
+            double acc = 0.0;
+#pragma unroll
+            for (int t = 0; t < 16; ++t) acc += Ti[(16 * i + rr) + (16 * i + t) * TP] * Pt[(j << 8) + (t << 4) + cc];
+            Ti[(16 * i + rr) + (16 * j + cc) * TP] = -acc;
+        }
+        __syncthreads();
+    }
+}
+
+// Factor the nb x nb diagonal block at (j0, j0) in place. Executed by one block:
+// four 16-column sub-panels; warp 0 factors each 16 x 16 pivot block in registers
+// (shuffles), the block solves the rows below it and updates the trailing part.
+// Returns false (and sets *info) on a failed pivot.
+__device__ bool potf2_dev(double *L, long ld, int j0, int nb, double *Dinv, long ldd, int *info, double *sm) {
+    double *T = sm;  // T[r + c*TP]
+    __shared__ int fail;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int idx = tid; idx < 64 * nb; idx += blockDim.x) {
+        const int r = idx & 63, c = idx >> 6;
+        const bool ok = r < nb && r >= c;
+        cpa8(&T[r + c * TP], ok ? L + (size_t) (j0 + r) + (size_t) (j0 + c) * ld : L, ok);
+    }
+    cpa_wait_all();
+    if (tid == 0) fail = 0;
+    __syncthreads();
+    for (int s0 = 0; s0 < nb; s0 += 16) {
+        const int sb = min(16, nb - s0);
+        if (warp == 0) {
+            // lane r < sb holds row s0 + r of the pivot block
+            double d[16];
+#pragma unroll
+            for (int q = 0; q < 16; ++q) d[q] = (lane < sb && q <= lane) ? T[(s0 + lane) + (s0 + q) * TP] : 0.0;
+            bool bad = false;
+#pragma unroll
+            for (int c = 0; c < 16; ++c) {
+                if (c < sb) {
+                    const double dc = __shfl_sync(0xffffffffu, d[c], c);
+                    if (!(dc > 0.0)) bad = true;
+                    const double pv = sqrt(dc), ip = 1.0 / pv;
+                    if (lane == c) d[c] = pv;
+                    else if (lane > c) d[c] *= ip;
+#pragma unroll
+                    for (int q = c + 1; q < 16; ++q) {
+                        const double lqc = __shfl_sync(0xffffffffu, d[c], q);
+                        if (lane >= q) d[q] -= d[c] * lqc;
+                    }
+                }
+            }
+            if (lane == 0 && bad) {
+                // locate the first failing pivot column (sequential re-check on the host side is not
+                // needed: report the sub-panel start like a failed dpotrf)
+                fail = s0 + 1;
+            }
+#pragma unroll
+            for (int q = 0; q < 16; ++q)
+                if (lane < sb && q <= lane) T[(s0 + lane) + (s0 + q) * TP] = d[q];
+        }
+        __syncthreads();
+        if (fail) break;
+        // rows below the pivot block inside this 64-block: x . D^T = t  (forward substitution)
+        const int r = s0 + sb + tid;
+        if (tid < 64 && r < nb) {
+#pragma unroll 4
+            for (int c = 0; c < sb; ++c) {
+                double x = T[r + (s0 + c) * TP];
+                for (int k = 0; k < c; ++k) x -= T[r + (s0 + k) * TP] * T[(s0 + c) + (s0 + k) * TP];
+                T[r + (s0 + c) * TP] = x * (1.0 / T[(s0 + c) + (s0 + c) * TP]);
+            }
+        }
+        __syncthreads();
+        // trailing update of the rest of the 64-block with this 16-column sub-panel
+        {
+            const int base = s0 + sb, rem = nb - base;
+            const int rr = base + (tid & 63);
+            if ((tid & 63) < rem) {
+                for (int q = base + (tid >> 6); q <= rr; q += 4) {
+                    double acc = 0.0;
+#pragma unroll 4
+                    for (int k = 0; k < sb; ++k) acc += T[rr + (s0 + k) * TP] * T[q + (s0 + k) * TP];
+                    T[rr + q * TP] -= acc;
+                }
+            }
+        }
+        __syncthreads();
+    }
+    __syncthreads();
+    if (fail) {
+        if (tid == 0) *info = j0 + fail;
+        return false;
+    }
+    for (int idx = tid; idx < nb * nb; idx += blockDim.x) {
+        const int r = idx % nb, cc = idx / nb;
+        if (r >= cc) L[(size_t) (j0 + r) + (size_t) (j0 + cc) * ld] = T[r + cc * TP];
+    }
+    __syncthreads();
+    trinv64_dev(T, sm + 64 * TP, sm + 128 * TP, nb);
+    const double *Ti = sm + 64 * TP;
+    for (int idx = tid; idx < NB * NB; idx += blockDim.x) {
+        const int r = idx & 63, cc = idx >> 6;
+        if (r < nb) Dinv[(size_t) (j0 + r) + (size_t) cc * ldd] = (cc < nb) ? Ti[r + cc * TP] : 0.0;
+    }
+    __syncthreads();
+    return true;
+}
+
+// Tile product on the DMMA path over K = nb <= 64:
+//   mode 0:  C -= A * op(B)      mode 1:  C = A * op(B)
+// A(r, k) = Ab[r + k*lda]; op(B)(k, c) = bt ? Bb[c + k*ldb] : Bb[k + c*ldb].
+// C is the 64 x 64 tile at Cb (pitch ldc) clipped to mr x nc; with diag set only
+// row >= col entries are written. Operands are staged in shared memory first, so C
+// may alias A or B (in-place panel solves).
+__device__ void tile_mma_dev(double *Cb, long ldc, int mr, int nc, const double *Ab, long lda, int ar,
+                             const double *Bb, long ldb, int bt, int bc, int nb, bool diag, int mode, double *sm) {
+    double *As = sm, *Bs = sm + 64 * TP;   // As[r + k*TP], Bs[c + k*TP]
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const int kp = (nb + 3) & ~3;
+    for (int idx = tid; idx < 64 * kp; idx += blockDim.x) {
+        const int r = idx & 63, k = idx >> 6;
+        const bool oka = r < ar && k < nb;
+        cpa8(&As[r + k * TP], oka ? Ab + (size_t) r + (size_t) k * lda : Ab, oka);
+        const bool okb = r < bc && k < nb;
+        cpa8(&Bs[r + k * TP], okb ? (bt ? Bb + (size_t) r + (size_t) k * ldb : Bb + (size_t) k + (size_t) r * ldb) : Bb,
+             okb);
+    }
+    const int wm = (w & 1) * 32, wn = (w >> 1) * 16;
+    // prefetch the C tile while the operand copies are in flight (mode 0)
+    double cv[4][2][2];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 2; ++j)
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+                const int r = wm + i * 8 + (lane >> 2), c = wn + j * 8 + (lane & 3) * 2 + e;
+                cv[i][j][e] = (mode == 0 && r < mr && c < nc && !(diag && r < c)) ? Cb[(size_t) r + (size_t) c * ldc] : 0.0;
+            }
+    cpa_wait_all();
+    __syncthreads();
+    double acc[4][2][2];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 2; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+    for (int k = 0; k < kp; k += 4) {
+        const int kk = k + (lane & 3);
+        double a[4], b[2];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) a[i] = As[(wm + i * 8 + (lane >> 2)) + kk * TP];
+#pragma unroll
+        for (int j = 0; j < 2; ++j) b[j] = Bs[(wn + j * 8 + (lane >> 2)) + kk * TP];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 2; ++j) dmma_c(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int r = wm + i * 8 + (lane >> 2);
+        if (r >= mr) continue;
+#pragma unroll
+        for (int j = 0; j < 2; ++j)
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+                const int c = wn + j * 8 + (lane & 3) * 2 + e;
+                if (c >= nc || (diag && r < c)) continue;
+                Cb[(size_t) r + (size_t) c * ldc] = (mode == 0) ? cv[i][j][e] - acc[i][j][e] : acc[i][j][e];
+            }
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ void tri_index(long t, int &ti, int &tj) {
+    ti = (int) ((sqrt(8.0 * (double) t + 1.0) - 1.0) * 0.5);
+    while ((long) ti * (ti + 1) / 2 > t) --ti;
+    while ((long) (ti + 1) * (ti + 2) / 2 <= t) ++ti;
+    tj = (int) (t - (long) ti * (ti + 1) / 2);
+}
+
+// Right-looking blocked Cholesky with one-panel look-ahead: in the update phase of
+// panel j, block 0 first updates the diagonal tile of panel j+1 and factors it while
+// the other blocks update the rest of the trailing matrix.
+__global__ void __launch_bounds__(COOP_THREADS) potrf_coop_kernel(double *L, long ld, int n, double *Dinv,
+                                                                  long ldd, int *info) {
+    cg::grid_group grid = cg::this_grid();
+    extern __shared__ double sm[];
+    if (blockIdx.x == 0) potf2_dev(L, ld, 0, min(NB, n), Dinv, ldd, info, sm);
+    grid.sync();
+    for (int j0 = 0; j0 < n; j0 += NB) {
+        if (*(volatile int *) info) return;
+        const int nb = min(NB, n - j0);
+        const int rows = n - j0 - nb;
+        if (rows <= 0) break;
+        double *P = L + (size_t) (j0 + nb) + (size_t) j0 * ld;
+        const int nchunk = (rows + 63) / 64;
+        const int pj = (j0 / NB) * 8;
+        if (blockIdx.x <= 1) stamp(pj + 4 * blockIdx.x + 0);
+        for (int ch = blockIdx.x; ch < nchunk; ch += gridDim.x) {
+            const int mr = min(64, rows - ch * 64);
+            tile_mma_dev(P + ch * 64, ld, mr, nb, P + ch * 64, ld, mr, Dinv + j0, ldd, 1, nb, nb, false, 1, sm);
+        }
+        if (blockIdx.x <= 1) stamp(pj + 4 * blockIdx.x + 1);
+        grid.sync();
+        const long ntile = (long) nchunk * (nchunk + 1) / 2;
+        double *A22 = L + (size_t) (j0 + nb) + (size_t) (j0 + nb) * ld;
+        if (blockIdx.x == 0) {
+            // tile (0, 0) is the next diagonal block: update it, then factor it
+            const int mr = min(64, rows);
+            stamp(pj + 2);
+            tile_mma_dev(A22, ld, mr, mr, P, ld, mr, P, ld, 1, mr, nb, true, 0, sm);
+            potf2_dev(L, ld, j0 + nb, min(NB, rows), Dinv, ldd, info, sm);
+            stamp(pj + 3);
+        }
+        // remaining tiles, spread over the other blocks (block 0 joins when the grid has one block)
+        const int nworker = (gridDim.x > 1) ? (int) gridDim.x - 1 : 1;
+        const int wid = (gridDim.x > 1) ? (int) blockIdx.x - 1 : 0;
+        if (wid >= 0) {
+            for (long t = 1 + wid; t < ntile; t += nworker) {
+                int ti, tj;
+                tri_index(t, ti, tj);
+                const int mr = min(64, rows - ti * 64), nc = min(64, rows - tj * 64);
+                tile_mma_dev(A22 + (size_t) ti * 64 + (size_t) tj * 64 * ld, ld, mr, nc, P + ti * 64, ld, mr,
+                             P + tj * 64, ld, 1, nc, nb, ti == tj, 0, sm);
+            }
+        }
+        if (blockIdx.x == 1) stamp(pj + 6);
+        grid.sync();
+    }
+}
+
+__global__ void __launch_bounds__(COOP_THREADS) trtri_coop_kernel(const double *L, double *K, long ld, int n,
+                                                                  const double *Dinv, long ldd) {
+    cg::grid_group grid = cg::this_grid();
+    extern __shared__ double sm[];
+    for (int i0 = 0; i0 < n; i0 += NB) {
+        const int nb = min(NB, n - i0);
+        const int cend = i0 + nb;
+        const int nchunk = (cend + 63) / 64;
+        for (int ch = blockIdx.x; ch < nchunk; ch += gridDim.x) {
+            // X_i chunk <- Dinv_i * X_i chunk  (in place)
+            const int nc = min(64, cend - ch * 64);
+            double *Xc = K + i0 + (size_t) ch * 64 * ld;
+            tile_mma_dev(Xc, ld, nb, nc, Dinv + i0, ldd, nb, Xc, ld, 0, nc, nb, false, 1, sm);
+        }
+        grid.sync();
+        const int rows = n - cend;
+        if (rows <= 0) break;
+        const int rt = (rows + 63) / 64;
+        const long ntile = (long) rt * nchunk;
+        for (long t = blockIdx.x; t < ntile; t += gridDim.x) {
+            const int ti = (int) (t % rt), tj = (int) (t / rt);
+            const int mr = min(64, rows - ti * 64), nc = min(64, cend - tj * 64);
+            // C = K[cend + 64 ti.., 64 tj..] -= L[cend + 64 ti.., i0..i0+nb) * K[i0..i0+nb, 64 tj..]
+            tile_mma_dev(K + (size_t) (cend + ti * 64) + (size_t) tj * 64 * ld, ld, mr, nc,
+                         L + (size_t) (cend + ti * 64) + (size_t) i0 * ld, ld, mr, K + i0 + (size_t) tj * 64 * ld, ld,
+                         0, nc, nb, false, 0, sm);
+        }
+        grid.sync();
+    }
+}
+
+__global__ void copy_lower_k(int n, const double *S, long lds, double *L, long ldl) {
+    const long total = (long) n * n;
+    for (long idx = blockIdx.x * (long) blockDim.x + threadIdx.x; idx < total; idx += (long) gridDim.x * blockDim.x) {
+        const int r = (int) (idx % n), c = (int) (idx / n);
+        L[(size_t) r + (size_t) c * ldl] = (r >= c) ? S[(size_t) r + (size_t) c * lds] : 0.0;
+    }
+}
+
+__global__ void identity_k(int n, double *A, long lda) {
+    const long total = (long) n * n;
+    for (long idx = blockIdx.x * (long) blockDim.x + threadIdx.x; idx < total; idx += (long) gridDim.x * blockDim.x) {
+        const int r = (int) (idx % n), c = (int) (idx / n);
+        A[(size_t) r + (size_t) c * lda] = (r == c) ? 1.0 : 0.0;
+    }
+}
+
+__global__ void zero_info_k(int *p) { *p = 0; }
+
+int coop_grid(const void *fn) {
+    static int cached[2] = {0, 0};
+    const int slot = (fn == (const void *) potrf_coop_kernel) ? 0 : 1;
+    if (cached[slot]) return cached[slot];
+    const int smem = SM_DOUBLES * (int) sizeof(double);
+    HB_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    int dev = 0, sms = 0, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, COOP_THREADS, smem);
+    cached[slot] = std::max(1, sms * std::max(per, 1));
+    return cached[slot];
+}
+
+int grid_for_n(long total) {
+    long b = (total + 255) / 256;
+    return (int) std::min<long>(std::max<long>(b, 1), 148L * 16);
+}
+}  // namespace
+
+bool coop_factorize_enqueue(cudaStream_t s, DenseFactor &F, const double *S, long ldS) {
+    const int n = F.n;
+    zero_info_k<<<1, 1, 0, s>>>(F.d_info);
+    copy_lower_k<<<grid_for_n((long) n * n), 256, 0, s>>>(n, S, ldS, F.L, F.ld);
+    const void *fn = (const void *) potrf_coop_kernel;
+    const long t0 = (long) ((n - 1) / 64 + 1);
+    const int grid = (int) std::max(1L, std::min<long>(coop_grid(fn), t0 * (t0 + 1) / 2));
+    double *Lp = F.L;
+    long ld = F.ld;
+    int nn = n;
+    double *Dp = F.Dinv;
+    long ldd = F.ld;
+    int *ip = F.d_info;
+    void *args[] = {&Lp, &ld, &nn, &Dp, &ldd, &ip};
+    cudaError_t e = cudaLaunchCooperativeKernel(fn, grid, COOP_THREADS, args, SM_DOUBLES * sizeof(double), s);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return true;
+}
+
+bool coop_inverse_enqueue(cudaStream_t s, DenseFactor &F) {
+    const int n = F.n;
+    identity_k<<<grid_for_n((long) n * n), 256, 0, s>>>(n, F.K, F.ld);
+    const void *fn = (const void *) trtri_coop_kernel;
+    const long t0 = (long) ((n - 1) / 64 + 1);
+    const int grid = (int) std::max(1L, std::min<long>(coop_grid(fn), t0 * t0 / 4 + 1));
+    const double *Lp = F.L;
+    double *Kp = F.K;
+    long ld = F.ld;
+    int nn = n;
+    const double *Dp = F.Dinv;
+    long ldd = F.ld;
+    void *args[] = {&Lp, &Kp, &ld, &nn, &Dp, &ldd};
+    cudaError_t e = cudaLaunchCooperativeKernel(fn, grid, COOP_THREADS, args, SM_DOUBLES * sizeof(double), s);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return true;
+}
+
+}  // namespace hb
+
+namespace hb {
+// Debug probe: factor a well-conditioned n x n matrix and return per-panel phase
+// timestamps (ns, relative to the first) in out[0 .. 8 * panels).
+int chol_phase_probe(int n, double *out) {
+    cudaStream_t s;
+    cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    const long ld = pad_ld(n);
+    double *A = nullptr;
+    unsigned long long *st = nullptr;
+    cudaMalloc(&A, sizeof(double) * ld * n);
+    cudaMalloc(&st, sizeof(unsigned long long) * 4096);
+    cudaMemset(st, 0, sizeof(unsigned long long) * 4096);
+    std::vector<double> h((size_t) ld * n, 0.0);
+    for (int j = 0; j < n; ++j)
+        for (int i = 0; i < n; ++i) h[(size_t) j * ld + i] = (i == j) ? 2.0 : 1.0 / (1.0 + i + j);
+    cudaMemcpy(A, h.data(), sizeof(double) * ld * n, cudaMemcpyHostToDevice);
+    DenseFactor F;
+    F.alloc(n);
+    factorize(s, F, A, ld);  // warm
+    cudaMemcpyToSymbol(g_chol_stamps, &st, sizeof(st));
+    factorize(s, F, A, ld);
+    unsigned long long *nul = nullptr;
+    cudaMemcpyToSymbol(g_chol_stamps, &nul, sizeof(nul));
+    std::vector<unsigned long long> hs(4096);
+    cudaMemcpy(hs.data(), st, sizeof(unsigned long long) * 4096, cudaMemcpyDeviceToHost);
+    const int panels = (n + 63) / 64;
+    const unsigned long long t0 = hs[0];
+    for (int i = 0; i < 8 * panels && i < 4096; ++i) out[i] = hs[i] ? (double) (hs[i] - t0) : -1.0;
+    F.release();
+    cudaFree(A);
+    cudaFree(st);
+    cudaStreamDestroy(s);
+    return 0;
+}
+}  // namespace hb

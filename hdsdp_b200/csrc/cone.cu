@@ -624,13 +624,24 @@ hdsdp_retcode KKT::build(SdpCone &cone, int type) {
         HB_CUDA(cudaStreamSynchronize(s));
         dTraceSinv += cone.h_scal[0];
     }
+    double tq = wall();
     dev.schur_matrix(Wp, ld, M, ldm);
+    if (tm) {
+        HB_CUDA(cudaStreamSynchronize(s));
+        tm->sch_matrix += wall() - tq;
+        tq = wall();
+    }
     dev.inner_all(Wp, ld, cone.d_vec);
     add_host(asinv, cone.d_vec, h_buf, m, 1.0, s);
+    if (tm) {
+        tm->sch_inner += wall() - tq;
+        tq = wall();
+    }
     if (r != 0.0) {
         dev.inner_all_sq(Wp, ld, cone.d_vec);
         add_host(asinvrd, cone.d_vec, h_buf, m, r, s);
     }
+    if (tm) tm->sch_innersq += wall() - tq;
     if (type == KKT_TYPE_HOMOGENEOUS) {
         // B = W C W; <A_i, B>, <C, W>, <C, B>, r * tr(B)
         gemm(s, n, n, n, 1.0, dev.Cfull, dev.ld, 0, Wp, ld, 0, 0.0, dev.T1, dev.ld, 0);
@@ -830,46 +841,57 @@ __global__ void lanczos_resid_kernel(int n, double *z, const double *x, double l
     if (threadIdx.x == 0) *out = v;
 }
 
-// Eigen-decomposition of a small symmetric matrix by cyclic Jacobi rotations.
-void jacobi_eig(int n, std::vector<double> &A, std::vector<double> &evals, std::vector<double> &evecs) {
-    evecs.assign((size_t) n * n, 0.0);
-    for (int i = 0; i < n; ++i) evecs[(size_t) i * n + i] = 1.0;
-    auto a = [&](int i, int j) -> double & { return A[(size_t) i + (size_t) j * n]; };
-    auto v = [&](int i, int j) -> double & { return evecs[(size_t) i + (size_t) j * n]; };
-    for (int sweep = 0; sweep < 100; ++sweep) {
-        double off = 0.0, tot = 0.0;
-        for (int i = 0; i < n; ++i)
-            for (int j = 0; j < n; ++j) {
-                tot += a(i, j) * a(i, j);
-                if (i != j) off += a(i, j) * a(i, j);
+// All eigenpairs of the symmetric tridiagonal matrix with diagonal d[0..n) and
+// off-diagonal e[0..n-1): QL iteration with implicit Wilkinson shifts, rotations
+// accumulated into Z (column-major n x n, columns are eigenvectors).
+void tridiag_eig(int n, std::vector<double> d, std::vector<double> e, std::vector<double> &evals,
+                 std::vector<double> &Z) {
+    Z.assign((size_t) n * n, 0.0);
+    for (int i = 0; i < n; ++i) Z[(size_t) i * n + i] = 1.0;
+    e.resize(n, 0.0);
+    e[n - 1] = 0.0;
+    for (int l = 0; l < n; ++l) {
+        for (int iter = 0; iter < 60; ++iter) {
+            int mm = l;
+            for (; mm < n - 1; ++mm) {
+                const double dd = std::fabs(d[mm]) + std::fabs(d[mm + 1]);
+                if (std::fabs(e[mm]) <= 1e-15 * dd) break;
             }
-        if (off <= 1e-32 * tot || off == 0.0) break;
-        for (int p = 0; p < n - 1; ++p)
-            for (int q = p + 1; q < n; ++q) {
-                const double apq = a(p, q);
-                if (apq == 0.0) continue;
-                const double theta = (a(q, q) - a(p, p)) / (2.0 * apq);
-                const double t = (theta >= 0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
-                const double c = 1.0 / std::sqrt(t * t + 1.0), sn = t * c;
-                for (int k = 0; k < n; ++k) {
-                    const double akp = a(k, p), akq = a(k, q);
-                    a(k, p) = c * akp - sn * akq;
-                    a(k, q) = sn * akp + c * akq;
+            if (mm == l) break;
+            double g = (d[l + 1] - d[l]) / (2.0 * e[l]);
+            double r = std::hypot(g, 1.0);
+            g = d[mm] - d[l] + e[l] / (g + (g >= 0 ? r : -r));
+            double sn = 1.0, c = 1.0, p = 0.0;
+            int i = mm - 1;
+            for (; i >= l; --i) {
+                double f = sn * e[i], b = c * e[i];
+                r = std::hypot(f, g);
+                e[i + 1] = r;
+                if (r == 0.0) {
+                    d[i + 1] -= p;
+                    e[mm] = 0.0;
+                    break;
                 }
+                sn = f / r;
+                c = g / r;
+                g = d[i + 1] - p;
+                r = (d[i] - g) * sn + 2.0 * c * b;
+                p = sn * r;
+                d[i + 1] = g + p;
+                g = c * r - b;
                 for (int k = 0; k < n; ++k) {
-                    const double apk = a(p, k), aqk = a(q, k);
-                    a(p, k) = c * apk - sn * aqk;
-                    a(q, k) = sn * apk + c * aqk;
-                }
-                for (int k = 0; k < n; ++k) {
-                    const double vkp = v(k, p), vkq = v(k, q);
-                    v(k, p) = c * vkp - sn * vkq;
-                    v(k, q) = sn * vkp + c * vkq;
+                    f = Z[(size_t) (i + 1) * n + k];
+                    Z[(size_t) (i + 1) * n + k] = sn * Z[(size_t) i * n + k] + c * f;
+                    Z[(size_t) i * n + k] = c * Z[(size_t) i * n + k] - sn * f;
                 }
             }
+            if (r == 0.0 && i >= l) continue;
+            d[l] -= p;
+            e[l] = g;
+            e[mm] = 0.0;
+        }
     }
-    evals.resize(n);
-    for (int i = 0; i < n; ++i) evals[i] = a(i, i);
+    evals = d;
 }
 }  // namespace
 
@@ -878,7 +900,7 @@ void Lanczos::init(int n_, cudaStream_t s_) {
     s = s_;
     ld = pad_ld(n);
     HB_CUDA(cudaMalloc(&V, sizeof(double) * ld * (maxdim + 1)));
-    for (double **p : {&w, &z1, &z2, &t1, &warm, &init_vec, &pert_vec}) HB_CUDA(cudaMalloc(p, sizeof(double) * ld));
+    for (double **p : {&w, &z1, &z2, &t1, &u, &warm, &init_vec, &pert_vec}) HB_CUDA(cudaMalloc(p, sizeof(double) * ld));
     HB_CUDA(cudaMalloc(&d_ab, sizeof(double) * (2 * maxdim + 2)));
     HB_CUDA(cudaMallocHost(&h_ab, sizeof(double) * (2 * maxdim + 2)));
     HB_CUDA(cudaMalloc(&d_y, sizeof(double) * 2 * (maxdim + 1)));
@@ -908,7 +930,7 @@ void Lanczos::init(int n_, cudaStream_t s_) {
 }
 
 void Lanczos::release() {
-    for (double **p : {&V, &w, &z1, &z2, &t1, &warm, &init_vec, &pert_vec, &d_ab, &d_y, &d_scal}) {
+    for (double **p : {&V, &w, &z1, &z2, &t1, &u, &warm, &init_vec, &pert_vec, &d_ab, &d_y, &d_scal}) {
         if (*p) cudaFree(*p);
         *p = nullptr;
     }
@@ -920,9 +942,11 @@ void Lanczos::release() {
 hdsdp_retcode Lanczos::solve(DenseFactor &F, const double *D, long ldD, double *maxStep, Timers *tm) {
     double t0 = wall();
     compute_inverse_factor(s, F);
+    if (tm) {
+        HB_CUDA(cudaStreamSynchronize(s));
+        tm->lz_inverse += wall() - t0;
+    }
     // buffers: V columns, w (Mv), t1 / z1 / z2 temporaries
-    double *u = nullptr;
-    HB_CUDA(cudaMallocAsync(&u, sizeof(double) * ld, s));
     auto mv = [&](const double *x, double *y) {
         coldot(s, n, n, F.K, F.ld, x, t1, 1.0, 0.0, 1);   // t1 = L^-T x
         coldot(s, n, n, D, ldD, t1, u, -1.0, 0.0, 0);     // u  = -D t1
@@ -945,7 +969,10 @@ hdsdp_retcode Lanczos::solve(DenseFactor &F, const double *D, long ldD, double *
         const bool sched = ((k + 1) % freq == 0) || k >= maxdim - 1;
         if (!sched) continue;
         HB_CUDA(cudaMemcpyAsync(h_ab, d_ab, sizeof(double) * (2 * maxdim + 2), cudaMemcpyDeviceToHost, s));
+        double tw = wall();
         HB_CUDA(cudaStreamSynchronize(s));
+        if (tm) tm->lz_wait += wall() - tw;
+        double th = wall();
         // The reference also checks as soon as a step breaks down (zero norm).
         int kc = k;
         for (int q = lastChecked + 1; q <= k; ++q)
@@ -956,12 +983,10 @@ hdsdp_retcode Lanczos::solve(DenseFactor &F, const double *D, long ldD, double *
             ret = HDSDP_RETCODE_FAILED;
             break;
         }
-        T.assign((size_t) kp1 * kp1, 0.0);
-        for (int i = 0; i < kp1; ++i) {
-            T[(size_t) i + (size_t) i * kp1] = h_ab[i];
-            if (i + 1 < kp1) T[(size_t) (i + 1) + (size_t) i * kp1] = T[(size_t) i + (size_t) (i + 1) * kp1] = h_ab[maxdim + i];
-        }
-        jacobi_eig(kp1, T, ev, evec);
+        std::vector<double> dd(h_ab, h_ab + kp1), ee(h_ab + maxdim, h_ab + maxdim + kp1);
+        ee[kp1 - 1] = 0.0;
+        tridiag_eig(kp1, dd, ee, ev, evec);
+        if (tm) tm->lz_host += wall() - th;
         int i1 = 0, i2 = 0;  // largest, second largest
         for (int i = 1; i < kp1; ++i)
             if (ev[i] > ev[i1]) i1 = i;
@@ -1007,7 +1032,6 @@ hdsdp_retcode Lanczos::solve(DenseFactor &F, const double *D, long ldD, double *
             if (kc != k) done = true;
         }
     }
-    HB_CUDA(cudaFreeAsync(u, s));
     HB_CUDA(cudaStreamSynchronize(s));
     if (ret == HDSDP_RETCODE_OK) nComputed += 1;
     if (tm) {

@@ -4,6 +4,7 @@
 #include <cstring>
 #include <cmath>
 #include <vector>
+#include <cooperative_groups.h>
 
 using namespace hb;
 
@@ -29,11 +30,12 @@ int HDSDPGetIterLog(hdsdp *h, int maxLen, double *t, double *pObj, double *dObj,
     return n;
 }
 
-void HDSDPGetTimers(hdsdp *h, double out[14]) {
+void HDSDPGetTimers(hdsdp *h, double out[20]) {
     const Timers &t = h->timers;
-    const double v[14] = {t.schur, t.schur_factor, t.schur_solve, t.s_factor, t.s_inverse, t.lanczos, t.assemble,
+    const double v[20] = {t.schur, t.schur_factor, t.schur_solve, t.s_factor, t.s_inverse, t.lanczos, t.assemble,
                           t.primal, t.total, (double) t.n_schur, (double) t.n_sfactor, (double) t.n_lanczos,
-                          (double) t.n_lanczos_mv, (double) t.n_schur_solve};
+                          (double) t.n_lanczos_mv, (double) t.n_schur_solve, t.lz_inverse, t.lz_host, t.lz_wait,
+                          t.sch_matrix, t.sch_inner, t.sch_innersq};
     std::memcpy(out, v, sizeof(v));
 }
 
@@ -249,3 +251,35 @@ extern "C" int hdsdpb_kernel_timing(int which, int n, int reps, double *ms) {
     cudaStreamDestroy(s);
     return device_error_flag() ? -1 : 0;
 }
+
+namespace {
+__global__ void gridsync_probe_kernel(int reps, int *sink) {
+    cooperative_groups::grid_group g = cooperative_groups::this_grid();
+    for (int i = 0; i < reps; ++i) g.sync();
+    if (blockIdx.x == 0 && threadIdx.x == 0) *sink = reps;
+}
+}  // namespace
+
+// Milliseconds for `reps` grid-wide barriers of a cooperative launch of `blocks` x 256 threads.
+extern "C" int hdsdpb_gridsync_probe(int blocks, int reps, double *ms) {
+    int *sink = nullptr;
+    cudaMalloc(&sink, sizeof(int));
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    void *args[] = {&reps, &sink};
+    cudaEventRecord(e0, 0);
+    cudaError_t e = cudaLaunchCooperativeKernel((const void *) gridsync_probe_kernel, blocks, 256, args, 0, 0);
+    cudaEventRecord(e1, 0);
+    cudaEventSynchronize(e1);
+    float t = 0.f;
+    cudaEventElapsedTime(&t, e0, e1);
+    *ms = t;
+    cudaFree(sink);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return e == cudaSuccess ? 0 : -1;
+}
+
+namespace hb { int chol_phase_probe(int n, double *out); }
+extern "C" int hdsdpb_chol_phase_probe(int n, double *out) { return hb::chol_phase_probe(n, out); }

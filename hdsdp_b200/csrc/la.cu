@@ -554,11 +554,18 @@ static void ensure_attrs() {
     init = true;
 }
 
+bool coop_factorize_enqueue(cudaStream_t s, DenseFactor &F, const double *S, long ldS);
+bool coop_inverse_enqueue(cudaStream_t s, DenseFactor &F);
+
 void factorize_async(cudaStream_t s, DenseFactor &F, const double *S, long ldS) {
     ensure_attrs();
     const int n = F.n;
     F.k_valid = false;
     F.factored = true;
+    if (coop_factorize_enqueue(s, F, S, ldS)) {
+        HB_CUDA(cudaMemcpyAsync(F.h_info, F.d_info, sizeof(int), cudaMemcpyDeviceToHost, s));
+        return;
+    }
     zero_int_kernel<<<1, 1, 0, s>>>(F.d_info);
     copy_lower_kernel<<<grid_for((long) n * n), 256, 0, s>>>(n, S, ldS, F.L, F.ld);
     for (int j0 = 0; j0 < n; j0 += NB) {
@@ -594,6 +601,11 @@ void compute_inverse_factor(cudaStream_t s, DenseFactor &F) {
     const int n = F.n;
     if (!F.K) HB_CUDA(cudaMalloc(&F.K, sizeof(double) * F.ld * n));
     if (!F.KT) HB_CUDA(cudaMalloc(&F.KT, sizeof(double) * F.ld * n));
+    if (coop_inverse_enqueue(s, F)) {
+        transpose(s, n, F.K, F.ld, F.KT, F.ld);
+        F.k_valid = true;
+        return;
+    }
     set_identity_kernel<<<grid_for((long) n * n), 256, 0, s>>>(n, F.K, F.ld);
     for (int i0 = 0; i0 < n; i0 += NB) {
         const int nb = std::min(NB, n - i0);

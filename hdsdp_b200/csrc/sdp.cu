@@ -346,6 +346,8 @@ void SdpDevice::upload(int n_, int m_, const HostCoeff &C, const std::vector<Hos
     }
     const int vcols = std::max(std::max(nr1d, nr1s), 1);
     HB_CUDA(cudaMalloc(&V, sizeof(double) * ld * vcols));
+    if (nr1d > 0) HB_CUDA(cudaMalloc(&Vt, sizeof(double) * ld * nr1d));
+    if (nr1s > 0 && nsp > 0) HB_CUDA(cudaMalloc(&Vs, sizeof(double) * ld * nr1s));
 
     ndr = (int) dr_id.size();
     for (int i = 0; i < ndr; ++i) {
@@ -398,7 +400,7 @@ void SdpDevice::release() {
     f(Cfull);
     f(sp_id); f(sp_ptr); f(sp_r); f(sp_c); f(sp_v);
     f(r1s_id); f(r1s_ptr); f(r1s_p); f(r1s_a); f(r1s_sign);
-    f(r1d_id); f(r1d_sign); f(A1); f(G); f(V);
+    f(r1d_id); f(r1d_sign); f(A1); f(G); f(V); f(Vt); f(Vs);
     for (double *p : dr_mat) f(p);
     dr_mat.clear();
     f(pos_r); f(pos_c); f(pos_ptr); f(ent_j); f(ent_v);
@@ -455,14 +457,11 @@ void SdpDevice::schur_matrix(const double *W, long ldW, double *M, long ldM) {
         }
     }
     if (nr1s > 0 && nsp > 0) {
-        double *Vs = nullptr;
-        HB_CUDA(cudaMallocAsync(&Vs, sizeof(double) * ld * nr1s, s));
         dim3 gv(grid1(n) > 64 ? 64 : grid1(n), nr1s);
         r1s_build_v_kernel<<<gv, 256, 0, s>>>(n, nr1s, r1s_ptr, r1s_p, r1s_a, W, ldW, Vs, ld);
         dim3 g3((nsp + 31) / 32, (nr1s + 7) / 8);
         schur_r1_sp_kernel<<<g3, blk, 0, s>>>(nr1s, r1s_id, r1s_sign, Vs, ld, nsp, sp_id, sp_ptr, sp_r, sp_c, sp_v,
                                               M, ldM);
-        HB_CUDA(cudaFreeAsync(Vs, s));
     }
     for (int i = 0; i < ndr; ++i) {
         // B_i = W A_i W, then M_ij = <A_j, B_i>
@@ -481,11 +480,8 @@ void SdpDevice::inner_all(const double *Z, long ldZ, double *out) {
     if (nr1s > 0)
         inner_r1s_kernel<<<grid1(nr1s), 256, 0, s>>>(nr1s, r1s_id, r1s_ptr, r1s_p, r1s_a, r1s_sign, Z, ldZ, out);
     if (nr1d > 0) {
-        double *Vt = nullptr;
-        HB_CUDA(cudaMallocAsync(&Vt, sizeof(double) * ld * nr1d, s));
         gemm(s, n, nr1d, n, 1.0, Z, ldZ, 0, A1, ld, 0, 0.0, Vt, ld, 0);
         coldot_pair_kernel<<<(nr1d * 32 + 255) / 256, 256, 0, s>>>(n, nr1d, r1d_id, r1d_sign, A1, ld, Vt, ld, out);
-        HB_CUDA(cudaFreeAsync(Vt, s));
     }
     for (int i = 0; i < ndr; ++i) frob_dot(s, n, dr_mat[i], ld, Z, ldZ, out + dr_id[i]);
     HB_CUDA(cudaGetLastError());
@@ -499,11 +495,8 @@ void SdpDevice::inner_all_sq(const double *W, long ldW, double *out) {
         innersq_r1s_kernel<<<(nr1s * 32 + 255) / 256, 256, 0, s>>>(n, nr1s, r1s_id, r1s_ptr, r1s_p, r1s_a, r1s_sign,
                                                                    W, ldW, out);
     if (nr1d > 0) {
-        double *Vt = nullptr;
-        HB_CUDA(cudaMallocAsync(&Vt, sizeof(double) * ld * nr1d, s));
         gemm(s, n, nr1d, n, 1.0, W, ldW, 0, A1, ld, 0, 0.0, Vt, ld, 0);
         coldot_pair_kernel<<<(nr1d * 32 + 255) / 256, 256, 0, s>>>(n, nr1d, r1d_id, r1d_sign, Vt, ld, Vt, ld, out);
-        HB_CUDA(cudaFreeAsync(Vt, s));
     }
     for (int i = 0; i < ndr; ++i) {
         gemm(s, n, n, n, 1.0, dr_mat[i], ld, 0, W, ldW, 0, 0.0, T1, ld, 0);

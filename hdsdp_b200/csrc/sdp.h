@@ -71,6 +71,8 @@ struct SdpDevice {
 
     // scratch
     double *V = nullptr;       // n x max(nr1d, nr1s) (W * A_r1)
+    double *Vt = nullptr;      // n x nr1d scratch for inner products
+    double *Vs = nullptr;      // n x nr1s scratch for rank-one x sparse cross terms
     double *G = nullptr;       // nr1d x nr1d
     double *T1 = nullptr;      // n x n
     double *T2 = nullptr;      // n x n

@@ -37,6 +37,8 @@ struct Timers {
     double schur = 0, schur_factor = 0, schur_solve = 0, s_factor = 0, s_inverse = 0, lanczos = 0,
            assemble = 0, primal = 0, total = 0;
     long n_schur = 0, n_sfactor = 0, n_lanczos = 0, n_lanczos_mv = 0, n_schur_solve = 0;
+    // finer split (seconds)
+    double lz_inverse = 0, lz_host = 0, lz_wait = 0, sch_matrix = 0, sch_inner = 0, sch_innersq = 0;
 };
 
 // Lanczos maximum-step estimator (linalg/hdsdp_lanczos.c:161-292) on the GPU.
@@ -44,7 +46,7 @@ struct Lanczos {
     int n = 0, maxdim = 30;
     long ld = 0;
     cudaStream_t s = nullptr;
-    double *V = nullptr, *w = nullptr, *z1 = nullptr, *z2 = nullptr, *t1 = nullptr, *warm = nullptr;
+    double *V = nullptr, *w = nullptr, *z1 = nullptr, *z2 = nullptr, *t1 = nullptr, *u = nullptr, *warm = nullptr;
     double *d_ab = nullptr;   // alpha[0..maxdim), beta[maxdim..2*maxdim+1)
     double *h_ab = nullptr;   // pinned
     double *d_y = nullptr;    // 2 * (maxdim + 1)

@@ -41,8 +41,10 @@ extern int HDSDPGetIterLog( hdsdp *HSolver, int maxLen, double *t, double *pObj,
    [0] Schur assembly  [1] Schur factorisation  [2] Schur solves  [3] S factorisations
    [4] S inverse       [5] Lanczos              [6] S assembly    [7] primal recovery
    [8] total           [9] #Schur builds       [10] #S factorisations
-   [11] #Lanczos runs  [12] #Lanczos matvecs    [13] #Schur solves */
-extern void HDSDPGetTimers( hdsdp *HSolver, double out[14] );
+   [11] #Lanczos runs  [12] #Lanczos matvecs    [13] #Schur solves
+   [14] Lanczos: L^-1  [15] Lanczos: host eigen [16] Lanczos: device wait
+   [17] Schur: matrix  [18] Schur: <A_i, W>     [19] Schur: <A_i, W^2> */
+extern void HDSDPGetTimers( hdsdp *HSolver, double out[20] );
 
 /* ---- Kernel-level entry points (host buffers in, host buffers out) ---------------- */
 
@@ -84,6 +86,10 @@ extern int hdsdpb_gemm( int M, int N, int K, double alpha, const double *A, int 
    2 Cholesky, 3 triangular inverse L^-1, 4 matrix-vector product,
    5 Lanczos step bound, 6 rank-64 SYRK update. Writes milliseconds per call. */
 extern int hdsdpb_kernel_timing( int which, int n, int reps, double *ms );
+
+/* Milliseconds taken by `reps` grid-wide barriers in one cooperative launch of
+   `blocks` blocks of 256 threads (cost model of the persistent factorisation). */
+extern int hdsdpb_gridsync_probe( int blocks, int reps, double *ms );
 
 #ifdef __cplusplus
 }
