@@ -1,0 +1,401 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 dual-scaling IPM: time to a 1e-6 relative gap.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                    [--workload rank1_n1000_m2000] [--precision fp64|split]
+
+One step is one complete solve of the workload through the hdsdp.h C API
+(create, set cone data, set the dual objective, optimize, read the dual)
+with the five-step primal refinement off, so the solve stops at the
+reference's own relative-gap test (1e-6). Printed as one JSON line:
+
+  value  seconds per solve for the iterations alone (data resident on the
+         device; CUDA events on the solver stream, inside the library)
+  e2e    seconds per solve through the public API from pinned host buffers,
+         host->device upload and device->host read of y included (CUDA
+         events around each call)
+  roofline  the kernel family with the largest device time in the timed
+         region: algorithmic flops (or bytes) per launch over its CUDA-event
+         duration, against MEASURED_PEAKS.json
+  cpu_baseline  the reference CPU solver (oracle/_ref, all host threads) on a
+         bounded sample of the same solve: the first few iterations, scaled
+         to the reference's full iteration count
+
+--impl reference times the reference CPU solver alone (rank 0) on the same
+workload and prints the same metric with "impl": "reference". Multi-GPU runs
+are independent replicas, one solve per GPU per step ("scaling": "weak"),
+timed as the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "time to 1e-6 rel gap (dual-scaling IPM solve)"
+UNIT = "s"
+FLUSH_BYTES = 256 << 20  # larger than the 126 MB L2
+FAMILIES = ["fp64_gemm_dmma", "potrf_coop", "trtri_coop", "schur_pair_gather", "bf16x3_gemm_tcgen05"]
+FAMILY_BOUND = ["tensor", "tensor", "tensor", "hbm", "tensor"]
+# ncu dram__bytes_read.sum + dram__bytes_write.sum per launch of the top kernel on
+# the bench workload, from the capture summarised under profiles/ (None until captured).
+TRAFFIC_PER_LAUNCH = {}
+REF_SAMPLE_ITERS = 5
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="rank1_n1000_m2000")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "split"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
+def host_cores() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return {"hbm_gbs": p["hbm_gbs"], "bf16_tflops": p["bf16_tflops"],
+                "bf16_tflops_sustained": p["bf16_tflops_sustained"], "source": "measured"}
+    except (OSError, KeyError, ValueError):
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0, "source": "fallback"}
+
+
+class ClockSampler:
+    """nvidia-smi samples of this GPU's clocks and throttle reasons during the timed region."""
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, bus_id: str | None):
+        self.bus_id = bus_id
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", ".clocks_%d.csv" % os.getpid())
+
+    def start(self):
+        os.makedirs(os.path.dirname(self.path), exist_ok=True)
+        cmd = ["nvidia-smi", "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits", "-lms", "200"]
+        if self.bus_id:
+            cmd += ["-i", self.bus_id]
+        try:
+            self.out = open(self.path, "w")
+            self.proc = subprocess.Popen(cmd, stdout=self.out, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.out.close()
+        sm, smax, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax = max(smax, float(parts[1]))
+            except ValueError:
+                continue
+            for name, v in zip(names, parts[3:7]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        os.remove(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def max_over_ranks(x: float, world: int, device: str) -> float:
+    """Max of a per-rank time over all ranks (every rank takes this collective)."""
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------
+# reference CPU solver (oracle/_ref): the cpu_baseline leg and --impl reference
+
+def reference_iters(workload: str):
+    """The reference's full iteration count for the workload (committed golden fixture)."""
+    try:
+        with open(os.path.join(ROOT, "tests", "golden", "golden.json")) as f:
+            g = json.load(f)
+        return g["solves"]["%s/psdp0" % workload]["iters"]
+    except (OSError, KeyError, ValueError):
+        return None
+
+
+def reference_sample(inst, workload: str, iters: int, threads: int, fallback_iters=None):
+    """Seconds to a 1e-6 gap for the reference CPU solver, estimated from two bounded runs.
+
+    A run capped at one iteration gives the set-up cost plus one iteration; a run
+    capped at 1 + `iters` adds `iters` iterations. The estimate is the first plus
+    the marginal per-iteration cost times the reference's remaining iterations.
+    """
+    from oracle import ref_api
+    ref_api.set_threads(threads)
+    r1 = ref_api.solve(inst, want_x=False, params={0: 1, 4: 0})
+    rk = ref_api.solve(inst, want_x=False, params={0: 1 + iters, 4: 0})
+    done = max(1, rk["iters"] - r1["iters"])
+    per_iter = max(0.0, rk["time"] - r1["time"]) / done
+    full = reference_iters(workload) or fallback_iters or rk["iters"]
+    return r1["time"] + per_iter * (full - r1["iters"]), r1["time"] + rk["time"], done, full
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    from hdsdp_b200 import instances
+    from oracle import ref_api
+    base = {"metric": METRIC, "unit": UNIT, "impl": "reference", "higher_is_better": False}
+    if not ref_api.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built (make -C oracle)"}))
+        return
+    inst = instances.WORKLOADS[args.workload]()
+    cores = host_cores()
+    from oracle import ref_api as _ra
+    _ra.set_threads(cores)
+    for _ in range(args.warmup):
+        _ra.solve(inst, want_x=False, params={0: 1, 4: 0})
+    vals, raw = [], []
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        est, t, done, full = reference_sample(inst, args.workload, REF_SAMPLE_ITERS, cores)
+        vals.append(est)
+        raw.append(t)
+    wall = time.perf_counter() - t0
+    value = statistics.mean(vals)
+    sample = ("per step: %s solves capped at 1 and %d IPM iterations (%.2f s of CPU work); set-up + "
+              "marginal s/iter scaled to the reference's %d iterations" % (args.workload, 1 + REF_SAMPLE_ITERS,
+                                                                         statistics.mean(raw), full))
+    line = dict(base, value=value, n_gpus=args.gpus, steps=args.steps, warmup=args.warmup,
+                ms_per_step=1e3 * wall / args.steps, scaling="weak", vs_baseline=None, dtype="f64",
+                data="synthetic (seeded generator, hdsdp_b200/instances.py)",
+                config={"workload": args.workload, "n": inst.n, "m": inst.m, "primal_refinement": False,
+                        "l2": "n/a (CPU)"},
+                cpu_baseline={"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
+                              "sample": sample},
+                e2e={"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+                s_per_iter=value / full)
+    print(json.dumps(line))
+
+
+# ---------------------------------------------------------------------------
+# B200 arm
+
+def run_b200(args):
+    rank, world, local_rank = dist_env()
+    if world > 1 and "CUDA_VISIBLE_DEVICES" not in os.environ:
+        os.environ["CUDA_VISIBLE_DEVICES"] = str(local_rank)
+    import ctypes as C
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    from hdsdp_b200 import _lib, api, instances
+
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py: no CUDA device (the B200 arm has no CPU path)")
+    torch.cuda.set_device(0)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", 0))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    L = _lib.load()
+    inst = instances.WORKLOADS[args.workload]()
+    precision = 1 if args.precision == "split" else 0
+
+    # pinned host copies of the step's inputs
+    def pinned(a, dtype):
+        a = np.ascontiguousarray(a, dtype=dtype)
+        t = torch.empty(a.shape, dtype={np.int32: torch.int32, np.float64: torch.float64}[dtype], pin_memory=True)
+        out = t.numpy()
+        out[...] = a
+        return out, t
+
+    Ap, _tAp = pinned(inst.Ap, np.int32)
+    Ai, _tAi = pinned(inst.Ai, np.int32)
+    Ax, _tAx = pinned(inst.Ax, np.float64)
+    bvec, _tb = pinned(inst.b, np.float64)
+    yout, _ty = pinned(np.zeros(inst.m), np.float64)
+    h2d = Ap.nbytes + Ai.nbytes + Ax.nbytes + bvec.nbytes
+    d2h = yout.nbytes + 2 * 8
+
+    def one_solve():
+        s = api.Solver()
+        try:
+            s.init(inst.m, 1)
+            if s.set_cone(inst.m, inst.n, Ap, Ai, Ax) != 0:
+                raise RuntimeError("HDSDPSetCone rejected the block")
+            s.set_dual_objective(bvec)
+            s.set_primal_refinement(False)
+            s.set_precision(precision)
+            ret = s.optimize(0)
+            po, do = C.c_double(), C.c_double()
+            L.HDSDPGetRowDual(s.h, C.byref(po), C.byref(do), yout.ctypes.data_as(C.POINTER(C.c_double)))
+            return {"ret": ret, "status": s.status(), "iters": s.iters(), "timers": s.timers(),
+                    "log": s.iter_log(), "pobj": po.value, "dobj": do.value}
+        finally:
+            s.close()
+
+    flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    for _ in range(max(3, args.warmup)):
+        one_solve()
+
+    bus = None
+    try:
+        p = torch.cuda.get_device_properties(0)
+        bus = "%08X:%02X:%02X.0" % (p.pci_domain_id, p.pci_bus_id, p.pci_device_id)
+    except Exception:
+        bus = None
+    clocks = ClockSampler(bus)
+    L.hdsdpb_kstat_enable((1 << len(FAMILIES)) - 1)
+    launches0 = L.hdsdpb_launch_count()
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    time.sleep(0.3)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    results = []
+    w0 = time.perf_counter()
+    for k in range(args.steps):
+        flush.zero_()  # evict the previous solve's working set from L2
+        torch.cuda.synchronize()
+        ev[k][0].record()
+        results.append(one_solve())
+        ev[k][1].record()
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - w0
+    barrier()
+    clk = clocks.stop()
+    launches = L.hdsdpb_launch_count() - launches0
+    fam = []
+    for f in range(len(FAMILIES)):
+        n_l, ms, work = C.c_longlong(), C.c_double(), C.c_double()
+        L.hdsdpb_kstat_read(f, C.byref(n_l), C.byref(ms), C.byref(work))
+        fam.append((n_l.value, ms.value, work.value))
+    L.hdsdpb_kstat_enable(0)
+
+    e2e_s = [ev[k][0].elapsed_time(ev[k][1]) * 1e-3 for k in range(args.steps)]
+    ipm_s = [r["timers"]["ipm_device"] for r in results]
+    iters = results[-1]["iters"]
+    value = max_over_ranks(statistics.mean(ipm_s), world, "cuda")
+    e2e = max_over_ranks(statistics.mean(e2e_s), world, "cuda")
+    last = results[-1]
+    gap = np.asarray(last["log"]["gap"])
+    tlog = np.asarray(last["log"]["t"])
+    hit = np.flatnonzero(gap <= 1e-6)
+    time_to_gap = float(tlog[hit[0]] - last["timers"]["setup"]) if hit.size else None
+
+    pk = peaks()
+    top = max(range(len(FAMILIES)), key=lambda f: fam[f][1])
+    n_l, ms, work = fam[top]
+    if FAMILY_BOUND[top] == "tensor":
+        achieved = work / (ms * 1e-3) / 1e12 if ms > 0 else 0.0
+        peak, unit = pk["bf16_tflops_sustained"], "TFLOP/s"
+    else:
+        achieved = work / (ms * 1e-3) / 1e9 if ms > 0 else 0.0
+        peak, unit = pk["hbm_gbs"], "GB/s"
+    roofline = {"bound": FAMILY_BOUND[top], "kernel": FAMILIES[top], "achieved": achieved, "peak": peak,
+                "unit": unit, "frac": achieved / peak, "peak_source": pk["source"],
+                "traffic": TRAFFIC_PER_LAUNCH.get((args.workload, FAMILIES[top])),
+                "launches": n_l, "ms_total": ms, "share_of_ipm": ms * 1e-3 / sum(ipm_s)}
+    if FAMILIES[top] == "bf16x3_gemm_tcgen05":
+        roofline["note"] = "achieved counts the three BF16 products of each split product"
+    elif FAMILY_BOUND[top] == "tensor":
+        roofline["note"] = ("FP64 DMMA (mma.sync m8n8k4 f64): tcgen05 has no f64 kind; peak is the measured "
+                            "sustained bf16 figure, nominal FP64 tensor peak is about 40 TFLOP/s")
+    kernels = {FAMILIES[f]: {"launches": fam[f][0], "ms": fam[f][1],
+                             ("tflops" if FAMILY_BOUND[f] == "tensor" else "gbs"):
+                                 (fam[f][2] / (fam[f][1] * 1e-3) / (1e12 if FAMILY_BOUND[f] == "tensor" else 1e9)
+                                  if fam[f][1] > 0 else None)}
+               for f in range(len(FAMILIES))}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            from oracle import ref_api
+            if ref_api.available():
+                cores = host_cores()
+                est, t, done, full = reference_sample(inst, args.workload, REF_SAMPLE_ITERS, cores,
+                                                      fallback_iters=iters)
+                cpu = {"value": est, "unit": UNIT, "cores": cores, "kind": "reference",
+                       "sample": "reference CPU solves capped at 1 and %d IPM iterations (%.2f s of CPU work); "
+                                 "set-up + marginal s/iter scaled to its %d iterations" % (1 + done, t, full)}
+        except Exception as exc:  # the baseline is reported, never required
+            cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": "failed: %s" % exc}
+
+    t = last["timers"]
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": max(3, args.warmup), "ms_per_step": 1e3 * value, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if precision == 0 else "bf16x3+f64",
+        "data": "synthetic (seeded generator, hdsdp_b200/instances.py)",
+        "config": {"workload": args.workload, "n": inst.n, "m": inst.m, "primal_refinement": False,
+                   "precision": args.precision, "parallelism": "replicas" if world > 1 else "single",
+                   "l2": "flushed between steps (256 MB write)"},
+        "iters": iters, "s_per_iter": value / max(1, iters), "time_to_gap_s": time_to_gap,
+        "status": last["status"], "dobj": last["dobj"], "pobj": last["pobj"],
+        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "roofline": roofline, "kernels": kernels, "cpu_baseline": cpu, "clocks": clk,
+        "gpu_launches": launches, "wall_s": wall,
+        "split_s": {k: t[k] for k in ("schur", "schur_factor", "schur_solve", "s_factor", "s_inverse",
+                                      "lanczos", "assemble", "primal", "setup", "total")},
+    }
+    if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

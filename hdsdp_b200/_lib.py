@@ -20,9 +20,10 @@ EXPORTS = [
     "HUserDataCreate", "HUserDataSetConeData", "HUserDataChooseCone", "HUserDataClear",
     "HUserDataDestroy",
     "HDSDPGetStatus", "HDSDPGetIterCount", "HDSDPSetPrimalRefinement", "HDSDPSetPrecision",
-    "HDSDPGetIterLog", "HDSDPGetTimers",
+    "HDSDPGetIterLog", "HDSDPGetTimers", "HDSDPAdjoint",
     "hdsdpb_schur_probe", "hdsdpb_ratio_probe", "hdsdpb_cholesky", "hdsdpb_inverse", "hdsdpb_gemm",
-    "hdsdpb_kernel_timing", "hdsdpb_gridsync_probe",
+    "hdsdpb_kernel_timing", "hdsdpb_gridsync_probe", "hdsdpb_launch_count",
+    "hdsdpb_kstat_enable", "hdsdpb_kstat_read", "hdsdpb_split_gemm",
 ]
 
 _lib = None
@@ -62,6 +63,7 @@ def load():
         "HDSDPSetPrecision": ([vp, i], None),
         "HDSDPGetIterLog": ([vp, i, dp, dp, dp, dp, dp, ip], i),
         "HDSDPGetTimers": ([vp, dp], None),
+        "HDSDPAdjoint": ([vp, dp, dp, dp, dp, dp], i),
         "hdsdpb_schur_probe": ([i, i, ip, ip, dp, dp, d, i, dp, dp, dp, dp], i),
         "hdsdpb_ratio_probe": ([i, i, ip, ip, dp, dp, d, dp, d, dp, dp], i),
         "hdsdpb_cholesky": ([i, dp, dp, dp], i),
@@ -69,6 +71,10 @@ def load():
         "hdsdpb_gemm": ([i, i, i, d, dp, i, i, dp, i, i, d, dp, i], i),
         "hdsdpb_kernel_timing": ([i, i, i, dp], i),
         "hdsdpb_gridsync_probe": ([i, i, dp], i),
+        "hdsdpb_launch_count": ([], C.c_longlong),
+        "hdsdpb_kstat_enable": ([i], i),
+        "hdsdpb_split_gemm": ([i, i, i, dp, i, i, dp, i, i, dp, i], i),
+        "hdsdpb_kstat_read": ([i, C.POINTER(C.c_longlong), dp, dp], i),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

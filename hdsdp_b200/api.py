@@ -110,12 +110,27 @@ class Solver:
         return arr
 
     def timers(self):
-        t = np.zeros(20)
+        t = np.zeros(22)
         self.L.HDSDPGetTimers(self.h, _dp(t))
         keys = ["schur", "schur_factor", "schur_solve", "s_factor", "s_inverse", "lanczos", "assemble",
                 "primal", "total", "n_schur", "n_sfactor", "n_lanczos", "n_lanczos_mv", "n_schur_solve",
-                "lz_inverse", "lz_host", "lz_wait", "sch_matrix", "sch_inner", "sch_innersq"]
+                "lz_inverse", "lz_host", "lz_wait", "sch_matrix", "sch_inner", "sch_innersq", "setup",
+                "ipm_device"]
         return dict(zip(keys, t.tolist()))
+
+    def adjoint(self, gy=None, GX=None, want_gC=True):
+        """Gradients (gb, gC, gAx) of <GX, X*> + gy^T y* after optimize() (HDSDPAdjoint)."""
+        n, m = self.n, self.m
+        gyv = None if gy is None else np.ascontiguousarray(gy, dtype=np.float64)
+        GXf = None if GX is None else np.asfortranarray(GX, dtype=np.float64)
+        gb = np.zeros(m)
+        gC = np.zeros((n, n), order="F") if want_gC else None
+        gAx = np.zeros(len(self._keep[2]))
+        r = self.L.HDSDPAdjoint(self.h, None if gyv is None else _dp(gyv), None if GXf is None else _dp(GXf),
+                                _dp(gb), None if gC is None else _dp(gC), _dp(gAx))
+        if r != 0:
+            raise RuntimeError("HDSDPAdjoint failed (%d)" % r)
+        return gb, gC, gAx
 
     def close(self):
         if self.ud:
@@ -162,3 +177,99 @@ def solve(inst, want_x: bool = True, primal_refinement: bool = True, precision: 
         return out
     finally:
         s.close()
+
+
+# ---------------------------------------------------------------------------
+# Kernel-level entry points (include/hdsdp_b200.h), host buffers in and out.
+
+def _csc(inst):
+    return (np.ascontiguousarray(inst.Ap, dtype=np.int32), np.ascontiguousarray(inst.Ai, dtype=np.int32),
+            np.ascontiguousarray(inst.Ax, dtype=np.float64))
+
+
+def schur_probe(inst, y, resi, precision: int = 0) -> dict:
+    """GPU Schur complement at S = C - A^T y - resi I (lower triangle of M, full storage)."""
+    L = _lib.load()
+    Ap, Ai, Ax = _csc(inst)
+    y = np.ascontiguousarray(y, dtype=np.float64)
+    m = inst.m
+    M = np.zeros(m * m)
+    asinv, asinvrd = np.zeros(m), np.zeros(m)
+    tr = C.c_double()
+    r = L.hdsdpb_schur_probe(m, inst.n, _ip(Ap), _ip(Ai), _dp(Ax), _dp(y), float(resi), int(precision),
+                             _dp(M), _dp(asinv), _dp(asinvrd), C.byref(tr))
+    if r != 0:
+        raise RuntimeError("hdsdpb_schur_probe returned %d" % r)
+    return {"M": np.tril(M.reshape(m, m, order="F")), "asinv": asinv, "asinvrd": asinvrd,
+            "tracesinv": tr.value}
+
+
+def ratio_probe(inst, y, resi, dy, ada: float):
+    """GPU Lanczos step bound and log det S (first ratio test of a fresh block)."""
+    L = _lib.load()
+    Ap, Ai, Ax = _csc(inst)
+    y = np.ascontiguousarray(y, dtype=np.float64)
+    dy = np.ascontiguousarray(dy, dtype=np.float64)
+    step, logdet = C.c_double(), C.c_double()
+    r = L.hdsdpb_ratio_probe(inst.m, inst.n, _ip(Ap), _ip(Ai), _dp(Ax), _dp(y), float(resi), _dp(dy),
+                             float(ada), C.byref(step), C.byref(logdet))
+    if r != 0:
+        raise RuntimeError("hdsdpb_ratio_probe returned %d" % r)
+    return step.value, logdet.value
+
+
+def cholesky(S):
+    """(L, sum log L_ii, positive definite?) of a symmetric matrix on the GPU."""
+    L = _lib.load()
+    S = np.asfortranarray(S, dtype=np.float64)
+    n = S.shape[0]
+    out = np.zeros((n, n), order="F")
+    ld = C.c_double()
+    r = L.hdsdpb_cholesky(n, _dp(S), _dp(out), C.byref(ld))
+    if r < 0:
+        raise RuntimeError("hdsdpb_cholesky returned %d" % r)
+    return out, ld.value, r == 0
+
+
+def inverse(S):
+    """S^-1 of a symmetric positive definite matrix on the GPU (None if not positive definite)."""
+    L = _lib.load()
+    S = np.asfortranarray(S, dtype=np.float64)
+    n = S.shape[0]
+    out = np.zeros((n, n), order="F")
+    r = L.hdsdpb_inverse(n, _dp(S), _dp(out))
+    if r < 0:
+        raise RuntimeError("hdsdpb_inverse returned %d" % r)
+    return out if r == 0 else None
+
+
+def gemm(alpha, A, B, beta=0.0, Cm=None, transA=False, transB=False):
+    """alpha op(A) op(B) + beta C on the FP64 tensor-core path."""
+    L = _lib.load()
+    A = np.asfortranarray(A, dtype=np.float64)
+    B = np.asfortranarray(B, dtype=np.float64)
+    M = A.shape[1] if transA else A.shape[0]
+    K = A.shape[0] if transA else A.shape[1]
+    N = B.shape[0] if transB else B.shape[1]
+    Cm = np.zeros((M, N), order="F") if Cm is None else np.asfortranarray(Cm, dtype=np.float64).copy(order="F")
+    r = L.hdsdpb_gemm(M, N, K, float(alpha), _dp(A), max(1, A.shape[0]), int(transA), _dp(B), max(1, B.shape[0]),
+                      int(transB), float(beta), _dp(Cm), max(1, M))
+    if r != 0:
+        raise RuntimeError("hdsdpb_gemm returned %d" % r)
+    return Cm
+
+
+def split_gemm(A, B, transA=False, transB=False):
+    """op(A) op(B) as BF16x3 products with FP32 accumulation on the tcgen05 tensor cores."""
+    L = _lib.load()
+    A = np.asfortranarray(A, dtype=np.float64)
+    B = np.asfortranarray(B, dtype=np.float64)
+    M = A.shape[1] if transA else A.shape[0]
+    K = A.shape[0] if transA else A.shape[1]
+    N = B.shape[0] if transB else B.shape[1]
+    Cm = np.zeros((M, N), order="F")
+    r = L.hdsdpb_split_gemm(M, N, K, _dp(A), max(1, A.shape[0]), int(transA), _dp(B), max(1, B.shape[0]),
+                            int(transB), _dp(Cm), max(1, M))
+    if r != 0:
+        raise RuntimeError("hdsdpb_split_gemm returned %d" % r)
+    return Cm

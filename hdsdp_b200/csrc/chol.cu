@@ -19,19 +19,9 @@ namespace cg = cooperative_groups;
 
 namespace hb {
 
-// Optional per-phase timestamps of the factorisation (null in normal runs).
-__device__ unsigned long long *g_chol_stamps = nullptr;
-
 namespace {
 constexpr int NB = 64;
 
-__device__ __forceinline__ void stamp(int slot) {
-    if (g_chol_stamps && threadIdx.x == 0 && slot < 4096) {
-        unsigned long long t;
-        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-        g_chol_stamps[slot] = t;
-    }
-}
 constexpr int TP = 68;                         // tile pitch (conflict-free DMMA fragment reads)
 constexpr int SM_DOUBLES = 3 * 64 * TP;        // three 64 x 68 tiles
 constexpr int COOP_THREADS = 256;
@@ -290,23 +280,18 @@ __global__ void __launch_bounds__(COOP_THREADS) potrf_coop_kernel(double *L, lon
         if (rows <= 0) break;
         double *P = L + (size_t) (j0 + nb) + (size_t) j0 * ld;
         const int nchunk = (rows + 63) / 64;
-        const int pj = (j0 / NB) * 8;
-        if (blockIdx.x <= 1) stamp(pj + 4 * blockIdx.x + 0);
         for (int ch = blockIdx.x; ch < nchunk; ch += gridDim.x) {
             const int mr = min(64, rows - ch * 64);
             tile_mma_dev(P + ch * 64, ld, mr, nb, P + ch * 64, ld, mr, Dinv + j0, ldd, 1, nb, nb, false, 1, sm);
         }
-        if (blockIdx.x <= 1) stamp(pj + 4 * blockIdx.x + 1);
         grid.sync();
         const long ntile = (long) nchunk * (nchunk + 1) / 2;
         double *A22 = L + (size_t) (j0 + nb) + (size_t) (j0 + nb) * ld;
         if (blockIdx.x == 0) {
             // tile (0, 0) is the next diagonal block: update it, then factor it
             const int mr = min(64, rows);
-            stamp(pj + 2);
             tile_mma_dev(A22, ld, mr, mr, P, ld, mr, P, ld, 1, mr, nb, true, 0, sm);
             potf2_dev(L, ld, j0 + nb, min(NB, rows), Dinv, ldd, info, sm);
-            stamp(pj + 3);
         }
         // remaining tiles, spread over the other blocks (block 0 joins when the grid has one block)
         const int nworker = (gridDim.x > 1) ? (int) gridDim.x - 1 : 1;
@@ -320,7 +305,6 @@ __global__ void __launch_bounds__(COOP_THREADS) potrf_coop_kernel(double *L, lon
                              P + tj * 64, ld, 1, nc, nb, ti == tj, 0, sm);
             }
         }
-        if (blockIdx.x == 1) stamp(pj + 6);
         grid.sync();
     }
 }
@@ -396,8 +380,8 @@ int grid_for_n(long total) {
 
 bool coop_factorize_enqueue(cudaStream_t s, DenseFactor &F, const double *S, long ldS) {
     const int n = F.n;
-    zero_info_k<<<1, 1, 0, s>>>(F.d_info);
-    copy_lower_k<<<grid_for_n((long) n * n), 256, 0, s>>>(n, S, ldS, F.L, F.ld);
+    zero_info_k<<<hb::counted(1), 1, 0, s>>>(F.d_info);
+    copy_lower_k<<<hb::counted(grid_for_n((long) n * n)), 256, 0, s>>>(n, S, ldS, F.L, F.ld);
     const void *fn = (const void *) potrf_coop_kernel;
     const long t0 = (long) ((n - 1) / 64 + 1);
     const int grid = (int) std::max(1L, std::min<long>(coop_grid(fn), t0 * (t0 + 1) / 2));
@@ -408,7 +392,10 @@ bool coop_factorize_enqueue(cudaStream_t s, DenseFactor &F, const double *S, lon
     long ldd = F.ld;
     int *ip = F.d_info;
     void *args[] = {&Lp, &ld, &nn, &Dp, &ldd, &ip};
-    cudaError_t e = cudaLaunchCooperativeKernel(fn, grid, COOP_THREADS, args, SM_DOUBLES * sizeof(double), s);
+    const bool timed = kstat_on(KF_POTRF);
+    if (timed) kstat_begin(KF_POTRF, s, (double) n * n * n / 3.0);
+    cudaError_t e = cudaLaunchCooperativeKernel(fn, hb::counted(grid), COOP_THREADS, args, SM_DOUBLES * sizeof(double), s);
+    if (timed) kstat_end(s);
     if (e != cudaSuccess) {
         cudaGetLastError();
         return false;
@@ -418,7 +405,7 @@ bool coop_factorize_enqueue(cudaStream_t s, DenseFactor &F, const double *S, lon
 
 bool coop_inverse_enqueue(cudaStream_t s, DenseFactor &F) {
     const int n = F.n;
-    identity_k<<<grid_for_n((long) n * n), 256, 0, s>>>(n, F.K, F.ld);
+    identity_k<<<hb::counted(grid_for_n((long) n * n)), 256, 0, s>>>(n, F.K, F.ld);
     const void *fn = (const void *) trtri_coop_kernel;
     const long t0 = (long) ((n - 1) / 64 + 1);
     const int grid = (int) std::max(1L, std::min<long>(coop_grid(fn), t0 * t0 / 4 + 1));
@@ -429,7 +416,10 @@ bool coop_inverse_enqueue(cudaStream_t s, DenseFactor &F) {
     const double *Dp = F.Dinv;
     long ldd = F.ld;
     void *args[] = {&Lp, &Kp, &ld, &nn, &Dp, &ldd};
-    cudaError_t e = cudaLaunchCooperativeKernel(fn, grid, COOP_THREADS, args, SM_DOUBLES * sizeof(double), s);
+    const bool timed = kstat_on(KF_TRTRI);
+    if (timed) kstat_begin(KF_TRTRI, s, (double) n * n * n / 3.0);
+    cudaError_t e = cudaLaunchCooperativeKernel(fn, hb::counted(grid), COOP_THREADS, args, SM_DOUBLES * sizeof(double), s);
+    if (timed) kstat_end(s);
     if (e != cudaSuccess) {
         cudaGetLastError();
         return false;
@@ -437,40 +427,4 @@ bool coop_inverse_enqueue(cudaStream_t s, DenseFactor &F) {
     return true;
 }
 
-}  // namespace hb
-
-namespace hb {
-// Debug probe: factor a well-conditioned n x n matrix and return per-panel phase
-// timestamps (ns, relative to the first) in out[0 .. 8 * panels).
-int chol_phase_probe(int n, double *out) {
-    cudaStream_t s;
-    cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
-    const long ld = pad_ld(n);
-    double *A = nullptr;
-    unsigned long long *st = nullptr;
-    cudaMalloc(&A, sizeof(double) * ld * n);
-    cudaMalloc(&st, sizeof(unsigned long long) * 4096);
-    cudaMemset(st, 0, sizeof(unsigned long long) * 4096);
-    std::vector<double> h((size_t) ld * n, 0.0);
-    for (int j = 0; j < n; ++j)
-        for (int i = 0; i < n; ++i) h[(size_t) j * ld + i] = (i == j) ? 2.0 : 1.0 / (1.0 + i + j);
-    cudaMemcpy(A, h.data(), sizeof(double) * ld * n, cudaMemcpyHostToDevice);
-    DenseFactor F;
-    F.alloc(n);
-    factorize(s, F, A, ld);  // warm
-    cudaMemcpyToSymbol(g_chol_stamps, &st, sizeof(st));
-    factorize(s, F, A, ld);
-    unsigned long long *nul = nullptr;
-    cudaMemcpyToSymbol(g_chol_stamps, &nul, sizeof(nul));
-    std::vector<unsigned long long> hs(4096);
-    cudaMemcpy(hs.data(), st, sizeof(unsigned long long) * 4096, cudaMemcpyDeviceToHost);
-    const int panels = (n + 63) / 64;
-    const unsigned long long t0 = hs[0];
-    for (int i = 0; i < 8 * panels && i < 4096; ++i) out[i] = hs[i] ? (double) (hs[i] - t0) : -1.0;
-    F.release();
-    cudaFree(A);
-    cudaFree(st);
-    cudaStreamDestroy(s);
-    return 0;
-}
 }  // namespace hb

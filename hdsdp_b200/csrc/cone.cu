@@ -297,6 +297,7 @@ hdsdp_retcode SdpCone::setup_device(cudaStream_t stream, Timers *t) {
     // device copy of the (scaled) objective from its lower triplets
     HostCoeff Cdev = C;
     for (double &v : Cdev.v) v *= objScal;
+    dev.precision = precision;
     dev.upload(n, m, Cdev, A, s);
     HB_CUDA(cudaMalloc(&Svar, sizeof(double) * ld * n));
     HB_CUDA(cudaMalloc(&Scheck, sizeof(double) * ld * n));
@@ -612,7 +613,7 @@ hdsdp_retcode KKT::build(SdpCone &cone, int type) {
         dev.inner_all(Wp, ld, cone.d_vec);
         add_host(asinv, cone.d_vec, h_buf, m, 1.0, s);
         if (r != 0.0) {
-            dev.inner_all_sq(Wp, ld, cone.d_vec);
+            dev.inner_all_sq(Wp, ld, cone.d_vec, false, true);
             add_host(asinvrd, cone.d_vec, h_buf, m, r, s);
         }
         if (tm) tm->schur += wall() - t0;
@@ -625,20 +626,20 @@ hdsdp_retcode KKT::build(SdpCone &cone, int type) {
         dTraceSinv += cone.h_scal[0];
     }
     double tq = wall();
-    dev.schur_matrix(Wp, ld, M, ldm);
+    dev.schur_matrix(Wp, ld, M, ldm, (type == KKT_TYPE_PRIMAL) ? nullptr : cone.Fvar.K);
     if (tm) {
         HB_CUDA(cudaStreamSynchronize(s));
         tm->sch_matrix += wall() - tq;
         tq = wall();
     }
-    dev.inner_all(Wp, ld, cone.d_vec);
+    dev.inner_all(Wp, ld, cone.d_vec, true);
     add_host(asinv, cone.d_vec, h_buf, m, 1.0, s);
     if (tm) {
         tm->sch_inner += wall() - tq;
         tq = wall();
     }
     if (r != 0.0) {
-        dev.inner_all_sq(Wp, ld, cone.d_vec);
+        dev.inner_all_sq(Wp, ld, cone.d_vec, true);
         add_host(asinvrd, cone.d_vec, h_buf, m, r, s);
     }
     if (tm) tm->sch_innersq += wall() - tq;
@@ -955,8 +956,8 @@ hdsdp_retcode Lanczos::solve(DenseFactor &F, const double *D, long ldD, double *
     };
     HB_CUDA(cudaMemsetAsync(V, 0, sizeof(double) * ld * (maxdim + 1), s));
     HB_CUDA(cudaMemsetAsync(d_ab, 0, sizeof(double) * (2 * maxdim + 2), s));
-    if (nComputed == 0) lanczos_start_kernel<<<1, 1024, 0, s>>>(n, nullptr, init_vec, V);
-    else lanczos_start_kernel<<<1, 1024, 0, s>>>(n, warm, pert_vec, V);
+    if (nComputed == 0) lanczos_start_kernel<<<hb::counted(1), 1024, 0, s>>>(n, nullptr, init_vec, V);
+    else lanczos_start_kernel<<<hb::counted(1), 1024, 0, s>>>(n, warm, pert_vec, V);
 
     hdsdp_retcode ret = HDSDP_RETCODE_OK;
     bool done = false;
@@ -965,7 +966,7 @@ hdsdp_retcode Lanczos::solve(DenseFactor &F, const double *D, long ldD, double *
     std::vector<double> T, ev, evec;
     for (int k = 0; k < maxdim && !done; ++k) {
         mv(V + (size_t) k * ld, w);
-        lanczos_orth_kernel<<<1, 1024, 0, s>>>(n, V, ld, k, w, d_ab, maxdim);
+        lanczos_orth_kernel<<<hb::counted(1), 1024, 0, s>>>(n, V, ld, k, w, d_ab, maxdim);
         const bool sched = ((k + 1) % freq == 0) || k >= maxdim - 1;
         if (!sched) continue;
         HB_CUDA(cudaMemcpyAsync(h_ab, d_ab, sizeof(double) * (2 * maxdim + 2), cudaMemcpyDeviceToHost, s));
@@ -1006,13 +1007,13 @@ hdsdp_retcode Lanczos::solve(DenseFactor &F, const double *D, long ldD, double *
             yy[kp1 + i] = evec[(size_t) i + (size_t) i2 * kp1];
         }
         HB_CUDA(cudaMemcpyAsync(d_y, yy.data(), sizeof(double) * 2 * kp1, cudaMemcpyHostToDevice, s));
-        lanczos_combine_kernel<<<(n + 255) / 256, 256, 0, s>>>(n, V, ld, kp1, d_y, z1);
+        lanczos_combine_kernel<<<hb::counted((n + 255) / 256), 256, 0, s>>>(n, V, ld, kp1, d_y, z1);
         mv(z1, z2);
         HB_CUDA(cudaMemcpyAsync(warm, z2, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
-        lanczos_resid_kernel<<<1, 1024, 0, s>>>(n, z2, z1, eigMin1, d_scal);
-        lanczos_combine_kernel<<<(n + 255) / 256, 256, 0, s>>>(n, V, ld, kp1, d_y + kp1, z2);
+        lanczos_resid_kernel<<<hb::counted(1), 1024, 0, s>>>(n, z2, z1, eigMin1, d_scal);
+        lanczos_combine_kernel<<<hb::counted((n + 255) / 256), 256, 0, s>>>(n, V, ld, kp1, d_y + kp1, z2);
         mv(z2, z1);
-        lanczos_resid_kernel<<<1, 1024, 0, s>>>(n, z1, z2, eigMin1, d_scal + 1);
+        lanczos_resid_kernel<<<hb::counted(1), 1024, 0, s>>>(n, z1, z2, eigMin1, d_scal + 1);
         HB_CUDA(cudaMemcpyAsync(h_scal, d_scal, sizeof(double) * 2, cudaMemcpyDeviceToHost, s));
         HB_CUDA(cudaStreamSynchronize(s));
         const double resiVal1 = h_scal[0], resiVal2 = h_scal[1];

@@ -22,6 +22,25 @@ __host__ __device__ __forceinline__ size_t cm(long i, long j, long ld) { return 
 
 int &device_error_flag();
 
+// Host-side count of kernel launches issued by this library (all threads).
+long long &launch_counter();
+// Every launch site passes its grid through counted(), which bumps the counter.
+template <class G>
+inline G counted(G grid) {
+    __atomic_fetch_add(&launch_counter(), 1LL, __ATOMIC_RELAXED);
+    return grid;
+}
+
+// Live per-family kernel timing: while a family is enabled, every launch of it
+// is bracketed by CUDA events on its own stream and its algorithmic work
+// (flops or bytes) is recorded; kstat_read() resolves the events.
+enum KFamily { KF_GEMM = 0, KF_POTRF = 1, KF_TRTRI = 2, KF_SCHUR_PAIR = 3, KF_SPLIT_GEMM = 4, KF_COUNT = 5 };
+void kstat_enable(int mask);
+bool kstat_on(int family);
+void kstat_begin(int family, cudaStream_t s, double work);
+void kstat_end(cudaStream_t s);
+int kstat_read(int family, long long *launches, double *ms, double *work);
+
 // Leading dimensions are padded to a multiple of 32 doubles (256 bytes) so that
 // every column starts on a 256-byte boundary.
 inline long pad_ld(long n) { return ((n + 31) / 32) * 32; }

@@ -1,5 +1,6 @@
 // Extension entry points of the B200 HDSDP library (include/hdsdp_b200.h).
 #include "solver.h"
+#include "split.h"
 #include "../../include/hdsdp_b200.h"
 #include <cstring>
 #include <cmath>
@@ -30,13 +31,24 @@ int HDSDPGetIterLog(hdsdp *h, int maxLen, double *t, double *pObj, double *dObj,
     return n;
 }
 
-void HDSDPGetTimers(hdsdp *h, double out[20]) {
+void HDSDPGetTimers(hdsdp *h, double out[22]) {
     const Timers &t = h->timers;
-    const double v[20] = {t.schur, t.schur_factor, t.schur_solve, t.s_factor, t.s_inverse, t.lanczos, t.assemble,
+    const double v[22] = {t.schur, t.schur_factor, t.schur_solve, t.s_factor, t.s_inverse, t.lanczos, t.assemble,
                           t.primal, t.total, (double) t.n_schur, (double) t.n_sfactor, (double) t.n_lanczos,
                           (double) t.n_lanczos_mv, (double) t.n_schur_solve, t.lz_inverse, t.lz_host, t.lz_wait,
-                          t.sch_matrix, t.sch_inner, t.sch_innersq};
+                          t.sch_matrix, t.sch_inner, t.sch_innersq, t.setup, t.ipm_device};
     std::memcpy(out, v, sizeof(v));
+}
+
+long long hdsdpb_launch_count(void) { return hb::launch_counter(); }
+
+int hdsdpb_kstat_enable(int mask) {
+    hb::kstat_enable(mask);
+    return 0;
+}
+
+int hdsdpb_kstat_read(int family, long long *launches, double *ms, double *work) {
+    return hb::kstat_read(family, launches, ms, work);
 }
 
 static int probe_setup(SdpCone &c, cudaStream_t s, int m, int n, const int *Ap, const int *Ai, const double *Ax,
@@ -104,6 +116,11 @@ int hdsdpb_ratio_probe(int m, int n, const int *Ap, const int *Ai, const double 
 }
 
 int hdsdpb_cholesky(int n, const double *S, double *L, double *logdiag) {
+    if (n < 0 || (n > 0 && !S)) return -1;
+    if (n == 0) {
+        if (logdiag) *logdiag = 0.0;
+        return 0;
+    }
     cudaStream_t s;
     if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return -1;
     const long ld = pad_ld(n);
@@ -135,6 +152,8 @@ int hdsdpb_cholesky(int n, const double *S, double *L, double *logdiag) {
 }
 
 int hdsdpb_inverse(int n, const double *S, double *Sinv) {
+    if (n < 0 || (n > 0 && (!S || !Sinv))) return -1;
+    if (n == 0) return 0;
     cudaStream_t s;
     if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return -1;
     const long ld = pad_ld(n);
@@ -161,10 +180,13 @@ int hdsdpb_inverse(int n, const double *S, double *Sinv) {
 
 int hdsdpb_gemm(int M, int N, int K, double alpha, const double *A, int lda, int transA, const double *B, int ldb,
                 int transB, double beta, double *C, int ldc) {
-    cudaStream_t s;
-    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return -1;
     const int ar = transA ? K : M, ac = transA ? M : K;
     const int br = transB ? N : K, bc = transB ? K : N;
+    if (M < 0 || N < 0 || K < 0 || lda < (ar > 1 ? ar : 1) || ldb < (br > 1 ? br : 1) || ldc < (M > 1 ? M : 1))
+        return -1;
+    if (M == 0 || N == 0) return 0;
+    cudaStream_t s;
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return -1;
     double *dA = nullptr, *dB = nullptr, *dC = nullptr;
     cudaMalloc(&dA, sizeof(double) * (size_t) lda * ac);
     cudaMalloc(&dB, sizeof(double) * (size_t) ldb * bc);
@@ -172,8 +194,6 @@ int hdsdpb_gemm(int M, int N, int K, double alpha, const double *A, int lda, int
     cudaMemcpy(dA, A, sizeof(double) * (size_t) lda * ac, cudaMemcpyHostToDevice);
     cudaMemcpy(dB, B, sizeof(double) * (size_t) ldb * bc, cudaMemcpyHostToDevice);
     cudaMemcpy(dC, C, sizeof(double) * (size_t) ldc * N, cudaMemcpyHostToDevice);
-    (void) ar;
-    (void) br;
     gemm(s, M, N, K, alpha, dA, lda, transA, dB, ldb, transB, beta, dC, ldc, 0);
     cudaMemcpyAsync(C, dC, sizeof(double) * (size_t) ldc * N, cudaMemcpyDeviceToHost, s);
     cudaStreamSynchronize(s);
@@ -182,6 +202,50 @@ int hdsdpb_gemm(int M, int N, int K, double alpha, const double *A, int lda, int
     cudaFree(dC);
     cudaStreamDestroy(s);
     return device_error_flag() ? -1 : 0;
+}
+
+int hdsdpb_split_gemm(int M, int N, int K, const double *A, int lda, int transA, const double *B, int ldb,
+                      int transB, double *C, int ldc) {
+    const int ar = transA ? K : M, ac = transA ? M : K;
+    const int br = transB ? N : K, bc = transB ? K : N;
+    if (M < 0 || N < 0 || K < 0 || lda < (ar > 1 ? ar : 1) || ldb < (br > 1 ? br : 1) || ldc < (M > 1 ? M : 1))
+        return -1;
+    if (M == 0 || N == 0) return 0;
+    cudaStream_t s;
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return -1;
+    double *dA = nullptr, *dB = nullptr, *dC = nullptr;
+    HB_CUDA(cudaMalloc(&dA, sizeof(double) * (size_t) lda * (ac > 0 ? ac : 1)));
+    HB_CUDA(cudaMalloc(&dB, sizeof(double) * (size_t) ldb * (bc > 0 ? bc : 1)));
+    HB_CUDA(cudaMalloc(&dC, sizeof(double) * (size_t) ldc * N));
+    HB_CUDA(cudaMemcpy(dA, A, sizeof(double) * (size_t) lda * ac, cudaMemcpyHostToDevice));
+    HB_CUDA(cudaMemcpy(dB, B, sizeof(double) * (size_t) ldb * bc, cudaMemcpyHostToDevice));
+    HB_CUDA(cudaMemset(dC, 0, sizeof(double) * (size_t) ldc * N));
+    SplitOperand opA, opB;
+    int ret = 0;
+    if (!opA.alloc(M, K) || !opB.alloc(N, K)) ret = 2;
+    if (ret == 0) {
+        // operand rows: op(A)(r, k) and op(B)(k, c) read as rows c
+        split_from_f64(s, opA, dA, lda, transA != 0);
+        split_from_f64(s, opB, dB, ldb, transB == 0);
+        SplitGemm g;
+        g.M = M;
+        g.N = N;
+        g.K = K;
+        g.C = dC;
+        g.ldc = ldc;
+        if (!split_gemm(s, opA, opB, g)) ret = 2;
+    }
+    HB_CUDA(cudaStreamSynchronize(s));
+    if (ret == 0 && split_error(s)) ret = -1;
+    if (ret == 0) HB_CUDA(cudaMemcpy(C, dC, sizeof(double) * (size_t) ldc * N, cudaMemcpyDeviceToHost));
+    opA.release();
+    opB.release();
+    cudaFree(dA);
+    cudaFree(dB);
+    cudaFree(dC);
+    cudaStreamDestroy(s);
+    if (device_error_flag()) return -1;
+    return ret;
 }
 
 }  // extern "C"
@@ -212,8 +276,8 @@ extern "C" int hdsdpb_kernel_timing(int which, int n, int reps, double *ms) {
     cudaMalloc(&Cm, sizeof(double) * ld * n);
     cudaMalloc(&x, sizeof(double) * ld);
     cudaMalloc(&y, sizeof(double) * ld);
-    fill_spd_kernel<<<1024, 256, 0, s>>>(n, A, ld, 1u);
-    fill_spd_kernel<<<1024, 256, 0, s>>>(n, B, ld, 7u);
+    fill_spd_kernel<<<hb::counted(1024), 256, 0, s>>>(n, A, ld, 1u);
+    fill_spd_kernel<<<hb::counted(1024), 256, 0, s>>>(n, B, ld, 7u);
     fill(s, x, 1.0, n);
     DenseFactor F;
     F.alloc(n);
@@ -269,7 +333,7 @@ extern "C" int hdsdpb_gridsync_probe(int blocks, int reps, double *ms) {
     cudaEventCreate(&e1);
     void *args[] = {&reps, &sink};
     cudaEventRecord(e0, 0);
-    cudaError_t e = cudaLaunchCooperativeKernel((const void *) gridsync_probe_kernel, blocks, 256, args, 0, 0);
+    cudaError_t e = cudaLaunchCooperativeKernel((const void *) gridsync_probe_kernel, hb::counted(blocks), 256, args, 0, 0);
     cudaEventRecord(e1, 0);
     cudaEventSynchronize(e1);
     float t = 0.f;
@@ -281,5 +345,3 @@ extern "C" int hdsdpb_gridsync_probe(int blocks, int reps, double *ms) {
     return e == cudaSuccess ? 0 : -1;
 }
 
-namespace hb { int chol_phase_probe(int n, double *out); }
-extern "C" int hdsdpb_chol_phase_probe(int n, double *out) { return hb::chol_phase_probe(n, out); }

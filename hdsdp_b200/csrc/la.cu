@@ -5,6 +5,7 @@
 // instruction on B200. Every factorisation routine below reduces to this
 // GEMM plus small 64 x 64 kernels.
 #include "la.h"
+#include <vector>
 #include <cmath>
 #include <algorithm>
 
@@ -13,6 +14,88 @@ namespace hb {
 int &device_error_flag() {
     static int flag = 0;
     return flag;
+}
+
+long long &launch_counter() {
+    static long long count = 0;
+    return count;
+}
+
+namespace {
+struct KStatRec {
+    int family;
+    cudaEvent_t e0, e1;
+    double work;
+};
+struct KStatState {
+    int mask = 0;
+    std::vector<KStatRec> pending;
+    std::vector<cudaEvent_t> pool;
+    long long launches[KF_COUNT] = {};
+    double ms[KF_COUNT] = {}, work[KF_COUNT] = {};
+    cudaEvent_t take() {
+        cudaEvent_t e;
+        if (!pool.empty()) {
+            e = pool.back();
+            pool.pop_back();
+        } else {
+            HB_CUDA(cudaEventCreate(&e));
+        }
+        return e;
+    }
+    void resolve() {
+        for (KStatRec &r : pending) {
+            float t = 0.f;
+            HB_CUDA(cudaEventSynchronize(r.e1));
+            HB_CUDA(cudaEventElapsedTime(&t, r.e0, r.e1));
+            launches[r.family] += 1;
+            ms[r.family] += t;
+            work[r.family] += r.work;
+            pool.push_back(r.e0);
+            pool.push_back(r.e1);
+        }
+        pending.clear();
+    }
+};
+KStatState &kstat() {
+    static KStatState st;
+    return st;
+}
+}  // namespace
+
+void kstat_enable(int mask) {
+    KStatState &st = kstat();
+    st.resolve();
+    st.mask = mask;
+    for (int f = 0; f < KF_COUNT; ++f) {
+        st.launches[f] = 0;
+        st.ms[f] = st.work[f] = 0.0;
+    }
+}
+
+bool kstat_on(int family) { return (kstat().mask >> family) & 1; }
+
+void kstat_begin(int family, cudaStream_t s, double work) {
+    KStatState &st = kstat();
+    KStatRec r{family, st.take(), st.take(), work};
+    HB_CUDA(cudaEventRecord(r.e0, s));
+    st.pending.push_back(r);
+}
+
+void kstat_end(cudaStream_t s) {
+    KStatState &st = kstat();
+    HB_CUDA(cudaEventRecord(st.pending.back().e1, s));
+    if (st.pending.size() > 4096) st.resolve();
+}
+
+int kstat_read(int family, long long *launches, double *ms, double *work) {
+    if (family < 0 || family >= KF_COUNT) return -1;
+    KStatState &st = kstat();
+    st.resolve();
+    if (launches) *launches = st.launches[family];
+    if (ms) *ms = st.ms[family];
+    if (work) *work = st.work[family];
+    return 0;
 }
 
 // ------------------------------------------------------------------------------------
@@ -303,7 +386,7 @@ void launch_large(const GemmP &p, cudaStream_t s) {
         init = true;
     }
     dim3 grid((p.M + L_BM - 1) / L_BM, (p.N + L_BN - 1) / L_BN);
-    gemm_large_kernel<TA, TB><<<grid, L_T, L_SMEM, s>>>(p);
+    gemm_large_kernel<TA, TB><<<hb::counted(grid), L_T, L_SMEM, s>>>(p);
 }
 }  // namespace
 
@@ -312,6 +395,15 @@ void gemm(cudaStream_t s, int M, int N, int K, double alpha, const double *A, lo
           const int *abort_flag) {
     if (M <= 0 || N <= 0) return;
     GemmP p{M, N, K, alpha, beta, A, lda, transA, B, ldb, transB, C, ldc, flags, abort_flag};
+    const bool timed = kstat_on(KF_GEMM);
+    if (timed) {
+        // algorithmic flops: halve for a triangular output or a triangular operand
+        double f = 2.0 * M * N * (double) K;
+        if (flags & GEMM_C_LOWER) f *= 0.5;
+        if (flags & (GEMM_A_LOWER | GEMM_A_UPPER)) f *= 0.5;
+        if (flags & (GEMM_B_LOWER | GEMM_B_UPPER)) f *= 0.5;
+        kstat_begin(KF_GEMM, s, f);
+    }
     // Large tiles once the 128 x 128 grid fills the machine; 64 x 64 tiles otherwise.
     const long tiles = (long) ((M + L_BM - 1) / L_BM) * ((N + L_BN - 1) / L_BN);
     if (tiles >= 96 && K >= 64) {
@@ -321,9 +413,10 @@ void gemm(cudaStream_t s, int M, int N, int K, double alpha, const double *A, lo
         else launch_large<1, 1>(p, s);
     } else {
         dim3 grid((M + BM - 1) / BM, (N + BN - 1) / BN);
-        gemm_kernel<<<grid, GT, 0, s>>>(p);
+        gemm_kernel<<<hb::counted(grid), GT, 0, s>>>(p);
     }
     HB_CUDA(cudaGetLastError());
+    if (timed) kstat_end(s);
 }
 
 // ------------------------------------------------------------------------------------
@@ -363,7 +456,7 @@ void coldot(cudaStream_t s, int nrows, int ncols, const double *A, long lda, con
     const int threads = 256;
     const long warps = ncols;
     const int blocks = (int) ((warps * 32 + threads - 1) / threads);
-    coldot_kernel<<<blocks, threads, 0, s>>>(nrows, ncols, A, lda, x, out, alpha, beta, mode);
+    coldot_kernel<<<hb::counted(blocks), threads, 0, s>>>(nrows, ncols, A, lda, x, out, alpha, beta, mode);
     HB_CUDA(cudaGetLastError());
 }
 
@@ -566,15 +659,15 @@ void factorize_async(cudaStream_t s, DenseFactor &F, const double *S, long ldS) 
         HB_CUDA(cudaMemcpyAsync(F.h_info, F.d_info, sizeof(int), cudaMemcpyDeviceToHost, s));
         return;
     }
-    zero_int_kernel<<<1, 1, 0, s>>>(F.d_info);
-    copy_lower_kernel<<<grid_for((long) n * n), 256, 0, s>>>(n, S, ldS, F.L, F.ld);
+    zero_int_kernel<<<hb::counted(1), 1, 0, s>>>(F.d_info);
+    copy_lower_kernel<<<hb::counted(grid_for((long) n * n)), 256, 0, s>>>(n, S, ldS, F.L, F.ld);
     for (int j0 = 0; j0 < n; j0 += NB) {
         const int nb = std::min(NB, n - j0);
-        potf2_kernel<<<1, 256, smem_bytes(), s>>>(F.L, F.ld, nb, j0, F.Dinv, F.ld, F.d_info);
+        potf2_kernel<<<hb::counted(1), 256, smem_bytes(), s>>>(F.L, F.ld, nb, j0, F.Dinv, F.ld, F.d_info);
         const int rows = n - j0 - nb;
         if (rows > 0) {
             double *P = F.L + (size_t) (j0 + nb) + (size_t) j0 * F.ld;
-            trsm_panel_kernel<<<(rows + 63) / 64, 256, smem_bytes(), s>>>(P, F.ld, rows, nb,
+            trsm_panel_kernel<<<hb::counted((rows + 63) / 64), 256, smem_bytes(), s>>>(P, F.ld, rows, nb,
                                                                          F.Dinv + j0, F.ld, F.d_info);
             double *A22 = F.L + (size_t) (j0 + nb) + (size_t) (j0 + nb) * F.ld;
             gemm(s, rows, rows, nb, -1.0, P, F.ld, 0, P, F.ld, 1, 1.0, A22, F.ld, GEMM_C_LOWER, F.d_info);
@@ -606,11 +699,11 @@ void compute_inverse_factor(cudaStream_t s, DenseFactor &F) {
         F.k_valid = true;
         return;
     }
-    set_identity_kernel<<<grid_for((long) n * n), 256, 0, s>>>(n, F.K, F.ld);
+    set_identity_kernel<<<hb::counted(grid_for((long) n * n)), 256, 0, s>>>(n, F.K, F.ld);
     for (int i0 = 0; i0 < n; i0 += NB) {
         const int nb = std::min(NB, n - i0);
         const int cend = i0 + nb;
-        tri_left_kernel<<<(cend + 63) / 64, 256, smem_bytes(), s>>>(F.K + i0, F.ld, nb, cend, F.Dinv + i0, F.ld);
+        tri_left_kernel<<<hb::counted((cend + 63) / 64), 256, smem_bytes(), s>>>(F.K + i0, F.ld, nb, cend, F.Dinv + i0, F.ld);
         const int rows = n - cend;
         if (rows > 0) {
             gemm(s, rows, cend, nb, -1.0, F.L + (size_t) cend + (size_t) i0 * F.ld, F.ld, 0, F.K + i0, F.ld, 0,
@@ -774,73 +867,73 @@ __global__ void dot_kernel(int n, const double *x, const double *y, double *out)
 }  // namespace
 
 void log_diag_sum(cudaStream_t s, const DenseFactor &F, double *d_out) {
-    logdiag_kernel<<<1, 1024, 0, s>>>(F.n, F.L, F.ld, d_out);
+    logdiag_kernel<<<hb::counted(1), 1024, 0, s>>>(F.n, F.L, F.ld, d_out);
     HB_CUDA(cudaGetLastError());
 }
 
 void copy_diag(cudaStream_t s, const DenseFactor &F, double *d_out) {
-    copydiag_kernel<<<grid_for(F.n), 256, 0, s>>>(F.n, F.L, F.ld, d_out);
+    copydiag_kernel<<<hb::counted(grid_for(F.n)), 256, 0, s>>>(F.n, F.L, F.ld, d_out);
 }
 
 void fill(cudaStream_t s, double *x, double v, size_t n) {
     if (!n) return;
-    fill_kernel<<<grid_for((long) n), 256, 0, s>>>(x, v, n);
+    fill_kernel<<<hb::counted(grid_for((long) n)), 256, 0, s>>>(x, v, n);
 }
 
 void axpy(cudaStream_t s, int n, double a, const double *x, double *y) {
     if (n <= 0) return;
-    axpy_kernel<<<grid_for(n), 256, 0, s>>>(n, a, x, y);
+    axpy_kernel<<<hb::counted(grid_for(n)), 256, 0, s>>>(n, a, x, y);
 }
 
 void symmetrize_lower(cudaStream_t s, int n, double *A, long lda) {
-    symlower_kernel<<<grid_for((long) n * n), 256, 0, s>>>(n, A, lda);
+    symlower_kernel<<<hb::counted(grid_for((long) n * n)), 256, 0, s>>>(n, A, lda);
 }
 
 void symmetrize_avg(cudaStream_t s, int n, double *A, long lda) {
-    symavg_kernel<<<grid_for((long) n * n), 256, 0, s>>>(n, A, lda);
+    symavg_kernel<<<hb::counted(grid_for((long) n * n)), 256, 0, s>>>(n, A, lda);
 }
 
 void add_diag(cudaStream_t s, int n, double *A, long lda, double v) {
-    adddiag_kernel<<<grid_for(n), 256, 0, s>>>(n, A, lda, v);
+    adddiag_kernel<<<hb::counted(grid_for(n)), 256, 0, s>>>(n, A, lda, v);
 }
 
 void add_diag_vec(cudaStream_t s, int n, double *A, long lda, const double *d) {
-    adddiagvec_kernel<<<grid_for(n), 256, 0, s>>>(n, A, lda, d);
+    adddiagvec_kernel<<<hb::counted(grid_for(n)), 256, 0, s>>>(n, A, lda, d);
 }
 
 void copy_matrix(cudaStream_t s, int rows, int cols, const double *A, long lda, double *B, long ldb) {
     if (rows <= 0 || cols <= 0) return;
-    copymat_kernel<<<grid_for((long) rows * cols), 256, 0, s>>>(rows, cols, A, lda, B, ldb);
+    copymat_kernel<<<hb::counted(grid_for((long) rows * cols)), 256, 0, s>>>(rows, cols, A, lda, B, ldb);
 }
 
 void transpose(cudaStream_t s, int n, const double *A, long lda, double *B, long ldb) {
     dim3 grid((n + 31) / 32, (n + 31) / 32), block(32, 8);
-    transpose_kernel<<<grid, block, 0, s>>>(n, A, lda, B, ldb);
+    transpose_kernel<<<hb::counted(grid), block, 0, s>>>(n, A, lda, B, ldb);
 }
 
 void scale_matrix(cudaStream_t s, int rows, int cols, double *A, long lda, double a) {
-    scalemat_kernel<<<grid_for((long) rows * cols), 256, 0, s>>>(rows, cols, A, lda, a);
+    scalemat_kernel<<<hb::counted(grid_for((long) rows * cols)), 256, 0, s>>>(rows, cols, A, lda, a);
 }
 
 void scale_columns(cudaStream_t s, int rows, int cols, const double *A, long lda, const double *d,
                    double *B, long ldb) {
-    scalecols_kernel<<<grid_for((long) rows * cols), 256, 0, s>>>(rows, cols, A, lda, d, B, ldb);
+    scalecols_kernel<<<hb::counted(grid_for((long) rows * cols)), 256, 0, s>>>(rows, cols, A, lda, d, B, ldb);
 }
 
 void frob_dot(cudaStream_t s, int n, const double *A, long lda, const double *B, long ldb, double *d_out) {
     static double *part = nullptr;
     const int np = 296;
     if (!part) HB_CUDA(cudaMalloc(&part, sizeof(double) * np));
-    frob_partial_kernel<<<np, 256, 0, s>>>(n, A, lda, B, ldb, part);
-    sum_partials_kernel<<<1, 512, 0, s>>>(np, part, d_out);
+    frob_partial_kernel<<<hb::counted(np), 256, 0, s>>>(n, A, lda, B, ldb, part);
+    sum_partials_kernel<<<hb::counted(1), 512, 0, s>>>(np, part, d_out);
 }
 
 void trace(cudaStream_t s, int n, const double *A, long lda, double *d_out) {
-    trace_kernel<<<1, 1024, 0, s>>>(n, A, lda, d_out);
+    trace_kernel<<<hb::counted(1), 1024, 0, s>>>(n, A, lda, d_out);
 }
 
 void dot(cudaStream_t s, int n, const double *x, const double *y, double *d_out) {
-    dot_kernel<<<1, 1024, 0, s>>>(n, x, y, d_out);
+    dot_kernel<<<hb::counted(1), 1024, 0, s>>>(n, x, y, d_out);
 }
 
 }  // namespace hb

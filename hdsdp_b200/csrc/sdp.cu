@@ -211,6 +211,18 @@ __global__ void coldot_pair_kernel(int n, int k, const int *id, const double *sg
     if (lane == 0) out[id[a]] = sg[a] * acc;
 }
 
+// out[id_a] = s_a G_aa
+__global__ void r1d_diag_kernel(int k, const int *id, const double *sg, const double *G, long ldg, double *out) {
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a < k) out[id[a]] = sg[a] * G[(size_t) a * (ldg + 1)];
+}
+
+// out[id_a] = s_a v_a
+__global__ void r1d_scatter_kernel(int k, const int *id, const double *sg, const double *v, double *out) {
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a < k) out[id[a]] = sg[a] * v[a];
+}
+
 // <A_a, W^2> for SP: sum_e v_e (r != c ? 2 : 1) * W[:,r].W[:,c]   (warp per constraint)
 __global__ void innersq_sp_kernel(int n, int nsp, const int *id, const int *ptr, const int *rr, const int *cc,
                                   const double *vv, const double *W, long ldw, double *out) {
@@ -260,7 +272,7 @@ void SdpDevice::upload(int n_, int m_, const HostCoeff &C, const std::vector<Hos
     if (!C.r.empty()) {
         int *dr = upload_vec(C.r, s), *dc = upload_vec(C.c, s);
         double *dv = upload_vec(C.v, s);
-        scatter_sym_kernel<<<grid1((long) C.r.size()), 256, 0, s>>>((int) C.r.size(), dr, dc, dv, Cfull, ld);
+        scatter_sym_kernel<<<hb::counted(grid1((long) C.r.size())), 256, 0, s>>>((int) C.r.size(), dr, dc, dv, Cfull, ld);
         HB_CUDA(cudaStreamSynchronize(s));
         cudaFree(dr);
         cudaFree(dc);
@@ -343,6 +355,13 @@ void SdpDevice::upload(int n_, int m_, const HostCoeff &C, const std::vector<Hos
         }
         A1 = upload_vec(hA1, s);
         HB_CUDA(cudaMalloc(&G, sizeof(double) * pad_ld(nr1d) * nr1d));
+        if (precision == 1) {
+            // the factors a_i are fixed: split them once
+            bool ok = opA1.alloc(nr1d, n) && opK.alloc(n, n) && opKT.alloc(n, n) && opB.alloc(nr1d, n);
+            HB_CUDA(cudaMalloc(&colsq, sizeof(double) * nr1d));
+            if (ok) split_from_f64(s, opA1, A1, ld, true);
+            else opA1.release();
+        }
     }
     const int vcols = std::max(std::max(nr1d, nr1s), 1);
     HB_CUDA(cudaMalloc(&V, sizeof(double) * ld * vcols));
@@ -358,7 +377,7 @@ void SdpDevice::upload(int n_, int m_, const HostCoeff &C, const std::vector<Hos
         int *dr = upload_vec(c.r, s), *dc = upload_vec(c.c, s);
         double *dv = upload_vec(c.v, s);
         if (!c.r.empty())
-            scatter_sym_kernel<<<grid1((long) c.r.size()), 256, 0, s>>>((int) c.r.size(), dr, dc, dv, mat, ld);
+            scatter_sym_kernel<<<hb::counted(grid1((long) c.r.size())), 256, 0, s>>>((int) c.r.size(), dr, dc, dv, mat, ld);
         HB_CUDA(cudaStreamSynchronize(s));
         cudaFree(dr);
         cudaFree(dc);
@@ -404,63 +423,100 @@ void SdpDevice::release() {
     for (double *p : dr_mat) f(p);
     dr_mat.clear();
     f(pos_r); f(pos_c); f(pos_ptr); f(ent_j); f(ent_v);
-    f(T1); f(T2); f(vecbuf); f(d_w); f(d_scal);
+    f(T1); f(T2); f(vecbuf); f(d_w); f(d_scal); f(colsq);
+    colsq = nullptr;
+    opA1.release();
+    opK.release();
+    opKT.release();
+    opB.release();
+    split_ready = false;
     if (h_scal) cudaFreeHost(h_scal);
     h_scal = nullptr;
 }
 
 void SdpDevice::assemble(double dC, double dA, const double *d_wvec, double dEye, double *S, long ldS) {
     cudaStream_t s = stream;
-    s_init_kernel<<<grid1((long) n * n), 256, 0, s>>>(n, Cfull, ld, dC, dEye, S, ldS);
+    s_init_kernel<<<hb::counted(grid1((long) n * n)), 256, 0, s>>>(n, Cfull, ld, dC, dEye, S, ldS);
     if (dA != 0.0) {
         if (npos > 0)
-            s_gather_kernel<<<grid1(npos), 256, 0, s>>>(npos, pos_r, pos_c, pos_ptr, ent_j, ent_v, d_wvec, dA, S, ldS);
+            s_gather_kernel<<<hb::counted(grid1(npos)), 256, 0, s>>>(npos, pos_r, pos_c, pos_ptr, ent_j, ent_v, d_wvec, dA, S, ldS);
         if (nr1d > 0) {
-            r1d_weights_kernel<<<grid1(nr1d), 256, 0, s>>>(nr1d, r1d_id, r1d_sign, d_wvec, dA, d_w);
+            r1d_weights_kernel<<<hb::counted(grid1(nr1d)), 256, 0, s>>>(nr1d, r1d_id, r1d_sign, d_wvec, dA, d_w);
             scale_columns(s, n, nr1d, A1, ld, d_w, V, ld);
             gemm(s, n, n, nr1d, 1.0, V, ld, 0, A1, ld, 1, 1.0, S, ldS, 0);
         }
         for (int i = 0; i < ndr; ++i)
-            axpy_mat_devscale_kernel<<<grid1((long) n * n), 256, 0, s>>>(n, dr_mat[i], ld, d_wvec, dr_id[i], dA, S, ldS);
+            axpy_mat_devscale_kernel<<<hb::counted(grid1((long) n * n)), 256, 0, s>>>(n, dr_mat[i], ld, d_wvec, dr_id[i], dA, S, ldS);
     }
     HB_CUDA(cudaGetLastError());
 }
 
-void SdpDevice::schur_matrix(const double *W, long ldW, double *M, long ldM) {
+void SdpDevice::schur_matrix(const double *W, long ldW, double *M, long ldM, const double *Kinv) {
     cudaStream_t s = stream;
+    split_ready = false;
     HB_CUDA(cudaMemsetAsync(M, 0, sizeof(double) * ldM * m, s));
     dim3 blk(32, 8);
+    // compulsory traffic of a gather pair kernel: the lower triangles of W (read) and of its M block (written)
+    const double wbytes = 8.0 * n * (n + 1) / 2;
     if (nsp > 0) {
         dim3 grd((nsp + 31) / 32, (nsp + 7) / 8);
-        schur_spsp_kernel<<<grd, blk, 0, s>>>(nsp, sp_id, sp_ptr, sp_r, sp_c, sp_v, W, ldW, M, ldM);
+        const bool timed = kstat_on(KF_SCHUR_PAIR);
+        if (timed) kstat_begin(KF_SCHUR_PAIR, s, wbytes + 8.0 * nsp * (nsp + 1) / 2);
+        schur_spsp_kernel<<<hb::counted(grd), blk, 0, s>>>(nsp, sp_id, sp_ptr, sp_r, sp_c, sp_v, W, ldW, M, ldM);
+        if (timed) kstat_end(s);
     }
     if (nr1s > 0) {
         dim3 grd((nr1s + 31) / 32, (nr1s + 7) / 8);
-        schur_r1s_kernel<<<grd, blk, 0, s>>>(nr1s, r1s_id, r1s_ptr, r1s_p, r1s_a, r1s_sign, W, ldW, M, ldM);
+        const bool timed = kstat_on(KF_SCHUR_PAIR);
+        if (timed) kstat_begin(KF_SCHUR_PAIR, s, wbytes + 8.0 * nr1s * (nr1s + 1) / 2);
+        schur_r1s_kernel<<<hb::counted(grd), blk, 0, s>>>(nr1s, r1s_id, r1s_ptr, r1s_p, r1s_a, r1s_sign, W, ldW, M, ldM);
+        if (timed) kstat_end(s);
     }
     if (nr1d > 0) {
-        // V = W * A1,  G = A1^T V (lower),  M = (s s^T) o G o G
-        gemm(s, n, nr1d, n, 1.0, W, ldW, 0, A1, ld, 0, 0.0, V, ld, 0);
         const long ldg = pad_ld(nr1d);
-        gemm(s, nr1d, nr1d, n, 1.0, A1, ld, 1, V, ld, 0, 0.0, G, ldg, GEMM_C_LOWER);
+        bool split = false;
+        if (precision == 1 && Kinv && opA1.hi) {
+            // B = L^-1 A1 (split operand), G = B^T B (lower) in BF16x3 with FP32 accumulation
+            split_from_f64(s, opK, Kinv, ld, false);
+            split_from_f64(s, opKT, Kinv, ld, true);
+            SplitGemm g1;
+            g1.M = n;
+            g1.N = nr1d;
+            g1.K = n;
+            g1.a_lower = true;
+            g1.epi = SPLIT_EPI_SPLIT;
+            g1.out = &opB;
+            SplitGemm g2;
+            g2.M = g2.N = nr1d;
+            g2.K = n;
+            g2.lower_tiles = true;
+            g2.C = G;
+            g2.ldc = ldg;
+            split = split_gemm(s, opK, opA1, g1) && split_gemm(s, opB, opB, g2);
+            split_ready = split;
+        }
+        // V = W * A1 (FP64): the whole product when not split, else only for the cross terms
+        if (!split || nr1s > 0 || nsp > 0) gemm(s, n, nr1d, n, 1.0, W, ldW, 0, A1, ld, 0, 0.0, V, ld, 0);
+        // G = A1^T V (lower),  M = (s s^T) o G o G
+        if (!split) gemm(s, nr1d, nr1d, n, 1.0, A1, ld, 1, V, ld, 0, 0.0, G, ldg, GEMM_C_LOWER);
         dim3 grd((nr1d + 31) / 32, (nr1d + 7) / 8);
-        schur_hadamard_kernel<<<grd, blk, 0, s>>>(nr1d, r1d_id, r1d_sign, G, ldg, M, ldM);
+        schur_hadamard_kernel<<<hb::counted(grd), blk, 0, s>>>(nr1d, r1d_id, r1d_sign, G, ldg, M, ldM);
         if (nr1s > 0) {
             dim3 g2((nr1s + 31) / 32, (nr1d + 7) / 8);
-            schur_r1d_r1s_kernel<<<g2, blk, 0, s>>>(nr1d, r1d_id, r1d_sign, V, ld, nr1s, r1s_id, r1s_ptr, r1s_p,
+            schur_r1d_r1s_kernel<<<hb::counted(g2), blk, 0, s>>>(nr1d, r1d_id, r1d_sign, V, ld, nr1s, r1s_id, r1s_ptr, r1s_p,
                                                     r1s_a, r1s_sign, M, ldM);
         }
         if (nsp > 0) {
             dim3 g3((nsp + 31) / 32, (nr1d + 7) / 8);
-            schur_r1_sp_kernel<<<g3, blk, 0, s>>>(nr1d, r1d_id, r1d_sign, V, ld, nsp, sp_id, sp_ptr, sp_r, sp_c,
+            schur_r1_sp_kernel<<<hb::counted(g3), blk, 0, s>>>(nr1d, r1d_id, r1d_sign, V, ld, nsp, sp_id, sp_ptr, sp_r, sp_c,
                                                   sp_v, M, ldM);
         }
     }
     if (nr1s > 0 && nsp > 0) {
         dim3 gv(grid1(n) > 64 ? 64 : grid1(n), nr1s);
-        r1s_build_v_kernel<<<gv, 256, 0, s>>>(n, nr1s, r1s_ptr, r1s_p, r1s_a, W, ldW, Vs, ld);
+        r1s_build_v_kernel<<<hb::counted(gv), 256, 0, s>>>(n, nr1s, r1s_ptr, r1s_p, r1s_a, W, ldW, Vs, ld);
         dim3 g3((nsp + 31) / 32, (nr1s + 7) / 8);
-        schur_r1_sp_kernel<<<g3, blk, 0, s>>>(nr1s, r1s_id, r1s_sign, Vs, ld, nsp, sp_id, sp_ptr, sp_r, sp_c, sp_v,
+        schur_r1_sp_kernel<<<hb::counted(g3), blk, 0, s>>>(nr1s, r1s_id, r1s_sign, Vs, ld, nsp, sp_id, sp_ptr, sp_r, sp_c, sp_v,
                                               M, ldM);
     }
     for (int i = 0; i < ndr; ++i) {
@@ -469,34 +525,55 @@ void SdpDevice::schur_matrix(const double *W, long ldW, double *M, long ldM) {
         gemm(s, n, n, n, 1.0, W, ldW, 0, T1, ld, 0, 0.0, T2, ld, 0);
         symmetrize_avg(s, n, T2, ld);
         inner_all(T2, ld, vecbuf);
-        scatter_row_kernel<<<grid1(m), 256, 0, s>>>(m, dr_id[i], vecbuf, M, ldM);
+        scatter_row_kernel<<<hb::counted(grid1(m)), 256, 0, s>>>(m, dr_id[i], vecbuf, M, ldM);
     }
     HB_CUDA(cudaGetLastError());
 }
 
-void SdpDevice::inner_all(const double *Z, long ldZ, double *out) {
+void SdpDevice::inner_all(const double *Z, long ldZ, double *out, bool reuse_v) {
     cudaStream_t s = stream;
-    if (nsp > 0) inner_sp_kernel<<<grid1(nsp), 256, 0, s>>>(nsp, sp_id, sp_ptr, sp_r, sp_c, sp_v, Z, ldZ, out);
+    if (nsp > 0) inner_sp_kernel<<<hb::counted(grid1(nsp)), 256, 0, s>>>(nsp, sp_id, sp_ptr, sp_r, sp_c, sp_v, Z, ldZ, out);
     if (nr1s > 0)
-        inner_r1s_kernel<<<grid1(nr1s), 256, 0, s>>>(nr1s, r1s_id, r1s_ptr, r1s_p, r1s_a, r1s_sign, Z, ldZ, out);
-    if (nr1d > 0) {
-        gemm(s, n, nr1d, n, 1.0, Z, ldZ, 0, A1, ld, 0, 0.0, Vt, ld, 0);
-        coldot_pair_kernel<<<(nr1d * 32 + 255) / 256, 256, 0, s>>>(n, nr1d, r1d_id, r1d_sign, A1, ld, Vt, ld, out);
+        inner_r1s_kernel<<<hb::counted(grid1(nr1s)), 256, 0, s>>>(nr1s, r1s_id, r1s_ptr, r1s_p, r1s_a, r1s_sign, Z, ldZ, out);
+    if (nr1d > 0 && reuse_v && split_ready) {
+        // <A_i, W> = s_i a_i^T W a_i = s_i G_ii
+        r1d_diag_kernel<<<hb::counted(grid1(nr1d)), 256, 0, s>>>(nr1d, r1d_id, r1d_sign, G, pad_ld(nr1d), out);
+    } else if (nr1d > 0) {
+        if (!reuse_v) gemm(s, n, nr1d, n, 1.0, Z, ldZ, 0, A1, ld, 0, 0.0, Vt, ld, 0);
+        const double *Vz = reuse_v ? V : Vt;
+        coldot_pair_kernel<<<hb::counted((nr1d * 32 + 255) / 256), 256, 0, s>>>(n, nr1d, r1d_id, r1d_sign, A1, ld, Vz, ld, out);
     }
     for (int i = 0; i < ndr; ++i) frob_dot(s, n, dr_mat[i], ld, Z, ldZ, out + dr_id[i]);
     HB_CUDA(cudaGetLastError());
 }
 
-void SdpDevice::inner_all_sq(const double *W, long ldW, double *out) {
+void SdpDevice::inner_all_sq(const double *W, long ldW, double *out, bool reuse_v, bool reuse_vt) {
     cudaStream_t s = stream;
     if (nsp > 0)
-        innersq_sp_kernel<<<(nsp * 32 + 255) / 256, 256, 0, s>>>(n, nsp, sp_id, sp_ptr, sp_r, sp_c, sp_v, W, ldW, out);
+        innersq_sp_kernel<<<hb::counted((nsp * 32 + 255) / 256), 256, 0, s>>>(n, nsp, sp_id, sp_ptr, sp_r, sp_c, sp_v, W, ldW, out);
     if (nr1s > 0)
-        innersq_r1s_kernel<<<(nr1s * 32 + 255) / 256, 256, 0, s>>>(n, nr1s, r1s_id, r1s_ptr, r1s_p, r1s_a, r1s_sign,
+        innersq_r1s_kernel<<<hb::counted((nr1s * 32 + 255) / 256), 256, 0, s>>>(n, nr1s, r1s_id, r1s_ptr, r1s_p, r1s_a, r1s_sign,
                                                                    W, ldW, out);
-    if (nr1d > 0) {
-        gemm(s, n, nr1d, n, 1.0, W, ldW, 0, A1, ld, 0, 0.0, Vt, ld, 0);
-        coldot_pair_kernel<<<(nr1d * 32 + 255) / 256, 256, 0, s>>>(n, nr1d, r1d_id, r1d_sign, Vt, ld, Vt, ld, out);
+    if (nr1d > 0 && reuse_v && split_ready) {
+        // <A_i, W^2> = s_i |W a_i|^2 = s_i |L^-T b_i|^2: column sums of squares of L^-T B
+        HB_CUDA(cudaMemsetAsync(colsq, 0, sizeof(double) * nr1d, s));
+        SplitGemm g;
+        g.M = n;
+        g.N = nr1d;
+        g.K = n;
+        g.epi = SPLIT_EPI_COLSQ;
+        g.colsq = colsq;
+        if (split_gemm(s, opKT, opB, g)) {
+            r1d_scatter_kernel<<<hb::counted(grid1(nr1d)), 256, 0, s>>>(nr1d, r1d_id, r1d_sign, colsq, out);
+        } else {
+            gemm(s, n, nr1d, n, 1.0, W, ldW, 0, A1, ld, 0, 0.0, Vt, ld, 0);
+            coldot_pair_kernel<<<hb::counted((nr1d * 32 + 255) / 256), 256, 0, s>>>(n, nr1d, r1d_id, r1d_sign, Vt, ld,
+                                                                                    Vt, ld, out);
+        }
+    } else if (nr1d > 0) {
+        if (!reuse_v && !reuse_vt) gemm(s, n, nr1d, n, 1.0, W, ldW, 0, A1, ld, 0, 0.0, Vt, ld, 0);
+        const double *Vw = reuse_v ? V : Vt;
+        coldot_pair_kernel<<<hb::counted((nr1d * 32 + 255) / 256), 256, 0, s>>>(n, nr1d, r1d_id, r1d_sign, Vw, ld, Vw, ld, out);
     }
     for (int i = 0; i < ndr; ++i) {
         gemm(s, n, n, n, 1.0, dr_mat[i], ld, 0, W, ldW, 0, 0.0, T1, ld, 0);

@@ -16,6 +16,7 @@
 #include <vector>
 #include <cuda_runtime.h>
 #include "la.h"
+#include "split.h"
 
 namespace hb {
 
@@ -81,6 +82,14 @@ struct SdpDevice {
     double *d_scal = nullptr;  // small scalars
     double *h_scal = nullptr;  // pinned mirror
 
+    // Split precision (BF16x3 on tcgen05) for the dense rank-one Schur block
+    int precision = 0;
+    SplitOperand opA1;        // rows: the nr1d factors a_i, K: n
+    SplitOperand opK, opKT;   // L^-1 and L^-T of the dual slack (rows n, K n)
+    SplitOperand opB;         // B = L^-1 A1 as rows b_i (rows nr1d, K n)
+    bool split_ready = false; // G and opB hold the last split Schur build
+    double *colsq = nullptr;  // nr1d
+
     void upload(int n_, int m_, const HostCoeff &C, const std::vector<HostCoeff> &A, cudaStream_t s);
     void release();
 
@@ -88,11 +97,16 @@ struct SdpDevice {
     void assemble(double dC, double dA, const double *d_wvec, double dEye, double *S, long ldS);
 
     // Schur complement M (m x m, lower triangle written) from symmetric W.
-    void schur_matrix(const double *W, long ldW, double *M, long ldM);
-    // out[j] = <A_j, Z> for all j (Z full symmetric)
-    void inner_all(const double *Z, long ldZ, double *out);
-    // out[j] = <A_j, W^2> for all j
-    void inner_all_sq(const double *W, long ldW, double *out);
+    // With precision 1 and Kinv = L^-1 (W = Kinv^T Kinv) the dense rank-one
+    // block is formed as (B^T B) o (B^T B), B = Kinv A1, in split precision.
+    void schur_matrix(const double *W, long ldW, double *M, long ldM, const double *Kinv = nullptr);
+    // out[j] = <A_j, Z> for all j (Z full symmetric). With reuse_v the dense
+    // rank-one part reads V = Z * A1 left by the last schur_matrix(Z) call;
+    // otherwise it forms Vt = Z * A1 and leaves it for inner_all_sq.
+    void inner_all(const double *Z, long ldZ, double *out, bool reuse_v = false);
+    // out[j] = <A_j, W^2> for all j: reuse_v as above; reuse_vt reads the Vt =
+    // W * A1 left by inner_all(W) just before.
+    void inner_all_sq(const double *W, long ldW, double *out, bool reuse_v = false, bool reuse_vt = false);
     // <C, Z>
     double c_inner(const double *Z, long ldZ);
 };

@@ -1375,6 +1375,7 @@ hdsdp_retcode HDSDPOptimize(hdsdp *h, int dOptOnly) {
     h->timeBegin = wall();
     h->timers = Timers();
     h->log.clear();
+    adjoint_release(h->adj);
     if (!h->usr) return HDSDP_RETCODE_FAILED;
     if (h->cone) {
         h->cone->release();
@@ -1400,9 +1401,24 @@ hdsdp_retcode HDSDPOptimize(hdsdp *h, int dOptOnly) {
                ip(h, INT_PARAM_CORRECTORB), h->bnd.lo, h->bnd.up, h->modelFeatures.c_str());
         printf("\n");
     }
-    retcode = conic_solve(h, dOptOnly);
-    if (h->HStatus != HDSDP_INFEAS_OR_UNBOUNDED && h->HStatus != HDSDP_SUSPECT_INFEAS_OR_UNBOUNDED)
-        retcode = HDSDPCheckSolution(h, h->dErrs);
+    {
+        // Iterations run on the solver stream with the data resident: time them with events there.
+        cudaEvent_t ev0, ev1;
+        HB_CUDA(cudaEventCreate(&ev0));
+        HB_CUDA(cudaEventCreate(&ev1));
+        h->timers.setup = wall() - h->timeBegin;
+        HB_CUDA(cudaEventRecord(ev0, h->stream));
+        retcode = conic_solve(h, dOptOnly);
+        if (h->HStatus != HDSDP_INFEAS_OR_UNBOUNDED && h->HStatus != HDSDP_SUSPECT_INFEAS_OR_UNBOUNDED)
+            retcode = HDSDPCheckSolution(h, h->dErrs);
+        HB_CUDA(cudaEventRecord(ev1, h->stream));
+        HB_CUDA(cudaEventSynchronize(ev1));
+        float ms = 0.f;
+        HB_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
+        h->timers.ipm_device = 1e-3 * ms;
+        cudaEventDestroy(ev0);
+        cudaEventDestroy(ev1);
+    }
     h->optimized = true;
     if (h->verbose)
         printf("DIMACS error metric:\n    %5.2e %5.2e %5.2e %5.2e %5.2e %5.2e \n", h->dErrs[0], h->dErrs[1],
@@ -1446,6 +1462,7 @@ void HDSDPGetConeValues(hdsdp *h, int iCone, double *conePrimal, double *coneDua
 
 void HDSDPClear(hdsdp *h) {
     if (!h) return;
+    adjoint_release(h->adj);
     if (h->cone) {
         h->cone->release();
         delete h->cone;
@@ -1470,4 +1487,7 @@ namespace hb {
 int solver_status(hdsdp *h) { return (int) h->HStatus; }
 int solver_iters(hdsdp *h) { return h->nIterCount; }
 void solver_set_psdp(hdsdp *h, int on) { h->HIntParams[INT_PARAM_PSDP] = on; }
+void solver_cone_values(hdsdp *h, double *X, double *S) { cone_values(h, X, S); }
+double solver_obj_scal(hdsdp *h) { return fd(h, D_OBJSCALING); }
+double solver_rhs_scal(hdsdp *h) { return fd(h, D_RHSSCALING); }
 }  // namespace hb

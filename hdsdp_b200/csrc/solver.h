@@ -39,6 +39,8 @@ struct Timers {
     long n_schur = 0, n_sfactor = 0, n_lanczos = 0, n_lanczos_mv = 0, n_schur_solve = 0;
     // finer split (seconds)
     double lz_inverse = 0, lz_host = 0, lz_wait = 0, sch_matrix = 0, sch_inner = 0, sch_innersq = 0;
+    // presolve + upload (host wall) and the device-timed iterations + final check (CUDA events)
+    double setup = 0, ipm_device = 0;
 };
 
 // Lanczos maximum-step estimator (linalg/hdsdp_lanczos.c:161-292) on the GPU.
@@ -149,6 +151,9 @@ struct KKT {
     hdsdp_retcode solve(const double *rhs, double *lhs);   // host vectors; lhs may alias rhs
 };
 
+struct AdjointState;
+void adjoint_release(AdjointState *&a);
+
 // Per-iteration record for time-to-gap reporting.
 struct IterRecord {
     double t, pobj, dobj, mu, gap;
@@ -192,4 +197,5 @@ struct hdsdp_solver_internal {
     int verbose = 0;
     std::vector<hb::IterRecord> log;
     std::string modelFeatures;
+    hb::AdjointState *adj = nullptr;  // cached adjoint factors of the last solve
 };

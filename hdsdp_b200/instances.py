@@ -137,6 +137,18 @@ def lovasz_theta(n: int = 300, p: float = 0.1, seed: int = 2) -> SDPInstance:
     """Lovasz theta SDP: min <-J, X> s.t. tr(X) = 1, X_ij = 0 for edges ij."""
     rng = np.random.default_rng(seed)
     ei, ej = _erdos_renyi_edges(n, p, rng)
+    inst = lovasz_theta_graph(n, list(zip(ei.tolist(), ej.tolist())))
+    inst.meta["seed"] = seed
+    return inst
+
+
+def lovasz_theta_graph(n: int, edges) -> SDPInstance:
+    """Lovasz theta SDP of a given graph; ``edges`` lists pairs (a, c) with a > c.
+
+    Known answers: theta(C_5) = sqrt(5), theta(K_n) = 1, theta(empty graph on n) = n.
+    """
+    ei = np.array([e[0] for e in edges], dtype=np.int64)
+    ej = np.array([e[1] for e in edges], dtype=np.int64)
     npack = n * (n + 1) // 2
     cols = [(np.arange(npack), -np.ones(npack))]
     cols.append((pack_idx(n, np.arange(n), np.arange(n)), np.ones(n)))
@@ -144,7 +156,7 @@ def lovasz_theta(n: int = 300, p: float = 0.1, seed: int = 2) -> SDPInstance:
         cols.append(([pack_idx(n, a, c)], [1.0]))
     b = np.zeros(1 + ei.size)
     b[0] = 1.0
-    return _assemble("theta", n, cols, b, {"edges": int(ei.size), "seed": seed})
+    return _assemble("theta", n, cols, b, {"edges": int(ei.size)})
 
 
 def rank_one(n: int = 1000, m: int = 2000, density: float = 0.1, seed: int = 3) -> SDPInstance:

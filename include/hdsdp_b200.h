@@ -43,8 +43,37 @@ extern int HDSDPGetIterLog( hdsdp *HSolver, int maxLen, double *t, double *pObj,
    [8] total           [9] #Schur builds       [10] #S factorisations
    [11] #Lanczos runs  [12] #Lanczos matvecs    [13] #Schur solves
    [14] Lanczos: L^-1  [15] Lanczos: host eigen [16] Lanczos: device wait
-   [17] Schur: matrix  [18] Schur: <A_i, W>     [19] Schur: <A_i, W^2> */
-extern void HDSDPGetTimers( hdsdp *HSolver, double out[20] );
+   [17] Schur: matrix  [18] Schur: <A_i, W>     [19] Schur: <A_i, W^2>
+   [20] presolve + upload of the data (host wall clock)
+   [21] iterations + final DIMACS check, CUDA events on the solver stream */
+extern void HDSDPGetTimers( hdsdp *HSolver, double out[22] );
+
+/* Number of kernel launches this library has issued in the process so far
+   (all solvers and entry points). No reference counterpart. */
+extern long long hdsdpb_launch_count( void );
+
+/* Live kernel timing by family (no reference counterpart): bit f of `mask`
+   enables family f = 0 FP64 GEMM, 1 Cholesky (cooperative potrf),
+   2 triangular inverse, 3 Schur gather pair kernels. While enabled, each launch
+   of the family is bracketed by CUDA events on its own stream; enabling resets
+   the totals. hdsdpb_kstat_read returns the launches, the summed event time in
+   ms and the summed algorithmic work (flops for 0-2, compulsory bytes for 3). */
+extern int hdsdpb_kstat_enable( int mask );
+extern int hdsdpb_kstat_read( int family, long long *launches, double *ms, double *work );
+
+/* Vector-Jacobian product of the solution map of the last HDSDPOptimize
+   (no reference counterpart). gy (m) and GX (n x n, column-major,
+   symmetric) are the gradients of a loss with respect to y* and X*; either
+   may be NULL (zero). Writes the gradient with respect to b into gb (m),
+   with respect to C as a full symmetric n x n matrix into gC, and with
+   respect to every stored value of the cone's CSC data (columns 0..m, the
+   user's Ap[m+1] entries) into gAx; outputs may be NULL. Computed by
+   implicit differentiation of the optimality conditions at the final
+   iterate in the Nesterov-Todd scaling; the first call after a solve builds
+   and factors the scaled Schur matrix, later calls reuse it. The user's CSC
+   arrays must still be alive. Returns HDSDP_RETCODE_OK or HDSDP_RETCODE_FAILED. */
+extern hdsdp_retcode HDSDPAdjoint( hdsdp *HSolver, const double *gy, const double *GX, double *gb,
+                                   double *gC, double *gAx );
 
 /* ---- Kernel-level entry points (host buffers in, host buffers out) ---------------- */
 
@@ -80,6 +109,14 @@ extern int hdsdpb_inverse( int n, const double *S, double *Sinv );
    column-major host buffers (op = transpose when trans != 0). */
 extern int hdsdpb_gemm( int M, int N, int K, double alpha, const double *A, int lda, int transA,
                         const double *B, int ldb, int transB, double beta, double *C, int ldc );
+
+/* Split-precision product on the tcgen05 tensor cores: C = op(A) op(B) with
+   every FP64 operand split into BF16 hi + lo parts and the three products
+   hi*hi + hi*lo + lo*hi accumulated in FP32 (relative error about 2^-16 of
+   sum |a||b|). Column-major host buffers. Returns 0 on success, 2 if the
+   tensor-core path could not be set up, -1 on error. */
+extern int hdsdpb_split_gemm( int M, int N, int K, const double *A, int lda, int transA,
+                              const double *B, int ldb, int transB, double *C, int ldc );
 
 /* Device-resident timing of one kernel family on an n x n problem (CUDA events
    on the launching stream, 2 warm-up calls): 0 GEMM NN, 1 GEMM TN lower,

@@ -140,14 +140,15 @@ def solve(inst, want_x: bool = True, params: dict | None = None, quiet: bool = T
         L.HDSDPCheckSolution(h, _dp(errs))
         out["errs"] = errs
         out["status_after_check"] = int(L.oracle_status(h))
+        L.HUserDataDestroy(C.byref(ud))
+        L.HDSDPDestroy(C.byref(h))  # prints its closing line
     finally:
         if quiet:
             import sys
             sys.stdout.flush()
+            C.CDLL(None).fflush(None)  # C stdio buffers of the reference's log
             os.dup2(saved, 1)
             os.close(saved)
-    L.HUserDataDestroy(C.byref(ud))
-    L.HDSDPDestroy(C.byref(h))
     return out
 
 
@@ -172,6 +173,7 @@ def schur_probe(inst, y, resi, type_kkt: int = 0):
         r = L.oracle_schur_probe(m, n, _ip(Ap), _ip(Ai), _dp(Ax), _dp(y), float(resi), int(type_kkt),
                                  _dp(M), _dp(asinv), _dp(asinvrd), _dp(asinvcs), _dp(scal))
     finally:
+        C.CDLL(None).fflush(None)
         os.dup2(saved, 1)
         os.close(saved)
     if r != 0:
@@ -199,6 +201,7 @@ def ratio_probe(inst, y, resi, dy, ada):
         r = L.oracle_ratio_probe(inst.m, inst.n, _ip(Ap), _ip(Ai), _dp(Ax), _dp(y), float(resi),
                                  _dp(dy), float(ada), C.byref(step), C.byref(logdet))
     finally:
+        C.CDLL(None).fflush(None)
         os.dup2(saved, 1)
         os.close(saved)
     if r != 0:

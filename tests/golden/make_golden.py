@@ -1,0 +1,102 @@
+"""Generate the golden fixtures of tests/ by running the compiled reference.
+
+    make -C oracle && python tests/golden/make_golden.py [--full]
+
+Writes tests/golden/golden.json (solver results and probe outputs) and
+tests/golden/golden_arrays.npz (Schur matrices, dual vectors). The inputs are
+the seeded instances of hdsdp_b200/instances.py, so the same arrays are
+regenerated bit-for-bit wherever the tests run. --full also solves the
+full-size Lovasz-theta (n=300) and rank-one (n=1000, m=2000) workloads
+(about two minutes of CPU time with the reference).
+"""
+from __future__ import annotations
+
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from hdsdp_b200 import instances  # noqa: E402
+from oracle import ref_api  # noqa: E402
+
+# Small cases that the parity tests solve on every run.
+SMALL = {
+    "maxcut60": lambda: instances.maxcut(60, 0.1, seed=11),
+    "maxcut200": lambda: instances.maxcut(200, 0.05, seed=1),
+    "theta40": lambda: instances.lovasz_theta(40, 0.2, seed=3),
+    "rank1_50_80": lambda: instances.rank_one(50, 80, 0.2, seed=4),
+    "theta_adj40": lambda: instances.theta_adjoint(40, 0.2, 0.3, seed=2),
+}
+FULL = {
+    "theta_n300": lambda: instances.WORKLOADS["theta_n300"](),
+    "rank1_n1000_m2000": lambda: instances.WORKLOADS["rank1_n1000_m2000"](),
+}
+
+
+def probe_point(inst, seed=0):
+    rng = np.random.default_rng(seed)
+    y = -np.abs(rng.standard_normal(inst.m)) * 0.1
+    resi = -(inst.n + 10.0)
+    dy = rng.standard_normal(inst.m)
+    return y, resi, dy
+
+
+def main(full: bool):
+    out = {"solves": {}, "probes": {}}
+    arrays = {}
+    cases = dict(SMALL)
+    if full:
+        cases.update(FULL)
+    for name, make in cases.items():
+        inst = make()
+        for psdp in (0, 1):
+            r = ref_api.solve(inst, want_x=False, params={4: psdp})
+            key = "%s/psdp%d" % (name, psdp)
+            out["solves"][key] = {
+                "n": inst.n, "m": inst.m, "retcode": r["retcode"], "iters": r["iters"],
+                "status": r["status_after_check"], "pobj": r["pobj"], "dobj": r["dobj"],
+                "errs": [float(e) for e in r["errs"]], "time_s": r["time"],
+            }
+            arrays["y/" + key] = r["y"]
+            print(key, out["solves"][key]["iters"], out["solves"][key]["status"], r["pobj"], r["dobj"], flush=True)
+        if name in SMALL:
+            y, resi, dy = probe_point(inst)
+            sp = ref_api.schur_probe(inst, y, resi)
+            step, logdet = ref_api.ratio_probe(inst, y, resi, dy, 0.5)
+            out["probes"][name] = {"resi": resi, "tracesinv": sp["tracesinv"], "step": step, "logdet": logdet}
+            arrays["M/" + name] = np.tril(sp["M"])
+            arrays["asinv/" + name] = sp["asinv"]
+            arrays["asinvrd/" + name] = sp["asinvrd"]
+    # known answers of the Lovasz theta number, solved by the reference
+    ka = {}
+    for label, inst, value in [
+        ("theta_C5", instances.lovasz_theta_graph(5, [(1, 0), (2, 1), (3, 2), (4, 3), (4, 0)]), np.sqrt(5.0)),
+        ("theta_K6", instances.lovasz_theta_graph(6, [(i, j) for i in range(6) for j in range(i)]), 1.0),
+        ("theta_empty7", instances.lovasz_theta_graph(7, []), 7.0),
+    ]:
+        r = ref_api.solve(inst, want_x=False, params={4: 0})
+        ka[label] = {"theta": value, "ref_dobj": r["dobj"], "ref_status": r["status_after_check"]}
+        print(label, value, r["dobj"], flush=True)
+    out["known_answers"] = ka
+    if not full:
+        old = os.path.join(HERE, "golden.json")
+        if os.path.exists(old):
+            prev = json.load(open(old))
+            for k, v in prev.get("solves", {}).items():
+                if k.split("/")[0] in FULL:
+                    out["solves"][k] = v
+            prevarr = np.load(os.path.join(HERE, "golden_arrays.npz"))
+            for k in prevarr.files:
+                if k.split("/")[1] in FULL:
+                    arrays[k] = prevarr[k]
+    json.dump(out, open(os.path.join(HERE, "golden.json"), "w"), indent=1, sort_keys=True)
+    np.savez_compressed(os.path.join(HERE, "golden_arrays.npz"), **arrays)
+
+
+if __name__ == "__main__":
+    main("--full" in sys.argv)

@@ -1,0 +1,110 @@
+"""The oracle against the reference's golden vectors (CPU only).
+
+The NumPy restatement (oracle/kernels_ref.py) is pinned against Schur
+complements, inner-product vectors, log-determinants and Lanczos step bounds
+dumped from the compiled reference (tests/golden/make_golden.py), and the
+reference's solver results are checked for the properties the parity tests
+rely on.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from hdsdp_b200 import instances
+from make_golden import SMALL, probe_point
+from oracle import kernels_ref as K
+from oracle import ref_api
+
+
+@pytest.fixture(scope="module", params=sorted(SMALL))
+def case(request):
+    inst = SMALL[request.param]()
+    C, A = K.dense_data(inst)
+    return request.param, inst, C, A
+
+
+def test_schur_restatement_matches_reference(case, golden, golden_arrays):
+    name, inst, C, A = case
+    y, resi, _ = probe_point(inst)
+    r = K.schur(C, A, y, resi)
+    M = golden_arrays["M/" + name]
+    scale = np.abs(M).max()
+    assert np.abs(np.tril(r["M"]) - M).max() <= 1e-12 * scale
+    for key in ("asinv", "asinvrd"):
+        g = golden_arrays[key + "/" + name]
+        assert np.abs(r[key] - g).max() <= 1e-12 * max(1.0, np.abs(g).max())
+    assert r["tracesinv"] == pytest.approx(golden["probes"][name]["tracesinv"], rel=1e-12)
+
+
+def test_logdet_and_step_bound(case, golden):
+    name, inst, C, A = case
+    y, resi, dy = probe_point(inst)
+    p = golden["probes"][name]
+    S = K.dual_slack(C, A, y, 1.0, -1.0, -resi)
+    assert K.log_det(S) == pytest.approx(p["logdet"], rel=1e-12, abs=1e-10)
+    # the reference's Lanczos bound never exceeds the exact step and is within 1e-3 of it
+    dS = K.dual_slack(C, A, dy, 0.0, -1.0, 0.5 * resi)
+    exact = K.max_step(S, dS)
+    assert p["step"] <= exact * (1 + 1e-10)
+    assert p["step"] >= exact * (1 - 1e-3)
+
+
+@pytest.mark.parametrize("key", ["maxcut60/psdp0", "maxcut200/psdp0", "theta40/psdp0",
+                                 "rank1_50_80/psdp0", "theta_adj40/psdp0"])
+def test_reference_solution_is_dual_feasible(key, golden, golden_arrays):
+    inst = SMALL[key.split("/")[0]]()
+    C, A = K.dense_data(inst)
+    y = golden_arrays["y/" + key]
+    sol = golden["solves"][key]
+    assert sol["status"] == 3  # PRIMAL_DUAL_OPTIMAL
+    assert inst.b @ y == pytest.approx(sol["dobj"], rel=1e-12)
+    assert np.linalg.eigvalsh(K.dual_slack(C, A, y))[0] > -1e-8
+    assert abs(sol["pobj"] - sol["dobj"]) <= 1e-6 * (1 + abs(sol["dobj"]))
+
+
+def test_known_answers(golden):
+    for label, rec in golden["known_answers"].items():
+        assert rec["ref_status"] == 3, label
+        # min <-J, X>: the optimal value is -theta
+        assert -rec["ref_dobj"] == pytest.approx(rec["theta"], rel=1e-8), label
+
+
+def test_full_size_reference_results(golden):
+    for key, iters in (("theta_n300/psdp0", 30), ("rank1_n1000_m2000/psdp0", 53)):
+        sol = golden["solves"][key]
+        assert sol["status"] == 3 and sol["iters"] == iters
+
+
+@pytest.mark.skipif(not ref_api.available(), reason="oracle/_ref not built (make -C oracle)")
+def test_reference_reproduces_fixture(golden, golden_arrays):
+    inst = SMALL["maxcut60"]()
+    r = ref_api.solve(inst, want_x=False, params={4: 0})
+    sol = golden["solves"]["maxcut60/psdp0"]
+    assert r["iters"] == sol["iters"] and r["status_after_check"] == sol["status"]
+    assert r["dobj"] == pytest.approx(sol["dobj"], rel=1e-12)
+    np.testing.assert_allclose(r["y"], golden_arrays["y/maxcut60/psdp0"], rtol=1e-9, atol=1e-12)
+
+
+def test_pack_unpack_round_trip():
+    n = 7
+    rng = np.random.default_rng(0)
+    X = rng.standard_normal((n, n))
+    X = X + X.T
+    ii, jj = np.tril_indices(n)
+    rows = instances.pack_idx(n, ii, jj)
+    assert sorted(rows.tolist()) == list(range(n * (n + 1) // 2))
+    np.testing.assert_array_equal(K.unpack_column(n, rows, X[ii, jj]), X)
+
+
+def test_workload_shapes():
+    t = instances.WORKLOADS["theta_n300"]()
+    assert (t.n, t.m) == (300, 4577)
+    r = instances.WORKLOADS["rank1_n1000_m2000"]()
+    assert (r.n, r.m) == (1000, 2000)
+    mc = instances.maxcut(8000, seed=4, n_edges=40000, weights=(0.5, 1.5))
+    assert (mc.n, mc.m) == (8000, 8000) and mc.meta["edges"] == 40000
+    # seeded generators are deterministic
+    a, b = instances.rank_one(50, 80, 0.2, seed=4), instances.rank_one(50, 80, 0.2, seed=4)
+    np.testing.assert_array_equal(a.Ax, b.Ax)
+    np.testing.assert_array_equal(a.b, b.b)

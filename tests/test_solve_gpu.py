@@ -1,0 +1,90 @@
+"""Full IPM solves on the GPU against the compiled reference's results.
+
+Parity bar: same status, iteration count within 2, objectives within 1e-6
+relative, DIMACS primal/dual infeasibility within 1e-7 where the reference
+reaches PRIMAL_DUAL_OPTIMAL.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from hdsdp_b200 import api, instances
+from make_golden import FULL, SMALL
+from oracle import kernels_ref as K
+
+pytestmark = pytest.mark.gpu
+
+OPTIMAL = 3
+
+
+def check_parity(r, ref):
+    assert r["status_after_check"] == ref["status"]
+    assert abs(r["iters"] - ref["iters"]) <= 2, (r["iters"], ref["iters"])
+    assert r["dobj"] == pytest.approx(ref["dobj"], rel=1e-6, abs=1e-8)
+    assert r["pobj"] == pytest.approx(ref["pobj"], rel=1e-6, abs=1e-8)
+    if ref["status"] == OPTIMAL:
+        assert r["errs"][0] <= max(1e-7, 10 * ref["errs"][0])
+        assert r["errs"][1] <= 1e-7 and r["errs"][2] <= 1e-7 and r["errs"][3] <= 1e-7
+
+
+@pytest.mark.parametrize("psdp", [0, 1])
+@pytest.mark.parametrize("name", sorted(SMALL))
+def test_small_solve_parity(gpu_lib, name, psdp, golden):
+    inst = SMALL[name]()
+    r = api.solve(inst, want_x=False, primal_refinement=bool(psdp))
+    check_parity(r, golden["solves"]["%s/psdp%d" % (name, psdp)])
+
+
+@pytest.mark.parametrize("name", sorted(FULL))
+def test_full_size_parity(gpu_lib, name, golden):
+    inst = FULL[name]()
+    r = api.solve(inst, want_x=False, primal_refinement=False)
+    check_parity(r, golden["solves"]["%s/psdp0" % name])
+
+
+def test_full_size_with_primal_refinement(gpu_lib, golden):
+    inst = FULL["theta_n300"]()
+    r = api.solve(inst, want_x=False, primal_refinement=True)
+    check_parity(r, golden["solves"]["theta_n300/psdp1"])
+
+
+def test_known_answers(gpu_lib, golden):
+    graphs = {
+        "theta_C5": instances.lovasz_theta_graph(5, [(1, 0), (2, 1), (3, 2), (4, 3), (4, 0)]),
+        "theta_K6": instances.lovasz_theta_graph(6, [(i, j) for i in range(6) for j in range(i)]),
+        "theta_empty7": instances.lovasz_theta_graph(7, []),
+    }
+    for label, inst in graphs.items():
+        r = api.solve(inst, want_x=False, primal_refinement=False)
+        assert r["status_after_check"] == OPTIMAL, label
+        assert -r["dobj"] == pytest.approx(golden["known_answers"][label]["theta"], rel=1e-7), label
+
+
+def test_primal_dual_recovery(gpu_lib):
+    """X and S returned by HDSDPGetConeValues satisfy the optimality conditions."""
+    inst = SMALL["theta40"]()
+    r = api.solve(inst, want_x=True, primal_refinement=False)
+    C, A = K.dense_data(inst)
+    X, S = r["X"], r["S"]
+    np.testing.assert_allclose(S, K.dual_slack(C, A, r["y"]), atol=1e-9)
+    e = K.dimacs(C, A, inst.b, X, S, r["y"])
+    assert e[0] <= 1e-7 and e[1] <= 1e-7
+    assert abs(e[2]) <= 1e-6 and abs(e[3]) <= 1e-6
+    assert np.sum(C * X) == pytest.approx(r["pobj"], rel=1e-7)
+
+
+@pytest.mark.slow
+def test_maxcut_n8000_properties(gpu_lib):
+    """MaxCut n=8000 (40000 edges): optimal with a tight duality gap, diag(X) = 1."""
+    inst = instances.WORKLOADS["maxcut_n8000"]()
+    r = api.solve(inst, want_x=False, primal_refinement=False)
+    assert r["status_after_check"] == OPTIMAL
+    assert abs(r["pobj"] - r["dobj"]) <= 1e-6 * (1 + abs(r["dobj"]))
+    assert r["errs"][0] <= 1e-7
+    # the SDP bound lies between half the total edge weight and the total edge weight;
+    # C = -L/4 so the total weight is -2 trace(C)
+    rows, vals = inst.column(0)
+    i, j = K.packed_to_ij(inst.n, rows)
+    total = -2.0 * np.asarray(vals)[i == j].sum()
+    assert 0.5 * total <= -r["dobj"] <= total
