@@ -57,7 +57,7 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="rank1_n1000_m2000")
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "split"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "split", "adaptive"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -244,7 +244,7 @@ def run_b200(args):
 
     L = _lib.load()
     inst = instances.WORKLOADS[args.workload]()
-    precision = 1 if args.precision == "split" else 0
+    precision = {"fp64": 0, "split": 1, "adaptive": 2}[args.precision]
 
     # pinned host copies of the step's inputs
     def pinned(a, dtype):

@@ -46,6 +46,10 @@ class Solver:
         return self.L.HDSDPInit(self.h, n_rows, n_cones)
 
     def set_cone(self, m: int, n: int, Ap, Ai, Ax):
+        if len(Ap) != m + 2:
+            raise ValueError("Ap must hold m + 2 column pointers (column 0 is C), got %d for m = %d" % (len(Ap), m))
+        if len(Ai) < Ap[-1] or len(Ax) < Ap[-1]:
+            raise ValueError("Ai / Ax shorter than Ap[m + 1]")
         Ap = np.ascontiguousarray(Ap, dtype=np.int32)
         Ai = np.ascontiguousarray(Ai, dtype=np.int32)
         Ax = np.ascontiguousarray(Ax, dtype=np.float64)
@@ -110,12 +114,12 @@ class Solver:
         return arr
 
     def timers(self):
-        t = np.zeros(22)
+        t = np.zeros(23)
         self.L.HDSDPGetTimers(self.h, _dp(t))
         keys = ["schur", "schur_factor", "schur_solve", "s_factor", "s_inverse", "lanczos", "assemble",
                 "primal", "total", "n_schur", "n_sfactor", "n_lanczos", "n_lanczos_mv", "n_schur_solve",
                 "lz_inverse", "lz_host", "lz_wait", "sch_matrix", "sch_inner", "sch_innersq", "setup",
-                "ipm_device"]
+                "ipm_device", "n_factor_reuse"]
         return dict(zip(keys, t.tolist()))
 
     def adjoint(self, gy=None, GX=None, want_gC=True):

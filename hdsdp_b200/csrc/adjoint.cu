@@ -104,16 +104,19 @@ double host_scalar(cudaStream_t s, const double *d, double *h) {
     return *h;
 }
 
-// v = M^-1 u with the explicit inverse factor K (M = L L^T, K = L^-1), one refinement step.
+// v = M^-1 u with the explicit inverse factor K (M = L L^T, K = L^-1) and two steps of
+// iterative refinement (M is ill-conditioned in the directions of the optimal face).
 void schur_solve(cudaStream_t s, AdjointState &a, const double *u, double *v) {
     const int m = a.m;
     coldot(s, m, m, a.FM.KT, a.ldm, u, a.d_t, 1.0, 0.0, 2);   // t = K u
     coldot(s, m, m, a.FM.K, a.ldm, a.d_t, v, 1.0, 0.0, 1);    // v = K^T t
-    coldot(s, m, m, a.M, a.ldm, v, a.d_r, -1.0, 0.0, 0);      // r = -M v
-    axpy(s, m, 1.0, u, a.d_r);                               // r = u - M v
-    coldot(s, m, m, a.FM.KT, a.ldm, a.d_r, a.d_t, 1.0, 0.0, 2);
-    coldot(s, m, m, a.FM.K, a.ldm, a.d_t, a.d_r, 1.0, 0.0, 1);
-    axpy(s, m, 1.0, a.d_r, v);
+    for (int it = 0; it < 2; ++it) {
+        coldot(s, m, m, a.M, a.ldm, v, a.d_r, -1.0, 0.0, 0);  // r = -M v
+        axpy(s, m, 1.0, u, a.d_r);                           // r = u - M v
+        coldot(s, m, m, a.FM.KT, a.ldm, a.d_r, a.d_t, 1.0, 0.0, 2);
+        coldot(s, m, m, a.FM.K, a.ldm, a.d_t, a.d_r, 1.0, 0.0, 1);
+        axpy(s, m, 1.0, a.d_r, v);
+    }
 }
 
 hdsdp_retcode prepare(hdsdp *h, AdjointState &a) {
@@ -162,12 +165,14 @@ hdsdp_retcode prepare(hdsdp *h, AdjointState &a) {
     scale_matrix(s, n, n, a.Y, ld, 1.0 / cnorm);
     double *Yk = a.Y, *Yn = a.T1;
     bool converged = false;
-    for (int it = 0; it < 100 && !converged; ++it) {
+    int polish = 2;  // quadratic convergence: two more steps reach the rounding level
+    for (int it = 0; it < 100 && polish > 0; ++it) {
+        if (converged) --polish;
         gemm(s, n, n, n, 1.0, Yk, ld, 0, Yk, ld, 0, 0.0, a.P, ld, 0);                 // P = Y^2
         ns_step_kernel<<<hb::counted(grid_for((long) n * n)), 256, 0, s>>>(n, a.P, ld, a.N);  // T = 1.5 I - 0.5 P
         gemm(s, n, n, n, 1.0, Yk, ld, 0, a.N, ld, 0, 0.0, Yn, ld, 0);                 // Y <- Y T
         std::swap(Yk, Yn);
-        if (it % 4 == 3) {
+        if (!converged && it % 4 == 3) {
             add_diag(s, n, a.P, ld, -1.0);
             frob_dot(s, n, a.P, ld, a.P, ld, a.d_scal);
             converged = std::sqrt(host_scalar(s, a.d_scal, a.h_scal)) < 1e-12 * std::sqrt((double) n);

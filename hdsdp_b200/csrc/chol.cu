@@ -19,6 +19,25 @@ namespace cg = cooperative_groups;
 
 namespace hb {
 
+#ifdef HB_CHOL_STAMPS
+// Diagnostic build only (never defined in the library build): per-phase %globaltimer
+// stamps of the cooperative factorisation, written by thread 0 of a block.
+__device__ unsigned long long *g_chol_stamps = nullptr;
+void chol_set_stamps(unsigned long long *p) { cudaMemcpyToSymbol(g_chol_stamps, &p, sizeof(p)); }
+#define CHOL_STAMP(slot)                                                  \
+    do {                                                                  \
+        if (threadIdx.x == 0 && g_chol_stamps && (slot) < 8192) {         \
+            unsigned long long t_;                                        \
+            asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t_));        \
+            g_chol_stamps[(slot)] = t_;                                   \
+        }                                                                 \
+    } while (0)
+#else
+#define CHOL_STAMP(slot) \
+    do {                 \
+    } while (0)
+#endif
+
 namespace {
 constexpr int NB = 64;
 
@@ -42,152 +61,179 @@ __device__ __forceinline__ void dmma_c(double &d0, double &d1, double a, double 
 }
 
 
-// Inverse of the 64 x 64 lower-triangular T (pitch TP, entries beyond nb padded with the
-// identity) into Ti, in shared memory: four warps invert the 16 x 16 diagonal blocks in
-// registers, then off-diagonal blocks follow in three block-parallel stages
-// Ti_ij = -Ti_ii * sum_{k=j}^{i-1} T_ik Ti_kj.
-__device__ void trinv64_dev(double *T, double *Ti, double *Pt, int nb) {
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    for (int r = nb + tid; r < 64; r += blockDim.x) T[r + r * TP] = 1.0;
-    __syncthreads();
-    if (warp < 4 && lane < 16) {
-        const int b0 = warp * 16, c = lane;
-        double x[16];
+// ---------------------------------------------------------------------------------
+// Diagonal-block factorisation: four 16-column sub-panels. Warp 0 factors and inverts
+// each 16 x 16 pivot block in registers (lane r holds row r; shuffles broadcast the
+// pivot and the column); the panel below, the trailing update and the off-diagonal
+// blocks of the 64 x 64 inverse are DMMA products in shared memory with all warps.
+// ---------------------------------------------------------------------------------
+constexpr unsigned FULL = 0xffffffffu;
+
+// Factor T[off.., off..] (16 x 16, lower, pitch TP) in place and write its inverse to
+// X[off.., off..]. Executed by one whole warp (lanes 16-31 carry zeros).
+__device__ __forceinline__ bool warp_chol_inv16(double *T, double *X, int off, int lane) {
+    const bool act = lane < 16;
+    double d[16];
 #pragma unroll
-        for (int r = 0; r < 16; ++r) {
-            if (r < c) x[r] = 0.0;
-            else if (r == c) x[r] = 1.0 / T[(b0 + r) + (b0 + r) * TP];
-            else {
-                double acc = 0.0;
+    for (int q = 0; q < 16; ++q) d[q] = (act && q <= lane) ? T[(off + lane) + (off + q) * TP] : 0.0;
+    bool bad = false;
+    double rinv = 1.0;  // lane c: 1 / L_cc
 #pragma unroll
-                for (int k = 0; k < 16; ++k)
-                    if (k >= c && k < r) acc += T[(b0 + r) + (b0 + k) * TP] * x[k];
-                x[r] = -acc / T[(b0 + r) + (b0 + r) * TP];
+    for (int c = 0; c < 16; ++c) {
+        // one reciprocal square root per column: L_cc = d rsqrt(d), the column below scales by rsqrt(d)
+        const double dc = __shfl_sync(FULL, d[c], c);
+        if (!(dc > 0.0)) bad = true;
+        const double rs = rsqrt(dc);
+        if (lane == c) {
+            d[c] = dc * rs;
+            rinv = rs;
+        } else if (lane > c) {
+            d[c] *= rs;
+        }
+        // fixed trip counts keep d[] in registers (the loops unroll completely)
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+            if (q > c) {
+                const double lqc = __shfl_sync(FULL, d[c], q);
+                if (lane >= q) d[q] -= d[c] * lqc;
             }
         }
-#pragma unroll
-        for (int r = 0; r < 16; ++r) Ti[(b0 + r) + (b0 + c) * TP] = x[r];
     }
-    for (int idx = tid; idx < 64 * 64; idx += blockDim.x) {
-        const int r = idx & 63, c = idx >> 6;
-        if ((r >> 4) < (c >> 4)) Ti[r + c * TP] = 0.0;
+    if (act) {
+#pragma unroll
+        for (int q = 0; q < 16; ++q)
+            if (q <= lane) T[(off + lane) + (off + q) * TP] = d[q];
     }
-    __syncthreads();
-    for (int d = 1; d < 4; ++d) {
-        const int nblk = 4 - d;
-        for (int e = tid; e < nblk * 256; e += blockDim.x) {
-            const int j = e >> 8, i = j + d, rr = (e & 255) >> 4, cc = e & 15;
-            double acc = 0.0;
-            for (int k = j; k < i; ++k)
+    // column `lane` of L^-1 by forward substitution; L_rk broadcast from lane r
+    double x[16];
 #pragma unroll
-                for (int t = 0; t < 16; ++t) acc += T[(16 * i + rr) + (16 * k + t) * TP] * Ti[(16 * k + t) + (16 * j + cc) * TP];
-            Pt[(j << 8) + (rr << 4) + cc] = acc;
-        }
-        __syncthreads();
-        for (int e = tid; e < nblk * 256; e += blockDim.x) {
-            const int j = e >> 8, i = j + d, rr = (e & 255) >> 4, cc = e & 15;
-            double acc = 0.0;
+    for (int r = 0; r < 16; ++r) {
+        const double ir = __shfl_sync(FULL, rinv, r);
+        double acc = (r == lane) ? 1.0 : 0.0;
 #pragma unroll
-            for (int t = 0; t < 16; ++t) acc += Ti[(16 * i + rr) + (16 * i + t) * TP] * Pt[(j << 8) + (t << 4) + cc];
-            Ti[(16 * i + rr) + (16 * j + cc) * TP] = -acc;
+        for (int k = 0; k < 16; ++k)
+            if (k < r) acc -= __shfl_sync(FULL, d[k], r) * x[k];
+        x[r] = (r >= lane) ? acc * ir : 0.0;
+    }
+    if (act) {
+#pragma unroll
+        for (int r = 0; r < 16; ++r) X[(off + r) + (off + lane) * TP] = x[r];
+    }
+    return !bad;
+}
+
+// C (rows x cols, multiples of 8) = / += alpha * A (rows x K) * op(B), K a multiple of 4,
+// in shared memory (pitch TP) on the DMMA path; 8 x 8 tiles dealt to the warps starting
+// at warp `w0`. A(r, k) = Ab[r + k*TP]; op(B)(k, c) = bt ? Bb[c + k*TP] : Bb[k + c*TP].
+// With lower set, tiles strictly above the diagonal are skipped.
+__device__ __forceinline__ void smem_mma(double *Cb, const double *Ab, const double *Bb, int bt, int rows, int cols,
+                                         int K, double alpha, bool accumulate, bool lower) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int tr = rows >> 3, ntile = tr * (cols >> 3);
+    for (int t = w; t < ntile; t += nw) {
+        const int ti = t % tr, tj = t / tr;
+        if (lower && ti < tj) continue;
+        double c0 = 0.0, c1 = 0.0;
+        for (int k0 = 0; k0 < K; k0 += 4) {
+            const int kk = k0 + (lane & 3);
+            const double av = Ab[(ti * 8 + (lane >> 2)) + kk * TP];
+            const int cc = tj * 8 + (lane >> 2);
+            const double bv = bt ? Bb[cc + kk * TP] : Bb[kk + cc * TP];
+            dmma_c(c0, c1, av, bv);
         }
-        __syncthreads();
+        const int r = ti * 8 + (lane >> 2), c = tj * 8 + (lane & 3) * 2;
+        if (accumulate) {
+            Cb[r + c * TP] += alpha * c0;
+            Cb[r + (c + 1) * TP] += alpha * c1;
+        } else {
+            Cb[r + c * TP] = alpha * c0;
+            Cb[r + (c + 1) * TP] = alpha * c1;
+        }
     }
 }
 
-// Factor the nb x nb diagonal block at (j0, j0) in place. Executed by one block:
-// four 16-column sub-panels; warp 0 factors each 16 x 16 pivot block in registers
-// (shuffles), the block solves the rows below it and updates the trailing part.
-// Returns false (and sets *info) on a failed pivot.
-__device__ bool potf2_dev(double *L, long ld, int j0, int nb, double *Dinv, long ldd, int *info, double *sm) {
-    double *T = sm;  // T[r + c*TP]
+// Factor the nb x nb diagonal block at (j0, j0) and write its inverse to Dinv (64
+// columns, zero padded). With Pp set, the block is first updated in shared memory by
+// the previous panel's rows: A_jj -= Pp Pp^T (Pp: nb x 64, pitch ldp). Executed by one
+// block. Returns false (and sets *info) on a failed pivot.
+__device__ bool potf2_dev(double *L, long ld, int j0, int nb, double *Dinv, long ldd, int *info, double *sm,
+                          const double *Pp = nullptr, long ldp = 0) {
+    double *T = sm, *X = sm + 64 * TP, *P = sm + 128 * TP;
     __shared__ int fail;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    for (int idx = tid; idx < 64 * nb; idx += blockDim.x) {
+    for (int idx = tid; idx < 64 * 64; idx += blockDim.x) {
         const int r = idx & 63, c = idx >> 6;
-        const bool ok = r < nb && r >= c;
+        const bool ok = r < nb && c < nb && r >= c;
         cpa8(&T[r + c * TP], ok ? L + (size_t) (j0 + r) + (size_t) (j0 + c) * ld : L, ok);
+        if (Pp) {
+            const bool okp = r < nb;
+            cpa8(&P[r + c * TP], okp ? Pp + (size_t) r + (size_t) c * ldp : Pp, okp);
+        }
+        X[r + c * TP] = 0.0;
     }
     cpa_wait_all();
     if (tid == 0) fail = 0;
     __syncthreads();
-    for (int s0 = 0; s0 < nb; s0 += 16) {
-        const int sb = min(16, nb - s0);
-        if (warp == 0) {
-            // lane r < sb holds row s0 + r of the pivot block
-            double d[16];
-#pragma unroll
-            for (int q = 0; q < 16; ++q) d[q] = (lane < sb && q <= lane) ? T[(s0 + lane) + (s0 + q) * TP] : 0.0;
-            bool bad = false;
-#pragma unroll
-            for (int c = 0; c < 16; ++c) {
-                if (c < sb) {
-                    const double dc = __shfl_sync(0xffffffffu, d[c], c);
-                    if (!(dc > 0.0)) bad = true;
-                    const double pv = sqrt(dc), ip = 1.0 / pv;
-                    if (lane == c) d[c] = pv;
-                    else if (lane > c) d[c] *= ip;
-#pragma unroll
-                    for (int q = c + 1; q < 16; ++q) {
-                        const double lqc = __shfl_sync(0xffffffffu, d[c], q);
-                        if (lane >= q) d[q] -= d[c] * lqc;
-                    }
-                }
-            }
-            if (lane == 0 && bad) {
-                // locate the first failing pivot column (sequential re-check on the host side is not
-                // needed: report the sub-panel start like a failed dpotrf)
-                fail = s0 + 1;
-            }
-#pragma unroll
-            for (int q = 0; q < 16; ++q)
-                if (lane < sb && q <= lane) T[(s0 + lane) + (s0 + q) * TP] = d[q];
-        }
-        __syncthreads();
-        if (fail) break;
-        // rows below the pivot block inside this 64-block: x . D^T = t  (forward substitution)
-        const int r = s0 + sb + tid;
-        if (tid < 64 && r < nb) {
-#pragma unroll 4
-            for (int c = 0; c < sb; ++c) {
-                double x = T[r + (s0 + c) * TP];
-                for (int k = 0; k < c; ++k) x -= T[r + (s0 + k) * TP] * T[(s0 + c) + (s0 + k) * TP];
-                T[r + (s0 + c) * TP] = x * (1.0 / T[(s0 + c) + (s0 + c) * TP]);
-            }
-        }
-        __syncthreads();
-        // trailing update of the rest of the 64-block with this 16-column sub-panel
-        {
-            const int base = s0 + sb, rem = nb - base;
-            const int rr = base + (tid & 63);
-            if ((tid & 63) < rem) {
-                for (int q = base + (tid >> 6); q <= rr; q += 4) {
-                    double acc = 0.0;
-#pragma unroll 4
-                    for (int k = 0; k < sb; ++k) acc += T[rr + (s0 + k) * TP] * T[q + (s0 + k) * TP];
-                    T[rr + q * TP] -= acc;
-                }
-            }
-        }
+    if (Pp) {
+        smem_mma(T, P, P, 1, 64, 64, 64, -1.0, true, true);
         __syncthreads();
     }
+    for (int r = nb + tid; r < 64; r += blockDim.x) T[r + r * TP] = 1.0;  // pad with the identity
     __syncthreads();
+    const int sb = 4096 + (j0 / 64) * 32;
+    CHOL_STAMP(sb);
+    for (int s0 = 0; s0 < 64; s0 += 16) {
+        if (warp == 0) {
+            const bool ok = warp_chol_inv16(T, X, s0, lane);
+            if (lane == 0 && !ok) fail = s0 + 1;
+        }
+        __syncthreads();
+        CHOL_STAMP(sb + 1 + (s0 >> 4) * 2);
+        if (fail) break;
+        const int rem = 64 - s0 - 16;
+        if (rem > 0) {
+            // panel below: P = T_below X_ss^T; then T22 -= P P^T and the panel into T
+            smem_mma(P + s0 + 16, T + (s0 + 16) + s0 * TP, X + s0 + s0 * TP, 1, rem, 16, 16, 1.0, false, false);
+            __syncthreads();
+            smem_mma(T + (s0 + 16) + (s0 + 16) * TP, P + s0 + 16, P + s0 + 16, 1, rem, rem, 16, -1.0, true, true);
+            for (int idx = tid; idx < rem * 16; idx += blockDim.x) {
+                const int r = s0 + 16 + idx % rem, c = idx / rem;
+                T[r + (s0 + c) * TP] = P[r + c * TP];
+            }
+            __syncthreads();
+        }
+        CHOL_STAMP(sb + 2 + (s0 >> 4) * 2);
+    }
     if (fail) {
         if (tid == 0) *info = j0 + fail;
         return false;
     }
+    // off-diagonal 16 x 16 blocks of the inverse: X_ij = -X_ii sum_{k=j}^{i-1} L_ik X_kj
+    for (int d = 1; d < 4; ++d) {
+        for (int j = 0; j + d < 4; ++j) {
+            const int i = j + d;
+            smem_mma(P + 16 * j, T + 16 * i + 16 * j * TP, X + 16 * j + 16 * j * TP, 0, 16, 16, 16 * d, 1.0, false,
+                     false);
+        }
+        __syncthreads();
+        for (int j = 0; j + d < 4; ++j) {
+            const int i = j + d;
+            smem_mma(X + 16 * i + 16 * j * TP, X + 16 * i + 16 * i * TP, P + 16 * j, 0, 16, 16, 16, -1.0, false,
+                     false);
+        }
+        __syncthreads();
+    }
+    CHOL_STAMP(sb + 10);
     for (int idx = tid; idx < nb * nb; idx += blockDim.x) {
         const int r = idx % nb, cc = idx / nb;
         if (r >= cc) L[(size_t) (j0 + r) + (size_t) (j0 + cc) * ld] = T[r + cc * TP];
     }
-    __syncthreads();
-    trinv64_dev(T, sm + 64 * TP, sm + 128 * TP, nb);
-    const double *Ti = sm + 64 * TP;
     for (int idx = tid; idx < NB * NB; idx += blockDim.x) {
         const int r = idx & 63, cc = idx >> 6;
-        if (r < nb) Dinv[(size_t) (j0 + r) + (size_t) cc * ldd] = (cc < nb) ? Ti[r + cc * TP] : 0.0;
+        if (r < nb) Dinv[(size_t) (j0 + r) + (size_t) cc * ldd] = (cc < nb && r >= cc) ? X[r + cc * TP] : 0.0;
     }
     __syncthreads();
+    CHOL_STAMP(sb + 11);
     return true;
 }
 
@@ -267,7 +313,7 @@ __device__ __forceinline__ void tri_index(long t, int &ti, int &tj) {
 // Right-looking blocked Cholesky with one-panel look-ahead: in the update phase of
 // panel j, block 0 first updates the diagonal tile of panel j+1 and factors it while
 // the other blocks update the rest of the trailing matrix.
-__global__ void __launch_bounds__(COOP_THREADS) potrf_coop_kernel(double *L, long ld, int n, double *Dinv,
+__global__ void __launch_bounds__(COOP_THREADS, 2) potrf_coop_kernel(double *L, long ld, int n, double *Dinv,
                                                                   long ldd, int *info) {
     cg::grid_group grid = cg::this_grid();
     extern __shared__ double sm[];
@@ -280,18 +326,22 @@ __global__ void __launch_bounds__(COOP_THREADS) potrf_coop_kernel(double *L, lon
         if (rows <= 0) break;
         double *P = L + (size_t) (j0 + nb) + (size_t) j0 * ld;
         const int nchunk = (rows + 63) / 64;
+        const int pb = (j0 / 64) * 16 + (blockIdx.x == 1 ? 8 : 0);
+        if (blockIdx.x <= 1) CHOL_STAMP(pb + 0);
         for (int ch = blockIdx.x; ch < nchunk; ch += gridDim.x) {
             const int mr = min(64, rows - ch * 64);
             tile_mma_dev(P + ch * 64, ld, mr, nb, P + ch * 64, ld, mr, Dinv + j0, ldd, 1, nb, nb, false, 1, sm);
         }
+        if (blockIdx.x <= 1) CHOL_STAMP(pb + 1);
         grid.sync();
+        if (blockIdx.x <= 1) CHOL_STAMP(pb + 2);
         const long ntile = (long) nchunk * (nchunk + 1) / 2;
         double *A22 = L + (size_t) (j0 + nb) + (size_t) (j0 + nb) * ld;
         if (blockIdx.x == 0) {
-            // tile (0, 0) is the next diagonal block: update it, then factor it
-            const int mr = min(64, rows);
-            tile_mma_dev(A22, ld, mr, mr, P, ld, mr, P, ld, 1, mr, nb, true, 0, sm);
-            potf2_dev(L, ld, j0 + nb, min(NB, rows), Dinv, ldd, info, sm);
+            // tile (0, 0) is the next diagonal block: update it in shared memory and factor it
+            CHOL_STAMP(pb + 3);
+            potf2_dev(L, ld, j0 + nb, min(NB, rows), Dinv, ldd, info, sm, P, ld);
+            CHOL_STAMP(pb + 4);
         }
         // remaining tiles, spread over the other blocks (block 0 joins when the grid has one block)
         const int nworker = (gridDim.x > 1) ? (int) gridDim.x - 1 : 1;
@@ -305,7 +355,9 @@ __global__ void __launch_bounds__(COOP_THREADS) potrf_coop_kernel(double *L, lon
                              P + tj * 64, ld, 1, nc, nb, ti == tj, 0, sm);
             }
         }
+        if (blockIdx.x == 1) CHOL_STAMP(pb + 3);
         grid.sync();
+        if (blockIdx.x <= 1) CHOL_STAMP(pb + 5);
     }
 }
 

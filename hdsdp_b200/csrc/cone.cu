@@ -336,10 +336,39 @@ void SdpCone::update_buffer(double dC, double dAs, const double *y, double dEye,
     double t0 = wall();
     double *target = (which == BUFFER_DUALVAR) ? Svar : (which == BUFFER_DUALCHECK) ? Scheck : dS;
     if (which != BUFFER_DUALSTEP) dEye += dualPerturb;
+    if (which != BUFFER_DUALSTEP) {
+        SlackSig &sig = (which == BUFFER_DUALVAR) ? sigVar : sigCheck;
+        SlackSig next;
+        next.valid = true;
+        next.dC = dC;
+        next.dAs = dAs;
+        next.dEye = dEye;
+        next.y.assign(y, y + m);
+        if (sig.same(next)) {
+            if (tm) tm->assemble += wall() - t0;
+            return;  // the buffer already holds exactly this matrix
+        }
+        sig = std::move(next);
+    }
     std::memcpy(h_vec, y, sizeof(double) * m);
     HB_CUDA(cudaMemcpyAsync(d_y, h_vec, sizeof(double) * m, cudaMemcpyHostToDevice, s));
     dev.assemble(dC, dAs, d_y, dEye, target, ld);
     if (tm) tm->assemble += wall() - t0;
+}
+
+static void copy_factor(cudaStream_t s, DenseFactor &dst, const DenseFactor &src) {
+    HB_CUDA(cudaMemcpyAsync(dst.L, src.L, sizeof(double) * src.ld * src.n, cudaMemcpyDeviceToDevice, s));
+    HB_CUDA(cudaMemcpyAsync(dst.Dinv, src.Dinv, sizeof(double) * src.ld * 64, cudaMemcpyDeviceToDevice, s));
+    dst.k_valid = false;
+    if (src.k_valid && src.K && src.KT) {
+        if (!dst.K) HB_CUDA(cudaMalloc(&dst.K, sizeof(double) * dst.ld * dst.n));
+        if (!dst.KT) HB_CUDA(cudaMalloc(&dst.KT, sizeof(double) * dst.ld * dst.n));
+        HB_CUDA(cudaMemcpyAsync(dst.K, src.K, sizeof(double) * src.ld * src.n, cudaMemcpyDeviceToDevice, s));
+        HB_CUDA(cudaMemcpyAsync(dst.KT, src.KT, sizeof(double) * src.ld * src.n, cudaMemcpyDeviceToDevice, s));
+        dst.k_valid = true;
+    }
+    dst.factored = true;
+    dst.ok = src.ok;
 }
 
 hdsdp_retcode SdpCone::update(double tau, const double *y) {
@@ -354,6 +383,31 @@ static bool timed_factor(cudaStream_t s, DenseFactor &F, const double *S, long l
         tm->s_factor += wall() - t0;
         tm->n_sfactor += 1;
     }
+    return ok;
+}
+
+bool SdpCone::factor_buffer(int which) {
+    const bool var = (which == BUFFER_DUALVAR);
+    DenseFactor &F = var ? Fvar : Fcheck;
+    const SlackSig &sig = var ? sigVar : sigCheck;
+    SlackSig &fsig = var ? facVar : facCheck;
+    bool &fok = var ? facVarOk : facCheckOk;
+    const SlackSig &osig = var ? facCheck : facVar;
+    const bool ook = var ? facCheckOk : facVarOk;
+    if (sig.same(fsig)) {
+        ++nFactorReuse;
+        return fok;
+    }
+    if (sig.same(osig) && ook) {
+        copy_factor(s, F, var ? Fcheck : Fvar);
+        fsig = sig;
+        fok = true;
+        ++nFactorReuse;
+        return true;
+    }
+    const bool ok = timed_factor(s, F, var ? Svar : Scheck, ld, tm);
+    fsig = sig;
+    fok = ok;
     return ok;
 }
 
@@ -374,15 +428,14 @@ hdsdp_retcode SdpCone::ratio_test(double dtau, const double *dy, double ada, int
 
 hdsdp_retcode SdpCone::interior_check(double tau, const double *y, int *interior) {
     update(tau, y);
-    *interior = timed_factor(s, Fvar, Svar, ld, tm) ? 1 : 0;
+    *interior = factor_buffer(BUFFER_DUALVAR) ? 1 : 0;
     return device_error_flag() ? HDSDP_RETCODE_FAILED : HDSDP_RETCODE_OK;
 }
 
 hdsdp_retcode SdpCone::interior_check_expert(double dC, double dAs, const double *y, double dEye, int which,
                                              int *interior) {
     update_buffer(dC, dAs, y, dEye, which);
-    if (which == BUFFER_DUALVAR) *interior = timed_factor(s, Fvar, Svar, ld, tm) ? 1 : 0;
-    else *interior = timed_factor(s, Fcheck, Scheck, ld, tm) ? 1 : 0;
+    *interior = factor_buffer(which == BUFFER_DUALVAR ? BUFFER_DUALVAR : BUFFER_DUALCHECK) ? 1 : 0;
     return device_error_flag() ? HDSDP_RETCODE_FAILED : HDSDP_RETCODE_OK;
 }
 
@@ -390,7 +443,7 @@ hdsdp_retcode SdpCone::get_barrier(double tau, const double *y, int which, doubl
     DenseFactor &F = (which == BUFFER_DUALVAR) ? Fvar : Fcheck;
     if (y) {
         update(tau, y);
-        if (!timed_factor(s, Fvar, Svar, ld, tm)) return HDSDP_RETCODE_FAILED;
+        if (!factor_buffer(BUFFER_DUALVAR)) return HDSDP_RETCODE_FAILED;
     }
     log_diag_sum(s, F, d_scal);
     HB_CUDA(cudaMemcpyAsync(h_scal, d_scal, sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -402,11 +455,17 @@ hdsdp_retcode SdpCone::get_barrier(double tau, const double *y, int which, doubl
 hdsdp_retcode SdpCone::add_step_and_check(double step, int which, int *interior) {
     if (which == BUFFER_DUALVAR) {
         axpy(s, (int) (ld * n), step, dS, Svar);
-        *interior = timed_factor(s, Fvar, Svar, ld, tm) ? 1 : 0;
+        sigVar.valid = false;
+        facVar.valid = false;
+        facVarOk = timed_factor(s, Fvar, Svar, ld, tm);
+        *interior = facVarOk ? 1 : 0;
     } else {
         HB_CUDA(cudaMemcpyAsync(Scheck, Svar, sizeof(double) * ld * n, cudaMemcpyDeviceToDevice, s));
         axpy(s, (int) (ld * n), step, dS, Scheck);
-        *interior = timed_factor(s, Fcheck, Scheck, ld, tm) ? 1 : 0;
+        sigCheck.valid = false;
+        facCheck.valid = false;
+        facCheckOk = timed_factor(s, Fcheck, Scheck, ld, tm);
+        *interior = facCheckOk ? 1 : 0;
     }
     return device_error_flag() ? HDSDP_RETCODE_FAILED : HDSDP_RETCODE_OK;
 }

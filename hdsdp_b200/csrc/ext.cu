@@ -31,12 +31,13 @@ int HDSDPGetIterLog(hdsdp *h, int maxLen, double *t, double *pObj, double *dObj,
     return n;
 }
 
-void HDSDPGetTimers(hdsdp *h, double out[22]) {
+void HDSDPGetTimers(hdsdp *h, double out[23]) {
     const Timers &t = h->timers;
-    const double v[22] = {t.schur, t.schur_factor, t.schur_solve, t.s_factor, t.s_inverse, t.lanczos, t.assemble,
+    const double v[23] = {t.schur, t.schur_factor, t.schur_solve, t.s_factor, t.s_inverse, t.lanczos, t.assemble,
                           t.primal, t.total, (double) t.n_schur, (double) t.n_sfactor, (double) t.n_lanczos,
                           (double) t.n_lanczos_mv, (double) t.n_schur_solve, t.lz_inverse, t.lz_host, t.lz_wait,
-                          t.sch_matrix, t.sch_inner, t.sch_innersq, t.setup, t.ipm_device};
+                          t.sch_matrix, t.sch_inner, t.sch_innersq, t.setup, t.ipm_device,
+                          h->cone ? (double) h->cone->nFactorReuse : 0.0};
     std::memcpy(out, v, sizeof(v));
 }
 

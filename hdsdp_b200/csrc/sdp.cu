@@ -355,7 +355,7 @@ void SdpDevice::upload(int n_, int m_, const HostCoeff &C, const std::vector<Hos
         }
         A1 = upload_vec(hA1, s);
         HB_CUDA(cudaMalloc(&G, sizeof(double) * pad_ld(nr1d) * nr1d));
-        if (precision == 1) {
+        if (precision >= 1) {
             // the factors a_i are fixed: split them once
             bool ok = opA1.alloc(nr1d, n) && opK.alloc(n, n) && opKT.alloc(n, n) && opB.alloc(nr1d, n);
             HB_CUDA(cudaMalloc(&colsq, sizeof(double) * nr1d));

@@ -82,7 +82,8 @@ struct SdpDevice {
     double *d_scal = nullptr;  // small scalars
     double *h_scal = nullptr;  // pinned mirror
 
-    // Split precision (BF16x3 on tcgen05) for the dense rank-one Schur block
+    // Split precision (BF16x3 on tcgen05) for the dense rank-one Schur block:
+    // 0 FP64; 1 split for every build (set per build by the solver's policy)
     int precision = 0;
     SplitOperand opA1;        // rows: the nr1d factors a_i, K: n
     SplitOperand opK, opKT;   // L^-1 and L^-T of the dual slack (rows n, K n)

@@ -290,6 +290,20 @@ void print_log(hdsdp *h, int method) {
            (method == METHOD_HSD) ? HDSDP_INFINITY : h->pObjVal, h->dObjVal, infv, h->mu, h->dStep, third, elapsed);
 }
 
+// Arithmetic of the next full Schur build: mode 0 FP64; 1 split precision
+// throughout; 2 split precision while the relative gap is above 1e-3 (or not
+// yet defined), FP64 for the final iterations.
+void schur_precision(hdsdp *h) {
+    int p = 0;
+    if (h->precision == 1) {
+        p = 1;
+    } else if (h->precision == 2) {
+        const double gap = h->log.empty() ? HDSDP_INFINITY : std::fabs(h->log.back().gap);
+        p = (std::isfinite(gap) && gap < 1e-3) ? 0 : 1;
+    }
+    h->cone->dev.precision = p;
+}
+
 hdsdp_retcode check_interior(hdsdp *h, double tau, const double *y, int *interior) {
     (void) tau;
     hdsdp_retcode r = h->cone->interior_check(1.0, y, interior);
@@ -399,6 +413,7 @@ hdsdp_retcode phaseA_hsd(hdsdp *h, int dOnly) {
             retcode = HDSDP_RETCODE_FAILED;
             goto exit_cleanup;
         }
+        schur_precision(h);
         CALL(h->kkt.build(*h->cone, KKT_TYPE_HOMOGENEOUS));
         h->kkt.regularize(0.0);
         h->d2 = h->kkt.asinv;
@@ -675,6 +690,7 @@ hdsdp_retcode phaseA_infeasible(hdsdp *h, int dOnly) {
                 goto exit_cleanup;
             }
         }
+        schur_precision(h);
         CALL(h->kkt.build(*h->cone, KKT_TYPE_INFEASIBLE));
         h->kkt.add_bound(h->bnd, KKT_TYPE_INFEASIBLE);
         h->d2 = h->kkt.asinv;
@@ -982,6 +998,7 @@ hdsdp_retcode phaseB_potential(hdsdp *h) {
     while (true) {
         nIterInternal += 1;
         if (nIterInternal > 10) force = 0;
+        schur_precision(h);
         CALL(h->kkt.build(*h->cone, KKT_TYPE_INFEASIBLE));
         h->kkt.add_bound(h->bnd, KKT_TYPE_INFEASIBLE);
         if (h->mu > 1.0) h->kkt.regularize(1e-06);
@@ -1176,6 +1193,7 @@ exit_cleanup:
 double min_eig_estimate(hdsdp *h, double *X) {
     SdpCone &c = *h->cone;
     DenseFactor &F = c.Fcheck;
+    c.invalidate_check_factor();
     if (factorize(c.s, F, X, c.ld)) return 1.0;
     double lo = 0.0, hi = 1.0;
     double *T = c.dev.T1;

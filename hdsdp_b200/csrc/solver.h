@@ -61,6 +61,18 @@ struct Lanczos {
     hdsdp_retcode solve(DenseFactor &F, const double *D, long ldD, double *maxStep, Timers *tm);
 };
 
+// Inputs that produced a dual-slack buffer (dC*C + dAs*sum y_i A_i + dEye*I); a
+// factorisation of a buffer rebuilt from identical inputs is reused, which gives
+// bit-identical results because the factor kernels are deterministic.
+struct SlackSig {
+    bool valid = false;
+    double dC = 0, dAs = 0, dEye = 0;
+    std::vector<double> y;
+    bool same(const SlackSig &o) const {
+        return valid && o.valid && dC == o.dC && dAs == o.dAs && dEye == o.dEye && y == o.y;
+    }
+};
+
 // Dense SDP cone on the device (interface/hdsdp_conic_sdp.c dense half).
 struct SdpCone {
     int n = 0, m = 0;
@@ -74,6 +86,14 @@ struct SdpCone {
     int stats[5] = {0, 0, 0, 0, 0};
     double *Svar = nullptr, *Scheck = nullptr, *dS = nullptr, *W = nullptr;
     DenseFactor Fvar, Fcheck;
+    SlackSig sigVar, sigCheck;   // inputs of the current Svar / Scheck contents
+    SlackSig facVar, facCheck;   // inputs of the matrices factored in Fvar / Fcheck
+    bool facVarOk = false, facCheckOk = false;
+    long nFactorReuse = 0;
+    // Factor the buffer `which` (Svar into Fvar, Scheck into Fcheck), reusing a
+    // factor of the same inputs held by either factor object.
+    bool factor_buffer(int which);
+    void invalidate_check_factor() { facCheck.valid = false; }
     Lanczos lz;
     double dualResidual = 0.0, dualPerturb = 0.0;
     double *d_y = nullptr;       // device copy of the current coefficient vector

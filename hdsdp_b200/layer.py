@@ -23,8 +23,7 @@ class SDPLayer(torch.autograd.Function):
 
     @staticmethod
     def forward(ctx, Ax, b, Ap, Ai, n):
-        L = _lib.load()
-        m = len(Ap) - 1
+        m = len(Ap) - 2  # CSC column pointer of columns 0 (C) .. m (A_m)
         ax = np.ascontiguousarray(Ax.detach().cpu().numpy(), dtype=np.float64)
         bv = np.ascontiguousarray(b.detach().cpu().numpy(), dtype=np.float64)
         s = Solver()

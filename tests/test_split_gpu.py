@@ -40,3 +40,18 @@ def test_split_gemm_wide_dynamic_range(gpu_lib):
     ref = A @ B
     bound = np.abs(A) @ np.abs(B)
     assert np.all(np.abs(out - ref) <= 6e-5 * bound)
+
+
+def test_split_schur_rank_one(gpu_lib):
+    """Rank-one Schur block in split precision (B = L^-1 A1, G = B^T B) against the FP64 build."""
+    from hdsdp_b200 import instances
+    inst = instances.WORKLOADS["rank1_n1000_m2000"]()
+    rng = np.random.default_rng(7)
+    y = -np.abs(rng.standard_normal(inst.m)) * 1e-3
+    resi = -2.0
+    ref = api.schur_probe(inst, y, resi, precision=0)
+    spl = api.schur_probe(inst, y, resi, precision=1)
+    scale = np.abs(ref["M"]).max()
+    assert np.abs(spl["M"] - ref["M"]).max() <= 1e-4 * scale
+    np.testing.assert_allclose(spl["asinv"], ref["asinv"], rtol=1e-4)
+    np.testing.assert_allclose(spl["asinvrd"], ref["asinvrd"], rtol=1e-4)
