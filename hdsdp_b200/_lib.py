@@ -21,7 +21,7 @@ EXPORTS = [
     "HUserDataDestroy",
     "HDSDPGetStatus", "HDSDPGetIterCount", "HDSDPSetPrimalRefinement", "HDSDPSetPrecision",
     "HDSDPGetIterLog", "HDSDPGetTimers", "HDSDPAdjoint",
-    "hdsdpb_schur_probe", "hdsdpb_ratio_probe", "hdsdpb_cholesky", "hdsdpb_inverse", "hdsdpb_gemm",
+    "hdsdpb_schur_probe", "hdsdpb_ratio_probe", "hdsdpb_cholesky", "hdsdpb_cholesky_noalloc", "hdsdpb_inverse", "hdsdpb_gemm",
     "hdsdpb_kernel_timing", "hdsdpb_gridsync_probe", "hdsdpb_launch_count",
     "hdsdpb_kstat_enable", "hdsdpb_kstat_read", "hdsdpb_split_gemm",
 ]
@@ -67,6 +67,7 @@ def load():
         "hdsdpb_schur_probe": ([i, i, ip, ip, dp, dp, d, i, dp, dp, dp, dp], i),
         "hdsdpb_ratio_probe": ([i, i, ip, ip, dp, dp, d, dp, d, dp, dp], i),
         "hdsdpb_cholesky": ([i, dp, dp, dp], i),
+        "hdsdpb_cholesky_noalloc": ([i, dp, dp, dp], i),
         "hdsdpb_inverse": ([i, dp, dp], i),
         "hdsdpb_gemm": ([i, i, i, d, dp, i, i, dp, i, i, d, dp, i], i),
         "hdsdpb_kernel_timing": ([i, i, i, dp], i),

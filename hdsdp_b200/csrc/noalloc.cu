@@ -1,0 +1,94 @@
+// Allocation-free variant of the Cholesky entry point (no reference counterpart).
+//
+// hdsdpb_cholesky_noalloc factors an n x n matrix (n <= HDSDPB_NOALLOC_MAX_N) exactly
+// like hdsdpb_cholesky, but every device buffer it touches lives in one file-scope
+// __device__ array: nothing is allocated or freed per call, on the device or the host,
+// and no stream is created (work runs on the legacy default stream).
+//
+// Scratch layout (doubles, ld = 256): S copy [ld * 256] | L [ld * 256] |
+// diagonal-block inverses [ld * 64] | log-det slot [1] | info word [1 int].
+// Nothing has to start at zero: the factorisation clears the info word itself and
+// only the lower triangle of L (rows < n) is ever read back.
+//
+// The first call on a device looks up the array's device address with
+// cudaGetSymbolAddress (with that device current) and caches it, so that call should
+// come before any stream capture. All calls share the one array: calls that overlap
+// (from several host threads, or interleaved on several streams) race.
+#include "la.h"
+#include "../../include/hdsdp_b200.h"
+#include <cstdio>
+
+namespace hb {
+namespace {
+
+constexpr int kMaxN = HDSDPB_NOALLOC_MAX_N;
+constexpr long kLd = kMaxN;  // pad_ld(256) = 256
+constexpr size_t kMatDoubles = (size_t) kLd * kMaxN;
+constexpr size_t kScratchDoubles = 2 * kMatDoubles + (size_t) kLd * 64 + 2;
+
+__device__ __align__(256) double g_noalloc_scratch[kScratchDoubles];
+
+constexpr int kMaxDevices = 64;
+double *g_scratch_ptr[kMaxDevices] = {nullptr};
+
+double *scratch_for_current_device() {
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return nullptr;
+    if (!g_scratch_ptr[dev]) {
+        void *p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        g_scratch_ptr[dev] = (double *) p;
+    }
+    return g_scratch_ptr[dev];
+}
+
+}  // namespace
+}  // namespace hb
+
+using namespace hb;
+
+extern "C" int hdsdpb_cholesky_noalloc(int n, const double *S, double *L, double *logdiag) {
+    if (n < 0 || (n > 0 && !S)) return -1;
+    if (n > kMaxN) {
+        fprintf(stderr, "[hdsdp_b200] hdsdpb_cholesky_noalloc: n = %d exceeds the static scratch limit %d\n", n,
+                kMaxN);
+        return -2;
+    }
+    if (n == 0) {
+        if (logdiag) *logdiag = 0.0;
+        return 0;
+    }
+    double *base = scratch_for_current_device();
+    if (!base) return -1;
+    const long ld = pad_ld(n);
+    DenseFactor F;  // views into the scratch array (never alloc()/release()d)
+    int h_info = 0;
+    F.n = n;
+    F.ld = ld;
+    F.L = base + kMatDoubles;
+    F.Dinv = base + 2 * kMatDoubles;
+    F.d_info = (int *) (base + 2 * kMatDoubles + (size_t) kLd * 64 + 1);
+    F.h_info = &h_info;
+    double *dS = base, *dl = base + 2 * kMatDoubles + (size_t) kLd * 64;
+    cudaStream_t s = 0;
+    if (cudaMemcpy2D(dS, sizeof(double) * ld, S, sizeof(double) * n, sizeof(double) * n, n,
+                     cudaMemcpyHostToDevice) != cudaSuccess)
+        return -1;
+    const bool ok = factorize(s, F, dS, ld);
+    if (ok) {
+        log_diag_sum(s, F, dl);
+        if (logdiag && cudaMemcpy(logdiag, dl, sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
+        if (L) {
+            if (cudaMemcpy2D(L, sizeof(double) * n, F.L, sizeof(double) * ld, sizeof(double) * n, n,
+                             cudaMemcpyDeviceToHost) != cudaSuccess)
+                return -1;
+            for (int j = 0; j < n; ++j)
+                for (int i = 0; i < j; ++i) L[(size_t) j * n + i] = 0.0;
+        }
+    }
+    if (cudaDeviceSynchronize() != cudaSuccess || device_error_flag()) return -1;
+    return ok ? 0 : 1;
+}

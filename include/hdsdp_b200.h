@@ -102,6 +102,16 @@ extern int hdsdpb_ratio_probe( int m, int n, const int *Ap, const int *Ai, const
    upper part zero) and sum(log L_ii). Returns 0 if positive definite, 1 if not. */
 extern int hdsdpb_cholesky( int n, const double *S, double *L, double *logdiag );
 
+/* Allocation-free variant of hdsdpb_cholesky (no reference counterpart): same
+   arguments and return values, but all device scratch is one static device array
+   sized for n <= HDSDPB_NOALLOC_MAX_N, located once per device with
+   cudaGetSymbolAddress; nothing is allocated or freed per call. Returns -2 (with a
+   message on stderr) when n exceeds the limit. The first call on a device does the
+   set-up and should come before any stream capture; overlapping calls share the
+   scratch and race. */
+#define HDSDPB_NOALLOC_MAX_N 256
+extern int hdsdpb_cholesky_noalloc( int n, const double *S, double *L, double *logdiag );
+
 /* Inverse of a symmetric positive definite n x n matrix through its Cholesky
    factor (the reference's dpotri use, linalg/hdsdp_linsolver.c:647-669).
    Returns 0 on success, 1 if not positive definite. */
