@@ -69,6 +69,19 @@ __global__ void s_gather_kernel(int npos, const int *pr, const int *pc, const in
     }
 }
 
+// Same as s_gather_kernel over the rank-one gather map (64-bit entry offsets).
+__global__ void s_gather2_kernel(int npos, const int *pr, const int *pc, const long long *ptr, const int *ej,
+                                 const double *ev, const double *w, double dA, double *S, long lds) {
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npos; p += gridDim.x * blockDim.x) {
+        double acc = 0.0;
+        for (long long e = ptr[p]; e < ptr[p + 1]; ++e) acc += ev[e] * w[ej[e]];
+        acc *= dA;
+        const int r = pr[p], c = pc[p];
+        S[(size_t) r + (size_t) c * lds] += acc;
+        if (r != c) S[(size_t) c + (size_t) r * lds] += acc;
+    }
+}
+
 __global__ void r1d_weights_kernel(int k, const int *id, const double *sign, const double *w, double dA, double *d) {
     for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < k; a += gridDim.x * blockDim.x) d[a] = dA * sign[a] * w[id[a]];
 }
@@ -405,6 +418,66 @@ void SdpDevice::upload(int n_, int m_, const HostCoeff &C, const std::vector<Hos
     ent_j = upload_vec(ej, s);
     ent_v = upload_vec(ev, s);
 
+    // Rank-one gather map: cheaper than the rank-nr1d GEMM when its bytes (12 per entry)
+    // stay under a quarter of the GEMM's flops (DMMA ~20 TFLOP/s against ~5 TB/s HBM).
+    r1d_gather = false;
+    if (nr1d > 0) {
+        long long entries = 0;
+        for (int j : r1did) {
+            const long long k = (long long) A[j].aidx.size();
+            entries += k * (k + 1) / 2;
+        }
+        const double gemm_flops = 2.0 * n * (double) n * nr1d;
+        if (12.0 * (double) entries < 0.25 * gemm_flops && (long long) n * (n + 1) / 2 < (1LL << 31)) {
+            // counting sort by packed lower position, constraint order kept within a position
+            const long long npack = (long long) n * (n + 1) / 2;
+            const int nn = n;
+            auto pidx = [nn](int r, int c) { return (long long) (2LL * nn - c - 1) * c / 2 + r; };
+            std::vector<long long> cnt(npack + 1, 0);
+            for (int j : r1did) {
+                const HostCoeff &a = A[j];
+                for (size_t t = 0; t < a.aidx.size(); ++t)
+                    for (size_t u = 0; u <= t; ++u) cnt[pidx(a.aidx[t], a.aidx[u]) + 1] += 1;
+            }
+            std::vector<int> p2r, p2c;
+            std::vector<long long> p2ptr{0};
+            std::vector<long long> slot(npack, -1);
+            for (long long q = 0; q < npack; ++q) {
+                if (cnt[q + 1] == 0) continue;
+                slot[q] = (long long) p2r.size();
+                p2ptr.push_back(p2ptr.back() + cnt[q + 1]);
+                p2r.push_back(0);
+                p2c.push_back(0);
+            }
+            // row/column of each used position
+            for (int c = 0, q = 0; c < n; ++c)
+                for (int r = c; r < n; ++r, ++q)
+                    if (slot[q] >= 0) {
+                        p2r[slot[q]] = r;
+                        p2c[slot[q]] = c;
+                    }
+            std::vector<long long> fillpos(p2ptr.begin(), p2ptr.end() - 1);
+            std::vector<int> e2j(entries);
+            std::vector<double> e2v(entries);
+            for (int j : r1did) {
+                const HostCoeff &a = A[j];
+                for (size_t t = 0; t < a.aidx.size(); ++t)
+                    for (size_t u = 0; u <= t; ++u) {
+                        const long long at = fillpos[slot[pidx(a.aidx[t], a.aidx[u])]]++;
+                        e2j[at] = j;
+                        e2v[at] = a.sign * a.aval[t] * a.aval[u];
+                    }
+            }
+            npos2 = (int) p2r.size();
+            pos2_r = upload_vec(p2r, s);
+            pos2_c = upload_vec(p2c, s);
+            pos2_ptr = upload_vec(p2ptr, s);
+            ent2_j = upload_vec(e2j, s);
+            ent2_v = upload_vec(e2v, s);
+            r1d_gather = true;
+        }
+    }
+
     HB_CUDA(cudaMalloc(&T1, sizeof(double) * ld * n));
     HB_CUDA(cudaMalloc(&T2, sizeof(double) * ld * n));
     HB_CUDA(cudaMalloc(&vecbuf, sizeof(double) * std::max(m, 1)));
@@ -423,6 +496,12 @@ void SdpDevice::release() {
     for (double *p : dr_mat) f(p);
     dr_mat.clear();
     f(pos_r); f(pos_c); f(pos_ptr); f(ent_j); f(ent_v);
+    f(pos2_r); f(pos2_c); f(pos2_ptr); f(ent2_j); f(ent2_v);
+    pos2_r = pos2_c = ent2_j = nullptr;
+    pos2_ptr = nullptr;
+    ent2_v = nullptr;
+    npos2 = 0;
+    r1d_gather = false;
     f(T1); f(T2); f(vecbuf); f(d_w); f(d_scal); f(colsq);
     colsq = nullptr;
     opA1.release();
@@ -440,7 +519,10 @@ void SdpDevice::assemble(double dC, double dA, const double *d_wvec, double dEye
     if (dA != 0.0) {
         if (npos > 0)
             s_gather_kernel<<<hb::counted(grid1(npos)), 256, 0, s>>>(npos, pos_r, pos_c, pos_ptr, ent_j, ent_v, d_wvec, dA, S, ldS);
-        if (nr1d > 0) {
+        if (nr1d > 0 && r1d_gather) {
+            s_gather2_kernel<<<hb::counted(grid1(npos2)), 256, 0, s>>>(npos2, pos2_r, pos2_c, pos2_ptr, ent2_j,
+                                                                       ent2_v, d_wvec, dA, S, ldS);
+        } else if (nr1d > 0) {
             r1d_weights_kernel<<<hb::counted(grid1(nr1d)), 256, 0, s>>>(nr1d, r1d_id, r1d_sign, d_wvec, dA, d_w);
             scale_columns(s, n, nr1d, A1, ld, d_w, V, ld);
             gemm(s, n, n, nr1d, 1.0, V, ld, 0, A1, ld, 1, 1.0, S, ldS, 0);

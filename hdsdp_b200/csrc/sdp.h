@@ -69,6 +69,15 @@ struct SdpDevice {
     int npos = 0;
     int *pos_r = nullptr, *pos_c = nullptr, *pos_ptr = nullptr, *ent_j = nullptr;
     double *ent_v = nullptr;
+    // Gather map of the dense rank-one class over its supports (used instead of the
+    // rank-nr1d GEMM when the supports are sparse): per lower position the list of
+    // (constraint, s_i a_ip a_iq), in constraint order
+    bool r1d_gather = false;
+    int npos2 = 0;
+    int *pos2_r = nullptr, *pos2_c = nullptr;
+    long long *pos2_ptr = nullptr;
+    int *ent2_j = nullptr;
+    double *ent2_v = nullptr;
 
     // scratch
     double *V = nullptr;       // n x max(nr1d, nr1s) (W * A_r1)

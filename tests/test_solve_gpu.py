@@ -27,7 +27,10 @@ def check_parity(r, ref, psdp=False):
     # gap); solved to optimality they agree to 1e-6.
     tol = 5e-4 if psdp else 1e-6
     assert r["dobj"] == pytest.approx(ref["dobj"], rel=tol, abs=1e-8)
-    assert r["pobj"] == pytest.approx(ref["pobj"], rel=tol, abs=1e-8)
+    if ref["status"] == OPTIMAL:
+        # a run the reference itself ends as NUMERICAL (a gap of percents) has no
+        # meaningful primal objective to compare
+        assert r["pobj"] == pytest.approx(ref["pobj"], rel=tol, abs=1e-8)
     if ref["status"] == OPTIMAL:
         assert r["errs"][0] <= max(1e-7, 10 * ref["errs"][0])
         assert r["errs"][1] <= 1e-7 and r["errs"][2] <= 1e-7 and r["errs"][3] <= 1e-7
