@@ -1,19 +1,27 @@
 // Allocation-free variant of the Cholesky entry point (no reference counterpart).
 //
+// Some callers cannot call cudaMalloc on their call path: a host framework whose
+// caching allocator already owns the device memory budget, a plugin that is not
+// allowed to touch the allocator, or a latency-critical loop that cannot afford the
+// device-wide synchronisation cudaMalloc/cudaFree may imply. For them,
 // hdsdpb_cholesky_noalloc factors an n x n matrix (n <= HDSDPB_NOALLOC_MAX_N) exactly
 // like hdsdpb_cholesky, but every device buffer it touches lives in one file-scope
-// __device__ array: nothing is allocated or freed per call, on the device or the host,
-// and no stream is created (work runs on the legacy default stream).
+// static __device__ array (about 1.2 MB, held by every GPU that loads the library until
+// the process exits): nothing is allocated or freed per call, on the device or the
+// host, and no stream is created (work runs on the legacy default stream). The caller
+// passes its input matrix and output buffers on the host, as for hdsdpb_cholesky.
 //
 // Scratch layout (doubles, ld = 256): S copy [ld * 256] | L [ld * 256] |
 // diagonal-block inverses [ld * 64] | log-det slot [1] | info word [1 int].
-// Nothing has to start at zero: the factorisation clears the info word itself and
-// only the lower triangle of L (rows < n) is ever read back.
+// The array keeps the previous call's contents. Only the info word must start at zero,
+// and the factorisation clears it itself on every call; only the lower triangle of L
+// (rows < n) is ever read back, so stale entries elsewhere are harmless.
 //
-// The first call on a device looks up the array's device address with
-// cudaGetSymbolAddress (with that device current) and caches it, so that call should
-// come before any stream capture. All calls share the one array: calls that overlap
-// (from several host threads, or interleaved on several streams) race.
+// Host code cannot use the array's name as a device address. The first call on a
+// device looks the address up with cudaGetSymbolAddress (with that device current),
+// checks the result and caches it per device; that first call should therefore come
+// before any stream capture. All calls share the one array: calls that overlap on the
+// GPU (from several host threads, or interleaved on several streams) race.
 #include "la.h"
 #include "../../include/hdsdp_b200.h"
 #include <cstdio>
@@ -26,7 +34,7 @@ constexpr long kLd = kMaxN;  // pad_ld(256) = 256
 constexpr size_t kMatDoubles = (size_t) kLd * kMaxN;
 constexpr size_t kScratchDoubles = 2 * kMatDoubles + (size_t) kLd * 64 + 2;
 
-__device__ __align__(256) double g_noalloc_scratch[kScratchDoubles];
+static __device__ __align__(256) double g_noalloc_scratch[kScratchDoubles];
 
 constexpr int kMaxDevices = 64;
 double *g_scratch_ptr[kMaxDevices] = {nullptr};

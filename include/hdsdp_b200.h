@@ -102,13 +102,15 @@ extern int hdsdpb_ratio_probe( int m, int n, const int *Ap, const int *Ai, const
    upper part zero) and sum(log L_ii). Returns 0 if positive definite, 1 if not. */
 extern int hdsdpb_cholesky( int n, const double *S, double *L, double *logdiag );
 
-/* Allocation-free variant of hdsdpb_cholesky (no reference counterpart): same
-   arguments and return values, but all device scratch is one static device array
-   sized for n <= HDSDPB_NOALLOC_MAX_N, located once per device with
-   cudaGetSymbolAddress; nothing is allocated or freed per call. Returns -2 (with a
-   message on stderr) when n exceeds the limit. The first call on a device does the
-   set-up and should come before any stream capture; overlapping calls share the
-   scratch and race. */
+/* Allocation-free variant of hdsdpb_cholesky (no reference counterpart), for callers
+   that cannot call cudaMalloc on their call path (a host framework whose allocator
+   owns the device memory, a plugin barred from allocating, a latency-critical loop
+   that cannot take the synchronisation of cudaMalloc/cudaFree). Same arguments and
+   return values, but all device scratch is one static device array sized for
+   n <= HDSDPB_NOALLOC_MAX_N (about 1.2 MB per GPU, held until exit); nothing is
+   allocated or freed per call. Returns -2 (with a message on stderr) when n exceeds
+   the limit. The first call on a device looks up the array's address and should come
+   before any stream capture; calls that overlap on the GPU share the scratch and race. */
 #define HDSDPB_NOALLOC_MAX_N 256
 extern int hdsdpb_cholesky_noalloc( int n, const double *S, double *L, double *logdiag );
 

@@ -1,8 +1,11 @@
-"""hdsdpb_cholesky_noalloc (static device scratch, nothing allocated per call) against
-the allocating entry point hdsdpb_cholesky, two calls in a row per case.
+"""hdsdpb_cholesky_noalloc against the allocating entry point hdsdpb_cholesky.
 
-The file name sorts last, so in a full run it executes after every other GPU test in
-the same process; it must also pass alone in a fresh process.
+The no-allocation entry point exists for callers that cannot call cudaMalloc on their
+call path (their framework's allocator owns the device memory, or the allocator's
+synchronisation is not acceptable there); it keeps its scratch in a static device
+array. Each case is called twice in a row, because the array keeps the previous
+call's contents. The file name sorts last, so in a full run it executes after every
+other GPU test in the same process; it must also pass alone in a fresh process.
 """
 from __future__ import annotations
 
