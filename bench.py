@@ -376,6 +376,8 @@ def run_b200(args):
                    "precision": args.precision, "parallelism": "replicas" if world > 1 else "single",
                    "l2": "flushed between steps (256 MB write)"},
         "iters": iters, "s_per_iter": value / max(1, iters), "time_to_gap_s": time_to_gap,
+        "steps_ipm_s": [round(x, 4) for x in ipm_s], "steps_e2e_s": [round(x, 4) for x in e2e_s],
+        "setup_s": [round(r["timers"]["setup"], 4) for r in results],
         "status": last["status"], "dobj": last["dobj"], "pobj": last["pobj"],
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "roofline": roofline, "kernels": kernels, "cpu_baseline": cpu, "clocks": clk,

@@ -238,13 +238,15 @@ __device__ bool potf2_dev(double *L, long ld, int j0, int nb, double *Dinv, long
 }
 
 // Tile product on the DMMA path over K = nb <= 64:
-//   mode 0:  C -= A * op(B)      mode 1:  C = A * op(B)
+//   mode 0:  C -= A * op(B)      mode 1:  C = A * op(B)      mode 2:  C = -A * op(B)
+// With Ct set, the result is also written transposed to Ct (pitch ldct).
 // A(r, k) = Ab[r + k*lda]; op(B)(k, c) = bt ? Bb[c + k*ldb] : Bb[k + c*ldb].
 // C is the 64 x 64 tile at Cb (pitch ldc) clipped to mr x nc; with diag set only
 // row >= col entries are written. Operands are staged in shared memory first, so C
 // may alias A or B (in-place panel solves).
 __device__ void tile_mma_dev(double *Cb, long ldc, int mr, int nc, const double *Ab, long lda, int ar,
-                             const double *Bb, long ldb, int bt, int bc, int nb, bool diag, int mode, double *sm) {
+                             const double *Bb, long ldb, int bt, int bc, int nb, bool diag, int mode, double *sm,
+                             double *Ct = nullptr, long ldct = 0) {
     double *As = sm, *Bs = sm + 64 * TP;   // As[r + k*TP], Bs[c + k*TP]
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     const int kp = (nb + 3) & ~3;
@@ -297,7 +299,9 @@ __device__ void tile_mma_dev(double *Cb, long ldc, int mr, int nc, const double 
             for (int e = 0; e < 2; ++e) {
                 const int c = wn + j * 8 + (lane & 3) * 2 + e;
                 if (c >= nc || (diag && r < c)) continue;
-                Cb[(size_t) r + (size_t) c * ldc] = (mode == 0) ? cv[i][j][e] - acc[i][j][e] : acc[i][j][e];
+                const double val = (mode == 0) ? cv[i][j][e] - acc[i][j][e] : (mode == 2) ? -acc[i][j][e] : acc[i][j][e];
+                Cb[(size_t) r + (size_t) c * ldc] = val;
+                if (Ct) Ct[(size_t) c + (size_t) r * ldct] = val;
             }
     }
     __syncthreads();
@@ -313,10 +317,46 @@ __device__ __forceinline__ void tri_index(long t, int &ti, int &tj) {
 // Right-looking blocked Cholesky with one-panel look-ahead: in the update phase of
 // panel j, block 0 first updates the diagonal tile of panel j+1 and factors it while
 // the other blocks update the rest of the trailing matrix.
+//
+// With K set, the inverse factor K = L^-1 (and KT = K^T) is formed alongside, right
+// looking by 64-row blocks, on the blocks that would otherwise wait for block 0:
+// while panel j is solved, the rows below block j-1 of K receive
+// X(r, c) -= L(r, j-1) K(j-1, c) (the first update of a tile assigns -L K); while the
+// trailing matrix is updated, block row j is finalised as K(j, c) = Dinv_j X(j, c) and
+// K(j, j) = Dinv_j. The strictly upper blocks of K and the strictly lower blocks of KT
+// are never written (they must hold zeros).
+__device__ __forceinline__ void k_update_tile(const double *L, long ld, double *K, int n, int r, int c, int k,
+                                              double *sm) {
+    const int mr = min(64, n - 64 * r);
+    tile_mma_dev(K + (size_t) 64 * r + (size_t) 64 * c * ld, ld, mr, 64, L + (size_t) 64 * r + (size_t) 64 * k * ld,
+                 ld, mr, K + (size_t) 64 * k + (size_t) 64 * c * ld, ld, 0, 64, 64, false, (k == c) ? 2 : 0, sm);
+}
+
+__device__ __forceinline__ void k_final_tile(const double *Dinv, long ldd, double *K, double *KT, long ld, int n,
+                                             int bj, int c, double *sm) {
+    const int mr = min(64, n - 64 * bj);
+    if (c < bj) {
+        double *X = K + (size_t) 64 * bj + (size_t) 64 * c * ld;
+        tile_mma_dev(X, ld, mr, 64, Dinv + (size_t) 64 * bj, ldd, mr, X, ld, 0, 64, mr, false, 1, sm,
+                     KT + (size_t) 64 * c + (size_t) 64 * bj * ld, ld);
+    } else {
+        for (int idx = threadIdx.x; idx < 64 * 64; idx += blockDim.x) {
+            const int r = idx & 63, cc = idx >> 6;
+            if (r < mr && cc < mr) {
+                const double v = Dinv[(size_t) (64 * bj + r) + (size_t) cc * ldd];
+                K[(size_t) (64 * bj + r) + (size_t) (64 * bj + cc) * ld] = v;
+                KT[(size_t) (64 * bj + cc) + (size_t) (64 * bj + r) * ld] = v;
+            }
+        }
+        __syncthreads();
+    }
+}
+
 __global__ void __launch_bounds__(COOP_THREADS, 2) potrf_coop_kernel(double *L, long ld, int n, double *Dinv,
-                                                                  long ldd, int *info) {
+                                                                  long ldd, int *info, double *K, double *KT) {
     cg::grid_group grid = cg::this_grid();
     extern __shared__ double sm[];
+    const int nblk = (n + 63) / 64;
     if (blockIdx.x == 0) potf2_dev(L, ld, 0, min(NB, n), Dinv, ldd, info, sm);
     grid.sync();
     for (int j0 = 0; j0 < n; j0 += NB) {
@@ -324,18 +364,28 @@ __global__ void __launch_bounds__(COOP_THREADS, 2) potrf_coop_kernel(double *L, 
         const int nb = min(NB, n - j0);
         const int rows = n - j0 - nb;
         if (rows <= 0) break;
+        const int bj = j0 / 64;
         double *P = L + (size_t) (j0 + nb) + (size_t) j0 * ld;
         const int nchunk = (rows + 63) / 64;
         const int pb = (j0 / 64) * 16 + (blockIdx.x == 1 ? 8 : 0);
         if (blockIdx.x <= 1) CHOL_STAMP(pb + 0);
-        for (int ch = blockIdx.x; ch < nchunk; ch += gridDim.x) {
-            const int mr = min(64, rows - ch * 64);
-            tile_mma_dev(P + ch * 64, ld, mr, nb, P + ch * 64, ld, mr, Dinv + j0, ldd, 1, nb, nb, false, 1, sm);
+        // panel solve; with K, the update of K's rows r >= bj by block row bj - 1
+        const long nx = (K && bj >= 1) ? (long) (nblk - bj) * bj : 0;
+        for (long t = blockIdx.x; t < nchunk + nx; t += gridDim.x) {
+            if (t < nchunk) {
+                const int ch = (int) t;
+                const int mr = min(64, rows - ch * 64);
+                tile_mma_dev(P + ch * 64, ld, mr, nb, P + ch * 64, ld, mr, Dinv + j0, ldd, 1, nb, nb, false, 1, sm);
+            } else {
+                const long u = t - nchunk;
+                k_update_tile(L, ld, K, n, bj + (int) (u / bj), (int) (u % bj), bj - 1, sm);
+            }
         }
         if (blockIdx.x <= 1) CHOL_STAMP(pb + 1);
         grid.sync();
         if (blockIdx.x <= 1) CHOL_STAMP(pb + 2);
         const long ntile = (long) nchunk * (nchunk + 1) / 2;
+        const long nk = K ? bj + 1 : 0;
         double *A22 = L + (size_t) (j0 + nb) + (size_t) (j0 + nb) * ld;
         if (blockIdx.x == 0) {
             // tile (0, 0) is the next diagonal block: update it in shared memory and factor it
@@ -343,11 +393,16 @@ __global__ void __launch_bounds__(COOP_THREADS, 2) potrf_coop_kernel(double *L, 
             potf2_dev(L, ld, j0 + nb, min(NB, rows), Dinv, ldd, info, sm, P, ld);
             CHOL_STAMP(pb + 4);
         }
-        // remaining tiles, spread over the other blocks (block 0 joins when the grid has one block)
+        // remaining tiles (and K's block row bj), spread over the other blocks
+        // (block 0 joins when the grid has one block)
         const int nworker = (gridDim.x > 1) ? (int) gridDim.x - 1 : 1;
         const int wid = (gridDim.x > 1) ? (int) blockIdx.x - 1 : 0;
         if (wid >= 0) {
-            for (long t = 1 + wid; t < ntile; t += nworker) {
+            for (long t = 1 + wid; t < ntile + nk; t += nworker) {
+                if (t >= ntile) {
+                    k_final_tile(Dinv, ldd, K, KT, ld, n, bj, (int) (t - ntile), sm);
+                    continue;
+                }
                 int ti, tj;
                 tri_index(t, ti, tj);
                 const int mr = min(64, rows - ti * 64), nc = min(64, rows - tj * 64);
@@ -359,6 +414,14 @@ __global__ void __launch_bounds__(COOP_THREADS, 2) potrf_coop_kernel(double *L, 
         grid.sync();
         if (blockIdx.x <= 1) CHOL_STAMP(pb + 5);
     }
+    if (!K || *(volatile int *) info) return;
+    // the last block row of K: its update by block row nblk - 2, then its final form
+    const int bj = nblk - 1;
+    if (bj >= 1) {
+        for (int c = blockIdx.x; c < bj; c += gridDim.x) k_update_tile(L, ld, K, n, bj, c, bj - 1, sm);
+        grid.sync();
+    }
+    for (int c = blockIdx.x; c <= bj; c += gridDim.x) k_final_tile(Dinv, ldd, K, KT, ld, n, bj, c, sm);
 }
 
 __global__ void __launch_bounds__(COOP_THREADS) trtri_coop_kernel(const double *L, double *K, long ld, int n,
@@ -410,6 +473,17 @@ __global__ void identity_k(int n, double *A, long lda) {
 
 __global__ void zero_info_k(int *p) { *p = 0; }
 
+int sm_count() {
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = 1;
+    }
+    return sms;
+}
+
 int coop_grid(const void *fn) {
     static int cached[2] = {0, 0};
     const int slot = (fn == (const void *) potrf_coop_kernel) ? 0 : 1;
@@ -436,14 +510,19 @@ bool coop_factorize_enqueue(cudaStream_t s, DenseFactor &F, const double *S, lon
     copy_lower_k<<<hb::counted(grid_for_n((long) n * n)), 256, 0, s>>>(n, S, ldS, F.L, F.ld);
     const void *fn = (const void *) potrf_coop_kernel;
     const long t0 = (long) ((n - 1) / 64 + 1);
-    const int grid = (int) std::max(1L, std::min<long>(coop_grid(fn), t0 * (t0 + 1) / 2));
+    // with the fused inverse, the update of K's rows needs up to t0^2 / 4 tiles per phase
+    // at most one block per SM, so that the block factoring the diagonal never shares an SM
+    const long want = F.fuse_k ? t0 * (t0 + 1) / 2 + t0 * t0 / 4 : t0 * (t0 + 1) / 2;
+    const int grid = (int) std::max(1L, std::min<long>(std::min(coop_grid(fn), sm_count()), want));
     double *Lp = F.L;
     long ld = F.ld;
     int nn = n;
     double *Dp = F.Dinv;
     long ldd = F.ld;
     int *ip = F.d_info;
-    void *args[] = {&Lp, &ld, &nn, &Dp, &ldd, &ip};
+    double *Kp = F.fuse_k ? F.K : nullptr;
+    double *KTp = F.fuse_k ? F.KT : nullptr;
+    void *args[] = {&Lp, &ld, &nn, &Dp, &ldd, &ip, &Kp, &KTp};
     const bool timed = kstat_on(KF_POTRF);
     if (timed) kstat_begin(KF_POTRF, s, (double) n * n * n / 3.0);
     cudaError_t e = cudaLaunchCooperativeKernel(fn, hb::counted(grid), COOP_THREADS, args, SM_DOUBLES * sizeof(double), s);

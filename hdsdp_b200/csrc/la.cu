@@ -617,6 +617,13 @@ void DenseFactor::alloc(int n_) {
     *h_info = 0;
     HB_CUDA(cudaMemset(L, 0, sizeof(double) * ld * n));
     HB_CUDA(cudaMemset(Dinv, 0, sizeof(double) * ld * NB));
+    fuse_k = (n <= kFuseInverseMax);
+    if (fuse_k) {
+        HB_CUDA(cudaMalloc(&K, sizeof(double) * ld * n));
+        HB_CUDA(cudaMalloc(&KT, sizeof(double) * ld * n));
+        HB_CUDA(cudaMemset(K, 0, sizeof(double) * ld * n));
+        HB_CUDA(cudaMemset(KT, 0, sizeof(double) * ld * n));
+    }
 }
 
 void DenseFactor::release() {
@@ -629,7 +636,7 @@ void DenseFactor::release() {
     L = Dinv = K = KT = nullptr;
     d_info = nullptr;
     h_info = nullptr;
-    factored = ok = k_valid = false;
+    factored = ok = k_valid = fuse_k = k_pending = false;
 }
 
 static void set_smem(const void *fn, int bytes) {
@@ -654,8 +661,10 @@ void factorize_async(cudaStream_t s, DenseFactor &F, const double *S, long ldS) 
     ensure_attrs();
     const int n = F.n;
     F.k_valid = false;
+    F.k_pending = false;
     F.factored = true;
     if (coop_factorize_enqueue(s, F, S, ldS)) {
+        F.k_pending = F.fuse_k && F.K && F.KT;
         HB_CUDA(cudaMemcpyAsync(F.h_info, F.d_info, sizeof(int), cudaMemcpyDeviceToHost, s));
         return;
     }
@@ -680,6 +689,8 @@ void factorize_async(cudaStream_t s, DenseFactor &F, const double *S, long ldS) 
 bool factor_status(cudaStream_t s, DenseFactor &F) {
     HB_CUDA(cudaStreamSynchronize(s));
     F.ok = (*F.h_info == 0);
+    F.k_valid = F.ok && F.k_pending;  // K and KT were formed by the factorisation kernel
+    F.k_pending = false;
     return F.ok;
 }
 

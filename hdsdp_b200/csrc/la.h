@@ -46,9 +46,15 @@ struct DenseFactor {
     bool factored = false;
     bool ok = false;
     bool k_valid = false;
+    // n <= kFuseInverseMax: the factorisation kernel also forms K and KT (allocated with
+    // the factor, zero outside their triangles)
+    bool fuse_k = false;
+    bool k_pending = false;   // the last factorisation was enqueued with the fused inverse
     void alloc(int n_);
     void release();
 };
+
+constexpr int kFuseInverseMax = 2048;
 
 // Copy the lower triangle of S (n x n, ldS) into F.L and factorise it.
 // Returns true if S is positive definite (dpotrf semantics: fails on a
