@@ -13,7 +13,8 @@ CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libhdsdp_b200.so")
 SOURCES = ["la.cu", "chol.cu", "sdp.cu", "split.cu", "cone.cu", "solver.cu", "ext.cu", "adjoint.cu", "noalloc.cu"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
-              "-Xcompiler", "-fPIC", "-shared", "-cudart", "static", "-diag-suppress", "550"]
+              "-Xcompiler", "-fPIC", "-Xcompiler", "-fopenmp", "-shared", "-cudart", "static", "-diag-suppress", "550",
+              "-lgomp"]
 
 
 def nvcc() -> str:

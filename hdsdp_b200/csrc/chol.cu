@@ -181,6 +181,7 @@ __device__ bool potf2_dev(double *L, long ld, int j0, int nb, double *Dinv, long
     for (int r = nb + tid; r < 64; r += blockDim.x) T[r + r * TP] = 1.0;  // pad with the identity
     __syncthreads();
     const int sb = 4096 + (j0 / 64) * 32;
+    (void) sb;
     CHOL_STAMP(sb);
     for (int s0 = 0; s0 < 64; s0 += 16) {
         if (warp == 0) {
@@ -368,6 +369,7 @@ __global__ void __launch_bounds__(COOP_THREADS, 2) potrf_coop_kernel(double *L, 
         double *P = L + (size_t) (j0 + nb) + (size_t) j0 * ld;
         const int nchunk = (rows + 63) / 64;
         const int pb = (j0 / 64) * 16 + (blockIdx.x == 1 ? 8 : 0);
+        (void) pb;
         if (blockIdx.x <= 1) CHOL_STAMP(pb + 0);
         // panel solve; with K, the update of K's rows r >= bj by block row bj - 1
         const long nx = (K && bj >= 1) ? (long) (nblk - bj) * bj : 0;

@@ -118,13 +118,28 @@ hdsdp_retcode SdpCone::proc_data(int nRow, int nCol, const int *Ap, const int *A
             if (Ai[e] < 0 || Ai[e] >= npack) return HDSDP_RETCODE_FAILED;
             ent.push_back({(long) Ai[e], Ax[e]});
         }
-        std::stable_sort(ent.begin(), ent.end(), [](auto &x, auto &y) { return x.first < y.first; });
+        auto less = [](const std::pair<long, double> &x, const std::pair<long, double> &y) {
+            return x.first < y.first;
+        };
+        if (!std::is_sorted(ent.begin(), ent.end(), less)) std::stable_sort(ent.begin(), ent.end(), less);
         const int nnz = (int) ent.size();
         h.r.resize(nnz);
         h.c.resize(nnz);
         h.v.resize(nnz);
+        // sorted packed indices: walk the columns instead of searching for each entry
+        int jc = 0;
+        long colStart = 0, nextStart = n;
         for (int e = 0; e < nnz; ++e) {
-            unpack(n, ent[e].first, h.r[e], h.c[e]);
+            const long q = ent[e].first;
+            if (q >= nextStart) {
+                unpack(n, q, h.r[e], h.c[e]);
+                jc = h.c[e];
+                colStart = ((2L * n - jc - 1) * jc) / 2;  // packed index of (i, jc) is colStart + i
+                nextStart = colStart + n;                 // first index of column jc + 1
+            } else {
+                h.c[e] = jc;
+                h.r[e] = (int) (q - colStart);
+            }
             h.v[e] = ent[e].second;
         }
         // sdpDataMatSetData (linalg/hdsdp_sdpdata.c:2262-2286)
@@ -139,10 +154,12 @@ hdsdp_retcode SdpCone::proc_data(int nRow, int nCol, const int *Ap, const int *A
     };
     if (load(0, C, refTypeC) != HDSDP_RETCODE_OK) return HDSDP_RETCODE_FAILED;
     stats[refTypeC] += 1;
-    for (int i = 0; i < m; ++i) {
-        if (load(i + 1, A[i], refType[i]) != HDSDP_RETCODE_OK) return HDSDP_RETCODE_FAILED;
-        stats[refType[i]] += 1;
-    }
+    int bad = 0;
+#pragma omp parallel for schedule(dynamic, 16) reduction(+ : bad)
+    for (int i = 0; i < m; ++i)
+        if (load(i + 1, A[i], refType[i]) != HDSDP_RETCODE_OK) bad += 1;
+    if (bad) return HDSDP_RETCODE_FAILED;
+    for (int i = 0; i < m; ++i) stats[refType[i]] += 1;
     return HDSDP_RETCODE_OK;
 }
 
@@ -178,11 +195,10 @@ hdsdp_retcode SdpCone::presolve() {
         normalize_r1(h);
     };
     eig(C, refTypeC);
-    for (int i = 0; i < m; ++i) {
-        stats[refType[i]] -= 1;
-        eig(A[i], refType[i]);
-        stats[refType[i]] += 1;
-    }
+    for (int i = 0; i < m; ++i) stats[refType[i]] -= 1;
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int i = 0; i < m; ++i) eig(A[i], refType[i]);
+    for (int i = 0; i < m; ++i) stats[refType[i]] += 1;
     // device class per row
     for (int i = 0; i < m; ++i) {
         HostCoeff &h = A[i];

@@ -8,6 +8,7 @@
 //   <A, Z>        = sum_e v_e * (r != c ? 2 Z_rc : Z_rr)
 //   <A, W B W>    = sum_e sum_f v_e u_f * pair(e, f)       (pair below)
 #include "sdp.h"
+#include <chrono>
 #include <unordered_map>
 #include <algorithm>
 #include <cstring>
@@ -275,7 +276,12 @@ __global__ void innersq_r1s_kernel(int n, int k, const int *id, const int *ptr, 
 
 }  // namespace
 
+static double host_seconds() {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
 void SdpDevice::upload(int n_, int m_, const HostCoeff &C, const std::vector<HostCoeff> &A, cudaStream_t s) {
+    const double tu0 = host_seconds();
     n = n_;
     m = m_;
     ld = pad_ld(n);
@@ -421,6 +427,7 @@ void SdpDevice::upload(int n_, int m_, const HostCoeff &C, const std::vector<Hos
     // Rank-one gather map: cheaper than the rank-nr1d GEMM when its bytes (12 per entry)
     // stay under a quarter of the GEMM's flops (DMMA ~20 TFLOP/s against ~5 TB/s HBM).
     r1d_gather = false;
+    const double tm0 = host_seconds();
     if (nr1d > 0) {
         long long entries = 0;
         for (int j : r1did) {
@@ -429,44 +436,81 @@ void SdpDevice::upload(int n_, int m_, const HostCoeff &C, const std::vector<Hos
         }
         const double gemm_flops = 2.0 * n * (double) n * nr1d;
         if (12.0 * (double) entries < 0.25 * gemm_flops && (long long) n * (n + 1) / 2 < (1LL << 31)) {
-            // counting sort by packed lower position, constraint order kept within a position
+            // Per row q, the constraints whose support holds q, ascending, with a_jq. The
+            // entries of lower position (r, c) are the merge of rows r and c: constraint
+            // order within a position, built in parallel over columns, values
+            // s_j a_jr a_jc as before.
+            std::vector<int> rptr(n + 1, 0);
+            for (int j : r1did)
+                for (int q : A[j].aidx) rptr[q + 1] += 1;
+            for (int q = 0; q < n; ++q) rptr[q + 1] += rptr[q];
+            std::vector<int> rj(rptr[n]);
+            std::vector<double> ra(rptr[n]);
+            {
+                std::vector<int> fill(rptr.begin(), rptr.end() - 1);
+                for (int j : r1did) {  // r1did ascending: each row list ends up sorted by j
+                    const HostCoeff &a = A[j];
+                    for (size_t t = 0; t < a.aidx.size(); ++t) {
+                        const int at = fill[a.aidx[t]]++;
+                        rj[at] = j;
+                        ra[at] = a.aval[t];
+                    }
+                }
+            }
+            std::vector<double> sgn(m, 0.0);
+            for (int j : r1did) sgn[j] = A[j].sign;
+            // pass 1: entries per lower position, column by column
             const long long npack = (long long) n * (n + 1) / 2;
-            const int nn = n;
-            auto pidx = [nn](int r, int c) { return (long long) (2LL * nn - c - 1) * c / 2 + r; };
-            std::vector<long long> cnt(npack + 1, 0);
-            for (int j : r1did) {
-                const HostCoeff &a = A[j];
-                for (size_t t = 0; t < a.aidx.size(); ++t)
-                    for (size_t u = 0; u <= t; ++u) cnt[pidx(a.aidx[t], a.aidx[u]) + 1] += 1;
+            std::vector<int> cnt(npack, 0);
+            auto colbase = [&](int c) { return (long long) (2LL * n - c - 1) * c / 2; };
+#pragma omp parallel for schedule(dynamic, 8)
+            for (int c = 0; c < n; ++c) {
+                const long long base = colbase(c);
+                for (int r = c; r < n; ++r) {
+                    int x = rptr[r], xe = rptr[r + 1], y = rptr[c], ye = rptr[c + 1], k = 0;
+                    while (x < xe && y < ye) {
+                        if (rj[x] < rj[y]) ++x;
+                        else if (rj[x] > rj[y]) ++y;
+                        else { ++k; ++x; ++y; }
+                    }
+                    cnt[base + r] = k;
+                }
             }
+            // used positions and their entry offsets
             std::vector<int> p2r, p2c;
-            std::vector<long long> p2ptr{0};
-            std::vector<long long> slot(npack, -1);
-            for (long long q = 0; q < npack; ++q) {
-                if (cnt[q + 1] == 0) continue;
-                slot[q] = (long long) p2r.size();
-                p2ptr.push_back(p2ptr.back() + cnt[q + 1]);
-                p2r.push_back(0);
-                p2c.push_back(0);
-            }
-            // row/column of each used position
-            for (int c = 0, q = 0; c < n; ++c)
-                for (int r = c; r < n; ++r, ++q)
-                    if (slot[q] >= 0) {
-                        p2r[slot[q]] = r;
-                        p2c[slot[q]] = c;
+            std::vector<long long> p2ptr{0}, pslot(npack, -1);
+            for (int c = 0; c < n; ++c)
+                for (int r = c; r < n; ++r) {
+                    const long long q = colbase(c) + r;
+                    if (cnt[q] == 0) continue;
+                    pslot[q] = (long long) p2r.size();
+                    p2r.push_back(r);
+                    p2c.push_back(c);
+                    p2ptr.push_back(p2ptr.back() + cnt[q]);
+                }
+            std::vector<int> e2j(p2ptr.back());
+            std::vector<double> e2v(p2ptr.back());
+            // pass 2: fill in constraint order
+#pragma omp parallel for schedule(dynamic, 8)
+            for (int c = 0; c < n; ++c) {
+                const long long base = colbase(c);
+                for (int r = c; r < n; ++r) {
+                    const long long slot = pslot[base + r];
+                    if (slot < 0) continue;
+                    long long at = p2ptr[slot];
+                    int x = rptr[r], xe = rptr[r + 1], y = rptr[c], ye = rptr[c + 1];
+                    while (x < xe && y < ye) {
+                        if (rj[x] < rj[y]) ++x;
+                        else if (rj[x] > rj[y]) ++y;
+                        else {
+                            e2j[at] = rj[x];
+                            e2v[at] = sgn[rj[x]] * ra[x] * ra[y];
+                            ++at;
+                            ++x;
+                            ++y;
+                        }
                     }
-            std::vector<long long> fillpos(p2ptr.begin(), p2ptr.end() - 1);
-            std::vector<int> e2j(entries);
-            std::vector<double> e2v(entries);
-            for (int j : r1did) {
-                const HostCoeff &a = A[j];
-                for (size_t t = 0; t < a.aidx.size(); ++t)
-                    for (size_t u = 0; u <= t; ++u) {
-                        const long long at = fillpos[slot[pidx(a.aidx[t], a.aidx[u])]]++;
-                        e2j[at] = j;
-                        e2v[at] = a.sign * a.aval[t] * a.aval[u];
-                    }
+                }
             }
             npos2 = (int) p2r.size();
             pos2_r = upload_vec(p2r, s);
@@ -478,6 +522,7 @@ void SdpDevice::upload(int n_, int m_, const HostCoeff &C, const std::vector<Hos
         }
     }
 
+    t_upload_map = host_seconds() - tm0;
     HB_CUDA(cudaMalloc(&T1, sizeof(double) * ld * n));
     HB_CUDA(cudaMalloc(&T2, sizeof(double) * ld * n));
     HB_CUDA(cudaMalloc(&vecbuf, sizeof(double) * std::max(m, 1)));
@@ -485,6 +530,7 @@ void SdpDevice::upload(int n_, int m_, const HostCoeff &C, const std::vector<Hos
     HB_CUDA(cudaMalloc(&d_scal, sizeof(double) * 16));
     HB_CUDA(cudaMallocHost(&h_scal, sizeof(double) * 16));
     HB_CUDA(cudaStreamSynchronize(s));
+    t_upload_total = host_seconds() - tu0;
 }
 
 void SdpDevice::release() {

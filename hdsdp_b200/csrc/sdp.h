@@ -73,6 +73,7 @@ struct SdpDevice {
     // rank-nr1d GEMM when the supports are sparse): per lower position the list of
     // (constraint, s_i a_ip a_iq), in constraint order
     bool r1d_gather = false;
+    double t_upload_map = 0.0, t_upload_total = 0.0;  // host seconds spent in upload()
     int npos2 = 0;
     int *pos2_r = nullptr, *pos2_c = nullptr;
     long long *pos2_ptr = nullptr;

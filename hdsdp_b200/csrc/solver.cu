@@ -1390,6 +1390,7 @@ hdsdp_retcode HDSDPCheckSolution(hdsdp *h, double dErrs[6]) {
 
 hdsdp_retcode HDSDPOptimize(hdsdp *h, int dOptOnly) {
     hdsdp_retcode retcode = HDSDP_RETCODE_OK;
+    double tp0 = 0.0, tp1 = 0.0, tp2 = 0.0;
     h->timeBegin = wall();
     h->timers = Timers();
     h->log.clear();
@@ -1403,12 +1404,19 @@ hdsdp_retcode HDSDPOptimize(hdsdp *h, int dOptOnly) {
     h->cone = new SdpCone();
     h->cone->precision = h->precision;
     user_data *u = h->usr;
+    tp0 = wall();
     CALL(h->cone->proc_data(u->nConicRow, u->nConicCol, u->coneMatBeg, u->coneMatIdx, u->coneMatElem));
+    tp1 = wall();
     CALL(h->cone->presolve());
+    tp2 = wall();
     get_statistics(h);
     adjust_params(h);
     h->bnd.proc(h->nRows, dp(h, DBL_PARAM_DUALBOX_LOW), dp(h, DBL_PARAM_DUALBOX_UP));
     CALL(h->cone->setup_device(h->stream, &h->timers));
+    if (h->verbose)
+        printf("  set-up: data %.3f s, rank-one detection %.3f s, device upload %.3f s (coefficients %.3f s, "
+               "of which gather map %.3f s)\n",
+               tp1 - tp0, tp2 - tp1, wall() - tp2, h->cone->dev.t_upload_total, h->cone->dev.t_upload_map);
     h->kkt.init(h->nRows, h->stream, &h->timers);
     if (device_error_flag()) {
         retcode = HDSDP_RETCODE_MEMORY;
