@@ -46,7 +46,10 @@ FAMILIES = ["fp64_gemm_dmma", "potrf_coop", "trtri_coop", "schur_pair_gather", "
 FAMILY_BOUND = ["tensor", "tensor", "tensor", "hbm", "tensor"]
 # ncu dram__bytes_read.sum + dram__bytes_write.sum per launch of the top kernel on
 # the bench workload, from the capture summarised under profiles/ (None until captured).
-TRAFFIC_PER_LAUNCH = {}
+# DRAM bytes (read + write) per launch from one ncu capture (profiles/potrf_coop_n1000.md:
+# dram__bytes_read.sum + dram__bytes_write.sum of the n = 1000 factorisation, the size of the
+# bench workload's dual slack; the 53 Schur factorisations per solve are n = 2000).
+TRAFFIC_PER_LAUNCH = {("rank1_n1000_m2000", "potrf_coop"): 4.3282e6}
 REF_SAMPLE_ITERS = 5
 
 
@@ -59,6 +62,7 @@ def parse_args():
     ap.add_argument("--workload", default="rank1_n1000_m2000")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "split", "adaptive"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-precision-legs", action="store_true", help="skip the other-precision solves")
     return ap.parse_args()
 
 
@@ -160,21 +164,57 @@ def reference_iters(workload: str):
         return None
 
 
-def reference_sample(inst, workload: str, iters: int, threads: int, fallback_iters=None):
-    """Seconds to a 1e-6 gap for the reference CPU solver, estimated from two bounded runs.
-
-    A run capped at one iteration gives the set-up cost plus one iteration; a run
-    capped at 1 + `iters` adds `iters` iterations. The estimate is the first plus
-    the marginal per-iteration cost times the reference's remaining iterations.
-    """
+def _reference_child(workload, caps, threads, out):
+    """Child process: the reference solver on the workload, capped at each iteration count."""
+    from hdsdp_b200 import instances
     from oracle import ref_api
     ref_api.set_threads(threads)
-    r1 = ref_api.solve(inst, want_x=False, params={0: 1, 4: 0})
-    rk = ref_api.solve(inst, want_x=False, params={0: 1 + iters, 4: 0})
-    done = max(1, rk["iters"] - r1["iters"])
-    per_iter = max(0.0, rk["time"] - r1["time"]) / done
-    full = reference_iters(workload) or fallback_iters or rk["iters"]
-    return r1["time"] + per_iter * (full - r1["iters"]), r1["time"] + rk["time"], done, full
+    inst = instances.WORKLOADS[workload]()
+    res = []
+    for cap in caps:
+        r = ref_api.solve(inst, want_x=False, params={0: cap, 4: 0})
+        res.append((r["time"], r["iters"]))
+    out.put(res)
+
+
+def reference_runs(workload: str, caps, threads: int, timeout: float):
+    """(time, iterations) of reference solves capped at `caps`, run in a spawned child.
+
+    The child isolates the bench from the reference: its HDSDPOptimize smashes its own stack
+    when capped at one iteration on the MaxCut instances, and large workloads can exceed the
+    time allowed for a bounded sample. Returns (None, reason) on failure.
+    """
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    p = ctx.Process(target=_reference_child, args=(workload, list(caps), threads, q))
+    p.start()
+    p.join(timeout)
+    if p.is_alive():
+        p.kill()
+        p.join()
+        return None, "reference sample exceeded %.0f s" % timeout
+    if p.exitcode != 0:
+        return None, "reference process exited with code %s" % p.exitcode
+    return q.get(), ""
+
+
+def reference_sample(workload: str, iters: int, threads: int, fallback_iters=None, timeout: float = 240.0):
+    """Seconds to a 1e-6 gap for the reference CPU solver, estimated from two bounded runs.
+
+    A run capped at two iterations gives the set-up cost plus two iterations; a run capped
+    at 2 + `iters` adds `iters` iterations. The estimate is the first plus the marginal
+    per-iteration cost times the reference's remaining iterations. Returns None and a
+    reason when the sample fails.
+    """
+    res, why = reference_runs(workload, (2, 2 + iters), threads, timeout)
+    if res is None:
+        return None, why
+    (t1, i1), (tk, ik) = res
+    done = max(1, ik - i1)
+    per_iter = max(0.0, tk - t1) / done
+    full = reference_iters(workload) or fallback_iters or ik
+    return (t1 + per_iter * max(0, full - i1), t1 + tk, done, full), ""
 
 
 def run_reference(args):
@@ -189,20 +229,22 @@ def run_reference(args):
         return
     inst = instances.WORKLOADS[args.workload]()
     cores = host_cores()
-    from oracle import ref_api as _ra
-    _ra.set_threads(cores)
-    for _ in range(args.warmup):
-        _ra.solve(inst, want_x=False, params={0: 1, 4: 0})
+    for _ in range(args.warmup):  # untimed: a short capped solve in the same kind of child process
+        reference_runs(args.workload, (2,), cores, 240.0)
     vals, raw = [], []
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        est, t, done, full = reference_sample(inst, args.workload, REF_SAMPLE_ITERS, cores)
+        got, why = reference_sample(args.workload, REF_SAMPLE_ITERS, cores)
+        if got is None:
+            print(json.dumps({"impl": "reference", "unavailable": why}))
+            return
+        est, t, done, full = got
         vals.append(est)
         raw.append(t)
     wall = time.perf_counter() - t0
     value = statistics.mean(vals)
-    sample = ("per step: %s solves capped at 1 and %d IPM iterations (%.2f s of CPU work); set-up + "
-              "marginal s/iter scaled to the reference's %d iterations" % (args.workload, 1 + REF_SAMPLE_ITERS,
+    sample = ("per step: %s solves capped at 2 and %d IPM iterations (%.2f s of CPU work); set-up + "
+              "marginal s/iter scaled to the reference's %d iterations" % (args.workload, 2 + REF_SAMPLE_ITERS,
                                                                          statistics.mean(raw), full))
     line = dict(base, value=value, n_gpus=args.gpus, steps=args.steps, warmup=args.warmup,
                 ms_per_step=1e3 * wall / args.steps, scaling="weak", vs_baseline=None, dtype="f64",
@@ -218,6 +260,68 @@ def run_reference(args):
 
 # ---------------------------------------------------------------------------
 # B200 arm
+
+def adjoint_leg(L, api, instances, np):
+    """Adjoint ms on the theta-style layer (n = 200) against the mean IPM iteration of its solve."""
+    import ctypes as C
+    import torch
+    inst = instances.WORKLOADS["theta_adjoint_n200"]()
+    rng = np.random.default_rng(5)
+    G = rng.standard_normal((inst.n, inst.n))
+    G = np.asfortranarray(G + G.T)
+    h = rng.standard_normal(inst.m)
+    out = {}
+    for rep in range(2):  # the first solve warms the path; the second is measured
+        s = api.Solver()
+        try:
+            s.init(inst.m, 1)
+            s.set_cone(inst.m, inst.n, inst.Ap, inst.Ai, inst.Ax)
+            s.set_dual_objective(inst.b)
+            s.set_primal_refinement(False)
+            s.optimize(0)
+            t = s.timers()
+            iters = max(1, s.iters())
+            times = []
+            for _ in range(3):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                torch.cuda.synchronize()
+                e0.record()
+                s.adjoint(h, G)
+                e1.record()
+                torch.cuda.synchronize()
+                times.append(e0.elapsed_time(e1))
+            out = {"workload": "theta_adjoint_n200", "n": inst.n, "m": inst.m, "status": s.status(),
+                   "first_call_ms": times[0], "cached_call_ms": min(times[1:]),
+                   "ipm_iter_ms": 1e3 * t["ipm_device"] / iters, "iters": iters,
+                   "first_call_over_iter": times[0] / (1e3 * t["ipm_device"] / iters)}
+        finally:
+            s.close()
+    return out
+
+
+def precision_leg(api, inst, mode, solves, np):
+    """Mean device-timed solve and time to a 1e-6 gap with HDSDPSetPrecision(mode)."""
+    ipm, ttg, it, st = [], [], 0, 0
+    for _ in range(solves):
+        s = api.Solver()
+        try:
+            s.init(inst.m, 1)
+            s.set_cone(inst.m, inst.n, inst.Ap, inst.Ai, inst.Ax)
+            s.set_dual_objective(inst.b)
+            s.set_primal_refinement(False)
+            s.set_precision(mode)
+            s.optimize(0)
+            t = s.timers()
+            log = s.iter_log()
+            hit = np.flatnonzero(np.asarray(log["gap"]) <= 1e-6)
+            ttg.append(float(log["t"][hit[0]] - t["setup"]) if hit.size else None)
+            ipm.append(t["ipm_device"])
+            it, st = s.iters(), s.status()
+        finally:
+            s.close()
+    return {"value": float(np.mean(ipm)), "unit": UNIT, "iters": it, "status": st,
+            "time_to_gap_s": ttg[-1], "solves": solves}
+
 
 def run_b200(args):
     rank, world, local_rank = dist_env()
@@ -358,15 +462,28 @@ def run_b200(args):
             from oracle import ref_api
             if ref_api.available():
                 cores = host_cores()
-                est, t, done, full = reference_sample(inst, args.workload, REF_SAMPLE_ITERS, cores,
-                                                      fallback_iters=iters)
+                got, why = reference_sample(args.workload, REF_SAMPLE_ITERS, cores, fallback_iters=iters)
+                if got is None:
+                    raise RuntimeError(why)
+                est, t, done, full = got
                 cpu = {"value": est, "unit": UNIT, "cores": cores, "kind": "reference",
-                       "sample": "reference CPU solves capped at 1 and %d IPM iterations (%.2f s of CPU work); "
-                                 "set-up + marginal s/iter scaled to its %d iterations" % (1 + done, t, full)}
+                       "sample": "reference CPU solves capped at 2 and %d IPM iterations (%.2f s of CPU work); "
+                                 "set-up + marginal s/iter scaled to its %d iterations" % (2 + done, t, full)}
         except Exception as exc:  # the baseline is reported, never required
             cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": "failed: %s" % exc}
 
     t = last["timers"]
+    adj = adjoint_leg(L, api, instances, np) if rank == 0 else None
+    legs = None
+    if rank == 0 and not args.no_precision_legs:
+        # the other arithmetic on the same workload (two solves after the warm-up above)
+        other = {"fp64": 2, "split": 0, "adaptive": 0}[args.precision]
+        name = "fp64" if other == 0 else "split_adaptive"
+        legs = {args.precision if args.precision != "adaptive" else "split_adaptive": value,
+                name: precision_leg(api, inst, other, 2, np)}
+        if other == 2:
+            legs["fp64_over_split"] = value / legs[name]["value"]
+
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": max(3, args.warmup), "ms_per_step": 1e3 * value, "higher_is_better": False,
@@ -381,7 +498,7 @@ def run_b200(args):
         "status": last["status"], "dobj": last["dobj"], "pobj": last["pobj"],
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "roofline": roofline, "kernels": kernels, "cpu_baseline": cpu, "clocks": clk,
-        "gpu_launches": launches, "wall_s": wall,
+        "gpu_launches": launches, "wall_s": wall, "adjoint": adj, "precision_legs": legs,
         "split_s": {k: t[k] for k in ("schur", "schur_factor", "schur_solve", "s_factor", "s_inverse",
                                       "lanczos", "assemble", "primal", "setup", "total")},
     }
