@@ -135,7 +135,7 @@ hdsdp_retcode prepare(hdsdp *h, AdjointState &a) {
     HB_CUDA(cudaMalloc(&a.d_scal, sizeof(double) * 4));
     HB_CUDA(cudaMallocHost(&a.h_scal, sizeof(double) * 4));
     a.FS.alloc(n);
-    a.FM.alloc(m);
+    a.FM.alloc(m, 1);
     if (device_error_flag()) return HDSDP_RETCODE_MEMORY;
 
     // the solution in the user's units

@@ -625,7 +625,7 @@ void KKT::init(int m_, cudaStream_t stream, Timers *t) {
     ldm = pad_ld(m);
     HB_CUDA(cudaMalloc(&M, sizeof(double) * ldm * m));
     HB_CUDA(cudaMemsetAsync(M, 0, sizeof(double) * ldm * m, s));
-    F.alloc(m);
+    F.alloc(m, 1);  // the Schur solves always use K
     asinv.assign(m, 0.0);
     asinvrd.assign(m, 0.0);
     asinvcs.assign(m, 0.0);

@@ -281,7 +281,7 @@ extern "C" int hdsdpb_kernel_timing(int which, int n, int reps, double *ms) {
     fill_spd_kernel<<<hb::counted(1024), 256, 0, s>>>(n, B, ld, 7u);
     fill(s, x, 1.0, n);
     DenseFactor F;
-    F.alloc(n);
+    F.alloc(n, which == 7 ? 1 : (which == 8 ? 0 : -1));
     Lanczos lz;
     if (which == 5) lz.init(n, s);
     cudaEvent_t e0, e1;
@@ -296,6 +296,8 @@ extern "C" int hdsdpb_kernel_timing(int which, int n, int reps, double *ms) {
             case 4: coldot(s, n, n, A, ld, x, y, 1.0, 0.0, 0); break;
             case 5: { double st; lz.solve(F, B, ld, &st, nullptr); } break;
             case 6: gemm(s, n, n, 64, -1.0, A, ld, 0, B, ld, 1, 1.0, Cm, ld, GEMM_C_LOWER); break;
+            case 7:
+            case 8: factorize_async(s, F, A, ld); break;
         }
     };
     if (which == 3 || which == 5) factorize(s, F, A, ld);

@@ -450,13 +450,57 @@ __global__ void coldot_kernel(int nrows, int ncols, const double *__restrict__ A
 }
 }  // namespace
 
+// One block of S warps per column: the column's row range is cut into S segments of a
+// multiple of 32 rows, each warp reduces its segment, and warp 0 combines them. Used when
+// one warp per column would leave the SMs with too few loads in flight.
+template <int S>
+__global__ void __launch_bounds__(32 * S) coldot_seg_kernel(int nrows, const double *__restrict__ A, long lda,
+                                                          const double *__restrict__ x, double *out, double alpha,
+                                                          double beta, int mode) {
+    __shared__ double part[S];
+    const int i = blockIdx.x, w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int lo = 0, hi = nrows;
+    if (mode == 1) lo = i;
+    else if (mode == 2) hi = min(nrows, i + 1);
+    const int len = max(hi - lo, 0);
+    const int chunk = (((len + S - 1) / S) + 31) & ~31;
+    const int k0 = lo + w * chunk, k1 = min(hi, k0 + chunk);
+    const double *col = A + (size_t) i * lda;
+    double acc = 0.0;
+    int k = k0 + lane;
+    for (; k + 96 < k1; k += 128) {
+        acc += col[k] * x[k] + col[k + 32] * x[k + 32] + col[k + 64] * x[k + 64] + col[k + 96] * x[k + 96];
+    }
+    for (; k < k1; k += 32) acc += col[k] * x[k];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) part[w] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+#pragma unroll
+        for (int q = 0; q < S; ++q) t += part[q];
+        double v = alpha * t;
+        if (beta != 0.0) v += beta * out[i];
+        out[i] = v;
+    }
+}
+
 void coldot(cudaStream_t s, int nrows, int ncols, const double *A, long lda, const double *x,
             double *out, double alpha, double beta, int mode) {
     if (ncols <= 0) return;
-    const int threads = 256;
-    const long warps = ncols;
-    const int blocks = (int) ((warps * 32 + threads - 1) / threads);
-    coldot_kernel<<<hb::counted(blocks), threads, 0, s>>>(nrows, ncols, A, lda, x, out, alpha, beta, mode);
+    if (ncols < 4096 && nrows >= 256) {
+        // few columns: several warps per column keep enough loads in flight
+        if (ncols < 1024)
+            coldot_seg_kernel<8><<<hb::counted(ncols), 256, 0, s>>>(nrows, A, lda, x, out, alpha, beta, mode);
+        else
+            coldot_seg_kernel<4><<<hb::counted(ncols), 128, 0, s>>>(nrows, A, lda, x, out, alpha, beta, mode);
+    } else {
+        const int threads = 256;
+        const long warps = ncols;
+        const int blocks = (int) ((warps * 32 + threads - 1) / threads);
+        coldot_kernel<<<hb::counted(blocks), threads, 0, s>>>(nrows, ncols, A, lda, x, out, alpha, beta, mode);
+    }
     HB_CUDA(cudaGetLastError());
 }
 
@@ -607,7 +651,7 @@ int grid_for(long total, int threads = 256) {
 }
 }  // namespace
 
-void DenseFactor::alloc(int n_) {
+void DenseFactor::alloc(int n_, int fuse_inverse) {
     n = n_;
     ld = pad_ld(n);
     HB_CUDA(cudaMalloc(&L, sizeof(double) * ld * n));
@@ -617,7 +661,7 @@ void DenseFactor::alloc(int n_) {
     *h_info = 0;
     HB_CUDA(cudaMemset(L, 0, sizeof(double) * ld * n));
     HB_CUDA(cudaMemset(Dinv, 0, sizeof(double) * ld * NB));
-    fuse_k = (n <= kFuseInverseMax);
+    fuse_k = (fuse_inverse < 0) ? (n <= kFuseInverseMax) : (fuse_inverse != 0);
     if (fuse_k) {
         HB_CUDA(cudaMalloc(&K, sizeof(double) * ld * n));
         HB_CUDA(cudaMalloc(&KT, sizeof(double) * ld * n));

@@ -34,6 +34,8 @@ void coldot(cudaStream_t s, int nrows, int ncols, const double *A, long lda, con
 // Factor object for an n x n symmetric positive definite matrix.
 // L holds the lower Cholesky factor, Dinv the inverses of its 64 x 64
 // diagonal blocks, K = L^-1 and KT = L^-T (computed on demand).
+constexpr int kFuseInverseMax = 2048;
+
 struct DenseFactor {
     int n = 0;
     long ld = 0;
@@ -50,11 +52,12 @@ struct DenseFactor {
     // the factor, zero outside their triangles)
     bool fuse_k = false;
     bool k_pending = false;   // the last factorisation was enqueued with the fused inverse
-    void alloc(int n_);
+    // fuse_inverse: the factorisation kernel also forms K = L^-1 and K^T (worth it for a
+    // factor whose inverse is always used, and for small n where the K work hides behind
+    // the panel chain); -1 picks n <= kFuseInverseMax.
+    void alloc(int n_, int fuse_inverse = -1);
     void release();
 };
-
-constexpr int kFuseInverseMax = 2048;
 
 // Copy the lower triangle of S (n x n, ldS) into F.L and factorise it.
 // Returns true if S is positive definite (dpotrf semantics: fails on a

@@ -70,12 +70,15 @@ __global__ void s_gather_kernel(int npos, const int *pr, const int *pc, const in
     }
 }
 
-// Same as s_gather_kernel over the rank-one gather map (64-bit entry offsets).
-__global__ void s_gather2_kernel(int npos, const int *pr, const int *pc, const long long *ptr, const int *ej,
-                                 const double *ev, const double *w, double dA, double *S, long lds) {
+// Same as s_gather_kernel over the sliced rank-one gather map: a warp reads its slice's
+// entries e for all 32 lanes at once (coalesced); each position sums in entry order.
+__global__ void s_gather2_kernel(int npos, const int *pr, const int *pc, const long long *sptr, const int *cnt,
+                                 const int *ej, const double *ev, const double *w, double dA, double *S, long lds) {
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npos; p += gridDim.x * blockDim.x) {
+        const long long base = sptr[p >> 5] + (p & 31);
+        const int ne = cnt[p];
         double acc = 0.0;
-        for (long long e = ptr[p]; e < ptr[p + 1]; ++e) acc += ev[e] * w[ej[e]];
+        for (int e = 0; e < ne; ++e) acc += ev[base + 32LL * e] * w[ej[base + 32LL * e]];
         acc *= dA;
         const int r = pr[p], c = pc[p];
         S[(size_t) r + (size_t) c * lds] += acc;
@@ -476,9 +479,10 @@ void SdpDevice::upload(int n_, int m_, const HostCoeff &C, const std::vector<Hos
                     cnt[base + r] = k;
                 }
             }
-            // used positions and their entry offsets
-            std::vector<int> p2r, p2c;
-            std::vector<long long> p2ptr{0}, pslot(npack, -1);
+            // used positions, then the sliced layout: slices of 32 positions padded to
+            // their longest list; entry e of lane l at sptr[slice] + 32 e + l
+            std::vector<int> p2r, p2c, pc2;
+            std::vector<long long> pslot(npack, -1);
             for (int c = 0; c < n; ++c)
                 for (int r = c; r < n; ++r) {
                     const long long q = colbase(c) + r;
@@ -486,38 +490,46 @@ void SdpDevice::upload(int n_, int m_, const HostCoeff &C, const std::vector<Hos
                     pslot[q] = (long long) p2r.size();
                     p2r.push_back(r);
                     p2c.push_back(c);
-                    p2ptr.push_back(p2ptr.back() + cnt[q]);
+                    pc2.push_back(cnt[q]);
                 }
-            std::vector<int> e2j(p2ptr.back());
-            std::vector<double> e2v(p2ptr.back());
-            // pass 2: fill in constraint order
+            npos2 = (int) p2r.size();
+            const int nslice = (npos2 + 31) / 32;
+            std::vector<long long> sptr(nslice + 1, 0);
+            for (int sl = 0; sl < nslice; ++sl) {
+                int kmax = 0;
+                for (int q = sl * 32; q < std::min(npos2, sl * 32 + 32); ++q) kmax = std::max(kmax, pc2[q]);
+                sptr[sl + 1] = sptr[sl] + 32LL * kmax;
+            }
+            std::vector<int> s2j(sptr[nslice], 0);
+            std::vector<double> s2v(sptr[nslice], 0.0);
+            // pass 2: fill in constraint order, straight into the sliced layout
 #pragma omp parallel for schedule(dynamic, 8)
             for (int c = 0; c < n; ++c) {
                 const long long base = colbase(c);
                 for (int r = c; r < n; ++r) {
                     const long long slot = pslot[base + r];
                     if (slot < 0) continue;
-                    long long at = p2ptr[slot];
+                    long long at = sptr[slot >> 5] + (slot & 31);
                     int x = rptr[r], xe = rptr[r + 1], y = rptr[c], ye = rptr[c + 1];
                     while (x < xe && y < ye) {
                         if (rj[x] < rj[y]) ++x;
                         else if (rj[x] > rj[y]) ++y;
                         else {
-                            e2j[at] = rj[x];
-                            e2v[at] = sgn[rj[x]] * ra[x] * ra[y];
-                            ++at;
+                            s2j[at] = rj[x];
+                            s2v[at] = sgn[rj[x]] * ra[x] * ra[y];
+                            at += 32;
                             ++x;
                             ++y;
                         }
                     }
                 }
             }
-            npos2 = (int) p2r.size();
             pos2_r = upload_vec(p2r, s);
             pos2_c = upload_vec(p2c, s);
-            pos2_ptr = upload_vec(p2ptr, s);
-            ent2_j = upload_vec(e2j, s);
-            ent2_v = upload_vec(e2v, s);
+            pos2_cnt = upload_vec(pc2, s);
+            pos2_ptr = upload_vec(sptr, s);
+            ent2_j = upload_vec(s2j, s);
+            ent2_v = upload_vec(s2v, s);
             r1d_gather = true;
         }
     }
@@ -542,8 +554,8 @@ void SdpDevice::release() {
     for (double *p : dr_mat) f(p);
     dr_mat.clear();
     f(pos_r); f(pos_c); f(pos_ptr); f(ent_j); f(ent_v);
-    f(pos2_r); f(pos2_c); f(pos2_ptr); f(ent2_j); f(ent2_v);
-    pos2_r = pos2_c = ent2_j = nullptr;
+    f(pos2_r); f(pos2_c); f(pos2_cnt); f(pos2_ptr); f(ent2_j); f(ent2_v);
+    pos2_r = pos2_c = pos2_cnt = ent2_j = nullptr;
     pos2_ptr = nullptr;
     ent2_v = nullptr;
     npos2 = 0;
@@ -566,8 +578,8 @@ void SdpDevice::assemble(double dC, double dA, const double *d_wvec, double dEye
         if (npos > 0)
             s_gather_kernel<<<hb::counted(grid1(npos)), 256, 0, s>>>(npos, pos_r, pos_c, pos_ptr, ent_j, ent_v, d_wvec, dA, S, ldS);
         if (nr1d > 0 && r1d_gather) {
-            s_gather2_kernel<<<hb::counted(grid1(npos2)), 256, 0, s>>>(npos2, pos2_r, pos2_c, pos2_ptr, ent2_j,
-                                                                       ent2_v, d_wvec, dA, S, ldS);
+            s_gather2_kernel<<<hb::counted(grid1(npos2)), 256, 0, s>>>(npos2, pos2_r, pos2_c, pos2_ptr, pos2_cnt,
+                                                                       ent2_j, ent2_v, d_wvec, dA, S, ldS);
         } else if (nr1d > 0) {
             r1d_weights_kernel<<<hb::counted(grid1(nr1d)), 256, 0, s>>>(nr1d, r1d_id, r1d_sign, d_wvec, dA, d_w);
             scale_columns(s, n, nr1d, A1, ld, d_w, V, ld);

@@ -74,8 +74,10 @@ struct SdpDevice {
     // (constraint, s_i a_ip a_iq), in constraint order
     bool r1d_gather = false;
     double t_upload_map = 0.0, t_upload_total = 0.0;  // host seconds spent in upload()
+    // sliced layout: positions in slices of 32; entry e of the slice's lane l sits at
+    // slice_ptr[slice] + 32 e + l (slices padded to their longest list, pos2_cnt per position)
     int npos2 = 0;
-    int *pos2_r = nullptr, *pos2_c = nullptr;
+    int *pos2_r = nullptr, *pos2_c = nullptr, *pos2_cnt = nullptr;
     long long *pos2_ptr = nullptr;
     int *ent2_j = nullptr;
     double *ent2_v = nullptr;

@@ -135,7 +135,8 @@ extern int hdsdpb_split_gemm( int M, int N, int K, const double *A, int lda, int
 /* Device-resident timing of one kernel family on an n x n problem (CUDA events
    on the launching stream, 2 warm-up calls): 0 GEMM NN, 1 GEMM TN lower,
    2 Cholesky, 3 triangular inverse L^-1, 4 matrix-vector product,
-   5 Lanczos step bound, 6 rank-64 SYRK update. Writes milliseconds per call. */
+   5 Lanczos step bound, 6 rank-64 SYRK update, 7 Cholesky that also forms L^-1,
+   8 Cholesky without it. Writes milliseconds per call. */
 extern int hdsdpb_kernel_timing( int which, int n, int reps, double *ms );
 
 /* Milliseconds taken by `reps` grid-wide barriers in one cooperative launch of
