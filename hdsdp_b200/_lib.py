@@ -22,7 +22,7 @@ EXPORTS = [
     "HDSDPGetStatus", "HDSDPGetIterCount", "HDSDPSetPrimalRefinement", "HDSDPSetPrecision",
     "HDSDPGetIterLog", "HDSDPGetTimers", "HDSDPAdjoint",
     "hdsdpb_schur_probe", "hdsdpb_ratio_probe", "hdsdpb_cholesky", "hdsdpb_cholesky_noalloc", "hdsdpb_inverse", "hdsdpb_gemm",
-    "hdsdpb_kernel_timing", "hdsdpb_gridsync_probe", "hdsdpb_launch_count",
+    "hdsdpb_kernel_timing", "hdsdpb_gridsync_probe", "hdsdpb_launch_count", "hdsdpb_release_cached_memory",
     "hdsdpb_kstat_enable", "hdsdpb_kstat_read", "hdsdpb_split_gemm",
 ]
 
@@ -73,6 +73,7 @@ def load():
         "hdsdpb_kernel_timing": ([i, i, i, dp], i),
         "hdsdpb_gridsync_probe": ([i, i, dp], i),
         "hdsdpb_launch_count": ([], C.c_longlong),
+        "hdsdpb_release_cached_memory": ([], None),
         "hdsdpb_kstat_enable": ([i], i),
         "hdsdpb_split_gemm": ([i, i, i, dp, i, i, dp, i, i, dp, i], i),
         "hdsdpb_kstat_read": ([i, C.POINTER(C.c_longlong), dp, dp], i),

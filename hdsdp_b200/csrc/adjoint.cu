@@ -76,10 +76,10 @@ struct AdjointState {
 
     void release() {
         for (double *p : {X, S, N, T1, T2, Y, Z, P, D, M, d_u, d_v, d_t, d_r, d_y, d_scal, d_gax})
-            if (p) cudaFree(p);
+            if (p) hb::cache_free(p);
         for (int *p : {d_col, d_ri, d_ci})
-            if (p) cudaFree(p);
-        if (h_scal) cudaFreeHost(h_scal);
+            if (p) hb::cache_free(p);
+        if (h_scal) hb::cache_free_host(h_scal);
         X = S = N = T1 = T2 = Y = Z = P = D = M = d_u = d_v = d_t = d_r = d_y = d_scal = d_gax = nullptr;
         d_col = d_ri = d_ci = nullptr;
         h_scal = nullptr;
@@ -129,11 +129,11 @@ hdsdp_retcode prepare(hdsdp *h, AdjointState &a) {
     a.ld = ld;
     a.ldm = ldm;
     for (double **p : {&a.X, &a.S, &a.N, &a.T1, &a.T2, &a.Y, &a.Z, &a.P, &a.D})
-        HB_CUDA(cudaMalloc(p, sizeof(double) * ld * n));
-    HB_CUDA(cudaMalloc(&a.M, sizeof(double) * ldm * m));
-    for (double **p : {&a.d_u, &a.d_v, &a.d_t, &a.d_r, &a.d_y}) HB_CUDA(cudaMalloc(p, sizeof(double) * (m + 1)));
-    HB_CUDA(cudaMalloc(&a.d_scal, sizeof(double) * 4));
-    HB_CUDA(cudaMallocHost(&a.h_scal, sizeof(double) * 4));
+        HB_CUDA(hb::cmalloc(p, sizeof(double) * ld * n));
+    HB_CUDA(hb::cmalloc(&a.M, sizeof(double) * ldm * m));
+    for (double **p : {&a.d_u, &a.d_v, &a.d_t, &a.d_r, &a.d_y}) HB_CUDA(hb::cmalloc(p, sizeof(double) * (m + 1)));
+    HB_CUDA(hb::cmalloc(&a.d_scal, sizeof(double) * 4));
+    HB_CUDA(hb::cmalloc_host(&a.h_scal, sizeof(double) * 4));
     a.FS.alloc(n);
     a.FM.alloc(m, 1);
     if (device_error_flag()) return HDSDP_RETCODE_MEMORY;
@@ -222,10 +222,10 @@ hdsdp_retcode prepare(hdsdp *h, AdjointState &a) {
             ri[e] = (int) (p - start[j] + j);
         }
     if (a.nnz > 0) {
-        HB_CUDA(cudaMalloc(&a.d_col, sizeof(int) * a.nnz));
-        HB_CUDA(cudaMalloc(&a.d_ri, sizeof(int) * a.nnz));
-        HB_CUDA(cudaMalloc(&a.d_ci, sizeof(int) * a.nnz));
-        HB_CUDA(cudaMalloc(&a.d_gax, sizeof(double) * a.nnz));
+        HB_CUDA(hb::cmalloc(&a.d_col, sizeof(int) * a.nnz));
+        HB_CUDA(hb::cmalloc(&a.d_ri, sizeof(int) * a.nnz));
+        HB_CUDA(hb::cmalloc(&a.d_ci, sizeof(int) * a.nnz));
+        HB_CUDA(hb::cmalloc(&a.d_gax, sizeof(double) * a.nnz));
         HB_CUDA(cudaMemcpyAsync(a.d_col, col.data(), sizeof(int) * a.nnz, cudaMemcpyHostToDevice, s));
         HB_CUDA(cudaMemcpyAsync(a.d_ri, ri.data(), sizeof(int) * a.nnz, cudaMemcpyHostToDevice, s));
         HB_CUDA(cudaMemcpyAsync(a.d_ci, ci.data(), sizeof(int) * a.nnz, cudaMemcpyHostToDevice, s));

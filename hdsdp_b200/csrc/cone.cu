@@ -315,31 +315,31 @@ hdsdp_retcode SdpCone::setup_device(cudaStream_t stream, Timers *t) {
     for (double &v : Cdev.v) v *= objScal;
     dev.precision = precision;
     dev.upload(n, m, Cdev, A, s);
-    HB_CUDA(cudaMalloc(&Svar, sizeof(double) * ld * n));
-    HB_CUDA(cudaMalloc(&Scheck, sizeof(double) * ld * n));
-    HB_CUDA(cudaMalloc(&dS, sizeof(double) * ld * n));
-    HB_CUDA(cudaMalloc(&W, sizeof(double) * ld * n));
+    HB_CUDA(hb::cmalloc(&Svar, sizeof(double) * ld * n));
+    HB_CUDA(hb::cmalloc(&Scheck, sizeof(double) * ld * n));
+    HB_CUDA(hb::cmalloc(&dS, sizeof(double) * ld * n));
+    HB_CUDA(hb::cmalloc(&W, sizeof(double) * ld * n));
     HB_CUDA(cudaMemsetAsync(Svar, 0, sizeof(double) * ld * n, s));
     HB_CUDA(cudaMemsetAsync(Scheck, 0, sizeof(double) * ld * n, s));
     HB_CUDA(cudaMemsetAsync(dS, 0, sizeof(double) * ld * n, s));
     Fvar.alloc(n);
     Fcheck.alloc(n);
     lz.init(n, s);
-    HB_CUDA(cudaMalloc(&d_y, sizeof(double) * std::max(m, 1)));
-    HB_CUDA(cudaMalloc(&d_vec, sizeof(double) * std::max(m, 1)));
-    HB_CUDA(cudaMallocHost(&h_vec, sizeof(double) * std::max(m, 1)));
-    HB_CUDA(cudaMalloc(&d_scal, sizeof(double) * 8));
-    HB_CUDA(cudaMallocHost(&h_scal, sizeof(double) * 8));
+    HB_CUDA(hb::cmalloc(&d_y, sizeof(double) * std::max(m, 1)));
+    HB_CUDA(hb::cmalloc(&d_vec, sizeof(double) * std::max(m, 1)));
+    HB_CUDA(hb::cmalloc_host(&h_vec, sizeof(double) * std::max(m, 1)));
+    HB_CUDA(hb::cmalloc(&d_scal, sizeof(double) * 8));
+    HB_CUDA(hb::cmalloc_host(&h_scal, sizeof(double) * 8));
     HB_CUDA(cudaStreamSynchronize(s));
     return device_error_flag() ? HDSDP_RETCODE_MEMORY : HDSDP_RETCODE_OK;
 }
 
 void SdpCone::release() {
     dev.release();
-    auto f = [](void *p) { if (p) cudaFree(p); };
+    auto f = [](void *p) { if (p) hb::cache_free(p); };
     f(Svar); f(Scheck); f(dS); f(W); f(d_y); f(d_vec); f(d_scal);
-    if (h_vec) cudaFreeHost(h_vec);
-    if (h_scal) cudaFreeHost(h_scal);
+    if (h_vec) hb::cache_free_host(h_vec);
+    if (h_scal) hb::cache_free_host(h_scal);
     Svar = Scheck = dS = W = d_y = d_vec = d_scal = h_vec = h_scal = nullptr;
     Fvar.release();
     Fcheck.release();
@@ -377,8 +377,8 @@ static void copy_factor(cudaStream_t s, DenseFactor &dst, const DenseFactor &src
     HB_CUDA(cudaMemcpyAsync(dst.Dinv, src.Dinv, sizeof(double) * src.ld * 64, cudaMemcpyDeviceToDevice, s));
     dst.k_valid = false;
     if (src.k_valid && src.K && src.KT) {
-        if (!dst.K) HB_CUDA(cudaMalloc(&dst.K, sizeof(double) * dst.ld * dst.n));
-        if (!dst.KT) HB_CUDA(cudaMalloc(&dst.KT, sizeof(double) * dst.ld * dst.n));
+        if (!dst.K) HB_CUDA(hb::cmalloc(&dst.K, sizeof(double) * dst.ld * dst.n));
+        if (!dst.KT) HB_CUDA(hb::cmalloc(&dst.KT, sizeof(double) * dst.ld * dst.n));
         HB_CUDA(cudaMemcpyAsync(dst.K, src.K, sizeof(double) * src.ld * src.n, cudaMemcpyDeviceToDevice, s));
         HB_CUDA(cudaMemcpyAsync(dst.KT, src.KT, sizeof(double) * src.ld * src.n, cudaMemcpyDeviceToDevice, s));
         dst.k_valid = true;
@@ -623,26 +623,26 @@ void KKT::init(int m_, cudaStream_t stream, Timers *t) {
     s = stream;
     tm = t;
     ldm = pad_ld(m);
-    HB_CUDA(cudaMalloc(&M, sizeof(double) * ldm * m));
+    HB_CUDA(hb::cmalloc(&M, sizeof(double) * ldm * m));
     HB_CUDA(cudaMemsetAsync(M, 0, sizeof(double) * ldm * m, s));
     F.alloc(m, 1);  // the Schur solves always use K
     asinv.assign(m, 0.0);
     asinvrd.assign(m, 0.0);
     asinvcs.assign(m, 0.0);
     diag_add.assign(m, 0.0);
-    for (double **p : {&d_rhs, &d_x, &d_r, &d_t, &d_diag}) HB_CUDA(cudaMalloc(p, sizeof(double) * m));
-    HB_CUDA(cudaMallocHost(&h_buf, sizeof(double) * m));
+    for (double **p : {&d_rhs, &d_x, &d_r, &d_t, &d_diag}) HB_CUDA(hb::cmalloc(p, sizeof(double) * m));
+    HB_CUDA(hb::cmalloc_host(&h_buf, sizeof(double) * m));
 }
 
 void KKT::release() {
-    if (M) cudaFree(M);
+    if (M) hb::cache_free(M);
     M = nullptr;
     F.release();
     for (double **p : {&d_rhs, &d_x, &d_r, &d_t, &d_diag}) {
-        if (*p) cudaFree(*p);
+        if (*p) hb::cache_free(*p);
         *p = nullptr;
     }
-    if (h_buf) cudaFreeHost(h_buf);
+    if (h_buf) hb::cache_free_host(h_buf);
     h_buf = nullptr;
 }
 
@@ -975,13 +975,13 @@ void Lanczos::init(int n_, cudaStream_t s_) {
     n = n_;
     s = s_;
     ld = pad_ld(n);
-    HB_CUDA(cudaMalloc(&V, sizeof(double) * ld * (maxdim + 1)));
-    for (double **p : {&w, &z1, &z2, &t1, &u, &warm, &init_vec, &pert_vec}) HB_CUDA(cudaMalloc(p, sizeof(double) * ld));
-    HB_CUDA(cudaMalloc(&d_ab, sizeof(double) * (2 * maxdim + 2)));
-    HB_CUDA(cudaMallocHost(&h_ab, sizeof(double) * (2 * maxdim + 2)));
-    HB_CUDA(cudaMalloc(&d_y, sizeof(double) * 2 * (maxdim + 1)));
-    HB_CUDA(cudaMalloc(&d_scal, sizeof(double) * 4));
-    HB_CUDA(cudaMallocHost(&h_scal, sizeof(double) * 4));
+    HB_CUDA(hb::cmalloc(&V, sizeof(double) * ld * (maxdim + 1)));
+    for (double **p : {&w, &z1, &z2, &t1, &u, &warm, &init_vec, &pert_vec}) HB_CUDA(hb::cmalloc(p, sizeof(double) * ld));
+    HB_CUDA(hb::cmalloc(&d_ab, sizeof(double) * (2 * maxdim + 2)));
+    HB_CUDA(hb::cmalloc_host(&h_ab, sizeof(double) * (2 * maxdim + 2)));
+    HB_CUDA(hb::cmalloc(&d_y, sizeof(double) * 2 * (maxdim + 1)));
+    HB_CUDA(hb::cmalloc(&d_scal, sizeof(double) * 4));
+    HB_CUDA(hb::cmalloc_host(&h_scal, sizeof(double) * 4));
     // Deterministic start and perturbation vectors: srand(n) then, per entry,
     // srand(rand()) and sqrt(sqrt(rand() % 1627)) * (rand() % 2 - 0.5)
     // (HLanczosIPrepare / HLanczosIPerturb, linalg/hdsdp_lanczos.c:33-53).
@@ -1007,11 +1007,11 @@ void Lanczos::init(int n_, cudaStream_t s_) {
 
 void Lanczos::release() {
     for (double **p : {&V, &w, &z1, &z2, &t1, &u, &warm, &init_vec, &pert_vec, &d_ab, &d_y, &d_scal}) {
-        if (*p) cudaFree(*p);
+        if (*p) hb::cache_free(*p);
         *p = nullptr;
     }
-    if (h_ab) cudaFreeHost(h_ab);
-    if (h_scal) cudaFreeHost(h_scal);
+    if (h_ab) hb::cache_free_host(h_ab);
+    if (h_scal) hb::cache_free_host(h_scal);
     h_ab = h_scal = nullptr;
 }
 

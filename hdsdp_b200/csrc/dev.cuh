@@ -41,6 +41,26 @@ void kstat_begin(int family, cudaStream_t s, double work);
 void kstat_end(cudaStream_t s);
 int kstat_read(int family, long long *launches, double *ms, double *work);
 
+// Caching allocator for the library's device and pinned host buffers: a freed block
+// goes to a free list keyed by its exact size and is handed out again to the next
+// request of that size, so consecutive solvers (and per-call scratch) do not go back to
+// the driver. hdsdpb_release_cached_memory() returns the cached blocks. A block is only
+// freed here after the stream work that uses it has been synchronised, so a block handed
+// out again is never still in use.
+cudaError_t cache_malloc(void **p, size_t bytes);
+void cache_free(void *p);
+cudaError_t cache_malloc_host(void **p, size_t bytes);
+void cache_free_host(void *p);
+void cache_release();
+template <class T>
+inline cudaError_t cmalloc(T **p, size_t bytes) {
+    return cache_malloc((void **) p, bytes);
+}
+template <class T>
+inline cudaError_t cmalloc_host(T **p, size_t bytes) {
+    return cache_malloc_host((void **) p, bytes);
+}
+
 // Leading dimensions are padded to a multiple of 32 doubles (256 bytes) so that
 // every column starts on a 256-byte boundary.
 inline long pad_ld(long n) { return ((n + 31) / 32) * 32; }

@@ -43,6 +43,11 @@ void HDSDPGetTimers(hdsdp *h, double out[23]) {
 
 long long hdsdpb_launch_count(void) { return hb::launch_counter(); }
 
+void hdsdpb_release_cached_memory(void) {
+    cudaDeviceSynchronize();
+    hb::cache_release();
+}
+
 int hdsdpb_kstat_enable(int mask) {
     hb::kstat_enable(mask);
     return 0;
@@ -126,8 +131,8 @@ int hdsdpb_cholesky(int n, const double *S, double *L, double *logdiag) {
     if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return -1;
     const long ld = pad_ld(n);
     double *dS = nullptr, *dl = nullptr;
-    cudaMalloc(&dS, sizeof(double) * ld * n);
-    cudaMalloc(&dl, sizeof(double));
+    hb::cmalloc(&dS, sizeof(double) * ld * n);
+    hb::cmalloc(&dl, sizeof(double));
     cudaMemcpy2D(dS, sizeof(double) * ld, S, sizeof(double) * n, sizeof(double) * n, n, cudaMemcpyHostToDevice);
     DenseFactor F;
     F.alloc(n);
@@ -145,8 +150,8 @@ int hdsdpb_cholesky(int n, const double *S, double *L, double *logdiag) {
     }
     cudaStreamSynchronize(s);
     F.release();
-    cudaFree(dS);
-    cudaFree(dl);
+    hb::cache_free(dS);
+    hb::cache_free(dl);
     cudaStreamDestroy(s);
     if (device_error_flag()) return -1;
     return ok ? 0 : 1;
@@ -159,8 +164,8 @@ int hdsdpb_inverse(int n, const double *S, double *Sinv) {
     if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return -1;
     const long ld = pad_ld(n);
     double *dS = nullptr, *dW = nullptr;
-    cudaMalloc(&dS, sizeof(double) * ld * n);
-    cudaMalloc(&dW, sizeof(double) * ld * n);
+    hb::cmalloc(&dS, sizeof(double) * ld * n);
+    hb::cmalloc(&dW, sizeof(double) * ld * n);
     cudaMemcpy2D(dS, sizeof(double) * ld, S, sizeof(double) * n, sizeof(double) * n, n, cudaMemcpyHostToDevice);
     DenseFactor F;
     F.alloc(n);
@@ -172,8 +177,8 @@ int hdsdpb_inverse(int n, const double *S, double *Sinv) {
     }
     cudaStreamSynchronize(s);
     F.release();
-    cudaFree(dS);
-    cudaFree(dW);
+    hb::cache_free(dS);
+    hb::cache_free(dW);
     cudaStreamDestroy(s);
     if (device_error_flag()) return -1;
     return ok ? 0 : 1;
@@ -189,18 +194,18 @@ int hdsdpb_gemm(int M, int N, int K, double alpha, const double *A, int lda, int
     cudaStream_t s;
     if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return -1;
     double *dA = nullptr, *dB = nullptr, *dC = nullptr;
-    cudaMalloc(&dA, sizeof(double) * (size_t) lda * ac);
-    cudaMalloc(&dB, sizeof(double) * (size_t) ldb * bc);
-    cudaMalloc(&dC, sizeof(double) * (size_t) ldc * N);
+    hb::cmalloc(&dA, sizeof(double) * (size_t) lda * ac);
+    hb::cmalloc(&dB, sizeof(double) * (size_t) ldb * bc);
+    hb::cmalloc(&dC, sizeof(double) * (size_t) ldc * N);
     cudaMemcpy(dA, A, sizeof(double) * (size_t) lda * ac, cudaMemcpyHostToDevice);
     cudaMemcpy(dB, B, sizeof(double) * (size_t) ldb * bc, cudaMemcpyHostToDevice);
     cudaMemcpy(dC, C, sizeof(double) * (size_t) ldc * N, cudaMemcpyHostToDevice);
     gemm(s, M, N, K, alpha, dA, lda, transA, dB, ldb, transB, beta, dC, ldc, 0);
     cudaMemcpyAsync(C, dC, sizeof(double) * (size_t) ldc * N, cudaMemcpyDeviceToHost, s);
     cudaStreamSynchronize(s);
-    cudaFree(dA);
-    cudaFree(dB);
-    cudaFree(dC);
+    hb::cache_free(dA);
+    hb::cache_free(dB);
+    hb::cache_free(dC);
     cudaStreamDestroy(s);
     return device_error_flag() ? -1 : 0;
 }
@@ -215,9 +220,9 @@ int hdsdpb_split_gemm(int M, int N, int K, const double *A, int lda, int transA,
     cudaStream_t s;
     if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return -1;
     double *dA = nullptr, *dB = nullptr, *dC = nullptr;
-    HB_CUDA(cudaMalloc(&dA, sizeof(double) * (size_t) lda * (ac > 0 ? ac : 1)));
-    HB_CUDA(cudaMalloc(&dB, sizeof(double) * (size_t) ldb * (bc > 0 ? bc : 1)));
-    HB_CUDA(cudaMalloc(&dC, sizeof(double) * (size_t) ldc * N));
+    HB_CUDA(hb::cmalloc(&dA, sizeof(double) * (size_t) lda * (ac > 0 ? ac : 1)));
+    HB_CUDA(hb::cmalloc(&dB, sizeof(double) * (size_t) ldb * (bc > 0 ? bc : 1)));
+    HB_CUDA(hb::cmalloc(&dC, sizeof(double) * (size_t) ldc * N));
     HB_CUDA(cudaMemcpy(dA, A, sizeof(double) * (size_t) lda * ac, cudaMemcpyHostToDevice));
     HB_CUDA(cudaMemcpy(dB, B, sizeof(double) * (size_t) ldb * bc, cudaMemcpyHostToDevice));
     HB_CUDA(cudaMemset(dC, 0, sizeof(double) * (size_t) ldc * N));
@@ -241,9 +246,9 @@ int hdsdpb_split_gemm(int M, int N, int K, const double *A, int lda, int transA,
     if (ret == 0) HB_CUDA(cudaMemcpy(C, dC, sizeof(double) * (size_t) ldc * N, cudaMemcpyDeviceToHost));
     opA.release();
     opB.release();
-    cudaFree(dA);
-    cudaFree(dB);
-    cudaFree(dC);
+    hb::cache_free(dA);
+    hb::cache_free(dB);
+    hb::cache_free(dC);
     cudaStreamDestroy(s);
     if (device_error_flag()) return -1;
     return ret;
@@ -272,11 +277,11 @@ extern "C" int hdsdpb_kernel_timing(int which, int n, int reps, double *ms) {
     if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return -1;
     const long ld = pad_ld(n);
     double *A = nullptr, *B = nullptr, *Cm = nullptr, *x = nullptr, *y = nullptr;
-    cudaMalloc(&A, sizeof(double) * ld * n);
-    cudaMalloc(&B, sizeof(double) * ld * n);
-    cudaMalloc(&Cm, sizeof(double) * ld * n);
-    cudaMalloc(&x, sizeof(double) * ld);
-    cudaMalloc(&y, sizeof(double) * ld);
+    hb::cmalloc(&A, sizeof(double) * ld * n);
+    hb::cmalloc(&B, sizeof(double) * ld * n);
+    hb::cmalloc(&Cm, sizeof(double) * ld * n);
+    hb::cmalloc(&x, sizeof(double) * ld);
+    hb::cmalloc(&y, sizeof(double) * ld);
     fill_spd_kernel<<<hb::counted(1024), 256, 0, s>>>(n, A, ld, 1u);
     fill_spd_kernel<<<hb::counted(1024), 256, 0, s>>>(n, B, ld, 7u);
     fill(s, x, 1.0, n);
@@ -314,7 +319,7 @@ extern "C" int hdsdpb_kernel_timing(int which, int n, int reps, double *ms) {
     cudaEventDestroy(e1);
     if (which == 5) lz.release();
     F.release();
-    for (double *p : {A, B, Cm, x, y}) cudaFree(p);
+    for (double *p : {A, B, Cm, x, y}) hb::cache_free(p);
     cudaStreamDestroy(s);
     return device_error_flag() ? -1 : 0;
 }
@@ -330,7 +335,7 @@ __global__ void gridsync_probe_kernel(int reps, int *sink) {
 // Milliseconds for `reps` grid-wide barriers of a cooperative launch of `blocks` x 256 threads.
 extern "C" int hdsdpb_gridsync_probe(int blocks, int reps, double *ms) {
     int *sink = nullptr;
-    cudaMalloc(&sink, sizeof(int));
+    hb::cmalloc(&sink, sizeof(int));
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
@@ -342,7 +347,7 @@ extern "C" int hdsdpb_gridsync_probe(int blocks, int reps, double *ms) {
     float t = 0.f;
     cudaEventElapsedTime(&t, e0, e1);
     *ms = t;
-    cudaFree(sink);
+    hb::cache_free(sink);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     return e == cudaSuccess ? 0 : -1;

@@ -6,6 +6,8 @@
 // GEMM plus small 64 x 64 kernels.
 #include "la.h"
 #include <vector>
+#include <mutex>
+#include <unordered_map>
 #include <cmath>
 #include <algorithm>
 
@@ -14,6 +16,108 @@ namespace hb {
 int &device_error_flag() {
     static int flag = 0;
     return flag;
+}
+
+namespace {
+struct BlockCache {
+    std::mutex mu;
+    std::unordered_map<size_t, std::vector<void *>> free_dev, free_host;
+    std::unordered_map<void *, size_t> size_dev, size_host;
+};
+BlockCache &block_cache() {
+    static BlockCache *c = new BlockCache();  // never destroyed: frees may run during exit
+    return *c;
+}
+}  // namespace
+
+cudaError_t cache_malloc(void **p, size_t bytes) {
+    BlockCache &c = block_cache();
+    if (bytes == 0) bytes = 1;
+    {
+        std::lock_guard<std::mutex> g(c.mu);
+        auto it = c.free_dev.find(bytes);
+        if (it != c.free_dev.end() && !it->second.empty()) {
+            *p = it->second.back();
+            it->second.pop_back();
+            return cudaSuccess;
+        }
+    }
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e == cudaErrorMemoryAllocation) {
+        cudaGetLastError();
+        cache_release();
+        e = cudaMalloc(p, bytes);
+    }
+    if (e == cudaSuccess) {
+        std::lock_guard<std::mutex> g(c.mu);
+        c.size_dev[*p] = bytes;
+    } else {
+        *p = nullptr;
+    }
+    return e;
+}
+
+void cache_free(void *p) {
+    if (!p) return;
+    BlockCache &c = block_cache();
+    std::lock_guard<std::mutex> g(c.mu);
+    auto it = c.size_dev.find(p);
+    if (it == c.size_dev.end()) {
+        cudaFree(p);  // not ours: hand it back directly
+        return;
+    }
+    c.free_dev[it->second].push_back(p);
+}
+
+cudaError_t cache_malloc_host(void **p, size_t bytes) {
+    BlockCache &c = block_cache();
+    if (bytes == 0) bytes = 1;
+    {
+        std::lock_guard<std::mutex> g(c.mu);
+        auto it = c.free_host.find(bytes);
+        if (it != c.free_host.end() && !it->second.empty()) {
+            *p = it->second.back();
+            it->second.pop_back();
+            return cudaSuccess;
+        }
+    }
+    cudaError_t e = cudaMallocHost(p, bytes);
+    if (e == cudaSuccess) {
+        std::lock_guard<std::mutex> g(c.mu);
+        c.size_host[*p] = bytes;
+    } else {
+        *p = nullptr;
+    }
+    return e;
+}
+
+void cache_free_host(void *p) {
+    if (!p) return;
+    BlockCache &c = block_cache();
+    std::lock_guard<std::mutex> g(c.mu);
+    auto it = c.size_host.find(p);
+    if (it == c.size_host.end()) {
+        cudaFreeHost(p);
+        return;
+    }
+    c.free_host[it->second].push_back(p);
+}
+
+void cache_release() {
+    BlockCache &c = block_cache();
+    std::lock_guard<std::mutex> g(c.mu);
+    for (auto &kv : c.free_dev)
+        for (void *q : kv.second) {
+            cudaFree(q);
+            c.size_dev.erase(q);
+        }
+    for (auto &kv : c.free_host)
+        for (void *q : kv.second) {
+            cudaFreeHost(q);
+            c.size_host.erase(q);
+        }
+    c.free_dev.clear();
+    c.free_host.clear();
 }
 
 long long &launch_counter() {
@@ -654,29 +758,29 @@ int grid_for(long total, int threads = 256) {
 void DenseFactor::alloc(int n_, int fuse_inverse) {
     n = n_;
     ld = pad_ld(n);
-    HB_CUDA(cudaMalloc(&L, sizeof(double) * ld * n));
-    HB_CUDA(cudaMalloc(&Dinv, sizeof(double) * ld * NB));
-    HB_CUDA(cudaMalloc(&d_info, sizeof(int)));
-    HB_CUDA(cudaMallocHost(&h_info, sizeof(int)));
+    HB_CUDA(hb::cmalloc(&L, sizeof(double) * ld * n));
+    HB_CUDA(hb::cmalloc(&Dinv, sizeof(double) * ld * NB));
+    HB_CUDA(hb::cmalloc(&d_info, sizeof(int)));
+    HB_CUDA(hb::cmalloc_host(&h_info, sizeof(int)));
     *h_info = 0;
     HB_CUDA(cudaMemset(L, 0, sizeof(double) * ld * n));
     HB_CUDA(cudaMemset(Dinv, 0, sizeof(double) * ld * NB));
     fuse_k = (fuse_inverse < 0) ? (n <= kFuseInverseMax) : (fuse_inverse != 0);
     if (fuse_k) {
-        HB_CUDA(cudaMalloc(&K, sizeof(double) * ld * n));
-        HB_CUDA(cudaMalloc(&KT, sizeof(double) * ld * n));
+        HB_CUDA(hb::cmalloc(&K, sizeof(double) * ld * n));
+        HB_CUDA(hb::cmalloc(&KT, sizeof(double) * ld * n));
         HB_CUDA(cudaMemset(K, 0, sizeof(double) * ld * n));
         HB_CUDA(cudaMemset(KT, 0, sizeof(double) * ld * n));
     }
 }
 
 void DenseFactor::release() {
-    if (L) cudaFree(L);
-    if (Dinv) cudaFree(Dinv);
-    if (K) cudaFree(K);
-    if (KT) cudaFree(KT);
-    if (d_info) cudaFree(d_info);
-    if (h_info) cudaFreeHost(h_info);
+    if (L) hb::cache_free(L);
+    if (Dinv) hb::cache_free(Dinv);
+    if (K) hb::cache_free(K);
+    if (KT) hb::cache_free(KT);
+    if (d_info) hb::cache_free(d_info);
+    if (h_info) hb::cache_free_host(h_info);
     L = Dinv = K = KT = nullptr;
     d_info = nullptr;
     h_info = nullptr;
@@ -747,8 +851,8 @@ void compute_inverse_factor(cudaStream_t s, DenseFactor &F) {
     ensure_attrs();
     if (F.k_valid) return;
     const int n = F.n;
-    if (!F.K) HB_CUDA(cudaMalloc(&F.K, sizeof(double) * F.ld * n));
-    if (!F.KT) HB_CUDA(cudaMalloc(&F.KT, sizeof(double) * F.ld * n));
+    if (!F.K) HB_CUDA(hb::cmalloc(&F.K, sizeof(double) * F.ld * n));
+    if (!F.KT) HB_CUDA(hb::cmalloc(&F.KT, sizeof(double) * F.ld * n));
     if (coop_inverse_enqueue(s, F)) {
         transpose(s, n, F.K, F.ld, F.KT, F.ld);
         F.k_valid = true;
@@ -978,7 +1082,7 @@ void scale_columns(cudaStream_t s, int rows, int cols, const double *A, long lda
 void frob_dot(cudaStream_t s, int n, const double *A, long lda, const double *B, long ldb, double *d_out) {
     static double *part = nullptr;
     const int np = 296;
-    if (!part) HB_CUDA(cudaMalloc(&part, sizeof(double) * np));
+    if (!part) HB_CUDA(hb::cmalloc(&part, sizeof(double) * np));
     frob_partial_kernel<<<hb::counted(np), 256, 0, s>>>(n, A, lda, B, ldb, part);
     sum_partials_kernel<<<hb::counted(1), 512, 0, s>>>(np, part, d_out);
 }

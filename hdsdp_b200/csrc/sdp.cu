@@ -21,7 +21,7 @@ template <typename T>
 T *upload_vec(const std::vector<T> &h, cudaStream_t s) {
     if (h.empty()) return nullptr;
     T *d = nullptr;
-    HB_CUDA(cudaMalloc(&d, sizeof(T) * h.size()));
+    HB_CUDA(hb::cmalloc(&d, sizeof(T) * h.size()));
     HB_CUDA(cudaMemcpyAsync(d, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice, s));
     return d;
 }
@@ -289,16 +289,16 @@ void SdpDevice::upload(int n_, int m_, const HostCoeff &C, const std::vector<Hos
     m = m_;
     ld = pad_ld(n);
     stream = s;
-    HB_CUDA(cudaMalloc(&Cfull, sizeof(double) * ld * n));
+    HB_CUDA(hb::cmalloc(&Cfull, sizeof(double) * ld * n));
     HB_CUDA(cudaMemsetAsync(Cfull, 0, sizeof(double) * ld * n, s));
     if (!C.r.empty()) {
         int *dr = upload_vec(C.r, s), *dc = upload_vec(C.c, s);
         double *dv = upload_vec(C.v, s);
         scatter_sym_kernel<<<hb::counted(grid1((long) C.r.size())), 256, 0, s>>>((int) C.r.size(), dr, dc, dv, Cfull, ld);
         HB_CUDA(cudaStreamSynchronize(s));
-        cudaFree(dr);
-        cudaFree(dc);
-        cudaFree(dv);
+        hb::cache_free(dr);
+        hb::cache_free(dc);
+        hb::cache_free(dv);
     }
 
     std::vector<int> spid, spptr{0}, spr, spc;
@@ -376,34 +376,34 @@ void SdpDevice::upload(int n_, int m_, const HostCoeff &C, const std::vector<Hos
             for (size_t t = 0; t < c.aidx.size(); ++t) hA1[(size_t) a * ld + c.aidx[t]] = c.aval[t];
         }
         A1 = upload_vec(hA1, s);
-        HB_CUDA(cudaMalloc(&G, sizeof(double) * pad_ld(nr1d) * nr1d));
+        HB_CUDA(hb::cmalloc(&G, sizeof(double) * pad_ld(nr1d) * nr1d));
         if (precision >= 1) {
             // the factors a_i are fixed: split them once
             bool ok = opA1.alloc(nr1d, n) && opK.alloc(n, n) && opKT.alloc(n, n) && opB.alloc(nr1d, n);
-            HB_CUDA(cudaMalloc(&colsq, sizeof(double) * nr1d));
+            HB_CUDA(hb::cmalloc(&colsq, sizeof(double) * nr1d));
             if (ok) split_from_f64(s, opA1, A1, ld, true);
             else opA1.release();
         }
     }
     const int vcols = std::max(std::max(nr1d, nr1s), 1);
-    HB_CUDA(cudaMalloc(&V, sizeof(double) * ld * vcols));
-    if (nr1d > 0) HB_CUDA(cudaMalloc(&Vt, sizeof(double) * ld * nr1d));
-    if (nr1s > 0 && nsp > 0) HB_CUDA(cudaMalloc(&Vs, sizeof(double) * ld * nr1s));
+    HB_CUDA(hb::cmalloc(&V, sizeof(double) * ld * vcols));
+    if (nr1d > 0) HB_CUDA(hb::cmalloc(&Vt, sizeof(double) * ld * nr1d));
+    if (nr1s > 0 && nsp > 0) HB_CUDA(hb::cmalloc(&Vs, sizeof(double) * ld * nr1s));
 
     ndr = (int) dr_id.size();
     for (int i = 0; i < ndr; ++i) {
         const HostCoeff &c = A[dr_id[i]];
         double *mat = nullptr;
-        HB_CUDA(cudaMalloc(&mat, sizeof(double) * ld * n));
+        HB_CUDA(hb::cmalloc(&mat, sizeof(double) * ld * n));
         HB_CUDA(cudaMemsetAsync(mat, 0, sizeof(double) * ld * n, s));
         int *dr = upload_vec(c.r, s), *dc = upload_vec(c.c, s);
         double *dv = upload_vec(c.v, s);
         if (!c.r.empty())
             scatter_sym_kernel<<<hb::counted(grid1((long) c.r.size())), 256, 0, s>>>((int) c.r.size(), dr, dc, dv, mat, ld);
         HB_CUDA(cudaStreamSynchronize(s));
-        cudaFree(dr);
-        cudaFree(dc);
-        cudaFree(dv);
+        hb::cache_free(dr);
+        hb::cache_free(dc);
+        hb::cache_free(dv);
         dr_mat.push_back(mat);
     }
 
@@ -535,18 +535,18 @@ void SdpDevice::upload(int n_, int m_, const HostCoeff &C, const std::vector<Hos
     }
 
     t_upload_map = host_seconds() - tm0;
-    HB_CUDA(cudaMalloc(&T1, sizeof(double) * ld * n));
-    HB_CUDA(cudaMalloc(&T2, sizeof(double) * ld * n));
-    HB_CUDA(cudaMalloc(&vecbuf, sizeof(double) * std::max(m, 1)));
-    HB_CUDA(cudaMalloc(&d_w, sizeof(double) * (std::max(m, nr1d) + 1)));
-    HB_CUDA(cudaMalloc(&d_scal, sizeof(double) * 16));
-    HB_CUDA(cudaMallocHost(&h_scal, sizeof(double) * 16));
+    HB_CUDA(hb::cmalloc(&T1, sizeof(double) * ld * n));
+    HB_CUDA(hb::cmalloc(&T2, sizeof(double) * ld * n));
+    HB_CUDA(hb::cmalloc(&vecbuf, sizeof(double) * std::max(m, 1)));
+    HB_CUDA(hb::cmalloc(&d_w, sizeof(double) * (std::max(m, nr1d) + 1)));
+    HB_CUDA(hb::cmalloc(&d_scal, sizeof(double) * 16));
+    HB_CUDA(hb::cmalloc_host(&h_scal, sizeof(double) * 16));
     HB_CUDA(cudaStreamSynchronize(s));
     t_upload_total = host_seconds() - tu0;
 }
 
 void SdpDevice::release() {
-    auto f = [](void *p) { if (p) cudaFree(p); };
+    auto f = [](void *p) { if (p) hb::cache_free(p); };
     f(Cfull);
     f(sp_id); f(sp_ptr); f(sp_r); f(sp_c); f(sp_v);
     f(r1s_id); f(r1s_ptr); f(r1s_p); f(r1s_a); f(r1s_sign);
@@ -567,7 +567,7 @@ void SdpDevice::release() {
     opKT.release();
     opB.release();
     split_ready = false;
-    if (h_scal) cudaFreeHost(h_scal);
+    if (h_scal) hb::cache_free_host(h_scal);
     h_scal = nullptr;
 }
 

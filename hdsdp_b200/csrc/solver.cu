@@ -1086,7 +1086,7 @@ hdsdp_retcode run_psdp(hdsdp *h) {
     const double relOpt = dp(h, DBL_PARAM_RELOPTTOL), absOpt = dp(h, DBL_PARAM_ABSOPTTOL);
     const double pdScal = fd(h, D_OBJSCALING) * fd(h, D_RHSSCALING);
     if (h->nCones > 1 || h->dInfeas > 0.0) return HDSDP_RETCODE_FAILED;
-    for (double **p : {&X, &X0, &S, &XStep, &Buf}) HB_CUDA(cudaMalloc(p, sizeof(double) * ld * n));
+    for (double **p : {&X, &X0, &S, &XStep, &Buf}) HB_CUDA(hb::cmalloc(p, sizeof(double) * ld * n));
     XF.alloc(n);
     lzp.init(n, s);
     cone_values(h, X, nullptr);
@@ -1168,7 +1168,7 @@ hdsdp_retcode run_psdp(hdsdp *h) {
 exit_cleanup:
     h->kkt.primalX = nullptr;
     for (double *p : {X, X0, S, XStep, Buf})
-        if (p) cudaFree(p);
+        if (p) hb::cache_free(p);
     XF.release();
     lzp.release();
     return retcode;
@@ -1341,8 +1341,8 @@ hdsdp_retcode HDSDPCheckSolution(hdsdp *h, double dErrs[6]) {
     double primalObj = 0.0, dualObj = 0.0;
     const double pScal = fd(h, D_RHSSCALING), dScal = fd(h, D_OBJSCALING);
     double *X = nullptr, *S = nullptr;
-    HB_CUDA(cudaMalloc(&X, sizeof(double) * ld * n));
-    HB_CUDA(cudaMalloc(&S, sizeof(double) * ld * n));
+    HB_CUDA(hb::cmalloc(&X, sizeof(double) * ld * n));
+    HB_CUDA(hb::cmalloc(&S, sizeof(double) * ld * n));
     HB_CUDA(cudaMemsetAsync(X, 0, sizeof(double) * ld * n, c.s));
     for (int i = 0; i < m; ++i) dualObj += h->rowRHS[i] * h->y[i];
     cone_values(h, X, S);
@@ -1354,8 +1354,8 @@ hdsdp_retcode HDSDPCheckSolution(hdsdp *h, double dErrs[6]) {
     const double compl_ = c.h_scal[0];
     primalObj = c.trace_cx(X);
     const double minEig = min_eig_estimate(h, X);
-    cudaFree(X);
-    cudaFree(S);
+    hb::cache_free(X);
+    hb::cache_free(S);
     dualObj /= (pScal * dScal);
     primalObj /= (pScal * dScal);
     double pinf = 0.0;
@@ -1468,8 +1468,8 @@ void HDSDPGetConeValues(hdsdp *h, int iCone, double *conePrimal, double *coneDua
     const int n = c.n;
     const long ld = c.ld;
     double *X = nullptr, *S = nullptr;
-    if (conePrimal) HB_CUDA(cudaMalloc(&X, sizeof(double) * ld * n));
-    if (coneDual) HB_CUDA(cudaMalloc(&S, sizeof(double) * ld * n));
+    if (conePrimal) HB_CUDA(hb::cmalloc(&X, sizeof(double) * ld * n));
+    if (coneDual) HB_CUDA(hb::cmalloc(&S, sizeof(double) * ld * n));
     if (X) {
         HB_CUDA(cudaMemcpy2DAsync(X, sizeof(double) * ld, conePrimal, sizeof(double) * n, sizeof(double) * n, n,
                                   cudaMemcpyHostToDevice, c.s));
@@ -1482,8 +1482,8 @@ void HDSDPGetConeValues(hdsdp *h, int iCone, double *conePrimal, double *coneDua
         HB_CUDA(cudaMemcpy2DAsync(coneDual, sizeof(double) * n, S, sizeof(double) * ld, sizeof(double) * n, n,
                                   cudaMemcpyDeviceToHost, c.s));
     HB_CUDA(cudaStreamSynchronize(c.s));
-    if (X) cudaFree(X);
-    if (S) cudaFree(S);
+    if (X) hb::cache_free(X);
+    if (S) hb::cache_free(S);
 }
 
 void HDSDPClear(hdsdp *h) {

@@ -347,8 +347,8 @@ bool SplitOperand::alloc(int rows_, int k_) {
     rows_alloc = ra;
     kpad = kp;
     const size_t bytes = (size_t) ra * kp * sizeof(__nv_bfloat16);
-    HB_CUDA(cudaMalloc(&hi, bytes));
-    HB_CUDA(cudaMalloc(&lo, bytes));
+    HB_CUDA(hb::cmalloc(&hi, bytes));
+    HB_CUDA(hb::cmalloc(&lo, bytes));
     HB_CUDA(cudaMemset(hi, 0, bytes));
     HB_CUDA(cudaMemset(lo, 0, bytes));
     if (!hi || !lo) return false;
@@ -356,8 +356,8 @@ bool SplitOperand::alloc(int rows_, int k_) {
 }
 
 void SplitOperand::release() {
-    if (hi) cudaFree(hi);
-    if (lo) cudaFree(lo);
+    if (hi) hb::cache_free(hi);
+    if (lo) hb::cache_free(lo);
     hi = lo = nullptr;
     rows = k = rows_alloc = kpad = 0;
 }

@@ -50,6 +50,12 @@ extern int HDSDPGetIterLog( hdsdp *HSolver, int maxLen, double *t, double *pObj,
    [22] #S factorisations reused (the same dual slack factored before) */
 extern void HDSDPGetTimers( hdsdp *HSolver, double out[23] );
 
+/* The library keeps freed device and pinned host buffers for reuse by later
+   solvers of the same sizes (no reference counterpart). This hands the cached
+   buffers back to the driver; call it when the library will not be used for a
+   while. */
+extern void hdsdpb_release_cached_memory( void );
+
 /* Number of kernel launches this library has issued in the process so far
    (all solvers and entry points). No reference counterpart. */
 extern long long hdsdpb_launch_count( void );
