@@ -16,7 +16,9 @@
 //     u = g_y + A(N G_X N),   v = M^-1 u,   Z = N (A^T(v) - G_X) N,
 //     dL/db = v,   dL/dC = Z,   dL/dA_i = -v_i Xhat - y_i Z.
 // For strictly complementary solutions the result does not depend on mu to
-// first order; mu is <X*, S*>/n clipped to [1e-12, 1e-6]. M is assembled by
+// first order; mu is <X*, S*>/n clipped to [1e-8, 1e-6]: the condition number of M
+// grows like 1/mu^2, and below 1e-8 it passes what FP64 resolves (about 1e16), so a
+// smaller mu only adds rounding noise to the gradient. M is assembled by
 // the solver's Schur kernels with N in place of S^-1. N, M and its factor are
 // cached after the first call for a solve, so further calls cost two n x n
 // products, one Schur solve and the A(.)/A^T(.) maps.
@@ -155,7 +157,7 @@ hdsdp_retcode prepare(hdsdp *h, AdjointState &a) {
     // (sign Z by the Newton-Schulz iteration Y <- Y (3I - Y^2)/2, GEMMs only).
     frob_dot(s, n, a.X, ld, a.S, ld, a.d_scal);
     const double xs = host_scalar(s, a.d_scal, a.h_scal) / n;
-    const double mu = std::min(1e-6, std::max(1e-12, xs));
+    const double mu = std::min(1e-6, std::max(1e-8, xs));
     copy_matrix(s, n, n, a.X, ld, a.Z, ld);
     axpy(s, (int) (ld * n), -1.0, a.S, a.Z);
     frob_dot(s, n, a.Z, ld, a.Z, ld, a.d_scal);

@@ -42,7 +42,8 @@ namespace {
 constexpr int NB = 64;
 
 constexpr int TP = 68;                         // tile pitch (conflict-free DMMA fragment reads)
-constexpr int SM_DOUBLES = 3 * 64 * TP;        // three 64 x 68 tiles
+constexpr int SM_DOUBLES = 3 * 64 * TP;        // three 64 x 68 tiles (triangular inverse)
+constexpr int SM_DOUBLES_POTRF = 4 * 64 * TP;  // four tiles (factorisation)
 constexpr int COOP_THREADS = 256;
 
 __device__ __forceinline__ void cpa8(double *sdst, const double *gsrc, bool pred) {
@@ -54,6 +55,33 @@ __device__ __forceinline__ void cpa_wait_all() {
     asm volatile("cp.async.wait_group 0;\n" ::);
 }
 
+// 16-byte copy of which the first `bytes` (0, 8 or 16) come from global memory and the
+// rest is zero filled; both addresses 16-byte aligned.
+__device__ __forceinline__ void cpa16(double *sdst, const double *gsrc, int bytes) {
+    const unsigned saddr = (unsigned) __cvta_generic_to_shared(sdst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(saddr), "l"(gsrc), "r"(bytes));
+}
+
+// Stage columns 0..ncols-1 of the 64-row tile G (column-major, pitch ldg) into S (pitch
+// TP): entries with row < nr and column < nc are copied, the rest of those columns is
+// zero. Two rows move per copy when G and ldg keep every pair 16-byte aligned. The
+// caller waits with cpa_wait_all().
+__device__ __forceinline__ void stage_tile(double *S, const double *G, long ldg, int nr, int nc, int ncols) {
+    if (((((size_t) G) & 15) == 0) && ((ldg & 1) == 0)) {
+        for (int idx = threadIdx.x; idx < 32 * ncols; idx += blockDim.x) {
+            const int r = (idx & 31) * 2, c = idx >> 5;
+            const int cnt = (c < nc) ? min(2, max(0, nr - r)) : 0;
+            cpa16(&S[r + c * TP], cnt ? G + (size_t) r + (size_t) c * ldg : G, 8 * cnt);
+        }
+    } else {
+        for (int idx = threadIdx.x; idx < 64 * ncols; idx += blockDim.x) {
+            const int r = idx & 63, c = idx >> 6;
+            const bool ok = r < nr && c < nc;
+            cpa8(&S[r + c * TP], ok ? G + (size_t) r + (size_t) c * ldg : G, ok);
+        }
+    }
+}
+
 __device__ __forceinline__ void dmma_c(double &d0, double &d1, double a, double b) {
     asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
                  : "+d"(d0), "+d"(d1)
@@ -63,61 +91,63 @@ __device__ __forceinline__ void dmma_c(double &d0, double &d1, double a, double 
 
 // ---------------------------------------------------------------------------------
 // Diagonal-block factorisation: four 16-column sub-panels. Warp 0 factors and inverts
-// each 16 x 16 pivot block in registers (lane r holds row r; shuffles broadcast the
-// pivot and the column); the panel below, the trailing update and the off-diagonal
-// blocks of the 64 x 64 inverse are DMMA products in shared memory with all warps.
+// each 16 x 16 pivot block in registers; the panel below, the trailing update and the
+// off-diagonal blocks of the 64 x 64 inverse are DMMA products in shared memory with
+// the other warps.
 // ---------------------------------------------------------------------------------
 constexpr unsigned FULL = 0xffffffffu;
 
 // Factor T[off.., off..] (16 x 16, lower, pitch TP) in place and write its inverse to
-// X[off.., off..]. Executed by one whole warp (lanes 16-31 carry zeros).
+// X[off.., off..]. Executed by one whole warp with two lane roles: lane r < 16 holds row
+// r of the block, lane 16 + k holds column k of the inverse (starting as e_k). For each
+// column c one set of broadcasts of L(q, c), q > c, drives both the trailing update
+// A(r, q) -= L(r, c) L(q, c) and the forward elimination X(q, k) -= L(q, c) X(c, k):
+// the two are the same instruction, v[q] -= v[c] L(q, c), on every lane (a lane of the
+// second role is never masked by the row test). The broadcasts of a column are issued
+// before their uses so that their latencies overlap.
 __device__ __forceinline__ bool warp_chol_inv16(double *T, double *X, int off, int lane) {
-    const bool act = lane < 16;
-    double d[16];
+    const bool row_role = lane < 16;
+    double v[16];
 #pragma unroll
-    for (int q = 0; q < 16; ++q) d[q] = (act && q <= lane) ? T[(off + lane) + (off + q) * TP] : 0.0;
-    bool bad = false;
-    double rinv = 1.0;  // lane c: 1 / L_cc
+    for (int q = 0; q < 16; ++q)
+        v[q] = row_role ? ((q <= lane) ? T[(off + lane) + (off + q) * TP] : 0.0) : ((q == lane - 16) ? 1.0 : 0.0);
+    // one reciprocal square root per column: L_cc = p rsqrt(p), the column below scales
+    // by rsqrt(p), and so does row c of the inverse. The pivot of column c + 1 only
+    // needs L(c + 1, c), so it is formed first and its reciprocal square root runs
+    // while the rest of column c is applied.
+    double p = __shfl_sync(FULL, v[0], 0);
+    bool bad = !(p > 0.0);
+    double rs = rsqrt(p);
+    // fixed trip counts keep v[] and lq[] in registers (the loops unroll completely)
 #pragma unroll
     for (int c = 0; c < 16; ++c) {
-        // one reciprocal square root per column: L_cc = d rsqrt(d), the column below scales by rsqrt(d)
-        const double dc = __shfl_sync(FULL, d[c], c);
-        if (!(dc > 0.0)) bad = true;
-        const double rs = rsqrt(dc);
-        if (lane == c) {
-            d[c] = dc * rs;
-            rinv = rs;
-        } else if (lane > c) {
-            d[c] *= rs;
+        v[c] = (lane == c) ? p * rs : v[c] * rs;
+        double pn = 1.0, rn = 1.0;
+        if (c + 1 < 16) {
+            const double l1 = __shfl_sync(FULL, v[c], c + 1);
+            if (lane >= c + 1) v[c + 1] -= v[c] * l1;
+            pn = __shfl_sync(FULL, v[c + 1], c + 1);
+            if (!(pn > 0.0)) bad = true;
+            rn = rsqrt(pn);
         }
-        // fixed trip counts keep d[] in registers (the loops unroll completely)
+        double lq[16];
 #pragma unroll
-        for (int q = 0; q < 16; ++q) {
-            if (q > c) {
-                const double lqc = __shfl_sync(FULL, d[c], q);
-                if (lane >= q) d[q] -= d[c] * lqc;
-            }
-        }
+        for (int q = c + 2; q < 16; ++q) lq[q] = __shfl_sync(FULL, v[c], q);
+#pragma unroll
+        for (int q = c + 2; q < 16; ++q)
+            if (lane >= q) v[q] -= v[c] * lq[q];
+        p = pn;
+        rs = rn;
     }
-    if (act) {
+    if (row_role) {
 #pragma unroll
         for (int q = 0; q < 16; ++q)
-            if (q <= lane) T[(off + lane) + (off + q) * TP] = d[q];
-    }
-    // column `lane` of L^-1 by forward substitution; L_rk broadcast from lane r
-    double x[16];
+            if (q <= lane) T[(off + lane) + (off + q) * TP] = v[q];
+    } else {
+        const int k = lane - 16;
 #pragma unroll
-    for (int r = 0; r < 16; ++r) {
-        const double ir = __shfl_sync(FULL, rinv, r);
-        double acc = (r == lane) ? 1.0 : 0.0;
-#pragma unroll
-        for (int k = 0; k < 16; ++k)
-            if (k < r) acc -= __shfl_sync(FULL, d[k], r) * x[k];
-        x[r] = (r >= lane) ? acc * ir : 0.0;
-    }
-    if (act) {
-#pragma unroll
-        for (int r = 0; r < 16; ++r) X[(off + r) + (off + lane) * TP] = x[r];
+        for (int q = 0; q < 16; ++q)
+            if (q >= k) X[(off + q) + (off + k) * TP] = v[q];
     }
     return !bad;
 }
@@ -126,9 +156,12 @@ __device__ __forceinline__ bool warp_chol_inv16(double *T, double *X, int off, i
 // in shared memory (pitch TP) on the DMMA path; 8 x 8 tiles dealt to the warps starting
 // at warp `w0`. A(r, k) = Ab[r + k*TP]; op(B)(k, c) = bt ? Bb[c + k*TP] : Bb[k + c*TP].
 // With lower set, tiles strictly above the diagonal are skipped.
+// With nwarp set, only warps w0 .. w0 + nwarp - 1 take part (and all of them must call).
 __device__ __forceinline__ void smem_mma(double *Cb, const double *Ab, const double *Bb, int bt, int rows, int cols,
-                                         int K, double alpha, bool accumulate, bool lower) {
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+                                         int K, double alpha, bool accumulate, bool lower, int w0 = 0,
+                                         int nwarp = 0) {
+    const int lane = threadIdx.x & 31, w = (threadIdx.x >> 5) - w0;
+    const int nw = nwarp ? nwarp : (int) (blockDim.x >> 5);
     const int tr = rows >> 3, ntile = tr * (cols >> 3);
     for (int t = w; t < ntile; t += nw) {
         const int ti = t % tr, tj = t / tr;
@@ -152,29 +185,50 @@ __device__ __forceinline__ void smem_mma(double *Cb, const double *Ab, const dou
     }
 }
 
+// Shared-memory regions of the factorisation kernel (64 x TP doubles each): tile
+// products use regions 0 and 1; the diagonal-block factorisation keeps its block in
+// region 3, the previous panel's rows in region 2 and the inverse in region 1.
+constexpr int R_X = 1, R_P = 2, R_T = 3;
+__device__ __forceinline__ double *region(double *sm, int r) { return sm + (size_t) r * 64 * TP; }
+
+// Block row i of the inverse of the 64 x 64 diagonal block, off the diagonal:
+// X_ij = -X_ii sum_{k=j}^{i-1} L_ik X_kj for j < i (16 x 16 blocks), by warps
+// w0 .. w0 + nwarp - 1 (nwarp 0: all warps); `bar` synchronises exactly those warps
+// between the two products. Scratch: rows 0-15, columns 16-63 of P.
+template <typename Bar>
+__device__ __forceinline__ void inverse_block_row(const double *T, double *X, double *P, int i, int w0, int nwarp,
+                                                  Bar bar) {
+    for (int j = 0; j < i; ++j)
+        smem_mma(P + 16 * (j + 1) * TP, T + 16 * i + 16 * j * TP, X + 16 * j + 16 * j * TP, 0, 16, 16, 16 * (i - j),
+                 1.0, false, false, w0, nwarp);
+    bar();
+    for (int j = 0; j < i; ++j)
+        smem_mma(X + 16 * i + 16 * j * TP, X + 16 * i + 16 * i * TP, P + 16 * (j + 1) * TP, 0, 16, 16, 16, -1.0,
+                 false, false, w0, nwarp);
+}
+
 // Factor the nb x nb diagonal block at (j0, j0) and write its inverse to Dinv (64
-// columns, zero padded). With Pp set, the block is first updated in shared memory by
-// the previous panel's rows: A_jj -= Pp Pp^T (Pp: nb x 64, pitch ldp). Executed by one
-// block. Returns false (and sets *info) on a failed pivot.
+// columns, zero padded). The block is first updated in shared memory by the previous
+// panel's rows, A_jj -= P P^T, when they are given: `staged` (block and rows already in
+// regions 3 and 2, copies possibly still in flight) or Pp (nb x 64 rows, pitch ldp,
+// staged here). Executed by one block. Returns false (and sets *info) on a failed
+// pivot. The strictly upper part of the diagonal block in L holds zeros (copy_lower_k
+// and every later write keep it so), which lets whole column segments be staged.
 __device__ bool potf2_dev(double *L, long ld, int j0, int nb, double *Dinv, long ldd, int *info, double *sm,
-                          const double *Pp = nullptr, long ldp = 0) {
-    double *T = sm, *X = sm + 64 * TP, *P = sm + 128 * TP;
+                          const double *Pp = nullptr, long ldp = 0, bool staged = false) {
+    double *T = region(sm, R_T), *X = region(sm, R_X), *P = region(sm, R_P);
     __shared__ int fail;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    for (int idx = tid; idx < 64 * 64; idx += blockDim.x) {
-        const int r = idx & 63, c = idx >> 6;
-        const bool ok = r < nb && c < nb && r >= c;
-        cpa8(&T[r + c * TP], ok ? L + (size_t) (j0 + r) + (size_t) (j0 + c) * ld : L, ok);
-        if (Pp) {
-            const bool okp = r < nb;
-            cpa8(&P[r + c * TP], okp ? Pp + (size_t) r + (size_t) c * ldp : Pp, okp);
-        }
-        X[r + c * TP] = 0.0;
+    double *Ljj = L + (size_t) j0 + (size_t) j0 * ld;
+    if (!staged) {
+        stage_tile(T, Ljj, ld, nb, nb, 64);
+        if (Pp) stage_tile(P, Pp, ldp, nb, 64, 64);
     }
+    for (int idx = tid; idx < 64 * 64; idx += blockDim.x) X[(idx & 63) + (idx >> 6) * TP] = 0.0;
     cpa_wait_all();
     if (tid == 0) fail = 0;
     __syncthreads();
-    if (Pp) {
+    if (staged || Pp) {
         smem_mma(T, P, P, 1, 64, 64, 64, -1.0, true, true);
         __syncthreads();
     }
@@ -183,10 +237,15 @@ __device__ bool potf2_dev(double *L, long ld, int j0, int nb, double *Dinv, long
     const int sb = 4096 + (j0 / 64) * 32;
     (void) sb;
     CHOL_STAMP(sb);
+    const int nwork = (int) (blockDim.x >> 5) - 1;
+    auto bar_workers = [nwork]() { asm volatile("bar.sync 1, %0;\n" ::"r"(32 * nwork) : "memory"); };
     for (int s0 = 0; s0 < 64; s0 += 16) {
         if (warp == 0) {
             const bool ok = warp_chol_inv16(T, X, s0, lane);
             if (lane == 0 && !ok) fail = s0 + 1;
+        } else if (s0 >= 32) {
+            // block row s0/16 - 1 of the inverse while warp 0 factors block s0/16
+            inverse_block_row(T, X, P, s0 / 16 - 1, 1, nwork, bar_workers);
         }
         __syncthreads();
         CHOL_STAMP(sb + 1 + (s0 >> 4) * 2);
@@ -198,7 +257,7 @@ __device__ bool potf2_dev(double *L, long ld, int j0, int nb, double *Dinv, long
             __syncthreads();
             smem_mma(T + (s0 + 16) + (s0 + 16) * TP, P + s0 + 16, P + s0 + 16, 1, rem, rem, 16, -1.0, true, true);
             for (int idx = tid; idx < rem * 16; idx += blockDim.x) {
-                const int r = s0 + 16 + idx % rem, c = idx / rem;
+                const int r = s0 + 16 + (idx & 15) + 16 * (idx >> 8), c = (idx >> 4) & 15;
                 T[r + (s0 + c) * TP] = P[r + c * TP];
             }
             __syncthreads();
@@ -209,29 +268,35 @@ __device__ bool potf2_dev(double *L, long ld, int j0, int nb, double *Dinv, long
         if (tid == 0) *info = j0 + fail;
         return false;
     }
-    // off-diagonal 16 x 16 blocks of the inverse: X_ij = -X_ii sum_{k=j}^{i-1} L_ik X_kj
-    for (int d = 1; d < 4; ++d) {
-        for (int j = 0; j + d < 4; ++j) {
-            const int i = j + d;
-            smem_mma(P + 16 * j, T + 16 * i + 16 * j * TP, X + 16 * j + 16 * j * TP, 0, 16, 16, 16 * d, 1.0, false,
-                     false);
-        }
-        __syncthreads();
-        for (int j = 0; j + d < 4; ++j) {
-            const int i = j + d;
-            smem_mma(X + 16 * i + 16 * j * TP, X + 16 * i + 16 * i * TP, P + 16 * j, 0, 16, 16, 16, -1.0, false,
-                     false);
-        }
-        __syncthreads();
-    }
+    // the last block row of the inverse, with all warps
+    inverse_block_row(T, X, P, 3, 0, 0, []() { __syncthreads(); });
+    __syncthreads();
     CHOL_STAMP(sb + 10);
-    for (int idx = tid; idx < nb * nb; idx += blockDim.x) {
-        const int r = idx % nb, cc = idx / nb;
-        if (r >= cc) L[(size_t) (j0 + r) + (size_t) (j0 + cc) * ld] = T[r + cc * TP];
-    }
-    for (int idx = tid; idx < NB * NB; idx += blockDim.x) {
-        const int r = idx & 63, cc = idx >> 6;
-        if (r < nb) Dinv[(size_t) (j0 + r) + (size_t) cc * ldd] = (cc < nb && r >= cc) ? X[r + cc * TP] : 0.0;
+    // write L (lower part only) and Dinv (zero beyond column nb), two rows per store
+    const bool vl = ((((size_t) Ljj) & 15) == 0) && ((ld & 1) == 0);
+    const bool vd = ((((size_t) (Dinv + j0)) & 15) == 0) && ((ldd & 1) == 0);
+    for (int idx = tid; idx < 32 * 64; idx += blockDim.x) {
+        const int r = (idx & 31) * 2, cc = idx >> 5;
+        if (r >= nb) continue;
+        const bool two = r + 1 < nb;
+        if (cc < nb && r + 1 >= cc) {
+            double *dst = Ljj + (size_t) r + (size_t) cc * ld;
+            if (two && r >= cc && vl) {
+                *reinterpret_cast<double2 *>(dst) = make_double2(T[r + cc * TP], T[r + 1 + cc * TP]);
+            } else {
+                if (r >= cc) dst[0] = T[r + cc * TP];
+                if (two) dst[1] = T[r + 1 + cc * TP];
+            }
+        }
+        const double d0 = (cc < nb) ? X[r + cc * TP] : 0.0;
+        const double d1 = (cc < nb) ? X[r + 1 + cc * TP] : 0.0;
+        double *dd = Dinv + (size_t) (j0 + r) + (size_t) cc * ldd;
+        if (two && vd) {
+            *reinterpret_cast<double2 *>(dd) = make_double2(d0, d1);
+        } else {
+            dd[0] = d0;
+            if (two) dd[1] = d1;
+        }
     }
     __syncthreads();
     CHOL_STAMP(sb + 11);
@@ -247,17 +312,19 @@ __device__ bool potf2_dev(double *L, long ld, int j0, int nb, double *Dinv, long
 // may alias A or B (in-place panel solves).
 __device__ void tile_mma_dev(double *Cb, long ldc, int mr, int nc, const double *Ab, long lda, int ar,
                              const double *Bb, long ldb, int bt, int bc, int nb, bool diag, int mode, double *sm,
-                             double *Ct = nullptr, long ldct = 0) {
+                             double *Ct = nullptr, long ldct = 0, double *Csm = nullptr) {
     double *As = sm, *Bs = sm + 64 * TP;   // As[r + k*TP], Bs[c + k*TP]
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     const int kp = (nb + 3) & ~3;
-    for (int idx = tid; idx < 64 * kp; idx += blockDim.x) {
-        const int r = idx & 63, k = idx >> 6;
-        const bool oka = r < ar && k < nb;
-        cpa8(&As[r + k * TP], oka ? Ab + (size_t) r + (size_t) k * lda : Ab, oka);
-        const bool okb = r < bc && k < nb;
-        cpa8(&Bs[r + k * TP], okb ? (bt ? Bb + (size_t) r + (size_t) k * ldb : Bb + (size_t) k + (size_t) r * ldb) : Bb,
-             okb);
+    stage_tile(As, Ab, lda, ar, nb, kp);
+    if (bt) {
+        stage_tile(Bs, Bb, ldb, bc, nb, kp);
+    } else {
+        for (int idx = tid; idx < 64 * kp; idx += blockDim.x) {
+            const int r = idx & 63, k = idx >> 6;
+            const bool okb = r < bc && k < nb;
+            cpa8(&Bs[r + k * TP], okb ? Bb + (size_t) k + (size_t) r * ldb : Bb, okb);
+        }
     }
     const int wm = (w & 1) * 32, wn = (w >> 1) * 16;
     // prefetch the C tile while the operand copies are in flight (mode 0)
@@ -293,16 +360,18 @@ __device__ void tile_mma_dev(double *Cb, long ldc, int mr, int nc, const double 
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
         const int r = wm + i * 8 + (lane >> 2);
-        if (r >= mr) continue;
 #pragma unroll
         for (int j = 0; j < 2; ++j)
 #pragma unroll
             for (int e = 0; e < 2; ++e) {
                 const int c = wn + j * 8 + (lane & 3) * 2 + e;
-                if (c >= nc || (diag && r < c)) continue;
+                const bool valid = r < mr && c < nc && !(diag && r < c);
                 const double val = (mode == 0) ? cv[i][j][e] - acc[i][j][e] : (mode == 2) ? -acc[i][j][e] : acc[i][j][e];
-                Cb[(size_t) r + (size_t) c * ldc] = val;
-                if (Ct) Ct[(size_t) c + (size_t) r * ldct] = val;
+                if (valid) {
+                    Cb[(size_t) r + (size_t) c * ldc] = val;
+                    if (Ct) Ct[(size_t) c + (size_t) r * ldct] = val;
+                }
+                if (Csm) Csm[r + c * TP] = valid ? val : 0.0;
             }
     }
     __syncthreads();
@@ -353,7 +422,7 @@ __device__ __forceinline__ void k_final_tile(const double *Dinv, long ldd, doubl
     }
 }
 
-__global__ void __launch_bounds__(COOP_THREADS, 2) potrf_coop_kernel(double *L, long ld, int n, double *Dinv,
+__global__ void __launch_bounds__(COOP_THREADS, 1) potrf_coop_kernel(double *L, long ld, int n, double *Dinv,
                                                                   long ldd, int *info, double *K, double *KT) {
     cg::grid_group grid = cg::this_grid();
     extern __shared__ double sm[];
@@ -373,11 +442,17 @@ __global__ void __launch_bounds__(COOP_THREADS, 2) potrf_coop_kernel(double *L, 
         if (blockIdx.x <= 1) CHOL_STAMP(pb + 0);
         // panel solve; with K, the update of K's rows r >= bj by block row bj - 1
         const long nx = (K && bj >= 1) ? (long) (nblk - bj) * bj : 0;
+        // block 0 stages the next diagonal block now (its updates by earlier panels are
+        // complete) and keeps its own solved chunk 0, the rows that update that block
+        const int nbn = min(NB, rows);
+        if (blockIdx.x == 0)
+            stage_tile(region(sm, R_T), L + (size_t) (j0 + nb) + (size_t) (j0 + nb) * ld, ld, nbn, nbn, 64);
         for (long t = blockIdx.x; t < nchunk + nx; t += gridDim.x) {
             if (t < nchunk) {
                 const int ch = (int) t;
                 const int mr = min(64, rows - ch * 64);
-                tile_mma_dev(P + ch * 64, ld, mr, nb, P + ch * 64, ld, mr, Dinv + j0, ldd, 1, nb, nb, false, 1, sm);
+                tile_mma_dev(P + ch * 64, ld, mr, nb, P + ch * 64, ld, mr, Dinv + j0, ldd, 1, nb, nb, false, 1, sm,
+                             nullptr, 0, (t == 0) ? region(sm, R_P) : nullptr);
             } else {
                 const long u = t - nchunk;
                 k_update_tile(L, ld, K, n, bj + (int) (u / bj), (int) (u % bj), bj - 1, sm);
@@ -392,7 +467,7 @@ __global__ void __launch_bounds__(COOP_THREADS, 2) potrf_coop_kernel(double *L, 
         if (blockIdx.x == 0) {
             // tile (0, 0) is the next diagonal block: update it in shared memory and factor it
             CHOL_STAMP(pb + 3);
-            potf2_dev(L, ld, j0 + nb, min(NB, rows), Dinv, ldd, info, sm, P, ld);
+            potf2_dev(L, ld, j0 + nb, nbn, Dinv, ldd, info, sm, nullptr, 0, true);
             CHOL_STAMP(pb + 4);
         }
         // remaining tiles (and K's block row bj), spread over the other blocks
@@ -490,7 +565,7 @@ int coop_grid(const void *fn) {
     static int cached[2] = {0, 0};
     const int slot = (fn == (const void *) potrf_coop_kernel) ? 0 : 1;
     if (cached[slot]) return cached[slot];
-    const int smem = SM_DOUBLES * (int) sizeof(double);
+    const int smem = (slot == 0 ? SM_DOUBLES_POTRF : SM_DOUBLES) * (int) sizeof(double);
     HB_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     int dev = 0, sms = 0, per = 0;
     cudaGetDevice(&dev);
@@ -527,7 +602,7 @@ bool coop_factorize_enqueue(cudaStream_t s, DenseFactor &F, const double *S, lon
     void *args[] = {&Lp, &ld, &nn, &Dp, &ldd, &ip, &Kp, &KTp};
     const bool timed = kstat_on(KF_POTRF);
     if (timed) kstat_begin(KF_POTRF, s, (double) n * n * n / 3.0);
-    cudaError_t e = cudaLaunchCooperativeKernel(fn, hb::counted(grid), COOP_THREADS, args, SM_DOUBLES * sizeof(double), s);
+    cudaError_t e = cudaLaunchCooperativeKernel(fn, hb::counted(grid), COOP_THREADS, args, SM_DOUBLES_POTRF * sizeof(double), s);
     if (timed) kstat_end(s);
     if (e != cudaSuccess) {
         cudaGetLastError();

@@ -36,7 +36,9 @@ def vjp(inst, y, X, gy, GX, mu=None):
     C, A = K.dense_data(inst)
     S = K.dual_slack(C, A, y)
     if mu is None:
-        mu = min(1e-6, max(1e-12, float(np.sum(X * S)) / inst.n))
+        # the central point at mu = <X, S>/n clipped to [1e-8, 1e-6] (the Schur matrix in
+        # this scaling has a condition number near 1/mu^2, past FP64's reach below 1e-8)
+        mu = min(1e-6, max(1e-8, float(np.sum(X * S)) / inst.n))
     N, Xh = purified_scaling(X, S, mu)
     m = inst.m
     NA = [N @ Ai @ N for Ai in A]
