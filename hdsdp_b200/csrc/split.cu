@@ -10,11 +10,11 @@ namespace hb {
 namespace {
 
 constexpr int BM = 128, BN = 128, BK = 64;  // BK = 64 BF16 = one 128-byte swizzle row
-constexpr int STAGES = 4;
+constexpr int STAGES = 3;
 constexpr int TILE_BYTES = BM * BK * 2;     // 16 KB per operand tile
-constexpr int STAGE_BYTES = 2 * TILE_BYTES;
+constexpr int STAGE_BYTES = 4 * TILE_BYTES; // A hi, A lo, B hi, B lo of one K block: all three products
 constexpr int THREADS = 192;                // warp 0 TMA, warp 1 MMA + TMEM owner, warps 2-5 epilogue
-constexpr int TMEM_COLS = BN;               // FP32 accumulator: one column per output column
+constexpr int TMEM_COLS = 2 * BN;           // two FP32 accumulators: one tile drains while the next accumulates
 constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 /* alignment */ + 256 /* barriers */;
 constexpr long WAIT_LIMIT = 1L << 24;       // bounded mbarrier polls (about a second)
 
@@ -49,6 +49,10 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
     }
     atomicExch(&g_split_err, 1);
     return false;
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
 
 __device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
@@ -138,6 +142,12 @@ __device__ __forceinline__ void tile_of(const KernelArgs &p, int b, int &tm, int
     }
 }
 
+// Persistent: CTA b takes tiles b, b + grid, ... The producer warp streams K blocks of
+// all its tiles through a ring of stages, each holding the four operand tiles of one
+// K block (A hi, A lo, B hi, B lo), from which the MMA thread issues the three
+// products hi*hi, hi*lo, lo*hi into one FP32 accumulator. Tiles alternate between two
+// accumulators in tensor memory, so the epilogue warps drain one tile while the next
+// one accumulates.
 __global__ void __launch_bounds__(THREADS, 1)
     split_gemm_kernel(const __grid_constant__ CUtensorMap a_hi, const __grid_constant__ CUtensorMap a_lo,
                       const __grid_constant__ CUtensorMap b_hi, const __grid_constant__ CUtensorMap b_lo,
@@ -146,26 +156,27 @@ __global__ void __launch_bounds__(THREADS, 1)
     const uint32_t raw = smem_u32(smem_raw);
     const uint32_t base = (raw + 1023u) & ~1023u;
     uint8_t *gbase = smem_raw + (base - raw);
-    const uint32_t bar0 = base + STAGES * STAGE_BYTES;  // full[STAGES], empty[STAGES], accum, tmem slot
+    // barriers: full[STAGES], empty[STAGES], acc_full[2], acc_empty[2], then the TMEM slot
+    const uint32_t bar0 = base + STAGES * STAGE_BYTES;
     auto full = [&](int st) { return bar0 + 8u * st; };
     auto empty = [&](int st) { return bar0 + 8u * (STAGES + st); };
-    const uint32_t accum = bar0 + 8u * (2 * STAGES);
-    volatile uint32_t *tmem_slot = (volatile uint32_t *) (gbase + STAGES * STAGE_BYTES + 8 * (2 * STAGES + 1));
+    auto acc_full = [&](int b) { return bar0 + 8u * (2 * STAGES + b); };
+    auto acc_empty = [&](int b) { return bar0 + 8u * (2 * STAGES + 2 + b); };
+    volatile uint32_t *tmem_slot = (volatile uint32_t *) (gbase + STAGES * STAGE_BYTES + 8 * (2 * STAGES + 4));
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    int tm, tn;
-    tile_of(p, blockIdx.x, tm, tn);
-    const int m0 = tm * BM, n0 = tn * BN;
-    int nkb = p.nkb;
-    if (p.a_lower) nkb = min(nkb, (m0 + BM + BK - 1) / BK);
-    const int total = 3 * nkb;
+    const int ntiles = p.lower_tiles ? p.tiles_m * (p.tiles_m + 1) / 2 : p.tiles_m * p.tiles_n;
+    auto kblocks = [&](int m0) { return p.a_lower ? min(p.nkb, (m0 + BM + BK - 1) / BK) : p.nkb; };
 
     if (threadIdx.x == 0) {
         for (int st = 0; st < STAGES; ++st) {
             mbar_init(full(st), 1);
             mbar_init(empty(st), 1);
         }
-        mbar_init(accum, 1);
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(acc_full(b), 1);
+            mbar_init(acc_empty(b), 4);  // one arrival per epilogue warp
+        }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     }
@@ -181,45 +192,77 @@ __global__ void __launch_bounds__(THREADS, 1)
     const uint32_t tmem = *tmem_slot;
 
     if (warp == 0 && lane == 0) {
-        // producer: segment 0 = (A hi, B hi), 1 = (A hi, B lo), 2 = (A lo, B hi)
-        for (int kb = 0; kb < total; ++kb) {
-            const int st = kb % STAGES;
-            const uint32_t ph = (uint32_t) (kb / STAGES) & 1u;
-            if (!mbar_wait(empty(st), ph ^ 1u)) break;
-            const int seg = kb / nkb, kk = kb - seg * nkb;
-            mbar_expect_tx(full(st), STAGE_BYTES);
-            const uint32_t sa = base + st * STAGE_BYTES, sb = sa + TILE_BYTES;
-            tma_load_2d(sa, seg == 2 ? &a_lo : &a_hi, kk * BK, m0, full(st));
-            tma_load_2d(sb, seg == 1 ? &b_lo : &b_hi, kk * BK, n0, full(st));
+        // producer
+        int it = 0;
+        bool ok = true;
+        for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+            int tm, tn;
+            tile_of(p, tile, tm, tn);
+            const int m0 = tm * BM, n0 = tn * BN, nkb = kblocks(m0);
+            for (int kb = 0; kb < nkb; ++kb, ++it) {
+                const int st = it % STAGES;
+                const uint32_t ph = (uint32_t) (it / STAGES) & 1u;
+                if (!mbar_wait(empty(st), ph ^ 1u)) {
+                    ok = false;
+                    break;
+                }
+                mbar_expect_tx(full(st), STAGE_BYTES);
+                const uint32_t sa = base + st * STAGE_BYTES;
+                tma_load_2d(sa, &a_hi, kb * BK, m0, full(st));
+                tma_load_2d(sa + TILE_BYTES, &a_lo, kb * BK, m0, full(st));
+                tma_load_2d(sa + 2 * TILE_BYTES, &b_hi, kb * BK, n0, full(st));
+                tma_load_2d(sa + 3 * TILE_BYTES, &b_lo, kb * BK, n0, full(st));
+            }
         }
     } else if (warp == 1 && lane == 0) {
-        // MMA issuer: four K=16 steps per 64-wide stage
+        // MMA issuer: per stage, four K=16 steps of each of the three products
+        int it = 0, tc = 0;
         bool ok = true;
-        for (int kb = 0; kb < total; ++kb) {
-            const int st = kb % STAGES;
-            const uint32_t ph = (uint32_t) (kb / STAGES) & 1u;
-            if (!mbar_wait(full(st), ph)) {
-                ok = false;
-                break;
-            }
+        for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x, ++tc) {
+            int tm, tn;
+            tile_of(p, tile, tm, tn);
+            const int nkb = kblocks(tm * BM);
+            const int b = tc & 1;
+            if (!mbar_wait(acc_empty(b), ((uint32_t) (tc >> 1) & 1u) ^ 1u)) break;
             fence_after();
-            const uint64_t da = smem_desc(base + st * STAGE_BYTES);
-            const uint64_t db = smem_desc(base + st * STAGE_BYTES + TILE_BYTES);
+            const uint32_t d = tmem + (uint32_t) (b * BN);
+            for (int kb = 0; kb < nkb; ++kb, ++it) {
+                const int st = it % STAGES;
+                const uint32_t ph = (uint32_t) (it / STAGES) & 1u;
+                if (!mbar_wait(full(st), ph)) {
+                    ok = false;
+                    break;
+                }
+                fence_after();
+                const uint32_t sa = base + st * STAGE_BYTES;
+                const uint64_t dah = smem_desc(sa), dal = smem_desc(sa + TILE_BYTES);
+                const uint64_t dbh = smem_desc(sa + 2 * TILE_BYTES), dbl = smem_desc(sa + 3 * TILE_BYTES);
 #pragma unroll
-            for (int k = 0; k < BK / 16; ++k)
-                mma_bf16(tmem, da + (uint64_t) (2 * k), db + (uint64_t) (2 * k), (kb | k) != 0 ? 1u : 0u);
-            mma_commit(empty(st));
+                for (int k = 0; k < BK / 16; ++k)
+                    mma_bf16(d, dah + (uint64_t) (2 * k), dbh + (uint64_t) (2 * k), (kb | k) != 0 ? 1u : 0u);
+#pragma unroll
+                for (int k = 0; k < BK / 16; ++k) mma_bf16(d, dah + (uint64_t) (2 * k), dbl + (uint64_t) (2 * k), 1u);
+#pragma unroll
+                for (int k = 0; k < BK / 16; ++k) mma_bf16(d, dal + (uint64_t) (2 * k), dbh + (uint64_t) (2 * k), 1u);
+                mma_commit(empty(st));
+            }
+            if (ok) mma_commit(acc_full(b));
         }
-        if (ok) mma_commit(accum);
     } else if (warp >= 2) {
         // epilogue: warp w reads accumulator lanes 32 * (w % 4) ...
         const int q = warp & 3;
-        const int r = m0 + q * 32 + lane;
-        if (mbar_wait(accum, 0)) {
+        int tc = 0;
+        for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++tc) {
+            int tm, tn;
+            tile_of(p, tile, tm, tn);
+            const int m0 = tm * BM, n0 = tn * BN;
+            const int r = m0 + q * 32 + lane;
+            const int b = tc & 1;
+            if (!mbar_wait(acc_full(b), (uint32_t) (tc >> 1) & 1u)) break;
             fence_after();
             for (int c0 = 0; c0 < BN; c0 += 32) {
                 float v[32];
-                tmem_ld32(tmem + ((uint32_t) (q * 32) << 16) + (uint32_t) c0, v);
+                tmem_ld32(tmem + ((uint32_t) (q * 32) << 16) + (uint32_t) (b * BN + c0), v);
                 if (p.epi == SPLIT_EPI_F64) {
                     if (r < p.M) {
 #pragma unroll
@@ -256,6 +299,10 @@ __global__ void __launch_bounds__(THREADS, 1)
                     }
                 }
             }
+            // the accumulator may be overwritten once all four warps have read it
+            fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(acc_empty(b));
         }
     }
     fence_before();
@@ -408,7 +455,15 @@ bool split_gemm(cudaStream_t s, const SplitOperand &A, const SplitOperand &B, co
     }
     p.colsq = g.colsq;
     if (p.nkb <= 0) return false;
-    const long blocks = g.lower_tiles ? (long) p.tiles_m * (p.tiles_m + 1) / 2 : (long) p.tiles_m * p.tiles_n;
+    const long tiles = g.lower_tiles ? (long) p.tiles_m * (p.tiles_m + 1) / 2 : (long) p.tiles_m * p.tiles_n;
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = 1;
+    }
+    const long blocks = std::min<long>(tiles, sms);  // persistent: one CTA per SM at most
     const bool timed = kstat_on(KF_SPLIT_GEMM);
     if (timed) {
         double f = 3.0 * 2.0 * g.M * (double) g.N * g.K;

@@ -16,7 +16,7 @@ pytestmark = pytest.mark.gpu
 
 
 @pytest.mark.parametrize("M,N,K", [(1, 1, 1), (128, 128, 64), (300, 200, 150), (129, 257, 65),
-                                   (1000, 2000, 1000), (2000, 2000, 1000)])
+                                   (1000, 2000, 1000), (2000, 2000, 1000), (3000, 2500, 700)])
 @pytest.mark.parametrize("tA,tB", [(False, False), (True, False), (False, True)])
 def test_split_gemm_accuracy(gpu_lib, M, N, K, tA, tB):
     rng = np.random.default_rng(M + 3 * N + 7 * K)
