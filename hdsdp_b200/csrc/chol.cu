@@ -42,8 +42,7 @@ namespace {
 constexpr int NB = 64;
 
 constexpr int TP = 68;                         // tile pitch (conflict-free DMMA fragment reads)
-constexpr int SM_DOUBLES = 3 * 64 * TP;        // three 64 x 68 tiles (triangular inverse)
-constexpr int SM_DOUBLES_POTRF = 4 * 64 * TP;  // four tiles (factorisation)
+constexpr int SM_DOUBLES = 4 * 64 * TP;        // four 64 x 68 tiles
 constexpr int COOP_THREADS = 256;
 
 __device__ __forceinline__ void cpa8(double *sdst, const double *gsrc, bool pred) {
@@ -305,30 +304,42 @@ __device__ bool potf2_dev(double *L, long ld, int j0, int nb, double *Dinv, long
 
 // Tile product on the DMMA path over K = nb <= 64:
 //   mode 0:  C -= A * op(B)      mode 1:  C = A * op(B)      mode 2:  C = -A * op(B)
-// With Ct set, the result is also written transposed to Ct (pitch ldct).
-// A(r, k) = Ab[r + k*lda]; op(B)(k, c) = bt ? Bb[c + k*ldb] : Bb[k + c*ldb].
-// C is the 64 x 64 tile at Cb (pitch ldc) clipped to mr x nc; with diag set only
-// row >= col entries are written. Operands are staged in shared memory first, so C
-// may alias A or B (in-place panel solves).
-__device__ void tile_mma_dev(double *Cb, long ldc, int mr, int nc, const double *Ab, long lda, int ar,
-                             const double *Bb, long ldb, int bt, int bc, int nb, bool diag, int mode, double *sm,
-                             double *Ct = nullptr, long ldct = 0, double *Csm = nullptr) {
-    double *As = sm, *Bs = sm + 64 * TP;   // As[r + k*TP], Bs[c + k*TP]
-    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-    const int kp = (nb + 3) & ~3;
-    stage_tile(As, Ab, lda, ar, nb, kp);
-    if (bt) {
-        stage_tile(Bs, Bb, ldb, bc, nb, kp);
+// A(r, k) = A[r + k*lda]; op(B)(k, c) = bt ? B[c + k*ldb] : B[k + c*ldb].
+// C is the 64 x 64 tile at C (pitch ldc) clipped to mr x nc; with diag set only
+// row >= col entries are written.
+struct TileJob {
+    double *C;
+    long ldc;
+    int mr, nc;
+    const double *A;
+    long lda;
+    int ar;
+    const double *B;
+    long ldb;
+    int bt, bc, nb;
+    bool diag;
+    int mode;
+};
+
+// Issue the copies of a job's operands into As / Bs (pitch TP, zero padded).
+__device__ __forceinline__ void stage_job(const TileJob &J, double *As, double *Bs) {
+    const int kp = (J.nb + 3) & ~3;
+    stage_tile(As, J.A, J.lda, J.ar, J.nb, kp);
+    if (J.bt) {
+        stage_tile(Bs, J.B, J.ldb, J.bc, J.nb, kp);
     } else {
-        for (int idx = tid; idx < 64 * kp; idx += blockDim.x) {
+        for (int idx = threadIdx.x; idx < 64 * kp; idx += blockDim.x) {
             const int r = idx & 63, k = idx >> 6;
-            const bool okb = r < bc && k < nb;
-            cpa8(&Bs[r + k * TP], okb ? Bb + (size_t) k + (size_t) r * ldb : Bb, okb);
+            const bool okb = r < J.bc && k < J.nb;
+            cpa8(&Bs[r + k * TP], okb ? J.B + (size_t) k + (size_t) r * J.ldb : J.B, okb);
         }
     }
+}
+
+// This thread's C entries of a mode-0 job (zero otherwise), in fragment order.
+__device__ __forceinline__ void load_c(const TileJob &J, double (&cv)[4][2][2]) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int wm = (w & 1) * 32, wn = (w >> 1) * 16;
-    // prefetch the C tile while the operand copies are in flight (mode 0)
-    double cv[4][2][2];
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
@@ -336,11 +347,16 @@ __device__ void tile_mma_dev(double *Cb, long ldc, int mr, int nc, const double 
 #pragma unroll
             for (int e = 0; e < 2; ++e) {
                 const int r = wm + i * 8 + (lane >> 2), c = wn + j * 8 + (lane & 3) * 2 + e;
-                cv[i][j][e] = (mode == 0 && r < mr && c < nc && !(diag && r < c)) ? Cb[(size_t) r + (size_t) c * ldc] : 0.0;
+                cv[i][j][e] = (J.mode == 0 && r < J.mr && c < J.nc && !(J.diag && r < c))
+                                  ? J.C[(size_t) r + (size_t) c * J.ldc]
+                                  : 0.0;
             }
-    cpa_wait_all();
-    __syncthreads();
-    double acc[4][2][2];
+}
+
+// acc = As * Bs^T over k < kp (8 warps: a 32 x 16 block of 8 x 8 DMMA tiles each).
+__device__ __forceinline__ void dmma_tile(const double *As, const double *Bs, int kp, double (&acc)[4][2][2]) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int wm = (w & 1) * 32, wn = (w >> 1) * 16;
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
@@ -357,6 +373,14 @@ __device__ void tile_mma_dev(double *Cb, long ldc, int mr, int nc, const double 
 #pragma unroll
             for (int j = 0; j < 2; ++j) dmma_c(acc[i][j][0], acc[i][j][1], a[i], b[j]);
     }
+}
+
+// Write the job's result; with Ct also transposed to Ct (pitch ldct), with Csm also
+// into shared memory (pitch TP, zeros outside the written entries).
+__device__ __forceinline__ void store_tile(const TileJob &J, const double (&cv)[4][2][2],
+                                           const double (&acc)[4][2][2], double *Ct, long ldct, double *Csm) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int wm = (w & 1) * 32, wn = (w >> 1) * 16;
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
         const int r = wm + i * 8 + (lane >> 2);
@@ -365,16 +389,77 @@ __device__ void tile_mma_dev(double *Cb, long ldc, int mr, int nc, const double 
 #pragma unroll
             for (int e = 0; e < 2; ++e) {
                 const int c = wn + j * 8 + (lane & 3) * 2 + e;
-                const bool valid = r < mr && c < nc && !(diag && r < c);
-                const double val = (mode == 0) ? cv[i][j][e] - acc[i][j][e] : (mode == 2) ? -acc[i][j][e] : acc[i][j][e];
+                const bool valid = r < J.mr && c < J.nc && !(J.diag && r < c);
+                const double val =
+                    (J.mode == 0) ? cv[i][j][e] - acc[i][j][e] : (J.mode == 2) ? -acc[i][j][e] : acc[i][j][e];
                 if (valid) {
-                    Cb[(size_t) r + (size_t) c * ldc] = val;
+                    J.C[(size_t) r + (size_t) c * J.ldc] = val;
                     if (Ct) Ct[(size_t) c + (size_t) r * ldct] = val;
                 }
                 if (Csm) Csm[r + c * TP] = valid ? val : 0.0;
             }
     }
+}
+
+// One tile product with its operands staged in regions 0 and 1. Operands are staged
+// first, so C may alias A or B (in-place panel solves).
+__device__ void tile_mma_dev(double *Cb, long ldc, int mr, int nc, const double *Ab, long lda, int ar,
+                             const double *Bb, long ldb, int bt, int bc, int nb, bool diag, int mode, double *sm,
+                             double *Ct = nullptr, long ldct = 0, double *Csm = nullptr) {
+    const TileJob J{Cb, ldc, mr, nc, Ab, lda, ar, Bb, ldb, bt, bc, nb, diag, mode};
+    double *As = sm, *Bs = sm + 64 * TP;
+    stage_job(J, As, Bs);
+    double cv[4][2][2];
+    load_c(J, cv);  // while the operand copies are in flight
+    cpa_wait_all();
     __syncthreads();
+    double acc[4][2][2];
+    dmma_tile(As, Bs, (nb + 3) & ~3, acc);
+    store_tile(J, cv, acc, Ct, ldct, Csm);
+    __syncthreads();
+}
+
+// Mode-0 jobs t0, t0 + step, ... (< t1) of one block, double buffered: the operands
+// of the next job are copied into the other pair of regions (0/1 and 2/3) and its C
+// entries loaded into registers while the current job's products run. The jobs'
+// C tiles must be disjoint from each other and from every operand.
+template <typename JobOf>
+__device__ void tile_stream(JobOf job_of, long t0, long t1, long step, double *sm) {
+    if (t0 >= t1) return;
+    TileJob cur, nxt;
+    job_of(t0, cur);
+    int b = 0;
+    stage_job(cur, sm + (size_t) (2 * b) * 64 * TP, sm + (size_t) (2 * b + 1) * 64 * TP);
+    asm volatile("cp.async.commit_group;\n" ::);
+    double cv[4][2][2], cvn[4][2][2];
+    load_c(cur, cv);
+    for (long t = t0;; t += step) {
+        const bool more = t + step < t1;
+        if (more) {
+            job_of(t + step, nxt);
+            stage_job(nxt, sm + (size_t) (2 * (b ^ 1)) * 64 * TP, sm + (size_t) (2 * (b ^ 1) + 1) * 64 * TP);
+            asm volatile("cp.async.commit_group;\n" ::);
+            load_c(nxt, cvn);
+            asm volatile("cp.async.wait_group 1;\n" ::);
+        } else {
+            asm volatile("cp.async.wait_group 0;\n" ::);
+        }
+        __syncthreads();
+        double acc[4][2][2];
+        dmma_tile(sm + (size_t) (2 * b) * 64 * TP, sm + (size_t) (2 * b + 1) * 64 * TP, (cur.nb + 3) & ~3, acc);
+        store_tile(cur, cv, acc, nullptr, 0, nullptr);
+        __syncthreads();  // the buffer just read may be refilled
+        if (!more) break;
+        cur = nxt;
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+                cv[i][j][0] = cvn[i][j][0];
+                cv[i][j][1] = cvn[i][j][1];
+            }
+        b ^= 1;
+    }
 }
 
 __device__ __forceinline__ void tri_index(long t, int &ti, int &tj) {
@@ -475,17 +560,16 @@ __global__ void __launch_bounds__(COOP_THREADS, 1) potrf_coop_kernel(double *L, 
         const int nworker = (gridDim.x > 1) ? (int) gridDim.x - 1 : 1;
         const int wid = (gridDim.x > 1) ? (int) blockIdx.x - 1 : 0;
         if (wid >= 0) {
-            for (long t = 1 + wid; t < ntile + nk; t += nworker) {
-                if (t >= ntile) {
-                    k_final_tile(Dinv, ldd, K, KT, ld, n, bj, (int) (t - ntile), sm);
-                    continue;
-                }
+            auto trailing = [&](long t, TileJob &J) {
                 int ti, tj;
                 tri_index(t, ti, tj);
                 const int mr = min(64, rows - ti * 64), nc = min(64, rows - tj * 64);
-                tile_mma_dev(A22 + (size_t) ti * 64 + (size_t) tj * 64 * ld, ld, mr, nc, P + ti * 64, ld, mr,
-                             P + tj * 64, ld, 1, nc, nb, ti == tj, 0, sm);
-            }
+                J = TileJob{A22 + (size_t) ti * 64 + (size_t) tj * 64 * ld, ld, mr, nc, P + ti * 64, ld, mr,
+                            P + tj * 64, ld, 1, nc, nb, ti == tj, 0};
+            };
+            tile_stream(trailing, 1 + wid, ntile, nworker, sm);
+            for (long t = 1 + wid; t < ntile + nk; t += nworker)
+                if (t >= ntile) k_final_tile(Dinv, ldd, K, KT, ld, n, bj, (int) (t - ntile), sm);
         }
         if (blockIdx.x == 1) CHOL_STAMP(pb + 3);
         grid.sync();
@@ -501,7 +585,7 @@ __global__ void __launch_bounds__(COOP_THREADS, 1) potrf_coop_kernel(double *L, 
     for (int c = blockIdx.x; c <= bj; c += gridDim.x) k_final_tile(Dinv, ldd, K, KT, ld, n, bj, c, sm);
 }
 
-__global__ void __launch_bounds__(COOP_THREADS) trtri_coop_kernel(const double *L, double *K, long ld, int n,
+__global__ void __launch_bounds__(COOP_THREADS, 1) trtri_coop_kernel(const double *L, double *K, long ld, int n,
                                                                   const double *Dinv, long ldd) {
     cg::grid_group grid = cg::this_grid();
     extern __shared__ double sm[];
@@ -520,14 +604,15 @@ __global__ void __launch_bounds__(COOP_THREADS) trtri_coop_kernel(const double *
         if (rows <= 0) break;
         const int rt = (rows + 63) / 64;
         const long ntile = (long) rt * nchunk;
-        for (long t = blockIdx.x; t < ntile; t += gridDim.x) {
+        // C = K[cend + 64 ti.., 64 tj..] -= L[cend + 64 ti.., i0..i0+nb) * K[i0..i0+nb, 64 tj..]
+        auto update = [&](long t, TileJob &J) {
             const int ti = (int) (t % rt), tj = (int) (t / rt);
             const int mr = min(64, rows - ti * 64), nc = min(64, cend - tj * 64);
-            // C = K[cend + 64 ti.., 64 tj..] -= L[cend + 64 ti.., i0..i0+nb) * K[i0..i0+nb, 64 tj..]
-            tile_mma_dev(K + (size_t) (cend + ti * 64) + (size_t) tj * 64 * ld, ld, mr, nc,
-                         L + (size_t) (cend + ti * 64) + (size_t) i0 * ld, ld, mr, K + i0 + (size_t) tj * 64 * ld, ld,
-                         0, nc, nb, false, 0, sm);
-        }
+            J = TileJob{K + (size_t) (cend + ti * 64) + (size_t) tj * 64 * ld, ld, mr, nc,
+                        L + (size_t) (cend + ti * 64) + (size_t) i0 * ld, ld, mr, K + i0 + (size_t) tj * 64 * ld, ld,
+                        0, nc, nb, false, 0};
+        };
+        tile_stream(update, blockIdx.x, ntile, gridDim.x, sm);
         grid.sync();
     }
 }
@@ -565,7 +650,7 @@ int coop_grid(const void *fn) {
     static int cached[2] = {0, 0};
     const int slot = (fn == (const void *) potrf_coop_kernel) ? 0 : 1;
     if (cached[slot]) return cached[slot];
-    const int smem = (slot == 0 ? SM_DOUBLES_POTRF : SM_DOUBLES) * (int) sizeof(double);
+    const int smem = SM_DOUBLES * (int) sizeof(double);
     HB_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     int dev = 0, sms = 0, per = 0;
     cudaGetDevice(&dev);
@@ -602,7 +687,7 @@ bool coop_factorize_enqueue(cudaStream_t s, DenseFactor &F, const double *S, lon
     void *args[] = {&Lp, &ld, &nn, &Dp, &ldd, &ip, &Kp, &KTp};
     const bool timed = kstat_on(KF_POTRF);
     if (timed) kstat_begin(KF_POTRF, s, (double) n * n * n / 3.0);
-    cudaError_t e = cudaLaunchCooperativeKernel(fn, hb::counted(grid), COOP_THREADS, args, SM_DOUBLES_POTRF * sizeof(double), s);
+    cudaError_t e = cudaLaunchCooperativeKernel(fn, hb::counted(grid), COOP_THREADS, args, SM_DOUBLES * sizeof(double), s);
     if (timed) kstat_end(s);
     if (e != cudaSuccess) {
         cudaGetLastError();

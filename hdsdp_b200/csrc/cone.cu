@@ -663,6 +663,10 @@ static void add_host(std::vector<double> &dst, const double *d_src, double *h_bu
     for (int i = 0; i < m; ++i) dst[i] += scale * h_buf[i];
 }
 
+// Smallest block order for which split precision also forms S^-1 on the tensor cores
+// (the n^3/3 product; below it the FP64 product takes tens of microseconds).
+constexpr int kSplitInverseMinN = 1024;
+
 // sdpDenseConeGetKKT / GetKKTByFixedStrategy (interface/hdsdp_conic_sdp.c:1722-1872)
 hdsdp_retcode KKT::build(SdpCone &cone, int type) {
     double t0 = wall();
@@ -676,7 +680,13 @@ hdsdp_retcode KKT::build(SdpCone &cone, int type) {
         Wp = primalX;
     } else {
         double ti = wall();
-        compute_inverse(s, cone.Fvar, cone.W, ld);
+        // split precision: W = K^T K on the tensor cores once n makes the product worth it
+        bool done = false;
+        if (cone.dev.precision == 1 && n >= kSplitInverseMinN) {
+            compute_inverse_factor(s, cone.Fvar);
+            done = cone.dev.split_inverse(cone.Fvar.K, cone.W, ld);
+        }
+        if (!done) compute_inverse(s, cone.Fvar, cone.W, ld);
         if (tm) {
             HB_CUDA(cudaStreamSynchronize(s));
             tm->s_inverse += wall() - ti;

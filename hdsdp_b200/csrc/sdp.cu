@@ -670,6 +670,22 @@ void SdpDevice::schur_matrix(const double *W, long ldW, double *M, long ldM, con
     HB_CUDA(cudaGetLastError());
 }
 
+bool SdpDevice::split_inverse(const double *Kinv, double *W, long ldW) {
+    if (!opKT.hi || opKT.rows != n || opKT.k != n) {
+        if (!opKT.alloc(n, n)) return false;
+    }
+    split_from_f64(stream, opKT, Kinv, ld, true);  // the rows of the operand are the columns of Kinv
+    SplitGemm g;
+    g.M = g.N = g.K = n;
+    g.lower_tiles = true;
+    g.a_upper = true;  // column i of Kinv vanishes above row i
+    g.C = W;
+    g.ldc = ldW;
+    if (!split_gemm(stream, opKT, opKT, g)) return false;
+    symmetrize_lower(stream, n, W, ldW);
+    return true;
+}
+
 void SdpDevice::inner_all(const double *Z, long ldZ, double *out, bool reuse_v) {
     cudaStream_t s = stream;
     if (nsp > 0) inner_sp_kernel<<<hb::counted(grid1(nsp)), 256, 0, s>>>(nsp, sp_id, sp_ptr, sp_r, sp_c, sp_v, Z, ldZ, out);

@@ -122,6 +122,11 @@ struct SdpDevice {
     void inner_all_sq(const double *W, long ldW, double *out, bool reuse_v = false, bool reuse_vt = false);
     // <C, Z>
     double c_inner(const double *Z, long ldZ);
+    // W = S^-1 = Kinv^T Kinv (Kinv = L^-1, lower) as the lower part of a BF16x3 split
+    // product on the tensor cores, then mirrored to the full matrix. Used in split
+    // precision for the blocks that read W (sparse, sparse rank-one and dense
+    // coefficients). False if the tensor-core path is unavailable.
+    bool split_inverse(const double *Kinv, double *W, long ldW);
 };
 
 }  // namespace hb

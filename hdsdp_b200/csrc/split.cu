@@ -117,7 +117,7 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float *v) {
 struct KernelArgs {
     int M, N, nkb;             // nkb: K blocks per product (K padded to 64)
     int tiles_m, tiles_n;
-    int lower_tiles, a_lower;
+    int lower_tiles, a_lower, a_upper;
     int epi;
     double alpha, beta;
     double *C;
@@ -142,7 +142,8 @@ __device__ __forceinline__ void tile_of(const KernelArgs &p, int b, int &tm, int
     }
 }
 
-// Persistent: CTA b takes tiles b, b + grid, ... The producer warp streams K blocks of
+// Persistent: each CTA takes one tile per round of gridDim.x tiles (see tile_seq). The
+// producer warp streams K blocks of
 // all its tiles through a ring of stages, each holding the four operand tiles of one
 // K block (A hi, A lo, B hi, B lo), from which the MMA thread issues the three
 // products hi*hi, hi*lo, lo*hi into one FP32 accumulator. Tiles alternate between two
@@ -166,7 +167,16 @@ __global__ void __launch_bounds__(THREADS, 1)
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int ntiles = p.lower_tiles ? p.tiles_m * (p.tiles_m + 1) / 2 : p.tiles_m * p.tiles_n;
-    auto kblocks = [&](int m0) { return p.a_lower ? min(p.nkb, (m0 + BM + BK - 1) / BK) : p.nkb; };
+    // Tile i of this CTA (i = 0, 1, ...): rounds of gridDim.x tiles, dealt left to right
+    // in even rounds and right to left in odd ones, which evens out the work when the
+    // tiles' K ranges shrink along the tile order (triangular operands). Increasing in i.
+    auto tile_seq = [&](int i) {
+        const int pos = (i & 1) ? (int) gridDim.x - 1 - (int) blockIdx.x : (int) blockIdx.x;
+        return i * (int) gridDim.x + pos;
+    };
+    // the K blocks a tile needs: [kfirst, klast)
+    auto klast = [&](int m0) { return p.a_lower ? min(p.nkb, (m0 + BM + BK - 1) / BK) : p.nkb; };
+    auto kfirst = [&](int m0) { return p.a_upper ? min(m0 / BK, p.nkb - 1) : 0; };
 
     if (threadIdx.x == 0) {
         for (int st = 0; st < STAGES; ++st) {
@@ -195,11 +205,11 @@ __global__ void __launch_bounds__(THREADS, 1)
         // producer
         int it = 0;
         bool ok = true;
-        for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+        for (int i = 0, tile; ok && (tile = tile_seq(i)) < ntiles; ++i) {
             int tm, tn;
             tile_of(p, tile, tm, tn);
-            const int m0 = tm * BM, n0 = tn * BN, nkb = kblocks(m0);
-            for (int kb = 0; kb < nkb; ++kb, ++it) {
+            const int m0 = tm * BM, n0 = tn * BN, kb0 = kfirst(m0), kb1 = klast(m0);
+            for (int kb = kb0; kb < kb1; ++kb, ++it) {
                 const int st = it % STAGES;
                 const uint32_t ph = (uint32_t) (it / STAGES) & 1u;
                 if (!mbar_wait(empty(st), ph ^ 1u)) {
@@ -216,17 +226,17 @@ __global__ void __launch_bounds__(THREADS, 1)
         }
     } else if (warp == 1 && lane == 0) {
         // MMA issuer: per stage, four K=16 steps of each of the three products
-        int it = 0, tc = 0;
+        int it = 0;
         bool ok = true;
-        for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x, ++tc) {
+        for (int tc = 0, tile; ok && (tile = tile_seq(tc)) < ntiles; ++tc) {
             int tm, tn;
             tile_of(p, tile, tm, tn);
-            const int nkb = kblocks(tm * BM);
+            const int kb0 = kfirst(tm * BM), kb1 = klast(tm * BM);
             const int b = tc & 1;
             if (!mbar_wait(acc_empty(b), ((uint32_t) (tc >> 1) & 1u) ^ 1u)) break;
             fence_after();
             const uint32_t d = tmem + (uint32_t) (b * BN);
-            for (int kb = 0; kb < nkb; ++kb, ++it) {
+            for (int kb = kb0; kb < kb1; ++kb, ++it) {
                 const int st = it % STAGES;
                 const uint32_t ph = (uint32_t) (it / STAGES) & 1u;
                 if (!mbar_wait(full(st), ph)) {
@@ -239,7 +249,7 @@ __global__ void __launch_bounds__(THREADS, 1)
                 const uint64_t dbh = smem_desc(sa + 2 * TILE_BYTES), dbl = smem_desc(sa + 3 * TILE_BYTES);
 #pragma unroll
                 for (int k = 0; k < BK / 16; ++k)
-                    mma_bf16(d, dah + (uint64_t) (2 * k), dbh + (uint64_t) (2 * k), (kb | k) != 0 ? 1u : 0u);
+                    mma_bf16(d, dah + (uint64_t) (2 * k), dbh + (uint64_t) (2 * k), (kb != kb0 || k != 0) ? 1u : 0u);
 #pragma unroll
                 for (int k = 0; k < BK / 16; ++k) mma_bf16(d, dah + (uint64_t) (2 * k), dbl + (uint64_t) (2 * k), 1u);
 #pragma unroll
@@ -251,8 +261,7 @@ __global__ void __launch_bounds__(THREADS, 1)
     } else if (warp >= 2) {
         // epilogue: warp w reads accumulator lanes 32 * (w % 4) ...
         const int q = warp & 3;
-        int tc = 0;
-        for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++tc) {
+        for (int tc = 0, tile; (tile = tile_seq(tc)) < ntiles; ++tc) {
             int tm, tn;
             tile_of(p, tile, tm, tn);
             const int m0 = tm * BM, n0 = tn * BN;
@@ -440,6 +449,7 @@ bool split_gemm(cudaStream_t s, const SplitOperand &A, const SplitOperand &B, co
     p.tiles_n = (g.N + BN - 1) / BN;
     p.lower_tiles = g.lower_tiles ? 1 : 0;
     p.a_lower = g.a_lower ? 1 : 0;
+    p.a_upper = g.a_upper ? 1 : 0;
     p.epi = g.epi;
     p.alpha = g.alpha;
     p.beta = g.beta;
@@ -469,6 +479,7 @@ bool split_gemm(cudaStream_t s, const SplitOperand &A, const SplitOperand &B, co
         double f = 3.0 * 2.0 * g.M * (double) g.N * g.K;
         if (g.lower_tiles) f *= 0.5;
         if (g.a_lower) f *= 0.5;
+        if (g.a_upper) f *= (g.lower_tiles ? 1.0 / 3.0 : 0.5);  // lower part of a product of triangles: n^3/3 per product
         kstat_begin(KF_SPLIT_GEMM, s, f);
     }
     split_gemm_kernel<<<hb::counted((int) blocks), THREADS, SMEM_BYTES, s>>>(A.map_hi, A.map_lo, B.map_hi, B.map_lo,

@@ -9,10 +9,12 @@
 // Operands are stored K-major: row r of an operand holds its K entries
 // contiguously (BF16, rows padded to 128, K padded to 64), the layout the
 // TMA engine copies into 128-byte-swizzled shared-memory tiles for
-// tcgen05.mma. One CTA computes a 128 x 128 output tile: a producer warp
-// issues TMA copies into a 4-stage ring, one thread issues the MMAs and
-// commits each stage back to the producer, and four warps read the
-// accumulator out of tensor memory for the epilogue.
+// tcgen05.mma. Persistent CTAs take 128 x 128 output tiles in turn: a
+// producer warp streams the four operand tiles of each K block (A hi, A lo,
+// B hi, B lo) into a 3-stage ring by TMA, one thread issues the three
+// products and commits each stage back to the producer, and four warps read
+// the accumulator out of tensor memory for the epilogue, from one of two
+// accumulators while the next tile fills the other.
 #pragma once
 #include <cuda.h>
 #include <cuda_bf16.h>
@@ -44,6 +46,7 @@ struct SplitGemm {
     int M = 0, N = 0, K = 0;
     bool lower_tiles = false;  // compute only tiles meeting r >= c (write only r >= c)
     bool a_lower = false;      // A(r, k) = 0 for k > r: stop the K loop at the tile's last row
+    bool a_upper = false;      // A(r, k) = 0 for k < r: start the K loop at the tile's first row
     int epi = SPLIT_EPI_F64;
     double alpha = 1.0, beta = 0.0;
     double *C = nullptr;
