@@ -235,6 +235,19 @@ def cholesky(S):
     return out, ld.value, r == 0
 
 
+def cholesky_solve(S, b):
+    """x with S x = b by the Cholesky factor and blocked substitution (hdsdpb_cholesky_solve);
+    None if S is not positive definite."""
+    S = np.asfortranarray(S, dtype=np.float64)
+    b = np.ascontiguousarray(b, dtype=np.float64)
+    n = S.shape[0]
+    x = np.zeros(n)
+    r = _lib.load().hdsdpb_cholesky_solve(n, _dp(S), _dp(b), _dp(x))
+    if r < 0:
+        raise RuntimeError("hdsdpb_cholesky_solve failed")
+    return None if r == 1 else x
+
+
 def inverse(S):
     """S^-1 of a symmetric positive definite matrix on the GPU (None if not positive definite)."""
     L = _lib.load()

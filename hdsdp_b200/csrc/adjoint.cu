@@ -106,19 +106,33 @@ double host_scalar(cudaStream_t s, const double *d, double *h) {
     return *h;
 }
 
-// v = M^-1 u with the explicit inverse factor K (M = L L^T, K = L^-1) and two steps of
-// iterative refinement (M is ill-conditioned in the directions of the optimal face).
-void schur_solve(cudaStream_t s, AdjointState &a, const double *u, double *v) {
+// Schur systems of at least this order are solved with L (triangular solves) instead
+// of through the explicit inverse factor, which would cost a second factorisation.
+constexpr int kAdjTriSolveMinM = 6000;
+
+// x = M^-1 y with the factor: through K = L^-1 (M = L L^T) for small m, by triangular
+// solves with L for large m.
+bool factor_apply(cudaStream_t s, AdjointState &a, const double *y, double *x) {
+    if (a.FM.fuse_k) {
+        coldot(s, a.m, a.m, a.FM.KT, a.ldm, y, a.d_t, 1.0, 0.0, 2);  // t = K y
+        coldot(s, a.m, a.m, a.FM.K, a.ldm, a.d_t, x, 1.0, 0.0, 1);   // x = K^T t
+        return true;
+    }
+    return chol_solve(s, a.FM, y, x);
+}
+
+// v = M^-1 u with two steps of iterative refinement (M is ill-conditioned in the
+// directions of the optimal face).
+bool schur_solve(cudaStream_t s, AdjointState &a, const double *u, double *v) {
     const int m = a.m;
-    coldot(s, m, m, a.FM.KT, a.ldm, u, a.d_t, 1.0, 0.0, 2);   // t = K u
-    coldot(s, m, m, a.FM.K, a.ldm, a.d_t, v, 1.0, 0.0, 1);    // v = K^T t
+    bool ok = factor_apply(s, a, u, v);
     for (int it = 0; it < 2; ++it) {
         coldot(s, m, m, a.M, a.ldm, v, a.d_r, -1.0, 0.0, 0);  // r = -M v
         axpy(s, m, 1.0, u, a.d_r);                           // r = u - M v
-        coldot(s, m, m, a.FM.KT, a.ldm, a.d_r, a.d_t, 1.0, 0.0, 2);
-        coldot(s, m, m, a.FM.K, a.ldm, a.d_t, a.d_r, 1.0, 0.0, 1);
+        ok = ok && factor_apply(s, a, a.d_r, a.d_r);
         axpy(s, m, 1.0, a.d_r, v);
     }
+    return ok;
 }
 
 hdsdp_retcode prepare(hdsdp *h, AdjointState &a) {
@@ -137,7 +151,7 @@ hdsdp_retcode prepare(hdsdp *h, AdjointState &a) {
     HB_CUDA(hb::cmalloc(&a.d_scal, sizeof(double) * 4));
     HB_CUDA(hb::cmalloc_host(&a.h_scal, sizeof(double) * 4));
     a.FS.alloc(n);
-    a.FM.alloc(m, 1);
+    a.FM.alloc(m, m < kAdjTriSolveMinM ? 1 : 0);
     if (device_error_flag()) return HDSDP_RETCODE_MEMORY;
 
     // the solution in the user's units
@@ -207,7 +221,7 @@ hdsdp_retcode prepare(hdsdp *h, AdjointState &a) {
     c.dev.schur_matrix(a.N, ld, a.M, ldm);
     symmetrize_lower(s, m, a.M, ldm);
     if (!factorize(s, a.FM, a.M, ldm)) return HDSDP_RETCODE_FAILED;
-    compute_inverse_factor(s, a.FM);
+    if (a.FM.fuse_k) compute_inverse_factor(s, a.FM);
 
     // (column, row, col) of every stored value of the user's CSC data
     const user_data *u = h->usr;
@@ -275,7 +289,7 @@ hdsdp_retcode adjoint_vjp(hdsdp *h, AdjointState *&state, const double *gy, cons
         axpy(s, m, 1.0, a.d_r, a.d_u);
     }
     // v = M^-1 u
-    schur_solve(s, a, a.d_u, a.d_v);
+    if (!schur_solve(s, a, a.d_u, a.d_v)) return HDSDP_RETCODE_FAILED;
     // Z = N (A^T v - G_X) N
     c.dev.assemble(0.0, 1.0, a.d_v, 0.0, a.T2, ld);
     axpy(s, (int) (ld * n), -1.0, a.D, a.T2);
@@ -292,6 +306,7 @@ hdsdp_retcode adjoint_vjp(hdsdp *h, AdjointState *&state, const double *gy, cons
         HB_CUDA(cudaMemcpyAsync(gAx, a.d_gax, sizeof(double) * a.nnz, cudaMemcpyDeviceToHost, s));
     }
     HB_CUDA(cudaStreamSynchronize(s));
+    if (!a.FM.fuse_k && chol_solve_error()) return HDSDP_RETCODE_FAILED;
     return device_error_flag() ? HDSDP_RETCODE_FAILED : HDSDP_RETCODE_OK;
 }
 

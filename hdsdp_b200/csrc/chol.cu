@@ -617,6 +617,173 @@ __global__ void __launch_bounds__(COOP_THREADS, 1) trtri_coop_kernel(const doubl
     }
 }
 
+// Blocked substitution for L L^T x = b, one cooperative launch. The 64-row blocks of
+// the vector are dealt to the CTAs (block k to CTA k mod grid); a CTA keeps, in shared
+// memory, the accumulated products of its blocks with the solved ones. Forward sweep:
+// the owner of block j forms t_j = Dinv_j (b_j - acc_j), publishes it with flag_f[j] =
+// epoch, and every CTA then adds L_kj t_j to its blocks k > j. The owner of block j + 1
+// applies t_j to that block first and publishes t_{j+1} before its other updates, so
+// the chain from block to block holds one small product. After a grid barrier the
+// backward sweep does the same from the last block up with L^T and Dinv^T. Every wait
+// on a flag is bounded; on giving up the CTA raises g_tri_err and the rest skip their
+// work (every CTA still reaches the grid barrier).
+__device__ int g_tri_err = 0;
+constexpr long TRI_WAIT_LIMIT = 1L << 22;
+
+__device__ __forceinline__ bool tri_wait(const unsigned *flag, unsigned epoch) {
+    for (long it = 0; it < TRI_WAIT_LIMIT; ++it) {
+        if ((int) (*(volatile const unsigned *) flag - epoch) >= 0) return true;
+        if ((it & 1023) == 1023 && *(volatile int *) &g_tri_err) return false;
+    }
+    atomicExch(&g_tri_err, 1);
+    return false;
+}
+
+__global__ void __launch_bounds__(COOP_THREADS, 1)
+    tri_solve_coop_kernel(const double *__restrict__ L, long ld, int n, const double *__restrict__ Dinv, long ldd,
+                          const double *b, double *t, double *x, unsigned *flag_f, unsigned *flag_b,
+                          unsigned epoch) {
+    cg::grid_group grid = cg::this_grid();
+    extern __shared__ double sm[];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int G = gridDim.x, me = blockIdx.x;
+    const int nblk = (n + 63) / 64;
+    const int nown = (me < nblk) ? (nblk - 1 - me) / G + 1 : 0;
+    double *acc = sm;                    // nown x 64
+    double *xs = sm + (size_t) nown * 64; // the solved block being applied
+    double *xn = xs + 64;                // the block this CTA just published
+    double *red = xn + 64;               // 4 x 64 partial sums
+    __shared__ int abort_;
+    if (tid == 0) abort_ = 0;
+    for (int i = tid; i < nown * 64; i += blockDim.x) acc[i] = 0.0;
+    __syncthreads();
+    auto nbof = [&](int j) { return min(64, n - 64 * j); };
+    // v = rhs_j - acc_j, then out_j = Dinv_j v (transpose: Dinv_j^T v) into xn and out
+    auto finish = [&](int j, const double *rhs, double *out, bool transpose) {
+        const int nb = nbof(j);
+        double *a = acc + (size_t) (j / G) * 64;
+        if (tid < 64) red[tid] = (tid < nb) ? rhs[64 * j + tid] - a[tid] : 0.0;
+        __syncthreads();
+        // 8 warps x 8 outputs, lanes over the contraction index (two each)
+        for (int o = warp; o < 64; o += 8) {
+            double sum = 0.0;
+            if (o < nb) {  // warp-uniform; rows and columns of Dinv beyond nb are not read
+                for (int q = lane; q < nb; q += 32) {
+                    const double d = transpose ? Dinv[(size_t) (64 * j + q) + (size_t) o * ldd]
+                                               : Dinv[(size_t) (64 * j + o) + (size_t) q * ldd];
+                    sum += d * red[q];
+                }
+            }
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, off);
+            if (lane == 0) xn[o] = (o < nb) ? sum : 0.0;
+        }
+        __syncthreads();
+        if (tid < nb) out[64 * j + tid] = xn[tid];
+        __threadfence();
+        __syncthreads();
+    };
+    // forward: acc_k += L_kj v (v in xs)
+    auto update_f = [&](int k, int j) {
+        const int nbk = nbof(k);
+        const int r = tid & 63, q = tid >> 6;
+        double sum = 0.0;
+        if (r < nbk) {
+            const double *col = L + (size_t) (64 * k + r) + (size_t) (64 * j) * ld;
+            for (int c = 16 * q; c < 16 * q + 16; ++c) sum += col[(size_t) c * ld] * xs[c];
+        }
+        red[q * 64 + r] = sum;
+        __syncthreads();
+        if (tid < 64) acc[(size_t) (k / G) * 64 + tid] += red[tid] + red[64 + tid] + red[128 + tid] + red[192 + tid];
+        __syncthreads();
+    };
+    // backward: acc_k += L_jk^T v (v in xs), a warp per output
+    auto update_b = [&](int k, int j) {
+        const int nbj = nbof(j);
+        for (int o = warp; o < 64; o += 8) {
+            double sum = 0.0;
+            const double *col = L + (size_t) (64 * j) + (size_t) (64 * k + o) * ld;
+            for (int q = lane; q < nbj; q += 32) sum += col[q] * xs[q];
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, off);
+            if (lane == 0) acc[(size_t) (k / G) * 64 + o] += sum;
+        }
+        __syncthreads();
+    };
+    auto fetch = [&](const double *v, int j, const unsigned *flag) {
+        if (tid == 0 && !tri_wait(flag + j, epoch)) abort_ = 1;
+        __threadfence();
+        __syncthreads();
+        if (tid < 64) xs[tid] = (!abort_ && tid < nbof(j)) ? __ldcg(v + 64 * j + tid) : 0.0;
+        __syncthreads();
+    };
+    auto publish = [&](unsigned *flag, int j) {
+        if (tid == 0) atomicExch(flag + j, epoch);
+    };
+
+    const int last = (nown > 0) ? me + (nown - 1) * G : -1;  // this CTA's last block
+    // ---- forward sweep: t = L^-1 b
+    if (nown > 0 && !*(volatile int *) &g_tri_err) {
+        bool have_next = false;  // xn holds t_j, published by this CTA
+        if (me == 0) {
+            finish(0, b, t, false);
+            publish(flag_f, 0);
+            have_next = true;
+        }
+        for (int j = 0; j < last && !abort_; ++j) {
+            if (have_next) {
+                if (tid < 64) xs[tid] = xn[tid];
+                __syncthreads();
+                have_next = false;
+            } else {
+                fetch(t, j, flag_f);
+                if (abort_) break;
+            }
+            const int k1 = j + 1;
+            if (k1 % G == me) {
+                update_f(k1, j);
+                finish(k1, b, t, false);
+                publish(flag_f, k1);
+                have_next = true;
+            }
+            for (int k = (k1 % G == me) ? k1 + G : k1 + ((me - k1 % G + G) % G); k <= last; k += G)
+                if (k > j) update_f(k, j);
+        }
+    }
+    grid.sync();
+    // ---- backward sweep: x = L^-T t
+    for (int i = tid; i < nown * 64; i += blockDim.x) acc[i] = 0.0;
+    __syncthreads();
+    if (nown > 0 && !*(volatile int *) &g_tri_err) {
+        const int first = me;  // this CTA's first block
+        bool have_next = false;
+        if (me == (nblk - 1) % G) {
+            finish(nblk - 1, t, x, true);
+            publish(flag_b, nblk - 1);
+            have_next = true;
+        }
+        for (int j = nblk - 1; j > first && !abort_; --j) {
+            if (have_next) {
+                if (tid < 64) xs[tid] = xn[tid];
+                __syncthreads();
+                have_next = false;
+            } else {
+                fetch(x, j, flag_b);
+                if (abort_) break;
+            }
+            const int k1 = j - 1;
+            if (k1 % G == me) {
+                update_b(k1, j);
+                finish(k1, t, x, true);
+                publish(flag_b, k1);
+                have_next = true;
+            }
+            for (int k = me; k < j; k += G)
+                if (k != k1 || k1 % G != me) update_b(k, j);
+        }
+    }
+}
+
 __global__ void copy_lower_k(int n, const double *S, long lds, double *L, long ldl) {
     const long total = (long) n * n;
     for (long idx = blockIdx.x * (long) blockDim.x + threadIdx.x; idx < total; idx += (long) gridDim.x * blockDim.x) {
@@ -694,6 +861,55 @@ bool coop_factorize_enqueue(cudaStream_t s, DenseFactor &F, const double *S, lon
         return false;
     }
     return true;
+}
+
+bool chol_solve(cudaStream_t s, DenseFactor &F, const double *b, double *x) {
+    const int n = F.n;
+    if (n <= 0) return true;
+    const int nblk = (n + 63) / 64;
+    if (!F.d_flags) {
+        HB_CUDA(hb::cmalloc(&F.d_flags, sizeof(unsigned) * 2 * nblk));
+        HB_CUDA(cudaMemsetAsync(F.d_flags, 0, sizeof(unsigned) * 2 * nblk, s));
+        F.epoch = 0;
+    }
+    if (!F.d_tmp) HB_CUDA(hb::cmalloc(&F.d_tmp, sizeof(double) * n));
+    if (!F.d_flags || !F.d_tmp) return false;
+    F.epoch += 1;
+    const void *fn = (const void *) tri_solve_coop_kernel;
+    const int G = std::min(nblk, sm_count());
+    const int nown = (nblk + G - 1) / G;
+    const int smem = (nown * 64 + 2 * 64 + 4 * 64) * (int) sizeof(double);
+    static int smem_set = 0;
+    if (smem > smem_set) {
+        if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess) return false;
+        smem_set = smem;
+    }
+    const double *Lp = F.L;
+    long ld = F.ld;
+    int nn = n;
+    const double *Dp = F.Dinv;
+    long ldd = F.ld;
+    const double *bp = b;
+    double *tp = F.d_tmp, *xp = x;
+    unsigned *ff = F.d_flags, *fb = F.d_flags + nblk;
+    unsigned ep = F.epoch;
+    void *args[] = {&Lp, &ld, &nn, &Dp, &ldd, &bp, &tp, &xp, &ff, &fb, &ep};
+    cudaError_t e = cudaLaunchCooperativeKernel(fn, hb::counted(G), COOP_THREADS, args, smem, s);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return true;
+}
+
+int chol_solve_error() {
+    int h = 0;
+    cudaMemcpyFromSymbol(&h, g_tri_err, sizeof(int));
+    if (h) {
+        const int z = 0;
+        cudaMemcpyToSymbol(g_tri_err, &z, sizeof(int));
+    }
+    return h;
 }
 
 bool coop_inverse_enqueue(cudaStream_t s, DenseFactor &F) {

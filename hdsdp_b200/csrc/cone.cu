@@ -9,6 +9,12 @@
 
 namespace hb {
 
+// Schur systems of at least this order are solved by triangular solves with L rather
+// than through K = L^-1: forming K costs as much as the factorisation, while a solve
+// with L reads L once.
+constexpr int kTriSolveMinM = 6000;
+
+
 static double wall() {
     using namespace std::chrono;
     return duration<double>(steady_clock::now().time_since_epoch()).count();
@@ -625,7 +631,9 @@ void KKT::init(int m_, cudaStream_t stream, Timers *t) {
     ldm = pad_ld(m);
     HB_CUDA(hb::cmalloc(&M, sizeof(double) * ldm * m));
     HB_CUDA(cudaMemsetAsync(M, 0, sizeof(double) * ldm * m, s));
-    F.alloc(m, 1);  // the Schur solves always use K
+    // Up to kTriSolveMinM the Schur solves use K = L^-1 (formed inside the factorisation);
+    // above it they are triangular solves with L, which read L once instead of forming K.
+    F.alloc(m, m < kTriSolveMinM ? 1 : 0);
     asinv.assign(m, 0.0);
     asinvrd.assign(m, 0.0);
     asinvcs.assign(m, 0.0);
@@ -814,7 +822,7 @@ hdsdp_retcode KKT::factorize() {
         }
         if (ok) printf("KKT system is almost indefinite. Using a shifted Cholesky factor. \n");
     }
-    if (ok) compute_inverse_factor(s, F);
+    if (ok && F.fuse_k) compute_inverse_factor(s, F);
     HB_CUDA(cudaStreamSynchronize(s));
     if (tm) tm->schur_factor += wall() - t0;
     return ok && !device_error_flag() ? HDSDP_RETCODE_OK : HDSDP_RETCODE_FAILED;
@@ -825,16 +833,27 @@ hdsdp_retcode KKT::solve(const double *rhs, double *lhs) {
     double t0 = wall();
     std::memcpy(h_buf, rhs, sizeof(double) * m);
     HB_CUDA(cudaMemcpyAsync(d_rhs, h_buf, sizeof(double) * m, cudaMemcpyHostToDevice, s));
-    coldot(s, m, m, F.KT, F.ld, d_rhs, d_t, 1.0, 0.0, 2);   // t = K b
-    coldot(s, m, m, F.K, F.ld, d_t, d_x, 1.0, 0.0, 1);      // x = K^T t
+    bool ok = true;
+    if (F.fuse_k) {
+        coldot(s, m, m, F.KT, F.ld, d_rhs, d_t, 1.0, 0.0, 2);   // t = K b
+        coldot(s, m, m, F.K, F.ld, d_t, d_x, 1.0, 0.0, 1);      // x = K^T t
+    } else {
+        ok = chol_solve(s, F, d_rhs, d_x);
+    }
     HB_CUDA(cudaMemcpyAsync(d_r, d_rhs, sizeof(double) * m, cudaMemcpyDeviceToDevice, s));
     coldot(s, m, m, M, ldm, d_x, d_r, -1.0, 1.0, 0);        // r = b - M x
     if (shift != 0.0) axpy(s, m, shift, d_x, d_r);          // residual of the unshifted system
-    coldot(s, m, m, F.KT, F.ld, d_r, d_t, 1.0, 0.0, 2);
-    coldot(s, m, m, F.K, F.ld, d_t, d_r, 1.0, 0.0, 1);
+    if (F.fuse_k) {
+        coldot(s, m, m, F.KT, F.ld, d_r, d_t, 1.0, 0.0, 2);
+        coldot(s, m, m, F.K, F.ld, d_t, d_r, 1.0, 0.0, 1);
+    } else {
+        ok = ok && chol_solve(s, F, d_r, d_r);
+    }
     axpy(s, m, 1.0, d_r, d_x);
     HB_CUDA(cudaMemcpyAsync(h_buf, d_x, sizeof(double) * m, cudaMemcpyDeviceToHost, s));
     HB_CUDA(cudaStreamSynchronize(s));
+    if (!F.fuse_k && chol_solve_error()) ok = false;
+    if (!ok) device_error_flag() = 1;
     std::memcpy(lhs, h_buf, sizeof(double) * m);
     if (tm) {
         tm->schur_solve += wall() - t0;

@@ -157,6 +157,35 @@ int hdsdpb_cholesky(int n, const double *S, double *L, double *logdiag) {
     return ok ? 0 : 1;
 }
 
+int hdsdpb_cholesky_solve(int n, const double *S, const double *b, double *x) {
+    if (n < 0 || (n > 0 && (!S || !b || !x))) return -1;
+    if (n == 0) return 0;
+    cudaStream_t s;
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return -1;
+    const long ld = pad_ld(n);
+    double *dS = nullptr, *dx = nullptr;
+    hb::cmalloc(&dS, sizeof(double) * ld * n);
+    hb::cmalloc(&dx, sizeof(double) * n);
+    cudaMemcpy2D(dS, sizeof(double) * ld, S, sizeof(double) * n, sizeof(double) * n, n, cudaMemcpyHostToDevice);
+    cudaMemcpy(dx, b, sizeof(double) * n, cudaMemcpyHostToDevice);
+    DenseFactor F;
+    F.alloc(n, 0);
+    bool ok = factorize(s, F, dS, ld);
+    int ret = ok ? 0 : 1;
+    if (ok) {
+        if (!chol_solve(s, F, dx, dx)) ret = -1;
+        cudaMemcpyAsync(x, dx, sizeof(double) * n, cudaMemcpyDeviceToHost, s);
+    }
+    cudaStreamSynchronize(s);
+    if (ok && chol_solve_error()) ret = -1;
+    F.release();
+    hb::cache_free(dS);
+    hb::cache_free(dx);
+    cudaStreamDestroy(s);
+    if (device_error_flag()) return -1;
+    return ret;
+}
+
 int hdsdpb_inverse(int n, const double *S, double *Sinv) {
     if (n < 0 || (n > 0 && (!S || !Sinv))) return -1;
     if (n == 0) return 0;
@@ -286,7 +315,7 @@ extern "C" int hdsdpb_kernel_timing(int which, int n, int reps, double *ms) {
     fill_spd_kernel<<<hb::counted(1024), 256, 0, s>>>(n, B, ld, 7u);
     fill(s, x, 1.0, n);
     DenseFactor F;
-    F.alloc(n, which == 7 ? 1 : (which == 8 ? 0 : -1));
+    F.alloc(n, which == 7 ? 1 : ((which == 8 || which == 9) ? 0 : -1));
     Lanczos lz;
     if (which == 5) lz.init(n, s);
     cudaEvent_t e0, e1;
@@ -303,9 +332,10 @@ extern "C" int hdsdpb_kernel_timing(int which, int n, int reps, double *ms) {
             case 6: gemm(s, n, n, 64, -1.0, A, ld, 0, B, ld, 1, 1.0, Cm, ld, GEMM_C_LOWER); break;
             case 7:
             case 8: factorize_async(s, F, A, ld); break;
+            case 9: chol_solve(s, F, x, y); break;
         }
     };
-    if (which == 3 || which == 5) factorize(s, F, A, ld);
+    if (which == 3 || which == 5 || which == 9) factorize(s, F, A, ld);
     for (int i = 0; i < 2; ++i) once();
     cudaStreamSynchronize(s);
     cudaEventRecord(e0, s);
@@ -318,10 +348,11 @@ extern "C" int hdsdpb_kernel_timing(int which, int n, int reps, double *ms) {
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (which == 5) lz.release();
+    const bool solve_failed = (which == 9) && chol_solve_error();
     F.release();
     for (double *p : {A, B, Cm, x, y}) hb::cache_free(p);
     cudaStreamDestroy(s);
-    return device_error_flag() ? -1 : 0;
+    return (device_error_flag() || solve_failed) ? -1 : 0;
 }
 
 namespace {

@@ -756,6 +756,12 @@ int grid_for(long total, int threads = 256) {
 }  // namespace
 
 void DenseFactor::alloc(int n_, int fuse_inverse) {
+    // the solve scratch is sized for n: drop any from an earlier size
+    if (d_flags) hb::cache_free(d_flags);
+    if (d_tmp) hb::cache_free(d_tmp);
+    d_flags = nullptr;
+    d_tmp = nullptr;
+    epoch = 0;
     n = n_;
     ld = pad_ld(n);
     HB_CUDA(hb::cmalloc(&L, sizeof(double) * ld * n));
@@ -780,6 +786,11 @@ void DenseFactor::release() {
     if (K) hb::cache_free(K);
     if (KT) hb::cache_free(KT);
     if (d_info) hb::cache_free(d_info);
+    if (d_flags) hb::cache_free(d_flags);
+    if (d_tmp) hb::cache_free(d_tmp);
+    d_flags = nullptr;
+    d_tmp = nullptr;
+    epoch = 0;
     if (h_info) hb::cache_free_host(h_info);
     L = Dinv = K = KT = nullptr;
     d_info = nullptr;

@@ -55,9 +55,22 @@ struct DenseFactor {
     // fuse_inverse: the factorisation kernel also forms K = L^-1 and K^T (worth it for a
     // factor whose inverse is always used, and for small n where the K work hides behind
     // the panel chain); -1 picks n <= kFuseInverseMax.
+    // scratch of chol_solve (allocated on first use): per-block ready flags of the forward
+    // and backward sweeps, the intermediate vector, and the epoch tag of the last solve
+    unsigned *d_flags = nullptr;
+    double *d_tmp = nullptr;
+    unsigned epoch = 0;
     void alloc(int n_, int fuse_inverse = -1);
     void release();
 };
+
+// x = (L L^T)^-1 b with the factor's L and diagonal-block inverses (no K needed): a
+// forward and a backward blocked substitution in one cooperative launch. b and x are
+// device vectors of length n and may alias. Returns false if the launch failed or a
+// bounded wait inside it gave up.
+bool chol_solve(cudaStream_t s, DenseFactor &F, const double *b, double *x);
+// Reads and clears the flag raised when a wait inside chol_solve gave up (synchronising).
+int chol_solve_error();
 
 // Copy the lower triangle of S (n x n, ldS) into F.L and factorise it.
 // Returns true if S is positive definite (dpotrf semantics: fails on a

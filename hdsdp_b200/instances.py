@@ -222,4 +222,7 @@ WORKLOADS = {
     "rank1_n1000_m2000": lambda: rank_one(1000, 2000, 0.1, seed=3),
     "maxcut_n8000": lambda: maxcut(8000, seed=4, n_edges=40000, weights=(0.5, 1.5)),
     "theta_adjoint_n200": lambda: theta_adjoint(200, 0.1, 0.2, seed=5),
+    # the n = 2000 layer with 2 % of the non-edges fixed to zero (m about 39,600; the 20 %
+    # subset of the full-size layer would need a 1.25 TB dense Schur matrix)
+    "theta_adjoint_n2000_r2": lambda: theta_adjoint(2000, 0.01, 0.02, seed=6),
 }

@@ -108,6 +108,12 @@ extern int hdsdpb_ratio_probe( int m, int n, const int *Ap, const int *Ai, const
    upper part zero) and sum(log L_ii). Returns 0 if positive definite, 1 if not. */
 extern int hdsdpb_cholesky( int n, const double *S, double *L, double *logdiag );
 
+/* Solution of S x = b through the Cholesky factor of S by blocked forward and backward
+   substitution with L (the reference's dpotrs use, linalg/hdsdp_linsolver.c:607-633; the
+   solver uses it for Schur systems of order >= 6000). Returns 0 on success, 1 if S is
+   not positive definite, -1 on error. */
+extern int hdsdpb_cholesky_solve( int n, const double *S, const double *b, double *x );
+
 /* Allocation-free variant of hdsdpb_cholesky (no reference counterpart), for callers
    that cannot call cudaMalloc on their call path (a host framework whose allocator
    owns the device memory, a plugin barred from allocating, a latency-critical loop
@@ -142,7 +148,8 @@ extern int hdsdpb_split_gemm( int M, int N, int K, const double *A, int lda, int
    on the launching stream, 2 warm-up calls): 0 GEMM NN, 1 GEMM TN lower,
    2 Cholesky, 3 triangular inverse L^-1, 4 matrix-vector product,
    5 Lanczos step bound, 6 rank-64 SYRK update, 7 Cholesky that also forms L^-1,
-   8 Cholesky without it. Writes milliseconds per call. */
+   8 Cholesky without it, 9 solve with the factor (forward and backward substitution).
+   Writes milliseconds per call. */
 extern int hdsdpb_kernel_timing( int which, int n, int reps, double *ms );
 
 /* Milliseconds taken by `reps` grid-wide barriers in one cooperative launch of

@@ -99,3 +99,28 @@ def test_gemm(gpu_lib, M, N, Kd, tA, tB):
     out = api.gemm(0.7, A, B, beta=-0.3, Cm=C0, transA=tA, transB=tB)
     ref = 0.7 * ((A.T if tA else A) @ (B.T if tB else B)) - 0.3 * C0
     assert np.abs(out - ref).max() <= 1e-12 * max(1.0, Kd) * max(1.0, np.abs(ref).max())
+
+
+@pytest.mark.parametrize("n", [1, 2, 63, 64, 65, 200, 1000, 2100, 9600])
+def test_cholesky_solve(gpu_lib, n):
+    """Blocked forward / backward substitution with the factor (the Schur-solve path for
+    m >= 6000); n = 9600 gives 150 row blocks, so some CTAs own two."""
+    rng = np.random.default_rng(n + 11)
+    if n <= 2100:
+        S = _spd(n, n + 1)
+    else:
+        R = rng.standard_normal((n, 40))
+        S = R @ R.T / 40.0 + np.eye(n)
+    b = rng.standard_normal(n)
+    x = api.cholesky_solve(S, b)
+    assert x is not None
+    res = np.abs(S @ x - b).max()
+    assert res <= 1e-11 * np.abs(S).max() * max(1.0, np.abs(x).max())
+    x2 = api.cholesky_solve(S, b)  # a second solve reuses nothing stale
+    np.testing.assert_array_equal(x2, x)
+
+
+def test_cholesky_solve_indefinite(gpu_lib):
+    S = _spd(100, 5)
+    S[50, 50] = -1.0
+    assert api.cholesky_solve(S, np.ones(100)) is None
