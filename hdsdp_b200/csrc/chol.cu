@@ -619,14 +619,16 @@ __global__ void __launch_bounds__(COOP_THREADS, 1) trtri_coop_kernel(const doubl
 
 // Blocked substitution for L L^T x = b, one cooperative launch. The 64-row blocks of
 // the vector are dealt to the CTAs (block k to CTA k mod grid); a CTA keeps, in shared
-// memory, the accumulated products of its blocks with the solved ones. Forward sweep:
-// the owner of block j forms t_j = Dinv_j (b_j - acc_j), publishes it with flag_f[j] =
-// epoch, and every CTA then adds L_kj t_j to its blocks k > j. The owner of block j + 1
-// applies t_j to that block first and publishes t_{j+1} before its other updates, so
-// the chain from block to block holds one small product. After a grid barrier the
-// backward sweep does the same from the last block up with L^T and Dinv^T. Every wait
-// on a flag is bounded; on giving up the CTA raises g_tri_err and the rest skip their
-// work (every CTA still reaches the grid barrier).
+// memory, the accumulated products of its unfinished blocks with the solved ones.
+// Forward sweep: the owner of block j forms t_j = Dinv_j (b_j - acc_j) and publishes it
+// with flag_f[j] = epoch; every CTA then adds L_kj t_j to its unfinished blocks. The
+// chain from block to block is kept short: each CTA prefetches into shared memory the
+// tile L_{k,k-1} and Dinv_k of its next block k while it works on older ones, and when
+// t_{k-1} appears it finishes and publishes block k before any other update. The other
+// updates of a step are one pass over all of the CTA's unfinished blocks (many loads in
+// flight). After a grid barrier the backward sweep does the same from the last block up
+// with L^T and Dinv^T. Every wait on a flag is bounded; on giving up the CTA raises
+// g_tri_err and the others skip their work (every CTA still reaches the grid barrier).
 __device__ int g_tri_err = 0;
 constexpr long TRI_WAIT_LIMIT = 1L << 22;
 
@@ -649,67 +651,16 @@ __global__ void __launch_bounds__(COOP_THREADS, 1)
     const int G = gridDim.x, me = blockIdx.x;
     const int nblk = (n + 63) / 64;
     const int nown = (me < nblk) ? (nblk - 1 - me) / G + 1 : 0;
-    double *acc = sm;                    // nown x 64
-    double *xs = sm + (size_t) nown * 64; // the solved block being applied
-    double *xn = xs + 64;                // the block this CTA just published
-    double *red = xn + 64;               // 4 x 64 partial sums
+    double *Lt = sm;                       // 64 x TP: the tile that feeds the next block
+    double *Dt = sm + 64 * TP;             // 64 x TP: that block's Dinv
+    double *acc = sm + 2 * 64 * TP;        // nown x 64
+    double *xs = acc + (size_t) nown * 64; // the solved block being applied
+    double *xn = xs + 64;                  // the block this CTA just published
+    double *red = xn + 64;                 // 4 x 64 partial sums
     __shared__ int abort_;
     if (tid == 0) abort_ = 0;
-    for (int i = tid; i < nown * 64; i += blockDim.x) acc[i] = 0.0;
-    __syncthreads();
+    auto kof = [&](int c) { return me + c * G; };
     auto nbof = [&](int j) { return min(64, n - 64 * j); };
-    // v = rhs_j - acc_j, then out_j = Dinv_j v (transpose: Dinv_j^T v) into xn and out
-    auto finish = [&](int j, const double *rhs, double *out, bool transpose) {
-        const int nb = nbof(j);
-        double *a = acc + (size_t) (j / G) * 64;
-        if (tid < 64) red[tid] = (tid < nb) ? rhs[64 * j + tid] - a[tid] : 0.0;
-        __syncthreads();
-        // 8 warps x 8 outputs, lanes over the contraction index (two each)
-        for (int o = warp; o < 64; o += 8) {
-            double sum = 0.0;
-            if (o < nb) {  // warp-uniform; rows and columns of Dinv beyond nb are not read
-                for (int q = lane; q < nb; q += 32) {
-                    const double d = transpose ? Dinv[(size_t) (64 * j + q) + (size_t) o * ldd]
-                                               : Dinv[(size_t) (64 * j + o) + (size_t) q * ldd];
-                    sum += d * red[q];
-                }
-            }
-#pragma unroll
-            for (int off = 16; off > 0; off >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, off);
-            if (lane == 0) xn[o] = (o < nb) ? sum : 0.0;
-        }
-        __syncthreads();
-        if (tid < nb) out[64 * j + tid] = xn[tid];
-        __threadfence();
-        __syncthreads();
-    };
-    // forward: acc_k += L_kj v (v in xs)
-    auto update_f = [&](int k, int j) {
-        const int nbk = nbof(k);
-        const int r = tid & 63, q = tid >> 6;
-        double sum = 0.0;
-        if (r < nbk) {
-            const double *col = L + (size_t) (64 * k + r) + (size_t) (64 * j) * ld;
-            for (int c = 16 * q; c < 16 * q + 16; ++c) sum += col[(size_t) c * ld] * xs[c];
-        }
-        red[q * 64 + r] = sum;
-        __syncthreads();
-        if (tid < 64) acc[(size_t) (k / G) * 64 + tid] += red[tid] + red[64 + tid] + red[128 + tid] + red[192 + tid];
-        __syncthreads();
-    };
-    // backward: acc_k += L_jk^T v (v in xs), a warp per output
-    auto update_b = [&](int k, int j) {
-        const int nbj = nbof(j);
-        for (int o = warp; o < 64; o += 8) {
-            double sum = 0.0;
-            const double *col = L + (size_t) (64 * j) + (size_t) (64 * k + o) * ld;
-            for (int q = lane; q < nbj; q += 32) sum += col[q] * xs[q];
-#pragma unroll
-            for (int off = 16; off > 0; off >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, off);
-            if (lane == 0) acc[(size_t) (k / G) * 64 + o] += sum;
-        }
-        __syncthreads();
-    };
     auto fetch = [&](const double *v, int j, const unsigned *flag) {
         if (tid == 0 && !tri_wait(flag + j, epoch)) abort_ = 1;
         __threadfence();
@@ -717,71 +668,170 @@ __global__ void __launch_bounds__(COOP_THREADS, 1)
         if (tid < 64) xs[tid] = (!abort_ && tid < nbof(j)) ? __ldcg(v + 64 * j + tid) : 0.0;
         __syncthreads();
     };
-    auto publish = [&](unsigned *flag, int j) {
-        if (tid == 0) atomicExch(flag + j, epoch);
+    auto take_next = [&]() {
+        if (tid < 64) xs[tid] = xn[tid];
+        __syncthreads();
+    };
+    // v = rhs_k - acc_c; out_k = Dt v (transpose: Dt^T v) into xn and out, then publish
+    auto finish = [&](int c, const double *rhs, double *out, bool transpose, unsigned *flag) {
+        const int k = kof(c), nb = nbof(k);
+        double *a = acc + (size_t) c * 64;
+        if (tid < 64) red[tid] = (tid < nb) ? rhs[64 * k + tid] - a[tid] : 0.0;
+        __syncthreads();
+        for (int o = warp; o < 64; o += 8) {
+            double sum = 0.0;
+            for (int q = lane; q < 64; q += 32) sum += (transpose ? Dt[q + o * TP] : Dt[o + q * TP]) * red[q];
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, off);
+            if (lane == 0) xn[o] = (o < nb) ? sum : 0.0;
+        }
+        __syncthreads();
+        if (tid < nb) out[64 * k + tid] = xn[tid];
+        __threadfence();
+        __syncthreads();
+        if (tid == 0) atomicExch(flag + k, epoch);
+    };
+    auto wait_tiles = [&]() {
+        asm volatile("cp.async.wait_all;\n" ::);
+        __syncthreads();
     };
 
-    const int last = (nown > 0) ? me + (nown - 1) * G : -1;  // this CTA's last block
     // ---- forward sweep: t = L^-1 b
+    for (int i = tid; i < nown * 64; i += blockDim.x) acc[i] = 0.0;
+    __syncthreads();
     if (nown > 0 && !*(volatile int *) &g_tri_err) {
-        bool have_next = false;  // xn holds t_j, published by this CTA
+        // next block k: L_{k,k-1} (rows of k, columns of k-1) and Dinv_k
+        auto prefetch_f = [&](int k) {
+            if (k > 0) stage_tile(Lt, L + (size_t) (64 * k) + (size_t) (64 * (k - 1)) * ld, ld, nbof(k), 64, 64);
+            stage_tile(Dt, Dinv + (size_t) (64 * k), ldd, nbof(k), nbof(k), 64);
+            asm volatile("cp.async.commit_group;\n" ::);
+        };
+        int c = 0;
+        bool have = false;
+        prefetch_f(kof(0));
         if (me == 0) {
-            finish(0, b, t, false);
-            publish(flag_f, 0);
-            have_next = true;
+            wait_tiles();
+            finish(0, b, t, false, flag_f);
+            have = true;
+            c = 1;
+            if (c < nown) prefetch_f(kof(c));
         }
+        const int last = kof(nown - 1);
         for (int j = 0; j < last && !abort_; ++j) {
-            if (have_next) {
-                if (tid < 64) xs[tid] = xn[tid];
-                __syncthreads();
-                have_next = false;
+            if (have) {
+                take_next();
+                have = false;
             } else {
                 fetch(t, j, flag_f);
                 if (abort_) break;
             }
-            const int k1 = j + 1;
-            if (k1 % G == me) {
-                update_f(k1, j);
-                finish(k1, b, t, false);
-                publish(flag_f, k1);
-                have_next = true;
+            if (c < nown && kof(c) == j + 1) {
+                // the next block: acc += L_{j+1,j} t_j from the prefetched tile, then finish it
+                wait_tiles();
+                {
+                    const int r = tid & 63, q = tid >> 6;
+                    double sum = 0.0;
+#pragma unroll
+                    for (int cc = 16 * q; cc < 16 * q + 16; ++cc) sum += Lt[r + cc * TP] * xs[cc];
+                    red[q * 64 + r] = sum;
+                }
+                __syncthreads();
+                if (tid < 64) acc[(size_t) c * 64 + tid] += red[tid] + red[64 + tid] + red[128 + tid] + red[192 + tid];
+                __syncthreads();
+                finish(c, b, t, false, flag_f);
+                have = true;
+                ++c;
+                if (c < nown) prefetch_f(kof(c));
             }
-            for (int k = (k1 % G == me) ? k1 + G : k1 + ((me - k1 % G + G) % G); k <= last; k += G)
-                if (k > j) update_f(k, j);
+            // every other unfinished block (all beyond block j + 1): acc_k += L_kj t_j
+            for (int item = tid; item < (nown - c) * 64; item += blockDim.x) {
+                const int cc = c + (item >> 6), r = item & 63, k = kof(cc);
+                if (r >= nbof(k)) continue;
+                const double *row = L + (size_t) (64 * k + r) + (size_t) (64 * j) * ld;
+                double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+#pragma unroll 4
+                for (int q = 0; q < 64; q += 4) {
+                    s0 += row[(size_t) q * ld] * xs[q];
+                    s1 += row[(size_t) (q + 1) * ld] * xs[q + 1];
+                    s2 += row[(size_t) (q + 2) * ld] * xs[q + 2];
+                    s3 += row[(size_t) (q + 3) * ld] * xs[q + 3];
+                }
+                acc[(size_t) cc * 64 + r] += (s0 + s1) + (s2 + s3);
+            }
+            __syncthreads();
         }
     }
+    asm volatile("cp.async.wait_all;\n" ::);
     grid.sync();
     // ---- backward sweep: x = L^-T t
     for (int i = tid; i < nown * 64; i += blockDim.x) acc[i] = 0.0;
     __syncthreads();
     if (nown > 0 && !*(volatile int *) &g_tri_err) {
-        const int first = me;  // this CTA's first block
-        bool have_next = false;
-        if (me == (nblk - 1) % G) {
-            finish(nblk - 1, t, x, true);
-            publish(flag_b, nblk - 1);
-            have_next = true;
+        // next block k (downwards): L_{k+1,k} (rows of k+1, columns of k) and Dinv_k
+        auto prefetch_b = [&](int k) {
+            if (k < nblk - 1) stage_tile(Lt, L + (size_t) (64 * (k + 1)) + (size_t) (64 * k) * ld, ld, nbof(k + 1), 64, 64);
+            stage_tile(Dt, Dinv + (size_t) (64 * k), ldd, nbof(k), nbof(k), 64);
+            asm volatile("cp.async.commit_group;\n" ::);
+        };
+        int c = nown - 1;
+        bool have = false;
+        prefetch_b(kof(c));
+        if (kof(c) == nblk - 1) {
+            wait_tiles();
+            finish(c, t, x, true, flag_b);
+            have = true;
+            --c;
+            if (c >= 0) prefetch_b(kof(c));
         }
-        for (int j = nblk - 1; j > first && !abort_; --j) {
-            if (have_next) {
-                if (tid < 64) xs[tid] = xn[tid];
-                __syncthreads();
-                have_next = false;
+        for (int j = nblk - 1; j > me && !abort_; --j) {
+            if (have) {
+                take_next();
+                have = false;
             } else {
                 fetch(x, j, flag_b);
                 if (abort_) break;
             }
-            const int k1 = j - 1;
-            if (k1 % G == me) {
-                update_b(k1, j);
-                finish(k1, t, x, true);
-                publish(flag_b, k1);
-                have_next = true;
+            if (c >= 0 && kof(c) == j - 1) {
+                // the next block: acc += L_{j,j-1}^T x_j from the prefetched tile, then finish it
+                wait_tiles();
+                for (int o = warp; o < 64; o += 8) {
+                    double sum = 0.0;
+                    for (int q = lane; q < 64; q += 32) sum += Lt[q + o * TP] * xs[q];
+#pragma unroll
+                    for (int off = 16; off > 0; off >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, off);
+                    if (lane == 0) acc[(size_t) c * 64 + o] += sum;
+                }
+                __syncthreads();
+                finish(c, t, x, true, flag_b);
+                have = true;
+                --c;
+                if (c >= 0) prefetch_b(kof(c));
             }
-            for (int k = me; k < j; k += G)
-                if (k != k1 || k1 % G != me) update_b(k, j);
+            // every other unfinished block (all below block j - 1): acc_k += L_jk^T x_j,
+            // a warp per output column, four columns at a time
+            const int nbj = nbof(j);
+            for (int item = warp * 4; item < (c + 1) * 64; item += 32) {
+                double s4[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int cc = (item + u) >> 6, o = (item + u) & 63, k = kof(cc);
+                    const double *col = L + (size_t) (64 * j) + (size_t) (64 * k + o) * ld;
+                    for (int q = lane; q < nbj; q += 32) s4[u] += col[q] * xs[q];
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+#pragma unroll
+                    for (int off = 16; off > 0; off >>= 1) s4[u] += __shfl_xor_sync(0xffffffffu, s4[u], off);
+                }
+                if (lane == 0) {
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) acc[(size_t) ((item + u) >> 6) * 64 + ((item + u) & 63)] += s4[u];
+                }
+            }
+            __syncthreads();
         }
     }
+    asm volatile("cp.async.wait_all;\n" ::);
 }
 
 __global__ void copy_lower_k(int n, const double *S, long lds, double *L, long ldl) {
@@ -878,7 +928,7 @@ bool chol_solve(cudaStream_t s, DenseFactor &F, const double *b, double *x) {
     const void *fn = (const void *) tri_solve_coop_kernel;
     const int G = std::min(nblk, sm_count());
     const int nown = (nblk + G - 1) / G;
-    const int smem = (nown * 64 + 2 * 64 + 4 * 64) * (int) sizeof(double);
+    const int smem = (2 * 64 * TP + nown * 64 + 2 * 64 + 4 * 64) * (int) sizeof(double);
     static int smem_set = 0;
     if (smem > smem_set) {
         if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess) return false;

@@ -1031,6 +1031,7 @@ void Lanczos::init(int n_, cudaStream_t s_) {
         h[i] = 1e-03 * std::sqrt(std::sqrt((double) r1)) * (r2 - 0.5);
     }
     HB_CUDA(cudaMemcpy(pert_vec, h.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+    legacy_fence();
     nComputed = 0;
 }
 

@@ -22,6 +22,12 @@ __host__ __device__ __forceinline__ size_t cm(long i, long j, long ld) { return 
 
 int &device_error_flag();
 
+// Plain cudaMemset / cudaMemcpy run on the legacy default stream, which the library's
+// non-blocking streams do not wait for (a pageable host-to-device copy may still be in
+// flight when cudaMemcpy returns). Call this after such set-up copies and before the
+// first launch that reads their destination on another stream.
+inline void legacy_fence() { HB_CUDA(cudaStreamSynchronize(cudaStreamLegacy)); }
+
 // Host-side count of kernel launches issued by this library (all threads).
 long long &launch_counter();
 // Every launch site passes its grid through counted(), which bumps the counter.

@@ -134,6 +134,7 @@ int hdsdpb_cholesky(int n, const double *S, double *L, double *logdiag) {
     hb::cmalloc(&dS, sizeof(double) * ld * n);
     hb::cmalloc(&dl, sizeof(double));
     cudaMemcpy2D(dS, sizeof(double) * ld, S, sizeof(double) * n, sizeof(double) * n, n, cudaMemcpyHostToDevice);
+    legacy_fence();
     DenseFactor F;
     F.alloc(n);
     const bool ok = factorize(s, F, dS, ld);
@@ -168,6 +169,7 @@ int hdsdpb_cholesky_solve(int n, const double *S, const double *b, double *x) {
     hb::cmalloc(&dx, sizeof(double) * n);
     cudaMemcpy2D(dS, sizeof(double) * ld, S, sizeof(double) * n, sizeof(double) * n, n, cudaMemcpyHostToDevice);
     cudaMemcpy(dx, b, sizeof(double) * n, cudaMemcpyHostToDevice);
+    legacy_fence();
     DenseFactor F;
     F.alloc(n, 0);
     bool ok = factorize(s, F, dS, ld);
@@ -196,6 +198,7 @@ int hdsdpb_inverse(int n, const double *S, double *Sinv) {
     hb::cmalloc(&dS, sizeof(double) * ld * n);
     hb::cmalloc(&dW, sizeof(double) * ld * n);
     cudaMemcpy2D(dS, sizeof(double) * ld, S, sizeof(double) * n, sizeof(double) * n, n, cudaMemcpyHostToDevice);
+    legacy_fence();
     DenseFactor F;
     F.alloc(n);
     const bool ok = factorize(s, F, dS, ld);
@@ -229,6 +232,7 @@ int hdsdpb_gemm(int M, int N, int K, double alpha, const double *A, int lda, int
     cudaMemcpy(dA, A, sizeof(double) * (size_t) lda * ac, cudaMemcpyHostToDevice);
     cudaMemcpy(dB, B, sizeof(double) * (size_t) ldb * bc, cudaMemcpyHostToDevice);
     cudaMemcpy(dC, C, sizeof(double) * (size_t) ldc * N, cudaMemcpyHostToDevice);
+    legacy_fence();
     gemm(s, M, N, K, alpha, dA, lda, transA, dB, ldb, transB, beta, dC, ldc, 0);
     cudaMemcpyAsync(C, dC, sizeof(double) * (size_t) ldc * N, cudaMemcpyDeviceToHost, s);
     cudaStreamSynchronize(s);
@@ -255,6 +259,7 @@ int hdsdpb_split_gemm(int M, int N, int K, const double *A, int lda, int transA,
     HB_CUDA(cudaMemcpy(dA, A, sizeof(double) * (size_t) lda * ac, cudaMemcpyHostToDevice));
     HB_CUDA(cudaMemcpy(dB, B, sizeof(double) * (size_t) ldb * bc, cudaMemcpyHostToDevice));
     HB_CUDA(cudaMemset(dC, 0, sizeof(double) * (size_t) ldc * N));
+    legacy_fence();
     SplitOperand opA, opB;
     int ret = 0;
     if (!opA.alloc(M, K) || !opB.alloc(N, K)) ret = 2;

@@ -778,6 +778,7 @@ void DenseFactor::alloc(int n_, int fuse_inverse) {
         HB_CUDA(cudaMemset(K, 0, sizeof(double) * ld * n));
         HB_CUDA(cudaMemset(KT, 0, sizeof(double) * ld * n));
     }
+    legacy_fence();
 }
 
 void DenseFactor::release() {

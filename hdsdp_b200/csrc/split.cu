@@ -407,6 +407,7 @@ bool SplitOperand::alloc(int rows_, int k_) {
     HB_CUDA(hb::cmalloc(&lo, bytes));
     HB_CUDA(cudaMemset(hi, 0, bytes));
     HB_CUDA(cudaMemset(lo, 0, bytes));
+    legacy_fence();
     if (!hi || !lo) return false;
     return encode_map(&map_hi, hi, ra, kp) && encode_map(&map_lo, lo, ra, kp);
 }
