@@ -8,6 +8,7 @@
 //   <A, Z>        = sum_e v_e * (r != c ? 2 Z_rc : Z_rr)
 //   <A, W B W>    = sum_e sum_f v_e u_f * pair(e, f)       (pair below)
 #include "sdp.h"
+#include <cub/device/device_scan.cuh>
 #include <chrono>
 #include <unordered_map>
 #include <algorithm>
@@ -24,6 +25,90 @@ T *upload_vec(const std::vector<T> &h, cudaStream_t s) {
     HB_CUDA(hb::cmalloc(&d, sizeof(T) * h.size()));
     HB_CUDA(cudaMemcpyAsync(d, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice, s));
     return d;
+}
+
+// ---- rank-one gather map, built on the device. Row q of the coefficient factors lists
+// the constraints whose support holds q, ascending, with a_jq (rptr / rj / ra). The
+// entries of lower position (r, c) (packed index (2n - c - 1) c / 2 + r) are the merge
+// of rows r and c. Launched on a grid of (row blocks, columns c); rows below c return.
+__device__ __forceinline__ long long r1map_pos(int n, int r, int c) { return (long long) (2LL * n - c - 1) * c / 2 + r; }
+
+__global__ void r1map_count_kernel(int n, const int *__restrict__ rptr, const int *__restrict__ rj, int *cnt,
+                                   int *used) {
+    const int c = blockIdx.y, r = c + blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    int x = rptr[r], xe = rptr[r + 1], y = rptr[c], ye = rptr[c + 1], k = 0;
+    while (x < xe && y < ye) {
+        const int a = rj[x], b = rj[y];
+        if (a < b) ++x;
+        else if (a > b) ++y;
+        else { ++k; ++x; ++y; }
+    }
+    const long long q = r1map_pos(n, r, c);
+    cnt[q] = k;
+    used[q] = k > 0;
+}
+
+// used positions in packed order: row, column and entry count at their slot
+__global__ void r1map_place_kernel(int n, const int *__restrict__ cnt, const int *__restrict__ slot, int *pr, int *pc,
+                                   int *pcnt) {
+    const int c = blockIdx.y, r = c + blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    const long long q = r1map_pos(n, r, c);
+    const int k = cnt[q];
+    if (k == 0) return;
+    const int sl = slot[q];
+    pr[sl] = r;
+    pc[sl] = c;
+    pcnt[sl] = k;
+}
+
+// slices of 32 positions padded to their longest list: 32 * max count per slice
+__global__ void r1map_slice_kernel(int npos, int nslice, const int *__restrict__ pcnt, long long *len) {
+    const int sl = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (sl > nslice) return;
+    int k = 0;
+    if (sl < nslice && sl * 32 + lane < npos) k = pcnt[sl * 32 + lane];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) k = max(k, __shfl_xor_sync(0xffffffffu, k, off));
+    if (lane == 0) len[sl] = (sl < nslice) ? 32LL * k : 0LL;
+}
+
+// entry e of the position at slot p lands at sptr[p / 32] + 32 e + p % 32, in constraint
+// order, with value s_j a_jr a_jc
+__global__ void r1map_fill_kernel(int n, const int *__restrict__ rptr, const int *__restrict__ rj,
+                                  const double *__restrict__ ra, const double *__restrict__ sgn,
+                                  const int *__restrict__ cnt, const int *__restrict__ slot,
+                                  const long long *__restrict__ sptr, int *ej, double *ev) {
+    const int c = blockIdx.y, r = c + blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    const long long q = r1map_pos(n, r, c);
+    if (cnt[q] == 0) return;
+    const int sl = slot[q];
+    long long at = sptr[sl >> 5] + (sl & 31);
+    int x = rptr[r], xe = rptr[r + 1], y = rptr[c], ye = rptr[c + 1];
+    while (x < xe && y < ye) {
+        const int a = rj[x], b = rj[y];
+        if (a < b) ++x;
+        else if (a > b) ++y;
+        else {
+            ej[at] = a;
+            ev[at] = sgn[a] * ra[x] * ra[y];
+            at += 32;
+            ++x;
+            ++y;
+        }
+    }
+}
+
+template <typename T>
+void exclusive_sum(cudaStream_t s, const T *in, T *out, long long count) {
+    size_t bytes = 0;
+    HB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, bytes, in, out, (int64_t) count, s));
+    void *tmp = nullptr;
+    HB_CUDA(hb::cmalloc(&tmp, bytes));
+    HB_CUDA(cub::DeviceScan::ExclusiveSum(tmp, bytes, in, out, (int64_t) count, s));
+    hb::cache_free(tmp);
 }
 
 int grid1(long total, int threads = 256) {
@@ -439,10 +524,10 @@ void SdpDevice::upload(int n_, int m_, const HostCoeff &C, const std::vector<Hos
         }
         const double gemm_flops = 2.0 * n * (double) n * nr1d;
         if (12.0 * (double) entries < 0.25 * gemm_flops && (long long) n * (n + 1) / 2 < (1LL << 31)) {
-            // Per row q, the constraints whose support holds q, ascending, with a_jq. The
-            // entries of lower position (r, c) are the merge of rows r and c: constraint
-            // order within a position, built in parallel over columns, values
-            // s_j a_jr a_jc as before.
+            // Per row q, the constraints whose support holds q, ascending, with a_jq (host).
+            // The entries of lower position (r, c) are the merge of rows r and c, in
+            // constraint order, with values s_j a_jr a_jc; the merges, the compaction of
+            // the used positions and the sliced layout run on the device (r1map_*).
             std::vector<int> rptr(n + 1, 0);
             for (int j : r1did)
                 for (int q : A[j].aidx) rptr[q + 1] += 1;
@@ -462,74 +547,48 @@ void SdpDevice::upload(int n_, int m_, const HostCoeff &C, const std::vector<Hos
             }
             std::vector<double> sgn(m, 0.0);
             for (int j : r1did) sgn[j] = A[j].sign;
-            // pass 1: entries per lower position, column by column
+            // the map itself is built on the device from the row lists
             const long long npack = (long long) n * (n + 1) / 2;
-            std::vector<int> cnt(npack, 0);
-            auto colbase = [&](int c) { return (long long) (2LL * n - c - 1) * c / 2; };
-#pragma omp parallel for schedule(dynamic, 8)
-            for (int c = 0; c < n; ++c) {
-                const long long base = colbase(c);
-                for (int r = c; r < n; ++r) {
-                    int x = rptr[r], xe = rptr[r + 1], y = rptr[c], ye = rptr[c + 1], k = 0;
-                    while (x < xe && y < ye) {
-                        if (rj[x] < rj[y]) ++x;
-                        else if (rj[x] > rj[y]) ++y;
-                        else { ++k; ++x; ++y; }
-                    }
-                    cnt[base + r] = k;
-                }
-            }
-            // used positions, then the sliced layout: slices of 32 positions padded to
-            // their longest list; entry e of lane l at sptr[slice] + 32 e + l
-            std::vector<int> p2r, p2c, pc2;
-            std::vector<long long> pslot(npack, -1);
-            for (int c = 0; c < n; ++c)
-                for (int r = c; r < n; ++r) {
-                    const long long q = colbase(c) + r;
-                    if (cnt[q] == 0) continue;
-                    pslot[q] = (long long) p2r.size();
-                    p2r.push_back(r);
-                    p2c.push_back(c);
-                    pc2.push_back(cnt[q]);
-                }
-            npos2 = (int) p2r.size();
+            int *d_rptr = upload_vec(rptr, s), *d_rj = upload_vec(rj, s);
+            double *d_ra = upload_vec(ra, s), *d_sgn = upload_vec(sgn, s);
+            int *d_cnt = nullptr, *d_used = nullptr, *d_slot = nullptr;
+            HB_CUDA(hb::cmalloc(&d_cnt, sizeof(int) * npack));
+            HB_CUDA(hb::cmalloc(&d_used, sizeof(int) * npack));
+            HB_CUDA(hb::cmalloc(&d_slot, sizeof(int) * npack));
+            const dim3 pgrid((n + 255) / 256, n);
+            r1map_count_kernel<<<hb::counted(pgrid), 256, 0, s>>>(n, d_rptr, d_rj, d_cnt, d_used);
+            exclusive_sum(s, d_used, d_slot, npack);
+            int tail[2] = {0, 0};
+            HB_CUDA(cudaMemcpyAsync(&tail[0], d_slot + npack - 1, sizeof(int), cudaMemcpyDeviceToHost, s));
+            HB_CUDA(cudaMemcpyAsync(&tail[1], d_used + npack - 1, sizeof(int), cudaMemcpyDeviceToHost, s));
+            HB_CUDA(cudaStreamSynchronize(s));
+            npos2 = tail[0] + tail[1];
             const int nslice = (npos2 + 31) / 32;
-            std::vector<long long> sptr(nslice + 1, 0);
-            for (int sl = 0; sl < nslice; ++sl) {
-                int kmax = 0;
-                for (int q = sl * 32; q < std::min(npos2, sl * 32 + 32); ++q) kmax = std::max(kmax, pc2[q]);
-                sptr[sl + 1] = sptr[sl] + 32LL * kmax;
-            }
-            std::vector<int> s2j(sptr[nslice], 0);
-            std::vector<double> s2v(sptr[nslice], 0.0);
-            // pass 2: fill in constraint order, straight into the sliced layout
-#pragma omp parallel for schedule(dynamic, 8)
-            for (int c = 0; c < n; ++c) {
-                const long long base = colbase(c);
-                for (int r = c; r < n; ++r) {
-                    const long long slot = pslot[base + r];
-                    if (slot < 0) continue;
-                    long long at = sptr[slot >> 5] + (slot & 31);
-                    int x = rptr[r], xe = rptr[r + 1], y = rptr[c], ye = rptr[c + 1];
-                    while (x < xe && y < ye) {
-                        if (rj[x] < rj[y]) ++x;
-                        else if (rj[x] > rj[y]) ++y;
-                        else {
-                            s2j[at] = rj[x];
-                            s2v[at] = sgn[rj[x]] * ra[x] * ra[y];
-                            at += 32;
-                            ++x;
-                            ++y;
-                        }
-                    }
-                }
-            }
-            pos2_r = upload_vec(p2r, s);
-            pos2_c = upload_vec(p2c, s);
-            pos2_cnt = upload_vec(pc2, s);
-            pos2_ptr = upload_vec(sptr, s);
-            ent2_j = upload_vec(s2j, s);
-            ent2_v = upload_vec(s2v, s);
+            HB_CUDA(hb::cmalloc(&pos2_r, sizeof(int) * std::max(npos2, 1)));
+            HB_CUDA(hb::cmalloc(&pos2_c, sizeof(int) * std::max(npos2, 1)));
+            HB_CUDA(hb::cmalloc(&pos2_cnt, sizeof(int) * std::max(npos2, 1)));
+            HB_CUDA(hb::cmalloc(&pos2_ptr, sizeof(long long) * (nslice + 1)));
+            long long *d_len = nullptr;
+            HB_CUDA(hb::cmalloc(&d_len, sizeof(long long) * (nslice + 1)));
+            r1map_place_kernel<<<hb::counted(pgrid), 256, 0, s>>>(n, d_cnt, d_slot, pos2_r, pos2_c, pos2_cnt);
+            r1map_slice_kernel<<<hb::counted((int) ((32LL * (nslice + 1) + 255) / 256)), 256, 0, s>>>(
+                npos2, nslice, pos2_cnt, d_len);
+            exclusive_sum(s, d_len, pos2_ptr, (long long) nslice + 1);
+            long long total = 0;
+            HB_CUDA(cudaMemcpyAsync(&total, pos2_ptr + nslice, sizeof(long long), cudaMemcpyDeviceToHost, s));
+            HB_CUDA(cudaStreamSynchronize(s));
+            HB_CUDA(hb::cmalloc(&ent2_j, sizeof(int) * std::max(total, 1LL)));
+            HB_CUDA(hb::cmalloc(&ent2_v, sizeof(double) * std::max(total, 1LL)));
+            HB_CUDA(cudaMemsetAsync(ent2_j, 0, sizeof(int) * std::max(total, 1LL), s));
+            HB_CUDA(cudaMemsetAsync(ent2_v, 0, sizeof(double) * std::max(total, 1LL), s));
+            r1map_fill_kernel<<<hb::counted(pgrid), 256, 0, s>>>(n, d_rptr, d_rj, d_ra, d_sgn, d_cnt, d_slot, pos2_ptr,
+                                                                 ent2_j, ent2_v);
+            HB_CUDA(cudaGetLastError());
+            HB_CUDA(cudaStreamSynchronize(s));
+            for (int *p : {d_rptr, d_rj, d_cnt, d_used, d_slot}) hb::cache_free(p);
+            hb::cache_free(d_ra);
+            hb::cache_free(d_sgn);
+            hb::cache_free(d_len);
             r1d_gather = true;
         }
     }
