@@ -496,7 +496,9 @@ def run_b200(args):
         "steps_ipm_s": [round(x, 4) for x in ipm_s], "steps_e2e_s": [round(x, 4) for x in e2e_s],
         "setup_s": [round(r["timers"]["setup"], 4) for r in results],
         "status": last["status"], "dobj": last["dobj"], "pobj": last["pobj"],
-        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "bytes_note": "h2d counts the CSC arrays and b handed to the C API from pinned memory; "
+                              "the library reads them on the host and uploads the presolved coefficients"},
         "roofline": roofline, "kernels": kernels, "cpu_baseline": cpu, "clocks": clk,
         "gpu_launches": launches, "wall_s": wall, "adjoint": adj, "precision_legs": legs,
         "split_s": {k: t[k] for k in ("schur", "schur_factor", "schur_solve", "s_factor", "s_inverse",
