@@ -23,7 +23,7 @@ EXPORTS = [
     "HDSDPGetIterLog", "HDSDPGetTimers", "HDSDPAdjoint",
     "hdsdpb_schur_probe", "hdsdpb_ratio_probe", "hdsdpb_cholesky", "hdsdpb_cholesky_noalloc", "hdsdpb_inverse", "hdsdpb_gemm",
     "hdsdpb_kernel_timing", "hdsdpb_gridsync_probe", "hdsdpb_launch_count", "hdsdpb_release_cached_memory",
-    "hdsdpb_kstat_enable", "hdsdpb_kstat_read", "hdsdpb_split_gemm", "hdsdpb_cholesky_solve",
+    "hdsdpb_kstat_enable", "hdsdpb_kstat_read", "hdsdpb_split_gemm", "hdsdpb_cholesky_solve", "HReadSDPA",
 ]
 
 _lib = None
@@ -70,6 +70,7 @@ def load():
         "hdsdpb_cholesky_noalloc": ([i, dp, dp, dp], i),
         "hdsdpb_inverse": ([i, dp, dp], i),
         "hdsdpb_cholesky_solve": ([i, dp, dp, dp], i),
+        "HReadSDPA": ([C.c_char_p] + [vp] * 13, i),
         "hdsdpb_gemm": ([i, i, i, d, dp, i, i, dp, i, i, d, dp, i], i),
         "hdsdpb_kernel_timing": ([i, i, i, dp], i),
         "hdsdpb_gridsync_probe": ([i, i, dp], i),

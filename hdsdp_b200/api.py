@@ -9,6 +9,7 @@ oracle's driver so that parity tests compare like with like.
 from __future__ import annotations
 
 import ctypes as C
+import os
 import time
 
 import numpy as np
@@ -185,6 +186,64 @@ def solve(inst, want_x: bool = True, primal_refinement: bool = True, precision: 
 
 # ---------------------------------------------------------------------------
 # Kernel-level entry points (include/hdsdp_b200.h), host buffers in and out.
+
+def read_sdpa_with(lib, path):
+    """Call an HReadSDPA (this library's or another build of the same interface) on an SDPA
+    file; returns the blocks as NumPy CSC arrays and frees the C arrays."""
+    nC, nB, nCols, nLP, nE = (C.c_int() for _ in range(5))
+    dims, lbeg, lidx = C.POINTER(C.c_int)(), C.POINTER(C.c_int)(), C.POINTER(C.c_int)()
+    rhs, lval = C.POINTER(C.c_double)(), C.POINTER(C.c_double)()
+    beg, idx = C.POINTER(C.POINTER(C.c_int))(), C.POINTER(C.POINTER(C.c_int))()
+    elem = C.POINTER(C.POINTER(C.c_double))()
+    outs = (nC, nB, dims, rhs, beg, idx, elem, nCols, nLP, lbeg, lidx, lval, nE)
+    fn = lib.HReadSDPA
+    fn.argtypes = [C.c_char_p] + [C.c_void_p] * 13
+    fn.restype = C.c_int
+    r = fn(str(path).encode(), *[C.addressof(x) for x in outs])
+    if r != 0:
+        raise RuntimeError("HReadSDPA returned %d" % r)
+    free = C.CDLL(None).free
+    free.argtypes = [C.c_void_p]
+    m = nC.value
+    blocks = []
+    for k in range(nB.value):
+        n = dims[k]
+        Ap = np.ctypeslib.as_array(beg[k], shape=(m + 2,)).copy()
+        nnz = int(Ap[-1])
+        Ai = np.ctypeslib.as_array(idx[k], shape=(max(nnz, 1),))[:nnz].copy()
+        Ax = np.ctypeslib.as_array(elem[k], shape=(max(nnz, 1),))[:nnz].copy()
+        blocks.append((n, Ap, Ai, Ax))
+        for p in (beg[k], idx[k], elem[k]):
+            free(C.cast(p, C.c_void_p))
+    b = np.ctypeslib.as_array(rhs, shape=(max(m, 1),))[:m].copy()
+    lp = None
+    if nLP.value > 0:
+        Ap = np.ctypeslib.as_array(lbeg, shape=(m + 2,)).copy()
+        nnz = int(Ap[-1])
+        lp = (nLP.value, Ap, np.ctypeslib.as_array(lidx, shape=(max(nnz, 1),))[:nnz].copy(),
+              np.ctypeslib.as_array(lval, shape=(max(nnz, 1),))[:nnz].copy())
+        for p in (lbeg, lidx, lval):
+            free(C.cast(p, C.c_void_p))
+    for p in (dims, rhs, beg, idx, elem):
+        free(C.cast(p, C.c_void_p))
+    return {"m": m, "blocks": blocks, "b": b, "lp": lp, "n_cols": nCols.value, "n_elems": nE.value}
+
+
+def read_sdpa(path):
+    """An SDPA file through this library's HReadSDPA (include/hdsdp_file_io.h)."""
+    return read_sdpa_with(_lib.load(), path)
+
+
+def sdpa_instance(path):
+    """An SDPA file with one SDP block and no LP block as an instance for solve()."""
+    from hdsdp_b200.instances import SDPInstance
+    d = read_sdpa(path)
+    if len(d["blocks"]) != 1 or d["lp"] is not None:
+        raise ValueError("this solver takes one SDP block and no LP block")
+    n, Ap, Ai, Ax = d["blocks"][0]
+    return SDPInstance(os.path.basename(str(path)), n, d["m"], Ap.astype(np.int32), Ai.astype(np.int32),
+                       Ax.astype(np.float64), d["b"].astype(np.float64))
+
 
 def _csc(inst):
     return (np.ascontiguousarray(inst.Ap, dtype=np.int32), np.ascontiguousarray(inst.Ai, dtype=np.int32),

@@ -11,7 +11,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libhdsdp_b200.so")
-SOURCES = ["la.cu", "chol.cu", "sdp.cu", "split.cu", "cone.cu", "solver.cu", "ext.cu", "adjoint.cu", "noalloc.cu"]
+SOURCES = ["la.cu", "chol.cu", "sdp.cu", "split.cu", "cone.cu", "solver.cu", "ext.cu", "adjoint.cu", "noalloc.cu", "file_io.cpp"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
               "-Xcompiler", "-fPIC", "-Xcompiler", "-fopenmp", "-shared", "-cudart", "static", "-diag-suppress", "550",
               "-lgomp"]
@@ -26,7 +26,7 @@ def nvcc() -> str:
 
 def build(force: bool = False) -> str:
     srcs = [os.path.join(CSRC, s) for s in SOURCES if os.path.exists(os.path.join(CSRC, s))]
-    deps = srcs + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
+    deps = srcs + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh", ".cpp"))]
     if not force and os.path.exists(OUT):
         t = os.path.getmtime(OUT)
         if all(os.path.getmtime(d) <= t for d in deps):

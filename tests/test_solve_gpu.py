@@ -96,3 +96,18 @@ def test_maxcut_n8000_properties(gpu_lib):
     i, j = K.packed_to_ij(inst.n, rows)
     total = -2.0 * np.asarray(vals)[i == j].sum()
     assert 0.5 * total <= -r["dobj"] <= total
+
+
+def test_sdpa_file_solve(gpu_lib, tmp_path):
+    """An instance written as an SDPA file, read back with HReadSDPA and solved, gives the
+    same solve as the instance itself."""
+    from test_file_io_cpu import write_sdpa
+    inst = SMALL["theta40"]()
+    path = tmp_path / "theta40.dat-s"
+    write_sdpa(path, inst)
+    via_file = api.solve(api.sdpa_instance(path), want_x=False, primal_refinement=False)
+    direct = api.solve(inst, want_x=False, primal_refinement=False)
+    assert via_file["status_after_check"] == direct["status_after_check"] == OPTIMAL
+    assert via_file["iters"] == direct["iters"]
+    assert via_file["dobj"] == pytest.approx(direct["dobj"], rel=1e-12)
+    assert via_file["pobj"] == pytest.approx(direct["pobj"], rel=1e-12)
