@@ -16,6 +16,7 @@ import numpy as np
 
 from . import _lib
 
+CONETYPE_LP = 1  # HDSDP_CONETYPE_LP
 CONETYPE_DENSE_SDP = 4
 
 STATUS_NAMES = ["UNKNOWN", "DUAL_FEASIBLE", "DUAL_OPTIMAL", "PRIMAL_DUAL_OPTIMAL", "MAXITER",
@@ -60,6 +61,26 @@ class Solver:
             raise RuntimeError("HUserDataCreate failed")
         self.L.HUserDataSetConeData(self.ud, CONETYPE_DENSE_SDP, m, n, _ip(Ap), _ip(Ai), _dp(Ax))
         return self.L.HDSDPSetCone(self.h, 0, self.ud)
+
+    def set_lp_cone(self, m: int, n_lp: int, Ap, Ai, Ax):
+        """The LP cone s = c - A^T y >= 0 as cone 1 (init with n_cones = 2): user CSC with
+        m + 1 columns, column 0 the costs c, column i the coefficients of constraint i."""
+        Ap = np.ascontiguousarray(Ap, dtype=np.int32)
+        Ai = np.ascontiguousarray(Ai, dtype=np.int32)
+        Ax = np.ascontiguousarray(Ax, dtype=np.float64)
+        self._keep_lp = [Ap, Ai, Ax]
+        self.n_lp = n_lp
+        self.ud_lp = C.c_void_p()
+        if self.L.HUserDataCreate(C.byref(self.ud_lp)) != 0:
+            raise RuntimeError("HUserDataCreate failed")
+        self.L.HUserDataSetConeData(self.ud_lp, CONETYPE_LP, m, n_lp, _ip(Ap), _ip(Ai), _dp(Ax))
+        return self.L.HDSDPSetCone(self.h, 1, self.ud_lp)
+
+    def get_lp_values(self):
+        """(x, s) of the LP cone."""
+        x, sl, aux = np.zeros(self.n_lp), np.zeros(self.n_lp), np.zeros(self.n_lp)
+        self.L.HDSDPGetConeValues(self.h, 1, _dp(x), _dp(sl), _dp(aux))
+        return x, sl
 
     def set_dual_objective(self, b):
         b = np.ascontiguousarray(b, dtype=np.float64)
@@ -140,6 +161,8 @@ class Solver:
     def close(self):
         if self.ud:
             self.L.HUserDataDestroy(C.byref(self.ud))
+            if getattr(self, "ud_lp", None):
+                self.L.HUserDataDestroy(C.byref(self.ud_lp))
             self.ud = C.c_void_p()
         if self.h:
             self.L.HDSDPDestroy(C.byref(self.h))
@@ -153,13 +176,16 @@ class Solver:
 
 
 def solve(inst, want_x: bool = True, primal_refinement: bool = True, precision: int = 0,
-          params: dict | None = None) -> dict:
-    """Solve ``inst`` on the GPU; returns the oracle driver's fields plus the iteration log."""
+          params: dict | None = None, lp=None) -> dict:
+    """Solve ``inst`` on the GPU (with the LP cone ``lp`` = (n_lp, Ap, Ai, Ax) as cone 1 when
+    given); returns the oracle driver's fields plus the iteration log."""
     s = Solver()
     try:
-        assert s.init(inst.m, 1) == 0
+        assert s.init(inst.m, 2 if lp is not None else 1) == 0
         if s.set_cone(inst.m, inst.n, inst.Ap, inst.Ai, inst.Ax) != 0:
             raise RuntimeError("HDSDPSetCone rejected the block")
+        if lp is not None and s.set_lp_cone(inst.m, int(lp[0]), lp[1], lp[2], lp[3]) != 0:
+            raise RuntimeError("HDSDPSetCone rejected the LP cone")
         s.set_dual_objective(inst.b)
         s.set_primal_refinement(primal_refinement)
         s.set_precision(precision)
@@ -177,6 +203,8 @@ def solve(inst, want_x: bool = True, primal_refinement: bool = True, precision: 
         if want_x:
             X, S = s.get_cone_values()
             out["X"], out["S"] = X, S
+        if lp is not None:
+            out["x_lp"], out["s_lp"] = s.get_lp_values()
         out["errs"] = s.check_solution()
         out["status_after_check"] = s.status()
         return out

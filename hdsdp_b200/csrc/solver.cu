@@ -72,17 +72,27 @@ void default_params(hdsdp *h) {
 // ---------------------------------------------------------------- statistics / tuning
 void get_statistics(hdsdp *h) {
     SdpCone &c = *h->cone;
+    const int sumDims = c.n + (h->lp ? h->lp->nCol : 0);
     fi(h, N_MAXCONEDIM) = c.n;
-    fi(h, N_SUMCONEDIMS) = c.n;
+    fi(h, N_SUMCONEDIMS) = sumDims;
     fi(h, N_ROWS) = h->nRows;
     fi(h, N_CONES) = h->nCones;
-    h->allConeDims = (double) c.n + 2.0 * h->nRows;
-    const double objOne = c.obj_norm(ABS_NORM);
-    const double dataOne = c.coeff_norm(ABS_NORM);
-    const double objFro = c.obj_norm(FRO_NORM);
-    const double dataFro = c.coeff_norm(FRO_NORM);
-    fd(h, D_OBJFRONORM) = std::sqrt(objFro * objFro);
-    fd(h, D_DATAFRONORM) = std::sqrt(dataFro * dataFro);
+    h->allConeDims = (double) sumDims + 2.0 * h->nRows;
+    // sums over the cones (the SDP block, then the LP cone), as the reference adds them
+    double objOne = c.obj_norm(ABS_NORM);
+    double dataOne = c.coeff_norm(ABS_NORM);
+    double objFro2 = c.obj_norm(FRO_NORM), dataFro2 = c.coeff_norm(FRO_NORM);
+    objFro2 *= objFro2;
+    dataFro2 *= dataFro2;
+    if (h->lp) {
+        objOne += h->lp->obj_norm(ABS_NORM);
+        dataOne += h->lp->coeff_norm(ABS_NORM);
+        const double of = h->lp->obj_norm(FRO_NORM), df = h->lp->coeff_norm(FRO_NORM);
+        objFro2 += of * of;
+        dataFro2 += df * df;
+    }
+    fd(h, D_OBJFRONORM) = std::sqrt(objFro2);
+    fd(h, D_DATAFRONORM) = std::sqrt(dataFro2);
     fd(h, D_OBJONENORM) = objOne;
     fd(h, D_DATAONENORM) = dataOne;
     double one = 0, fro = 0, inf = 0;
@@ -98,12 +108,13 @@ void get_statistics(hdsdp *h) {
     if (h->nCones >= 100) fi(h, I_MANYCONES) = 1;
     fi(h, N_DSSDPCONES) = 1;
     fi(h, N_SPSDPCONES) = 0;
-    fi(h, N_LPCONES) = 0;
+    fi(h, N_LPCONES) = h->lp ? 1 : 0;
 }
 
 void adjust_cone_params(hdsdp *h) {
     SdpCone &c = *h->cone;
     c.detect_feature(h->rowRHS.data(), h->HIntFeatures, h->HDblFeatures);
+    if (h->lp && fi(h, N_CONES) < 10) h->lp->detect_feature(h->HIntFeatures, h->HDblFeatures);
     const int impTrace = fi(h, I_IMPTRACE), noPInt = fi(h, I_NOPINTERIOR), noDInt = fi(h, I_NODINTERIOR);
     const int dense = fi(h, I_VERYDENSE), impDual = fi(h, I_IMPYBOUND), noObj = fi(h, I_NULLOBJ);
     h->modelFeatures.clear();
@@ -196,6 +207,7 @@ void adjust_params(hdsdp *h) {
     fd(h, D_OBJSCALING) = objScal;
     fd(h, D_RHSSCALING) = rhsScal;
     h->cone->scal(objScal);
+    if (h->lp) h->lp->scal(objScal);
     for (int i = 0; i < h->nRows; ++i) h->rowRHS[i] *= rhsScal;
     // thread count: the GPU build records the host default
     ip(h, INT_PARAM_THREADS) = std::min(ip(h, INT_PARAM_THREADS), 12);
@@ -240,6 +252,8 @@ void adjust_params(hdsdp *h) {
 }
 
 // ---------------------------------------------------------------- algorithm helpers
+void cones_set_start(hdsdp *h, double r);
+
 void set_start(hdsdp *h, int method, int dOnly) {
     std::fill(h->y.begin(), h->y.end(), 0.0);
     h->tau = 1.0;
@@ -256,7 +270,7 @@ void set_start(hdsdp *h, int method, int dOnly) {
         h->mu = h->mu / h->allConeDims;
     }
     if (h->verbose) printf("Initialize with dual residual %3.1e\n", -h->resi);
-    h->cone->set_start(h->resi);
+    cones_set_start(h, h->resi);
 }
 
 void reset_start(hdsdp *h) {
@@ -267,7 +281,7 @@ void reset_start(hdsdp *h) {
     h->resi = -std::max(objFro, 1e+02) * 1e+06;
     h->resi = std::max(h->resi, -1e+15);
     if (h->verbose) printf("Reset with dual residual %3.1e\n", -h->resi);
-    h->cone->set_start(h->resi);
+    cones_set_start(h, h->resi);
 }
 
 void print_log(hdsdp *h, int method) {
@@ -304,9 +318,47 @@ void schur_precision(hdsdp *h) {
     h->cone->dev.precision = p;
 }
 
+// ---- the cone list in the reference's order: the SDP block, then the LP cone when set
+hdsdp_retcode cones_interior(hdsdp *h, double tau, const double *y, int *interior) {
+    hdsdp_retcode r = h->cone->interior_check(tau, y, interior);
+    if (r != HDSDP_RETCODE_OK || !*interior || !h->lp) return r;
+    *interior = h->lp->interior_check(tau, y);
+    return HDSDP_RETCODE_OK;
+}
+
+hdsdp_retcode cones_interior_expert(hdsdp *h, double dC, double dAs, const double *y, double dEye, int which,
+                                    int *interior) {
+    hdsdp_retcode r = h->cone->interior_check_expert(dC, dAs, y, dEye, which, interior);
+    if (r != HDSDP_RETCODE_OK || !*interior || !h->lp) return r;
+    *interior = h->lp->interior_check_expert(dC, dAs, y, dEye, which);
+    return HDSDP_RETCODE_OK;
+}
+
+// running minimum of the cones' step bounds
+hdsdp_retcode cones_ratio(hdsdp *h, double dtau, const double *dy, double ada, int which, double *mx) {
+    double st = 0.0;
+    hdsdp_retcode r = h->cone->ratio_test(dtau, dy, ada, which, &st);
+    if (r != HDSDP_RETCODE_OK) return r;
+    *mx = std::min(*mx, st);
+    if (h->lp) *mx = std::min(*mx, h->lp->ratio_test(dtau, dy, ada, which));
+    return HDSDP_RETCODE_OK;
+}
+
+hdsdp_retcode cones_add_step(hdsdp *h, double step, int which, int *interior) {
+    hdsdp_retcode r = h->cone->add_step_and_check(step, which, interior);
+    if (r != HDSDP_RETCODE_OK || !*interior || !h->lp) return r;
+    *interior = h->lp->add_step_and_check(step, which);
+    return HDSDP_RETCODE_OK;
+}
+
+void cones_set_start(hdsdp *h, double r) {
+    h->cone->set_start(r);
+    if (h->lp) h->lp->set_start(r);
+}
+
 hdsdp_retcode check_interior(hdsdp *h, double tau, const double *y, int *interior) {
     (void) tau;
-    hdsdp_retcode r = h->cone->interior_check(1.0, y, interior);
+    hdsdp_retcode r = cones_interior(h, 1.0, y, interior);
     if (r != HDSDP_RETCODE_OK) return r;
     if (!*interior) return HDSDP_RETCODE_OK;
     if (h->whichMethod != METHOD_HSD) *interior = h->bnd.interior_check(1.0, y);
@@ -324,6 +376,7 @@ hdsdp_retcode get_log_barrier(hdsdp *h, double tau, const double *y, int which, 
     hdsdp_retcode r = h->cone->get_barrier(tau, y, which, &ld);
     if (r != HDSDP_RETCODE_OK) return r;
     bv -= ld;
+    if (h->lp) bv -= h->lp->get_barrier(tau, y, which);
     if (h->whichMethod != METHOD_HSD) {
         r = h->bnd.get_barrier(tau, y, which, &ld);
         if (r != HDSDP_RETCODE_OK) return r;
@@ -333,7 +386,10 @@ hdsdp_retcode get_log_barrier(hdsdp *h, double tau, const double *y, int which, 
     return HDSDP_RETCODE_OK;
 }
 
-void set_residual(hdsdp *h, double r) { h->cone->reduce_resi(r); }
+void set_residual(hdsdp *h, double r) {
+    h->cone->reduce_resi(r);
+    if (h->lp) h->lp->reduce_resi(r);
+}
 
 hdsdp_retcode kkt_solve(hdsdp *h, std::vector<double> &rhs, std::vector<double> *lhs) {
     return h->kkt.solve(rhs.data(), lhs ? lhs->data() : rhs.data());
@@ -367,8 +423,7 @@ hdsdp_retcode hsd_ratio_test(hdsdp *h, double *maxDist) {
     double mx = HDSDP_INFINITY, st = 0.0;
     st = h->tau / h->dtau;
     if (st < 0.0) mx = std::min(mx, -st);
-    CALL(h->cone->ratio_test(h->dtau, h->dy.data(), 1.0, BUFFER_DUALVAR, &st));
-    mx = std::min(mx, st);
+    CALL(cones_ratio(h, h->dtau, h->dy.data(), 1.0, BUFFER_DUALVAR, &mx));
     if (h->whichMethod != METHOD_HSD) st = h->bnd.ratio_test(h->dtau, h->dy.data(), BUFFER_DUALVAR);
     if (mx < 1e-02) {
         h->nSmallStep += 1;
@@ -400,7 +455,7 @@ hdsdp_retcode phaseA_hsd(hdsdp *h, int dOnly) {
     if (h->verbose) printf("HDSDP starts. Using self-dual method \n\n");
     while (true) {
         int interior = 0;
-        CALL(h->cone->interior_check(h->tau, h->y.data(), &interior));
+        CALL(cones_interior(h, h->tau, h->y.data(), &interior));
         if (!interior) {
             if (h->nIterCount == 0) {
                 if (h->verbose) printf("Initial point is not in the cone. Adding slack value.\n");
@@ -415,6 +470,7 @@ hdsdp_retcode phaseA_hsd(hdsdp *h, int dOnly) {
         }
         schur_precision(h);
         CALL(h->kkt.build(*h->cone, KKT_TYPE_HOMOGENEOUS));
+        if (h->lp) h->kkt.add_lp(*h->lp, KKT_TYPE_HOMOGENEOUS);
         h->kkt.regularize(0.0);
         h->d2 = h->kkt.asinv;
         h->d3 = h->kkt.asinvrd;
@@ -493,7 +549,7 @@ int prox_measure(hdsdp *h) {
     isPFeasible = h->bnd.interior_check_expert(1.0, 1.0, h->aux2.data(), BUFFER_DUALCHECK);
     if (isPFeasible) {
         int in = 0;
-        h->cone->interior_check_expert(1.0, 1.0, h->aux2.data(), -h->resi, BUFFER_DUALCHECK, &in);
+        cones_interior_expert(h, 1.0, 1.0, h->aux2.data(), -h->resi, BUFFER_DUALCHECK, &in);
         isPFeasible = in;
     }
     if (isPFeasible) {
@@ -537,21 +593,19 @@ hdsdp_retcode phaseA_adaptive_resi(hdsdp *h, double *rate) {
     double alphaC = 0, alphaInf = 0, ada = 0, mx = HDSDP_INFINITY, st = 0;
     int interior = 0;
     for (int i = 0; i < h->nRows; ++i) h->aux1[i] = -h->d2[i];
-    CALL(h->cone->ratio_test(0.0, h->aux1.data(), 0.0, BUFFER_DUALVAR, &st));
-    mx = std::min(mx, st);
+    CALL(cones_ratio(h, 0.0, h->aux1.data(), 0.0, BUFFER_DUALVAR, &mx));
     st = h->bnd.ratio_test(0.0, h->aux1.data(), BUFFER_DUALVAR);
     mx = std::min(mx, st);
     alphaC = std::min(0.98 * mx, 1.0);
     mx = alphaC;
     while (!interior && alphaC > 1e-02 * mx) {
-        CALL(h->cone->add_step_and_check(alphaC, BUFFER_DUALCHECK, &interior));
-        // the bound-cone result replaces the SDP result here, as in the reference
+        CALL(cones_add_step(h, alphaC, BUFFER_DUALCHECK, &interior));
+        // the bound-cone result replaces the cones' result here, as in the reference
         interior = h->bnd.add_step_and_check(alphaC, BUFFER_DUALCHECK);
         if (!interior) alphaC *= 0.8;
     }
     mx = HDSDP_INFINITY;
-    CALL(h->cone->ratio_test(0.0, h->d3.data(), 1.0, BUFFER_DUALCHECK, &st));
-    mx = std::min(mx, st);
+    CALL(cones_ratio(h, 0.0, h->d3.data(), 1.0, BUFFER_DUALCHECK, &mx));
     alphaInf = mx;
     ada = alphaInf / alphaC;
     ada = std::min(0.98 * ada, 1.0);
@@ -570,8 +624,7 @@ void infeasible_build_step(hdsdp *h, double ada) {
 hdsdp_retcode ratio_test_all(hdsdp *h, double ada, double *maxDist) {
     hdsdp_retcode retcode = HDSDP_RETCODE_OK;
     double mx = HDSDP_INFINITY, st = 0.0;
-    CALL(h->cone->ratio_test(0.0, h->dy.data(), ada, BUFFER_DUALVAR, &st));
-    mx = std::min(mx, st);
+    CALL(cones_ratio(h, 0.0, h->dy.data(), ada, BUFFER_DUALVAR, &mx));
     st = h->bnd.ratio_test(0.0, h->dy.data(), BUFFER_DUALVAR);
     mx = std::min(mx, st);
 exit_cleanup:
@@ -592,6 +645,7 @@ hdsdp_retcode infeasible_corrector(hdsdp *h) {
     for (int nCorr = 0; nCorr < nMaxCorr; ++nCorr) {
         if (!h->resi) break;
         CALL(h->kkt.build(*h->cone, KKT_TYPE_CORRECTOR));
+        if (h->lp) h->kkt.add_lp(*h->lp, KKT_TYPE_CORRECTOR);
         h->kkt.add_bound(h->bnd, KKT_TYPE_CORRECTOR);
         h->d2 = h->kkt.asinv;
         h->d3 = h->kkt.asinvrd;
@@ -619,8 +673,7 @@ hdsdp_retcode infeasible_corrector(hdsdp *h) {
         }
         alphaC = mx;
         mx = HDSDP_INFINITY;
-        CALL(h->cone->ratio_test(0.0, h->d3.data(), 1.0, BUFFER_DUALVAR, &st));
-        mx = std::min(mx, st);
+        CALL(cones_ratio(h, 0.0, h->d3.data(), 1.0, BUFFER_DUALVAR, &mx));
         st = h->bnd.ratio_test(0.0, h->d3.data(), BUFFER_DUALVAR);
         mx = std::min(mx, st);
         alphaInf = mx;
@@ -673,7 +726,7 @@ hdsdp_retcode phaseA_infeasible(hdsdp *h, int dOnly) {
     double ada = 0.0;
     int interior = 0, pObjFound = 0, pObjType = 0;
     set_start(h, METHOD_INFEAS, 0);
-    CALL(h->cone->interior_check(h->tau, h->y.data(), &interior));
+    CALL(cones_interior(h, h->tau, h->y.data(), &interior));
     if (interior) interior = h->bnd.interior_check(h->tau, h->y.data());
     if (!interior) {
         if (h->verbose) printf("Initial point is not in the cone. Adding slack value.\n");
@@ -684,7 +737,7 @@ hdsdp_retcode phaseA_infeasible(hdsdp *h, int dOnly) {
         if (h->nIterCount == 3 && !pObjFound && allowReset) {
             if (h->verbose) printf("Increasing dual infeasibility \n");
             reset_start(h);
-            CALL(h->cone->interior_check(h->tau, h->y.data(), &interior));
+            CALL(cones_interior(h, h->tau, h->y.data(), &interior));
             if (!interior) {
                 retcode = HDSDP_RETCODE_FAILED;
                 goto exit_cleanup;
@@ -692,6 +745,7 @@ hdsdp_retcode phaseA_infeasible(hdsdp *h, int dOnly) {
         }
         schur_precision(h);
         CALL(h->kkt.build(*h->cone, KKT_TYPE_INFEASIBLE));
+        if (h->lp) h->kkt.add_lp(*h->lp, KKT_TYPE_INFEASIBLE);
         h->kkt.add_bound(h->bnd, KKT_TYPE_INFEASIBLE);
         h->d2 = h->kkt.asinv;
         h->d3 = h->kkt.asinvrd;
@@ -754,22 +808,20 @@ hdsdp_retcode phaseB_choose_barrier(hdsdp *h, int pObjType) {
     double mx = HDSDP_INFINITY, pst = 0.0, st = 0.0;
     if (pObjType > 0) {
         for (int i = 0; i < h->nRows; ++i) h->aux1[i] = -h->d1[i] / h->mu;
-        CALL(h->cone->ratio_test(0.0, h->aux1.data(), 0.0, BUFFER_DUALCHECK, &st));
-        mx = std::min(mx, st);
+        CALL(cones_ratio(h, 0.0, h->aux1.data(), 0.0, BUFFER_DUALCHECK, &mx));
         st = h->bnd.ratio_test(0.0, h->aux1.data(), BUFFER_DUALCHECK);
         mx = std::min(mx, st);
         mx = std::min(mx * 0.97, 1e+05);
         h->mu = h->mu / (1.0 + mx);
     } else {
         for (int i = 0; i < h->nRows; ++i) h->aux2[i] = -h->d1[i] / h->mu + h->d2[i];
-        CALL(h->cone->ratio_test(0.0, h->aux2.data(), 0.0, BUFFER_DUALVAR, &st));
-        mx = std::min(mx, st);
+        CALL(cones_ratio(h, 0.0, h->aux2.data(), 0.0, BUFFER_DUALVAR, &mx));
         st = h->bnd.ratio_test(0.0, h->aux2.data(), BUFFER_DUALVAR);
         pst = std::min(mx, st);
         if (pst < 1.0) pst = 0.97 * pst;
         int interior = 0;
         for (int iTry = 0;; ++iTry) {
-            CALL(h->cone->add_step_and_check(pst, BUFFER_DUALCHECK, &interior));
+            CALL(cones_add_step(h, pst, BUFFER_DUALCHECK, &interior));
             interior = h->bnd.add_step_and_check(pst, BUFFER_DUALCHECK);
             if (!interior) pst = (iTry > 2) ? pst * 0.97 : pst * 0.5;
             else break;
@@ -779,8 +831,7 @@ hdsdp_retcode phaseB_choose_barrier(hdsdp *h, int pObjType) {
             }
         }
         for (int i = 0; i < h->nRows; ++i) h->aux1[i] = -pst * h->d1[i] / h->mu;
-        CALL(h->cone->ratio_test(0.0, h->aux1.data(), 0.0, BUFFER_DUALCHECK, &st));
-        mx = std::min(mx, st);
+        CALL(cones_ratio(h, 0.0, h->aux1.data(), 0.0, BUFFER_DUALCHECK, &mx));
         st = h->bnd.ratio_test(0.0, h->aux1.data(), BUFFER_DUALCHECK);
         mx = std::min(mx, st);
         mx = std::min(mx * 0.97, 1e+05);
@@ -818,6 +869,7 @@ double get_potential(hdsdp *h, double rho, const double *y, int which) {
     double pot = 0.0, obj = 0.0, ld = 0.0;
     h->cone->get_barrier(0.0, nullptr, which, &ld);
     pot -= ld;
+    if (h->lp) pot -= h->lp->get_barrier(0.0, nullptr, which);
     h->bnd.get_barrier(0.0, nullptr, which, &ld);
     pot -= ld;
     for (int i = 0; i < h->nRows; ++i) obj += h->rowRHS[i] * y[i];
@@ -868,6 +920,7 @@ double get_barrier_val(hdsdp *h, const double *y, int which) {
     double bv = 0.0, obj = 0.0, ld = 0.0;
     h->cone->get_barrier(0.0, nullptr, which, &ld);
     bv += ld;
+    if (h->lp) bv += h->lp->get_barrier(0.0, nullptr, which);
     h->bnd.get_barrier(0.0, nullptr, which, &ld);
     bv += ld;
     for (int i = 0; i < h->nRows; ++i) obj += h->rowRHS[i] * y[i];
@@ -899,6 +952,7 @@ hdsdp_retcode feasible_corrector(hdsdp *h) {
     for (int nCorr = 0; nCorr < nMaxCorr; ++nCorr) {
         if (h->mu < 1e-05) break;
         CALL(h->kkt.build(*h->cone, KKT_TYPE_CORRECTOR));
+        if (h->lp) h->kkt.add_lp(*h->lp, KKT_TYPE_CORRECTOR);
         h->kkt.add_bound(h->bnd, KKT_TYPE_CORRECTOR);
         h->d2 = h->kkt.asinv;
         CALL(kkt_solve(h, h->d2, nullptr));
@@ -912,8 +966,7 @@ hdsdp_retcode feasible_corrector(hdsdp *h) {
         }
         double mx = HDSDP_INFINITY, st = 0.0;
         bNow = get_barrier_val(h, h->y.data(), BUFFER_DUALVAR);
-        CALL(h->cone->ratio_test(0.0, h->aux1.data(), 0.0, BUFFER_DUALVAR, &st));
-        mx = std::min(mx, st);
+        CALL(cones_ratio(h, 0.0, h->aux1.data(), 0.0, BUFFER_DUALVAR, &mx));
         st = h->bnd.ratio_test(0.0, h->aux1.data(), BUFFER_DUALVAR);
         mx = std::min(mx, st);
         mx = std::min(mx * 0.95, mx);
@@ -954,7 +1007,7 @@ int phaseB_ray_check(hdsdp *h, int force) {
         for (int i = 0; i < h->nRows; ++i) nrm += h->y[i] * h->y[i];
         nrm = std::sqrt(nrm);
         for (int i = 0; i < h->nRows; ++i) h->aux1[i] = h->y[i] / nrm;
-        h->cone->interior_check_expert(0.0, -1.0, h->aux1.data(), 1e-08, BUFFER_DUALCHECK, &interior);
+        cones_interior_expert(h, 0.0, -1.0, h->aux1.data(), 1e-08, BUFFER_DUALCHECK, &interior);
         if (interior) ray = 1;
     }
     return ray;
@@ -990,8 +1043,9 @@ hdsdp_retcode phaseB_potential(hdsdp *h) {
         printf("Dual infeasibility from previous algorithm exceeds user-specified tolerance \n");
     h->perturb = -10.0 * h->resi;
     h->resi = 0.0;
-    h->cone->reduce_resi(0.0);
+    set_residual(h, 0.0);
     h->cone->set_perturb(h->perturb);
+    if (h->lp) h->lp->set_perturb(h->perturb);
     if (h->perturb != 0.0) is_interior(h, h->y.data());
     pObjStart = h->pObjInternal;
     if (h->verbose) printf("HDSDP re-starts. Using feasible dual method \n\n");
@@ -1000,6 +1054,7 @@ hdsdp_retcode phaseB_potential(hdsdp *h) {
         if (nIterInternal > 10) force = 0;
         schur_precision(h);
         CALL(h->kkt.build(*h->cone, KKT_TYPE_INFEASIBLE));
+        if (h->lp) h->kkt.add_lp(*h->lp, KKT_TYPE_INFEASIBLE);
         h->kkt.add_bound(h->bnd, KKT_TYPE_INFEASIBLE);
         if (h->mu > 1.0) h->kkt.regularize(1e-06);
         h->d2 = h->kkt.asinv;
@@ -1069,6 +1124,19 @@ void cone_values(hdsdp *h, double *X, double *S) {
     }
     if (X) h->cone->get_primal(mu, y->data(), dy->data(), X);
     if (S) h->cone->get_dual(S);
+}
+
+// x and s of the LP cone at the same primal marker (host vectors of its dimension)
+void lp_values(hdsdp *h, double *x, double *sl) {
+    double mu = h->accMu;
+    const std::vector<double> *y = &h->accY, *dy = &h->accDy;
+    if (mu <= 0.0) {
+        mu = h->inaccMu;
+        y = &h->inaccY;
+        dy = &h->inaccDy;
+    }
+    if (x) h->lp->get_primal(mu, y->data(), dy->data(), x);
+    if (sl) h->lp->get_dual(sl);
 }
 
 // ---------------------------------------------------------------- primal refinement
@@ -1301,11 +1369,17 @@ hdsdp_retcode HDSDPInit(hdsdp *h, int nRows, int nCones) {
 }
 
 hdsdp_retcode HDSDPSetCone(hdsdp *h, int iCone, void *userCone) {
-    if (iCone != 0 || h->nCones != 1) {
-        fprintf(stderr, "[hdsdp_b200] only a single dense SDP block is supported\n");
+    user_data *u = (user_data *) userCone;
+    // one dense SDP block, optionally followed by one LP cone (the reference's own
+    // drivers put the LP cone last)
+    if (h->nCones == 2 && iCone == 1 && u && HUserDataChooseCone(u) == HDSDP_CONETYPE_LP) {
+        h->usrLp = u;
+        return HDSDP_RETCODE_OK;
+    }
+    if (iCone != 0 || h->nCones < 1 || h->nCones > 2) {
+        fprintf(stderr, "[hdsdp_b200] supported: one dense SDP block (cone 0) and optionally one LP cone (cone 1)\n");
         return HDSDP_RETCODE_FAILED;
     }
-    user_data *u = (user_data *) userCone;
     if (HUserDataChooseCone(u) != HDSDP_CONETYPE_DENSE_SDP) {
         fprintf(stderr, "[hdsdp_b200] the block is not a dense SDP cone\n");
         return HDSDP_RETCODE_FAILED;
@@ -1351,9 +1425,22 @@ hdsdp_retcode HDSDPCheckSolution(hdsdp *h, double dErrs[6]) {
     frob_dot(c.s, n, X, ld, S, ld, c.d_scal);
     HB_CUDA(cudaMemcpyAsync(c.h_scal, c.d_scal, sizeof(double), cudaMemcpyDeviceToHost, c.s));
     HB_CUDA(cudaStreamSynchronize(c.s));
-    const double compl_ = c.h_scal[0];
+    double compl_ = c.h_scal[0];
     primalObj = c.trace_cx(X);
-    const double minEig = min_eig_estimate(h, X);
+    double minEig = min_eig_estimate(h, X);
+    if (h->lp) {
+        // the LP cone: A x into the residual, x . s, c . x, and min x in place of lambda_min
+        std::vector<double> xl(h->lp->nCol, 0.0), sl(h->lp->nCol, 0.0);
+        lp_values(h, xl.data(), sl.data());
+        h->lp->atimesx(xl.data(), ax.data());
+        double d = 0.0;
+        for (int k = 0; k < h->lp->nCol; ++k) d += xl[k] * sl[k];
+        compl_ += d;
+        primalObj += h->lp->trace_cx(xl.data());
+        double mn = HDSDP_INFINITY;
+        for (double v : xl) mn = std::min(mn, v);
+        minEig = std::min(minEig, mn);
+    }
     hb::cache_free(X);
     hb::cache_free(S);
     dualObj /= (pScal * dScal);
@@ -1396,10 +1483,16 @@ hdsdp_retcode HDSDPOptimize(hdsdp *h, int dOptOnly) {
     h->log.clear();
     adjoint_release(h->adj);
     if (!h->usr) return HDSDP_RETCODE_FAILED;
+    if (h->nCones == 2 && !h->usrLp) return HDSDP_RETCODE_FAILED;
     if (h->cone) {
         h->cone->release();
         delete h->cone;
         h->kkt.release();
+    }
+    if (h->lp) {
+        h->lp->release();
+        delete h->lp;
+        h->lp = nullptr;
     }
     h->cone = new SdpCone();
     h->cone->precision = h->precision;
@@ -1408,6 +1501,16 @@ hdsdp_retcode HDSDPOptimize(hdsdp *h, int dOptOnly) {
     CALL(h->cone->proc_data(u->nConicRow, u->nConicCol, u->coneMatBeg, u->coneMatIdx, u->coneMatElem));
     tp1 = wall();
     CALL(h->cone->presolve());
+    if (h->nCones == 2) {
+        user_data *ul = h->usrLp;
+        if (ul->nConicRow != h->nRows) {
+            retcode = HDSDP_RETCODE_FAILED;
+            goto exit_cleanup;
+        }
+        h->lp = new LpCone();
+        CALL(h->lp->proc_data(ul->nConicRow, ul->nConicCol, ul->coneMatBeg, ul->coneMatIdx, ul->coneMatElem,
+                              h->stream));
+    }
     tp2 = wall();
     get_statistics(h);
     adjust_params(h);
@@ -1463,6 +1566,10 @@ hdsdp_retcode HDSDPGetRowDual(hdsdp *h, double *pObjVal, double *dObjVal, double
 
 void HDSDPGetConeValues(hdsdp *h, int iCone, double *conePrimal, double *coneDual, double *coneAuxi) {
     (void) coneAuxi;
+    if (iCone == 1 && h->lp) {
+        lp_values(h, conePrimal, coneDual);  // x and s of the LP cone
+        return;
+    }
     if (iCone != 0 || !h->cone) return;
     SdpCone &c = *h->cone;
     const int n = c.n;
@@ -1495,6 +1602,11 @@ void HDSDPClear(hdsdp *h) {
         h->cone = nullptr;
     }
     h->kkt.release();
+    if (h->lp) {
+        h->lp->release();
+        delete h->lp;
+        h->lp = nullptr;
+    }
 }
 
 void HDSDPDestroy(hdsdp **pHSolver) {

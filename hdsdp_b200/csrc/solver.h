@@ -146,6 +146,46 @@ struct BoundCone {
     void get_primal(double mu, const double *y, const double *dy, double *lower, double *upper) const;
 };
 
+// LP cone s = c - A^T y - r >= 0 (interface/hdsdp_conic_lp.c), host-side O(nnz)
+// except its Schur block, added on the device. A is stored by constraint: column i
+// (0 .. m-1) lists the LP columns k with A_ki, in the user's order.
+struct LpCone {
+    int m = 0, nCol = 0;
+    std::vector<double> obj;                  // c
+    std::vector<int> beg, idx;
+    std::vector<double> val;
+    std::vector<double> s, sChk, sStep, sInv, buf;
+    double dualResidual = 0.0, dualPerturb = 0.0;
+    // Schur block: the lower pairs (i >= j) of constraints that share an LP column, and
+    // the per-build values added to M there
+    std::vector<int> pairI, pairJ;
+    std::vector<double> pairVal;
+    int *d_pi = nullptr, *d_pj = nullptr;
+    double *d_pv = nullptr;
+    cudaStream_t st = nullptr;
+
+    hdsdp_retcode proc_data(int nRow, int nCol_, const int *Ap, const int *Ai, const double *Ax, cudaStream_t stream);
+    void release();
+    double obj_norm(int type) const;
+    double coeff_norm(int type) const;
+    void scal(double a);
+    void detect_feature(int intF[20], double dblF[20]) const;
+    void update_buffer(double dC, double dAs, const double *y, double dEye, int which);
+    void set_start(double r) { dualResidual = r; }
+    void reduce_resi(double r) { dualResidual = r; }
+    void set_perturb(double p) { dualPerturb = p; }
+    void update(double tau, const double *y) { update_buffer(tau, -1.0, y, -dualResidual, BUFFER_DUALVAR); }
+    double ratio_test(double dtau, const double *dy, double ada, int which);
+    int interior_check(double tau, const double *y);
+    int interior_check_expert(double dC, double dAs, const double *y, double dEye, int which);
+    double get_barrier(double tau, const double *y, int which);
+    int add_step_and_check(double step, int which);
+    void get_primal(double mu, const double *y, const double *dy, double *x);   // host x (nCol)
+    void get_dual(double *out) const;                                         // host (nCol)
+    void atimesx(const double *x, double *out) const;                         // out (m) accumulated
+    double trace_cx(const double *x) const;
+};
+
 // Schur complement system (interface/hdsdp_schur.c).
 struct KKT {
     int m = 0;
@@ -165,6 +205,7 @@ struct KKT {
     void release();
     void clean(int type);
     hdsdp_retcode build(SdpCone &cone, int type);
+    void add_lp(LpCone &lp, int type);
     void add_bound(BoundCone &b, int type);
     void regularize(double reg);
     hdsdp_retcode factorize();
@@ -188,6 +229,8 @@ struct hdsdp_solver_internal {
     std::vector<double> rowRHS;
     hb::SdpCone *cone = nullptr;
     user_data *usr = nullptr;
+    hb::LpCone *lp = nullptr;      // optional LP cone (the last cone, as in the reference's drivers)
+    user_data *usrLp = nullptr;
     hb::BoundCone bnd;
     hb::KKT kkt;
     cudaStream_t stream = nullptr;

@@ -216,6 +216,31 @@ def theta_adjoint(n: int = 200, p: float = 0.1, zero_frac: float = 0.2, seed: in
                      {"edges": int(ei.size), "zeros": int(zi.size), "seed": seed})
 
 
+def lp_block(m: int, n_lp: int, per_col: int = 2, seed: int = 7):
+    """An LP cone for an instance with m constraints, in the user CSC layout the LP cone
+    takes (interface/hdsdp_conic_lp.c:99-158): column 0 the costs c (U(0.5, 1.5)),
+    column i the coefficients of constraint i on the LP columns. Each LP column k gets
+    `per_col` constraints with U(0.2, 1) coefficients, so s = c - A^T y > 0 for every
+    y <= 0; returns (n_lp, Ap, Ai, Ax)."""
+    rng = np.random.default_rng(seed)
+    c = rng.uniform(0.5, 1.5, size=n_lp)
+    cols = [[] for _ in range(m)]
+    for k in range(n_lp):
+        for i in rng.choice(m, size=min(per_col, m), replace=False):
+            cols[int(i)].append((k, float(rng.uniform(0.2, 1.0))))
+    Ap, Ai, Ax = [0], [], []
+    for k in range(n_lp):
+        Ai.append(k)
+        Ax.append(float(c[k]))
+    Ap.append(len(Ai))
+    for i in range(m):
+        for k, v in sorted(cols[i]):
+            Ai.append(k)
+            Ax.append(v)
+        Ap.append(len(Ai))
+    return n_lp, np.asarray(Ap, np.int32), np.asarray(Ai, np.int32), np.asarray(Ax, np.float64)
+
+
 WORKLOADS = {
     "maxcut_n200": lambda: maxcut(200, 0.05, seed=1),
     "theta_n300": lambda: lovasz_theta(300, 0.1, seed=2),

@@ -18,6 +18,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_ref", "libhdsdp_ref.so")
 
+CONETYPE_LP = 1  # HDSDP_CONETYPE_LP
 CONETYPE_DENSE_SDP = 4  # interface/def_hdsdp_conic.h:22-32
 
 _lib = None
@@ -89,8 +90,9 @@ def set_threads(n: int):
         pass
 
 
-def solve(inst, want_x: bool = True, params: dict | None = None, quiet: bool = True) -> dict:
-    """Run HDSDPOptimize on ``inst``; return y, objectives, status, X, S, errors, time."""
+def solve(inst, want_x: bool = True, params: dict | None = None, quiet: bool = True, lp=None) -> dict:
+    """Run HDSDPOptimize on ``inst`` (plus the LP cone ``lp`` = (n_lp, Ap, Ai, Ax) as cone 1,
+    as the reference's own driver adds it); return y, objectives, status, X, S, errors, time."""
     L = lib()
     Ap = np.ascontiguousarray(inst.Ap, dtype=np.int32)
     Ai = np.ascontiguousarray(inst.Ai, dtype=np.int32)
@@ -101,8 +103,17 @@ def solve(inst, want_x: bool = True, params: dict | None = None, quiet: bool = T
     assert L.HDSDPCreate(C.byref(h)) == 0
     assert L.HUserDataCreate(C.byref(ud)) == 0
     L.HUserDataSetConeData(ud, CONETYPE_DENSE_SDP, inst.m, inst.n, _ip(Ap), _ip(Ai), _dp(Ax))
-    assert L.HDSDPInit(h, inst.m, 1) == 0
+    ulp = C.c_void_p()
+    keep = []
+    assert L.HDSDPInit(h, inst.m, 2 if lp is not None else 1) == 0
     assert L.HDSDPSetCone(h, 0, ud) == 0
+    if lp is not None:
+        nlp, lAp, lAi, lAx = lp
+        keep = [np.ascontiguousarray(lAp, dtype=np.int32), np.ascontiguousarray(lAi, dtype=np.int32),
+                np.ascontiguousarray(lAx, dtype=np.float64)]
+        assert L.HUserDataCreate(C.byref(ulp)) == 0
+        L.HUserDataSetConeData(ulp, CONETYPE_LP, inst.m, int(nlp), _ip(keep[0]), _ip(keep[1]), _dp(keep[2]))
+        assert L.HDSDPSetCone(h, 1, ulp) == 0
     L.HDSDPSetDualObjective(h, _dp(b))
     for k, v in (params or {}).items():
         if isinstance(v, int):
@@ -140,6 +151,11 @@ def solve(inst, want_x: bool = True, params: dict | None = None, quiet: bool = T
         L.HDSDPCheckSolution(h, _dp(errs))
         out["errs"] = errs
         out["status_after_check"] = int(L.oracle_status(h))
+        if lp is not None:
+            xl, sl = np.zeros(int(lp[0])), np.zeros(int(lp[0]))
+            L.HDSDPGetConeValues(h, 1, _dp(xl), _dp(sl), _dp(np.zeros(int(lp[0]))))
+            out["x_lp"], out["s_lp"] = xl, sl
+            L.HUserDataDestroy(C.byref(ulp))
         L.HUserDataDestroy(C.byref(ud))
         L.HDSDPDestroy(C.byref(h))  # prints its closing line
     finally:

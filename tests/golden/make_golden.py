@@ -32,6 +32,20 @@ SMALL = {
     "rank1_50_80": lambda: instances.rank_one(50, 80, 0.2, seed=4),
     "theta_adj40": lambda: instances.theta_adjoint(40, 0.2, 0.3, seed=2),
 }
+# The small SDP blocks with an LP cone as cone 1 (instances.lp_block).
+LP_CASES = {
+    "maxcut60+lp9": ("maxcut60", 9, 2, 11),
+    "theta40+lp25": ("theta40", 25, 2, 12),
+    "rank1_50_80+lp31": ("rank1_50_80", 31, 3, 13),
+}
+
+
+def lp_case(name):
+    base, nlp, per, seed = LP_CASES[name]
+    inst = SMALL[base]()
+    return inst, instances.lp_block(inst.m, nlp, per, seed=seed)
+
+
 FULL = {
     "theta_n300": lambda: instances.WORKLOADS["theta_n300"](),
     "rank1_n1000_m2000": lambda: instances.WORKLOADS["rank1_n1000_m2000"](),
@@ -72,6 +86,21 @@ def main(full: bool):
             arrays["M/" + name] = np.tril(sp["M"])
             arrays["asinv/" + name] = sp["asinv"]
             arrays["asinvrd/" + name] = sp["asinvrd"]
+    # SDP block + LP cone
+    out["lp_solves"] = {}
+    for name in LP_CASES:
+        inst, lp = lp_case(name)
+        for psdp in (0, 1):
+            r = ref_api.solve(inst, want_x=False, params={4: psdp}, lp=lp)
+            key = "%s/psdp%d" % (name, psdp)
+            out["lp_solves"][key] = {
+                "n": inst.n, "m": inst.m, "n_lp": int(lp[0]), "retcode": r["retcode"], "iters": r["iters"],
+                "status": r["status_after_check"], "pobj": r["pobj"], "dobj": r["dobj"],
+                "errs": [float(e) for e in r["errs"]],
+            }
+            arrays["y/" + key] = r["y"]
+            arrays["x_lp/" + key] = r["x_lp"]
+            print(key, r["iters"], r["status_after_check"], r["pobj"], r["dobj"], flush=True)
     # known answers of the Lovasz theta number, solved by the reference
     ka = {}
     for label, inst, value in [

@@ -111,3 +111,18 @@ def test_sdpa_file_solve(gpu_lib, tmp_path):
     assert via_file["iters"] == direct["iters"]
     assert via_file["dobj"] == pytest.approx(direct["dobj"], rel=1e-12)
     assert via_file["pobj"] == pytest.approx(direct["pobj"], rel=1e-12)
+
+
+@pytest.mark.parametrize("psdp", [0, 1])
+@pytest.mark.parametrize("name", ["maxcut60+lp9", "theta40+lp25", "rank1_50_80+lp31"])
+def test_sdp_plus_lp_parity(gpu_lib, name, psdp, golden):
+    """One SDP block with an LP cone as cone 1 (interface/hdsdp_conic_lp.c) against the
+    compiled reference on the same data; with primal refinement on, the reference
+    declines it for more than one cone and ends at Phase B's 10 % gap."""
+    from make_golden import lp_case
+    inst, lp = lp_case(name)
+    r = api.solve(inst, want_x=False, primal_refinement=bool(psdp), lp=lp)
+    ref = golden["lp_solves"]["%s/psdp%d" % (name, psdp)]
+    check_parity(r, ref, psdp=bool(psdp))
+    if ref["status"] == OPTIMAL and not psdp:
+        assert r["x_lp"].min() >= -1e-7 and r["s_lp"].min() > 0.0
