@@ -262,6 +262,23 @@ def read_sdpa(path):
     return read_sdpa_with(_lib.load(), path)
 
 
+def sdpa_problem(path):
+    """An SDPA file with one SDP block and at most one LP block: (instance, lp) for
+    solve(instance, lp=lp), lp None without an LP block."""
+    from hdsdp_b200.instances import SDPInstance
+    d = read_sdpa(path)
+    if len(d["blocks"]) != 1:
+        raise ValueError("this solver takes one SDP block (and optionally one LP block)")
+    n, Ap, Ai, Ax = d["blocks"][0]
+    inst = SDPInstance(os.path.basename(str(path)), n, d["m"], Ap.astype(np.int32), Ai.astype(np.int32),
+                       Ax.astype(np.float64), d["b"].astype(np.float64))
+    lp = None
+    if d["lp"] is not None:
+        nlp, lAp, lAi, lAx = d["lp"]
+        lp = (nlp, lAp.astype(np.int32), lAi.astype(np.int32), lAx.astype(np.float64))
+    return inst, lp
+
+
 def sdpa_instance(path):
     """An SDPA file with one SDP block and no LP block as an instance for solve()."""
     from hdsdp_b200.instances import SDPInstance

@@ -38,6 +38,22 @@ def write_sdpa(path, inst, header_style=0):
         f.write("\n".join(lines) + "\n")
 
 
+def write_sdpa_lp(path, inst, lp):
+    """An instance and an LP cone (n_lp, Ap, Ai, Ax) as an SDPA file with a diagonal LP block
+    (negative block size): LP column k is diagonal entry (k, k) of block 2."""
+    write_sdpa(path, inst)
+    nlp, Ap, Ai, Ax = lp
+    lines = open(path).read().splitlines()
+    lines[3] = "2 = nBLOCK"
+    lines[4] = "%d %d = bLOCKsTRUCT" % (inst.n, -nlp)
+    for k in range(inst.m + 1):
+        sign = -1.0 if k == 0 else 1.0
+        for e in range(Ap[k], Ap[k + 1]):
+            lines.append("%d 2 %d %d %.17g" % (k, Ai[e] + 1, Ai[e] + 1, sign * Ax[e]))
+    with open(path, "w") as f:
+        f.write("\n".join(lines) + "\n")
+
+
 @pytest.fixture(scope="module")
 def libs():
     build()
@@ -149,3 +165,23 @@ def test_sdpa_instance(libs, tmp_path):
     got = api.sdpa_instance(path)
     assert got.n == inst.n and got.m == inst.m
     np.testing.assert_array_equal(got.b, inst.b)
+
+
+def test_sdpa_with_lp_block(libs, tmp_path):
+    """An SDP block plus an LP cone written as SDPA and read back: the same LP arrays as the
+    reference reader, and the LP cone the solver takes."""
+    from make_golden import lp_case
+    ours, ref = libs
+    inst, lp = lp_case("theta40+lp25")
+    path = tmp_path / "lp.dat-s"
+    write_sdpa_lp(path, inst, lp)
+    a = api.read_sdpa_with(ours, path)
+    same(a, api.read_sdpa_with(ref, path))
+    got_inst, got_lp = api.sdpa_problem(path)
+    assert got_lp[0] == lp[0]
+    for k in range(inst.m + 1):
+        lo, hi = lp[1][k], lp[1][k + 1]
+        glo, ghi = got_lp[1][k], got_lp[1][k + 1]
+        np.testing.assert_array_equal(np.sort(lp[2][lo:hi]), np.sort(got_lp[2][glo:ghi]))
+        np.testing.assert_array_equal(lp[3][lo:hi][np.argsort(lp[2][lo:hi])],
+                                      got_lp[3][glo:ghi][np.argsort(got_lp[2][glo:ghi])])

@@ -126,3 +126,19 @@ def test_sdp_plus_lp_parity(gpu_lib, name, psdp, golden):
     check_parity(r, ref, psdp=bool(psdp))
     if ref["status"] == OPTIMAL and not psdp:
         assert r["x_lp"].min() >= -1e-7 and r["s_lp"].min() > 0.0
+
+
+def test_sdpa_file_with_lp_block_solve(gpu_lib, tmp_path):
+    """An SDP block plus an LP cone written as an SDPA file (diagonal LP block), read back and
+    solved, matches the reference's solve of the same data."""
+    from make_golden import lp_case
+    from test_file_io_cpu import write_sdpa_lp
+    inst, lp = lp_case("theta40+lp25")
+    path = tmp_path / "theta40_lp.dat-s"
+    write_sdpa_lp(path, inst, lp)
+    finst, flp = api.sdpa_problem(path)
+    r = api.solve(finst, want_x=False, primal_refinement=False, lp=flp)
+    direct = api.solve(inst, want_x=False, primal_refinement=False, lp=lp)
+    assert r["status_after_check"] == direct["status_after_check"] == OPTIMAL
+    assert abs(r["iters"] - direct["iters"]) <= 2
+    assert r["dobj"] == pytest.approx(direct["dobj"], rel=1e-8)
