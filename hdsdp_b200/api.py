@@ -42,6 +42,7 @@ class Solver:
         if self.L.HDSDPCreate(C.byref(self.h)) != 0:
             raise RuntimeError("HDSDPCreate failed (no CUDA device?)")
         self._keep = []
+        self._cones = {}  # cone index -> (kind, dim, user data, arrays held until optimize)
 
     def init(self, n_rows: int, n_cones: int = 1):
         self.m = n_rows
@@ -75,6 +76,32 @@ class Solver:
             raise RuntimeError("HUserDataCreate failed")
         self.L.HUserDataSetConeData(self.ud_lp, CONETYPE_LP, m, n_lp, _ip(Ap), _ip(Ai), _dp(Ax))
         return self.L.HDSDPSetCone(self.h, 1, self.ud_lp)
+
+    def set_cone_at(self, i: int, kind: str, m: int, dim: int, Ap, Ai, Ax):
+        """Cone ``i`` of a multi-cone problem: kind "sdp" (a block of order dim, the user CSC
+        layout with packed lower-triangle rows; the library picks a dense or sparse cone)
+        or "lp" (dim columns)."""
+        if len(Ap) != m + 2:
+            raise ValueError("Ap must hold m + 2 column pointers (column 0 is the objective)")
+        arrs = [np.ascontiguousarray(Ap, dtype=np.int32), np.ascontiguousarray(Ai, dtype=np.int32),
+                np.ascontiguousarray(Ax, dtype=np.float64)]
+        ud = C.c_void_p()
+        if self.L.HUserDataCreate(C.byref(ud)) != 0:
+            raise RuntimeError("HUserDataCreate failed")
+        self.L.HUserDataSetConeData(ud, CONETYPE_DENSE_SDP if kind == "sdp" else CONETYPE_LP, m, dim,
+                                    _ip(arrs[0]), _ip(arrs[1]), _dp(arrs[2]))
+        self._cones[i] = (kind, dim, ud, arrs)
+        return self.L.HDSDPSetCone(self.h, i, ud)
+
+    def get_cone_values_at(self, i: int):
+        """(X, S) of SDP cone i (n x n), or (x, s) of LP cone i."""
+        kind, dim = self._cones[i][:2]
+        size = dim * dim if kind == "sdp" else dim
+        P, D, aux = np.zeros(size), np.zeros(size), np.zeros(size)
+        self.L.HDSDPGetConeValues(self.h, i, _dp(P), _dp(D), _dp(aux))
+        if kind == "sdp":
+            return P.reshape(dim, dim, order="F"), D.reshape(dim, dim, order="F")
+        return P, D
 
     def get_lp_values(self):
         """(x, s) of the LP cone."""
@@ -159,6 +186,9 @@ class Solver:
         return gb, gC, gAx
 
     def close(self):
+        for kind, dim, ud, arrs in self._cones.values():
+            self.L.HUserDataDestroy(C.byref(ud))
+        self._cones = {}
         if self.ud:
             self.L.HUserDataDestroy(C.byref(self.ud))
             if getattr(self, "ud_lp", None):
@@ -205,6 +235,38 @@ def solve(inst, want_x: bool = True, primal_refinement: bool = True, precision: 
             out["X"], out["S"] = X, S
         if lp is not None:
             out["x_lp"], out["s_lp"] = s.get_lp_values()
+        out["errs"] = s.check_solution()
+        out["status_after_check"] = s.status()
+        return out
+    finally:
+        s.close()
+
+
+def solve_problem(prob, primal_refinement: bool = True, precision: int = 0, params: dict | None = None) -> dict:
+    """Solve a multi-cone problem (instances.ConicProblem: SDP blocks and LP cones over one
+    set of constraints) on the GPU; returns y, objectives, status, iterations, the iteration
+    log, DIMACS errors and per cone (X, S) or (x, s)."""
+    s = Solver()
+    try:
+        assert s.init(prob.m, len(prob.cones)) == 0
+        for k, (kind, dim, Ap, Ai, Ax) in enumerate(prob.cones):
+            if s.set_cone_at(k, kind, prob.m, int(dim), Ap, Ai, Ax) != 0:
+                raise RuntimeError("HDSDPSetCone rejected cone %d" % k)
+        s.set_dual_objective(prob.b)
+        s.set_primal_refinement(primal_refinement)
+        s.set_precision(precision)
+        for k, v in (params or {}).items():
+            if isinstance(v, int):
+                s.set_int_param(k, v)
+            else:
+                s.set_dbl_param(k, v)
+        t0 = time.perf_counter()
+        ret = s.optimize(0)
+        t1 = time.perf_counter()
+        po, do, y = s.get_row_dual()
+        out = {"retcode": int(ret), "time": t1 - t0, "y": y, "pobj": po, "dobj": do,
+               "status": s.status(), "iters": s.iters(), "log": s.iter_log(), "timers": s.timers()}
+        out["values"] = [s.get_cone_values_at(k) for k in range(len(prob.cones))]
         out["errs"] = s.check_solution()
         out["status_after_check"] = s.status()
         return out
@@ -260,6 +322,20 @@ def read_sdpa_with(lib, path):
 def read_sdpa(path):
     """An SDPA file through this library's HReadSDPA (include/hdsdp_file_io.h)."""
     return read_sdpa_with(_lib.load(), path)
+
+
+def sdpa_cones(path):
+    """An SDPA file with any number of SDP blocks and an optional LP block as a multi-cone
+    problem for solve_problem(): the SDP blocks in file order, then the LP cone (the order
+    the reference's own driver sets them in)."""
+    from hdsdp_b200.instances import ConicProblem
+    d = read_sdpa(path)
+    cones = [("sdp", int(n), Ap.astype(np.int32), Ai.astype(np.int32), Ax.astype(np.float64))
+             for (n, Ap, Ai, Ax) in d["blocks"]]
+    if d["lp"] is not None:
+        nlp, lAp, lAi, lAx = d["lp"]
+        cones.append(("lp", int(nlp), lAp.astype(np.int32), lAi.astype(np.int32), lAx.astype(np.float64)))
+    return ConicProblem(os.path.basename(str(path)), int(d["m"]), d["b"].astype(np.float64), cones)
 
 
 def sdpa_problem(path):

@@ -224,7 +224,7 @@ hdsdp_retcode prepare(hdsdp *h, AdjointState &a) {
     if (a.FM.fuse_k) compute_inverse_factor(s, a.FM);
 
     // (column, row, col) of every stored value of the user's CSC data
-    const user_data *u = h->usr;
+    const user_data *u = h->cones[0].usr;
     a.nnz = u->coneMatBeg[m + 1];
     std::vector<int> col(a.nnz), ri(a.nnz), ci(a.nnz);
     std::vector<long> start(n);
@@ -256,7 +256,8 @@ hdsdp_retcode prepare(hdsdp *h, AdjointState &a) {
 
 hdsdp_retcode adjoint_vjp(hdsdp *h, AdjointState *&state, const double *gy, const double *GX, double *gb,
                           double *gC, double *gAx) {
-    if (!h || !h->optimized || !h->cone || !h->usr) return HDSDP_RETCODE_FAILED;
+    // defined for a problem of one dense SDP cone
+    if (!h || !h->optimized || !h->cone || h->nCones != 1 || h->cone->sparse) return HDSDP_RETCODE_FAILED;
     if (!state) state = new AdjointState();
     AdjointState &a = *state;
     if (!a.ready) {

@@ -109,12 +109,24 @@ void normalize_r1(HostCoeff &h) {
 
 }  // namespace
 
-hdsdp_retcode SdpCone::proc_data(int nRow, int nCol, const int *Ap, const int *Ai, const double *Ax) {
+// sdpDenseConeProcDataImpl / sdpSparseConeProcDataImpl (interface/hdsdp_conic_sdp.c:1407-1484):
+// a sparse cone keeps the constraints with a nonzero column, counting the others as zero
+// coefficients.
+hdsdp_retcode SdpCone::proc_data(int nRow, int nCol, const int *Ap, const int *Ai, const double *Ax,
+                                 bool sparseCone) {
     n = nCol;
-    m = nRow;
+    mAll = nRow;
+    sparse = sparseCone;
+    rows.clear();
+    if (sparse) {
+        for (int i = 0; i < nRow; ++i)
+            if (Ap[i + 2] - Ap[i + 1] > 0) rows.push_back(i);
+    }
+    m = sparse ? (int) rows.size() : nRow;
     A.assign(m, HostCoeff());
     refType.assign(m, REF_ZERO);
     for (int k = 0; k < 5; ++k) stats[k] = 0;
+    if (sparse) stats[REF_ZERO] = nRow - m;
     const long npack = (long) n * (n + 1) / 2;
     auto load = [&](int col, HostCoeff &h, int &type) -> hdsdp_retcode {
         const int s0 = Ap[col], s1 = Ap[col + 1];
@@ -163,10 +175,17 @@ hdsdp_retcode SdpCone::proc_data(int nRow, int nCol, const int *Ap, const int *A
     int bad = 0;
 #pragma omp parallel for schedule(dynamic, 16) reduction(+ : bad)
     for (int i = 0; i < m; ++i)
-        if (load(i + 1, A[i], refType[i]) != HDSDP_RETCODE_OK) bad += 1;
+        if (load((sparse ? rows[i] : i) + 1, A[i], refType[i]) != HDSDP_RETCODE_OK) bad += 1;
     if (bad) return HDSDP_RETCODE_FAILED;
     for (int i = 0; i < m; ++i) stats[refType[i]] += 1;
     return HDSDP_RETCODE_OK;
+}
+
+const double *SdpCone::local(const double *v) {
+    if (!sparse || !v) return v;
+    ybuf.resize(m);
+    for (int i = 0; i < m; ++i) ybuf[i] = v[rows[i]];
+    return ybuf.data();
 }
 
 // sdpDenseConePresolveImpl (interface/hdsdp_conic_sdp.c:1486-1514): rank-one detection.
@@ -333,6 +352,10 @@ hdsdp_retcode SdpCone::setup_device(cudaStream_t stream, Timers *t) {
     lz.init(n, s);
     HB_CUDA(hb::cmalloc(&d_y, sizeof(double) * std::max(m, 1)));
     HB_CUDA(hb::cmalloc(&d_vec, sizeof(double) * std::max(m, 1)));
+    if (sparse && m > 0) {
+        HB_CUDA(hb::cmalloc(&d_rows, sizeof(int) * m));
+        HB_CUDA(cudaMemcpyAsync(d_rows, rows.data(), sizeof(int) * m, cudaMemcpyHostToDevice, s));
+    }
     HB_CUDA(hb::cmalloc_host(&h_vec, sizeof(double) * std::max(m, 1)));
     HB_CUDA(hb::cmalloc(&d_scal, sizeof(double) * 8));
     HB_CUDA(hb::cmalloc_host(&h_scal, sizeof(double) * 8));
@@ -343,10 +366,11 @@ hdsdp_retcode SdpCone::setup_device(cudaStream_t stream, Timers *t) {
 void SdpCone::release() {
     dev.release();
     auto f = [](void *p) { if (p) hb::cache_free(p); };
-    f(Svar); f(Scheck); f(dS); f(W); f(d_y); f(d_vec); f(d_scal);
+    f(Svar); f(Scheck); f(dS); f(W); f(d_y); f(d_vec); f(d_scal); f(d_rows);
     if (h_vec) hb::cache_free_host(h_vec);
     if (h_scal) hb::cache_free_host(h_scal);
     Svar = Scheck = dS = W = d_y = d_vec = d_scal = h_vec = h_scal = nullptr;
+    d_rows = nullptr;
     Fvar.release();
     Fcheck.release();
     lz.release();
@@ -356,6 +380,7 @@ void SdpCone::release() {
 // (sdpDenseConeIUpdateBuffer, interface/hdsdp_conic_sdp.c:343-402)
 void SdpCone::update_buffer(double dC, double dAs, const double *y, double dEye, int which) {
     double t0 = wall();
+    y = local(y);
     double *target = (which == BUFFER_DUALVAR) ? Svar : (which == BUFFER_DUALCHECK) ? Scheck : dS;
     if (which != BUFFER_DUALSTEP) dEye += dualPerturb;
     if (which != BUFFER_DUALSTEP) {
@@ -522,10 +547,11 @@ void SdpCone::get_dual(double *S) {
 }
 
 void SdpCone::atimesx(const double *X, double *out) {
+    if (m == 0) return;
     dev.inner_all(X, ld, d_vec);
     HB_CUDA(cudaMemcpyAsync(h_vec, d_vec, sizeof(double) * m, cudaMemcpyDeviceToHost, s));
     HB_CUDA(cudaStreamSynchronize(s));
-    std::memcpy(out, h_vec, sizeof(double) * m);
+    for (int i = 0; i < m; ++i) out[sparse ? rows[i] : i] += h_vec[i];
 }
 
 double SdpCone::trace_cx(const double *X) { return dev.c_inner(X, ld); }
@@ -645,6 +671,9 @@ void KKT::init(int m_, cudaStream_t stream, Timers *t) {
 void KKT::release() {
     if (M) hb::cache_free(M);
     M = nullptr;
+    if (Msub) hb::cache_free(Msub);
+    Msub = nullptr;
+    msubCap = 0;
     F.release();
     for (double **p : {&d_rhs, &d_x, &d_r, &d_t, &d_diag}) {
         if (*p) hb::cache_free(*p);
@@ -662,13 +691,39 @@ void KKT::clean(int type) {
         dCSinv = dCSinvCSinv = dCSinvRdSinv = 0.0;
     }
     dTraceSinv = 0.0;
+    // HKKTClean (interface/hdsdp_schur.c:141-164): these builds form M anew
+    if (type == KKT_TYPE_INFEASIBLE || type == KKT_TYPE_HOMOGENEOUS || type == KKT_TYPE_PRIMAL) mOpen = false;
 }
 
+void KKT::open_m() {
+    if (mOpen) return;
+    HB_CUDA(cudaMemsetAsync(M, 0, sizeof(double) * ldm * m, s));
+    mOpen = true;
+}
+
+// M[rows[i], rows[j]] += B[i, j] over the lower triangle i >= j of a cone's Schur block
+// (rows == nullptr: the identity). rows increases, so the lower triangle of B lands in the
+// lower triangle of M.
+__global__ void scatter_lower_kernel(int mk, const double *__restrict__ B, long ldb, const int *__restrict__ rows,
+                                     double *__restrict__ M, long ldm) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    for (int j = blockIdx.y * blockDim.y + threadIdx.y; j < mk; j += gridDim.y * blockDim.y) {
+        if (i < j || i >= mk) continue;
+        const long gi = rows ? rows[i] : i, gj = rows ? rows[j] : j;
+        M[gi + gj * ldm] += B[i + (long) j * ldb];
+    }
+}
+
+// dst[rows[i]] += scale * d_src[i] (rows == nullptr: the identity)
 static void add_host(std::vector<double> &dst, const double *d_src, double *h_buf, int m, double scale,
-                     cudaStream_t s) {
+                     cudaStream_t s, const std::vector<int> *rows = nullptr) {
+    if (m == 0) return;
     HB_CUDA(cudaMemcpyAsync(h_buf, d_src, sizeof(double) * m, cudaMemcpyDeviceToHost, s));
     HB_CUDA(cudaStreamSynchronize(s));
-    for (int i = 0; i < m; ++i) dst[i] += scale * h_buf[i];
+    if (rows)
+        for (int i = 0; i < m; ++i) dst[(*rows)[i]] += scale * h_buf[i];
+    else
+        for (int i = 0; i < m; ++i) dst[i] += scale * h_buf[i];
 }
 
 // Smallest block order for which split precision also forms S^-1 on the tensor cores
@@ -676,10 +731,12 @@ static void add_host(std::vector<double> &dst, const double *d_src, double *h_bu
 constexpr int kSplitInverseMinN = 1024;
 
 // sdpDenseConeGetKKT / GetKKTByFixedStrategy (interface/hdsdp_conic_sdp.c:1722-1872)
-hdsdp_retcode KKT::build(SdpCone &cone, int type) {
+// (interface/hdsdp_conic_sdp.c:1874-1938 for a sparse cone): adds the cone's terms to M and
+// to the right-hand-side vectors of the build that clean() opened.
+hdsdp_retcode KKT::add_sdp(SdpCone &cone, int type) {
     double t0 = wall();
-    clean(type);
     const int n = cone.n;
+    const std::vector<int> *rows = cone.sparse ? &cone.rows : nullptr;
     const long ld = cone.ld;
     const double r = cone.dualResidual;
     const double *Wp = nullptr;
@@ -704,10 +761,10 @@ hdsdp_retcode KKT::build(SdpCone &cone, int type) {
     SdpDevice &dev = cone.dev;
     if (type == KKT_TYPE_CORRECTOR) {
         dev.inner_all(Wp, ld, cone.d_vec);
-        add_host(asinv, cone.d_vec, h_buf, m, 1.0, s);
+        add_host(asinv, cone.d_vec, h_buf, cone.m, 1.0, s, rows);
         if (r != 0.0) {
             dev.inner_all_sq(Wp, ld, cone.d_vec, false, true);
-            add_host(asinvrd, cone.d_vec, h_buf, m, r, s);
+            add_host(asinvrd, cone.d_vec, h_buf, cone.m, r, s, rows);
         }
         if (tm) tm->schur += wall() - t0;
         return device_error_flag() ? HDSDP_RETCODE_FAILED : HDSDP_RETCODE_OK;
@@ -719,21 +776,38 @@ hdsdp_retcode KKT::build(SdpCone &cone, int type) {
         dTraceSinv += cone.h_scal[0];
     }
     double tq = wall();
-    dev.schur_matrix(Wp, ld, M, ldm, (type == KKT_TYPE_PRIMAL) ? nullptr : cone.Fvar.K);
+    if (!rows && !mOpen) {
+        // the first contribution, from a cone holding every constraint: written outright
+        dev.schur_matrix(Wp, ld, M, ldm, (type == KKT_TYPE_PRIMAL) ? nullptr : cone.Fvar.K);
+        mOpen = true;
+    } else if (cone.m > 0) {
+        open_m();
+        const int mk = cone.m;
+        const long ldk = pad_ld(mk);
+        if (msubCap < (size_t) ldk * mk) {
+            if (Msub) hb::cache_free(Msub);
+            msubCap = (size_t) ldk * mk;
+            HB_CUDA(hb::cmalloc(&Msub, sizeof(double) * msubCap));
+        }
+        dev.schur_matrix(Wp, ld, Msub, ldk, (type == KKT_TYPE_PRIMAL) ? nullptr : cone.Fvar.K);
+        dim3 blk(32, 8), grd((mk + 31) / 32, std::min((mk + 7) / 8, 4096));
+        scatter_lower_kernel<<<hb::counted(grd), blk, 0, s>>>(mk, Msub, ldk, cone.d_rows, M, ldm);
+        HB_CUDA(cudaGetLastError());
+    }
     if (tm) {
         HB_CUDA(cudaStreamSynchronize(s));
         tm->sch_matrix += wall() - tq;
         tq = wall();
     }
     dev.inner_all(Wp, ld, cone.d_vec, true);
-    add_host(asinv, cone.d_vec, h_buf, m, 1.0, s);
+    add_host(asinv, cone.d_vec, h_buf, cone.m, 1.0, s, rows);
     if (tm) {
         tm->sch_inner += wall() - tq;
         tq = wall();
     }
     if (r != 0.0) {
         dev.inner_all_sq(Wp, ld, cone.d_vec, true);
-        add_host(asinvrd, cone.d_vec, h_buf, m, r, s);
+        add_host(asinvrd, cone.d_vec, h_buf, cone.m, r, s, rows);
     }
     if (tm) tm->sch_innersq += wall() - tq;
     if (type == KKT_TYPE_HOMOGENEOUS) {
@@ -742,7 +816,7 @@ hdsdp_retcode KKT::build(SdpCone &cone, int type) {
         gemm(s, n, n, n, 1.0, Wp, ld, 0, dev.T1, dev.ld, 0, 0.0, dev.T2, dev.ld, 0);
         symmetrize_avg(s, n, dev.T2, dev.ld);
         dev.inner_all(dev.T2, dev.ld, cone.d_vec);
-        add_host(asinvcs, cone.d_vec, h_buf, m, 1.0, s);
+        add_host(asinvcs, cone.d_vec, h_buf, cone.m, 1.0, s, rows);
         dCSinv += dev.c_inner(Wp, ld);
         dCSinvCSinv += dev.c_inner(dev.T2, dev.ld);
         if (r != 0.0) {
@@ -772,6 +846,7 @@ void KKT::add_bound(BoundCone &b, int type) {
     }
     if (type == KKT_TYPE_CORRECTOR) return;
     for (int i = 0; i < b.m; ++i) h_buf[i] = b.dlInv[i] * b.dlInv[i] + b.duInv[i] * b.duInv[i];
+    open_m();
     HB_CUDA(cudaMemcpyAsync(d_diag, h_buf, sizeof(double) * m, cudaMemcpyHostToDevice, s));
     add_diag_vec(s, m, M, ldm, d_diag);
     HB_CUDA(cudaStreamSynchronize(s));

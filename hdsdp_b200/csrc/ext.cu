@@ -33,11 +33,14 @@ int HDSDPGetIterLog(hdsdp *h, int maxLen, double *t, double *pObj, double *dObj,
 
 void HDSDPGetTimers(hdsdp *h, double out[23]) {
     const Timers &t = h->timers;
+    long reuse = 0;
+    for (const hb::ConeSlot &k : h->cones)
+        if (k.sdp) reuse += k.sdp->nFactorReuse;
     const double v[23] = {t.schur, t.schur_factor, t.schur_solve, t.s_factor, t.s_inverse, t.lanczos, t.assemble,
                           t.primal, t.total, (double) t.n_schur, (double) t.n_sfactor, (double) t.n_lanczos,
                           (double) t.n_lanczos_mv, (double) t.n_schur_solve, t.lz_inverse, t.lz_host, t.lz_wait,
                           t.sch_matrix, t.sch_inner, t.sch_innersq, t.setup, t.ipm_device,
-                          h->cone ? (double) h->cone->nFactorReuse : 0.0};
+                          (double) reuse};
     std::memcpy(out, v, sizeof(v));
 }
 

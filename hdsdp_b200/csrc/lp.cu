@@ -264,6 +264,7 @@ void KKT::add_lp(LpCone &lp, int type) {
         atx(lp.buf, asinvrd);
     }
     if (type == KKT_TYPE_CORRECTOR) return;
+    open_m();
     // M_ij += sum over column j of A_kj (A_ki / s_k^2), the value for column i kept per LP
     // column (the last of a repeated index wins, as in the reference's buffer)
     if (!lp.pairI.empty()) {

@@ -747,6 +747,8 @@ bool SdpDevice::split_inverse(const double *Kinv, double *W, long ldW) {
 
 void SdpDevice::inner_all(const double *Z, long ldZ, double *out, bool reuse_v) {
     cudaStream_t s = stream;
+    // rows with a zero coefficient (another cone's constraints) are written by no kernel
+    if (nsp + nr1s + nr1d + ndr < m) HB_CUDA(cudaMemsetAsync(out, 0, sizeof(double) * m, s));
     if (nsp > 0) inner_sp_kernel<<<hb::counted(grid1(nsp)), 256, 0, s>>>(nsp, sp_id, sp_ptr, sp_r, sp_c, sp_v, Z, ldZ, out);
     if (nr1s > 0)
         inner_r1s_kernel<<<hb::counted(grid1(nr1s)), 256, 0, s>>>(nr1s, r1s_id, r1s_ptr, r1s_p, r1s_a, r1s_sign, Z, ldZ, out);
@@ -764,6 +766,7 @@ void SdpDevice::inner_all(const double *Z, long ldZ, double *out, bool reuse_v) 
 
 void SdpDevice::inner_all_sq(const double *W, long ldW, double *out, bool reuse_v, bool reuse_vt) {
     cudaStream_t s = stream;
+    if (nsp + nr1s + nr1d + ndr < m) HB_CUDA(cudaMemsetAsync(out, 0, sizeof(double) * m, s));
     if (nsp > 0)
         innersq_sp_kernel<<<hb::counted((nsp * 32 + 255) / 256), 256, 0, s>>>(n, nsp, sp_id, sp_ptr, sp_r, sp_c, sp_v, W, ldW, out);
     if (nr1s > 0)

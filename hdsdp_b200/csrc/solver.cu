@@ -71,26 +71,35 @@ void default_params(hdsdp *h) {
 
 // ---------------------------------------------------------------- statistics / tuning
 void get_statistics(hdsdp *h) {
-    SdpCone &c = *h->cone;
-    const int sumDims = c.n + (h->lp ? h->lp->nCol : 0);
-    fi(h, N_MAXCONEDIM) = c.n;
+    int sumDims = 0, maxDim = 0, nDense = 0, nSparse = 0, nLp = 0;
+    // sums over the cones in the user's order, as the reference adds them
+    double objOne = 0.0, dataOne = 0.0, objFro2 = 0.0, dataFro2 = 0.0;
+    for (ConeSlot &k : h->cones) {
+        double of, df;
+        if (k.sdp) {
+            maxDim = std::max(maxDim, k.sdp->n);
+            sumDims += k.sdp->n;
+            objOne += k.sdp->obj_norm(ABS_NORM);
+            dataOne += k.sdp->coeff_norm(ABS_NORM);
+            of = k.sdp->obj_norm(FRO_NORM);
+            df = k.sdp->coeff_norm(FRO_NORM);
+            (k.sdp->sparse ? nSparse : nDense) += 1;
+        } else {
+            sumDims += k.lp->nCol;
+            objOne += k.lp->obj_norm(ABS_NORM);
+            dataOne += k.lp->coeff_norm(ABS_NORM);
+            of = k.lp->obj_norm(FRO_NORM);
+            df = k.lp->coeff_norm(FRO_NORM);
+            nLp += 1;
+        }
+        objFro2 += of * of;
+        dataFro2 += df * df;
+    }
+    fi(h, N_MAXCONEDIM) = maxDim;
     fi(h, N_SUMCONEDIMS) = sumDims;
     fi(h, N_ROWS) = h->nRows;
     fi(h, N_CONES) = h->nCones;
     h->allConeDims = (double) sumDims + 2.0 * h->nRows;
-    // sums over the cones (the SDP block, then the LP cone), as the reference adds them
-    double objOne = c.obj_norm(ABS_NORM);
-    double dataOne = c.coeff_norm(ABS_NORM);
-    double objFro2 = c.obj_norm(FRO_NORM), dataFro2 = c.coeff_norm(FRO_NORM);
-    objFro2 *= objFro2;
-    dataFro2 *= dataFro2;
-    if (h->lp) {
-        objOne += h->lp->obj_norm(ABS_NORM);
-        dataOne += h->lp->coeff_norm(ABS_NORM);
-        const double of = h->lp->obj_norm(FRO_NORM), df = h->lp->coeff_norm(FRO_NORM);
-        objFro2 += of * of;
-        dataFro2 += df * df;
-    }
     fd(h, D_OBJFRONORM) = std::sqrt(objFro2);
     fd(h, D_DATAFRONORM) = std::sqrt(dataFro2);
     fd(h, D_OBJONENORM) = objOne;
@@ -106,15 +115,37 @@ void get_statistics(hdsdp *h) {
     fd(h, D_RHSINFNORM) = inf;
     if (fd(h, D_OBJFRONORM) == 0.0) fi(h, I_NULLOBJ) = 1;
     if (h->nCones >= 100) fi(h, I_MANYCONES) = 1;
-    fi(h, N_DSSDPCONES) = 1;
-    fi(h, N_SPSDPCONES) = 0;
-    fi(h, N_LPCONES) = h->lp ? 1 : 0;
+    fi(h, N_DSSDPCONES) = nDense;
+    fi(h, N_SPSDPCONES) = nSparse;
+    fi(h, N_LPCONES) = nLp;
 }
 
+// HConeDetectFeature of one cone: the dense SDP cone's structure tests
+// (conic_sdp.c:2560-2654), only the coefficient counts for a sparse SDP cone
+// (conic_sdp.c:2656-2667), the LP cone's tests (conic_lp.c)
+void detect_feature_of(hdsdp *h, ConeSlot &k) {
+    if (k.lp) {
+        k.lp->detect_feature(h->HIntFeatures, h->HDblFeatures);
+    } else if (!k.sdp->sparse) {
+        k.sdp->detect_feature(h->rowRHS.data(), h->HIntFeatures, h->HDblFeatures);
+    } else {
+        const int *st = k.sdp->stats;
+        h->HIntFeatures[15] = st[REF_ZERO];
+        h->HIntFeatures[17] = st[REF_DENSE];
+        h->HIntFeatures[16] = st[REF_SPARSE];
+        h->HIntFeatures[18] = st[REF_SPR1];
+        h->HIntFeatures[19] = st[REF_DSR1];
+    }
+}
+
+// HDSDPIAdjustConeParams (interface/hdsdp.c:136-152): structure detection on the first
+// cone when there is one SDP cone, on the last cone when LP cones are present (fewer
+// than ten cones); primal refinement only with a single SDP cone
 void adjust_cone_params(hdsdp *h) {
-    SdpCone &c = *h->cone;
-    c.detect_feature(h->rowRHS.data(), h->HIntFeatures, h->HDblFeatures);
-    if (h->lp && fi(h, N_CONES) < 10) h->lp->detect_feature(h->HIntFeatures, h->HDblFeatures);
+    const bool oneCone = fi(h, N_DSSDPCONES) + fi(h, N_SPSDPCONES) <= 1;
+    if (!oneCone) ip(h, INT_PARAM_PSDP) = 0;
+    if (oneCone) detect_feature_of(h, h->cones[0]);
+    if (fi(h, N_LPCONES) && fi(h, N_CONES) < 10) detect_feature_of(h, h->cones[h->nCones - 1]);
     const int impTrace = fi(h, I_IMPTRACE), noPInt = fi(h, I_NOPINTERIOR), noDInt = fi(h, I_NODINTERIOR);
     const int dense = fi(h, I_VERYDENSE), impDual = fi(h, I_IMPYBOUND), noObj = fi(h, I_NULLOBJ);
     h->modelFeatures.clear();
@@ -206,8 +237,10 @@ void adjust_params(hdsdp *h) {
     else rhsScal = 1.0;
     fd(h, D_OBJSCALING) = objScal;
     fd(h, D_RHSSCALING) = rhsScal;
-    h->cone->scal(objScal);
-    if (h->lp) h->lp->scal(objScal);
+    for (ConeSlot &k : h->cones) {
+        if (k.sdp) k.sdp->scal(objScal);
+        else k.lp->scal(objScal);
+    }
     for (int i = 0; i < h->nRows; ++i) h->rowRHS[i] *= rhsScal;
     // thread count: the GPU build records the host default
     ip(h, INT_PARAM_THREADS) = std::min(ip(h, INT_PARAM_THREADS), 12);
@@ -315,45 +348,104 @@ void schur_precision(hdsdp *h) {
         const double gap = h->log.empty() ? HDSDP_INFINITY : std::fabs(h->log.back().gap);
         p = (std::isfinite(gap) && gap < 1e-3) ? 0 : 1;
     }
-    h->cone->dev.precision = p;
+    for (ConeSlot &k : h->cones)
+        if (k.sdp) k.sdp->dev.precision = p;
 }
 
-// ---- the cone list in the reference's order: the SDP block, then the LP cone when set
+// ---- the cones in the user's order (interface/hdsdp_algo.c: every loop over HCones)
 hdsdp_retcode cones_interior(hdsdp *h, double tau, const double *y, int *interior) {
-    hdsdp_retcode r = h->cone->interior_check(tau, y, interior);
-    if (r != HDSDP_RETCODE_OK || !*interior || !h->lp) return r;
-    *interior = h->lp->interior_check(tau, y);
+    *interior = 1;
+    for (ConeSlot &k : h->cones) {
+        if (k.sdp) {
+            hdsdp_retcode r = k.sdp->interior_check(tau, y, interior);
+            if (r != HDSDP_RETCODE_OK) return r;
+        } else {
+            *interior = k.lp->interior_check(tau, y);
+        }
+        if (!*interior) break;
+    }
     return HDSDP_RETCODE_OK;
 }
 
 hdsdp_retcode cones_interior_expert(hdsdp *h, double dC, double dAs, const double *y, double dEye, int which,
                                     int *interior) {
-    hdsdp_retcode r = h->cone->interior_check_expert(dC, dAs, y, dEye, which, interior);
-    if (r != HDSDP_RETCODE_OK || !*interior || !h->lp) return r;
-    *interior = h->lp->interior_check_expert(dC, dAs, y, dEye, which);
+    *interior = 1;
+    for (ConeSlot &k : h->cones) {
+        if (k.sdp) {
+            hdsdp_retcode r = k.sdp->interior_check_expert(dC, dAs, y, dEye, which, interior);
+            if (r != HDSDP_RETCODE_OK) return r;
+        } else {
+            *interior = k.lp->interior_check_expert(dC, dAs, y, dEye, which);
+        }
+        if (!*interior) break;
+    }
     return HDSDP_RETCODE_OK;
 }
 
 // running minimum of the cones' step bounds
 hdsdp_retcode cones_ratio(hdsdp *h, double dtau, const double *dy, double ada, int which, double *mx) {
-    double st = 0.0;
-    hdsdp_retcode r = h->cone->ratio_test(dtau, dy, ada, which, &st);
-    if (r != HDSDP_RETCODE_OK) return r;
-    *mx = std::min(*mx, st);
-    if (h->lp) *mx = std::min(*mx, h->lp->ratio_test(dtau, dy, ada, which));
+    for (ConeSlot &k : h->cones) {
+        double st = 0.0;
+        if (k.sdp) {
+            hdsdp_retcode r = k.sdp->ratio_test(dtau, dy, ada, which, &st);
+            if (r != HDSDP_RETCODE_OK) return r;
+        } else {
+            st = k.lp->ratio_test(dtau, dy, ada, which);
+        }
+        *mx = std::min(*mx, st);
+    }
     return HDSDP_RETCODE_OK;
 }
 
 hdsdp_retcode cones_add_step(hdsdp *h, double step, int which, int *interior) {
-    hdsdp_retcode r = h->cone->add_step_and_check(step, which, interior);
-    if (r != HDSDP_RETCODE_OK || !*interior || !h->lp) return r;
-    *interior = h->lp->add_step_and_check(step, which);
+    *interior = 1;
+    for (ConeSlot &k : h->cones) {
+        if (k.sdp) {
+            hdsdp_retcode r = k.sdp->add_step_and_check(step, which, interior);
+            if (r != HDSDP_RETCODE_OK) return r;
+        } else {
+            *interior = k.lp->add_step_and_check(step, which);
+        }
+        if (!*interior) break;
+    }
     return HDSDP_RETCODE_OK;
 }
 
 void cones_set_start(hdsdp *h, double r) {
-    h->cone->set_start(r);
-    if (h->lp) h->lp->set_start(r);
+    for (ConeSlot &k : h->cones) {
+        if (k.sdp) k.sdp->set_start(r);
+        else k.lp->set_start(r);
+    }
+}
+
+// sum of the cones' log det (SDP) or sum log s (LP) at the buffer `which`
+hdsdp_retcode cones_barrier(hdsdp *h, double tau, const double *y, int which, double *sum) {
+    *sum = 0.0;
+    for (ConeSlot &k : h->cones) {
+        if (k.sdp) {
+            double ld = 0.0;
+            hdsdp_retcode r = k.sdp->get_barrier(tau, y, which, &ld);
+            if (r != HDSDP_RETCODE_OK) return r;
+            *sum += ld;
+        } else {
+            *sum += k.lp->get_barrier(tau, y, which);
+        }
+    }
+    return HDSDP_RETCODE_OK;
+}
+
+// HKKTBuildUp (interface/hdsdp_schur.c:256-268): clean, then every cone in order
+hdsdp_retcode build_kkt(hdsdp *h, int type) {
+    h->kkt.clean(type);
+    for (ConeSlot &k : h->cones) {
+        if (k.sdp) {
+            hdsdp_retcode r = h->kkt.add_sdp(*k.sdp, type);
+            if (r != HDSDP_RETCODE_OK) return r;
+        } else {
+            h->kkt.add_lp(*k.lp, type);
+        }
+    }
+    return HDSDP_RETCODE_OK;
 }
 
 hdsdp_retcode check_interior(hdsdp *h, double tau, const double *y, int *interior) {
@@ -373,10 +465,9 @@ int is_interior(hdsdp *h, const double *y) {
 
 hdsdp_retcode get_log_barrier(hdsdp *h, double tau, const double *y, int which, double *val) {
     double ld = 0.0, bv = 0.0;
-    hdsdp_retcode r = h->cone->get_barrier(tau, y, which, &ld);
+    hdsdp_retcode r = cones_barrier(h, tau, y, which, &ld);
     if (r != HDSDP_RETCODE_OK) return r;
     bv -= ld;
-    if (h->lp) bv -= h->lp->get_barrier(tau, y, which);
     if (h->whichMethod != METHOD_HSD) {
         r = h->bnd.get_barrier(tau, y, which, &ld);
         if (r != HDSDP_RETCODE_OK) return r;
@@ -387,8 +478,10 @@ hdsdp_retcode get_log_barrier(hdsdp *h, double tau, const double *y, int which, 
 }
 
 void set_residual(hdsdp *h, double r) {
-    h->cone->reduce_resi(r);
-    if (h->lp) h->lp->reduce_resi(r);
+    for (ConeSlot &k : h->cones) {
+        if (k.sdp) k.sdp->reduce_resi(r);
+        else k.lp->reduce_resi(r);
+    }
 }
 
 hdsdp_retcode kkt_solve(hdsdp *h, std::vector<double> &rhs, std::vector<double> *lhs) {
@@ -469,8 +562,7 @@ hdsdp_retcode phaseA_hsd(hdsdp *h, int dOnly) {
             goto exit_cleanup;
         }
         schur_precision(h);
-        CALL(h->kkt.build(*h->cone, KKT_TYPE_HOMOGENEOUS));
-        if (h->lp) h->kkt.add_lp(*h->lp, KKT_TYPE_HOMOGENEOUS);
+        CALL(build_kkt(h, KKT_TYPE_HOMOGENEOUS));
         h->kkt.regularize(0.0);
         h->d2 = h->kkt.asinv;
         h->d3 = h->kkt.asinvrd;
@@ -644,8 +736,7 @@ hdsdp_retcode infeasible_corrector(hdsdp *h) {
     CALL(get_log_barrier(h, 0.0, nullptr, BUFFER_DUALVAR, &barrier));
     for (int nCorr = 0; nCorr < nMaxCorr; ++nCorr) {
         if (!h->resi) break;
-        CALL(h->kkt.build(*h->cone, KKT_TYPE_CORRECTOR));
-        if (h->lp) h->kkt.add_lp(*h->lp, KKT_TYPE_CORRECTOR);
+        CALL(build_kkt(h, KKT_TYPE_CORRECTOR));
         h->kkt.add_bound(h->bnd, KKT_TYPE_CORRECTOR);
         h->d2 = h->kkt.asinv;
         h->d3 = h->kkt.asinvrd;
@@ -744,8 +835,7 @@ hdsdp_retcode phaseA_infeasible(hdsdp *h, int dOnly) {
             }
         }
         schur_precision(h);
-        CALL(h->kkt.build(*h->cone, KKT_TYPE_INFEASIBLE));
-        if (h->lp) h->kkt.add_lp(*h->lp, KKT_TYPE_INFEASIBLE);
+        CALL(build_kkt(h, KKT_TYPE_INFEASIBLE));
         h->kkt.add_bound(h->bnd, KKT_TYPE_INFEASIBLE);
         h->d2 = h->kkt.asinv;
         h->d3 = h->kkt.asinvrd;
@@ -867,9 +957,8 @@ void feasible_build_step(hdsdp *h) {
 
 double get_potential(hdsdp *h, double rho, const double *y, int which) {
     double pot = 0.0, obj = 0.0, ld = 0.0;
-    h->cone->get_barrier(0.0, nullptr, which, &ld);
+    cones_barrier(h, 0.0, nullptr, which, &ld);
     pot -= ld;
-    if (h->lp) pot -= h->lp->get_barrier(0.0, nullptr, which);
     h->bnd.get_barrier(0.0, nullptr, which, &ld);
     pot -= ld;
     for (int i = 0; i < h->nRows; ++i) obj += h->rowRHS[i] * y[i];
@@ -918,9 +1007,8 @@ exit_cleanup:
 
 double get_barrier_val(hdsdp *h, const double *y, int which) {
     double bv = 0.0, obj = 0.0, ld = 0.0;
-    h->cone->get_barrier(0.0, nullptr, which, &ld);
+    cones_barrier(h, 0.0, nullptr, which, &ld);
     bv += ld;
-    if (h->lp) bv += h->lp->get_barrier(0.0, nullptr, which);
     h->bnd.get_barrier(0.0, nullptr, which, &ld);
     bv += ld;
     for (int i = 0; i < h->nRows; ++i) obj += h->rowRHS[i] * y[i];
@@ -951,8 +1039,7 @@ hdsdp_retcode feasible_corrector(hdsdp *h) {
     for (int i = 0; i < h->nRows; ++i) bDotD1 += h->d1[i] * h->rowRHS[i];
     for (int nCorr = 0; nCorr < nMaxCorr; ++nCorr) {
         if (h->mu < 1e-05) break;
-        CALL(h->kkt.build(*h->cone, KKT_TYPE_CORRECTOR));
-        if (h->lp) h->kkt.add_lp(*h->lp, KKT_TYPE_CORRECTOR);
+        CALL(build_kkt(h, KKT_TYPE_CORRECTOR));
         h->kkt.add_bound(h->bnd, KKT_TYPE_CORRECTOR);
         h->d2 = h->kkt.asinv;
         CALL(kkt_solve(h, h->d2, nullptr));
@@ -1044,8 +1131,10 @@ hdsdp_retcode phaseB_potential(hdsdp *h) {
     h->perturb = -10.0 * h->resi;
     h->resi = 0.0;
     set_residual(h, 0.0);
-    h->cone->set_perturb(h->perturb);
-    if (h->lp) h->lp->set_perturb(h->perturb);
+    for (ConeSlot &k : h->cones) {
+        if (k.sdp) k.sdp->set_perturb(h->perturb);
+        else k.lp->set_perturb(h->perturb);
+    }
     if (h->perturb != 0.0) is_interior(h, h->y.data());
     pObjStart = h->pObjInternal;
     if (h->verbose) printf("HDSDP re-starts. Using feasible dual method \n\n");
@@ -1053,8 +1142,7 @@ hdsdp_retcode phaseB_potential(hdsdp *h) {
         nIterInternal += 1;
         if (nIterInternal > 10) force = 0;
         schur_precision(h);
-        CALL(h->kkt.build(*h->cone, KKT_TYPE_INFEASIBLE));
-        if (h->lp) h->kkt.add_lp(*h->lp, KKT_TYPE_INFEASIBLE);
+        CALL(build_kkt(h, KKT_TYPE_INFEASIBLE));
         h->kkt.add_bound(h->bnd, KKT_TYPE_INFEASIBLE);
         if (h->mu > 1.0) h->kkt.regularize(1e-06);
         h->d2 = h->kkt.asinv;
@@ -1114,29 +1202,35 @@ exit_cleanup:
 }
 
 // ---------------------------------------------------------------- primal values
-void cone_values(hdsdp *h, double *X, double *S) {
-    double mu = h->accMu;
-    const std::vector<double> *y = &h->accY, *dy = &h->accDy;
+// The primal marker (mu, y, dy) of HDSDPGetConeValues (interface/hdsdp.c:711-745): the
+// accurate one when it exists, else the inaccurate one.
+void primal_marker(hdsdp *h, double &mu, const std::vector<double> *&y, const std::vector<double> *&dy) {
+    mu = h->accMu;
+    y = &h->accY;
+    dy = &h->accDy;
     if (mu <= 0.0) {
         mu = h->inaccMu;
         y = &h->inaccY;
         dy = &h->inaccDy;
     }
-    if (X) h->cone->get_primal(mu, y->data(), dy->data(), X);
-    if (S) h->cone->get_dual(S);
 }
 
-// x and s of the LP cone at the same primal marker (host vectors of its dimension)
-void lp_values(hdsdp *h, double *x, double *sl) {
-    double mu = h->accMu;
-    const std::vector<double> *y = &h->accY, *dy = &h->accDy;
-    if (mu <= 0.0) {
-        mu = h->inaccMu;
-        y = &h->inaccY;
-        dy = &h->inaccDy;
-    }
-    if (x) h->lp->get_primal(mu, y->data(), dy->data(), x);
-    if (sl) h->lp->get_dual(sl);
+// X and S of an SDP cone (device, leading dimension c.ld)
+void sdp_values(hdsdp *h, SdpCone &c, double *X, double *S) {
+    double mu;
+    const std::vector<double> *y, *dy;
+    primal_marker(h, mu, y, dy);
+    if (X) c.get_primal(mu, y->data(), dy->data(), X);
+    if (S) c.get_dual(S);
+}
+
+// x and s of an LP cone (host vectors of its dimension)
+void lp_values(hdsdp *h, LpCone &lp, double *x, double *sl) {
+    double mu;
+    const std::vector<double> *y, *dy;
+    primal_marker(h, mu, y, dy);
+    if (x) lp.get_primal(mu, y->data(), dy->data(), x);
+    if (sl) lp.get_dual(sl);
 }
 
 // ---------------------------------------------------------------- primal refinement
@@ -1153,17 +1247,19 @@ hdsdp_retcode run_psdp(hdsdp *h) {
     double mu = h->mu;
     const double relOpt = dp(h, DBL_PARAM_RELOPTTOL), absOpt = dp(h, DBL_PARAM_ABSOPTTOL);
     const double pdScal = fd(h, D_OBJSCALING) * fd(h, D_RHSSCALING);
-    if (h->nCones > 1 || h->dInfeas > 0.0) return HDSDP_RETCODE_FAILED;
+    // HPSDPInit (interface/hdsdp_psdp.c:81-90): one dense SDP cone, dual feasible
+    if (h->nCones > 1 || h->dInfeas > 0.0 || h->cones[0].type != HDSDP_CONETYPE_DENSE_SDP) return HDSDP_RETCODE_FAILED;
     for (double **p : {&X, &X0, &S, &XStep, &Buf}) HB_CUDA(hb::cmalloc(p, sizeof(double) * ld * n));
     XF.alloc(n);
     lzp.init(n, s);
-    cone_values(h, X, nullptr);
+    sdp_values(h, c, X, nullptr);
     HB_CUDA(cudaMemcpyAsync(X0, X, sizeof(double) * ld * n, cudaMemcpyDeviceToDevice, s));
     h->kkt.primalX = X;
     if (h->verbose) printf("Primal solver is initialized. \n");
     CALL(h->kkt.build(c, KKT_TYPE_PRIMAL));
     CALL(h->kkt.factorize());
     for (int it = 0; it < 5; ++it) {
+        std::fill(pinf.begin(), pinf.end(), 0.0);
         c.atimesx(X, pinf.data());
         double pinfNorm = 0.0;
         for (int i = 0; i < m; ++i) {
@@ -1176,6 +1272,7 @@ hdsdp_retcode run_psdp(hdsdp *h) {
         gemm(s, n, n, n, 1.0, S, ld, 0, X, ld, 0, 0.0, XStep, ld, 0);
         gemm(s, n, n, n, 1.0, X, ld, 0, XStep, ld, 0, 0.0, Buf, ld, 0);
         symmetrize_avg(s, n, Buf, ld);
+        std::fill(rhs.begin(), rhs.end(), 0.0);
         c.atimesx(Buf, rhs.data());
         for (int i = 0; i < m; ++i) rhs[i] -= mu * pinf[i];
         CALL(h->kkt.solve(rhs.data(), h->dy.data()));
@@ -1258,8 +1355,7 @@ exit_cleanup:
 
 // Smallest eigenvalue sign test of X: Cholesky succeeds -> lambda_min > 0; otherwise the
 // most negative eigenvalue is bracketed by bisection on X + sigma I.
-double min_eig_estimate(hdsdp *h, double *X) {
-    SdpCone &c = *h->cone;
+double min_eig_estimate(SdpCone &c, double *X) {
     DenseFactor &F = c.Fcheck;
     c.invalidate_check_factor();
     if (factorize(c.s, F, X, c.ld)) return 1.0;
@@ -1280,6 +1376,23 @@ double min_eig_estimate(hdsdp *h, double *X) {
         else lo = mid;
     }
     return -0.5 * (lo + hi);
+}
+
+// free the cones' device and host data (the user data stays set)
+void release_cones(hdsdp *h) {
+    for (ConeSlot &k : h->cones) {
+        if (k.sdp) {
+            k.sdp->release();
+            delete k.sdp;
+            k.sdp = nullptr;
+        }
+        if (k.lp) {
+            k.lp->release();
+            delete k.lp;
+            k.lp = nullptr;
+        }
+    }
+    h->cone = nullptr;
 }
 
 }  // namespace
@@ -1353,8 +1466,11 @@ hdsdp_retcode HDSDPCreate(hdsdp **pHSolver) {
 }
 
 hdsdp_retcode HDSDPInit(hdsdp *h, int nRows, int nCones) {
+    if (nRows < 1 || nCones < 1) return HDSDP_RETCODE_FAILED;
+    release_cones(h);
     h->nRows = nRows;
     h->nCones = nCones;
+    h->cones.assign(nCones, ConeSlot());
     default_params(h);
     h->rowRHS.assign(nRows, 0.0);
     for (auto *v : {&h->y, &h->dy, &h->d1, &h->d2, &h->d3, &h->d4, &h->aux1, &h->aux2, &h->pInfUp, &h->pInfLow,
@@ -1370,21 +1486,16 @@ hdsdp_retcode HDSDPInit(hdsdp *h, int nRows, int nCones) {
 
 hdsdp_retcode HDSDPSetCone(hdsdp *h, int iCone, void *userCone) {
     user_data *u = (user_data *) userCone;
-    // one dense SDP block, optionally followed by one LP cone (the reference's own
-    // drivers put the LP cone last)
-    if (h->nCones == 2 && iCone == 1 && u && HUserDataChooseCone(u) == HDSDP_CONETYPE_LP) {
-        h->usrLp = u;
-        return HDSDP_RETCODE_OK;
-    }
-    if (iCone != 0 || h->nCones < 1 || h->nCones > 2) {
-        fprintf(stderr, "[hdsdp_b200] supported: one dense SDP block (cone 0) and optionally one LP cone (cone 1)\n");
+    if (!u || iCone < 0 || iCone >= h->nCones || (int) h->cones.size() != h->nCones) return HDSDP_RETCODE_FAILED;
+    // HConeSetData (interface/hdsdp_conic.c:50-60) takes the type HUserDataChooseCone picks
+    const cone_type t = HUserDataChooseCone(u);
+    if (t != HDSDP_CONETYPE_DENSE_SDP && t != HDSDP_CONETYPE_SPARSE_SDP && t != HDSDP_CONETYPE_LP) {
+        fprintf(stderr, "[hdsdp_b200] cone %d: type %d is not supported (SDP blocks and LP cones are)\n", iCone,
+                (int) t);
         return HDSDP_RETCODE_FAILED;
     }
-    if (HUserDataChooseCone(u) != HDSDP_CONETYPE_DENSE_SDP) {
-        fprintf(stderr, "[hdsdp_b200] the block is not a dense SDP cone\n");
-        return HDSDP_RETCODE_FAILED;
-    }
-    h->usr = u;
+    h->cones[iCone].usr = u;
+    h->cones[iCone].type = t;
     return HDSDP_RETCODE_OK;
 }
 
@@ -1408,41 +1519,46 @@ hdsdp_retcode HDSDPCheckSolution(hdsdp *h, double dErrs[6]) {
         h->HStatus = HDSDP_NUMERICAL;
         return HDSDP_RETCODE_OK;
     }
-    SdpCone &c = *h->cone;
-    const int n = c.n, m = h->nRows;
-    const long ld = c.ld;
+    const int m = h->nRows;
     double dualInfeas = h->perturb * std::sqrt((double) fi(h, N_SUMCONEDIMS));
-    double primalObj = 0.0, dualObj = 0.0;
+    double primalObj = 0.0, dualObj = 0.0, compl_ = 0.0, minEig = HDSDP_INFINITY;
     const double pScal = fd(h, D_RHSSCALING), dScal = fd(h, D_OBJSCALING);
-    double *X = nullptr, *S = nullptr;
-    HB_CUDA(hb::cmalloc(&X, sizeof(double) * ld * n));
-    HB_CUDA(hb::cmalloc(&S, sizeof(double) * ld * n));
-    HB_CUDA(cudaMemsetAsync(X, 0, sizeof(double) * ld * n, c.s));
     for (int i = 0; i < m; ++i) dualObj += h->rowRHS[i] * h->y[i];
-    cone_values(h, X, S);
-    std::vector<double> ax(m);
-    c.atimesx(X, ax.data());
-    frob_dot(c.s, n, X, ld, S, ld, c.d_scal);
-    HB_CUDA(cudaMemcpyAsync(c.h_scal, c.d_scal, sizeof(double), cudaMemcpyDeviceToHost, c.s));
-    HB_CUDA(cudaStreamSynchronize(c.s));
-    double compl_ = c.h_scal[0];
-    primalObj = c.trace_cx(X);
-    double minEig = min_eig_estimate(h, X);
-    if (h->lp) {
-        // the LP cone: A x into the residual, x . s, c . x, and min x in place of lambda_min
-        std::vector<double> xl(h->lp->nCol, 0.0), sl(h->lp->nCol, 0.0);
-        lp_values(h, xl.data(), sl.data());
-        h->lp->atimesx(xl.data(), ax.data());
-        double d = 0.0;
-        for (int k = 0; k < h->lp->nCol; ++k) d += xl[k] * sl[k];
-        compl_ += d;
-        primalObj += h->lp->trace_cx(xl.data());
-        double mn = HDSDP_INFINITY;
-        for (double v : xl) mn = std::min(mn, v);
-        minEig = std::min(minEig, mn);
+    std::vector<double> ax(m, 0.0);
+    // per cone: A X into the residual, <X, S>, <C, X>, and lambda_min(X) (min x for an LP cone)
+    for (ConeSlot &k : h->cones) {
+        if (k.sdp) {
+            SdpCone &c = *k.sdp;
+            const int n = c.n;
+            const long ld = c.ld;
+            double *X = nullptr, *S = nullptr;
+            HB_CUDA(hb::cmalloc(&X, sizeof(double) * ld * n));
+            HB_CUDA(hb::cmalloc(&S, sizeof(double) * ld * n));
+            HB_CUDA(cudaMemsetAsync(X, 0, sizeof(double) * ld * n, c.s));
+            sdp_values(h, c, X, S);
+            c.atimesx(X, ax.data());
+            frob_dot(c.s, n, X, ld, S, ld, c.d_scal);
+            HB_CUDA(cudaMemcpyAsync(c.h_scal, c.d_scal, sizeof(double), cudaMemcpyDeviceToHost, c.s));
+            HB_CUDA(cudaStreamSynchronize(c.s));
+            compl_ += c.h_scal[0];
+            primalObj += c.trace_cx(X);
+            minEig = std::min(minEig, min_eig_estimate(c, X));
+            hb::cache_free(X);
+            hb::cache_free(S);
+        } else {
+            LpCone &lp = *k.lp;
+            std::vector<double> xl(lp.nCol, 0.0), sl(lp.nCol, 0.0);
+            lp_values(h, lp, xl.data(), sl.data());
+            lp.atimesx(xl.data(), ax.data());
+            double d = 0.0;
+            for (int q = 0; q < lp.nCol; ++q) d += xl[q] * sl[q];
+            compl_ += d;
+            primalObj += lp.trace_cx(xl.data());
+            double mn = HDSDP_INFINITY;
+            for (double v : xl) mn = std::min(mn, v);
+            minEig = std::min(minEig, mn);
+        }
     }
-    hb::cache_free(X);
-    hb::cache_free(S);
     dualObj /= (pScal * dScal);
     primalObj /= (pScal * dScal);
     double pinf = 0.0;
@@ -1482,44 +1598,65 @@ hdsdp_retcode HDSDPOptimize(hdsdp *h, int dOptOnly) {
     h->timers = Timers();
     h->log.clear();
     adjoint_release(h->adj);
-    if (!h->usr) return HDSDP_RETCODE_FAILED;
-    if (h->nCones == 2 && !h->usrLp) return HDSDP_RETCODE_FAILED;
-    if (h->cone) {
-        h->cone->release();
-        delete h->cone;
-        h->kkt.release();
+    {
+        // every cone set, at least one of them an SDP block
+        int nSdp = 0;
+        if ((int) h->cones.size() != h->nCones) return HDSDP_RETCODE_FAILED;
+        for (ConeSlot &k : h->cones) {
+            if (!k.usr) return HDSDP_RETCODE_FAILED;
+            if (k.type != HDSDP_CONETYPE_LP) nSdp += 1;
+        }
+        if (nSdp == 0) {
+            fprintf(stderr, "[hdsdp_b200] the problem has no SDP cone\n");
+            return HDSDP_RETCODE_FAILED;
+        }
     }
-    if (h->lp) {
-        h->lp->release();
-        delete h->lp;
-        h->lp = nullptr;
-    }
-    h->cone = new SdpCone();
-    h->cone->precision = h->precision;
-    user_data *u = h->usr;
+    release_cones(h);
+    h->kkt.release();
     tp0 = wall();
-    CALL(h->cone->proc_data(u->nConicRow, u->nConicCol, u->coneMatBeg, u->coneMatIdx, u->coneMatElem));
-    tp1 = wall();
-    CALL(h->cone->presolve());
-    if (h->nCones == 2) {
-        user_data *ul = h->usrLp;
-        if (ul->nConicRow != h->nRows) {
+    // HConeProcData + HConePresolveData per cone in order (interface/hdsdp.c:630-633)
+    for (ConeSlot &k : h->cones) {
+        const user_data *u = k.usr;
+        if (u->nConicRow != h->nRows) {
             retcode = HDSDP_RETCODE_FAILED;
             goto exit_cleanup;
         }
-        h->lp = new LpCone();
-        CALL(h->lp->proc_data(ul->nConicRow, ul->nConicCol, ul->coneMatBeg, ul->coneMatIdx, ul->coneMatElem,
-                              h->stream));
+        if (k.type == HDSDP_CONETYPE_LP) {
+            k.lp = new LpCone();
+            CALL(k.lp->proc_data(u->nConicRow, u->nConicCol, u->coneMatBeg, u->coneMatIdx, u->coneMatElem, h->stream));
+        } else {
+            k.sdp = new SdpCone();
+            k.sdp->precision = h->precision;
+            CALL(k.sdp->proc_data(u->nConicRow, u->nConicCol, u->coneMatBeg, u->coneMatIdx, u->coneMatElem,
+                                  k.type == HDSDP_CONETYPE_SPARSE_SDP));
+            if (k.sdp->m == 0) {
+                fprintf(stderr, "[hdsdp_b200] an SDP block has no constraint\n");
+                retcode = HDSDP_RETCODE_FAILED;
+                goto exit_cleanup;
+            }
+            tp1 = wall();
+            CALL(k.sdp->presolve());
+            tp2 += wall() - tp1;
+            if (!h->cone) h->cone = k.sdp;
+        }
     }
-    tp2 = wall();
+    tp1 = wall();
     get_statistics(h);
     adjust_params(h);
     h->bnd.proc(h->nRows, dp(h, DBL_PARAM_DUALBOX_LOW), dp(h, DBL_PARAM_DUALBOX_UP));
-    CALL(h->cone->setup_device(h->stream, &h->timers));
-    if (h->verbose)
-        printf("  set-up: data %.3f s, rank-one detection %.3f s, device upload %.3f s (coefficients %.3f s, "
+    for (ConeSlot &k : h->cones)
+        if (k.sdp) CALL(k.sdp->setup_device(h->stream, &h->timers));
+    if (h->verbose) {
+        double up = 0.0, upMap = 0.0;
+        for (ConeSlot &k : h->cones)
+            if (k.sdp) {
+                up += k.sdp->dev.t_upload_total;
+                upMap += k.sdp->dev.t_upload_map;
+            }
+        printf("  set-up: data %.3f s (rank-one detection %.3f s), device upload %.3f s (coefficients %.3f s, "
                "of which gather map %.3f s)\n",
-               tp1 - tp0, tp2 - tp1, wall() - tp2, h->cone->dev.t_upload_total, h->cone->dev.t_upload_map);
+               tp1 - tp0, tp2, wall() - tp1, up, upMap);
+    }
     h->kkt.init(h->nRows, h->stream, &h->timers);
     if (device_error_flag()) {
         retcode = HDSDP_RETCODE_MEMORY;
@@ -1566,12 +1703,14 @@ hdsdp_retcode HDSDPGetRowDual(hdsdp *h, double *pObjVal, double *dObjVal, double
 
 void HDSDPGetConeValues(hdsdp *h, int iCone, double *conePrimal, double *coneDual, double *coneAuxi) {
     (void) coneAuxi;
-    if (iCone == 1 && h->lp) {
-        lp_values(h, conePrimal, coneDual);  // x and s of the LP cone
+    if (!h || iCone < 0 || iCone >= (int) h->cones.size()) return;
+    ConeSlot &k = h->cones[iCone];
+    if (k.lp) {
+        lp_values(h, *k.lp, conePrimal, coneDual);  // x and s of the LP cone
         return;
     }
-    if (iCone != 0 || !h->cone) return;
-    SdpCone &c = *h->cone;
+    if (!k.sdp) return;
+    SdpCone &c = *k.sdp;
     const int n = c.n;
     const long ld = c.ld;
     double *X = nullptr, *S = nullptr;
@@ -1581,7 +1720,7 @@ void HDSDPGetConeValues(hdsdp *h, int iCone, double *conePrimal, double *coneDua
         HB_CUDA(cudaMemcpy2DAsync(X, sizeof(double) * ld, conePrimal, sizeof(double) * n, sizeof(double) * n, n,
                                   cudaMemcpyHostToDevice, c.s));
     }
-    cone_values(h, X, S);
+    sdp_values(h, c, X, S);
     if (X)
         HB_CUDA(cudaMemcpy2DAsync(conePrimal, sizeof(double) * n, X, sizeof(double) * ld, sizeof(double) * n, n,
                                   cudaMemcpyDeviceToHost, c.s));
@@ -1596,17 +1735,8 @@ void HDSDPGetConeValues(hdsdp *h, int iCone, double *conePrimal, double *coneDua
 void HDSDPClear(hdsdp *h) {
     if (!h) return;
     adjoint_release(h->adj);
-    if (h->cone) {
-        h->cone->release();
-        delete h->cone;
-        h->cone = nullptr;
-    }
+    release_cones(h);
     h->kkt.release();
-    if (h->lp) {
-        h->lp->release();
-        delete h->lp;
-        h->lp = nullptr;
-    }
 }
 
 void HDSDPDestroy(hdsdp **pHSolver) {
@@ -1625,7 +1755,9 @@ namespace hb {
 int solver_status(hdsdp *h) { return (int) h->HStatus; }
 int solver_iters(hdsdp *h) { return h->nIterCount; }
 void solver_set_psdp(hdsdp *h, int on) { h->HIntParams[INT_PARAM_PSDP] = on; }
-void solver_cone_values(hdsdp *h, double *X, double *S) { cone_values(h, X, S); }
+void solver_cone_values(hdsdp *h, double *X, double *S) {
+    if (h->cone) sdp_values(h, *h->cone, X, S);
+}
 double solver_obj_scal(hdsdp *h) { return fd(h, D_OBJSCALING); }
 double solver_rhs_scal(hdsdp *h) { return fd(h, D_RHSSCALING); }
 }  // namespace hb

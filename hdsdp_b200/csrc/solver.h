@@ -73,9 +73,18 @@ struct SlackSig {
     }
 };
 
-// Dense SDP cone on the device (interface/hdsdp_conic_sdp.c dense half).
+// SDP cone on the device (interface/hdsdp_conic_sdp.c). A dense cone holds every
+// constraint of the problem; a sparse cone (at most 30% of the constraints have a
+// coefficient in the block, interface/hdsdp_user_data.c:73-86) holds only those,
+// listed in `rows`, and works on that subset: m is then the number of rows it holds,
+// its m-vectors are gathered from and scattered into the problem's by `rows`.
 struct SdpCone {
     int n = 0, m = 0;
+    int mAll = 0;                // constraints of the problem
+    bool sparse = false;
+    std::vector<int> rows;       // sparse cone: problem row of each local row (increasing)
+    int *d_rows = nullptr;       // device copy of rows
+    std::vector<double> ybuf;    // gathered coefficient vector
     long ld = 0;
     cudaStream_t s = nullptr;
     SdpDevice dev;
@@ -104,8 +113,11 @@ struct SdpCone {
     Timers *tm = nullptr;
     int precision = 0;
 
-    hdsdp_retcode proc_data(int nRow, int nCol, const int *Ap, const int *Ai, const double *Ax);
+    hdsdp_retcode proc_data(int nRow, int nCol, const int *Ap, const int *Ai, const double *Ax,
+                            bool sparseCone = false);
     hdsdp_retcode presolve();
+    // problem m-vector -> the cone's rows (the input itself for a dense cone)
+    const double *local(const double *v);
     hdsdp_retcode setup_device(cudaStream_t stream, Timers *t);
     void release();
 
@@ -126,7 +138,7 @@ struct SdpCone {
     hdsdp_retcode add_step_and_check(double step, int which, int *interior);
     void get_primal(double mu, const double *y, const double *dy, double *X);   // device X (ld)
     void get_dual(double *S);                                                  // device S (ld)
-    void atimesx(const double *X, double *out);                                // host out (m), overwritten
+    void atimesx(const double *X, double *out);                                // host out (problem m), accumulated
     double trace_cx(const double *X);
 };
 
@@ -201,10 +213,20 @@ struct KKT {
     double shift = 0.0;               // diagonal shift applied if the Cholesky of M failed
     const double *primalX = nullptr;  // device X for KKT_TYPE_PRIMAL
     Timers *tm = nullptr;
+    // M holds a partial sum of the current build (false after clean: the first dense SDP
+    // cone writes M outright, any other contribution zeroes it first)
+    bool mOpen = false;
+    double *Msub = nullptr;           // Schur block of a cone added into M (sparse or not first)
+    size_t msubCap = 0;
     void init(int m_, cudaStream_t stream, Timers *t);
     void release();
     void clean(int type);
-    hdsdp_retcode build(SdpCone &cone, int type);
+    void open_m();
+    hdsdp_retcode add_sdp(SdpCone &cone, int type);
+    hdsdp_retcode build(SdpCone &cone, int type) {  // a build with this single cone
+        clean(type);
+        return add_sdp(cone, type);
+    }
     void add_lp(LpCone &lp, int type);
     void add_bound(BoundCone &b, int type);
     void regularize(double reg);
@@ -223,14 +245,23 @@ struct IterRecord {
 
 }  // namespace hb
 
+namespace hb {
+// One cone of the problem in the user's order (interface/hdsdp.c:571-578): an SDP
+// block (dense or sparse cone) or an LP cone.
+struct ConeSlot {
+    user_data *usr = nullptr;
+    cone_type type = HDSDP_CONETYPE_UNKNOWN;
+    SdpCone *sdp = nullptr;
+    LpCone *lp = nullptr;
+};
+}  // namespace hb
+
 struct hdsdp_solver_internal {
     int nRows = 0;
     int nCones = 0;
     std::vector<double> rowRHS;
-    hb::SdpCone *cone = nullptr;
-    user_data *usr = nullptr;
-    hb::LpCone *lp = nullptr;      // optional LP cone (the last cone, as in the reference's drivers)
-    user_data *usrLp = nullptr;
+    std::vector<hb::ConeSlot> cones;
+    hb::SdpCone *cone = nullptr;   // the first SDP cone (the only one for primal refinement and the adjoint)
     hb::BoundCone bnd;
     hb::KKT kkt;
     cudaStream_t stream = nullptr;

@@ -241,6 +241,153 @@ def lp_block(m: int, n_lp: int, per_col: int = 2, seed: int = 7):
     return n_lp, np.asarray(Ap, np.int32), np.asarray(Ai, np.int32), np.asarray(Ax, np.float64)
 
 
+@dataclass
+class ConicProblem:
+    """Several cones sharing one set of m constraints, in the user layout: ``cones`` lists
+    (kind, dim, Ap, Ai, Ax) with kind "sdp" (a block of order dim, packed lower-triangle
+    rows) or "lp" (dim columns), each a CSC matrix with m + 1 columns, column 0 the cone's
+    objective. The problem is  min sum_k <C_k, X_k>  s.t.  sum_k <A_ik, X_k> = b_i."""
+
+    name: str
+    m: int
+    b: np.ndarray
+    cones: list
+    meta: dict = field(default_factory=dict)
+
+    def sdp_block(self, k: int) -> SDPInstance:
+        """Cone k (an SDP block) as an SDPInstance with this problem's right-hand side."""
+        kind, n, Ap, Ai, Ax = self.cones[k]
+        assert kind == "sdp"
+        return SDPInstance("%s[%d]" % (self.name, k), n, self.m, Ap, Ai, Ax, self.b)
+
+
+def _csc_columns(m, cols):
+    """CSC arrays from per-column (rows, values) lists (None = empty column), rows sorted."""
+    Ap, Ai, Ax = [0], [], []
+    for c in cols:
+        if c is not None:
+            idx = np.asarray(c[0], dtype=np.int64)
+            val = np.asarray(c[1], dtype=np.float64)
+            o = np.argsort(idx, kind="stable")
+            Ai.extend(idx[o].tolist())
+            Ax.extend(val[o].tolist())
+        Ap.append(len(Ai))
+    return np.asarray(Ap, np.int32), np.asarray(Ai, np.int32), np.asarray(Ax, np.float64)
+
+
+def multiblock(dims, m_local, m_couple: int, n_lp: int = 0, seed: int = 11, name: str = "multiblock") -> ConicProblem:
+    """SDP blocks of orders ``dims`` (an optional LP cone of ``n_lp`` columns last) with
+    ``m_local[k]`` constraints on block k alone and ``m_couple`` constraints on every block.
+
+    Coefficients are unit diagonals e_i e_i^T, edges E_ac + E_ca, sparse rank-one a a^T
+    (support 3) and sparse symmetric matrices, distinct within a block. C_k = I + R_k with a
+    few off-diagonal entries of size <= 0.1, and the LP costs are U(0.5, 1.5), so y = 0 is
+    strictly dual feasible; b = A(X0) at X0_k = I + G_k G_k^T / n_k (G_k n_k x 3) and the LP
+    point x0 = 1, so the primal is strictly feasible too.
+    """
+    rng = np.random.default_rng(seed)
+    K = len(dims)
+    m = int(sum(m_local)) + int(m_couple)
+    cols = [[None] * (m + 1) for _ in range(K)]
+    X0 = []
+    for k, n in enumerate(dims):
+        idx = [int(pack_idx(n, i, i)) for i in range(n)]
+        val = [1.0] * n
+        for _ in range(n // 2):
+            if n < 2:
+                break
+            a, c = sorted(rng.choice(n, size=2, replace=False).tolist(), reverse=True)
+            p = int(pack_idx(n, a, c))
+            if p not in idx:
+                idx.append(p)
+                val.append(float(rng.uniform(-0.1, 0.1)))
+        cols[k][0] = (idx, val)
+        G = rng.standard_normal((n, 3))
+        X0.append(np.eye(n) + G @ G.T / n)
+
+    def coeff(n, seen):
+        for _ in range(100):
+            t = 0 if n == 1 else int(rng.integers(0, 4))
+            if t == 0:
+                i = int(rng.integers(0, n))
+                ent = {(i, i): 1.0}
+            elif t == 1:
+                a, c = sorted(rng.choice(n, size=2, replace=False).tolist(), reverse=True)
+                ent = {(a, c): 1.0}
+            elif t == 2:
+                sup = np.sort(rng.choice(n, size=min(3, n), replace=False))
+                av = rng.standard_normal(sup.size)
+                ent = {}
+                for p in range(sup.size):
+                    for q in range(p + 1):
+                        ent[(int(sup[p]), int(sup[q]))] = float(av[p] * av[q])
+            else:
+                i = int(rng.integers(0, n))
+                ent = {(i, i): float(rng.uniform(0.5, 2.0))}
+                for _ in range(2):
+                    a, c = sorted(rng.choice(n, size=2, replace=False).tolist(), reverse=True)
+                    ent[(a, c)] = float(rng.uniform(-1.0, 1.0))
+            key = tuple(sorted((k2, round(v, 12)) for k2, v in ent.items()))
+            if key not in seen:
+                seen.add(key)
+                return ent
+        raise ValueError("block of order %d cannot hold that many distinct constraints" % n)
+
+    def add(k, row, ent):
+        n = dims[k]
+        idx = [int(pack_idx(n, a, c)) for (a, c) in ent]
+        val = list(ent.values())
+        cols[k][row + 1] = (idx, val)
+        return sum((v if a == c else 2.0 * v) * X0[k][a, c] for (a, c), v in ent.items())
+
+    b = np.zeros(m)
+    row = 0
+    for k, n in enumerate(dims):
+        seen = set()
+        for _ in range(m_local[k]):
+            b[row] = add(k, row, coeff(n, seen))
+            row += 1
+    for _ in range(m_couple):
+        for k, n in enumerate(dims):
+            b[row] += add(k, row, coeff(n, set()))
+        row += 1
+    cones = []
+    for k, n in enumerate(dims):
+        Ap, Ai, Ax = _csc_columns(m, cols[k])
+        cones.append(("sdp", int(n), Ap, Ai, Ax))
+    if n_lp > 0:
+        c = rng.uniform(0.5, 1.5, size=n_lp)
+        lcols = [None] * (m + 1)
+        lcols[0] = (list(range(n_lp)), c.tolist())
+        per = [dict() for _ in range(m)]
+        for q in range(n_lp):
+            for i in rng.choice(m, size=min(2, m), replace=False):
+                v = float(rng.uniform(-1.0, 1.0))
+                per[int(i)][q] = v
+                b[int(i)] += v  # x0 = 1
+        for i in range(m):
+            if per[i]:
+                lcols[i + 1] = (list(per[i].keys()), list(per[i].values()))
+        Ap, Ai, Ax = _csc_columns(m, lcols)
+        cones.append(("lp", int(n_lp), Ap, Ai, Ax))
+    return ConicProblem(name, m, b, cones, {"dims": list(map(int, dims)), "m_local": list(map(int, m_local)),
+                                            "m_couple": int(m_couple), "n_lp": int(n_lp), "seed": seed})
+
+
+# Multi-cone parity cases: all dense cones; dense and sparse cones with a 1 x 1 block; two
+# dense cones and an LP cone; a larger mixed case.
+MULTIBLOCK_CASES = {
+    "mb3": dict(dims=[20, 15, 10], m_local=[25, 20, 15], m_couple=6, seed=11),
+    "mb5_sparse": dict(dims=[12, 10, 8, 6, 1], m_local=[10, 8, 6, 4, 1], m_couple=3, seed=12),
+    "mb2_lp": dict(dims=[30, 25], m_local=[30, 30], m_couple=5, n_lp=12, seed=13),
+    "mb4_n500": dict(dims=[200, 150, 100, 50], m_local=[300, 200, 150, 100], m_couple=50, seed=14),
+}
+
+
+def multiblock_case(name: str) -> ConicProblem:
+    return multiblock(name=name, **MULTIBLOCK_CASES[name])
+
+
 WORKLOADS = {
     "maxcut_n200": lambda: maxcut(200, 0.05, seed=1),
     "theta_n300": lambda: lovasz_theta(300, 0.1, seed=2),

@@ -168,6 +168,77 @@ def solve(inst, want_x: bool = True, params: dict | None = None, quiet: bool = T
     return out
 
 
+def solve_problem(prob, params: dict | None = None, quiet: bool = True) -> dict:
+    """Run HDSDPOptimize on a multi-cone ``prob`` (instances.ConicProblem): every cone set in
+    its order through HDSDPSetCone (SDP blocks as dense SDP user data, the reference choosing
+    dense or sparse cones itself; LP cones as LP). Returns y, objectives, status, iterations,
+    DIMACS errors and per cone (X, S) or (x, s)."""
+    L = lib()
+    h = C.c_void_p()
+    assert L.HDSDPCreate(C.byref(h)) == 0
+    assert L.HDSDPInit(h, prob.m, len(prob.cones)) == 0
+    keep, uds = [], []
+    for k, (kind, dim, Ap, Ai, Ax) in enumerate(prob.cones):
+        arrs = [np.ascontiguousarray(Ap, dtype=np.int32), np.ascontiguousarray(Ai, dtype=np.int32),
+                np.ascontiguousarray(Ax, dtype=np.float64)]
+        keep.append(arrs)
+        ud = C.c_void_p()
+        assert L.HUserDataCreate(C.byref(ud)) == 0
+        L.HUserDataSetConeData(ud, CONETYPE_DENSE_SDP if kind == "sdp" else CONETYPE_LP, prob.m, int(dim),
+                               _ip(arrs[0]), _ip(arrs[1]), _dp(arrs[2]))
+        uds.append(ud)
+        assert L.HDSDPSetCone(h, k, ud) == 0
+    b = np.ascontiguousarray(prob.b, dtype=np.float64)
+    L.HDSDPSetDualObjective(h, _dp(b))
+    for k, v in (params or {}).items():
+        if isinstance(v, int):
+            if k >= 3:
+                L.oracle_set_int_param(h, k, v)
+            else:
+                L.HDSDPSetIntParam(h, k, v)
+        else:
+            L.HDSDPSetDblParam(h, k, float(v))
+    saved = None
+    if quiet:
+        saved = os.dup(1)
+        devnull = os.open(os.devnull, os.O_WRONLY)
+        os.dup2(devnull, 1)
+        os.close(devnull)
+    try:
+        t0 = time.perf_counter()
+        ret = L.HDSDPOptimize(h, 0)
+        t1 = time.perf_counter()
+        y = np.zeros(prob.m)
+        po, do = C.c_double(), C.c_double()
+        L.HDSDPGetRowDual(h, C.byref(po), C.byref(do), _dp(y))
+        out = {"retcode": int(ret), "time": t1 - t0, "y": y, "pobj": po.value, "dobj": do.value,
+               "status": int(L.oracle_status(h)), "iters": int(L.oracle_iters(h))}
+        values = []
+        for k, (kind, dim, _, _, _) in enumerate(prob.cones):
+            size = dim * dim if kind == "sdp" else dim
+            P, D, aux = np.zeros(size), np.zeros(size), np.zeros(size)
+            L.HDSDPGetConeValues(h, k, _dp(P), _dp(D), _dp(aux))
+            if kind == "sdp":
+                P, D = P.reshape(dim, dim, order="F"), D.reshape(dim, dim, order="F")
+            values.append((P, D))
+        out["values"] = values
+        errs = np.zeros(6)
+        L.HDSDPCheckSolution(h, _dp(errs))
+        out["errs"] = errs
+        out["status_after_check"] = int(L.oracle_status(h))
+        for ud in uds:
+            L.HUserDataDestroy(C.byref(ud))
+        L.HDSDPDestroy(C.byref(h))
+    finally:
+        if quiet:
+            import sys
+            sys.stdout.flush()
+            C.CDLL(None).fflush(None)
+            os.dup2(saved, 1)
+            os.close(saved)
+    return out
+
+
 def schur_probe(inst, y, resi, type_kkt: int = 0):
     """Reference Schur complement at (y, resi): returns dict(M lower, asinv, asinvrd, ...)."""
     L = lib()

@@ -101,6 +101,18 @@ def main(full: bool):
             arrays["y/" + key] = r["y"]
             arrays["x_lp/" + key] = r["x_lp"]
             print(key, r["iters"], r["status_after_check"], r["pobj"], r["dobj"], flush=True)
+    # several cones: SDP blocks (dense and sparse cones, a 1 x 1 block) and an LP cone
+    out["multiblock_solves"] = {}
+    for name in instances.MULTIBLOCK_CASES:
+        prob = instances.multiblock_case(name)
+        r = ref_api.solve_problem(prob)
+        out["multiblock_solves"][name] = {
+            "m": prob.m, "cones": [[c[0], int(c[1])] for c in prob.cones], "retcode": r["retcode"],
+            "iters": r["iters"], "status": r["status_after_check"], "pobj": r["pobj"], "dobj": r["dobj"],
+            "errs": [float(e) for e in r["errs"]],
+        }
+        arrays["y/" + name] = r["y"]
+        print(name, r["iters"], r["status_after_check"], r["pobj"], r["dobj"], flush=True)
     # known answers of the Lovasz theta number, solved by the reference
     ka = {}
     for label, inst, value in [

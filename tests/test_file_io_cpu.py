@@ -54,6 +54,33 @@ def write_sdpa_lp(path, inst, lp):
         f.write("\n".join(lines) + "\n")
 
 
+def write_sdpa_problem(path, prob):
+    """A multi-cone problem (instances.ConicProblem) as an SDPA file: its SDP blocks in
+    order, then its LP cone as a diagonal block (negative size); F0 = -C_k, 1-based upper
+    entries."""
+    sdp = [c for c in prob.cones if c[0] == "sdp"]
+    lps = [c for c in prob.cones if c[0] == "lp"]
+    assert len(lps) <= 1 and prob.cones[:len(sdp)] == sdp
+    sizes = [str(c[1]) for c in sdp] + ["-%d" % c[1] for c in lps]
+    lines = ['"generated from %s' % prob.name, "%d = mDIM" % prob.m, "%d = nBLOCK" % len(sizes),
+             " ".join(sizes) + " = bLOCKsTRUCT", " ".join("%.17g" % v for v in prob.b)]
+    for blk, (kind, n, Ap, Ai, Ax) in enumerate(prob.cones):
+        for k in range(prob.m + 1):
+            sign = -1.0 if k == 0 else 1.0
+            rows, vals = Ai[Ap[k]:Ap[k + 1]], Ax[Ap[k]:Ap[k + 1]]
+            if kind == "lp":
+                for q, v in zip(rows, vals):
+                    lines.append("%d %d %d %d %.17g" % (k, blk + 1, q + 1, q + 1, sign * v))
+                continue
+            starts = instances.pack_idx(n, np.arange(n), np.arange(n))
+            j = np.searchsorted(starts, rows, side="right") - 1
+            i = rows - starts[j] + j
+            for a, c, v in zip(j, i, vals):
+                lines.append("%d %d %d %d %.17g" % (k, blk + 1, a + 1, c + 1, sign * v))
+    with open(path, "w") as f:
+        f.write("\n".join(lines) + "\n")
+
+
 @pytest.fixture(scope="module")
 def libs():
     build()
@@ -185,3 +212,26 @@ def test_sdpa_with_lp_block(libs, tmp_path):
         np.testing.assert_array_equal(np.sort(lp[2][lo:hi]), np.sort(got_lp[2][glo:ghi]))
         np.testing.assert_array_equal(lp[3][lo:hi][np.argsort(lp[2][lo:hi])],
                                       got_lp[3][glo:ghi][np.argsort(got_lp[2][glo:ghi])])
+
+
+@pytest.mark.parametrize("name", ["mb5_sparse", "mb2_lp"])
+def test_sdpa_multiblock(libs, tmp_path, name):
+    """Several SDP blocks (and an LP block) written as SDPA: both readers give the same
+    arrays, and sdpa_cones() gives back the problem's cones (entry order within a column
+    may differ)."""
+    ours, ref = libs
+    prob = instances.multiblock_case(name)
+    path = tmp_path / ("%s.dat-s" % name)
+    write_sdpa_problem(path, prob)
+    same(api.read_sdpa_with(ours, path), api.read_sdpa_with(ref, path))
+    got = api.sdpa_cones(path)
+    assert got.m == prob.m and len(got.cones) == len(prob.cones)
+    np.testing.assert_array_equal(got.b, prob.b)
+    for (k0, n0, p0, i0, x0), (k1, n1, p1, i1, x1) in zip(prob.cones, got.cones):
+        assert (k0, n0) == (k1, n1)
+        np.testing.assert_array_equal(p0, p1)
+        for k in range(prob.m + 1):
+            o0 = np.argsort(i0[p0[k]:p0[k + 1]], kind="stable")
+            o1 = np.argsort(i1[p1[k]:p1[k + 1]], kind="stable")
+            np.testing.assert_array_equal(i0[p0[k]:p0[k + 1]][o0], i1[p1[k]:p1[k + 1]][o1])
+            np.testing.assert_array_equal(x0[p0[k]:p0[k + 1]][o0], x1[p1[k]:p1[k + 1]][o1])
