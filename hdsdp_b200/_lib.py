@@ -20,6 +20,8 @@ EXPORTS = [
     "HUserDataCreate", "HUserDataSetConeData", "HUserDataChooseCone", "HUserDataClear",
     "HUserDataDestroy",
     "HDSDPGetStatus", "HDSDPGetIterCount", "HDSDPSetPrimalRefinement", "HDSDPSetPrecision",
+    "HDSDPSetSparseSlack", "HDSDPGetSparseSlackInfo", "hdsdpb_sparse_analyse",
+    "hdsdpb_sparse_cholesky",
     "HDSDPGetIterLog", "HDSDPGetTimers", "HDSDPAdjoint",
     "hdsdpb_schur_probe", "hdsdpb_ratio_probe", "hdsdpb_cholesky", "hdsdpb_cholesky_noalloc", "hdsdpb_inverse", "hdsdpb_gemm",
     "hdsdpb_kernel_timing", "hdsdpb_gridsync_probe", "hdsdpb_launch_count", "hdsdpb_release_cached_memory",
@@ -61,6 +63,10 @@ def load():
         "HDSDPGetIterCount": ([vp], i),
         "HDSDPSetPrimalRefinement": ([vp, i], None),
         "HDSDPSetPrecision": ([vp, i], None),
+        "HDSDPSetSparseSlack": ([vp, i], None),
+        "HDSDPGetSparseSlackInfo": ([vp, dp], None),
+        "hdsdpb_sparse_analyse": ([i, i, ip, ip, i, dp, ip], i),
+        "hdsdpb_sparse_cholesky": ([i, i, ip, ip, dp, i, i, dp], i),
         "HDSDPGetIterLog": ([vp, i, dp, dp, dp, dp, dp, ip], i),
         "HDSDPGetTimers": ([vp, dp], None),
         "HDSDPAdjoint": ([vp, dp, dp, dp, dp, dp], i),

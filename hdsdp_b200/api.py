@@ -125,6 +125,18 @@ class Solver:
     def set_precision(self, mode: int):
         self.L.HDSDPSetPrecision(self.h, int(mode))
 
+    def set_sparse_slack(self, mode: int):
+        """Factorisation of S in the positive-definiteness checks: -1 automatic, 0 dense,
+        1 sparse (minimum-degree rounds and a dense front) whenever the pattern allows."""
+        self.L.HDSDPSetSparseSlack(self.h, int(mode))
+
+    def sparse_slack_info(self) -> dict:
+        o = np.zeros(8)
+        self.L.HDSDPGetSparseSlackInfo(self.h, _dp(o))
+        return {"cones": int(o[0]), "front": int(o[1]), "rounds": int(o[2]), "factorisations": int(o[3]),
+                "eliminated": int(o[4]), "trial_factorisations": int(o[5]), "dense_after_var": int(o[6]),
+                "dense_after_check": int(o[7])}
+
     def optimize(self, d_only: int = 0) -> int:
         return self.L.HDSDPOptimize(self.h, int(d_only))
 
@@ -206,7 +218,7 @@ class Solver:
 
 
 def solve(inst, want_x: bool = True, primal_refinement: bool = True, precision: int = 0,
-          params: dict | None = None, lp=None) -> dict:
+          params: dict | None = None, lp=None, sparse_slack: int = 0) -> dict:
     """Solve ``inst`` on the GPU (with the LP cone ``lp`` = (n_lp, Ap, Ai, Ax) as cone 1 when
     given); returns the oracle driver's fields plus the iteration log."""
     s = Solver()
@@ -219,6 +231,7 @@ def solve(inst, want_x: bool = True, primal_refinement: bool = True, precision: 
         s.set_dual_objective(inst.b)
         s.set_primal_refinement(primal_refinement)
         s.set_precision(precision)
+        s.set_sparse_slack(sparse_slack)
         for k, v in (params or {}).items():
             if isinstance(v, int):
                 s.set_int_param(k, v)
@@ -229,7 +242,8 @@ def solve(inst, want_x: bool = True, primal_refinement: bool = True, precision: 
         t1 = time.perf_counter()
         po, do, y = s.get_row_dual()
         out = {"retcode": int(ret), "time": t1 - t0, "y": y, "pobj": po, "dobj": do,
-               "status": s.status(), "iters": s.iters(), "log": s.iter_log(), "timers": s.timers()}
+               "status": s.status(), "iters": s.iters(), "log": s.iter_log(), "timers": s.timers(),
+               "sparse_slack": s.sparse_slack_info()}
         if want_x:
             X, S = s.get_cone_values()
             out["X"], out["S"] = X, S
@@ -242,7 +256,8 @@ def solve(inst, want_x: bool = True, primal_refinement: bool = True, precision: 
         s.close()
 
 
-def solve_problem(prob, primal_refinement: bool = True, precision: int = 0, params: dict | None = None) -> dict:
+def solve_problem(prob, primal_refinement: bool = True, precision: int = 0, params: dict | None = None,
+                  sparse_slack: int = 0) -> dict:
     """Solve a multi-cone problem (instances.ConicProblem: SDP blocks and LP cones over one
     set of constraints) on the GPU; returns y, objectives, status, iterations, the iteration
     log, DIMACS errors and per cone (X, S) or (x, s)."""
@@ -255,6 +270,7 @@ def solve_problem(prob, primal_refinement: bool = True, precision: int = 0, para
         s.set_dual_objective(prob.b)
         s.set_primal_refinement(primal_refinement)
         s.set_precision(precision)
+        s.set_sparse_slack(sparse_slack)
         for k, v in (params or {}).items():
             if isinstance(v, int):
                 s.set_int_param(k, v)
@@ -265,7 +281,8 @@ def solve_problem(prob, primal_refinement: bool = True, precision: int = 0, para
         t1 = time.perf_counter()
         po, do, y = s.get_row_dual()
         out = {"retcode": int(ret), "time": t1 - t0, "y": y, "pobj": po, "dobj": do,
-               "status": s.status(), "iters": s.iters(), "log": s.iter_log(), "timers": s.timers()}
+               "status": s.status(), "iters": s.iters(), "log": s.iter_log(), "timers": s.timers(),
+               "sparse_slack": s.sparse_slack_info()}
         out["values"] = [s.get_cone_values_at(k) for k in range(len(prob.cones))]
         out["errs"] = s.check_solution()
         out["status_after_check"] = s.status()

@@ -14,6 +14,13 @@ namespace hb {
 // with L reads L once.
 constexpr int kTriSolveMinM = 6000;
 
+// Hybrid sparse factorisation of S: automatic from this order on, minimum-degree rounds
+// up to this degree, and used only when the dense front is at most this fraction of n
+// (front flops at most a third of the dense factorisation's).
+constexpr int kHybridMinN = 1500;
+constexpr int kHybridCap = 64;
+constexpr double kHybridMaxFront = 0.7;
+
 
 static double wall() {
     using namespace std::chrono;
@@ -331,6 +338,35 @@ void SdpCone::detect_feature(const double *rowRHS, int intF[20], double dblF[20]
     if (stats[REF_DENSE] >= 0.7 * m) intF[4] = 1;
 }
 
+// Pattern of S = C - sum y_i A_i (+ diagonal): neighbour lists from the stored lower
+// entries of C and of every A_i. False when it is too dense for a sparse factorisation
+// to pay (more than n^2 / 8 off-diagonal entries listed).
+static bool slack_pattern(int n, const HostCoeff &C, const std::vector<HostCoeff> &A,
+                          std::vector<std::vector<int>> &adj) {
+    long total = (long) C.r.size();
+    for (const HostCoeff &h : A) total += (long) h.r.size();
+    if (total > (long) n * n / 8) return false;
+    std::vector<long long> keys;
+    keys.reserve(total);
+    auto add = [&](const HostCoeff &h) {
+        for (size_t e = 0; e < h.r.size(); ++e)
+            if (h.r[e] != h.c[e]) keys.push_back((long long) h.r[e] * n + h.c[e]);
+    };
+    add(C);
+    for (const HostCoeff &h : A) add(h);
+    std::sort(keys.begin(), keys.end());
+    keys.erase(std::unique(keys.begin(), keys.end()), keys.end());
+    if ((long) keys.size() > (long) n * n / 8) return false;
+    adj.assign(n, {});
+    for (long long k : keys) {
+        const int a = (int) (k / n), b = (int) (k % n);
+        adj[a].push_back(b);
+        adj[b].push_back(a);
+    }
+    for (auto &l : adj) std::sort(l.begin(), l.end());
+    return true;
+}
+
 hdsdp_retcode SdpCone::setup_device(cudaStream_t stream, Timers *t) {
     s = stream;
     tm = t;
@@ -350,6 +386,20 @@ hdsdp_retcode SdpCone::setup_device(cudaStream_t stream, Timers *t) {
     Fvar.alloc(n);
     Fcheck.alloc(n);
     lz.init(n, s);
+    hyVar = hyCheck = false;
+    if (sparseMode != 0 && (sparseMode == 1 || n >= kHybridMinN)) {
+        std::vector<std::vector<int>> adj;
+        if (slack_pattern(n, C, A, adj)) {
+            hy = new HybridFactor();
+            if (hy->analyse(n, adj, kHybridCap, kHybridMaxFront, sparseMode == 1)) {
+                hy->upload(s);
+            } else {
+                hy->release();
+                delete hy;
+                hy = nullptr;
+            }
+        }
+    }
     HB_CUDA(hb::cmalloc(&d_y, sizeof(double) * std::max(m, 1)));
     HB_CUDA(hb::cmalloc(&d_vec, sizeof(double) * std::max(m, 1)));
     if (sparse && m > 0) {
@@ -374,6 +424,12 @@ void SdpCone::release() {
     Fvar.release();
     Fcheck.release();
     lz.release();
+    if (hy) {
+        hy->release();
+        delete hy;
+        hy = nullptr;
+    }
+    hyVar = hyCheck = false;
 }
 
 // target = dC*C + dAs*sum_i y_i A_i + (dEye [+ perturbation])*I
@@ -446,15 +502,60 @@ bool SdpCone::factor_buffer(int which) {
         return fok;
     }
     if (sig.same(osig) && ook) {
-        copy_factor(s, F, var ? Fcheck : Fvar);
+        if (var ? hyCheck : hyVar) {
+            // the other object holds a hybrid result for the same matrix
+            (var ? hyVar : hyCheck) = true;
+            (var ? hyLogdetVar : hyLogdetCheck) = var ? hyLogdetCheck : hyLogdetVar;
+            F.factored = F.ok = true;
+            F.k_valid = false;
+        } else {
+            copy_factor(s, F, var ? Fcheck : Fvar);
+            (var ? hyVar : hyCheck) = false;
+        }
         fsig = sig;
         fok = true;
         ++nFactorReuse;
         return true;
     }
-    const bool ok = timed_factor(s, F, var ? Svar : Scheck, ld, tm);
+    const bool ok = use_hybrid(which) ? hybrid_factor(which) : timed_factor(s, F, var ? Svar : Scheck, ld, tm);
+    if (!use_hybrid(which)) (var ? hyVar : hyCheck) = false;
     fsig = sig;
     fok = ok;
+    return ok;
+}
+
+// Positive-definiteness and log det of the buffer `which` through the hybrid factor.
+bool SdpCone::hybrid_factor(int which) {
+    const bool var = (which == BUFFER_DUALVAR);
+    const double t0 = wall();
+    hy->factor_async(s, var ? Svar : Scheck, ld);
+    double logdet = 0.0;
+    const bool ok = hy->finish(s, &logdet);
+    DenseFactor &F = var ? Fvar : Fcheck;
+    F.factored = true;
+    F.ok = ok;
+    F.k_valid = false;
+    (var ? hyVar : hyCheck) = true;
+    (var ? hyLogdetVar : hyLogdetCheck) = logdet;
+    ++nHybrid;
+    if (!var) ++nHybridCheck;
+    if (tm) {
+        tm->s_factor += wall() - t0;
+        tm->n_sfactor += 1;
+    }
+    return ok;
+}
+
+// The dense factor of the buffer `which` in Fvar / Fcheck, formed now if the last
+// factorisation of it was a hybrid one.
+bool SdpCone::ensure_dense(int which) {
+    const bool var = (which == BUFFER_DUALVAR);
+    bool &h = var ? hyVar : hyCheck;
+    DenseFactor &F = var ? Fvar : Fcheck;
+    if (!h) return F.ok;
+    const bool ok = timed_factor(s, F, var ? Svar : Scheck, ld, tm);
+    h = false;
+    ++nDenseAfter[var ? 0 : 1];
     return ok;
 }
 
@@ -470,6 +571,7 @@ hdsdp_retcode SdpCone::ratio_test(double dtau, const double *dy, double ada, int
         *step = (vals[0] > 0.0) ? HDSDP_INFINITY : (-vals[1] / vals[0]);
         return HDSDP_RETCODE_OK;
     }
+    if (!ensure_dense(which == BUFFER_DUALVAR ? BUFFER_DUALVAR : BUFFER_DUALCHECK)) return HDSDP_RETCODE_FAILED;
     return lz.solve(F, dS, ld, step, tm);
 }
 
@@ -492,6 +594,10 @@ hdsdp_retcode SdpCone::get_barrier(double tau, const double *y, int which, doubl
         update(tau, y);
         if (!factor_buffer(BUFFER_DUALVAR)) return HDSDP_RETCODE_FAILED;
     }
+    if (which == BUFFER_DUALVAR ? hyVar : hyCheck) {
+        *logdet = (which == BUFFER_DUALVAR) ? hyLogdetVar : hyLogdetCheck;
+        return HDSDP_RETCODE_OK;
+    }
     log_diag_sum(s, F, d_scal);
     HB_CUDA(cudaMemcpyAsync(h_scal, d_scal, sizeof(double), cudaMemcpyDeviceToHost, s));
     HB_CUDA(cudaStreamSynchronize(s));
@@ -504,14 +610,17 @@ hdsdp_retcode SdpCone::add_step_and_check(double step, int which, int *interior)
         axpy(s, (int) (ld * n), step, dS, Svar);
         sigVar.valid = false;
         facVar.valid = false;
-        facVarOk = timed_factor(s, Fvar, Svar, ld, tm);
+        facVarOk = use_hybrid(BUFFER_DUALVAR) ? hybrid_factor(BUFFER_DUALVAR) : timed_factor(s, Fvar, Svar, ld, tm);
+        if (!use_hybrid(BUFFER_DUALVAR)) hyVar = false;
         *interior = facVarOk ? 1 : 0;
     } else {
         HB_CUDA(cudaMemcpyAsync(Scheck, Svar, sizeof(double) * ld * n, cudaMemcpyDeviceToDevice, s));
         axpy(s, (int) (ld * n), step, dS, Scheck);
         sigCheck.valid = false;
         facCheck.valid = false;
-        facCheckOk = timed_factor(s, Fcheck, Scheck, ld, tm);
+        facCheckOk = use_hybrid(BUFFER_DUALCHECK) ? hybrid_factor(BUFFER_DUALCHECK)
+                                                  : timed_factor(s, Fcheck, Scheck, ld, tm);
+        if (!use_hybrid(BUFFER_DUALCHECK)) hyCheck = false;
         *interior = facCheckOk ? 1 : 0;
     }
     return device_error_flag() ? HDSDP_RETCODE_FAILED : HDSDP_RETCODE_OK;
@@ -524,6 +633,10 @@ void SdpCone::get_primal(double mu, const double *y, const double *dy, double *X
     int interior = 0;
     interior_check_expert(1.0, -1.0, y, 0.0, BUFFER_DUALCHECK, &interior);
     if (!interior) {
+        printf("Recovery step is infeasible\n");
+        return;
+    }
+    if (!ensure_dense(BUFFER_DUALCHECK)) {
         printf("Recovery step is infeasible\n");
         return;
     }
@@ -744,6 +857,7 @@ hdsdp_retcode KKT::add_sdp(SdpCone &cone, int type) {
         if (!primalX) return HDSDP_RETCODE_FAILED;
         Wp = primalX;
     } else {
+        if (!cone.ensure_dense(BUFFER_DUALVAR)) return HDSDP_RETCODE_FAILED;
         double ti = wall();
         // split precision: W = K^T K on the tensor cores once n makes the product worth it
         bool done = false;

@@ -2,6 +2,7 @@
 #include "solver.h"
 #include "split.h"
 #include "../../include/hdsdp_b200.h"
+#include <algorithm>
 #include <cstring>
 #include <cmath>
 #include <vector>
@@ -15,6 +16,53 @@ int HDSDPGetStatus(hdsdp *h) { return (int) h->HStatus; }
 int HDSDPGetIterCount(hdsdp *h) { return h->nIterCount; }
 void HDSDPSetPrimalRefinement(hdsdp *h, int on) { h->HIntParams[INT_PARAM_PSDP] = on ? 1 : 0; }
 void HDSDPSetPrecision(hdsdp *h, int mode) { h->precision = mode; }
+void HDSDPSetSparseSlack(hdsdp *h, int mode) { h->sparseSlack = mode; }
+
+// Host only (no device work): the ordering of the sparse factorisation of S for the
+// pattern of nedge off-diagonal pairs (ei[k], ej[k]) with degree cap `cap`.
+// out = {rounds, front order, eliminated vertices, slots, Schur contributions}; front
+// (length n, may be null) receives the front's vertices in increasing order.
+int hdsdpb_sparse_analyse(int n, int nedge, const int *ei, const int *ej, int cap, double out[5], int *front) {
+    if (n <= 0 || nedge < 0 || !out) return -1;
+    std::vector<std::vector<int>> adj(n);
+    for (int k = 0; k < nedge; ++k) {
+        if (ei[k] < 0 || ei[k] >= n || ej[k] < 0 || ej[k] >= n) return -1;
+        if (ei[k] == ej[k]) continue;
+        adj[ei[k]].push_back(ej[k]);
+        adj[ej[k]].push_back(ei[k]);
+    }
+    for (auto &l : adj) {
+        std::sort(l.begin(), l.end());
+        l.erase(std::unique(l.begin(), l.end()), l.end());
+    }
+    hb::HybridFactor f;
+    if (!f.analyse(n, adj, cap, 1.0, true)) return -1;
+    out[0] = f.nrounds;
+    out[1] = f.nfront;
+    out[2] = f.nelim;
+    out[3] = f.nslot;
+    out[4] = (double) f.ncontrib;
+    if (front)
+        for (int p = 0; p < f.nfront; ++p) front[p] = f.hFront[p];
+    return 0;
+}
+
+void HDSDPGetSparseSlackInfo(hdsdp *h, double out[8]) {
+    for (int i = 0; i < 8; ++i) out[i] = 0.0;
+    for (const hb::ConeSlot &k : h->cones) {
+        if (!k.sdp || !k.sdp->hy) continue;
+        if (out[0] == 0.0) {
+            out[1] = k.sdp->hy->nfront;
+            out[2] = k.sdp->hy->nrounds;
+            out[4] = k.sdp->hy->nelim;
+        }
+        out[0] += 1.0;
+        out[3] += (double) k.sdp->nHybrid;
+        out[5] += (double) k.sdp->nHybridCheck;
+        out[6] += (double) k.sdp->nDenseAfter[0];
+        out[7] += (double) k.sdp->nDenseAfter[1];
+    }
+}
 
 int HDSDPGetIterLog(hdsdp *h, int maxLen, double *t, double *pObj, double *dObj, double *mu, double *gap,
                     int *phase) {
@@ -159,6 +207,72 @@ int hdsdpb_cholesky(int n, const double *S, double *L, double *logdiag) {
     cudaStreamDestroy(s);
     if (device_error_flag()) return -1;
     return ok ? 0 : 1;
+}
+
+// The sparse factorisation of S (column-major n x n, host; its pattern given by the
+// nedge off-diagonal pairs) with degree cap `cap`, timed over `reps` calls after one
+// warm-up call, and the dense cooperative factorisation of the same S timed the same
+// way. out = {positive definite (1/0), log det, ms per sparse factorisation, ms per
+// dense factorisation, dense-front order}. Returns 0, or -1 on invalid input.
+int hdsdpb_sparse_cholesky(int n, int nedge, const int *ei, const int *ej, const double *S, int cap, int reps,
+                           double out[5]) {
+    if (n <= 0 || nedge < 0 || !S || !out || reps < 1) return -1;
+    std::vector<std::vector<int>> adj(n);
+    for (int k = 0; k < nedge; ++k) {
+        if (ei[k] < 0 || ei[k] >= n || ej[k] < 0 || ej[k] >= n) return -1;
+        if (ei[k] == ej[k]) continue;
+        adj[ei[k]].push_back(ej[k]);
+        adj[ej[k]].push_back(ei[k]);
+    }
+    for (auto &l : adj) {
+        std::sort(l.begin(), l.end());
+        l.erase(std::unique(l.begin(), l.end()), l.end());
+    }
+    hb::HybridFactor f;
+    if (!f.analyse(n, adj, cap, 1.0, true)) return -1;
+    cudaStream_t s;
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return -1;
+    f.upload(s);
+    const long ld = pad_ld(n);
+    double *dS = nullptr;
+    hb::cmalloc(&dS, sizeof(double) * ld * n);
+    cudaMemcpy2D(dS, sizeof(double) * ld, S, sizeof(double) * n, sizeof(double) * n, n, cudaMemcpyHostToDevice);
+    legacy_fence();
+    double logdet = 0.0;
+    f.factor_async(s, dS, ld);
+    bool ok = f.finish(s, &logdet);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, s);
+    for (int r = 0; r < reps; ++r) {
+        f.factor_async(s, dS, ld);
+        ok = f.finish(s, &logdet) && ok;
+    }
+    cudaEventRecord(e1, s);
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    out[0] = ok ? 1.0 : 0.0;
+    out[1] = logdet;
+    out[2] = ms / reps;
+    out[4] = f.nfront;
+    DenseFactor F;
+    F.alloc(n, 0);
+    factorize(s, F, dS, ld);
+    cudaEventRecord(e0, s);
+    for (int r = 0; r < reps; ++r) factorize(s, F, dS, ld);
+    cudaEventRecord(e1, s);
+    cudaEventSynchronize(e1);
+    cudaEventElapsedTime(&ms, e0, e1);
+    out[3] = ms / reps;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    F.release();
+    f.release();
+    hb::cache_free(dS);
+    cudaStreamDestroy(s);
+    return device_error_flag() ? -1 : 0;
 }
 
 int hdsdpb_cholesky_solve(int n, const double *S, const double *b, double *x) {

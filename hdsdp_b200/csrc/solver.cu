@@ -1627,6 +1627,7 @@ hdsdp_retcode HDSDPOptimize(hdsdp *h, int dOptOnly) {
         } else {
             k.sdp = new SdpCone();
             k.sdp->precision = h->precision;
+            k.sdp->sparseMode = h->sparseSlack;
             CALL(k.sdp->proc_data(u->nConicRow, u->nConicCol, u->coneMatBeg, u->coneMatIdx, u->coneMatElem,
                                   k.type == HDSDP_CONETYPE_SPARSE_SDP));
             if (k.sdp->m == 0) {

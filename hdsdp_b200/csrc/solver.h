@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 #include "la.h"
 #include "sdp.h"
+#include "sparse_chol.h"
 #include "../../include/hdsdp.h"
 #include "../../include/hdsdp_user_data.h"
 
@@ -103,6 +104,21 @@ struct SdpCone {
     // factor of the same inputs held by either factor object.
     bool factor_buffer(int which);
     void invalidate_check_factor() { facCheck.valid = false; }
+    // Sparse dual pattern: positive-definiteness checks and log det go through the
+    // hybrid sparse factorisation; Fvar / Fcheck then hold no dense factor of their
+    // buffer (hyVar / hyCheck) until ensure_dense() forms it for a consumer of L.
+    // 0 off, -1 trial points only (BUFFER_DUALCHECK: the accepted point's factor is
+    // nearly always needed by the Lanczos step and the Schur build), 1 both buffers
+    int sparseMode = 0;
+    HybridFactor *hy = nullptr;
+    bool hyVar = false, hyCheck = false;
+    double hyLogdetVar = 0.0, hyLogdetCheck = 0.0;
+    long nHybrid = 0, nHybridCheck = 0, nDenseAfter[2] = {0, 0};
+    bool use_hybrid(int which) const {
+        return hy && (sparseMode == 1 || which != BUFFER_DUALVAR);
+    }
+    bool hybrid_factor(int which);
+    bool ensure_dense(int which);
     Lanczos lz;
     double dualResidual = 0.0, dualPerturb = 0.0;
     double *d_y = nullptr;       // device copy of the current coefficient vector
@@ -288,6 +304,7 @@ struct hdsdp_solver_internal {
     double dErrs[6] = {0};
     bool optimized = false;
     int precision = 0;
+    int sparseSlack = 0;           // factorisation of S in PSD checks: 0 dense, -1 trial points sparse, 1 sparse
     int verbose = 0;
     std::vector<hb::IterRecord> log;
     std::string modelFeatures;

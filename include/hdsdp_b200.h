@@ -30,6 +30,25 @@ extern void HDSDPSetPrimalRefinement( hdsdp *HSolver, int on );
    2 = split precision while the relative gap is above 1e-3, FP64 after. */
 extern void HDSDPSetPrecision( hdsdp *HSolver, int mode );
 
+/* Factorisation of the dual slack S for positive-definiteness checks and log det:
+   0 = always the dense cooperative Cholesky (default); -1 = a sparse factorisation
+   (minimum-degree rounds on the device and a dense front) for the trial points of
+   blocks of order >= 1500 whose front is at most 70% of the order, the dense Cholesky
+   for the accepted point, whose factor the step bound and the Schur build use;
+   1 = sparse for every check whenever the pattern allows it. A consumer of L (the
+   Lanczos step bound, S^-1, primal recovery) refactors densely when its buffer was
+   factored sparsely. This is where the reference uses Pardiso for sparse dual
+   matrices (interface/hdsdp_conic_sdp.c:153-275). Takes effect at the next
+   HDSDPOptimize. */
+extern void HDSDPSetSparseSlack( hdsdp *HSolver, int mode );
+
+/* out[0] = SDP cones factored sparsely, out[1] = dense-front order of the first of
+   them, out[2] = its minimum-degree rounds, out[3] = sparse factorisations in the
+   last solve (all cones), out[4] = vertices eliminated before the front, out[5] = the
+   sparse factorisations of trial points, out[6] / out[7] = dense factorisations that
+   followed a sparse one because a consumer needed L (accepted point / trial point). */
+extern void HDSDPGetSparseSlackInfo( hdsdp *HSolver, double out[8] );
+
 /* Per-iteration record of the last solve: elapsed seconds, primal and dual
    objective, barrier parameter, relative gap (p - d) / (1 + |p| + |d|) and
    phase (0 infeasible, 1 embedding, 2 potential reduction, 3 refinement),
@@ -151,6 +170,22 @@ extern int hdsdpb_split_gemm( int M, int N, int K, const double *A, int lda, int
    8 Cholesky without it, 9 solve with the factor (forward and backward substitution).
    Writes milliseconds per call. */
 extern int hdsdpb_kernel_timing( int which, int n, int reps, double *ms );
+
+/* Host only (no device work): the ordering of the sparse factorisation of S for the
+   pattern of nedge off-diagonal pairs (ei[k], ej[k]) with degree cap `cap`.
+   out = {rounds, front order, eliminated vertices, slots, Schur contributions};
+   front (length n, may be NULL) receives the front's vertices in increasing order.
+   Returns 0, or -1 for invalid input. */
+extern int hdsdpb_sparse_analyse( int n, int nedge, const int *ei, const int *ej, int cap, double out[5],
+                                  int *front );
+
+/* The sparse factorisation of S (column-major n x n, host; pattern = the nedge
+   off-diagonal pairs) with degree cap `cap`, timed over `reps` calls after a warm-up,
+   beside the dense factorisation of the same S. out = {positive definite (1/0),
+   log det S, ms per sparse factorisation, ms per dense factorisation, front order}.
+   Returns 0, or -1 for invalid input. */
+extern int hdsdpb_sparse_cholesky( int n, int nedge, const int *ei, const int *ej, const double *S, int cap,
+                                   int reps, double out[5] );
 
 /* Milliseconds taken by `reps` grid-wide barriers in one cooperative launch of
    `blocks` blocks of 256 threads (cost model of the persistent factorisation). */
