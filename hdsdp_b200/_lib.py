@@ -21,7 +21,7 @@ EXPORTS = [
     "HUserDataDestroy",
     "HDSDPGetStatus", "HDSDPGetIterCount", "HDSDPSetPrimalRefinement", "HDSDPSetPrecision",
     "HDSDPSetSparseSlack", "HDSDPGetSparseSlackInfo", "hdsdpb_sparse_analyse",
-    "hdsdpb_sparse_cholesky",
+    "hdsdpb_sparse_cholesky", "hdsdpb_sparse_congruence",
     "HDSDPGetIterLog", "HDSDPGetTimers", "HDSDPAdjoint",
     "hdsdpb_schur_probe", "hdsdpb_ratio_probe", "hdsdpb_cholesky", "hdsdpb_cholesky_noalloc", "hdsdpb_inverse", "hdsdpb_gemm",
     "hdsdpb_kernel_timing", "hdsdpb_gridsync_probe", "hdsdpb_launch_count", "hdsdpb_release_cached_memory",
@@ -67,6 +67,7 @@ def load():
         "HDSDPGetSparseSlackInfo": ([vp, dp], None),
         "hdsdpb_sparse_analyse": ([i, i, ip, ip, i, dp, ip], i),
         "hdsdpb_sparse_cholesky": ([i, i, ip, ip, dp, i, i, dp], i),
+        "hdsdpb_sparse_congruence": ([i, i, ip, ip, dp, dp, dp, dp, dp], i),
         "HDSDPGetIterLog": ([vp, i, dp, dp, dp, dp, dp, ip], i),
         "HDSDPGetTimers": ([vp, dp], None),
         "HDSDPAdjoint": ([vp, dp, dp, dp, dp, dp], i),

@@ -218,7 +218,7 @@ class Solver:
 
 
 def solve(inst, want_x: bool = True, primal_refinement: bool = True, precision: int = 0,
-          params: dict | None = None, lp=None, sparse_slack: int = 0) -> dict:
+          params: dict | None = None, lp=None, sparse_slack: int = -1) -> dict:
     """Solve ``inst`` on the GPU (with the LP cone ``lp`` = (n_lp, Ap, Ai, Ax) as cone 1 when
     given); returns the oracle driver's fields plus the iteration log."""
     s = Solver()
@@ -257,7 +257,7 @@ def solve(inst, want_x: bool = True, primal_refinement: bool = True, precision: 
 
 
 def solve_problem(prob, primal_refinement: bool = True, precision: int = 0, params: dict | None = None,
-                  sparse_slack: int = 0) -> dict:
+                  sparse_slack: int = -1) -> dict:
     """Solve a multi-cone problem (instances.ConicProblem: SDP blocks and LP cones over one
     set of constraints) on the GPU; returns y, objectives, status, iterations, the iteration
     log, DIMACS errors and per cone (X, S) or (x, s)."""

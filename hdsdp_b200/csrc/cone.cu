@@ -506,6 +506,7 @@ bool SdpCone::factor_buffer(int which) {
             // the other object holds a hybrid result for the same matrix
             (var ? hyVar : hyCheck) = true;
             (var ? hyLogdetVar : hyLogdetCheck) = var ? hyLogdetCheck : hyLogdetVar;
+            (var ? hySeqVar : hySeqCheck) = var ? hySeqCheck : hySeqVar;
             F.factored = F.ok = true;
             F.k_valid = false;
         } else {
@@ -537,6 +538,7 @@ bool SdpCone::hybrid_factor(int which) {
     F.k_valid = false;
     (var ? hyVar : hyCheck) = true;
     (var ? hyLogdetVar : hyLogdetCheck) = logdet;
+    (var ? hySeqVar : hySeqCheck) = hy->seq;
     ++nHybrid;
     if (!var) ++nHybridCheck;
     if (tm) {
@@ -571,7 +573,15 @@ hdsdp_retcode SdpCone::ratio_test(double dtau, const double *dy, double ada, int
         *step = (vals[0] > 0.0) ? HDSDP_INFINITY : (-vals[1] / vals[0]);
         return HDSDP_RETCODE_OK;
     }
-    if (!ensure_dense(which == BUFFER_DUALVAR ? BUFFER_DUALVAR : BUFFER_DUALCHECK)) return HDSDP_RETCODE_FAILED;
+    const bool var = (which == BUFFER_DUALVAR);
+    if (hy && (var ? hyVar : hyCheck) && (var ? hySeqVar : hySeqCheck) == hy->seq) {
+        // the sparse factor of this buffer is the one held: the step bound runs on it
+        lz.hyOp = hy;
+        const hdsdp_retcode r = lz.solve(F, dS, ld, step, tm);
+        lz.hyOp = nullptr;
+        return r;
+    }
+    if (!ensure_dense(var ? BUFFER_DUALVAR : BUFFER_DUALCHECK)) return HDSDP_RETCODE_FAILED;
     return lz.solve(F, dS, ld, step, tm);
 }
 
@@ -1236,16 +1246,24 @@ void Lanczos::release() {
 
 hdsdp_retcode Lanczos::solve(DenseFactor &F, const double *D, long ldD, double *maxStep, Timers *tm) {
     double t0 = wall();
-    compute_inverse_factor(s, F);
+    if (hyOp) {
+        if (hyOp->nfront > 0) compute_inverse_factor(s, hyOp->Ff);
+    } else {
+        compute_inverse_factor(s, F);
+    }
     if (tm) {
         HB_CUDA(cudaStreamSynchronize(s));
         tm->lz_inverse += wall() - t0;
     }
     // buffers: V columns, w (Mv), t1 / z1 / z2 temporaries
     auto mv = [&](const double *x, double *y) {
-        coldot(s, n, n, F.K, F.ld, x, t1, 1.0, 0.0, 1);   // t1 = L^-T x
-        coldot(s, n, n, D, ldD, t1, u, -1.0, 0.0, 0);     // u  = -D t1
-        coldot(s, n, n, F.KT, F.ld, u, y, 1.0, 0.0, 2);   // y  = L^-1 u
+        if (hyOp) {
+            hyOp->apply_congruence(s, D, ldD, -1.0, x, t1, u, y);  // y = L^-1 (-D) L^-T x
+        } else {
+            coldot(s, n, n, F.K, F.ld, x, t1, 1.0, 0.0, 1);   // t1 = L^-T x
+            coldot(s, n, n, D, ldD, t1, u, -1.0, 0.0, 0);     // u  = -D t1
+            coldot(s, n, n, F.KT, F.ld, u, y, 1.0, 0.0, 2);   // y  = L^-1 u
+        }
         if (tm) tm->n_lanczos_mv += 1;
     };
     HB_CUDA(cudaMemsetAsync(V, 0, sizeof(double) * ld * (maxdim + 1), s));

@@ -275,6 +275,55 @@ int hdsdpb_sparse_cholesky(int n, int nedge, const int *ei, const int *ej, const
     return device_error_flag() ? -1 : 0;
 }
 
+// With the sparse factor S = L L^T (pattern as above, cap 64): t = L^-T x and
+// y = L^-1 (D t) for host n x n D and n-vector x. Returns 0, 1 if S is not positive
+// definite, -1 on invalid input.
+int hdsdpb_sparse_congruence(int n, int nedge, const int *ei, const int *ej, const double *S, const double *D,
+                             const double *x, double *y, double *t) {
+    if (n <= 0 || nedge < 0 || !S || !D || !x || !y) return -1;
+    std::vector<std::vector<int>> adj(n);
+    for (int k = 0; k < nedge; ++k) {
+        if (ei[k] < 0 || ei[k] >= n || ej[k] < 0 || ej[k] >= n) return -1;
+        if (ei[k] == ej[k]) continue;
+        adj[ei[k]].push_back(ej[k]);
+        adj[ej[k]].push_back(ei[k]);
+    }
+    for (auto &l : adj) {
+        std::sort(l.begin(), l.end());
+        l.erase(std::unique(l.begin(), l.end()), l.end());
+    }
+    hb::HybridFactor f;
+    if (!f.analyse(n, adj, 64, 1.0, true)) return -1;
+    cudaStream_t s;
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return -1;
+    f.upload(s);
+    const long ld = pad_ld(n);
+    double *dS = nullptr, *dD = nullptr, *dv = nullptr;
+    hb::cmalloc(&dS, sizeof(double) * ld * n);
+    hb::cmalloc(&dD, sizeof(double) * ld * n);
+    hb::cmalloc(&dv, sizeof(double) * 4 * ld);
+    cudaMemcpy2D(dS, sizeof(double) * ld, S, sizeof(double) * n, sizeof(double) * n, n, cudaMemcpyHostToDevice);
+    cudaMemcpy2D(dD, sizeof(double) * ld, D, sizeof(double) * n, sizeof(double) * n, n, cudaMemcpyHostToDevice);
+    cudaMemcpy(dv, x, sizeof(double) * n, cudaMemcpyHostToDevice);
+    legacy_fence();
+    f.factor_async(s, dS, ld);
+    const bool ok = f.finish(s, nullptr);
+    if (ok) {
+        if (f.nfront > 0) compute_inverse_factor(s, f.Ff);
+        f.apply_congruence(s, dD, ld, 1.0, dv, dv + ld, dv + 2 * ld, dv + 3 * ld);
+        cudaMemcpyAsync(y, dv + 3 * ld, sizeof(double) * n, cudaMemcpyDeviceToHost, s);
+        if (t) cudaMemcpyAsync(t, dv + ld, sizeof(double) * n, cudaMemcpyDeviceToHost, s);
+    }
+    cudaStreamSynchronize(s);
+    f.release();
+    hb::cache_free(dS);
+    hb::cache_free(dD);
+    hb::cache_free(dv);
+    cudaStreamDestroy(s);
+    if (device_error_flag()) return -1;
+    return ok ? 0 : 1;
+}
+
 int hdsdpb_cholesky_solve(int n, const double *S, const double *b, double *x) {
     if (n < 0 || (n > 0 && (!S || !b || !x))) return -1;
     if (n == 0) return 0;

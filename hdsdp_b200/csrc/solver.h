@@ -56,6 +56,8 @@ struct Lanczos {
     double *d_scal = nullptr, *h_scal = nullptr;
     double *init_vec = nullptr, *pert_vec = nullptr;  // device, deterministic per n
     int nComputed = 0;
+    // when set, the operator is built from this sparse factor of S instead of F
+    HybridFactor *hyOp = nullptr;
     void init(int n_, cudaStream_t s_);
     void release();
     // Max alpha with  I + alpha * K (-D) K^T  psd, where K = L^-1 of the factor.
@@ -107,12 +109,13 @@ struct SdpCone {
     // Sparse dual pattern: positive-definiteness checks and log det go through the
     // hybrid sparse factorisation; Fvar / Fcheck then hold no dense factor of their
     // buffer (hyVar / hyCheck) until ensure_dense() forms it for a consumer of L.
-    // 0 off, -1 trial points only (BUFFER_DUALCHECK: the accepted point's factor is
-    // nearly always needed by the Lanczos step and the Schur build), 1 both buffers
-    int sparseMode = 0;
+    // -1 trial points only (BUFFER_DUALCHECK; the accepted point's S^-1 feeds the Schur
+    // build, which needs the dense factor), 0 off, 1 both buffers
+    int sparseMode = -1;
     HybridFactor *hy = nullptr;
     bool hyVar = false, hyCheck = false;
     double hyLogdetVar = 0.0, hyLogdetCheck = 0.0;
+    long hySeqVar = -1, hySeqCheck = -1;  // the sparse factorisation each buffer's result came from
     long nHybrid = 0, nHybridCheck = 0, nDenseAfter[2] = {0, 0};
     bool use_hybrid(int which) const {
         return hy && (sparseMode == 1 || which != BUFFER_DUALVAR);
@@ -304,7 +307,7 @@ struct hdsdp_solver_internal {
     double dErrs[6] = {0};
     bool optimized = false;
     int precision = 0;
-    int sparseSlack = 0;           // factorisation of S in PSD checks: 0 dense, -1 trial points sparse, 1 sparse
+    int sparseSlack = -1;          // factorisation of S in PSD checks: -1 trial points sparse (automatic), 0 dense, 1 sparse
     int verbose = 0;
     std::vector<hb::IterRecord> log;
     std::string modelFeatures;

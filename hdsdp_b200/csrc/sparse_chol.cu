@@ -81,6 +81,61 @@ __global__ void hy_logsum_kernel(int ne, const double *__restrict__ ldiag, doubl
     }
 }
 
+// Backward substitution through round r (rounds taken last to first):
+// u_v = (x_v - sum_a l_av u_a) / l_vv over the entries of column v.
+__global__ void hy_bwd_round_kernel(int e0, int e1, const int *__restrict__ elimv, const int *__restrict__ nptr,
+                                    const int *__restrict__ nbrv, const double *__restrict__ lval,
+                                    const double *__restrict__ ldiag, const double *__restrict__ x,
+                                    double *__restrict__ u) {
+    for (int j = e0 + blockIdx.x * blockDim.x + threadIdx.x; j < e1; j += gridDim.x * blockDim.x) {
+        const int v = elimv[j];
+        double acc = x[v];
+        for (int k = nptr[j]; k < nptr[j + 1]; ++k) acc = fma(-lval[k], u[nbrv[k]], acc);
+        u[v] = acc / ldiag[j];
+    }
+}
+
+// Forward substitution through round r: y_v = (w_v - sum over row v's entries l_vu y_u) / l_vv.
+__global__ void hy_fwd_round_kernel(int e0, int e1, const int *__restrict__ elimv, const int *__restrict__ inptr,
+                                    const int *__restrict__ inent, const int *__restrict__ colv,
+                                    const double *__restrict__ lval, const double *__restrict__ ldiag,
+                                    const double *__restrict__ w, double *__restrict__ y) {
+    for (int j = e0 + blockIdx.x * blockDim.x + threadIdx.x; j < e1; j += gridDim.x * blockDim.x) {
+        const int v = elimv[j];
+        double acc = w[v];
+        for (int q = inptr[j]; q < inptr[j + 1]; ++q) {
+            const int k = inent[q];
+            acc = fma(-lval[k], y[colv[k]], acc);
+        }
+        y[v] = acc / ldiag[j];
+    }
+}
+
+// The front's right-hand side after the rounds: z_p = w_F[p] - sum l_F[p],u y_u.
+__global__ void hy_fwd_front_kernel(int f, const int *__restrict__ front, const int *__restrict__ finptr,
+                                    const int *__restrict__ finent, const int *__restrict__ colv,
+                                    const double *__restrict__ lval, const double *__restrict__ w,
+                                    const double *__restrict__ y, double *__restrict__ z) {
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < f; p += gridDim.x * blockDim.x) {
+        double acc = w[front[p]];
+        for (int q = finptr[p]; q < finptr[p + 1]; ++q) {
+            const int k = finent[q];
+            acc = fma(-lval[k], y[colv[k]], acc);
+        }
+        z[p] = acc;
+    }
+}
+
+__global__ void hy_gather_vec_kernel(int f, const int *__restrict__ front, const double *__restrict__ x,
+                                     double *__restrict__ xf) {
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < f; p += gridDim.x * blockDim.x) xf[p] = x[front[p]];
+}
+
+__global__ void hy_scatter_vec_kernel(int f, const int *__restrict__ front, const double *__restrict__ xf,
+                                      double *__restrict__ x) {
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < f; p += gridDim.x * blockDim.x) x[front[p]] = xf[p];
+}
+
 template <class T>
 void to_device(T **d, const std::vector<T> &h) {
     HB_CUDA(hb::cmalloc(d, sizeof(T) * std::max<size_t>(h.size(), 1)));
@@ -94,7 +149,8 @@ int blocks_for(long work, int per) { return (int) std::max<long>(1, std::min<lon
 bool HybridFactor::analyse(int n_, const std::vector<std::vector<int>> &adj0, int cap, double maxFrontFrac,
                            bool force) {
     n = n_;
-    for (auto *v : {&hSrow, &hScol, &hDslot, &hNptr, &hNslot, &hTslot, &hCptr, &hCa, &hCb, &hFront, &hFixslot})
+    for (auto *v : {&hSrow, &hScol, &hDslot, &hNptr, &hNslot, &hTslot, &hCptr, &hCa, &hCb, &hFront, &hFixslot,
+                    &hNbrV, &hColV, &hElimV, &hInptr, &hInent, &hFinptr, &hFinent})
         v->clear();
     hFixpos.clear();
     std::vector<std::unordered_set<int>> A(n);
@@ -146,8 +202,13 @@ bool HybridFactor::analyse(int n_, const std::vector<std::vector<int>> &adj0, in
             std::vector<int> N(A[v].begin(), A[v].end());
             std::sort(N.begin(), N.end());
             hDslot.push_back(slot(v, v));
+            hElimV.push_back(v);
             const int base = (int) hNslot.size();
-            for (int a : N) hNslot.push_back(slot(a, v));
+            for (int a : N) {
+                hNslot.push_back(slot(a, v));
+                hNbrV.push_back(a);
+                hColV.push_back(v);
+            }
             hNptr.push_back((int) hNslot.size());
             for (size_t p = 0; p < N.size(); ++p)
                 for (size_t q = 0; q <= p; ++q) {
@@ -200,6 +261,27 @@ bool HybridFactor::analyse(int n_, const std::vector<std::vector<int>> &adj0, in
             hFixpos.push_back((long) p + (long) q * ldf);
         }
     }
+    // row structure of L: the entries of each eliminated row and of each front row, in
+    // entry order
+    std::vector<int> elimIdx(n, -1);
+    for (int j = 0; j < (int) hElimV.size(); ++j) elimIdx[hElimV[j]] = j;
+    std::vector<int> cntE(hElimV.size() + 1, 0), cntF(nfront + 1, 0);
+    for (size_t k = 0; k < hNbrV.size(); ++k) {
+        const int a = hNbrV[k];
+        if (elimIdx[a] >= 0) cntE[elimIdx[a] + 1] += 1;
+        else cntF[fidx[a] + 1] += 1;
+    }
+    for (size_t j = 0; j < hElimV.size(); ++j) cntE[j + 1] += cntE[j];
+    for (int p = 0; p < nfront; ++p) cntF[p + 1] += cntF[p];
+    hInptr = cntE;
+    hFinptr = cntF;
+    hInent.assign(cntE.back(), 0);
+    hFinent.assign(cntF.back(), 0);
+    for (size_t k = 0; k < hNbrV.size(); ++k) {
+        const int a = hNbrV[k];
+        if (elimIdx[a] >= 0) hInent[cntE[elimIdx[a]]++] = (int) k;
+        else hFinent[cntF[fidx[a]]++] = (int) k;
+    }
     nslot = (int) hSrow.size();
     nnbr = (long) hNslot.size();
     ncontrib = (long) hCa.size();
@@ -221,7 +303,15 @@ void HybridFactor::upload(cudaStream_t s) {
     to_device(&d_front, hFront);
     to_device(&d_fixslot, hFixslot);
     to_device(&d_fixpos, hFixpos);
-    for (auto *v : {&hSrow, &hScol, &hDslot, &hNptr, &hNslot, &hTslot, &hCptr, &hCa, &hCb, &hFront, &hFixslot})
+    to_device(&d_nbrv, hNbrV);
+    to_device(&d_colv, hColV);
+    to_device(&d_elimv, hElimV);
+    to_device(&d_inptr, hInptr);
+    to_device(&d_inent, hInent);
+    to_device(&d_finptr, hFinptr);
+    to_device(&d_finent, hFinent);
+    for (auto *v : {&hSrow, &hScol, &hDslot, &hNptr, &hNslot, &hTslot, &hCptr, &hCa, &hCb, &hFront, &hFixslot,
+                    &hNbrV, &hColV, &hElimV, &hInptr, &hInent, &hFinptr, &hFinent})
         std::vector<int>().swap(*v);
     std::vector<long>().swap(hFixpos);
     HB_CUDA(hb::cmalloc(&wv, sizeof(double) * std::max(nslot, 1)));
@@ -231,6 +321,8 @@ void HybridFactor::upload(cudaStream_t s) {
         HB_CUDA(hb::cmalloc(&Sf, sizeof(double) * ldf * nfront));
         HB_CUDA(cudaMemset(Sf, 0, sizeof(double) * ldf * nfront));
         Ff.alloc(nfront, 0);
+        HB_CUDA(hb::cmalloc(&fa, sizeof(double) * nfront));
+        HB_CUDA(hb::cmalloc(&fb, sizeof(double) * nfront));
     }
     HB_CUDA(hb::cmalloc(&d_info, sizeof(int)));
     HB_CUDA(hb::cmalloc_host(&h_info, sizeof(int)));
@@ -240,6 +332,7 @@ void HybridFactor::upload(cudaStream_t s) {
 }
 
 void HybridFactor::factor_async(cudaStream_t s, const double *S, long ld) {
+    ++seq;
     HB_CUDA(cudaMemsetAsync(d_info, 0, sizeof(int), s));
     HB_CUDA(cudaMemsetAsync(d_logdet, 0, sizeof(double) * 2, s));
     hy_gather_kernel<<<hb::counted(blocks_for(nslot, 256)), 256, 0, s>>>(nslot, d_srow, d_scol, S, ld, wv);
@@ -276,12 +369,47 @@ bool HybridFactor::finish(cudaStream_t s, double *logdet) {
     return ok;
 }
 
+void HybridFactor::apply_congruence(cudaStream_t s, const double *D, long ldD, double alpha, const double *x,
+                                    double *t, double *u, double *y) {
+    const int fb1 = blocks_for(nfront, 256);
+    // t = L^-T x: the front first (its block of L^-T is Kf^T), then the rounds last to first
+    if (nfront > 0) {
+        hy_gather_vec_kernel<<<hb::counted(fb1), 256, 0, s>>>(nfront, d_front, x, fa);
+        coldot(s, nfront, nfront, Ff.K, Ff.ld, fa, fb, 1.0, 0.0, 1);
+        hy_scatter_vec_kernel<<<hb::counted(fb1), 256, 0, s>>>(nfront, d_front, fb, t);
+    }
+    for (int r = nrounds - 1; r >= 0; --r) {
+        const int e0 = roundElim[r], e1 = roundElim[r + 1];
+        if (e1 > e0)
+            hy_bwd_round_kernel<<<hb::counted(blocks_for(e1 - e0, 128)), 128, 0, s>>>(e0, e1, d_elimv, d_nptr, d_nbrv,
+                                                                                    lval, ldiag, x, t);
+    }
+    // u = alpha D t
+    coldot(s, n, n, D, ldD, t, u, alpha, 0.0, 0);
+    // y = L^-1 u: the rounds first to last, then the front (its block of L^-1 is Kf)
+    for (int r = 0; r < nrounds; ++r) {
+        const int e0 = roundElim[r], e1 = roundElim[r + 1];
+        if (e1 > e0)
+            hy_fwd_round_kernel<<<hb::counted(blocks_for(e1 - e0, 128)), 128, 0, s>>>(e0, e1, d_elimv, d_inptr, d_inent,
+                                                                                    d_colv, lval, ldiag, u, y);
+    }
+    if (nfront > 0) {
+        hy_fwd_front_kernel<<<hb::counted(fb1), 256, 0, s>>>(nfront, d_front, d_finptr, d_finent, d_colv, lval, u, y, fa);
+        coldot(s, nfront, nfront, Ff.KT, Ff.ld, fa, fb, 1.0, 0.0, 2);
+        hy_scatter_vec_kernel<<<hb::counted(fb1), 256, 0, s>>>(nfront, d_front, fb, y);
+    }
+    HB_CUDA(cudaGetLastError());
+}
+
 void HybridFactor::release() {
     auto f = [](void *p) {
         if (p) hb::cache_free(p);
     };
     f(d_srow); f(d_scol); f(d_dslot); f(d_nptr); f(d_nslot); f(d_tslot); f(d_cptr); f(d_ca); f(d_cb);
     f(d_front); f(d_fixslot); f(d_fixpos); f(wv); f(lval); f(ldiag); f(Sf); f(d_info); f(d_logdet);
+    f(d_nbrv); f(d_colv); f(d_elimv); f(d_inptr); f(d_inent); f(d_finptr); f(d_finent); f(fa); f(fb);
+    d_nbrv = d_colv = d_elimv = d_inptr = d_inent = d_finptr = d_finent = nullptr;
+    fa = fb = nullptr;
     if (h_info) hb::cache_free_host(h_info);
     if (h_logdet) hb::cache_free_host(h_logdet);
     d_srow = d_scol = d_dslot = d_nptr = d_nslot = d_tslot = d_cptr = d_ca = d_cb = d_front = d_fixslot = nullptr;

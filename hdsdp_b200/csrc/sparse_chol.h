@@ -19,8 +19,10 @@
 // cooperative Cholesky. S is positive definite iff every pivot of the rounds and the
 // front factorisation is positive; log det S = 2 (sum log l_jj + sum log diag L_front).
 //
-// The factor answers positive-definiteness checks and log det only. Consumers that need
-// L itself (Lanczos, S^-1, primal recovery) run the dense factorisation of the same S.
+// The factor answers positive-definiteness checks and log det, and applies L^-1 and L^-T
+// for the Lanczos step bound (the rounds as triangular solves, the front through its
+// inverse factor). Consumers that need S^-1 or L as a matrix (the Schur build, primal
+// recovery) run the dense factorisation of the same S.
 #pragma once
 #include <vector>
 #include <cuda_runtime.h>
@@ -38,8 +40,15 @@ struct HybridFactor {
     int *d_tslot = nullptr, *d_cptr = nullptr, *d_ca = nullptr, *d_cb = nullptr;
     int *d_front = nullptr, *d_fixslot = nullptr;
     long *d_fixpos = nullptr;
+    // triangular solves: per entry its row and column vertex, per eliminated index its
+    // vertex, and the entries of each eliminated row / front row (row structure of L)
+    int *d_nbrv = nullptr, *d_colv = nullptr, *d_elimv = nullptr;
+    int *d_inptr = nullptr, *d_inent = nullptr, *d_finptr = nullptr, *d_finent = nullptr;
+    double *fa = nullptr, *fb = nullptr;  // front-length work vectors
+    long seq = 0;                         // numeric factorisations done (identifies the held factor)
     // host symbolic data, held from analyse() to upload()
     std::vector<int> hSrow, hScol, hDslot, hNptr, hNslot, hTslot, hCptr, hCa, hCb, hFront, hFixslot;
+    std::vector<int> hNbrV, hColV, hElimV, hInptr, hInent, hFinptr, hFinent;
     std::vector<long> hFixpos;
     // numeric workspace
     double *wv = nullptr, *lval = nullptr, *ldiag = nullptr, *Sf = nullptr;
@@ -57,6 +66,11 @@ struct HybridFactor {
     void factor_async(cudaStream_t s, const double *S, long ld);
     // Wait for it: true iff S is positive definite; logdet = log det S when it is.
     bool finish(cudaStream_t s, double *logdet);
+    // y = L^-1 (alpha D) L^-T x for the held factor (D dense n x n, vectors of length n in
+    // the original order; t is an n-vector of scratch). The front's inverse factor must
+    // have been formed (compute_inverse_factor(s, Ff)).
+    void apply_congruence(cudaStream_t s, const double *D, long ldD, double alpha, const double *x, double *t,
+                          double *u, double *y);
     void release();
 };
 

@@ -30,14 +30,13 @@ extern void HDSDPSetPrimalRefinement( hdsdp *HSolver, int on );
    2 = split precision while the relative gap is above 1e-3, FP64 after. */
 extern void HDSDPSetPrecision( hdsdp *HSolver, int mode );
 
-/* Factorisation of the dual slack S for positive-definiteness checks and log det:
-   0 = always the dense cooperative Cholesky (default); -1 = a sparse factorisation
-   (minimum-degree rounds on the device and a dense front) for the trial points of
-   blocks of order >= 1500 whose front is at most 70% of the order, the dense Cholesky
-   for the accepted point, whose factor the step bound and the Schur build use;
-   1 = sparse for every check whenever the pattern allows it. A consumer of L (the
-   Lanczos step bound, S^-1, primal recovery) refactors densely when its buffer was
-   factored sparsely. This is where the reference uses Pardiso for sparse dual
+/* Factorisation of the dual slack S for positive-definiteness checks, log det and the
+   Lanczos step bound: -1 = automatic (default): a sparse factorisation (minimum-degree
+   rounds on the device and a dense front) for the trial points of blocks of order
+   >= 1500 whose front is at most 70% of the order, the dense Cholesky for the accepted
+   point, whose S^-1 the Schur build uses; 0 = always the dense cooperative Cholesky;
+   1 = sparse for every check whenever the pattern allows it. S^-1 and primal recovery
+   refactor densely when their buffer was factored sparsely. This is where the reference uses Pardiso for sparse dual
    matrices (interface/hdsdp_conic_sdp.c:153-275). Takes effect at the next
    HDSDPOptimize. */
 extern void HDSDPSetSparseSlack( hdsdp *HSolver, int mode );
@@ -186,6 +185,13 @@ extern int hdsdpb_sparse_analyse( int n, int nedge, const int *ei, const int *ej
    Returns 0, or -1 for invalid input. */
 extern int hdsdpb_sparse_cholesky( int n, int nedge, const int *ei, const int *ej, const double *S, int cap,
                                    int reps, double out[5] );
+
+/* With the sparse factor S = L L^T (pattern as above, cap 64): t = L^-T x and
+   y = L^-1 (D t) for a host n x n D and n-vector x (t may be NULL). The operator the
+   Lanczos step bound uses with D = -dS. Returns 0, 1 if S is not positive definite,
+   -1 for invalid input. */
+extern int hdsdpb_sparse_congruence( int n, int nedge, const int *ei, const int *ej, const double *S,
+                                     const double *D, const double *x, double *y, double *t );
 
 /* Milliseconds taken by `reps` grid-wide barriers in one cooperative launch of
    `blocks` blocks of 256 threads (cost model of the persistent factorisation). */

@@ -118,3 +118,35 @@ def test_multiblock_with_sparse_slack(gpu_lib, golden):
     prob = instances.multiblock_case("mb4_n500")
     r = api.solve_problem(prob, sparse_slack=1)
     check_parity(r, golden["multiblock_solves"]["mb4_n500"])
+
+
+def test_sparse_congruence(gpu_lib):
+    """The Lanczos operator on the sparse factor: with D = S it is the identity, t = L^-T x
+    satisfies t^T S t = x^T x, and with D = -dS its spectrum is that of the pencil
+    (-dS, S), the same as through the dense factor."""
+    L = _lib.load()
+    rng = np.random.default_rng(2)
+    for n, m_edges in ((600, 2400), (200, 600)):
+        ei, ej, w = random_graph(n, m_edges, seed=n)
+        S = laplacian(n, ei, ej, w) + 0.7 * np.eye(n)
+        Sf = np.asfortranarray(S)
+        x = rng.standard_normal(n)
+        y, t = np.zeros(n), np.zeros(n)
+        assert L.hdsdpb_sparse_congruence(n, len(ei), _ip(ei), _ip(ej), _dp(Sf), _dp(Sf), _dp(x), _dp(y), _dp(t)) == 0
+        np.testing.assert_allclose(y, x, rtol=0, atol=1e-11 * np.abs(x).max())
+        assert t @ S @ t == pytest.approx(x @ x, rel=1e-12)
+    # n = 200: the whole operator for D = -dS, against Lc^-1 (-dS) Lc^-T of the dense factor
+    dS = laplacian(n, ei, ej, rng.uniform(-1, 1, len(ei))) + np.diag(rng.uniform(-1, 1, n))
+    D = np.asfortranarray(-dS)
+    T = np.zeros((n, n))
+    e = np.zeros(n)
+    for k in range(n):
+        e[:] = 0.0
+        e[k] = 1.0
+        assert L.hdsdpb_sparse_congruence(n, len(ei), _ip(ei), _ip(ej), _dp(Sf), _dp(D), _dp(e), _dp(y), None) == 0
+        T[:, k] = y
+    Lc = np.linalg.cholesky(S)
+    Tref = np.linalg.solve(Lc, np.linalg.solve(Lc, D).T).T
+    np.testing.assert_allclose(T, T.T, atol=1e-10 * np.abs(T).max())
+    np.testing.assert_allclose(np.linalg.eigvalsh(0.5 * (T + T.T)), np.linalg.eigvalsh(0.5 * (Tref + Tref.T)),
+                               atol=1e-10 * np.abs(Tref).max())
