@@ -1145,6 +1145,143 @@ __global__ void lanczos_resid_kernel(int n, double *z, const double *x, double l
     if (threadIdx.x == 0) *out = v;
 }
 
+// ---- Lanczos for blocks of order <= kSmallLanczosN: one CTA holds K = L^-1, D and the
+// Lanczos basis in shared memory and runs every step in one launch (the stepwise path
+// spends four launches per step, which dominates for small blocks).
+constexpr int kSmallLanczosN = 96;
+
+__host__ __device__ inline int small_ld(int n) { return n | 1; }  // odd stride: fewer bank conflicts
+
+inline size_t small_lanczos_smem(int n, int maxdim) {
+    return sizeof(double) * ((size_t) 2 * n * small_ld(n) + (size_t) (maxdim + 1) * n + 4 * (size_t) n);
+}
+
+// K (lower, leading dimension ldk) and D into shared memory (leading dimension small_ld(n))
+__device__ void small_load(int n, const double *K, long ldk, const double *D, long ldD, double *sK, double *sD) {
+    const int ls = small_ld(n);
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+        const int i = e % n, j = e / n;
+        sK[i + j * ls] = (i >= j) ? K[(size_t) i + (size_t) j * ldk] : 0.0;
+        sD[i + j * ls] = D[(size_t) i + (size_t) j * ldD];
+    }
+    __syncthreads();
+}
+
+// y = K (-D) (K^T x), one warp per output entry
+__device__ void small_mv(int n, const double *sK, const double *sD, const double *x, double *t, double *u,
+                         double *y) {
+    const int ls = small_ld(n), lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int i = warp; i < n; i += nw) {  // t = K^T x
+        double a = 0.0;
+        for (int k = i + lane; k < n; k += 32) a += sK[k + i * ls] * x[k];
+        for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+        if (lane == 0) t[i] = a;
+    }
+    __syncthreads();
+    for (int i = warp; i < n; i += nw) {  // u = -D t
+        double a = 0.0;
+        for (int k = lane; k < n; k += 32) a += sD[k + i * ls] * t[k];
+        for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+        if (lane == 0) u[i] = -a;
+    }
+    __syncthreads();
+    for (int i = warp; i < n; i += nw) {  // y = K u
+        double a = 0.0;
+        for (int k = lane; k <= i; k += 32) a += sK[i + k * ls] * u[k];
+        for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+        if (lane == 0) y[i] = a;
+    }
+    __syncthreads();
+}
+
+// Start vector v0 = normalise(a + b) (a may be null), then maxdim steps of the
+// three-term recurrence exactly as lanczos_orth_kernel takes them; the basis V (all
+// maxdim + 1 columns, zero past a breakdown) and alpha / beta go to global memory.
+__global__ void lanczos_small_kernel(int n, const double *K, long ldk, const double *D, long ldD, const double *a,
+                                     const double *b, double *V, long ldv, double *ab, int maxdim) {
+    extern __shared__ double sm[];
+    const int ls = small_ld(n);
+    double *sK = sm, *sD = sK + (size_t) n * ls, *sV = sD + (size_t) n * ls, *w = sV + (size_t) (maxdim + 1) * n;
+    double *t = w + n, *u = t + n, *sab = u + n;  // sab: 2 * maxdim + 2 <= 4n is not guaranteed: kept in ab
+    (void) sab;
+    small_load(n, K, ldk, D, ldD, sK, sD);
+    for (int e = threadIdx.x; e < (maxdim + 1) * n; e += blockDim.x) sV[e] = 0.0;
+    for (int e = threadIdx.x; e < 2 * maxdim + 2; e += blockDim.x) ab[e] = 0.0;
+    __syncthreads();
+    double acc = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const double x = (a ? a[i] : 0.0) + b[i];
+        sV[i] = x;
+        acc += x * x;
+    }
+    double nrm = sqrt(bsum(acc));
+    for (int i = threadIdx.x; i < n; i += blockDim.x) sV[i] = (nrm > 0.0) ? sV[i] / nrm : 0.0;
+    __syncthreads();
+    double betaPrev = 0.0;
+    for (int k = 0; k < maxdim; ++k) {
+        const double *vk = sV + (size_t) k * n;
+        small_mv(n, sK, sD, vk, t, u, w);
+        if (k > 0) {
+            const double *vp = sV + (size_t) (k - 1) * n;
+            for (int i = threadIdx.x; i < n; i += blockDim.x) w[i] -= betaPrev * vp[i];
+            __syncthreads();
+        }
+        acc = 0.0;
+        for (int i = threadIdx.x; i < n; i += blockDim.x) acc += w[i] * vk[i];
+        const double alp = bsum(acc);
+        acc = 0.0;
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            const double x = w[i] - alp * vk[i];
+            w[i] = x;
+            acc += x * x;
+        }
+        nrm = sqrt(bsum(acc));
+        if (threadIdx.x == 0) ab[k] = alp;
+        betaPrev = 0.0;
+        if (nrm > 0.0) {
+            double *vn = sV + (size_t) (k + 1) * n;
+            for (int i = threadIdx.x; i < n; i += blockDim.x) vn[i] = w[i] / nrm;
+            if (threadIdx.x == 0) ab[maxdim + k] = nrm;
+            betaPrev = nrm;
+        }
+        __syncthreads();
+    }
+    for (int e = threadIdx.x; e < (maxdim + 1) * n; e += blockDim.x) {
+        const int i = e % n, j = e / n;
+        V[(size_t) i + (size_t) j * ldv] = sV[e];
+    }
+}
+
+// The Ritz part of a converged check: z1 = V y1, z2 = M z1 (warm <- z2),
+// out[0] = |z2 - lam z1|; z2 = V y2, z1 = M z2, out[1] = |z1 - lam z2|.
+__global__ void lanczos_small_ritz_kernel(int n, const double *K, long ldk, const double *D, long ldD,
+                                          const double *V, long ldv, int kp1, const double *y, double lam,
+                                          double *warm, double *out) {
+    extern __shared__ double sm[];
+    const int ls = small_ld(n);
+    double *sK = sm, *sD = sK + (size_t) n * ls, *z1 = sD + (size_t) n * ls, *z2 = z1 + n, *t = z2 + n, *u = t + n;
+    small_load(n, K, ldk, D, ldD, sK, sD);
+    for (int pass = 0; pass < 2; ++pass) {
+        const double *yc = y + pass * kp1;
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            double a = 0.0;
+            for (int j = 0; j < kp1; ++j) a += V[(size_t) i + (size_t) j * ldv] * yc[j];
+            z1[i] = a;
+        }
+        __syncthreads();
+        small_mv(n, sK, sD, z1, t, u, z2);
+        double acc = 0.0;
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            if (pass == 0) warm[i] = z2[i];
+            const double r = z2[i] - lam * z1[i];
+            acc += r * r;
+        }
+        const double v = sqrt(bsum(acc));
+        if (threadIdx.x == 0) out[pass] = v;
+        __syncthreads();
+    }
+}
+
 // All eigenpairs of the symmetric tridiagonal matrix with diagonal d[0..n) and
 // off-diagonal e[0..n-1): QL iteration with implicit Wilkinson shifts, rotations
 // accumulated into Z (column-major n x n, columns are eigenvectors).
@@ -1266,10 +1403,32 @@ hdsdp_retcode Lanczos::solve(DenseFactor &F, const double *D, long ldD, double *
         }
         if (tm) tm->n_lanczos_mv += 1;
     };
-    HB_CUDA(cudaMemsetAsync(V, 0, sizeof(double) * ld * (maxdim + 1), s));
-    HB_CUDA(cudaMemsetAsync(d_ab, 0, sizeof(double) * (2 * maxdim + 2), s));
-    if (nComputed == 0) lanczos_start_kernel<<<hb::counted(1), 1024, 0, s>>>(n, nullptr, init_vec, V);
-    else lanczos_start_kernel<<<hb::counted(1), 1024, 0, s>>>(n, warm, pert_vec, V);
+    // small blocks: every step in one launch, then the checks below replay the schedule on
+    // the recorded alpha / beta (a step's values do not depend on later steps)
+    const bool small = !hyOp && n <= kSmallLanczosN;
+    if (small) {
+        static bool attr = false;
+        if (!attr) {
+            const int bytes = (int) small_lanczos_smem(kSmallLanczosN, 30);
+            HB_CUDA(cudaFuncSetAttribute((const void *) lanczos_small_kernel,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+            HB_CUDA(cudaFuncSetAttribute((const void *) lanczos_small_ritz_kernel,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+            attr = true;
+        }
+        lanczos_small_kernel<<<hb::counted(1), 256, small_lanczos_smem(n, maxdim), s>>>(
+            n, F.K, F.ld, D, ldD, nComputed == 0 ? nullptr : warm, nComputed == 0 ? init_vec : pert_vec, V, ld, d_ab,
+            maxdim);
+        HB_CUDA(cudaGetLastError());
+        HB_CUDA(cudaMemcpyAsync(h_ab, d_ab, sizeof(double) * (2 * maxdim + 2), cudaMemcpyDeviceToHost, s));
+        HB_CUDA(cudaStreamSynchronize(s));
+        if (tm) tm->n_lanczos_mv += maxdim;
+    } else {
+        HB_CUDA(cudaMemsetAsync(V, 0, sizeof(double) * ld * (maxdim + 1), s));
+        HB_CUDA(cudaMemsetAsync(d_ab, 0, sizeof(double) * (2 * maxdim + 2), s));
+        if (nComputed == 0) lanczos_start_kernel<<<hb::counted(1), 1024, 0, s>>>(n, nullptr, init_vec, V);
+        else lanczos_start_kernel<<<hb::counted(1), 1024, 0, s>>>(n, warm, pert_vec, V);
+    }
 
     hdsdp_retcode ret = HDSDP_RETCODE_OK;
     bool done = false;
@@ -1277,14 +1436,18 @@ hdsdp_retcode Lanczos::solve(DenseFactor &F, const double *D, long ldD, double *
     const int freq = std::min(maxdim / 5, 3);
     std::vector<double> T, ev, evec;
     for (int k = 0; k < maxdim && !done; ++k) {
-        mv(V + (size_t) k * ld, w);
-        lanczos_orth_kernel<<<hb::counted(1), 1024, 0, s>>>(n, V, ld, k, w, d_ab, maxdim);
+        if (!small) {
+            mv(V + (size_t) k * ld, w);
+            lanczos_orth_kernel<<<hb::counted(1), 1024, 0, s>>>(n, V, ld, k, w, d_ab, maxdim);
+        }
         const bool sched = ((k + 1) % freq == 0) || k >= maxdim - 1;
         if (!sched) continue;
-        HB_CUDA(cudaMemcpyAsync(h_ab, d_ab, sizeof(double) * (2 * maxdim + 2), cudaMemcpyDeviceToHost, s));
-        double tw = wall();
-        HB_CUDA(cudaStreamSynchronize(s));
-        if (tm) tm->lz_wait += wall() - tw;
+        if (!small) {
+            HB_CUDA(cudaMemcpyAsync(h_ab, d_ab, sizeof(double) * (2 * maxdim + 2), cudaMemcpyDeviceToHost, s));
+            double tw = wall();
+            HB_CUDA(cudaStreamSynchronize(s));
+            if (tm) tm->lz_wait += wall() - tw;
+        }
         double th = wall();
         // The reference also checks as soon as a step breaks down (zero norm).
         int kc = k;
@@ -1319,13 +1482,20 @@ hdsdp_retcode Lanczos::solve(DenseFactor &F, const double *D, long ldD, double *
             yy[kp1 + i] = evec[(size_t) i + (size_t) i2 * kp1];
         }
         HB_CUDA(cudaMemcpyAsync(d_y, yy.data(), sizeof(double) * 2 * kp1, cudaMemcpyHostToDevice, s));
-        lanczos_combine_kernel<<<hb::counted((n + 255) / 256), 256, 0, s>>>(n, V, ld, kp1, d_y, z1);
-        mv(z1, z2);
-        HB_CUDA(cudaMemcpyAsync(warm, z2, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
-        lanczos_resid_kernel<<<hb::counted(1), 1024, 0, s>>>(n, z2, z1, eigMin1, d_scal);
-        lanczos_combine_kernel<<<hb::counted((n + 255) / 256), 256, 0, s>>>(n, V, ld, kp1, d_y + kp1, z2);
-        mv(z2, z1);
-        lanczos_resid_kernel<<<hb::counted(1), 1024, 0, s>>>(n, z1, z2, eigMin1, d_scal + 1);
+        if (small) {
+            lanczos_small_ritz_kernel<<<hb::counted(1), 256, small_lanczos_smem(n, maxdim), s>>>(
+                n, F.K, F.ld, D, ldD, V, ld, kp1, d_y, eigMin1, warm, d_scal);
+            HB_CUDA(cudaGetLastError());
+            if (tm) tm->n_lanczos_mv += 2;
+        } else {
+            lanczos_combine_kernel<<<hb::counted((n + 255) / 256), 256, 0, s>>>(n, V, ld, kp1, d_y, z1);
+            mv(z1, z2);
+            HB_CUDA(cudaMemcpyAsync(warm, z2, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+            lanczos_resid_kernel<<<hb::counted(1), 1024, 0, s>>>(n, z2, z1, eigMin1, d_scal);
+            lanczos_combine_kernel<<<hb::counted((n + 255) / 256), 256, 0, s>>>(n, V, ld, kp1, d_y + kp1, z2);
+            mv(z2, z1);
+            lanczos_resid_kernel<<<hb::counted(1), 1024, 0, s>>>(n, z1, z2, eigMin1, d_scal + 1);
+        }
         HB_CUDA(cudaMemcpyAsync(h_scal, d_scal, sizeof(double) * 2, cudaMemcpyDeviceToHost, s));
         HB_CUDA(cudaStreamSynchronize(s));
         const double resiVal1 = h_scal[0], resiVal2 = h_scal[1];
