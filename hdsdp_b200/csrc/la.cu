@@ -1092,9 +1092,19 @@ void scale_columns(cudaStream_t s, int rows, int cols, const double *A, long lda
 }
 
 void frob_dot(cudaStream_t s, int n, const double *A, long lda, const double *B, long ldb, double *d_out) {
-    static double *part = nullptr;
+    // partial sums in a buffer of the stream's own: solver objects on different streams
+    // (one per host thread) must not share it
+    static std::mutex mu;
+    static std::unordered_map<cudaStream_t, double *> parts;
     const int np = 296;
-    if (!part) HB_CUDA(hb::cmalloc(&part, sizeof(double) * np));
+    double *part = nullptr;
+    {
+        std::lock_guard<std::mutex> g(mu);
+        double *&p = parts[s];
+        if (!p) HB_CUDA(hb::cmalloc(&p, sizeof(double) * np));
+        part = p;
+    }
+    if (!part) return;
     frob_partial_kernel<<<hb::counted(np), 256, 0, s>>>(n, A, lda, B, ldb, part);
     sum_partials_kernel<<<hb::counted(1), 512, 0, s>>>(np, part, d_out);
 }
