@@ -174,26 +174,3 @@ def test_multiblock_sdpa_solve(gpu_lib, tmp_path, golden):
     r = api.solve_problem(api.sdpa_cones(path))
     check_parity(r, golden["multiblock_solves"]["mb2_lp"])
 
-
-def test_concurrent_solvers(gpu_lib):
-    """Solver objects in different host threads (one CUDA stream each) run at the same time
-    and give the results they give alone (the library shares no mutable device scratch
-    between streams)."""
-    import threading
-    names = ["maxcut60", "theta40", "rank1_50_80", "maxcut60"]
-    alone = {n: api.solve(SMALL[n](), want_x=False, primal_refinement=False) for n in set(names)}
-    out = [None] * len(names)
-
-    def run(i, name):
-        out[i] = api.solve(SMALL[name](), want_x=False, primal_refinement=False)
-
-    threads = [threading.Thread(target=run, args=(i, nm)) for i, nm in enumerate(names)]
-    for t in threads:
-        t.start()
-    for t in threads:
-        t.join()
-    for nm, r in zip(names, out):
-        a = alone[nm]
-        assert r["status_after_check"] == a["status_after_check"] and r["iters"] == a["iters"]
-        assert r["dobj"] == a["dobj"] and r["pobj"] == a["pobj"]
-        np.testing.assert_array_equal(r["errs"], a["errs"])
