@@ -3,6 +3,7 @@
 #include "sparse_chol.h"
 #include "dev.cuh"
 #include <algorithm>
+#include <iterator>
 #include <cmath>
 #include <unordered_map>
 #include <unordered_set>
@@ -153,19 +154,43 @@ bool HybridFactor::analyse(int n_, const std::vector<std::vector<int>> &adj0, in
                     &hNbrV, &hColV, &hElimV, &hInptr, &hInent, &hFinptr, &hFinent})
         v->clear();
     hFixpos.clear();
-    std::vector<std::unordered_set<int>> A(n);
-    for (int v = 0; v < n; ++v) A[v].insert(adj0[v].begin(), adj0[v].end());
+    // adjacency as sorted vectors; eliminating v turns its neighbours into a clique
+    std::vector<std::vector<int>> A(adj0);
     std::vector<char> alive(n, 1), mark(n, 0);
-    std::unordered_map<long long, int> slotOf;
+    // slot of the entry (a, b), a >= b: open addressing on the key a * n + b
+    std::vector<long long> hkey((size_t) 1 << 16, -1);
+    std::vector<int> hval(hkey.size());
+    size_t hmask = hkey.size() - 1;
+    auto hpos = [&](long long key) {
+        size_t h = (size_t) ((unsigned long long) key * 0x9E3779B97F4A7C15ull >> 20) & hmask;
+        while (hkey[h] != -1 && hkey[h] != key) h = (h + 1) & hmask;
+        return h;
+    };
     auto slot = [&](int a, int b) {
         if (a < b) std::swap(a, b);
         const long long key = (long long) a * n + b;
-        auto it = slotOf.find(key);
-        if (it != slotOf.end()) return it->second;
+        size_t h = hpos(key);
+        if (hkey[h] == key) return hval[h];
         const int s = (int) hSrow.size();
-        slotOf.emplace(key, s);
         hSrow.push_back(a);
         hScol.push_back(b);
+        hkey[h] = key;
+        hval[h] = s;
+        if (2 * hSrow.size() > hkey.size()) {  // keep the load below one half
+            std::vector<long long> ok;
+            std::vector<int> ov;
+            ok.swap(hkey);
+            ov.swap(hval);
+            hkey.assign(ok.size() * 2, -1);
+            hval.assign(hkey.size(), 0);
+            hmask = hkey.size() - 1;
+            for (size_t i = 0; i < ok.size(); ++i)
+                if (ok[i] != -1) {
+                    const size_t g = hpos(ok[i]);
+                    hkey[g] = ok[i];
+                    hval[g] = ov[i];
+                }
+        }
         return s;
     };
     hNptr.push_back(0);
@@ -174,6 +199,9 @@ bool HybridFactor::analyse(int n_, const std::vector<std::vector<int>> &adj0, in
     roundTgt.assign(1, 0);
     const long maxContrib = 64L << 20;
     std::vector<std::pair<int, int>> order;
+    std::vector<int> tmp, N;
+    std::vector<int> tgtStamp, tgtLocal;  // per slot: round that made it a target, its index there
+    std::vector<int> tgtSlot, tri;        // tri: (local target, entry a, entry b) per contribution
     while (true) {
         order.clear();
         for (int v = 0; v < n; ++v)
@@ -195,12 +223,11 @@ bool HybridFactor::analyse(int n_, const std::vector<std::vector<int>> &adj0, in
         }
         // the round's columns and Schur updates; the picked set is independent, so one
         // column's elimination does not change another's neighbours
-        std::unordered_map<long long, int> tgtOf;
-        std::vector<std::vector<std::pair<int, int>>> contrib;
-        std::vector<int> tgtSlot;
+        const int round = (int) roundElim.size();
+        tgtSlot.clear();
+        tri.clear();
         for (int v : picked) {
-            std::vector<int> N(A[v].begin(), A[v].end());
-            std::sort(N.begin(), N.end());
+            N = A[v];  // sorted
             hDslot.push_back(slot(v, v));
             hElimV.push_back(v);
             const int base = (int) hNslot.size();
@@ -212,34 +239,48 @@ bool HybridFactor::analyse(int n_, const std::vector<std::vector<int>> &adj0, in
             hNptr.push_back((int) hNslot.size());
             for (size_t p = 0; p < N.size(); ++p)
                 for (size_t q = 0; q <= p; ++q) {
-                    const long long key = (long long) N[p] * n + N[q];
-                    auto it = tgtOf.find(key);
-                    int t;
-                    if (it == tgtOf.end()) {
-                        t = (int) contrib.size();
-                        tgtOf.emplace(key, t);
-                        contrib.emplace_back();
-                        tgtSlot.push_back(slot(N[p], N[q]));
-                    } else {
-                        t = it->second;
+                    const int sl = slot(N[p], N[q]);
+                    if ((size_t) sl >= tgtStamp.size()) {
+                        tgtStamp.resize(2 * (size_t) sl + 16, 0);
+                        tgtLocal.resize(tgtStamp.size(), 0);
                     }
-                    contrib[t].push_back({base + (int) p, base + (int) q});
+                    if (tgtStamp[sl] != round) {
+                        tgtStamp[sl] = round;
+                        tgtLocal[sl] = (int) tgtSlot.size();
+                        tgtSlot.push_back(sl);
+                    }
+                    const int t = tgtLocal[sl];
+                    tri.push_back(t);
+                    tri.push_back(base + (int) p);
+                    tri.push_back(base + (int) q);
                 }
             for (int u : N) {
-                A[u].erase(v);
-                for (int w : N)
-                    if (w != u) A[u].insert(w);
+                tmp.clear();
+                std::set_union(A[u].begin(), A[u].end(), N.begin(), N.end(), std::back_inserter(tmp));
+                tmp.erase(std::remove_if(tmp.begin(), tmp.end(), [&](int w) { return w == u || w == v; }),
+                          tmp.end());
+                A[u].swap(tmp);
             }
-            A[v].clear();
+            std::vector<int>().swap(A[v]);
             alive[v] = 0;
         }
-        for (size_t t = 0; t < contrib.size(); ++t) {
+        // contributions grouped by target (counting sort, insertion order kept)
+        const int nt = (int) tgtSlot.size();
+        std::vector<int> cnt(nt + 1, 0);
+        for (size_t c = 0; c < tri.size(); c += 3) cnt[tri[c] + 1] += 1;
+        for (int t = 0; t < nt; ++t) cnt[t + 1] += cnt[t];
+        const size_t c0 = hCa.size();
+        hCa.resize(c0 + tri.size() / 3);
+        hCb.resize(c0 + tri.size() / 3);
+        std::vector<int> cur(cnt.begin(), cnt.end() - 1);
+        for (size_t c = 0; c < tri.size(); c += 3) {
+            const int at = cur[tri[c]]++;
+            hCa[c0 + at] = tri[c + 1];
+            hCb[c0 + at] = tri[c + 2];
+        }
+        for (int t = 0; t < nt; ++t) {
             hTslot.push_back(tgtSlot[t]);
-            for (const auto &c : contrib[t]) {
-                hCa.push_back(c.first);
-                hCb.push_back(c.second);
-            }
-            hCptr.push_back((int) hCa.size());
+            hCptr.push_back((int) (c0 + cnt[t + 1]));
         }
         roundElim.push_back(roundElim.back() + (int) picked.size());
         roundTgt.push_back((int) hTslot.size());
