@@ -581,7 +581,7 @@ hdsdp_retcode SdpCone::ratio_test(double dtau, const double *dy, double ada, int
         lz.hyOp = nullptr;
         return r;
     }
-    if (!ensure_dense(var ? BUFFER_DUALVAR : BUFFER_DUALCHECK)) return HDSDP_RETCODE_FAILED;
+    if (hy && !ensure_dense(var ? BUFFER_DUALVAR : BUFFER_DUALCHECK)) return HDSDP_RETCODE_FAILED;
     return lz.solve(F, dS, ld, step, tm);
 }
 
@@ -646,7 +646,7 @@ void SdpCone::get_primal(double mu, const double *y, const double *dy, double *X
         printf("Recovery step is infeasible\n");
         return;
     }
-    if (!ensure_dense(BUFFER_DUALCHECK)) {
+    if (hy && !ensure_dense(BUFFER_DUALCHECK)) {
         printf("Recovery step is infeasible\n");
         return;
     }
@@ -867,7 +867,7 @@ hdsdp_retcode KKT::add_sdp(SdpCone &cone, int type) {
         if (!primalX) return HDSDP_RETCODE_FAILED;
         Wp = primalX;
     } else {
-        if (!cone.ensure_dense(BUFFER_DUALVAR)) return HDSDP_RETCODE_FAILED;
+        if (cone.hy && !cone.ensure_dense(BUFFER_DUALVAR)) return HDSDP_RETCODE_FAILED;
         double ti = wall();
         // split precision: W = K^T K on the tensor cores once n makes the product worth it
         bool done = false;

@@ -5,8 +5,6 @@
 #include <algorithm>
 #include <iterator>
 #include <cmath>
-#include <unordered_map>
-#include <unordered_set>
 #include <utility>
 
 namespace hb {
