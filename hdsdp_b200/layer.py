@@ -1,6 +1,6 @@
 """Differentiable SDP layer: torch.autograd.Function over the C ABI.
 
-Forward solves one dense SDP block (data given as the reference's CSC layout:
+Forward solves a problem of one dense SDP block (data given as the reference's CSC layout:
 column 0 is C, columns 1..m the A_i, packed lower-triangle rows) through
 HDSDPOptimize and returns (y*, X*). Backward calls HDSDPAdjoint, which
 differentiates the optimality conditions at the final iterate on the GPU and

@@ -8,8 +8,8 @@
  * block, returned as a CSC matrix with nLPCols rows and nConstrs + 1 columns. Each SDP
  * block is a CSC matrix with PACK_NNZ(n) rows (packed lower triangle) and nConstrs + 1
  * columns, column 0 being the objective matrix with its sign flipped, the form that
- * HUserDataSetConeData takes. The solver in this library runs one SDP block without an
- * LP block.
+ * HUserDataSetConeData takes: each SDP block becomes one cone (HDSDP_CONETYPE_DENSE_SDP
+ * user data) and the LP block one LP cone (HDSDP_CONETYPE_LP user data).
  */
 #ifndef HDSDP_FILE_IO_H
 #define HDSDP_FILE_IO_H
