@@ -167,3 +167,67 @@ def test_numeric_scheme(shift, pd):
     assert ok == pd == (sign > 0 and np.linalg.eigvalsh(S)[0] > 0)
     if pd:
         assert logdet == pytest.approx(ref, rel=1e-12)
+
+
+def hybrid_factor(S, rounds, front):
+    """The numbers the device factor holds: per eliminated vertex l_vv and its column
+    entries (l_av for a in N(v)), and the front's dense Cholesky factor."""
+    W = S.copy()
+    cols = {}
+    for rnd in rounds:
+        lv = []
+        for v, N in rnd:
+            l = np.sqrt(W[v, v])
+            x = W[N, v] / l
+            cols[v] = (l, N, x)
+            lv.append((N, x))
+        for N, x in lv:
+            W[np.ix_(N, N)] -= np.outer(x, x)
+    Lf = np.linalg.cholesky(W[np.ix_(front, front)]) if front else np.zeros((0, 0))
+    return cols, Lf
+
+
+def congruence(D, x, rounds, front, cols, Lf):
+    """y = L^-1 D L^-T x in the original order, the way the device applies it: L^-T by the
+    front and then the rounds last to first, L^-1 by the rounds first to last and then the
+    front."""
+    n = len(x)
+    t = np.zeros(n)
+    if front:
+        t[front] = np.linalg.solve(Lf.T, x[front])
+    for rnd in reversed(rounds):
+        for v, _ in rnd:
+            l, N, lv = cols[v]
+            t[v] = (x[v] - lv @ t[N]) / l
+    w = D @ t
+    y = np.zeros(n)
+    rem = w.copy()
+    for rnd in rounds:
+        for v, _ in rnd:
+            l, N, lv = cols[v]
+            y[v] = rem[v] / l
+        for v, _ in rnd:  # the round's columns pushed into the rows below them
+            l, N, lv = cols[v]
+            rem[N] -= lv * y[v]
+    if front:
+        y[front] = np.linalg.solve(Lf, rem[front])
+    return t, y
+
+
+@pytest.mark.parametrize("m_edges", [900, 300, 4000])
+def test_congruence_scheme(m_edges):
+    """With D = S the operator is the identity, and t = L^-T x has t^T S t = x^T x."""
+    n = 300
+    ei, ej, adj = graph(n, m_edges, seed=m_edges)
+    rng = np.random.default_rng(3)
+    w = rng.uniform(0.5, 1.5, len(ei))
+    S = np.zeros((n, n))
+    S[ei, ej] = -w
+    S[ej, ei] = -w
+    S[np.arange(n), np.arange(n)] = -S.sum(axis=1) + 0.5
+    rounds, front = mmd_rounds(n, adj, 64)
+    cols, Lf = hybrid_factor(S, rounds, front)
+    x = rng.standard_normal(n)
+    t, y = congruence(S, x, rounds, front, cols, Lf)
+    np.testing.assert_allclose(y, x, atol=1e-10 * np.abs(x).max())
+    assert t @ S @ t == pytest.approx(x @ x, rel=1e-11)
