@@ -150,3 +150,30 @@ def test_sparse_congruence(gpu_lib):
     np.testing.assert_allclose(T, T.T, atol=1e-10 * np.abs(T).max())
     np.testing.assert_allclose(np.linalg.eigvalsh(0.5 * (T + T.T)), np.linalg.eigvalsh(0.5 * (Tref + Tref.T)),
                                atol=1e-10 * np.abs(Tref).max())
+
+
+@pytest.mark.parametrize("kind", ["tree", "dense"])
+def test_sparse_cholesky_edge_patterns(gpu_lib, kind):
+    """A tree pattern is eliminated completely (no dense front); a dense pattern (degrees
+    above the cap) eliminates nothing and the front is the whole matrix."""
+    n = 300
+    if kind == "tree":
+        rng = np.random.default_rng(4)
+        ei = np.arange(1, n, dtype=np.int32)
+        ej = np.array([rng.integers(0, i) for i in range(1, n)], dtype=np.int32)
+    else:
+        ei, ej, _ = random_graph(n, n * 80, seed=9)
+    w = np.random.default_rng(5).uniform(0.5, 1.5, len(ei))
+    S = laplacian(n, ei, ej, w) + 0.3 * np.eye(n)
+    out = sparse_cholesky(S, ei, ej, reps=2)
+    sign, ref = np.linalg.slogdet(S)
+    assert out[0] == 1.0 and sign > 0
+    assert out[1] == pytest.approx(ref, rel=1e-11)
+    assert out[4] == (0 if kind == "tree" else n)
+    L = _lib.load()
+    x = np.random.default_rng(6).standard_normal(n)
+    y, t = np.zeros(n), np.zeros(n)
+    Sf = np.asfortranarray(S)
+    assert L.hdsdpb_sparse_congruence(n, len(ei), _ip(ei), _ip(ej), _dp(Sf), _dp(Sf), _dp(x), _dp(y), _dp(t)) == 0
+    np.testing.assert_allclose(y, x, rtol=0, atol=1e-10 * np.abs(x).max())
+    assert t @ S @ t == pytest.approx(x @ x, rel=1e-11)
