@@ -235,3 +235,35 @@ def test_sdpa_multiblock(libs, tmp_path, name):
             o1 = np.argsort(i1[p1[k]:p1[k + 1]], kind="stable")
             np.testing.assert_array_equal(i0[p0[k]:p0[k + 1]][o0], i1[p1[k]:p1[k + 1]][o1])
             np.testing.assert_array_equal(x0[p0[k]:p0[k + 1]][o0], x1[p1[k]:p1[k + 1]][o1])
+
+
+def test_sizes_over_several_lines(libs, tmp_path):
+    """Block sizes (and the right-hand side) spread over several lines read as the same file
+    on one line. The reference counts one line for each and then misplaces the data."""
+    ours, ref = libs
+    one = tmp_path / "one.dat-s"
+    one.write_text('"c\n1\n3\n2 2 -1\n1.0\n0 1 1 1 1.0\n1 1 1 2 0.5\n1 3 1 1 2.0\n')
+    multi = tmp_path / "multi.dat-s"
+    multi.write_text('"c\n1\n3\n2\n2\n-1\n1.0\n0 1 1 1 1.0\n1 1 1 2 0.5\n1 3 1 1 2.0\n')
+    same(api.read_sdpa_with(ours, multi), api.read_sdpa_with(ref, one))
+    with pytest.raises(RuntimeError):
+        api.read_sdpa_with(ref, multi)
+
+
+def test_index_outside_block_is_an_error(libs, tmp_path):
+    """An entry whose row or column exceeds its block's size is an error here; the reference
+    stores it at a packed index outside the block."""
+    ours, _ = libs
+    path = tmp_path / "oob.dat-s"
+    path.write_text("1\n1\n2\n1.0\n0 1 1 1 1.0\n1 1 3 1 0.5\n")
+    with pytest.raises(RuntimeError):
+        api.read_sdpa_with(ours, path)
+
+
+def test_lp_block_not_last_fails_like_the_reference(libs, tmp_path):
+    ours, ref = libs
+    path = tmp_path / "lpfirst.dat-s"
+    path.write_text("1\n2\n-2 2\n1.0\n0 2 1 1 1.0\n1 1 1 1 1.0\n1 2 1 2 0.5\n")
+    for L in (ours, ref):
+        with pytest.raises(RuntimeError):
+            api.read_sdpa_with(L, path)
