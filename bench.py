@@ -34,6 +34,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -97,7 +98,7 @@ class ClockSampler:
     def __init__(self, bus_id: str | None):
         self.bus_id = bus_id
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", ".clocks_%d.csv" % os.getpid())
+        self.path = os.path.join(tempfile.gettempdir(), "hdsdp_b200_clocks_%d.csv" % os.getpid())
 
     def start(self):
         os.makedirs(os.path.dirname(self.path), exist_ok=True)
