@@ -45,11 +45,9 @@ UNIT = "s"
 FLUSH_BYTES = 256 << 20  # larger than the 126 MB L2
 FAMILIES = ["fp64_gemm_dmma", "potrf_coop", "trtri_coop", "schur_pair_gather", "bf16x3_gemm_tcgen05"]
 FAMILY_BOUND = ["tensor", "tensor", "tensor", "hbm", "tensor"]
-# ncu dram__bytes_read.sum + dram__bytes_write.sum per launch of the top kernel on
-# the bench workload, from the capture summarised under profiles/ (None until captured).
-# DRAM bytes (read + write) per launch from one ncu capture (profiles/potrf_coop_n1000.md:
-# dram__bytes_read.sum + dram__bytes_write.sum of the n = 1000 factorisation, the size of the
-# bench workload's dual slack; the 53 Schur factorisations per solve are n = 2000).
+# DRAM bytes (ncu dram__bytes_read.sum + dram__bytes_write.sum) per launch of the top
+# kernel on the bench workload, from one ncu capture of the n = 1000 factorisation, the size
+# of the bench workload's dual slack (the 53 Schur factorisations per solve are n = 2000).
 TRAFFIC_PER_LAUNCH = {("rank1_n1000_m2000", "potrf_coop"): 4.3282e6}
 REF_SAMPLE_ITERS = 5
 

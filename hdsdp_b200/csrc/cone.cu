@@ -1008,7 +1008,7 @@ hdsdp_retcode KKT::factorize() {
     bool ok = hb::factorize(s, F, M, ldm);
     if (!ok) {
         // The reference switches to an LDL^T factorisation here (linsolver.c:1373-1377);
-        // this build retries the Cholesky with a small diagonal shift instead.
+        // this library retries the Cholesky with a small diagonal shift instead.
         copy_matrix(s, 1, m, M, ldm + 1, d_t, 1);
         HB_CUDA(cudaMemcpyAsync(h_buf, d_t, sizeof(double) * m, cudaMemcpyDeviceToHost, s));
         HB_CUDA(cudaStreamSynchronize(s));
