@@ -82,3 +82,26 @@ def test_reference_small_case_reproduces():
     r = ref_api.solve_problem(instances.multiblock_case("mb5_sparse"))
     assert r["iters"] == g["mb5_sparse"]["iters"]
     assert r["dobj"] == pytest.approx(g["mb5_sparse"]["dobj"], rel=1e-12)
+
+
+@pytest.mark.parametrize("m,nz", [(10, 3), (10, 4), (20, 6), (20, 7), (7, 0), (1, 1)])
+def test_cone_choice_at_the_threshold(m, nz):
+    """Dense when more than 0.3 m constraints have a coefficient in the block, sparse
+    otherwise (interface/hdsdp_user_data.c:82-85), for the same data in both libraries."""
+    build()
+    if not ref_api.available():
+        pytest.skip("oracle/_ref not built")
+    ours, ref = _lib.load(), ref_api.lib()
+    ref.HUserDataChooseCone.argtypes = [C.c_void_p]
+    n = 3
+    Ap = [0, 1] + [0] * m   # column 0 (C) holds one entry; then nz nonzero constraint columns
+    cnt = 1
+    for i in range(m):
+        cnt += 1 if i < nz else 0
+        Ap[i + 2] = cnt
+    Ap = np.asarray(Ap, dtype=np.int32)
+    Ai = np.zeros(max(cnt, 1), dtype=np.int32)
+    Ax = np.ones(max(cnt, 1))
+    a = _choose(ours, "sdp", m, n, Ap, Ai, Ax)
+    assert a == _choose(ref, "sdp", m, n, Ap, Ai, Ax)
+    assert a == (DENSE_SDP if nz > 0.3 * m else SPARSE_SDP)
