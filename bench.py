@@ -20,9 +20,15 @@ reference's own relative-gap test (1e-6). Printed as one JSON line:
   cpu_baseline  the reference CPU solver (oracle/_ref, all host threads) on a
          bounded sample of the same solve: the first few iterations, scaled
          to the reference's full iteration count
+  precision_legs  the same workload in split precision (mode 2) beside the
+         FP64 solve, with the split solve's error against the FP64 one per
+         iteration and for every final result
+  maxcut_n8000  MaxCut n=8000 (40,000 edges) solved in FP64 and in split
+         precision: device time, time to a 1e-6 gap, iterations, status
 
---impl reference times the reference CPU solver alone (rank 0) on the same
-workload and prints the same metric with "impl": "reference". Multi-GPU runs
+--impl reference times complete reference CPU solves (rank 0, all host
+threads) on the same workload and prints the same metric with "impl":
+"reference"; a time budget bounds how many solves are timed. Multi-GPU runs
 are independent replicas, one solve per GPU per step ("scaling": "weak"),
 timed as the max over ranks.
 """
@@ -43,13 +49,20 @@ sys.path.insert(0, ROOT)
 METRIC = "time to 1e-6 rel gap (dual-scaling IPM solve)"
 UNIT = "s"
 FLUSH_BYTES = 256 << 20  # larger than the 126 MB L2
-FAMILIES = ["fp64_gemm_dmma", "potrf_coop", "trtri_coop", "schur_pair_gather", "bf16x3_gemm_tcgen05"]
-FAMILY_BOUND = ["tensor", "tensor", "tensor", "hbm", "tensor"]
-# DRAM bytes (ncu dram__bytes_read.sum + dram__bytes_write.sum) per launch of the top
-# kernel on the bench workload, from one ncu capture of the n = 1000 factorisation, the size
-# of the bench workload's dual slack (the 53 Schur factorisations per solve are n = 2000).
-TRAFFIC_PER_LAUNCH = {("rank1_n1000_m2000", "potrf_coop"): 4.3282e6}
+# kernel-timing families of the library (hdsdpb_kstat_*), in its numbering
+FAMILIES = ["fp64_gemm_dmma", "potrf_coop_slack", "trtri_coop", "schur_pair_gather", "bf16x3_gemm_tcgen05",
+            "potrf_coop_schur"]
+FAMILY_BOUND = ["tensor", "tensor", "tensor", "hbm", "tensor", "tensor"]
+# DRAM bytes (ncu dram__bytes_read.sum + dram__bytes_write.sum) per launch of a kernel
+# family on a workload, with the ncu summary they were read from.
+TRAFFIC_PER_LAUNCH = {
+    ("rank1_n1000_m2000", "potrf_coop_slack"): (4.52e6, "profiles/potrf_coop_n1000.md (one launch, n = 1000)"),
+}
 REF_SAMPLE_ITERS = 5
+# a complete reference solve of the bench workload takes tens of seconds: time as many
+# as fit this budget (at least one)
+REF_BUDGET_S = 300.0
+L2_NOTE = "flushed between steps (256 MB write)"
 
 
 def parse_args():
@@ -62,7 +75,16 @@ def parse_args():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "split", "adaptive"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-precision-legs", action="store_true", help="skip the other-precision solves")
+    ap.add_argument("--no-maxcut-leg", action="store_true", help="skip the MaxCut n=8000 leg")
+    ap.add_argument("--ref-budget", type=float, default=REF_BUDGET_S,
+                    help="seconds of complete reference solves to time (--impl reference)")
     return ap.parse_args()
+
+
+def bench_config(args, inst, world):
+    """The workload configuration; both arms print the same keys and values."""
+    return {"workload": args.workload, "n": inst.n, "m": inst.m, "primal_refinement": False,
+            "precision": args.precision, "parallelism": "replicas" if world > 1 else "single", "l2": L2_NOTE}
 
 
 def dist_env():
@@ -171,8 +193,9 @@ def _reference_child(workload, caps, threads, out):
     inst = instances.WORKLOADS[workload]()
     res = []
     for cap in caps:
-        r = ref_api.solve(inst, want_x=False, params={0: cap, 4: 0})
-        res.append((r["time"], r["iters"]))
+        params = {4: 0} if cap is None else {0: cap, 4: 0}
+        r = ref_api.solve(inst, want_x=False, params=params)
+        res.append((r["time"], r["iters"], r["status_after_check"], r["dobj"]))
     out.put(res)
 
 
@@ -209,7 +232,7 @@ def reference_sample(workload: str, iters: int, threads: int, fallback_iters=Non
     res, why = reference_runs(workload, (2, 2 + iters), threads, timeout)
     if res is None:
         return None, why
-    (t1, i1), (tk, ik) = res
+    (t1, i1, _, _), (tk, ik, _, _) = res
     done = max(1, ik - i1)
     per_iter = max(0.0, tk - t1) / done
     full = reference_iters(workload) or fallback_iters or ik
@@ -217,9 +240,11 @@ def reference_sample(workload: str, iters: int, threads: int, fallback_iters=Non
 
 
 def run_reference(args):
+    """Complete reference solves of the workload on all host cores (rank 0 alone)."""
     rank, world, _ = dist_env()
     if rank != 0:
         return
+    import numpy as np
     from hdsdp_b200 import instances
     from oracle import ref_api
     base = {"metric": METRIC, "unit": UNIT, "impl": "reference", "higher_is_better": False}
@@ -230,30 +255,37 @@ def run_reference(args):
     cores = host_cores()
     for _ in range(args.warmup):  # untimed: a short capped solve in the same kind of child process
         reference_runs(args.workload, (2,), cores, 240.0)
-    vals, raw = [], []
+    flush = np.empty(FLUSH_BYTES // 8)
+    vals, iters, status, dobj = [], None, None, None
     t0 = time.perf_counter()
-    for _ in range(args.steps):
-        got, why = reference_sample(args.workload, REF_SAMPLE_ITERS, cores)
+    for k in range(args.steps):
+        flush.fill(float(k))  # evict the previous solve's data from the host caches
+        got, why = reference_runs(args.workload, (None,), cores, max(600.0, 3.0 * args.ref_budget))
         if got is None:
             print(json.dumps({"impl": "reference", "unavailable": why}))
             return
-        est, t, done, full = got
-        vals.append(est)
-        raw.append(t)
+        t, iters, status, dobj = got[0]
+        vals.append(t)
+        elapsed = time.perf_counter() - t0
+        if elapsed + statistics.mean(vals) > args.ref_budget:
+            break
     wall = time.perf_counter() - t0
     value = statistics.mean(vals)
-    sample = ("per step: %s solves capped at 2 and %d IPM iterations (%.2f s of CPU work); set-up + "
-              "marginal s/iter scaled to the reference's %d iterations" % (args.workload, 2 + REF_SAMPLE_ITERS,
-                                                                         statistics.mean(raw), full))
-    line = dict(base, value=value, n_gpus=args.gpus, steps=args.steps, warmup=args.warmup,
-                ms_per_step=1e3 * wall / args.steps, scaling="weak", vs_baseline=None, dtype="f64",
-                data="synthetic (seeded generator, hdsdp_b200/instances.py)",
-                config={"workload": args.workload, "n": inst.n, "m": inst.m, "primal_refinement": False,
-                        "l2": "n/a (CPU)"},
+    capped, _ = reference_sample(args.workload, REF_SAMPLE_ITERS, cores)
+    sample = ("%d complete %s solves (HDSDPOptimize, primal refinement off, %d iterations, status %s), "
+              "%.1f s of CPU work; at most %.0f s of solves are timed" % (len(vals), args.workload, iters, status,
+                                                                          sum(vals), args.ref_budget))
+    line = dict(base, value=value, n_gpus=args.gpus, steps=len(vals), steps_requested=args.steps,
+                warmup=args.warmup, ms_per_step=1e3 * wall / len(vals), scaling="weak", vs_baseline=None,
+                dtype="f64", data="synthetic (seeded generator, hdsdp_b200/instances.py)",
+                config=bench_config(args, inst, world),
                 cpu_baseline={"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
                               "sample": sample},
                 e2e={"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-                s_per_iter=value / full)
+                iters=iters, status=status, dobj=dobj, s_per_iter=value / max(1, iters),
+                steps_s=[round(v, 3) for v in vals],
+                extrapolated_from_capped=(None if capped is None else
+                                          {"value": capped[0], "capped_at": [2, 2 + REF_SAMPLE_ITERS]}))
     print(json.dumps(line))
 
 
@@ -299,8 +331,9 @@ def adjoint_leg(L, api, instances, np):
 
 
 def precision_leg(api, inst, mode, solves, np):
-    """Mean device-timed solve and time to a 1e-6 gap with HDSDPSetPrecision(mode)."""
-    ipm, ttg, it, st = [], [], 0, 0
+    """Mean device-timed solve, time to a 1e-6 gap and the last solve's results
+    (objectives, y, per-iteration log) with HDSDPSetPrecision(mode)."""
+    ipm, ttg, last = [], [], None
     for _ in range(solves):
         s = api.Solver()
         try:
@@ -315,11 +348,44 @@ def precision_leg(api, inst, mode, solves, np):
             hit = np.flatnonzero(np.asarray(log["gap"]) <= 1e-6)
             ttg.append(float(log["t"][hit[0]] - t["setup"]) if hit.size else None)
             ipm.append(t["ipm_device"])
-            it, st = s.iters(), s.status()
+            po, do, y = s.get_row_dual()
+            last = {"iters": s.iters(), "status": s.status(), "pobj": po, "dobj": do, "y": y, "log": log}
         finally:
             s.close()
-    return {"value": float(np.mean(ipm)), "unit": UNIT, "iters": it, "status": st,
-            "time_to_gap_s": ttg[-1], "solves": solves}
+    out = {"value": float(np.mean(ipm)), "unit": UNIT, "iters": last["iters"], "status": last["status"],
+           "time_to_gap_s": ttg[-1], "solves": solves}
+    return out, last
+
+
+def split_error(split, fp64, np):
+    """The split-precision solve's error against the FP64 solve: final objectives and y
+    (relative), and per iteration the relative differences of the dual objective and of
+    the relative gap."""
+    def rel(a, b):
+        return abs(a - b) / (1.0 + abs(b))
+    k = min(len(split["log"]["dobj"]), len(fp64["log"]["dobj"]))
+    dd = [rel(a, b) for a, b in zip(split["log"]["dobj"][:k], fp64["log"]["dobj"][:k])]
+    dg = [abs(a - b) for a, b in zip(split["log"]["gap"][:k], fp64["log"]["gap"][:k])]
+    return {"pobj_rel": rel(split["pobj"], fp64["pobj"]), "dobj_rel": rel(split["dobj"], fp64["dobj"]),
+            "y_rel": float(np.linalg.norm(split["y"] - fp64["y"]) / max(np.linalg.norm(fp64["y"]), 1e-300)),
+            "iters": [split["iters"], fp64["iters"]],
+            "per_iter_dobj_rel": [float("%.3g" % v) for v in dd],
+            "per_iter_gap_absdiff": [float("%.3g" % v) for v in dg]}
+
+
+def maxcut_leg(api, instances, np):
+    """MaxCut n=8000 (40,000 edges): FP64 (sparse dual-slack factorisation on trial
+    points) and split precision mode 2; one untimed solve, then two timed ones each."""
+    inst = instances.WORKLOADS["maxcut_n8000"]()
+    out = {"workload": "maxcut_n8000", "n": inst.n, "m": inst.m}
+    res = {}
+    for name, mode in (("fp64", 0), ("split_adaptive", 2)):
+        precision_leg(api, inst, mode, 1, np)
+        out[name], res[name] = precision_leg(api, inst, mode, 2, np)
+    out["fp64_over_split"] = out["fp64"]["value"] / out["split_adaptive"]["value"]
+    e = split_error(res["split_adaptive"], res["fp64"], np)
+    out["split_error"] = {k: e[k] for k in ("pobj_rel", "dobj_rel", "y_rel", "iters")}
+    return out
 
 
 def run_b200(args):
@@ -442,7 +508,8 @@ def run_b200(args):
         peak, unit = pk["hbm_gbs"], "GB/s"
     roofline = {"bound": FAMILY_BOUND[top], "kernel": FAMILIES[top], "achieved": achieved, "peak": peak,
                 "unit": unit, "frac": achieved / peak, "peak_source": pk["source"],
-                "traffic": TRAFFIC_PER_LAUNCH.get((args.workload, FAMILIES[top])),
+                "traffic": TRAFFIC_PER_LAUNCH.get((args.workload, FAMILIES[top]), (None, None))[0],
+                "traffic_source": TRAFFIC_PER_LAUNCH.get((args.workload, FAMILIES[top]), (None, None))[1],
                 "launches": n_l, "ms_total": ms, "share_of_ipm": ms * 1e-3 / sum(ipm_s)}
     if FAMILIES[top] == "bf16x3_gemm_tcgen05":
         roofline["note"] = "achieved counts the three BF16 products of each split product"
@@ -475,22 +542,23 @@ def run_b200(args):
     adj = adjoint_leg(L, api, instances, np) if rank == 0 else None
     legs = None
     if rank == 0 and not args.no_precision_legs:
-        # the other arithmetic on the same workload (two solves after the warm-up above)
-        other = {"fp64": 2, "split": 0, "adaptive": 0}[args.precision]
-        name = "fp64" if other == 0 else "split_adaptive"
-        legs = {args.precision if args.precision != "adaptive" else "split_adaptive": value,
-                name: precision_leg(api, inst, other, 2, np)}
-        if other == 2:
-            legs["fp64_over_split"] = value / legs[name]["value"]
+        # the same workload in FP64 and in split precision mode 2 (two solves each after
+        # the warm-up above), with the split solve's error against the FP64 solve
+        fp64_leg, fp64_last = precision_leg(api, inst, 0, 2, np)
+        split_leg, split_last = precision_leg(api, inst, 2, 2, np)
+        legs = {"fp64": fp64_leg, "split_adaptive": split_leg,
+                "fp64_over_split": fp64_leg["value"] / split_leg["value"],
+                "split_error_vs_fp64": split_error(split_last, fp64_last, np)}
+    mc = None
+    if rank == 0 and not args.no_maxcut_leg:
+        mc = maxcut_leg(api, instances, np)
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": max(3, args.warmup), "ms_per_step": 1e3 * value, "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64" if precision == 0 else "bf16x3+f64",
         "data": "synthetic (seeded generator, hdsdp_b200/instances.py)",
-        "config": {"workload": args.workload, "n": inst.n, "m": inst.m, "primal_refinement": False,
-                   "precision": args.precision, "parallelism": "replicas" if world > 1 else "single",
-                   "l2": "flushed between steps (256 MB write)"},
+        "config": bench_config(args, inst, world),
         "iters": iters, "s_per_iter": value / max(1, iters), "time_to_gap_s": time_to_gap,
         "steps_ipm_s": [round(x, 4) for x in ipm_s], "steps_e2e_s": [round(x, 4) for x in e2e_s],
         "setup_s": [round(r["timers"]["setup"], 4) for r in results],
@@ -499,7 +567,7 @@ def run_b200(args):
                 "bytes_note": "h2d counts the CSC arrays and b handed to the C API from pinned memory; "
                               "the library reads them on the host and uploads the presolved coefficients"},
         "roofline": roofline, "kernels": kernels, "cpu_baseline": cpu, "clocks": clk,
-        "gpu_launches": launches, "wall_s": wall, "adjoint": adj, "precision_legs": legs,
+        "gpu_launches": launches, "wall_s": wall, "adjoint": adj, "precision_legs": legs, "maxcut_n8000": mc,
         "split_s": {k: t[k] for k in ("schur", "schur_factor", "schur_solve", "s_factor", "s_inverse",
                                       "lanczos", "assemble", "primal", "setup", "total")},
     }

@@ -24,7 +24,7 @@ EXPORTS = [
     "hdsdpb_sparse_cholesky", "hdsdpb_sparse_congruence",
     "HDSDPGetIterLog", "HDSDPGetTimers", "HDSDPAdjoint",
     "hdsdpb_schur_probe", "hdsdpb_ratio_probe", "hdsdpb_cholesky", "hdsdpb_cholesky_noalloc", "hdsdpb_inverse", "hdsdpb_gemm",
-    "hdsdpb_kernel_timing", "hdsdpb_gridsync_probe", "hdsdpb_launch_count", "hdsdpb_release_cached_memory",
+    "hdsdpb_kernel_timing", "hdsdpb_gridsync_probe", "hdsdpb_launch_count", "hdsdpb_alloc_calls", "hdsdpb_release_cached_memory",
     "hdsdpb_kstat_enable", "hdsdpb_kstat_read", "hdsdpb_split_gemm", "hdsdpb_cholesky_solve", "HReadSDPA",
 ]
 
@@ -82,6 +82,7 @@ def load():
         "hdsdpb_kernel_timing": ([i, i, i, dp], i),
         "hdsdpb_gridsync_probe": ([i, i, dp], i),
         "hdsdpb_launch_count": ([], C.c_longlong),
+        "hdsdpb_alloc_calls": ([], C.c_longlong),
         "hdsdpb_release_cached_memory": ([], None),
         "hdsdpb_kstat_enable": ([i], i),
         "hdsdpb_split_gemm": ([i, i, i, dp, i, i, dp, i, i, dp, i], i),

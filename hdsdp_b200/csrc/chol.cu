@@ -12,6 +12,7 @@
 // X_i <- Dinv_i X_i, then X_below -= L_below,i X_i.
 #include "la.h"
 #include <cooperative_groups.h>
+#include <mutex>
 #include <algorithm>
 #include <vector>
 
@@ -852,29 +853,24 @@ __global__ void identity_k(int n, double *A, long lda) {
 
 __global__ void zero_info_k(int *p) { *p = 0; }
 
-int sm_count() {
-    static int sms = 0;
-    if (!sms) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (sms <= 0) sms = 1;
-    }
-    return sms;
-}
+int sm_count() { return device_sm_count(); }
 
 int coop_grid(const void *fn) {
-    static int cached[2] = {0, 0};
+    // resident cooperative CTAs, per device and kernel (two kernels use this)
+    static std::atomic<int> cached[kMaxDevices][2];
     const int slot = (fn == (const void *) potrf_coop_kernel) ? 0 : 1;
-    if (cached[slot]) return cached[slot];
-    const int smem = SM_DOUBLES * (int) sizeof(double);
-    HB_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    int dev = 0, sms = 0, per = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, COOP_THREADS, smem);
-    cached[slot] = std::max(1, sms * std::max(per, 1));
-    return cached[slot];
+    const int dev = current_device();
+    int v = cached[dev][slot].load(std::memory_order_acquire);
+    if (v) return v;
+    static std::atomic<unsigned long long> init[2];
+    once_per_device(init[slot], [&] {
+        const int smem = SM_DOUBLES * (int) sizeof(double);
+        HB_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        int per = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, COOP_THREADS, smem);
+        cached[dev][slot].store(std::max(1, device_sm_count() * std::max(per, 1)), std::memory_order_release);
+    });
+    return cached[dev][slot].load(std::memory_order_acquire);
 }
 
 int grid_for_n(long total) {
@@ -902,8 +898,8 @@ bool coop_factorize_enqueue(cudaStream_t s, DenseFactor &F, const double *S, lon
     double *Kp = F.fuse_k ? F.K : nullptr;
     double *KTp = F.fuse_k ? F.KT : nullptr;
     void *args[] = {&Lp, &ld, &nn, &Dp, &ldd, &ip, &Kp, &KTp};
-    const bool timed = kstat_on(KF_POTRF);
-    if (timed) kstat_begin(KF_POTRF, s, (double) n * n * n / 3.0);
+    const bool timed = kstat_on(F.kfamily);
+    if (timed) kstat_begin(F.kfamily, s, (double) n * n * n / 3.0);
     cudaError_t e = cudaLaunchCooperativeKernel(fn, hb::counted(grid), COOP_THREADS, args, SM_DOUBLES * sizeof(double), s);
     if (timed) kstat_end(s);
     if (e != cudaSuccess) {
@@ -929,10 +925,17 @@ bool chol_solve(cudaStream_t s, DenseFactor &F, const double *b, double *x) {
     const int G = std::min(nblk, sm_count());
     const int nown = (nblk + G - 1) / G;
     const int smem = (2 * 64 * TP + nown * 64 + 2 * 64 + 4 * 64) * (int) sizeof(double);
-    static int smem_set = 0;
-    if (smem > smem_set) {
-        if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess) return false;
-        smem_set = smem;
+    {
+        // the largest dynamic shared memory requested so far, per device
+        static std::mutex mu;
+        static int smem_set[kMaxDevices] = {0};
+        std::lock_guard<std::mutex> g(mu);
+        int &cur = smem_set[current_device()];
+        if (smem > cur) {
+            if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
+                return false;
+            cur = smem;
+        }
     }
     const double *Lp = F.L;
     long ld = F.ld;

@@ -783,6 +783,7 @@ void KKT::init(int m_, cudaStream_t stream, Timers *t) {
     // Up to kTriSolveMinM the Schur solves use K = L^-1 (formed inside the factorisation);
     // above it they are triangular solves with L, which read L once instead of forming K.
     F.alloc(m, m < kTriSolveMinM ? 1 : 0);
+    F.kfamily = KF_POTRF_SCHUR;
     asinv.assign(m, 0.0);
     asinvrd.assign(m, 0.0);
     asinvcs.assign(m, 0.0);
@@ -1407,15 +1408,14 @@ hdsdp_retcode Lanczos::solve(DenseFactor &F, const double *D, long ldD, double *
     // the recorded alpha / beta (a step's values do not depend on later steps)
     const bool small = !hyOp && n <= kSmallLanczosN;
     if (small) {
-        static bool attr = false;
-        if (!attr) {
+        static std::atomic<unsigned long long> attr{0};
+        once_per_device(attr, [] {
             const int bytes = (int) small_lanczos_smem(kSmallLanczosN, 30);
             HB_CUDA(cudaFuncSetAttribute((const void *) lanczos_small_kernel,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
             HB_CUDA(cudaFuncSetAttribute((const void *) lanczos_small_ritz_kernel,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-            attr = true;
-        }
+        });
         lanczos_small_kernel<<<hb::counted(1), 256, small_lanczos_smem(n, maxdim), s>>>(
             n, F.K, F.ld, D, ldD, nComputed == 0 ? nullptr : warm, nComputed == 0 ? init_vec : pert_vec, V, ld, d_ab,
             maxdim);

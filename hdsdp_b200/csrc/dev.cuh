@@ -1,8 +1,10 @@
 // Common device-side definitions for the B200 HDSDP library.
 #pragma once
 #include <cuda_runtime.h>
+#include <atomic>
 #include <cstdint>
 #include <cstdio>
+#include <functional>
 
 namespace hb {
 
@@ -22,6 +24,16 @@ __host__ __device__ __forceinline__ size_t cm(long i, long j, long ld) { return 
 
 int &device_error_flag();
 
+// Per-device one-time set-up. Function attributes and device properties belong to a
+// device, and first calls may come from several host threads at once (on one device or
+// several): fn() runs under a library-wide lock, once for each device, and the device's
+// bit in `mask` is published after it has run. Devices 0..63.
+constexpr int kMaxDevices = 64;
+int current_device();
+void once_per_device(std::atomic<unsigned long long> &mask, const std::function<void()> &fn);
+// The current device's SM count, cached per device.
+int device_sm_count();
+
 // Plain cudaMemset / cudaMemcpy run on the legacy default stream, which the library's
 // non-blocking streams do not wait for (a pageable host-to-device copy may still be in
 // flight when cudaMemcpy returns). Call this after such set-up copies and before the
@@ -40,7 +52,12 @@ inline G counted(G grid) {
 // Live per-family kernel timing: while a family is enabled, every launch of it
 // is bracketed by CUDA events on its own stream and its algorithmic work
 // (flops or bytes) is recorded; kstat_read() resolves the events.
-enum KFamily { KF_GEMM = 0, KF_POTRF = 1, KF_TRTRI = 2, KF_SCHUR_PAIR = 3, KF_SPLIT_GEMM = 4, KF_COUNT = 5 };
+// KF_POTRF counts the dual-slack factorisations (order n), KF_POTRF_SCHUR those of the
+// Schur matrix (order m): the same kernel, two workloads.
+enum KFamily {
+    KF_GEMM = 0, KF_POTRF = 1, KF_TRTRI = 2, KF_SCHUR_PAIR = 3, KF_SPLIT_GEMM = 4, KF_POTRF_SCHUR = 5,
+    KF_COUNT = 6
+};
 void kstat_enable(int mask);
 bool kstat_on(int family);
 void kstat_begin(int family, cudaStream_t s, double work);
@@ -58,6 +75,9 @@ void cache_free(void *p);
 cudaError_t cache_malloc_host(void **p, size_t bytes);
 void cache_free_host(void *p);
 void cache_release();
+// Host-side count of cache_malloc / cache_malloc_host calls (all threads), whether the
+// block came from a free list or from the driver.
+long long &alloc_counter();
 template <class T>
 inline cudaError_t cmalloc(T **p, size_t bytes) {
     return cache_malloc((void **) p, bytes);

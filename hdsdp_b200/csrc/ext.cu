@@ -94,6 +94,8 @@ void HDSDPGetTimers(hdsdp *h, double out[23]) {
 
 long long hdsdpb_launch_count(void) { return hb::launch_counter(); }
 
+long long hdsdpb_alloc_calls(void) { return hb::alloc_counter(); }
+
 void hdsdpb_release_cached_memory(void) {
     cudaDeviceSynchronize();
     hb::cache_release();

@@ -18,6 +18,39 @@ int &device_error_flag() {
     return flag;
 }
 
+int current_device() {
+    int d = 0;
+    if (cudaGetDevice(&d) != cudaSuccess || d < 0 || d >= kMaxDevices) d = 0;
+    return d;
+}
+
+namespace {
+std::mutex &init_mutex() {
+    static std::mutex *mu = new std::mutex();  // never destroyed: set-up may run during exit
+    return *mu;
+}
+}  // namespace
+
+void once_per_device(std::atomic<unsigned long long> &mask, const std::function<void()> &fn) {
+    const unsigned long long bit = 1ull << current_device();
+    if (mask.load(std::memory_order_acquire) & bit) return;
+    std::lock_guard<std::mutex> g(init_mutex());
+    if (mask.load(std::memory_order_relaxed) & bit) return;
+    fn();
+    mask.fetch_or(bit, std::memory_order_release);
+}
+
+int device_sm_count() {
+    static std::atomic<int> sms[kMaxDevices];
+    const int d = current_device();
+    int v = sms[d].load(std::memory_order_relaxed);
+    if (v > 0) return v;
+    cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, d);
+    if (v <= 0) v = 1;
+    sms[d].store(v, std::memory_order_relaxed);
+    return v;
+}
+
 namespace {
 struct BlockCache {
     std::mutex mu;
@@ -30,7 +63,13 @@ BlockCache &block_cache() {
 }
 }  // namespace
 
+long long &alloc_counter() {
+    static long long count = 0;
+    return count;
+}
+
 cudaError_t cache_malloc(void **p, size_t bytes) {
+    __atomic_fetch_add(&alloc_counter(), 1LL, __ATOMIC_RELAXED);
     BlockCache &c = block_cache();
     if (bytes == 0) bytes = 1;
     {
@@ -70,6 +109,7 @@ void cache_free(void *p) {
 }
 
 cudaError_t cache_malloc_host(void **p, size_t bytes) {
+    __atomic_fetch_add(&alloc_counter(), 1LL, __ATOMIC_RELAXED);
     BlockCache &c = block_cache();
     if (bytes == 0) bytes = 1;
     {
@@ -484,11 +524,10 @@ constexpr int L_SMEM = 2 * L_ST * L_STAGE * (int) sizeof(double);
 
 template <int TA, int TB>
 void launch_large(const GemmP &p, cudaStream_t s) {
-    static bool init = false;
-    if (!init) {
+    static std::atomic<unsigned long long> init{0};
+    once_per_device(init, [] {
         HB_CUDA(cudaFuncSetAttribute(gemm_large_kernel<TA, TB>, cudaFuncAttributeMaxDynamicSharedMemorySize, L_SMEM));
-        init = true;
-    }
+    });
     dim3 grid((p.M + L_BM - 1) / L_BM, (p.N + L_BN - 1) / L_BN);
     gemm_large_kernel<TA, TB><<<hb::counted(grid), L_T, L_SMEM, s>>>(p);
 }
@@ -806,12 +845,12 @@ static void set_smem(const void *fn, int bytes) {
 static int smem_bytes() { return 2 * 65 * 64 * (int) sizeof(double); }
 
 static void ensure_attrs() {
-    static bool init = false;
-    if (init) return;
-    set_smem((const void *) potf2_kernel, smem_bytes());
-    set_smem((const void *) trsm_panel_kernel, smem_bytes());
-    set_smem((const void *) tri_left_kernel, smem_bytes());
-    init = true;
+    static std::atomic<unsigned long long> init{0};
+    once_per_device(init, [] {
+        set_smem((const void *) potf2_kernel, smem_bytes());
+        set_smem((const void *) trsm_panel_kernel, smem_bytes());
+        set_smem((const void *) tri_left_kernel, smem_bytes());
+    });
 }
 
 bool coop_factorize_enqueue(cudaStream_t s, DenseFactor &F, const double *S, long ldS);

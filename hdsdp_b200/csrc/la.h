@@ -60,6 +60,7 @@ struct DenseFactor {
     unsigned *d_flags = nullptr;
     double *d_tmp = nullptr;
     unsigned epoch = 0;
+    int kfamily = KF_POTRF;   // kernel-timing family of this factor's factorisations
     void alloc(int n_, int fuse_inverse = -1);
     void release();
 };

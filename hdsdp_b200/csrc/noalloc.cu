@@ -19,12 +19,18 @@
 //
 // Host code cannot use the array's name as a device address. The first call on a
 // device looks the address up with cudaGetSymbolAddress (with that device current),
-// checks the result and caches it per device; that first call should therefore come
-// before any stream capture. All calls share the one array: calls that overlap on the
-// GPU (from several host threads, or interleaved on several streams) race.
+// checks the result and caches it per device under a lock; that first call should
+// therefore come before any stream capture. All calls share the one array: calls that
+// overlap on the GPU (from several host threads, or interleaved on several streams) race.
+//
+// The work runs on the legacy default stream, so a call also waits for, and holds back,
+// the caller's other blocking streams (not its non-blocking ones); the call returns after
+// synchronising that stream alone. The return code reflects this call's CUDA errors
+// only: the library's sticky error flag is compared with its value on entry.
 #include "la.h"
 #include "../../include/hdsdp_b200.h"
 #include <cstdio>
+#include <mutex>
 
 namespace hb {
 namespace {
@@ -36,21 +42,26 @@ constexpr size_t kScratchDoubles = 2 * kMatDoubles + (size_t) kLd * 64 + 2;
 
 static __device__ __align__(256) double g_noalloc_scratch[kScratchDoubles];
 
-constexpr int kMaxDevices = 64;
-double *g_scratch_ptr[kMaxDevices] = {nullptr};
+std::atomic<double *> g_scratch_ptr[kMaxDevices];
 
 double *scratch_for_current_device() {
     int dev = -1;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return nullptr;
-    if (!g_scratch_ptr[dev]) {
-        void *p = nullptr;
-        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess) {
+    double *p = g_scratch_ptr[dev].load(std::memory_order_acquire);
+    if (p) return p;
+    static std::mutex mu;
+    std::lock_guard<std::mutex> g(mu);
+    p = g_scratch_ptr[dev].load(std::memory_order_relaxed);
+    if (!p) {
+        void *q = nullptr;
+        if (cudaGetSymbolAddress(&q, g_noalloc_scratch) != cudaSuccess) {
             cudaGetLastError();
             return nullptr;
         }
-        g_scratch_ptr[dev] = (double *) p;
+        p = (double *) q;
+        g_scratch_ptr[dev].store(p, std::memory_order_release);
     }
-    return g_scratch_ptr[dev];
+    return p;
 }
 
 }  // namespace
@@ -71,6 +82,7 @@ extern "C" int hdsdpb_cholesky_noalloc(int n, const double *S, double *L, double
     }
     double *base = scratch_for_current_device();
     if (!base) return -1;
+    const int err_on_entry = device_error_flag();
     const long ld = pad_ld(n);
     DenseFactor F;  // views into the scratch array (never alloc()/release()d)
     int h_info = 0;
@@ -97,6 +109,7 @@ extern "C" int hdsdpb_cholesky_noalloc(int n, const double *S, double *L, double
                 for (int i = 0; i < j; ++i) L[(size_t) j * n + i] = 0.0;
         }
     }
-    if (cudaDeviceSynchronize() != cudaSuccess || device_error_flag()) return -1;
+    if (cudaStreamSynchronize(cudaStreamLegacy) != cudaSuccess || cudaGetLastError() != cudaSuccess) return -1;
+    if (device_error_flag() != err_on_entry) return -1;
     return ok ? 0 : 1;
 }

@@ -362,16 +362,15 @@ __global__ void read_err_kernel(int *out) {
 }
 
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
-    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-    static bool tried = false;
-    if (!tried) {
-        tried = true;
+    // a driver entry point is process-wide: looked up once (thread-safe static init)
+    static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
         void *p = nullptr;
         cudaDriverEntryPointQueryResult q;
         if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
             q == cudaDriverEntryPointSuccess)
-            fn = (PFN_cuTensorMapEncodeTiled_v12000) p;
-    }
+            return (PFN_cuTensorMapEncodeTiled_v12000) p;
+        return (PFN_cuTensorMapEncodeTiled_v12000) nullptr;
+    }();
     return fn;
 }
 
@@ -435,13 +434,13 @@ void split_from_f64(cudaStream_t s, SplitOperand &op, const double *X, long ld, 
 bool split_gemm(cudaStream_t s, const SplitOperand &A, const SplitOperand &B, const SplitGemm &g) {
     if (g.M <= 0 || g.N <= 0) return true;
     if (!A.hi || !B.hi || A.kpad != B.kpad || g.M > A.rows_alloc || g.N > B.rows_alloc) return false;
-    static bool attr = false;
-    if (!attr) {
-        if (cudaFuncSetAttribute(split_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES) !=
-            cudaSuccess)
-            return false;
-        attr = true;
-    }
+    static std::atomic<unsigned long long> attr{0};
+    bool attr_ok = true;
+    once_per_device(attr, [&] {
+        attr_ok = cudaFuncSetAttribute(split_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       SMEM_BYTES) == cudaSuccess;
+    });
+    if (!attr_ok) return false;
     KernelArgs p{};
     p.M = g.M;
     p.N = g.N;
@@ -467,14 +466,7 @@ bool split_gemm(cudaStream_t s, const SplitOperand &A, const SplitOperand &B, co
     p.colsq = g.colsq;
     if (p.nkb <= 0) return false;
     const long tiles = g.lower_tiles ? (long) p.tiles_m * (p.tiles_m + 1) / 2 : (long) p.tiles_m * p.tiles_n;
-    static int sms = 0;
-    if (!sms) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (sms <= 0) sms = 1;
-    }
-    const long blocks = std::min<long>(tiles, sms);  // persistent: one CTA per SM at most
+    const long blocks = std::min<long>(tiles, device_sm_count());  // persistent: one CTA per SM at most
     const bool timed = kstat_on(KF_SPLIT_GEMM);
     if (timed) {
         double f = 3.0 * 2.0 * g.M * (double) g.N * g.K;

@@ -216,6 +216,59 @@ def theta_adjoint(n: int = 200, p: float = 0.1, zero_frac: float = 0.2, seed: in
                      {"edges": int(ei.size), "zeros": int(zi.size), "seed": seed})
 
 
+def _dense_columns(n, mats):
+    """(packed index, value) columns of full symmetric matrices (their nonzero lower entries)."""
+    ii, jj = np.tril_indices(n)
+    idx = pack_idx(n, ii, jj)
+    cols = []
+    for M in mats:
+        v = M[ii, jj]
+        keep = v != 0
+        cols.append((idx[keep], v[keep]))
+    return cols
+
+
+def dense_coeff(n: int = 80, m: int = 40, seed: int = 21) -> SDPInstance:
+    """SDP whose constraint matrices are general dense symmetric matrices (full rank).
+
+    A_i = (R_i + R_i^T) / 2 with R_i Gaussian, so the presolve keeps them dense
+    (interface/hdsdp_sdpdata.c:2273) and the Schur rows take the dense-coefficient
+    path. X0 = I + G G^T / n (G n x 5) is primal feasible with b_i = <A_i, X0>,
+    and C = I + 0.1 (Q + Q^T) / (2 sqrt(n)) is positive definite, so y = 0 is a
+    strictly feasible dual point.
+    """
+    rng = np.random.default_rng(seed)
+    G = rng.standard_normal((n, 5))
+    X0 = np.eye(n) + G @ G.T / n
+    Q = rng.standard_normal((n, n))
+    C = np.eye(n) + 0.1 * (Q + Q.T) / (2.0 * np.sqrt(n))
+    mats, b = [C], np.zeros(m)
+    for t in range(m):
+        R = rng.standard_normal((n, n))
+        A = (R + R.T) / 2.0
+        mats.append(A)
+        b[t] = float(np.sum(A * X0))
+    return _assemble("dense_coeff", n, _dense_columns(n, mats), b, {"seed": seed})
+
+
+def dual_infeasible(n: int = 8, seed: int = 1) -> SDPInstance:
+    """An SDP with no dual feasible point, which sends the infeasible-start method into
+    the homogeneous self-dual embedding (interface/hdsdp_algo.c:1866-1870).
+
+    C = -I + 0.05 (G + G^T) with G Gaussian is negative definite, and only the first
+    n/2 diagonal entries are constrained (X_ii = 1), so C - sum_i y_i e_i e_i^T is
+    never positive semidefinite and the primal  min <C, X>  is unbounded.
+    """
+    rng = np.random.default_rng(seed)
+    G = rng.standard_normal((n, n)) * 0.05
+    mats = [-np.eye(n) + G + G.T]
+    for i in range(n // 2):
+        E = np.zeros((n, n))
+        E[i, i] = 1.0
+        mats.append(E)
+    return _assemble("dual_infeasible", n, _dense_columns(n, mats), np.ones(n // 2), {"seed": seed})
+
+
 def lp_block(m: int, n_lp: int, per_col: int = 2, seed: int = 7):
     """An LP cone for an instance with m constraints, in the user CSC layout the LP cone
     takes (interface/hdsdp_conic_lp.c:99-158): column 0 the costs c (U(0.5, 1.5)),

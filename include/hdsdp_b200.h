@@ -78,12 +78,19 @@ extern void hdsdpb_release_cached_memory( void );
    (all solvers and entry points). No reference counterpart. */
 extern long long hdsdpb_launch_count( void );
 
+/* Number of device and pinned-host buffer requests this library has made in the
+   process so far, whether served from its cache or by the driver (all solvers and
+   entry points). No reference counterpart; lets a caller confirm that a call path
+   allocates nothing. */
+extern long long hdsdpb_alloc_calls( void );
+
 /* Live kernel timing by family (no reference counterpart): bit f of `mask`
-   enables family f = 0 FP64 GEMM, 1 Cholesky (cooperative potrf),
-   2 triangular inverse, 3 Schur gather pair kernels. While enabled, each launch
-   of the family is bracketed by CUDA events on its own stream; enabling resets
-   the totals. hdsdpb_kstat_read returns the launches, the summed event time in
-   ms and the summed algorithmic work (flops for 0-2, compulsory bytes for 3). */
+   enables family f = 0 FP64 GEMM, 1 Cholesky of the dual slack (cooperative potrf,
+   order n), 2 triangular inverse, 3 Schur gather pair kernels, 4 BF16x3 split GEMM,
+   5 Cholesky of the Schur matrix (the same kernel, order m). While enabled, each
+   launch of the family is bracketed by CUDA events on its own stream; enabling
+   resets the totals. hdsdpb_kstat_read returns the launches, the summed event time
+   in ms and the summed algorithmic work (flops for 0-2, 4, 5; compulsory bytes for 3). */
 extern int hdsdpb_kstat_enable( int mask );
 extern int hdsdpb_kstat_read( int family, long long *launches, double *ms, double *work );
 
@@ -140,7 +147,9 @@ extern int hdsdpb_cholesky_solve( int n, const double *S, const double *b, doubl
    n <= HDSDPB_NOALLOC_MAX_N (about 1.2 MB per GPU, held until exit); nothing is
    allocated or freed per call. Returns -2 (with a message on stderr) when n exceeds
    the limit. The first call on a device looks up the array's address and should come
-   before any stream capture; calls that overlap on the GPU share the scratch and race. */
+   before any stream capture; calls that overlap on the GPU share the scratch and race.
+   The work runs on the legacy default stream (so it also waits for the caller's
+   blocking streams), and the call returns after synchronising that stream. */
 #define HDSDPB_NOALLOC_MAX_N 256
 extern int hdsdpb_cholesky_noalloc( int n, const double *S, double *L, double *logdiag );
 

@@ -17,23 +17,29 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_ref", "libhdsdp_ref.so")
+# The same sources built with the reference's own dual-storage rule (sparse CSC below 25 %
+# fill, interface/hdsdp_conic_sdp.c:33-35, :94); usable with primal refinement off only.
+LIB_PATH_STOCK = os.path.join(HERE, "_ref", "libhdsdp_ref_stock.so")
 
 CONETYPE_LP = 1  # HDSDP_CONETYPE_LP
 CONETYPE_DENSE_SDP = 4  # interface/def_hdsdp_conic.h:22-32
 
-_lib = None
+_libs = {}
 
 
-def available() -> bool:
-    return os.path.exists(LIB_PATH)
+def _path(variant: str) -> str:
+    return {"dense": LIB_PATH, "stock": LIB_PATH_STOCK}[variant]
 
 
-def lib():
-    global _lib
-    if _lib is None:
-        if not available():
+def available(variant: str = "dense") -> bool:
+    return os.path.exists(_path(variant))
+
+
+def lib(variant: str = "dense"):
+    if variant not in _libs:
+        if not available(variant):
             raise RuntimeError("reference oracle not built: run `make -C oracle` where the reference tree exists")
-        L = C.CDLL(LIB_PATH)
+        L = C.CDLL(_path(variant))
         vp = C.c_void_p
         L.HDSDPCreate.argtypes = [C.POINTER(vp)]
         L.HDSDPInit.argtypes = [vp, C.c_int, C.c_int]
@@ -69,8 +75,8 @@ def lib():
                                          C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_double,
                                          C.POINTER(C.c_double), C.c_double, C.POINTER(C.c_double),
                                          C.POINTER(C.c_double)]
-        _lib = L
-    return _lib
+        _libs[variant] = L
+    return _libs[variant]
 
 
 def _dp(a):
@@ -90,10 +96,12 @@ def set_threads(n: int):
         pass
 
 
-def solve(inst, want_x: bool = True, params: dict | None = None, quiet: bool = True, lp=None) -> dict:
+def solve(inst, want_x: bool = True, params: dict | None = None, quiet: bool = True, lp=None,
+          variant: str = "dense") -> dict:
     """Run HDSDPOptimize on ``inst`` (plus the LP cone ``lp`` = (n_lp, Ap, Ai, Ax) as cone 1,
-    as the reference's own driver adds it); return y, objectives, status, X, S, errors, time."""
-    L = lib()
+    as the reference's own driver adds it); return y, objectives, status, X, S, errors, time.
+    ``variant`` "stock" runs the build with the reference's own dual-storage rule."""
+    L = lib(variant)
     Ap = np.ascontiguousarray(inst.Ap, dtype=np.int32)
     Ai = np.ascontiguousarray(inst.Ai, dtype=np.int32)
     Ax = np.ascontiguousarray(inst.Ax, dtype=np.float64)

@@ -1,6 +1,13 @@
 """Generate the golden fixtures of tests/ by running the compiled reference.
 
     make -C oracle && python tests/golden/make_golden.py [--full]
+    python tests/golden/make_golden.py --add GROUP [GROUP ...]
+
+--add runs only the named groups (EXTRA below) and merges their results into
+the existing fixtures: "north_star" (MaxCut n=8000 and the theta layer n=200,
+primal refinement off; a few minutes), "stock" (the sparse-dual instances on
+the reference build with its own dual-storage rule), "hsd" (instances that end
+in the homogeneous self-dual embedding), "dense" (general dense coefficients).
 
 Writes tests/golden/golden.json (solver results and probe outputs) and
 tests/golden/golden_arrays.npz (Schur matrices, dual vectors). The inputs are
@@ -50,6 +57,90 @@ FULL = {
     "theta_n300": lambda: instances.WORKLOADS["theta_n300"](),
     "rank1_n1000_m2000": lambda: instances.WORKLOADS["rank1_n1000_m2000"](),
 }
+
+
+# Groups generated on demand (--add) and merged into the fixtures.
+NORTH_STAR = {
+    "maxcut_n8000": lambda: instances.WORKLOADS["maxcut_n8000"](),
+    "theta_adjoint_n200": lambda: instances.WORKLOADS["theta_adjoint_n200"](),
+}
+STOCK = {
+    "maxcut60": SMALL["maxcut60"],
+    "maxcut200": SMALL["maxcut200"],
+    "theta_adj40": SMALL["theta_adj40"],
+    "theta_adjoint_n200": NORTH_STAR["theta_adjoint_n200"],
+    "maxcut_n8000": NORTH_STAR["maxcut_n8000"],
+}
+HSD = {
+    "dinf8": lambda: instances.dual_infeasible(8, seed=1),
+    "dinf30": lambda: instances.dual_infeasible(30, seed=2),
+}
+# primal refinement on is not generated: the reference's PSDP asserts on dense
+# coefficients (linalg/hdsdp_sdpdata.c:1963)
+DENSE = {
+    "dense40": lambda: instances.dense_coeff(40, 20, seed=22),
+    "dense80": lambda: instances.dense_coeff(80, 40, seed=21),
+}
+
+
+def _solve_record(inst, r):
+    return {"n": inst.n, "m": inst.m, "retcode": r["retcode"], "iters": r["iters"],
+            "status": r["status_after_check"], "status_before_check": r["status"], "pobj": r["pobj"],
+            "dobj": r["dobj"], "errs": [float(e) for e in r["errs"]], "time_s": r["time"]}
+
+
+def add_groups(groups):
+    """Run the named groups and merge their results into the committed fixtures."""
+    gpath, apath = os.path.join(HERE, "golden.json"), os.path.join(HERE, "golden_arrays.npz")
+    out = json.load(open(gpath))
+    arrays = dict(np.load(apath))
+    for g in groups:
+        if g == "north_star":
+            for name, make in NORTH_STAR.items():
+                inst = make()
+                r = ref_api.solve(inst, want_x=False, params={4: 0})
+                key = "%s/psdp0" % name
+                out["solves"][key] = _solve_record(inst, r)
+                arrays["y/" + key] = r["y"]
+                print(key, r["iters"], r["status_after_check"], r["pobj"], r["dobj"], r["time"], flush=True)
+        elif g == "stock":
+            out.setdefault("solves_stock", {})
+            for name, make in STOCK.items():
+                inst = make()
+                r = ref_api.solve(inst, want_x=False, params={4: 0}, variant="stock")
+                key = "%s/psdp0" % name
+                out["solves_stock"][key] = _solve_record(inst, r)
+                arrays["y_stock/" + key] = r["y"]
+                print("stock", key, r["iters"], r["status_after_check"], r["pobj"], r["dobj"], r["time"], flush=True)
+        elif g == "hsd":
+            out.setdefault("hsd_solves", {})
+            for name, make in HSD.items():
+                inst = make()
+                for psdp in (0, 1):
+                    r = ref_api.solve(inst, want_x=False, params={4: psdp})
+                    key = "%s/psdp%d" % (name, psdp)
+                    out["hsd_solves"][key] = _solve_record(inst, r)
+                    print("hsd", key, r["iters"], r["status"], r["status_after_check"], r["pobj"], r["dobj"], flush=True)
+        elif g == "dense":
+            out.setdefault("dense_solves", {})
+            for name, make in DENSE.items():
+                inst = make()
+                r = ref_api.solve(inst, want_x=False, params={4: 0})
+                key = "%s/psdp0" % name
+                out["dense_solves"][key] = _solve_record(inst, r)
+                arrays["y/" + key] = r["y"]
+                print("dense", key, r["iters"], r["status_after_check"], r["pobj"], r["dobj"], flush=True)
+                y, resi, dy = probe_point(inst)
+                sp = ref_api.schur_probe(inst, y, resi)
+                step, logdet = ref_api.ratio_probe(inst, y, resi, dy, 0.5)
+                out["probes"][name] = {"resi": resi, "tracesinv": sp["tracesinv"], "step": step, "logdet": logdet}
+                arrays["M/" + name] = np.tril(sp["M"])
+                arrays["asinv/" + name] = sp["asinv"]
+                arrays["asinvrd/" + name] = sp["asinvrd"]
+        else:
+            raise SystemExit("unknown group %s" % g)
+        json.dump(out, open(gpath, "w"), indent=1, sort_keys=True)
+        np.savez_compressed(apath, **arrays)
 
 
 def probe_point(inst, seed=0):
@@ -140,4 +231,7 @@ def main(full: bool):
 
 
 if __name__ == "__main__":
-    main("--full" in sys.argv)
+    if "--add" in sys.argv:
+        add_groups(sys.argv[sys.argv.index("--add") + 1:])
+    else:
+        main("--full" in sys.argv)

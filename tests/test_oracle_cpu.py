@@ -108,3 +108,70 @@ def test_workload_shapes():
     a, b = instances.rank_one(50, 80, 0.2, seed=4), instances.rank_one(50, 80, 0.2, seed=4)
     np.testing.assert_array_equal(a.Ax, b.Ax)
     np.testing.assert_array_equal(a.b, b.b)
+
+
+@pytest.mark.parametrize("name", ["dense40", "dense80"])
+def test_dense_coefficient_restatement_matches_reference(name, golden, golden_arrays):
+    """General dense (full-rank) coefficients: the restated Schur complement matches the
+    reference's dense-coefficient rows (interface/hdsdp_conic_sdp.c:776-847)."""
+    from make_golden import DENSE
+    inst = DENSE[name]()
+    C, A = K.dense_data(inst)
+    y, resi, _ = probe_point(inst)
+    r = K.schur(C, A, y, resi)
+    M = golden_arrays["M/" + name]
+    assert np.abs(np.tril(r["M"]) - M).max() <= 1e-12 * np.abs(M).max()
+    for key in ("asinv", "asinvrd"):
+        g = golden_arrays[key + "/" + name]
+        assert np.abs(r[key] - g).max() <= 1e-12 * max(1.0, np.abs(g).max())
+    sol = golden["dense_solves"][name + "/psdp0"]
+    assert sol["status"] == 3
+    y = golden_arrays["y/%s/psdp0" % name]
+    assert np.linalg.eigvalsh(K.dual_slack(C, A, y))[0] > -1e-8
+
+
+def test_hsd_fixtures_end_in_the_embedding(golden):
+    """The dual-infeasible instances leave the infeasible-start method as suspected
+    infeasible (status 5) after the self-dual embedding has run its iterations."""
+    for key, sol in golden["hsd_solves"].items():
+        assert sol["status_before_check"] == 5, key
+        assert sol["iters"] > 20, key
+
+
+def test_north_star_reference_results(golden):
+    """Full reference solves of MaxCut n=8000 and the theta layer n=200 (primal refinement
+    off), with both dual-storage rules: optimal, and the two storage rules agree."""
+    for name in ("maxcut_n8000", "theta_adjoint_n200"):
+        a = golden["solves"][name + "/psdp0"]
+        b = golden["solves_stock"][name + "/psdp0"]
+        assert a["status"] == b["status"] == 3
+        assert abs(a["iters"] - b["iters"]) <= 2
+        assert a["dobj"] == pytest.approx(b["dobj"], rel=1e-6)
+
+
+def _psdp_child(name, threads, q):
+    from make_golden import SMALL as cases
+    ref_api.set_threads(threads)
+    r = ref_api.solve(cases[name](), want_x=False, params={4: 1})
+    q.put((r["pobj"], r["dobj"], r["iters"], r["status_after_check"]))
+
+
+@pytest.mark.skipif(not ref_api.available(), reason="oracle/_ref not built (make -C oracle)")
+def test_reference_psdp_spread_across_thread_counts():
+    """With primal refinement on, a run that the reference's DIMACS check ends as NUMERICAL
+    keeps the trajectory's floating-point drift: the reference against itself, with one and
+    with eight BLAS threads, differs by more than 1e-4 in the dual objective on rank1_50_80.
+    The GPU parity tests hold such runs to 5e-4 and optimal runs to 1e-6."""
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    res = []
+    for threads in (1, 8):
+        q = ctx.Queue()
+        p = ctx.Process(target=_psdp_child, args=("rank1_50_80", threads, q))
+        p.start()
+        res.append(q.get(timeout=120))
+        p.join(60)
+    (p1, d1, i1, s1), (p8, d8, i8, s8) = res
+    assert s1 == s8 == 10  # HDSDP_NUMERICAL after the DIMACS check
+    spread = abs(d1 - d8) / (1 + abs(d8))
+    assert 1e-4 < spread < 5e-4

@@ -22,10 +22,13 @@ def check_parity(r, ref, psdp=False):
     assert r["status_after_check"] == ref["status"]
     assert abs(r["iters"] - ref["iters"]) <= 2, (r["iters"], ref["iters"])
     # With primal refinement on, the dual phase stops at a 10% gap and five fixed
-    # refinement steps follow, so both objectives keep the trajectory's floating-point
-    # drift (the two solvers agree to about 1e-8 early on and to 1e-6..1e-4 at the 10%
-    # gap); solved to optimality they agree to 1e-6.
-    tol = 5e-4 if psdp else 1e-6
+    # refinement steps follow. Where the reference then reaches PRIMAL_DUAL_OPTIMAL the
+    # objectives meet the 1e-6 bar. Where its DIMACS check ends the run as NUMERICAL
+    # (a gap of percents), the objectives keep the trajectory's floating-point drift:
+    # the reference against itself with 1 and 8 BLAS threads differs by 2.7e-4 in the
+    # dual objective on rank1_50_80 (tests/test_oracle_cpu.py pins that spread), so
+    # those runs are held to 5e-4.
+    tol = 5e-4 if (psdp and ref["status"] != OPTIMAL) else 1e-6
     assert r["dobj"] == pytest.approx(ref["dobj"], rel=tol, abs=1e-8)
     if ref["status"] == OPTIMAL:
         # a run the reference itself ends as NUMERICAL (a gap of percents) has no

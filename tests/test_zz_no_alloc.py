@@ -43,11 +43,37 @@ def test_noalloc_matches_allocating_entry(gpu_lib, n):
     S = _spd(n, n)
     Lref, ldref, pd = api.cholesky(S)
     assert pd
+    Lnp = np.linalg.cholesky(S)
     for _ in range(2):
         r, L, ld = _noalloc(S)
         assert r == 0
         assert np.abs(L - Lref).max() <= 1e-12 * np.abs(Lref).max()
         assert ld == pytest.approx(ldref, rel=1e-12, abs=1e-12)
+        # and against NumPy's factor directly
+        assert np.abs(L - Lnp).max() <= 1e-10 * np.abs(Lnp).max()
+        assert ld == pytest.approx(np.log(np.diag(Lnp)).sum(), rel=1e-10, abs=1e-10)
+
+
+def test_noalloc_requests_no_buffers(gpu_lib):
+    """After the first call on the device, a call makes no buffer request at all (the
+    library's request counter counts its caching allocator's hits and misses alike)."""
+    L = _lib.load()
+    S = _spd(150, 5)
+    r, _, _ = _noalloc(S)
+    assert r == 0
+    before = L.hdsdpb_alloc_calls()
+    for _ in range(2):
+        r, _, _ = _noalloc(S)
+        assert r == 0
+    assert L.hdsdpb_alloc_calls() == before
+    # the allocating entry point does request buffers (the counter works)
+    api.cholesky(S)
+    assert L.hdsdpb_alloc_calls() > before
+
+
+def test_noalloc_empty_matrix(gpu_lib):
+    r, L, ld = _noalloc(np.zeros((0, 0)))
+    assert r == 0 and ld == 0.0 and L.shape == (0, 0)
 
 
 def test_noalloc_indefinite_and_size_limit(gpu_lib):
