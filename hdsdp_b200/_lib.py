@@ -26,6 +26,16 @@ EXPORTS = [
     "hdsdpb_schur_probe", "hdsdpb_ratio_probe", "hdsdpb_cholesky", "hdsdpb_cholesky_noalloc", "hdsdpb_inverse", "hdsdpb_gemm",
     "hdsdpb_kernel_timing", "hdsdpb_gridsync_probe", "hdsdpb_launch_count", "hdsdpb_alloc_calls", "hdsdpb_release_cached_memory",
     "hdsdpb_kstat_enable", "hdsdpb_kstat_read", "hdsdpb_split_gemm", "hdsdpb_cholesky_solve", "HReadSDPA",
+    # the conic callback interface and the KKT manager (include/hdsdp_conic.h)
+    "HConeCreate", "HConeGetVarBufferDim", "HConeSetData", "HConeProcData", "HConePresolveData", "HConeClear",
+    "HConeDestroy", "HConeView", "HConeDetectFeature", "HConeSetStart", "HConeUpdate", "HConeRatioTest",
+    "HConeGetSymNnz", "HConeAddSymNz", "HConeGetSymMapping", "HConeGetDim", "HConeGetCoeffNorm", "HConeGetObjNorm",
+    "HConeBuildSchurComplement", "HConeBuildSchurComplementFixed", "HConeGetLogBarrier",
+    "HConeAddStepToBufferAndCheck", "HConeCheckIsInterior", "HConeCheckIsInteriorExpert", "HConeReduceResi",
+    "HConeSetPerturb", "HConeGetPrimal", "HConeGetDual", "HConeComputeATimesX", "HConeComputeTraceCX",
+    "HConeScalByConstant",
+    "HKKTCreate", "HKKTInit", "HKKTBuildUp", "HKKTBuildUpExtraCone", "HKKTBuildUpFixed", "HKKTExport",
+    "HKKTFactorize", "HKKTSolve", "HKKTRegularize", "HKKTClear", "HKKTDestroy", "HKKTGetMatrix",
 ]
 
 _lib = None
@@ -87,6 +97,49 @@ def load():
         "hdsdpb_kstat_enable": ([i], i),
         "hdsdpb_split_gemm": ([i, i, i, dp, i, i, dp, i, i, dp, i], i),
         "hdsdpb_kstat_read": ([i, C.POINTER(C.c_longlong), dp, dp], i),
+        "HConeCreate": ([C.POINTER(vp)], i),
+        "HConeGetVarBufferDim": ([vp], i),
+        "HConeSetData": ([vp, vp], i),
+        "HConeProcData": ([vp], i),
+        "HConePresolveData": ([vp], i),
+        "HConeClear": ([vp], None),
+        "HConeDestroy": ([C.POINTER(vp)], None),
+        "HConeView": ([vp], None),
+        "HConeDetectFeature": ([vp, dp, ip, dp], None),
+        "HConeSetStart": ([vp, d], None),
+        "HConeUpdate": ([vp, d, dp], None),
+        "HConeRatioTest": ([vp, d, dp, d, i, dp], i),
+        "HConeGetSymNnz": ([vp], C.c_int64),
+        "HConeAddSymNz": ([vp, i, ip], None),
+        "HConeGetSymMapping": ([vp, i, ip], None),
+        "HConeGetDim": ([vp], i),
+        "HConeGetCoeffNorm": ([vp, i], d),
+        "HConeGetObjNorm": ([vp, i], d),
+        "HConeBuildSchurComplement": ([vp, vp, i], i),
+        "HConeBuildSchurComplementFixed": ([vp, vp, i, i], i),
+        "HConeGetLogBarrier": ([vp, d, dp, i, dp], i),
+        "HConeAddStepToBufferAndCheck": ([vp, d, i, ip], i),
+        "HConeCheckIsInterior": ([vp, d, dp, ip], i),
+        "HConeCheckIsInteriorExpert": ([vp, d, d, dp, d, i, ip], i),
+        "HConeReduceResi": ([vp, d], None),
+        "HConeSetPerturb": ([vp, d], None),
+        "HConeGetPrimal": ([vp, d, dp, dp, dp, dp], None),
+        "HConeGetDual": ([vp, dp, dp], None),
+        "HConeComputeATimesX": ([vp, dp, dp], None),
+        "HConeComputeTraceCX": ([vp, dp], d),
+        "HConeScalByConstant": ([vp, d], None),
+        "HKKTCreate": ([C.POINTER(vp)], i),
+        "HKKTInit": ([vp, i, i, C.POINTER(vp)], i),
+        "HKKTBuildUp": ([vp, i], i),
+        "HKKTBuildUpExtraCone": ([vp, vp, i], i),
+        "HKKTBuildUpFixed": ([vp, i, i], i),
+        "HKKTExport": ([vp, dp, dp, dp, dp, dp, dp, dp], None),
+        "HKKTFactorize": ([vp], i),
+        "HKKTSolve": ([vp, dp, dp], i),
+        "HKKTRegularize": ([vp, d], None),
+        "HKKTClear": ([vp], None),
+        "HKKTDestroy": ([C.POINTER(vp)], None),
+        "HKKTGetMatrix": ([vp, dp], i),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

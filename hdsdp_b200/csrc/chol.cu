@@ -124,9 +124,13 @@ __device__ __forceinline__ bool warp_chol_inv16(double *T, double *X, int off, i
         v[c] = (lane == c) ? p * rs : v[c] * rs;
         double pn = 1.0, rn = 1.0;
         if (c + 1 < 16) {
+            // lane c + 1 holds L(c + 1, c) itself: it forms the next pivot without waiting
+            // for the broadcast that the other lanes' update of column c + 1 needs (the same
+            // fused multiply-add, so the same value as that update gives)
+            const double own = v[c + 1] - v[c] * v[c];
+            pn = __shfl_sync(FULL, own, c + 1);
             const double l1 = __shfl_sync(FULL, v[c], c + 1);
             if (lane >= c + 1) v[c + 1] -= v[c] * l1;
-            pn = __shfl_sync(FULL, v[c + 1], c + 1);
             if (!(pn > 0.0)) bad = true;
             rn = rsqrt(pn);
         }

@@ -1,6 +1,7 @@
 // Dense SDP cone, scalar bound cone, Schur (KKT) system and Lanczos step
 // estimator of the B200 HDSDP solver.
 #include "solver.h"
+#include <cooperative_groups.h>
 #include <cmath>
 #include <cstring>
 #include <cstdlib>
@@ -1146,6 +1147,133 @@ __global__ void lanczos_resid_kernel(int n, double *z, const double *x, double l
     if (threadIdx.x == 0) *out = v;
 }
 
+// ---- Lanczos steps of larger blocks in one cooperative launch per check interval.
+//
+// Steps k0 .. k1-1 of the three-term recurrence for M = K (-D) K^T (K = L^-1 lower,
+// KT = K^T), taken exactly as lanczos_orth_kernel takes them (w = M v_k - beta v_{k-1},
+// alpha = w.v_k, w -= alpha v_k, beta = |w|, v_{k+1} = w / beta when beta > 0). Block b
+// owns columns [b*cpb, (b+1)*cpb) of every product and reduces each column with
+// kLzWpc warps; the dot products go through per-block partial sums that every block
+// adds up in the same order, so all blocks hold the same alpha and beta. Four grid-wide
+// barriers per step. Values written inside the launch are read with ld.global.cg.
+constexpr int kLzThreads = 1024, kLzWpc = 4;
+constexpr int kLzCols = kLzThreads / 32 / kLzWpc;   // columns per block and pass
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// out[j] = scale * sum_i A(i, j) x[i] over the rows of column j that `mode` keeps
+// (0 all, 1 i >= j, 2 i <= j), for the block's columns [j0, j1).
+__device__ void lz_block_coldot(int n, const double *__restrict__ A, long lda, const double *x, double *out,
+                                double scale, int mode, int j0, int j1, double *red) {
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int cslot = w / kLzWpc, seg = w % kLzWpc;
+    for (int jb = j0; jb < j1; jb += kLzCols) {
+        const int j = jb + cslot;
+        double acc = 0.0;
+        if (j < j1) {
+            const int lo = (mode == 1) ? j : 0, hi = (mode == 2) ? j + 1 : n;
+            const int len = hi - lo;
+            const int chunk = (((len + kLzWpc - 1) / kLzWpc) + 31) & ~31;
+            const int a0 = lo + seg * chunk, a1 = min(hi, a0 + chunk);
+            const double *col = A + (size_t) j * lda;
+            int k = a0 + lane;
+            for (; k + 32 < a1; k += 64) acc += __ldg(col + k) * __ldcg(x + k) + __ldg(col + k + 32) * __ldcg(x + k + 32);
+            for (; k < a1; k += 32) acc += __ldg(col + k) * __ldcg(x + k);
+        }
+        acc = warp_sum(acc);
+        if (lane == 0) red[w] = acc;
+        __syncthreads();
+        if (threadIdx.x < kLzCols && jb + (int) threadIdx.x < j1) {
+            double t = 0.0;
+#pragma unroll
+            for (int q = 0; q < kLzWpc; ++q) t += red[threadIdx.x * kLzWpc + q];
+            out[jb + threadIdx.x] = scale * t;
+        }
+        __syncthreads();
+    }
+}
+
+// sum of part[0 .. G) in a fixed order, the same in every block
+__device__ double lz_grid_sum(const double *part, int G, double *red) {
+    if (threadIdx.x < 32) {
+        double v = 0.0;
+        for (int q = threadIdx.x; q < G; q += 32) v += __ldcg(part + q);
+        v = warp_sum(v);
+        if (threadIdx.x == 0) red[0] = v;
+    }
+    __syncthreads();
+    const double v = red[0];
+    __syncthreads();
+    return v;
+}
+
+__global__ void __launch_bounds__(kLzThreads, 1)
+    lanczos_steps_kernel(int n, const double *K, const double *KT, long ldk, const double *D, long ldD, double *V,
+                         long ldv, double *ab, int maxdim, int k0, int k1, double *t, double *u, double *w,
+                         double *part) {
+    cooperative_groups::grid_group grid = cooperative_groups::this_grid();
+    __shared__ double red[kLzThreads / 32];
+    const int G = gridDim.x;
+    const int cpb = (n + G - 1) / G;
+    const int j0 = min(n, (int) blockIdx.x * cpb), j1 = min(n, j0 + cpb);
+    for (int k = k0; k < k1; ++k) {
+        const double *vk = V + (size_t) k * ldv;
+        lz_block_coldot(n, K, ldk, vk, t, 1.0, 1, j0, j1, red);     // t = K^T v_k
+        grid.sync();
+        lz_block_coldot(n, D, ldD, t, u, -1.0, 0, j0, j1, red);     // u = -D t
+        grid.sync();
+        lz_block_coldot(n, KT, ldk, u, w, 1.0, 2, j0, j1, red);     // w = K u
+        // w -= beta_{k-1} v_{k-1}; partial w.v_k (own columns, written by this block)
+        const double bprev = (k > 0) ? __ldcg(ab + maxdim + k - 1) : 0.0;
+        double pa = 0.0;
+        for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
+            double x = w[j];
+            if (k > 0) x -= bprev * __ldcg(V + (size_t) (k - 1) * ldv + j);
+            w[j] = x;
+            pa += x * __ldcg(vk + j);
+        }
+        pa = warp_sum(pa);
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = pa;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double v = 0.0;
+            for (int q = 0; q < kLzThreads / 32; ++q) v += red[q];
+            part[blockIdx.x] = v;
+        }
+        grid.sync();
+        const double alp = lz_grid_sum(part, G, red);
+        double pn = 0.0;
+        for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
+            const double x = w[j] - alp * __ldcg(vk + j);
+            w[j] = x;
+            pn += x * x;
+        }
+        pn = warp_sum(pn);
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = pn;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double v = 0.0;
+            for (int q = 0; q < kLzThreads / 32; ++q) v += red[q];
+            part[G + blockIdx.x] = v;
+        }
+        grid.sync();
+        const double nrm = sqrt(lz_grid_sum(part + G, G, red));
+        if (nrm > 0.0) {
+            double *vn = V + (size_t) (k + 1) * ldv;
+            for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) vn[j] = w[j] / nrm;
+        }
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            ab[k] = alp;
+            if (nrm > 0.0) ab[maxdim + k] = nrm;
+        }
+        grid.sync();
+    }
+}
+
 // ---- Lanczos for blocks of order <= kSmallLanczosN: one CTA holds K = L^-1, D and the
 // Lanczos basis in shared memory and runs every step in one launch (the stepwise path
 // spends four launches per step, which dominates for small blocks).
@@ -1345,6 +1473,7 @@ void Lanczos::init(int n_, cudaStream_t s_) {
     for (double **p : {&w, &z1, &z2, &t1, &u, &warm, &init_vec, &pert_vec}) HB_CUDA(hb::cmalloc(p, sizeof(double) * ld));
     HB_CUDA(hb::cmalloc(&d_ab, sizeof(double) * (2 * maxdim + 2)));
     HB_CUDA(hb::cmalloc_host(&h_ab, sizeof(double) * (2 * maxdim + 2)));
+    HB_CUDA(hb::cmalloc(&part, sizeof(double) * 2 * kLanczosMaxBlocks));
     HB_CUDA(hb::cmalloc(&d_y, sizeof(double) * 2 * (maxdim + 1)));
     HB_CUDA(hb::cmalloc(&d_scal, sizeof(double) * 4));
     HB_CUDA(hb::cmalloc_host(&h_scal, sizeof(double) * 4));
@@ -1373,7 +1502,7 @@ void Lanczos::init(int n_, cudaStream_t s_) {
 }
 
 void Lanczos::release() {
-    for (double **p : {&V, &w, &z1, &z2, &t1, &u, &warm, &init_vec, &pert_vec, &d_ab, &d_y, &d_scal}) {
+    for (double **p : {&V, &w, &z1, &z2, &t1, &u, &warm, &init_vec, &pert_vec, &d_ab, &d_y, &d_scal, &part}) {
         if (*p) hb::cache_free(*p);
         *p = nullptr;
     }
@@ -1429,18 +1558,49 @@ hdsdp_retcode Lanczos::solve(DenseFactor &F, const double *D, long ldD, double *
         if (nComputed == 0) lanczos_start_kernel<<<hb::counted(1), 1024, 0, s>>>(n, nullptr, init_vec, V);
         else lanczos_start_kernel<<<hb::counted(1), 1024, 0, s>>>(n, warm, pert_vec, V);
     }
+    // dense factor: the steps up to each check run in one cooperative launch
+    const bool fused = !small && !hyOp;
+    int lzGrid = 0;
+    if (fused) {
+        static std::atomic<int> capacity[kMaxDevices];
+        int cap = capacity[current_device()].load(std::memory_order_relaxed);
+        if (!cap) {
+            int per = 0;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, lanczos_steps_kernel, kLzThreads, 0);
+            cap = std::max(1, per) * device_sm_count();
+            capacity[current_device()].store(cap, std::memory_order_relaxed);
+        }
+        lzGrid = std::max(1, std::min(std::min(cap, kLanczosMaxBlocks), (n + kLzCols - 1) / kLzCols));
+    }
+    int stepsDone = 0;
 
     hdsdp_retcode ret = HDSDP_RETCODE_OK;
     bool done = false;
     int lastChecked = -1;
     const int freq = std::min(maxdim / 5, 3);
     std::vector<double> T, ev, evec;
+    auto scheduled = [&](int k) { return ((k + 1) % freq == 0) || k >= maxdim - 1; };
     for (int k = 0; k < maxdim && !done; ++k) {
-        if (!small) {
+        if (fused) {
+            if (k >= stepsDone) {
+                int k1 = k;
+                while (!scheduled(k1)) ++k1;
+                k1 += 1;  // through the next check
+                const double *Kp = F.K, *KTp = F.KT, *Dp = D;
+                long ldk = F.ld, ldd = ldD, ldv = ld;
+                int nn = n, md = maxdim, ka = k, kb = k1;
+                double *Vp = V, *abp = d_ab, *tp = t1, *up = u, *wp = w, *pp = part;
+                void *args[] = {&nn, &Kp, &KTp, &ldk, &Dp, &ldd, &Vp, &ldv, &abp, &md, &ka, &kb, &tp, &up, &wp, &pp};
+                HB_CUDA(cudaLaunchCooperativeKernel((const void *) lanczos_steps_kernel, hb::counted(lzGrid),
+                                                    kLzThreads, args, 0, s));
+                if (tm) tm->n_lanczos_mv += k1 - k;
+                stepsDone = k1;
+            }
+        } else if (!small) {
             mv(V + (size_t) k * ld, w);
             lanczos_orth_kernel<<<hb::counted(1), 1024, 0, s>>>(n, V, ld, k, w, d_ab, maxdim);
         }
-        const bool sched = ((k + 1) % freq == 0) || k >= maxdim - 1;
+        const bool sched = scheduled(k);
         if (!sched) continue;
         if (!small) {
             HB_CUDA(cudaMemcpyAsync(h_ab, d_ab, sizeof(double) * (2 * maxdim + 2), cudaMemcpyDeviceToHost, s));

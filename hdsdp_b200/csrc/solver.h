@@ -45,6 +45,7 @@ struct Timers {
 };
 
 // Lanczos maximum-step estimator (linalg/hdsdp_lanczos.c:161-292) on the GPU.
+constexpr int kLanczosMaxBlocks = 1024;   // grid bound of the fused Lanczos steps
 struct Lanczos {
     int n = 0, maxdim = 30;
     long ld = 0;
@@ -55,6 +56,7 @@ struct Lanczos {
     double *d_y = nullptr;    // 2 * (maxdim + 1)
     double *d_scal = nullptr, *h_scal = nullptr;
     double *init_vec = nullptr, *pert_vec = nullptr;  // device, deterministic per n
+    double *part = nullptr;   // per-block partial sums of the fused steps (2 x kLanczosMaxBlocks)
     int nComputed = 0;
     // when set, the operator is built from this sparse factor of S instead of F
     HybridFactor *hyOp = nullptr;

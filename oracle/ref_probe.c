@@ -127,3 +127,16 @@ exit_cleanup:
     (void) retcode;
     return ret;
 }
+
+/*
+ * The dense Schur complement a KKT object holds after HKKTBuildUp (the lower
+ * triangle of kktMatElem, interface/def_hdsdp_schur.h:42-80), copied into the
+ * column-major m x m array Mout. Returns 0, or -1 for a sparse Schur complement.
+ */
+int oracle_kkt_matrix(hdsdp_kkt *kkt, int m, double *Mout) {
+    if (!kkt || kkt->isKKTSparse || !kkt->kktMatElem) return -1;
+    for (int j = 0; j < m; ++j)
+        for (int i = j; i < m; ++i)
+            Mout[(size_t) j * m + i] = kkt->kktMatElem[(size_t) j * m + i];
+    return 0;
+}

@@ -32,8 +32,12 @@ def check_parity(r, ref, psdp=False):
     assert r["dobj"] == pytest.approx(ref["dobj"], rel=tol, abs=1e-8)
     if ref["status"] == OPTIMAL:
         # a run the reference itself ends as NUMERICAL (a gap of percents) has no
-        # meaningful primal objective to compare
-        assert r["pobj"] == pytest.approx(ref["pobj"], rel=tol, abs=1e-8)
+        # meaningful primal objective to compare. After the five fixed refinement steps
+        # the reference declares optimality at a DIMACS error up to 1e-2
+        # (interface/hdsdp.c:878-895): the primal objective is then good only to the
+        # run's own relative gap (err5; 1.4e-3 on theta_n300), and is held to that.
+        ptol = max(tol, ref["errs"][4]) if psdp else tol
+        assert r["pobj"] == pytest.approx(ref["pobj"], rel=ptol, abs=1e-8)
     if ref["status"] == OPTIMAL:
         assert r["errs"][0] <= max(1e-7, 10 * ref["errs"][0])
         assert r["errs"][1] <= 1e-7 and r["errs"][2] <= 1e-7 and r["errs"][3] <= 1e-7
