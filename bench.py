@@ -56,7 +56,7 @@ FAMILY_BOUND = ["tensor", "tensor", "tensor", "hbm", "tensor", "tensor"]
 # DRAM bytes (ncu dram__bytes_read.sum + dram__bytes_write.sum) per launch of a kernel
 # family on a workload, with the ncu summary they were read from.
 TRAFFIC_PER_LAUNCH = {
-    ("rank1_n1000_m2000", "potrf_coop_slack"): (4.52e6, "profiles/potrf_coop_n1000.md (one launch, n = 1000)"),
+    ("rank1_n1000_m2000", "potrf_coop_slack"): (4.53e6, "profiles/potrf_coop_n1000.md (one launch, n = 1000)"),
 }
 REF_SAMPLE_ITERS = 5
 # a complete reference solve of the bench workload takes tens of seconds: time as many

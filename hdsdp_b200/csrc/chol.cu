@@ -231,11 +231,6 @@ __device__ bool potf2_dev(double *L, long ld, int j0, int nb, double *Dinv, long
     for (int idx = tid; idx < 64 * 64; idx += blockDim.x) X[(idx & 63) + (idx >> 6) * TP] = 0.0;
     cpa_wait_all();
     if (tid == 0) fail = 0;
-    __syncthreads();
-    if (staged || Pp) {
-        smem_mma(T, P, P, 1, 64, 64, 64, -1.0, true, true);
-        __syncthreads();
-    }
     for (int r = nb + tid; r < 64; r += blockDim.x) T[r + r * TP] = 1.0;  // pad with the identity
     __syncthreads();
     const int sb = 4096 + (j0 / 64) * 32;
@@ -243,6 +238,22 @@ __device__ bool potf2_dev(double *L, long ld, int j0, int nb, double *Dinv, long
     CHOL_STAMP(sb);
     const int nwork = (int) (blockDim.x >> 5) - 1;
     auto bar_workers = [nwork]() { asm volatile("bar.sync 1, %0;\n" ::"r"(32 * nwork) : "memory"); };
+    // The update A_jj -= P P^T by the previous panel's rows: warp 0 updates the first 16 x 16
+    // diagonal block and starts factoring it while the other warps update the rest (the
+    // padded rows of P are zero, so the identity padding survives).
+    if (staged || Pp) {
+        if (warp == 0) {
+            smem_mma(T, P, P, 1, 16, 16, 64, -1.0, true, true, 0, 1);
+            __syncwarp();
+        } else {
+            smem_mma(T + 16, P + 16, P, 1, 48, 16, 64, -1.0, true, false, 1, nwork);
+            smem_mma(T + 16 + 16 * TP, P + 16, P + 16, 1, 48, 48, 64, -1.0, true, true, 1, nwork);
+        }
+    }
+    // Four 16-column sweeps with a one-block look-ahead: after sweep s and the panel below
+    // it, warp 0 updates only the next diagonal block and goes on to factor it, while the
+    // other warps apply the rest of the trailing update (and a block row of the inverse);
+    // sweep s + 1 touches only the next diagonal block of T and of X.
     for (int s0 = 0; s0 < 64; s0 += 16) {
         if (warp == 0) {
             const bool ok = warp_chol_inv16(T, X, s0, lane);
@@ -256,15 +267,28 @@ __device__ bool potf2_dev(double *L, long ld, int j0, int nb, double *Dinv, long
         if (fail) break;
         const int rem = 64 - s0 - 16;
         if (rem > 0) {
-            // panel below: P = T_below X_ss^T; then T22 -= P P^T and the panel into T
+            // panel below: P = T_below X_ss^T (all warps)
             smem_mma(P + s0 + 16, T + (s0 + 16) + s0 * TP, X + s0 + s0 * TP, 1, rem, 16, 16, 1.0, false, false);
             __syncthreads();
-            smem_mma(T + (s0 + 16) + (s0 + 16) * TP, P + s0 + 16, P + s0 + 16, 1, rem, rem, 16, -1.0, true, true);
-            for (int idx = tid; idx < rem * 16; idx += blockDim.x) {
-                const int r = s0 + 16 + (idx & 15) + 16 * (idx >> 8), c = (idx >> 4) & 15;
-                T[r + (s0 + c) * TP] = P[r + c * TP];
+            if (warp == 0) {
+                // the next diagonal block and its rows of the panel
+                const int r0 = s0 + 16;
+                smem_mma(T + r0 + r0 * TP, P + r0, P + r0, 1, 16, 16, 16, -1.0, true, true, 0, 1);
+                for (int idx = lane; idx < 256; idx += 32) {
+                    const int r = r0 + (idx & 15), c = idx >> 4;
+                    T[r + (s0 + c) * TP] = P[r + c * TP];
+                }
+                __syncwarp();
+            } else if (rem > 16) {
+                // rows below the next diagonal block: T[r1.., r0..] -= P_rest [P_next; P_rest]^T
+                const int r0 = s0 + 16, r1 = s0 + 32, rr = rem - 16;
+                smem_mma(T + r1 + r0 * TP, P + r1, P + r0, 1, rr, 16, 16, -1.0, true, false, 1, nwork);
+                smem_mma(T + r1 + r1 * TP, P + r1, P + r1, 1, rr, rr, 16, -1.0, true, true, 1, nwork);
+                for (int idx = tid - 32; idx < rr * 16; idx += 32 * nwork) {
+                    const int r = r1 + (idx & 15) + 16 * (idx >> 8), c = (idx >> 4) & 15;
+                    T[r + (s0 + c) * TP] = P[r + c * TP];
+                }
             }
-            __syncthreads();
         }
         CHOL_STAMP(sb + 2 + (s0 >> 4) * 2);
     }

@@ -1158,6 +1158,8 @@ __global__ void lanczos_resid_kernel(int n, double *z, const double *x, double l
 // barriers per step. Values written inside the launch are read with ld.global.cg.
 constexpr int kLzThreads = 1024, kLzWpc = 4;
 constexpr int kLzCols = kLzThreads / 32 / kLzWpc;   // columns per block and pass
+constexpr int kLzSmemMax = 200 * 1024;              // dynamic shared memory of the cached variant
+constexpr int kLzFusedMaxN = 2048;                  // K, K^T and D (3 x 8 n^2 bytes) still fit the L2
 
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
@@ -1211,6 +1213,68 @@ __device__ double lz_grid_sum(const double *part, int G, double *red) {
     return v;
 }
 
+// The block's columns held in shared memory for the whole launch: region K (column j,
+// rows j..n-1), region KT (rows 0..j), region D (rows 0..n-1), packed column after column;
+// a block with cpb columns holds cpb (2n + 1) doubles. Local column c starts at
+// c (n - j0) - c (c - 1) / 2 in K, c (j0 + 1) + c (c - 1) / 2 in KT and c n in D.
+__host__ __device__ inline long lz_cached_doubles(int n, int cpb) { return (long) cpb * (2L * n + 1); }
+
+// w -= beta_{k-1} v_{k-1} and the block's partial w.v_k into part[blockIdx.x]
+__device__ void lz_orth_partial(int j0, int j1, int k, const double *V, long ldv, const double *ab, int maxdim,
+                                double *w, double *part, double *red) {
+    const double *vk = V + (size_t) k * ldv;
+    const double bprev = (k > 0) ? __ldcg(ab + maxdim + k - 1) : 0.0;
+    double pa = 0.0;
+    for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
+        double x = w[j];
+        if (k > 0) x -= bprev * __ldcg(V + (size_t) (k - 1) * ldv + j);
+        w[j] = x;
+        pa += x * __ldcg(vk + j);
+    }
+    pa = warp_sum(pa);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = pa;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double v = 0.0;
+        for (int q = 0; q < kLzThreads / 32; ++q) v += red[q];
+        part[blockIdx.x] = v;
+    }
+}
+
+// w -= alpha v_k and the block's partial |w|^2 into part[G + blockIdx.x]
+__device__ void lz_norm_partial(int j0, int j1, int k, double alp, const double *V, long ldv, double *w, double *part,
+                                int G, double *red) {
+    const double *vk = V + (size_t) k * ldv;
+    double pn = 0.0;
+    for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
+        const double x = w[j] - alp * __ldcg(vk + j);
+        w[j] = x;
+        pn += x * x;
+    }
+    pn = warp_sum(pn);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = pn;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double v = 0.0;
+        for (int q = 0; q < kLzThreads / 32; ++q) v += red[q];
+        part[G + blockIdx.x] = v;
+    }
+}
+
+// v_{k+1} = w / beta over the block's columns; alpha and beta recorded by block 0
+__device__ void lz_next(int j0, int j1, int k, double alp, double nrm, double *V, long ldv, double *ab, int maxdim,
+                        const double *w) {
+    if (nrm > 0.0) {
+        double *vn = V + (size_t) (k + 1) * ldv;
+        for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) vn[j] = w[j] / nrm;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        ab[k] = alp;
+        if (nrm > 0.0) ab[maxdim + k] = nrm;
+    }
+}
+
+// Streaming variant: the block's columns of K, K^T and D are read from L2 in every step.
 __global__ void __launch_bounds__(kLzThreads, 1)
     lanczos_steps_kernel(int n, const double *K, const double *KT, long ldk, const double *D, long ldD, double *V,
                          long ldv, double *ab, int maxdim, int k0, int k1, double *t, double *u, double *w,
@@ -1227,7 +1291,121 @@ __global__ void __launch_bounds__(kLzThreads, 1)
         lz_block_coldot(n, D, ldD, t, u, -1.0, 0, j0, j1, red);     // u = -D t
         grid.sync();
         lz_block_coldot(n, KT, ldk, u, w, 1.0, 2, j0, j1, red);     // w = K u
-        // w -= beta_{k-1} v_{k-1}; partial w.v_k (own columns, written by this block)
+        lz_orth_partial(j0, j1, k, V, ldv, ab, maxdim, w, part, red);
+        grid.sync();
+        const double alp = lz_grid_sum(part, G, red);
+        lz_norm_partial(j0, j1, k, alp, V, ldv, w, part, G, red);
+        grid.sync();
+        const double nrm = sqrt(lz_grid_sum(part + G, G, red));
+        lz_next(j0, j1, k, alp, nrm, V, ldv, ab, maxdim, w);
+        grid.sync();
+    }
+}
+
+// Shared-memory variant (n small enough for a block's share of columns to fit): the
+// block's columns of K, K^T and D are loaded into shared memory once per launch
+// (lz_cached_doubles(n, cpb) doubles) and each product's input vector is staged there (n
+// more doubles); kLzWpc warps reduce each column. v_{k+1} = w / beta is read by the next
+// step's first product straight from w (the last grid barrier of a step publishes w, and
+// every block holds beta), so a step takes four grid-wide barriers.
+__global__ void __launch_bounds__(kLzThreads, 1)
+    lanczos_steps_smem_kernel(int n, const double *K, const double *KT, long ldk, const double *D, long ldD,
+                              double *V, long ldv, double *ab, int maxdim, int k0, int k1, double *w, double *tg,
+                              double *ug, double *part) {
+    cooperative_groups::grid_group grid = cooperative_groups::this_grid();
+    __shared__ double red[kLzThreads / 32];
+    __shared__ double scal[2];
+    extern __shared__ double dyn[];
+    const int G = gridDim.x;
+    const int cpb = (n + G - 1) / G;
+    const int j0 = min(n, (int) blockIdx.x * cpb), j1 = min(n, j0 + cpb);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = kLzThreads / 32;
+    const long nc = j1 - j0;
+    double *sK = dyn;
+    double *sKT = sK + (nc * (n - j0) - nc * (nc - 1) / 2);
+    double *sD = sKT + (nc * (j0 + 1) + nc * (nc - 1) / 2);
+    double *sx = dyn + lz_cached_doubles(n, cpb);
+    for (long c = 0; c < nc; ++c) {
+        const int j = j0 + (int) c;
+        double *dk = sK + c * (n - j0) - c * (c - 1) / 2;
+        double *dkt = sKT + c * (j0 + 1) + c * (c - 1) / 2;
+        double *dd = sD + c * n;
+        const double *gk = K + (size_t) j * ldk, *gkt = KT + (size_t) j * ldk, *gd = D + (size_t) j * ldD;
+        for (int i = j + threadIdx.x; i < n; i += blockDim.x) dk[i - j] = __ldg(gk + i);
+        for (int i = threadIdx.x; i <= j; i += blockDim.x) dkt[i] = __ldg(gkt + i);
+        for (int i = threadIdx.x; i < n; i += blockDim.x) dd[i] = __ldg(gd + i);
+    }
+    // sx = x / div (div 0: zeros; the same division that forms v_{k+1})
+    auto stage = [&](const double *x, double div) {
+        for (int i = threadIdx.x; i < n; i += blockDim.x)
+            sx[i] = (div == 1.0) ? __ldcg(x + i) : (div > 0.0) ? __ldcg(x + i) / div : 0.0;
+        __syncthreads();
+    };
+    // out[j] = scale * sum over the rows `mode` keeps (0 all, 1 i >= j, 2 i <= j) of column j
+    const int cslot = warp / kLzWpc, seg = warp % kLzWpc;
+    auto coldot = [&](int mode, const double *reg, double *out, double scale) {
+        for (int jb = j0; jb < j1; jb += kLzCols) {
+            const int j = jb + cslot;
+            double acc = 0.0;
+            if (j < j1) {
+                const long c = j - j0;
+                const int lo = (mode == 1) ? j : 0, hi = (mode == 2) ? j + 1 : n;
+                const double *col = (mode == 1)   ? reg + c * (n - j0) - c * (c - 1) / 2 - lo
+                                    : (mode == 2) ? reg + c * (j0 + 1) + c * (c - 1) / 2
+                                                  : reg + c * n;
+                const int len = hi - lo;
+                const int chunk = (((len + kLzWpc - 1) / kLzWpc) + 31) & ~31;
+                const int a0 = lo + seg * chunk, a1 = min(hi, a0 + chunk);
+                for (int k = a0 + lane; k < a1; k += 32) acc += col[k] * sx[k];
+            }
+            acc = warp_sum(acc);
+            if (lane == 0) red[warp] = acc;
+            __syncthreads();
+            if (threadIdx.x < kLzCols && jb + (int) threadIdx.x < j1) {
+                double t = 0.0;
+#pragma unroll
+                for (int q = 0; q < kLzWpc; ++q) t += red[threadIdx.x * kLzWpc + q];
+                out[jb + threadIdx.x] = scale * t;
+            }
+            if (jb + kLzCols < j1) __syncthreads();   // red is reused by the next pass
+        }
+    };
+    // block total of v (one value per thread) into *slot
+    auto block_part = [&](double v, double *slot) {
+        v = warp_sum(v);
+        if (lane == 0) red[warp] = v;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double tot = 0.0;
+            for (int q = 0; q < nwarp; ++q) tot += red[q];
+            *slot = tot;
+        }
+    };
+    // sum of p[0 .. G) in a fixed order, the same in every block
+    auto grid_total = [&](const double *p, int which) {
+        if (warp == 0) {
+            double v = 0.0;
+            for (int q = lane; q < G; q += 32) v += __ldcg(p + q);
+            v = warp_sum(v);
+            if (lane == 0) scal[which] = v;
+        }
+        __syncthreads();
+        return scal[which];
+    };
+    double nrmPrev = 0.0;
+    for (int k = k0; k < k1; ++k) {
+        const double *vk = V + (size_t) k * ldv;
+        if (k > k0) stage(w, nrmPrev);
+        else stage(vk, 1.0);
+        coldot(1, sK, tg, 1.0);     // t = K^T v_k
+        grid.sync();
+        stage(tg, 1.0);
+        coldot(0, sD, ug, -1.0);    // u = -D t
+        grid.sync();
+        stage(ug, 1.0);
+        coldot(2, sKT, w, 1.0);     // w = K u
+        __syncthreads();
+        // w -= beta_{k-1} v_{k-1}; partial w.v_k
         const double bprev = (k > 0) ? __ldcg(ab + maxdim + k - 1) : 0.0;
         double pa = 0.0;
         for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
@@ -1236,41 +1414,20 @@ __global__ void __launch_bounds__(kLzThreads, 1)
             w[j] = x;
             pa += x * __ldcg(vk + j);
         }
-        pa = warp_sum(pa);
-        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = pa;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            double v = 0.0;
-            for (int q = 0; q < kLzThreads / 32; ++q) v += red[q];
-            part[blockIdx.x] = v;
-        }
+        block_part(pa, part + blockIdx.x);
         grid.sync();
-        const double alp = lz_grid_sum(part, G, red);
+        const double alp = grid_total(part, 0);
         double pn = 0.0;
         for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
             const double x = w[j] - alp * __ldcg(vk + j);
             w[j] = x;
             pn += x * x;
         }
-        pn = warp_sum(pn);
-        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = pn;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            double v = 0.0;
-            for (int q = 0; q < kLzThreads / 32; ++q) v += red[q];
-            part[G + blockIdx.x] = v;
-        }
+        block_part(pn, part + G + blockIdx.x);
         grid.sync();
-        const double nrm = sqrt(lz_grid_sum(part + G, G, red));
-        if (nrm > 0.0) {
-            double *vn = V + (size_t) (k + 1) * ldv;
-            for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) vn[j] = w[j] / nrm;
-        }
-        if (blockIdx.x == 0 && threadIdx.x == 0) {
-            ab[k] = alp;
-            if (nrm > 0.0) ab[maxdim + k] = nrm;
-        }
-        grid.sync();
+        const double nrm = sqrt(grid_total(part + G, 1));
+        lz_next(j0, j1, k, alp, nrm, V, ldv, ab, maxdim, w);
+        nrmPrev = nrm;
     }
 }
 
@@ -1558,19 +1715,47 @@ hdsdp_retcode Lanczos::solve(DenseFactor &F, const double *D, long ldD, double *
         if (nComputed == 0) lanczos_start_kernel<<<hb::counted(1), 1024, 0, s>>>(n, nullptr, init_vec, V);
         else lanczos_start_kernel<<<hb::counted(1), 1024, 0, s>>>(n, warm, pert_vec, V);
     }
-    // dense factor: the steps up to each check run in one cooperative launch
-    const bool fused = !small && !hyOp;
+    // dense factor: the steps up to each check run in one cooperative launch; with the
+    // columns of K, K^T and D held in shared memory when one block's share fits. Above
+    // kLzFusedMaxN the three matrices stream from DRAM, where the per-step launches keep
+    // more loads in flight than the cooperative grid.
+    const bool fused = !small && !hyOp && n <= kLzFusedMaxN;
     int lzGrid = 0;
+    bool lzCached = false;
+    size_t lzSmem = 0;
     if (fused) {
-        static std::atomic<int> capacity[kMaxDevices];
-        int cap = capacity[current_device()].load(std::memory_order_relaxed);
+        static std::atomic<int> capacity[kMaxDevices][2];
+        static std::atomic<unsigned long long> attr{0};
+        once_per_device(attr, [] {
+            HB_CUDA(cudaFuncSetAttribute((const void *) lanczos_steps_smem_kernel,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, kLzSmemMax));
+        });
+        const int sms = device_sm_count();
+        const int cpbCached = (n + sms - 1) / sms;
+        const size_t need = sizeof(double) * (size_t) (lz_cached_doubles(n, cpbCached) + n);
+        lzCached = need <= (size_t) kLzSmemMax;
+        const int slot = lzCached ? 1 : 0;
+        int cap = capacity[current_device()][slot].load(std::memory_order_relaxed);
         if (!cap) {
             int per = 0;
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, lanczos_steps_kernel, kLzThreads, 0);
-            cap = std::max(1, per) * device_sm_count();
-            capacity[current_device()].store(cap, std::memory_order_relaxed);
+            if (lzCached)
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, lanczos_steps_smem_kernel, kLzThreads, kLzSmemMax);
+            else
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, lanczos_steps_kernel, kLzThreads, 0);
+            cap = std::max(1, per) * sms;
+            capacity[current_device()][slot].store(cap, std::memory_order_relaxed);
         }
-        lzGrid = std::max(1, std::min(std::min(cap, kLanczosMaxBlocks), (n + kLzCols - 1) / kLzCols));
+        if (lzCached) {
+            // one block per SM, so that every block's columns fit its shared memory
+            lzGrid = std::min(std::min(cap, sms), kLanczosMaxBlocks);
+            const int cpb = (n + lzGrid - 1) / lzGrid;
+            lzSmem = sizeof(double) * (size_t) (lz_cached_doubles(n, cpb) + n);
+            if (lzSmem > (size_t) kLzSmemMax) lzCached = false;
+        }
+        if (!lzCached) {
+            lzSmem = 0;
+            lzGrid = std::max(1, std::min(std::min(cap, kLanczosMaxBlocks), (n + kLzCols - 1) / kLzCols));
+        }
     }
     int stepsDone = 0;
 
@@ -1590,9 +1775,15 @@ hdsdp_retcode Lanczos::solve(DenseFactor &F, const double *D, long ldD, double *
                 long ldk = F.ld, ldd = ldD, ldv = ld;
                 int nn = n, md = maxdim, ka = k, kb = k1;
                 double *Vp = V, *abp = d_ab, *tp = t1, *up = u, *wp = w, *pp = part;
-                void *args[] = {&nn, &Kp, &KTp, &ldk, &Dp, &ldd, &Vp, &ldv, &abp, &md, &ka, &kb, &tp, &up, &wp, &pp};
-                HB_CUDA(cudaLaunchCooperativeKernel((const void *) lanczos_steps_kernel, hb::counted(lzGrid),
-                                                    kLzThreads, args, 0, s));
+                if (lzCached) {
+                    void *args[] = {&nn, &Kp, &KTp, &ldk, &Dp, &ldd, &Vp, &ldv, &abp, &md, &ka, &kb, &wp, &tp, &up, &pp};
+                    HB_CUDA(cudaLaunchCooperativeKernel((const void *) lanczos_steps_smem_kernel, hb::counted(lzGrid),
+                                                        kLzThreads, args, lzSmem, s));
+                } else {
+                    void *args[] = {&nn, &Kp, &KTp, &ldk, &Dp, &ldd, &Vp, &ldv, &abp, &md, &ka, &kb, &tp, &up, &wp, &pp};
+                    HB_CUDA(cudaLaunchCooperativeKernel((const void *) lanczos_steps_kernel, hb::counted(lzGrid),
+                                                        kLzThreads, args, 0, s));
+                }
                 if (tm) tm->n_lanczos_mv += k1 - k;
                 stepsDone = k1;
             }

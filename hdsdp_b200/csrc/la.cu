@@ -972,11 +972,22 @@ __global__ void axpy_kernel(int n, double a, const double *x, double *y) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) y[i] += a * x[i];
 }
 
+// Upper triangle := lower triangle, by 32 x 32 tiles: the block of tile (bi, bj), bi <= bj,
+// reads lower tile (bj, bi) along its columns into shared memory and writes upper tile
+// (bi, bj) along its columns, so both sides are coalesced.
 __global__ void symlower_kernel(int n, double *A, long lda) {
-    const long total = (long) n * n;
-    for (long idx = blockIdx.x * (long) blockDim.x + threadIdx.x; idx < total; idx += (long) gridDim.x * blockDim.x) {
-        int r = (int) (idx % n), c = (int) (idx / n);
-        if (r < c) A[(size_t) r + (size_t) c * lda] = A[(size_t) c + (size_t) r * lda];
+    __shared__ double tile[32][33];
+    const int bi = blockIdx.x, bj = blockIdx.y;
+    if (bi > bj) return;
+    const int tx = threadIdx.x, ty = threadIdx.y;   // 32 x 8 threads
+    for (int k = ty; k < 32; k += 8) {
+        const int r = bj * 32 + tx, c = bi * 32 + k;   // lower tile (bj, bi): row r, column c
+        if (r < n && c < n && r >= c) tile[k][tx] = A[(size_t) r + (size_t) c * lda];
+    }
+    __syncthreads();
+    for (int k = ty; k < 32; k += 8) {
+        const int r = bi * 32 + tx, c = bj * 32 + k;   // upper tile (bi, bj): row r, column c = element (c, r)
+        if (r < n && c < n && r < c) A[(size_t) r + (size_t) c * lda] = tile[tx][k];
     }
 }
 
@@ -1096,7 +1107,9 @@ void axpy(cudaStream_t s, int n, double a, const double *x, double *y) {
 }
 
 void symmetrize_lower(cudaStream_t s, int n, double *A, long lda) {
-    symlower_kernel<<<hb::counted(grid_for((long) n * n)), 256, 0, s>>>(n, A, lda);
+    if (n <= 0) return;
+    const int nt = (n + 31) / 32;
+    symlower_kernel<<<hb::counted(dim3(nt, nt)), dim3(32, 8), 0, s>>>(n, A, lda);
 }
 
 void symmetrize_avg(cudaStream_t s, int n, double *A, long lda) {

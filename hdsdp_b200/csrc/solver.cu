@@ -1355,30 +1355,42 @@ exit_cleanup:
 
 // Smallest eigenvalue sign test of X: Cholesky succeeds -> lambda_min > 0; otherwise the
 // most negative eigenvalue is bracketed by bisection on X + sigma I.
+// lambda_min(X) for the DIMACS check (the reference calls dsyevr, interface/hdsdp.c:833): 1 if
+// X is positive definite, else -t for the smallest shift t with X + t I positive definite,
+// found by Cholesky attempts: a geometric search up from 1e-14 max|X_ii| by factors of 16,
+// then a geometric bisection to 1e-3 relative (at most about 25 factorisations; a
+// shift below 1e-14 max|X_ii| is reported as that bound).
 double min_eig_estimate(SdpCone &c, double *X) {
     DenseFactor &F = c.Fcheck;
     c.invalidate_check_factor();
     if (factorize(c.s, F, X, c.ld)) return 1.0;
-    double lo = 0.0, hi = 1.0;
+    const int n = c.n;
     double *T = c.dev.T1;
-    for (int it = 0; it < 60; ++it) {
-        copy_matrix(c.s, c.n, c.n, X, c.ld, T, c.ld);
-        add_diag(c.s, c.n, T, c.ld, hi);
-        if (factorize(c.s, F, T, c.ld)) break;
+    double *dgd = c.dev.T2;   // n x ld scratch, free during the check
+    copy_matrix(c.s, 1, n, X, c.ld + 1, dgd, 1);
+    std::vector<double> dg(n);
+    HB_CUDA(cudaMemcpyAsync(dg.data(), dgd, sizeof(double) * n, cudaMemcpyDeviceToHost, c.s));
+    HB_CUDA(cudaStreamSynchronize(c.s));
+    double scale = 1.0;
+    for (double v : dg) scale = std::max(scale, std::fabs(v));
+    auto pd_at = [&](double t) {
+        copy_matrix(c.s, n, n, X, c.ld, T, c.ld);
+        add_diag(c.s, n, T, c.ld, t);
+        return factorize(c.s, F, T, c.ld);
+    };
+    double lo = 0.0, hi = 1e-14 * scale;
+    for (int it = 0; it < 40 && !pd_at(hi); ++it) {
         lo = hi;
-        hi *= 2.0;
+        hi *= 16.0;
     }
-    for (int it = 0; it < 50 && hi - lo > 1e-12 * std::max(1.0, hi); ++it) {
-        const double mid = 0.5 * (lo + hi);
-        copy_matrix(c.s, c.n, c.n, X, c.ld, T, c.ld);
-        add_diag(c.s, c.n, T, c.ld, mid);
-        if (factorize(c.s, F, T, c.ld)) hi = mid;
+    for (int it = 0; it < 40 && lo > 0.0 && hi > lo * (1.0 + 1e-3); ++it) {
+        const double mid = std::sqrt(lo * hi);
+        if (pd_at(mid)) hi = mid;
         else lo = mid;
     }
-    return -0.5 * (lo + hi);
+    return (lo > 0.0) ? -0.5 * (lo + hi) : -hi;
 }
 
-// free the cones' device and host data (the user data stays set)
 void release_cones(hdsdp *h) {
     for (ConeSlot &k : h->cones) {
         if (k.sdp) {
