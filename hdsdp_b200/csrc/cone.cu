@@ -473,6 +473,8 @@ static void copy_factor(cudaStream_t s, DenseFactor &dst, const DenseFactor &src
     }
     dst.factored = true;
     dst.ok = src.ok;
+    dst.logdet_valid = src.logdet_valid;
+    dst.logdet = src.logdet;
 }
 
 hdsdp_retcode SdpCone::update(double tau, const double *y) {
@@ -607,6 +609,10 @@ hdsdp_retcode SdpCone::get_barrier(double tau, const double *y, int which, doubl
     }
     if (which == BUFFER_DUALVAR ? hyVar : hyCheck) {
         *logdet = (which == BUFFER_DUALVAR) ? hyLogdetVar : hyLogdetCheck;
+        return HDSDP_RETCODE_OK;
+    }
+    if (F.logdet_valid) {   // read back with the factorisation's status
+        *logdet = F.logdet;
         return HDSDP_RETCODE_OK;
     }
     log_diag_sum(s, F, d_scal);

@@ -805,9 +805,12 @@ void DenseFactor::alloc(int n_, int fuse_inverse) {
     ld = pad_ld(n);
     HB_CUDA(hb::cmalloc(&L, sizeof(double) * ld * n));
     HB_CUDA(hb::cmalloc(&Dinv, sizeof(double) * ld * NB));
-    HB_CUDA(hb::cmalloc(&d_info, sizeof(int)));
-    HB_CUDA(hb::cmalloc_host(&h_info, sizeof(int)));
+    // the info word and, 8 bytes on, sum log L_ii of the last factorisation
+    HB_CUDA(hb::cmalloc(&d_info, 2 * sizeof(double)));
+    HB_CUDA(hb::cmalloc_host(&h_info, 2 * sizeof(double)));
     *h_info = 0;
+    stat_logdet = true;
+    logdet_valid = false;
     HB_CUDA(cudaMemset(L, 0, sizeof(double) * ld * n));
     HB_CUDA(cudaMemset(Dinv, 0, sizeof(double) * ld * NB));
     fuse_k = (fuse_inverse < 0) ? (n <= kFuseInverseMax) : (fuse_inverse != 0);
@@ -862,9 +865,19 @@ void factorize_async(cudaStream_t s, DenseFactor &F, const double *S, long ldS) 
     F.k_valid = false;
     F.k_pending = false;
     F.factored = true;
+    F.logdet_valid = false;
+    // info word (and sum log L_ii) back to the host in one copy
+    auto status_copy = [&]() {
+        if (F.stat_logdet) {
+            log_diag_sum(s, F, reinterpret_cast<double *>(F.d_info) + 1);
+            HB_CUDA(cudaMemcpyAsync(F.h_info, F.d_info, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+        } else {
+            HB_CUDA(cudaMemcpyAsync(F.h_info, F.d_info, sizeof(int), cudaMemcpyDeviceToHost, s));
+        }
+    };
     if (coop_factorize_enqueue(s, F, S, ldS)) {
         F.k_pending = F.fuse_k && F.K && F.KT;
-        HB_CUDA(cudaMemcpyAsync(F.h_info, F.d_info, sizeof(int), cudaMemcpyDeviceToHost, s));
+        status_copy();
         return;
     }
     zero_int_kernel<<<hb::counted(1), 1, 0, s>>>(F.d_info);
@@ -881,7 +894,7 @@ void factorize_async(cudaStream_t s, DenseFactor &F, const double *S, long ldS) 
             gemm(s, rows, rows, nb, -1.0, P, F.ld, 0, P, F.ld, 1, 1.0, A22, F.ld, GEMM_C_LOWER, F.d_info);
         }
     }
-    HB_CUDA(cudaMemcpyAsync(F.h_info, F.d_info, sizeof(int), cudaMemcpyDeviceToHost, s));
+    status_copy();
     HB_CUDA(cudaGetLastError());
 }
 
@@ -890,6 +903,8 @@ bool factor_status(cudaStream_t s, DenseFactor &F) {
     F.ok = (*F.h_info == 0);
     F.k_valid = F.ok && F.k_pending;  // K and KT were formed by the factorisation kernel
     F.k_pending = false;
+    F.logdet_valid = F.ok && F.stat_logdet;
+    if (F.logdet_valid) F.logdet = 2.0 * reinterpret_cast<const double *>(F.h_info)[1];
     return F.ok;
 }
 

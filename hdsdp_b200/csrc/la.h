@@ -45,6 +45,12 @@ struct DenseFactor {
     double *KT = nullptr;
     int *d_info = nullptr;    // device: 0 = success, k > 0 = pivot k failed
     int *h_info = nullptr;    // pinned host mirror
+    // With stat_logdet set (the default; alloc() makes d_info and h_info 16 bytes each), a
+    // factorisation also writes sum log L_ii next to the info word and both come back in one
+    // copy; factor_status() then holds log det = 2 sum log L_ii in `logdet`.
+    bool stat_logdet = true;
+    bool logdet_valid = false;
+    double logdet = 0.0;
     bool factored = false;
     bool ok = false;
     bool k_valid = false;

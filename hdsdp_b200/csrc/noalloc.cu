@@ -92,6 +92,7 @@ extern "C" int hdsdpb_cholesky_noalloc(int n, const double *S, double *L, double
     F.Dinv = base + 2 * kMatDoubles;
     F.d_info = (int *) (base + 2 * kMatDoubles + (size_t) kLd * 64 + 1);
     F.h_info = &h_info;
+    F.stat_logdet = false;   // the info word alone: the scratch keeps one slot for it
     double *dS = base, *dl = base + 2 * kMatDoubles + (size_t) kLd * 64;
     cudaStream_t s = 0;
     if (cudaMemcpy2D(dS, sizeof(double) * ld, S, sizeof(double) * n, sizeof(double) * n, n,

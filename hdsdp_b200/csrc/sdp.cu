@@ -33,8 +33,11 @@ T *upload_vec(const std::vector<T> &h, cudaStream_t s) {
 // of rows r and c. Launched on a grid of (row blocks, columns c); rows below c return.
 __device__ __forceinline__ long long r1map_pos(int n, int r, int c) { return (long long) (2LL * n - c - 1) * c / 2 + r; }
 
+// Lists longer than this leave the sliced layout for the warp-per-position one.
+constexpr int kLongList = 64;
+
 __global__ void r1map_count_kernel(int n, const int *__restrict__ rptr, const int *__restrict__ rj, int *cnt,
-                                   int *used) {
+                                   int *used, int *longf) {
     const int c = blockIdx.y, r = c + blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= n) return;
     int x = rptr[r], xe = rptr[r + 1], y = rptr[c], ye = rptr[c + 1], k = 0;
@@ -46,17 +49,26 @@ __global__ void r1map_count_kernel(int n, const int *__restrict__ rptr, const in
     }
     const long long q = r1map_pos(n, r, c);
     cnt[q] = k;
-    used[q] = k > 0;
+    used[q] = k > 0 && k <= kLongList;
+    longf[q] = k > kLongList;
 }
 
 // used positions in packed order: row, column and entry count at their slot
+// (short and long positions each in packed order: slot / lslot are their ranks)
 __global__ void r1map_place_kernel(int n, const int *__restrict__ cnt, const int *__restrict__ slot, int *pr, int *pc,
-                                   int *pcnt) {
+                                   int *pcnt, const int *__restrict__ lslot, int *lr, int *lc, long long *llen) {
     const int c = blockIdx.y, r = c + blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= n) return;
     const long long q = r1map_pos(n, r, c);
     const int k = cnt[q];
     if (k == 0) return;
+    if (k > kLongList) {
+        const int sl = lslot[q];
+        lr[sl] = r;
+        lc[sl] = c;
+        llen[sl] = k;
+        return;
+    }
     const int sl = slot[q];
     pr[sl] = r;
     pc[sl] = c;
@@ -74,27 +86,41 @@ __global__ void r1map_slice_kernel(int npos, int nslice, const int *__restrict__
     if (lane == 0) len[sl] = (sl < nslice) ? 32LL * k : 0LL;
 }
 
-// entry e of the position at slot p lands at sptr[p / 32] + 32 e + p % 32, in constraint
-// order, with value s_j a_jr a_jc
+// entry e of the short position at slot p lands at sptr[p / 32] + 32 e + p % 32, that of
+// the long position at lslot p at lptr[p] + e; in constraint order, with value s_j a_jr a_jc
 __global__ void r1map_fill_kernel(int n, const int *__restrict__ rptr, const int *__restrict__ rj,
                                   const double *__restrict__ ra, const double *__restrict__ sgn,
                                   const int *__restrict__ cnt, const int *__restrict__ slot,
-                                  const long long *__restrict__ sptr, int *ej, double *ev) {
+                                  const long long *__restrict__ sptr, int *ej, double *ev,
+                                  const int *__restrict__ lslot, const long long *__restrict__ lptr, int *lj,
+                                  double *lv) {
     const int c = blockIdx.y, r = c + blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= n) return;
     const long long q = r1map_pos(n, r, c);
-    if (cnt[q] == 0) return;
-    const int sl = slot[q];
-    long long at = sptr[sl >> 5] + (sl & 31);
+    const int k = cnt[q];
+    if (k == 0) return;
+    int *dj = ej;
+    double *dv = ev;
+    long long at, step;
+    if (k > kLongList) {
+        at = lptr[lslot[q]];
+        step = 1;
+        dj = lj;
+        dv = lv;
+    } else {
+        const int sl = slot[q];
+        at = sptr[sl >> 5] + (sl & 31);
+        step = 32;
+    }
     int x = rptr[r], xe = rptr[r + 1], y = rptr[c], ye = rptr[c + 1];
     while (x < xe && y < ye) {
         const int a = rj[x], b = rj[y];
         if (a < b) ++x;
         else if (a > b) ++y;
         else {
-            ej[at] = a;
-            ev[at] = sgn[a] * ra[x] * ra[y];
-            at += 32;
+            dj[at] = a;
+            dv[at] = sgn[a] * ra[x] * ra[y];
+            at += step;
             ++x;
             ++y;
         }
@@ -168,6 +194,26 @@ __global__ void s_gather2_kernel(int npos, const int *pr, const int *pc, const l
         const int r = pr[p], c = pc[p];
         S[(size_t) r + (size_t) c * lds] += acc;
         if (r != c) S[(size_t) c + (size_t) r * lds] += acc;
+    }
+}
+
+// The long lists, one warp per position in the contiguous layout: lane l sums entries
+// l, l + 32, ..., then the warp adds its lanes (a fixed order).
+__global__ void s_gather2_long_kernel(int npos, const int *pr, const int *pc, const long long *ptr, const int *ej,
+                                      const double *ev, const double *w, double dA, double *S, long lds) {
+    const int lane = threadIdx.x & 31;
+    for (int p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < npos; p += (gridDim.x * blockDim.x) >> 5) {
+        const long long b = ptr[p], e1 = ptr[p + 1];
+        double acc = 0.0;
+        for (long long e = b + lane; e < e1; e += 32) acc += ev[e] * w[ej[e]];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (lane == 0) {
+            acc *= dA;
+            const int r = pr[p], c = pc[p];
+            S[(size_t) r + (size_t) c * lds] += acc;
+            if (r != c) S[(size_t) c + (size_t) r * lds] += acc;
+        }
     }
 }
 
@@ -551,18 +597,30 @@ void SdpDevice::upload(int n_, int m_, const HostCoeff &C, const std::vector<Hos
             const long long npack = (long long) n * (n + 1) / 2;
             int *d_rptr = upload_vec(rptr, s), *d_rj = upload_vec(rj, s);
             double *d_ra = upload_vec(ra, s), *d_sgn = upload_vec(sgn, s);
-            int *d_cnt = nullptr, *d_used = nullptr, *d_slot = nullptr;
+            int *d_cnt = nullptr, *d_used = nullptr, *d_slot = nullptr, *d_long = nullptr, *d_lslot = nullptr;
             HB_CUDA(hb::cmalloc(&d_cnt, sizeof(int) * npack));
             HB_CUDA(hb::cmalloc(&d_used, sizeof(int) * npack));
             HB_CUDA(hb::cmalloc(&d_slot, sizeof(int) * npack));
+            HB_CUDA(hb::cmalloc(&d_long, sizeof(int) * npack));
+            HB_CUDA(hb::cmalloc(&d_lslot, sizeof(int) * npack));
             const dim3 pgrid((n + 255) / 256, n);
-            r1map_count_kernel<<<hb::counted(pgrid), 256, 0, s>>>(n, d_rptr, d_rj, d_cnt, d_used);
+            r1map_count_kernel<<<hb::counted(pgrid), 256, 0, s>>>(n, d_rptr, d_rj, d_cnt, d_used, d_long);
             exclusive_sum(s, d_used, d_slot, npack);
-            int tail[2] = {0, 0};
+            exclusive_sum(s, d_long, d_lslot, npack);
+            int tail[4] = {0, 0, 0, 0};
             HB_CUDA(cudaMemcpyAsync(&tail[0], d_slot + npack - 1, sizeof(int), cudaMemcpyDeviceToHost, s));
             HB_CUDA(cudaMemcpyAsync(&tail[1], d_used + npack - 1, sizeof(int), cudaMemcpyDeviceToHost, s));
+            HB_CUDA(cudaMemcpyAsync(&tail[2], d_lslot + npack - 1, sizeof(int), cudaMemcpyDeviceToHost, s));
+            HB_CUDA(cudaMemcpyAsync(&tail[3], d_long + npack - 1, sizeof(int), cudaMemcpyDeviceToHost, s));
             HB_CUDA(cudaStreamSynchronize(s));
             npos2 = tail[0] + tail[1];
+            nposL = tail[2] + tail[3];
+            HB_CUDA(hb::cmalloc(&posL_r, sizeof(int) * std::max(nposL, 1)));
+            HB_CUDA(hb::cmalloc(&posL_c, sizeof(int) * std::max(nposL, 1)));
+            HB_CUDA(hb::cmalloc(&posL_ptr, sizeof(long long) * (nposL + 1)));
+            long long *d_llen = nullptr;
+            HB_CUDA(hb::cmalloc(&d_llen, sizeof(long long) * (nposL + 1)));
+            HB_CUDA(cudaMemsetAsync(d_llen, 0, sizeof(long long) * (nposL + 1), s));
             const int nslice = (npos2 + 31) / 32;
             HB_CUDA(hb::cmalloc(&pos2_r, sizeof(int) * std::max(npos2, 1)));
             HB_CUDA(hb::cmalloc(&pos2_c, sizeof(int) * std::max(npos2, 1)));
@@ -570,7 +628,11 @@ void SdpDevice::upload(int n_, int m_, const HostCoeff &C, const std::vector<Hos
             HB_CUDA(hb::cmalloc(&pos2_ptr, sizeof(long long) * (nslice + 1)));
             long long *d_len = nullptr;
             HB_CUDA(hb::cmalloc(&d_len, sizeof(long long) * (nslice + 1)));
-            r1map_place_kernel<<<hb::counted(pgrid), 256, 0, s>>>(n, d_cnt, d_slot, pos2_r, pos2_c, pos2_cnt);
+            r1map_place_kernel<<<hb::counted(pgrid), 256, 0, s>>>(n, d_cnt, d_slot, pos2_r, pos2_c, pos2_cnt, d_lslot,
+                                                                  posL_r, posL_c, d_llen);
+            exclusive_sum(s, d_llen, posL_ptr, (long long) nposL + 1);
+            long long totalL = 0;
+            HB_CUDA(cudaMemcpyAsync(&totalL, posL_ptr + nposL, sizeof(long long), cudaMemcpyDeviceToHost, s));
             r1map_slice_kernel<<<hb::counted((int) ((32LL * (nslice + 1) + 255) / 256)), 256, 0, s>>>(
                 npos2, nslice, pos2_cnt, d_len);
             exclusive_sum(s, d_len, pos2_ptr, (long long) nslice + 1);
@@ -581,11 +643,14 @@ void SdpDevice::upload(int n_, int m_, const HostCoeff &C, const std::vector<Hos
             HB_CUDA(hb::cmalloc(&ent2_v, sizeof(double) * std::max(total, 1LL)));
             HB_CUDA(cudaMemsetAsync(ent2_j, 0, sizeof(int) * std::max(total, 1LL), s));
             HB_CUDA(cudaMemsetAsync(ent2_v, 0, sizeof(double) * std::max(total, 1LL), s));
+            HB_CUDA(hb::cmalloc(&entL_j, sizeof(int) * std::max(totalL, 1LL)));
+            HB_CUDA(hb::cmalloc(&entL_v, sizeof(double) * std::max(totalL, 1LL)));
             r1map_fill_kernel<<<hb::counted(pgrid), 256, 0, s>>>(n, d_rptr, d_rj, d_ra, d_sgn, d_cnt, d_slot, pos2_ptr,
-                                                                 ent2_j, ent2_v);
+                                                                 ent2_j, ent2_v, d_lslot, posL_ptr, entL_j, entL_v);
             HB_CUDA(cudaGetLastError());
             HB_CUDA(cudaStreamSynchronize(s));
-            for (int *p : {d_rptr, d_rj, d_cnt, d_used, d_slot}) hb::cache_free(p);
+            for (int *p : {d_rptr, d_rj, d_cnt, d_used, d_slot, d_long, d_lslot}) hb::cache_free(p);
+            hb::cache_free(d_llen);
             hb::cache_free(d_ra);
             hb::cache_free(d_sgn);
             hb::cache_free(d_len);
@@ -615,6 +680,11 @@ void SdpDevice::release() {
     f(pos_r); f(pos_c); f(pos_ptr); f(ent_j); f(ent_v);
     f(pos2_r); f(pos2_c); f(pos2_cnt); f(pos2_ptr); f(ent2_j); f(ent2_v);
     pos2_r = pos2_c = pos2_cnt = ent2_j = nullptr;
+    f(posL_r); f(posL_c); f(posL_ptr); f(entL_j); f(entL_v);
+    posL_r = posL_c = entL_j = nullptr;
+    posL_ptr = nullptr;
+    entL_v = nullptr;
+    nposL = 0;
     pos2_ptr = nullptr;
     ent2_v = nullptr;
     npos2 = 0;
@@ -637,8 +707,12 @@ void SdpDevice::assemble(double dC, double dA, const double *d_wvec, double dEye
         if (npos > 0)
             s_gather_kernel<<<hb::counted(grid1(npos)), 256, 0, s>>>(npos, pos_r, pos_c, pos_ptr, ent_j, ent_v, d_wvec, dA, S, ldS);
         if (nr1d > 0 && r1d_gather) {
-            s_gather2_kernel<<<hb::counted(grid1(npos2)), 256, 0, s>>>(npos2, pos2_r, pos2_c, pos2_ptr, pos2_cnt,
-                                                                       ent2_j, ent2_v, d_wvec, dA, S, ldS);
+            if (npos2 > 0)
+                s_gather2_kernel<<<hb::counted(grid1(npos2)), 256, 0, s>>>(npos2, pos2_r, pos2_c, pos2_ptr, pos2_cnt,
+                                                                           ent2_j, ent2_v, d_wvec, dA, S, ldS);
+            if (nposL > 0)
+                s_gather2_long_kernel<<<hb::counted(grid1(32L * nposL)), 256, 0, s>>>(
+                    nposL, posL_r, posL_c, posL_ptr, entL_j, entL_v, d_wvec, dA, S, ldS);
         } else if (nr1d > 0) {
             r1d_weights_kernel<<<hb::counted(grid1(nr1d)), 256, 0, s>>>(nr1d, r1d_id, r1d_sign, d_wvec, dA, d_w);
             scale_columns(s, n, nr1d, A1, ld, d_w, V, ld);

@@ -78,6 +78,15 @@ struct SdpDevice {
     // slice_ptr[slice] + 32 e + l (slices padded to their longest list, pos2_cnt per position)
     int npos2 = 0;
     int *pos2_r = nullptr, *pos2_c = nullptr, *pos2_cnt = nullptr;
+    // positions whose lists are longer than kLongList (the diagonal ones: one entry per
+    // constraint whose support holds the row) are kept out of the slices, whose padding
+    // and slowest lane they would set, in a contiguous layout summed by a warp each:
+    // entries of long position q at posL_ptr[q] .. posL_ptr[q + 1]
+    int nposL = 0;
+    int *posL_r = nullptr, *posL_c = nullptr;
+    long long *posL_ptr = nullptr;
+    int *entL_j = nullptr;
+    double *entL_v = nullptr;
     long long *pos2_ptr = nullptr;
     int *ent2_j = nullptr;
     double *ent2_v = nullptr;

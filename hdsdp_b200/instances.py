@@ -434,6 +434,9 @@ MULTIBLOCK_CASES = {
     "mb5_sparse": dict(dims=[12, 10, 8, 6, 1], m_local=[10, 8, 6, 4, 1], m_couple=3, seed=12),
     "mb2_lp": dict(dims=[30, 25], m_local=[30, 30], m_couple=5, n_lp=12, seed=13),
     "mb4_n500": dict(dims=[200, 150, 100, 50], m_local=[300, 200, 150, 100], m_couple=50, seed=14),
+    # six sparse cones (each holds at most 26 % of the rows) and no dense or LP cone: the
+    # reference takes its sparse Schur complement here (interface/hdsdp_schur.c:181-254)
+    "mb6_sparse": dict(dims=[30, 25, 20, 20, 15, 10], m_local=[40, 35, 30, 30, 25, 20], m_couple=8, seed=15),
 }
 
 

@@ -7,7 +7,8 @@
 the existing fixtures: "north_star" (MaxCut n=8000 and the theta layer n=200,
 primal refinement off; a few minutes), "stock" (the sparse-dual instances on
 the reference build with its own dual-storage rule), "hsd" (instances that end
-in the homogeneous self-dual embedding), "dense" (general dense coefficients).
+in the homogeneous self-dual embedding), "dense" (general dense coefficients),
+"multiblock" (multi-cone cases missing from the fixtures).
 
 Writes tests/golden/golden.json (solver results and probe outputs) and
 tests/golden/golden_arrays.npz (Schur matrices, dual vectors). The inputs are
@@ -121,6 +122,20 @@ def add_groups(groups):
                     key = "%s/psdp%d" % (name, psdp)
                     out["hsd_solves"][key] = _solve_record(inst, r)
                     print("hsd", key, r["iters"], r["status"], r["status_after_check"], r["pobj"], r["dobj"], flush=True)
+        elif g == "multiblock":
+            # multi-cone cases not yet in the fixtures
+            for name in instances.MULTIBLOCK_CASES:
+                if name in out.get("multiblock_solves", {}):
+                    continue
+                prob = instances.multiblock_case(name)
+                r = ref_api.solve_problem(prob)
+                out["multiblock_solves"][name] = {
+                    "m": prob.m, "cones": [[c[0], int(c[1])] for c in prob.cones], "retcode": r["retcode"],
+                    "iters": r["iters"], "status": r["status_after_check"], "pobj": r["pobj"], "dobj": r["dobj"],
+                    "errs": [float(e) for e in r["errs"]],
+                }
+                arrays["y/" + name] = r["y"]
+                print("multiblock", name, r["iters"], r["status_after_check"], r["pobj"], r["dobj"], flush=True)
         elif g == "dense":
             out.setdefault("dense_solves", {})
             for name, make in DENSE.items():
