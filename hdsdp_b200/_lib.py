@@ -20,7 +20,8 @@ EXPORTS = [
     "HUserDataCreate", "HUserDataSetConeData", "HUserDataChooseCone", "HUserDataClear",
     "HUserDataDestroy",
     "HDSDPGetStatus", "HDSDPGetIterCount", "HDSDPSetPrimalRefinement", "HDSDPSetPrecision",
-    "HDSDPSetSparseSlack", "HDSDPGetSparseSlackInfo", "hdsdpb_sparse_analyse",
+    "HDSDPSetSparseSlack", "HDSDPGetSparseSlackInfo", "HDSDPSetSparseSchur", "HDSDPGetSparseSchurInfo",
+    "hdsdpb_sparse_analyse",
     "hdsdpb_sparse_cholesky", "hdsdpb_sparse_congruence",
     "HDSDPGetIterLog", "HDSDPGetTimers", "HDSDPAdjoint",
     "hdsdpb_schur_probe", "hdsdpb_ratio_probe", "hdsdpb_cholesky", "hdsdpb_cholesky_noalloc", "hdsdpb_inverse", "hdsdpb_gemm",
@@ -75,6 +76,8 @@ def load():
         "HDSDPSetPrecision": ([vp, i], None),
         "HDSDPSetSparseSlack": ([vp, i], None),
         "HDSDPGetSparseSlackInfo": ([vp, dp], None),
+        "HDSDPSetSparseSchur": ([vp, i], None),
+        "HDSDPGetSparseSchurInfo": ([vp, dp], None),
         "hdsdpb_sparse_analyse": ([i, i, ip, ip, i, dp, ip], i),
         "hdsdpb_sparse_cholesky": ([i, i, ip, ip, dp, i, i, dp], i),
         "hdsdpb_sparse_congruence": ([i, i, ip, ip, dp, dp, dp, dp, dp], i),

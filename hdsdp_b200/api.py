@@ -137,6 +137,16 @@ class Solver:
                 "eliminated": int(o[4]), "trial_factorisations": int(o[5]), "dense_after_var": int(o[6]),
                 "dense_after_check": int(o[7])}
 
+    def set_sparse_schur(self, mode: int):
+        """Schur complement form when every cone is a sparse SDP cone: -1 automatic, 0 dense,
+        1 block arrow (per-cone local blocks and a coupling block)."""
+        self.L.HDSDPSetSparseSchur(self.h, int(mode))
+
+    def sparse_schur_info(self) -> dict:
+        o = np.zeros(4)
+        self.L.HDSDPGetSparseSchurInfo(self.h, _dp(o))
+        return {"arrow": bool(o[0]), "coupling": int(o[1]), "cones": int(o[2]), "max_local": int(o[3])}
+
     def optimize(self, d_only: int = 0) -> int:
         return self.L.HDSDPOptimize(self.h, int(d_only))
 
@@ -257,7 +267,7 @@ def solve(inst, want_x: bool = True, primal_refinement: bool = True, precision: 
 
 
 def solve_problem(prob, primal_refinement: bool = True, precision: int = 0, params: dict | None = None,
-                  sparse_slack: int = -1) -> dict:
+                  sparse_slack: int = -1, sparse_schur: int = -1) -> dict:
     """Solve a multi-cone problem (instances.ConicProblem: SDP blocks and LP cones over one
     set of constraints) on the GPU; returns y, objectives, status, iterations, the iteration
     log, DIMACS errors and per cone (X, S) or (x, s)."""
@@ -271,6 +281,7 @@ def solve_problem(prob, primal_refinement: bool = True, precision: int = 0, para
         s.set_primal_refinement(primal_refinement)
         s.set_precision(precision)
         s.set_sparse_slack(sparse_slack)
+        s.set_sparse_schur(sparse_schur)
         for k, v in (params or {}).items():
             if isinstance(v, int):
                 s.set_int_param(k, v)
@@ -282,7 +293,7 @@ def solve_problem(prob, primal_refinement: bool = True, precision: int = 0, para
         po, do, y = s.get_row_dual()
         out = {"retcode": int(ret), "time": t1 - t0, "y": y, "pobj": po, "dobj": do,
                "status": s.status(), "iters": s.iters(), "log": s.iter_log(), "timers": s.timers(),
-               "sparse_slack": s.sparse_slack_info()}
+               "sparse_slack": s.sparse_slack_info(), "sparse_schur": s.sparse_schur_info()}
         out["values"] = [s.get_cone_values_at(k) for k in range(len(prob.cones))]
         out["errs"] = s.check_solution()
         out["status_after_check"] = s.status()

@@ -13,7 +13,6 @@ namespace hb {
 // Schur systems of at least this order are solved by triangular solves with L rather
 // than through K = L^-1: forming K costs as much as the factorisation, while a solve
 // with L reads L once.
-constexpr int kTriSolveMinM = 6000;
 
 // Hybrid sparse factorisation of S: automatic from this order on, minimum-degree rounds
 // up to this degree, and used only when the dense front is at most this fraction of n
@@ -780,17 +779,17 @@ void BoundCone::get_primal(double mu, const double *y, const double *dy, double 
 // ======================================================================================
 // Schur complement system
 // ======================================================================================
-void KKT::init(int m_, cudaStream_t stream, Timers *t) {
+void KKT::init(int m_, cudaStream_t stream, Timers *t, bool denseM) {
     m = m_;
     s = stream;
     tm = t;
     ldm = pad_ld(m);
-    HB_CUDA(hb::cmalloc(&M, sizeof(double) * ldm * m));
-    HB_CUDA(cudaMemsetAsync(M, 0, sizeof(double) * ldm * m, s));
-    // Up to kTriSolveMinM the Schur solves use K = L^-1 (formed inside the factorisation);
-    // above it they are triangular solves with L, which read L once instead of forming K.
-    F.alloc(m, m < kTriSolveMinM ? 1 : 0);
-    F.kfamily = KF_POTRF_SCHUR;
+    if (denseM) {
+        HB_CUDA(hb::cmalloc(&M, sizeof(double) * ldm * m));
+        HB_CUDA(cudaMemsetAsync(M, 0, sizeof(double) * ldm * m, s));
+        F.alloc(m, m < kTriSolveMinM ? 1 : 0);
+        F.kfamily = KF_POTRF_SCHUR;
+    }
     asinv.assign(m, 0.0);
     asinvrd.assign(m, 0.0);
     asinvcs.assign(m, 0.0);
@@ -800,6 +799,7 @@ void KKT::init(int m_, cudaStream_t stream, Timers *t) {
 }
 
 void KKT::release() {
+    release_arrow();
     if (M) hb::cache_free(M);
     M = nullptr;
     if (Msub) hb::cache_free(Msub);
@@ -827,6 +827,7 @@ void KKT::clean(int type) {
 }
 
 void KKT::open_m() {
+    if (arrow) return arrow_open();
     if (mOpen) return;
     HB_CUDA(cudaMemsetAsync(M, 0, sizeof(double) * ldm * m, s));
     mOpen = true;
@@ -922,9 +923,13 @@ hdsdp_retcode KKT::add_sdp(SdpCone &cone, int type) {
             HB_CUDA(hb::cmalloc(&Msub, sizeof(double) * msubCap));
         }
         dev.schur_matrix(Wp, ld, Msub, ldk, (type == KKT_TYPE_PRIMAL) ? nullptr : cone.Fvar.K);
-        dim3 blk(32, 8), grd((mk + 31) / 32, std::min((mk + 7) / 8, 4096));
-        scatter_lower_kernel<<<hb::counted(grd), blk, 0, s>>>(mk, Msub, ldk, cone.d_rows, M, ldm);
-        HB_CUDA(cudaGetLastError());
+        if (arrow) {
+            arrow_add(cone, Msub, ldk);
+        } else {
+            dim3 blk(32, 8), grd((mk + 31) / 32, std::min((mk + 7) / 8, 4096));
+            scatter_lower_kernel<<<hb::counted(grd), blk, 0, s>>>(mk, Msub, ldk, cone.d_rows, M, ldm);
+            HB_CUDA(cudaGetLastError());
+        }
     }
     if (tm) {
         HB_CUDA(cudaStreamSynchronize(s));
@@ -978,10 +983,14 @@ void KKT::add_bound(BoundCone &b, int type) {
     }
     if (type == KKT_TYPE_CORRECTOR) return;
     for (int i = 0; i < b.m; ++i) h_buf[i] = b.dlInv[i] * b.dlInv[i] + b.duInv[i] * b.duInv[i];
-    open_m();
-    HB_CUDA(cudaMemcpyAsync(d_diag, h_buf, sizeof(double) * m, cudaMemcpyHostToDevice, s));
-    add_diag_vec(s, m, M, ldm, d_diag);
-    HB_CUDA(cudaStreamSynchronize(s));
+    if (arrow) {
+        arrow_add_diag(h_buf);
+    } else {
+        open_m();
+        HB_CUDA(cudaMemcpyAsync(d_diag, h_buf, sizeof(double) * m, cudaMemcpyHostToDevice, s));
+        add_diag_vec(s, m, M, ldm, d_diag);
+        HB_CUDA(cudaStreamSynchronize(s));
+    }
     if (type == KKT_TYPE_HOMOGENEOUS) {
         for (int i = 0; i < b.m; ++i) {
             dCSinv += b.up * b.duInv[i];
@@ -998,6 +1007,7 @@ void KKT::add_bound(BoundCone &b, int type) {
 
 // HKKTRegularize (interface/hdsdp_schur.c:348-373)
 void KKT::regularize(double reg) {
+    if (arrow) return arrow_regularize(reg);
     copy_matrix(s, 1, m, M, ldm + 1, d_t, 1);
     HB_CUDA(cudaMemcpyAsync(h_buf, d_t, sizeof(double) * m, cudaMemcpyDeviceToHost, s));
     HB_CUDA(cudaStreamSynchronize(s));
@@ -1011,6 +1021,11 @@ void KKT::regularize(double reg) {
 
 hdsdp_retcode KKT::factorize() {
     double t0 = wall();
+    if (arrow) {
+        const bool ok = arrow_factorize();
+        if (tm) tm->schur_factor += wall() - t0;
+        return ok && !device_error_flag() ? HDSDP_RETCODE_OK : HDSDP_RETCODE_FAILED;
+    }
     symmetrize_lower(s, m, M, ldm);
     shift = 0.0;
     bool ok = hb::factorize(s, F, M, ldm);
@@ -1038,6 +1053,14 @@ hdsdp_retcode KKT::factorize() {
 // x = M^-1 b with one step of iterative refinement on the FP64 residual.
 hdsdp_retcode KKT::solve(const double *rhs, double *lhs) {
     double t0 = wall();
+    if (arrow) {
+        if (!arrow_solve(rhs, lhs)) device_error_flag() = 1;
+        if (tm) {
+            tm->schur_solve += wall() - t0;
+            tm->n_schur_solve += 1;
+        }
+        return device_error_flag() ? HDSDP_RETCODE_FAILED : HDSDP_RETCODE_OK;
+    }
     std::memcpy(h_buf, rhs, sizeof(double) * m);
     HB_CUDA(cudaMemcpyAsync(d_rhs, h_buf, sizeof(double) * m, cudaMemcpyHostToDevice, s));
     bool ok = true;

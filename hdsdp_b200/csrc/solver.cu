@@ -1670,7 +1670,28 @@ hdsdp_retcode HDSDPOptimize(hdsdp *h, int dOptOnly) {
                "of which gather map %.3f s)\n",
                tp1 - tp0, tp2, wall() - tp1, up, upMap);
     }
-    h->kkt.init(h->nRows, h->stream, &h->timers);
+    {
+        // the block-arrow Schur complement when every cone is a sparse SDP cone (the
+        // reference's sparse KKT, interface/hdsdp_schur.c:224-246)
+        std::vector<SdpCone *> sp;
+        bool allSparse = true;
+        for (ConeSlot &k : h->cones) {
+            if (k.sdp && k.sdp->sparse) sp.push_back(k.sdp);
+            else allSparse = false;
+        }
+        const bool useArrow = allSparse && arrow_chosen(h->sparseSchur, h->nRows, sp);
+        h->kkt.init(h->nRows, h->stream, &h->timers, !useArrow);
+        if (useArrow && !h->kkt.setup_arrow(sp)) {
+            retcode = HDSDP_RETCODE_MEMORY;
+            goto exit_cleanup;
+        }
+        if (h->verbose && useArrow) {
+            double info[4];
+            h->kkt.arrow_info(info);
+            printf("  Schur complement: block arrow, %d cones (largest local block %d), %d coupling rows\n",
+                   (int) info[2], (int) info[3], (int) info[1]);
+        }
+    }
     if (device_error_flag()) {
         retcode = HDSDP_RETCODE_MEMORY;
         goto exit_cleanup;

@@ -219,6 +219,15 @@ struct LpCone {
     double trace_cx(const double *x) const;
 };
 
+// Up to this order the Schur solves use K = L^-1 (formed inside the factorisation); above
+// it they are triangular solves with L, which read L once instead of forming K.
+constexpr int kTriSolveMinM = 6000;
+
+struct ArrowSchur;
+// Whether the block-arrow Schur complement is used for these sparse SDP cones (the whole
+// problem; mode -1 automatic, 0 never, 1 always).
+bool arrow_chosen(int mode, int m, const std::vector<SdpCone *> &cones);
+
 // Schur complement system (interface/hdsdp_schur.c).
 struct KKT {
     int m = 0;
@@ -239,8 +248,23 @@ struct KKT {
     bool mOpen = false;
     double *Msub = nullptr;           // Schur block of a cone added into M (sparse or not first)
     size_t msubCap = 0;
-    void init(int m_, cudaStream_t stream, Timers *t);
+    // dense M and F are allocated unless denseM is false (the block-arrow form is used)
+    void init(int m_, cudaStream_t stream, Timers *t, bool denseM = true);
     void release();
+    // Block-arrow sparse Schur complement (arrow.cu) for problems whose cones are all sparse
+    // SDP cones: M kept as per-cone local blocks, their coupling rows and a coupling block.
+    // Engaged by setup_arrow after init(..., false); the methods below then route to it.
+    ArrowSchur *arrow = nullptr;
+    bool setup_arrow(const std::vector<SdpCone *> &cones);
+    void release_arrow();
+    void arrow_open();
+    void arrow_add(const SdpCone &cone, const double *Msub, long ldsub);
+    void arrow_add_diag(const double *h_diag);
+    void arrow_regularize(double reg);
+    bool arrow_factorize();
+    bool arrow_solve(const double *rhs, double *lhs);
+    // {engaged, coupling rows, cones, largest local block}
+    void arrow_info(double out[4]) const;
     void clean(int type);
     void open_m();
     hdsdp_retcode add_sdp(SdpCone &cone, int type);
@@ -310,6 +334,7 @@ struct hdsdp_solver_internal {
     bool optimized = false;
     int precision = 0;
     int sparseSlack = -1;          // factorisation of S in PSD checks: -1 trial points sparse (automatic), 0 dense, 1 sparse
+    int sparseSchur = -1;          // Schur complement form: -1 automatic, 0 dense, 1 block arrow when every cone is a sparse SDP cone
     int verbose = 0;
     std::vector<hb::IterRecord> log;
     std::string modelFeatures;

@@ -437,6 +437,9 @@ MULTIBLOCK_CASES = {
     # six sparse cones (each holds at most 26 % of the rows) and no dense or LP cone: the
     # reference takes its sparse Schur complement here (interface/hdsdp_schur.c:181-254)
     "mb6_sparse": dict(dims=[30, 25, 20, 20, 15, 10], m_local=[40, 35, 30, 30, 25, 20], m_couple=8, seed=15),
+    # 40 sparse cones of order 60 with 120 constraints each and 40 shared ones (m = 4,840):
+    # the Schur complement is a block arrow with 40 blocks of 120 rows and 40 coupling rows
+    "mb40_arrow": dict(dims=[60] * 40, m_local=[120] * 40, m_couple=40, seed=16),
 }
 
 

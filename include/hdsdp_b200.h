@@ -48,6 +48,20 @@ extern void HDSDPSetSparseSlack( hdsdp *HSolver, int mode );
    followed a sparse one because a consumer needed L (accepted point / trial point). */
 extern void HDSDPGetSparseSlackInfo( hdsdp *HSolver, double out[8] );
 
+/* Form of the Schur complement M when every cone of the problem is a sparse SDP cone (no
+   dense SDP cone, no LP cone; where the reference takes its sparse KKT,
+   interface/hdsdp_schur.c:224-246, factored through Pardiso): a block arrow. Rows held by
+   one cone only form that cone's diagonal block; rows held by several cones (or by none)
+   form the coupling block, factored after the Schur complement of the cones' blocks.
+   -1 = automatic (default): the block arrow for m >= 4096 when it needs at most a quarter
+   of the dense factorisation's flops; 0 = always the dense M; 1 = the block arrow whenever
+   the cones allow it. Takes effect at the next HDSDPOptimize. */
+extern void HDSDPSetSparseSchur( hdsdp *HSolver, int mode );
+
+/* out[0] = 1 if the last solve used the block arrow, out[1] = coupling rows, out[2] =
+   cones, out[3] = the largest cone's local rows. */
+extern void HDSDPGetSparseSchurInfo( hdsdp *HSolver, double out[4] );
+
 /* Per-iteration record of the last solve: elapsed seconds, primal and dual
    objective, barrier parameter, relative gap (p - d) / (1 + |p| + |d|) and
    phase (0 infeasible, 1 embedding, 2 potential reduction, 3 refinement),

@@ -125,7 +125,19 @@ def add_groups(groups):
         elif g == "multiblock":
             # multi-cone cases not yet in the fixtures
             for name in instances.MULTIBLOCK_CASES:
-                if name in out.get("multiblock_solves", {}):
+                rec = out.get("multiblock_solves", {}).get(name)
+                if rec is not None:
+                    if instances.multiblock_case(name).m >= 4096 and "iters_range" not in rec:
+                        # long runs: the reference's own iteration count depends on its BLAS
+                        # thread count (fixed when OpenBLAS loads); record the count of a
+                        # one-thread run in a child process beside the default
+                        import subprocess
+                        env = dict(os.environ, OPENBLAS_NUM_THREADS="1", OMP_NUM_THREADS="1")
+                        it1 = int(subprocess.run([sys.executable, os.path.abspath(__file__), "--iters", name],
+                                                 env=env, check=True, capture_output=True,
+                                                 text=True).stdout.strip().splitlines()[-1])
+                        rec["iters_range"] = [min(rec["iters"], it1), max(rec["iters"], it1)]
+                        print("multiblock", name, "one thread:", it1, flush=True)
                     continue
                 prob = instances.multiblock_case(name)
                 r = ref_api.solve_problem(prob)
@@ -246,7 +258,11 @@ def main(full: bool):
 
 
 if __name__ == "__main__":
-    if "--add" in sys.argv:
+    if "--iters" in sys.argv:
+        # iteration count of the reference's solve of one multi-block case (last line)
+        r = ref_api.solve_problem(instances.multiblock_case(sys.argv[sys.argv.index("--iters") + 1]))
+        print(r["iters"])
+    elif "--add" in sys.argv:
         add_groups(sys.argv[sys.argv.index("--add") + 1:])
     else:
         main("--full" in sys.argv)

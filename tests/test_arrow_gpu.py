@@ -1,0 +1,66 @@
+"""The block-arrow Schur complement (HDSDPSetSparseSchur) on problems whose cones are all
+sparse SDP cones, where the reference takes its sparse KKT (interface/hdsdp_schur.c:224-246,
+factored through Pardiso): against the compiled reference's solves of the same data and
+against this library's dense Schur complement."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from hdsdp_b200 import api, instances
+from test_solve_gpu import check_parity
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("mode", [1, 0, -1])
+def test_mb6_sparse_schur_modes(gpu_lib, mode, golden, golden_arrays):
+    """Six sparse cones (m = 188): the block arrow forced on (mode 1), off (0), and left to
+    the automatic rule (-1), which keeps the dense M below m = 4096."""
+    prob = instances.multiblock_case("mb6_sparse")
+    r = api.solve_problem(prob, sparse_schur=mode)
+    info = r["sparse_schur"]
+    if mode == 1:
+        assert info == {"arrow": True, "coupling": 8, "cones": 6, "max_local": 40}
+    else:
+        assert not info["arrow"]
+    check_parity(r, golden["multiblock_solves"]["mb6_sparse"])
+    np.testing.assert_allclose(r["y"], golden_arrays["y/mb6_sparse"], rtol=1e-4, atol=1e-5)
+
+
+def test_arrow_refused_with_a_dense_cone(gpu_lib, golden):
+    """A problem with a dense SDP cone or an LP cone keeps the dense M even when the block
+    arrow is asked for."""
+    for name in ("mb5_sparse", "mb2_lp"):
+        prob = instances.multiblock_case(name)
+        r = api.solve_problem(prob, sparse_schur=1)
+        assert not r["sparse_schur"]["arrow"]
+        check_parity(r, golden["multiblock_solves"][name])
+
+
+@pytest.mark.slow
+def test_mb40_arrow_against_dense(gpu_lib, golden, golden_arrays):
+    """40 sparse cones, m = 4,840: the automatic rule takes the block arrow (40 blocks of
+    120 rows, 40 coupling rows); the solve meets the reference's, and the dense Schur
+    complement on the same data ends at the same point."""
+    prob = instances.multiblock_case("mb40_arrow")
+    a = api.solve_problem(prob)
+    assert a["sparse_schur"] == {"arrow": True, "coupling": 40, "cones": 40, "max_local": 120}
+    ref = golden["multiblock_solves"]["mb40_arrow"]
+    check_parity(a, ref)
+    np.testing.assert_allclose(a["y"], golden_arrays["y/mb40_arrow"], rtol=1e-4, atol=1e-5)
+    d = api.solve_problem(prob, sparse_schur=0)
+    assert not d["sparse_schur"]["arrow"]
+    # the dense run ends at the same point; its iteration count (109 on a B200) sits just
+    # outside the reference's own range over BLAS thread counts (103 to 106), which the
+    # arrow run meets, so only the objectives and the status are compared
+    assert d["status_after_check"] == ref["status"]
+    assert d["dobj"] == pytest.approx(ref["dobj"], rel=1e-6)
+    assert d["pobj"] == pytest.approx(ref["pobj"], rel=1e-6)
+    assert a["dobj"] == pytest.approx(d["dobj"], rel=1e-8)
+    # the arrow factorises 40 blocks of order 120 and one of order 40 instead of m = 4,840
+    print("mb40_arrow: arrow %d iterations %.3f s (Schur factor %.3f s, solve %.3f s), dense %d iterations %.3f s "
+          "(Schur factor %.3f s, solve %.3f s)"
+          % (a["iters"], a["time"], a["timers"]["schur_factor"], a["timers"]["schur_solve"], d["iters"], d["time"],
+             d["timers"]["schur_factor"], d["timers"]["schur_solve"]))
+    assert a["timers"]["schur_factor"] < d["timers"]["schur_factor"]

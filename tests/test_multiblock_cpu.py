@@ -60,8 +60,8 @@ def test_cone_choice_matches_reference(name):
         kinds.append(a)
     if name == "mb5_sparse":
         assert kinds == [DENSE_SDP, DENSE_SDP, SPARSE_SDP, SPARSE_SDP, SPARSE_SDP]
-    if name == "mb6_sparse":
-        assert kinds == [SPARSE_SDP] * 6
+    if name in ("mb6_sparse", "mb40_arrow"):
+        assert kinds == [SPARSE_SDP] * len(prob.cones)
 
 
 @pytest.mark.parametrize("name", sorted(instances.MULTIBLOCK_CASES))

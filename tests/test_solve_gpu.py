@@ -20,7 +20,10 @@ OPTIMAL = 3
 
 def check_parity(r, ref, psdp=False):
     assert r["status_after_check"] == ref["status"]
-    assert abs(r["iters"] - ref["iters"]) <= 2, (r["iters"], ref["iters"])
+    # iterations within 2 of the reference's; for long runs, of the range the reference
+    # itself spans over BLAS thread counts (1 and 8 threads)
+    lo, hi = ref.get("iters_range", (ref["iters"], ref["iters"]))
+    assert lo - 2 <= r["iters"] <= hi + 2, (r["iters"], ref["iters"], lo, hi)
     # With primal refinement on, the dual phase stops at a 10% gap and five fixed
     # refinement steps follow. Where the reference then reaches PRIMAL_DUAL_OPTIMAL the
     # objectives meet the 1e-6 bar. Where its DIMACS check ends the run as NUMERICAL
