@@ -614,6 +614,64 @@ __global__ void __launch_bounds__(COOP_THREADS, 1) potrf_coop_kernel(double *L, 
     for (int c = blockIdx.x; c <= bj; c += gridDim.x) k_final_tile(Dinv, ldd, K, KT, ld, n, bj, c, sm);
 }
 
+// Several factorisations of order <= 64 in one launch, one CTA each: the copy of the lower
+// triangle, the diagonal-block factorisation and inverse (potf2_dev), K = L^-1 and K^T from
+// the inverse block, and sum log L_ii next to the info word, each as the cooperative
+// kernel and the log-diagonal kernel do them for a single 64-column panel.
+struct SmallFactorJob {
+    const double *S;
+    double *L, *Dinv, *K, *KT;
+    long lds, ld;
+    int *info;
+    int n, logdet;
+};
+constexpr int kSmallBatch = 40;
+struct SmallFactorBatch {
+    SmallFactorJob job[kSmallBatch];
+};
+
+__device__ double small_block_sum(double v) {
+    __shared__ double red[32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) red[w] = v;
+    __syncthreads();
+    const int nw = (blockDim.x + 31) >> 5;
+    v = (threadIdx.x < nw) ? red[threadIdx.x] : 0.0;
+    if (w == 0) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    }
+    __syncthreads();
+    return v;
+}
+
+__global__ void __launch_bounds__(COOP_THREADS, 1) potrf_small_batch_kernel(const SmallFactorBatch B) {
+    extern __shared__ double sm[];
+    const SmallFactorJob &J = B.job[blockIdx.x];
+    const int n = J.n;
+    for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
+        const int r = idx % n, c = idx / n;
+        J.L[(size_t) r + (size_t) c * J.ld] = (r >= c) ? J.S[(size_t) r + (size_t) c * J.lds] : 0.0;
+    }
+    if (threadIdx.x == 0) *J.info = 0;
+    __threadfence_block();
+    __syncthreads();
+    potf2_dev(J.L, J.ld, 0, n, J.Dinv, J.ld, J.info, sm);
+    __syncthreads();
+    const bool ok = (*(volatile int *) J.info == 0);
+    if (ok && J.K) k_final_tile(J.Dinv, J.ld, J.K, J.KT, J.ld, n, 0, 0, sm);
+    if (J.logdet) {
+        __threadfence_block();
+        __syncthreads();
+        double acc = 0.0;
+        for (int i = threadIdx.x; i < n; i += blockDim.x) acc += log(J.L[(size_t) i + (size_t) i * J.ld]);
+        acc = small_block_sum(acc);
+        if (threadIdx.x == 0) reinterpret_cast<double *>(J.info)[1] = acc;
+    }
+}
+
 __global__ void __launch_bounds__(COOP_THREADS, 1) trtri_coop_kernel(const double *L, double *K, long ld, int n,
                                                                   const double *Dinv, long ldd) {
     cg::grid_group grid = cg::this_grid();
@@ -933,6 +991,29 @@ bool coop_factorize_enqueue(cudaStream_t s, DenseFactor &F, const double *S, lon
     if (e != cudaSuccess) {
         cudaGetLastError();
         return false;
+    }
+    return true;
+}
+
+// The factorisations of F[0..count) (each n <= 64) of S[i] (ldS[i]) in launches of up to
+// kSmallBatch CTAs; returns false if a launch failed.
+bool small_factor_batch_enqueue(cudaStream_t s, DenseFactor *const *F, const double *const *S, const long *ldS,
+                                int count) {
+    static std::atomic<unsigned long long> attr{0};
+    once_per_device(attr, [] {
+        HB_CUDA(cudaFuncSetAttribute((const void *) potrf_small_batch_kernel,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, SM_DOUBLES * (int) sizeof(double)));
+    });
+    for (int b0 = 0; b0 < count; b0 += kSmallBatch) {
+        SmallFactorBatch B;
+        const int nb = std::min(kSmallBatch, count - b0);
+        for (int q = 0; q < nb; ++q) {
+            DenseFactor &G = *F[b0 + q];
+            B.job[q] = SmallFactorJob{S[b0 + q], G.L, G.Dinv, G.fuse_k ? G.K : nullptr, G.fuse_k ? G.KT : nullptr,
+                                      ldS[b0 + q], G.ld, G.d_info, G.n, G.stat_logdet ? 1 : 0};
+        }
+        potrf_small_batch_kernel<<<hb::counted(nb), COOP_THREADS, SM_DOUBLES * sizeof(double), s>>>(B);
+        if (cudaGetLastError() != cudaSuccess) return false;
     }
     return true;
 }

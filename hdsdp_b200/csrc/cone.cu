@@ -402,6 +402,8 @@ hdsdp_retcode SdpCone::setup_device(cudaStream_t stream, Timers *t) {
     }
     HB_CUDA(hb::cmalloc(&d_y, sizeof(double) * std::max(m, 1)));
     HB_CUDA(hb::cmalloc(&d_vec, sizeof(double) * std::max(m, 1)));
+    HB_CUDA(hb::cmalloc(&d_vec2, sizeof(double) * std::max(m, 1)));
+    HB_CUDA(hb::cmalloc_host(&h_vec2, sizeof(double) * std::max(m, 1)));
     if (sparse && m > 0) {
         HB_CUDA(hb::cmalloc(&d_rows, sizeof(int) * m));
         HB_CUDA(cudaMemcpyAsync(d_rows, rows.data(), sizeof(int) * m, cudaMemcpyHostToDevice, s));
@@ -416,8 +418,10 @@ hdsdp_retcode SdpCone::setup_device(cudaStream_t stream, Timers *t) {
 void SdpCone::release() {
     dev.release();
     auto f = [](void *p) { if (p) hb::cache_free(p); };
-    f(Svar); f(Scheck); f(dS); f(W); f(d_y); f(d_vec); f(d_scal); f(d_rows);
+    f(Svar); f(Scheck); f(dS); f(W); f(d_y); f(d_vec); f(d_vec2); f(d_scal); f(d_rows);
     if (h_vec) hb::cache_free_host(h_vec);
+    if (h_vec2) hb::cache_free_host(h_vec2);
+    d_vec2 = h_vec2 = nullptr;
     if (h_scal) hb::cache_free_host(h_scal);
     Svar = Scheck = dS = W = d_y = d_vec = d_scal = h_vec = h_scal = nullptr;
     d_rows = nullptr;
@@ -527,6 +531,66 @@ bool SdpCone::factor_buffer(int which) {
     return ok;
 }
 
+// factor_buffer in two phases, for several cones at once: factor_plan() settles what
+// factor_buffer would do without waiting for the device. FP_DONE: the result is known
+// (*ok); FP_SMALL: a dense factorisation of order <= kSmallFactorMaxN, to be enqueued by
+// the caller with the other cones' (factorize_small_batch); FP_ASYNC: enqueued here.
+// factor_finish() then reads the status of an FP_SMALL or FP_ASYNC factorisation.
+int SdpCone::factor_plan(int which, bool *ok) {
+    const bool var = (which == BUFFER_DUALVAR);
+    const SlackSig &sig = var ? sigVar : sigCheck;
+    const SlackSig &fsig = var ? facVar : facCheck;
+    const SlackSig &osig = var ? facCheck : facVar;
+    const bool ook = var ? facCheckOk : facVarOk;
+    if (sig.same(fsig) || (sig.same(osig) && ook) || use_hybrid(which)) {
+        *ok = factor_buffer(which);   // reuse, copy or the hybrid factorisation
+        return FP_DONE;
+    }
+    if (n <= kSmallFactorMaxN) return FP_SMALL;
+    factorize_async(s, var ? Fvar : Fcheck, var ? Svar : Scheck, ld);
+    return FP_ASYNC;
+}
+
+bool SdpCone::factor_finish(int which) {
+    const bool var = (which == BUFFER_DUALVAR);
+    DenseFactor &F = var ? Fvar : Fcheck;
+    const bool ok = factor_status(s, F);
+    (var ? hyVar : hyCheck) = false;
+    (var ? facVar : facCheck) = var ? sigVar : sigCheck;
+    (var ? facVarOk : facCheckOk) = ok;
+    if (tm) tm->n_sfactor += 1;
+    return ok;
+}
+
+// The buffer `which` of every cone of `cones` factored as factor_buffer does, with the
+// dense factorisations of small blocks in one batched launch and one wait for all.
+void factor_buffers(const std::vector<SdpCone *> &cones, int which, std::vector<char> &ok) {
+    const double t0 = wall();
+    ok.assign(cones.size(), 0);
+    std::vector<int> plan(cones.size(), 0);
+    std::vector<DenseFactor *> F;
+    std::vector<const double *> S;
+    std::vector<long> ldS;
+    const bool var = (which == BUFFER_DUALVAR);
+    Timers *tm = nullptr;
+    for (size_t q = 0; q < cones.size(); ++q) {
+        SdpCone &c = *cones[q];
+        bool r = false;
+        plan[q] = c.factor_plan(which, &r);
+        ok[q] = r ? 1 : 0;
+        if (plan[q] == SdpCone::FP_SMALL) {
+            F.push_back(var ? &c.Fvar : &c.Fcheck);
+            S.push_back(var ? c.Svar : c.Scheck);
+            ldS.push_back(c.ld);
+        }
+        if (c.tm) tm = c.tm;
+    }
+    if (!F.empty()) factorize_small_batch(cones[0]->s, F.data(), S.data(), ldS.data(), (int) F.size());
+    for (size_t q = 0; q < cones.size(); ++q)
+        if (plan[q] != SdpCone::FP_DONE) ok[q] = cones[q]->factor_finish(which) ? 1 : 0;
+    if (tm) tm->s_factor += wall() - t0;
+}
+
 // Positive-definiteness and log det of the buffer `which` through the hybrid factor.
 bool SdpCone::hybrid_factor(int which) {
     const bool var = (which == BUFFER_DUALVAR);
@@ -619,6 +683,19 @@ hdsdp_retcode SdpCone::get_barrier(double tau, const double *y, int which, doubl
     HB_CUDA(cudaStreamSynchronize(s));
     *logdet = 2.0 * h_scal[0];
     return HDSDP_RETCODE_OK;
+}
+
+void SdpCone::add_step(double step, int which) {
+    if (which == BUFFER_DUALVAR) {
+        axpy(s, (int) (ld * n), step, dS, Svar);
+        sigVar.valid = false;
+        facVar.valid = false;
+    } else {
+        HB_CUDA(cudaMemcpyAsync(Scheck, Svar, sizeof(double) * ld * n, cudaMemcpyDeviceToDevice, s));
+        axpy(s, (int) (ld * n), step, dS, Scheck);
+        sigCheck.valid = false;
+        facCheck.valid = false;
+    }
 }
 
 hdsdp_retcode SdpCone::add_step_and_check(double step, int which, int *interior) {
@@ -967,6 +1044,94 @@ hdsdp_retcode KKT::add_sdp(SdpCone &cone, int type) {
     if (tm) {
         tm->schur += wall() - t0;
         tm->n_schur += 1;
+    }
+    return device_error_flag() ? HDSDP_RETCODE_FAILED : HDSDP_RETCODE_OK;
+}
+
+// add_sdp for every cone of `cones` (a build of type KKT_TYPE_INFEASIBLE or
+// KKT_TYPE_CORRECTOR, the cones in the user's order): all device work is enqueued first,
+// each cone's vectors and trace come back into its own pinned buffers, and after one wait
+// the host sums are formed in the cones' order, with the operations add_sdp uses, so the
+// result is the same to the bit.
+hdsdp_retcode KKT::add_sdp_batch(const std::vector<SdpCone *> &cones, int type) {
+    const double t0 = wall();
+    for (SdpCone *cp : cones) {
+        SdpCone &cone = *cp;
+        const int n = cone.n;
+        const long ld = cone.ld;
+        const double r = cone.dualResidual;
+        if (cone.hy && !cone.ensure_dense(BUFFER_DUALVAR)) return HDSDP_RETCODE_FAILED;
+        bool done = false;
+        if (cone.dev.precision == 1 && n >= kSplitInverseMinN) {
+            compute_inverse_factor(s, cone.Fvar);
+            done = cone.dev.split_inverse(cone.Fvar.K, cone.W, ld);
+        }
+        if (!done) compute_inverse(s, cone.Fvar, cone.W, ld);
+        const double *Wp = cone.W;
+        SdpDevice &dev = cone.dev;
+        const int mk = cone.m;
+        if (type == KKT_TYPE_CORRECTOR) {
+            dev.inner_all(Wp, ld, cone.d_vec);
+            if (mk > 0) HB_CUDA(cudaMemcpyAsync(cone.h_vec, cone.d_vec, sizeof(double) * mk, cudaMemcpyDeviceToHost, s));
+            if (r != 0.0) {
+                dev.inner_all_sq(Wp, ld, cone.d_vec2, false, true);
+                if (mk > 0)
+                    HB_CUDA(cudaMemcpyAsync(cone.h_vec2, cone.d_vec2, sizeof(double) * mk, cudaMemcpyDeviceToHost, s));
+            }
+            continue;
+        }
+        if (r != 0.0) {
+            trace(s, n, Wp, ld, cone.d_scal);
+            HB_CUDA(cudaMemcpyAsync(cone.h_scal, cone.d_scal, sizeof(double), cudaMemcpyDeviceToHost, s));
+        }
+        if (!cone.sparse && !mOpen) {
+            dev.schur_matrix(Wp, ld, M, ldm, cone.Fvar.K);
+            mOpen = true;
+        } else if (mk > 0) {
+            open_m();
+            const long ldk = pad_ld(mk);
+            if (msubCap < (size_t) ldk * mk) {
+                // the scratch grows: the blocks enqueued so far must have read the old one
+                HB_CUDA(cudaStreamSynchronize(s));
+                if (Msub) hb::cache_free(Msub);
+                msubCap = (size_t) ldk * mk;
+                HB_CUDA(hb::cmalloc(&Msub, sizeof(double) * msubCap));
+            }
+            dev.schur_matrix(Wp, ld, Msub, ldk, cone.Fvar.K);
+            if (arrow) {
+                arrow_add(cone, Msub, ldk);
+            } else {
+                dim3 blk(32, 8), grd((mk + 31) / 32, std::min((mk + 7) / 8, 4096));
+                scatter_lower_kernel<<<hb::counted(grd), blk, 0, s>>>(mk, Msub, ldk, cone.d_rows, M, ldm);
+                HB_CUDA(cudaGetLastError());
+            }
+        }
+        dev.inner_all(Wp, ld, cone.d_vec, true);
+        if (mk > 0) HB_CUDA(cudaMemcpyAsync(cone.h_vec, cone.d_vec, sizeof(double) * mk, cudaMemcpyDeviceToHost, s));
+        if (r != 0.0) {
+            dev.inner_all_sq(Wp, ld, cone.d_vec2, true);
+            if (mk > 0)
+                HB_CUDA(cudaMemcpyAsync(cone.h_vec2, cone.d_vec2, sizeof(double) * mk, cudaMemcpyDeviceToHost, s));
+        }
+    }
+    HB_CUDA(cudaStreamSynchronize(s));
+    for (SdpCone *cp : cones) {
+        SdpCone &cone = *cp;
+        const double r = cone.dualResidual;
+        const std::vector<int> *rows = cone.sparse ? &cone.rows : nullptr;
+        auto acc = [&](std::vector<double> &dst, const double *h, double scale) {
+            if (rows)
+                for (int i = 0; i < cone.m; ++i) dst[(*rows)[i]] += scale * h[i];
+            else
+                for (int i = 0; i < cone.m; ++i) dst[i] += scale * h[i];
+        };
+        if (type != KKT_TYPE_CORRECTOR && r != 0.0) dTraceSinv += cone.h_scal[0];
+        acc(asinv, cone.h_vec, 1.0);
+        if (r != 0.0) acc(asinvrd, cone.h_vec2, r);
+    }
+    if (tm) {
+        tm->schur += wall() - t0;
+        if (type != KKT_TYPE_CORRECTOR) tm->n_schur += (long) cones.size();
     }
     return device_error_flag() ? HDSDP_RETCODE_FAILED : HDSDP_RETCODE_OK;
 }
@@ -1463,7 +1628,7 @@ __global__ void __launch_bounds__(kLzThreads, 1)
 // ---- Lanczos for blocks of order <= kSmallLanczosN: one CTA holds K = L^-1, D and the
 // Lanczos basis in shared memory and runs every step in one launch (the stepwise path
 // spends four launches per step, which dominates for small blocks).
-constexpr int kSmallLanczosN = 96;
+constexpr int kSmallLanczosN = kSmallLanczosMaxN;
 
 __host__ __device__ inline int small_ld(int n) { return n | 1; }  // odd stride: fewer bank conflicts
 
@@ -1512,8 +1677,8 @@ __device__ void small_mv(int n, const double *sK, const double *sD, const double
 // Start vector v0 = normalise(a + b) (a may be null), then maxdim steps of the
 // three-term recurrence exactly as lanczos_orth_kernel takes them; the basis V (all
 // maxdim + 1 columns, zero past a breakdown) and alpha / beta go to global memory.
-__global__ void lanczos_small_kernel(int n, const double *K, long ldk, const double *D, long ldD, const double *a,
-                                     const double *b, double *V, long ldv, double *ab, int maxdim) {
+__device__ void lanczos_small_body(int n, const double *K, long ldk, const double *D, long ldD, const double *a,
+                                   const double *b, double *V, long ldv, double *ab, int maxdim) {
     extern __shared__ double sm[];
     const int ls = small_ld(n);
     double *sK = sm, *sD = sK + (size_t) n * ls, *sV = sD + (size_t) n * ls, *w = sV + (size_t) (maxdim + 1) * n;
@@ -1569,9 +1734,9 @@ __global__ void lanczos_small_kernel(int n, const double *K, long ldk, const dou
 
 // The Ritz part of a converged check: z1 = V y1, z2 = M z1 (warm <- z2),
 // out[0] = |z2 - lam z1|; z2 = V y2, z1 = M z2, out[1] = |z1 - lam z2|.
-__global__ void lanczos_small_ritz_kernel(int n, const double *K, long ldk, const double *D, long ldD,
-                                          const double *V, long ldv, int kp1, const double *y, double lam,
-                                          double *warm, double *out) {
+__device__ void lanczos_small_ritz_body(int n, const double *K, long ldk, const double *D, long ldD,
+                                       const double *V, long ldv, int kp1, const double *y, double lam,
+                                       double *warm, double *out) {
     extern __shared__ double sm[];
     const int ls = small_ld(n);
     double *sK = sm, *sD = sK + (size_t) n * ls, *z1 = sD + (size_t) n * ls, *z2 = z1 + n, *t = z2 + n, *u = t + n;
@@ -1595,6 +1760,49 @@ __global__ void lanczos_small_ritz_kernel(int n, const double *K, long ldk, cons
         if (threadIdx.x == 0) out[pass] = v;
         __syncthreads();
     }
+}
+
+__global__ void lanczos_small_kernel(int n, const double *K, long ldk, const double *D, long ldD, const double *a,
+                                     const double *b, double *V, long ldv, double *ab, int maxdim) {
+    lanczos_small_body(n, K, ldk, D, ldD, a, b, V, ldv, ab, maxdim);
+}
+
+__global__ void lanczos_small_ritz_kernel(int n, const double *K, long ldk, const double *D, long ldD,
+                                          const double *V, long ldv, int kp1, const double *y, double lam,
+                                          double *warm, double *out) {
+    lanczos_small_ritz_body(n, K, ldk, D, ldD, V, ldv, kp1, y, lam, warm, out);
+}
+
+// Several cones' small-block runs in one launch, one CTA each (the jobs by value).
+struct LzStepJob {
+    const double *K, *D, *a, *b;
+    double *V, *ab;
+    long ldk, ldD, ldv;
+    int n, maxdim;
+};
+struct LzRitzJob {
+    const double *K, *D, *V, *y;
+    double *warm, *out;
+    long ldk, ldD, ldv;
+    double lam;
+    int n, kp1;
+};
+constexpr int kLzBatch = 36;
+struct LzStepBatch {
+    LzStepJob job[kLzBatch];
+};
+struct LzRitzBatch {
+    LzRitzJob job[kLzBatch];
+};
+
+__global__ void lanczos_small_batch_kernel(const LzStepBatch B) {
+    const LzStepJob &J = B.job[blockIdx.x];
+    lanczos_small_body(J.n, J.K, J.ldk, J.D, J.ldD, J.a, J.b, J.V, J.ldv, J.ab, J.maxdim);
+}
+
+__global__ void lanczos_small_ritz_batch_kernel(const LzRitzBatch B) {
+    const LzRitzJob &J = B.job[blockIdx.x];
+    lanczos_small_ritz_body(J.n, J.K, J.ldk, J.D, J.ldD, J.V, J.ldv, J.kp1, J.y, J.lam, J.warm, J.out);
 }
 
 // All eigenpairs of the symmetric tridiagonal matrix with diagonal d[0..n) and
@@ -1902,6 +2110,183 @@ hdsdp_retcode Lanczos::solve(DenseFactor &F, const double *D, long ldD, double *
         tm->n_lanczos += 1;
     }
     return ret;
+}
+
+// The small-block path of Lanczos::solve for several cones at once: their steps in one
+// launch, then the host replays each cone's check schedule; the Ritz evaluations that the
+// checks of one round ask for run in one launch and one wait. Per cone, every value and
+// decision is the one Lanczos::solve computes.
+namespace {
+struct LzRun {
+    LzTask *t;
+    int k = 0, lastChecked = -1;
+    bool done = false;
+    // the Ritz evaluation asked for
+    int kc = 0;
+    double eigMin1 = 0, eigMin2 = 0, betak = 0;
+    std::vector<double> ev, evec;
+};
+
+// runs the schedule from step k on; true when a Ritz evaluation is needed (its
+// coefficients uploaded), false when the run has ended
+bool lz_advance(LzRun &R) {
+    Lanczos &L = *R.t->lz;
+    const int maxdim = L.maxdim;
+    const int freq = std::min(maxdim / 5, 3);
+    auto scheduled = [&](int k) { return ((k + 1) % freq == 0) || k >= maxdim - 1; };
+    for (; R.k < maxdim && !R.done; ++R.k) {
+        const int k = R.k;
+        if (!scheduled(k)) continue;
+        const double th = wall();
+        int kc = k;
+        for (int q = R.lastChecked + 1; q <= k; ++q)
+            if (L.h_ab[maxdim + q] == 0.0) { kc = q; break; }
+        R.lastChecked = k;
+        const int kp1 = kc + 1;
+        if (kp1 < 2) {
+            R.t->ret = HDSDP_RETCODE_FAILED;
+            R.done = true;
+            return false;
+        }
+        std::vector<double> dd(L.h_ab, L.h_ab + kp1), ee(L.h_ab + maxdim, L.h_ab + maxdim + kp1);
+        ee[kp1 - 1] = 0.0;
+        tridiag_eig(kp1, dd, ee, R.ev, R.evec);
+        if (R.t->tm) R.t->tm->lz_host += wall() - th;
+        int i1 = 0, i2 = 0;
+        for (int i = 1; i < kp1; ++i)
+            if (R.ev[i] > R.ev[i1]) i1 = i;
+        i2 = (i1 == 0) ? 1 : 0;
+        for (int i = 0; i < kp1; ++i)
+            if (i != i1 && R.ev[i] > R.ev[i2]) i2 = i;
+        const double betak = L.h_ab[maxdim + kc];
+        const double resiVal = std::fabs(betak * R.evec[(size_t) kc + (size_t) i1 * kp1]);
+        if (!(resiVal < 1e-04 || kc >= maxdim - 1)) {
+            if (kc != k) R.done = true;
+            continue;
+        }
+        R.kc = kc;
+        R.eigMin1 = R.ev[i1];
+        R.eigMin2 = R.ev[i2];
+        R.betak = betak;
+        std::vector<double> yy(2 * kp1);
+        for (int i = 0; i < kp1; ++i) {
+            yy[i] = R.evec[(size_t) i + (size_t) i1 * kp1];
+            yy[kp1 + i] = R.evec[(size_t) i + (size_t) i2 * kp1];
+        }
+        HB_CUDA(cudaMemcpyAsync(L.d_y, yy.data(), sizeof(double) * 2 * kp1, cudaMemcpyHostToDevice, L.s));
+        return true;
+    }
+    return false;
+}
+
+// the outcome of the Ritz evaluation in h_scal; the schedule then moves on past step k
+void lz_ritz_done(LzRun &R) {
+    Lanczos &L = *R.t->lz;
+    const double resiVal1 = L.h_scal[0], resiVal2 = L.h_scal[1];
+    const double resiDiff = R.eigMin1 - R.eigMin2 - resiVal2;
+    double valGamma = (resiDiff > 0) ? resiDiff : 1e-16;
+    const double sq = resiVal1 * resiVal1 / valGamma;
+    valGamma = std::min(resiVal1, sq);
+    if (valGamma < 1e-03 || valGamma + R.eigMin1 <= 0.5) {
+        *R.t->maxStep = (valGamma + R.eigMin1 <= 0.0) ? HDSDP_INFINITY : 1.0 / (valGamma + R.eigMin1);
+        R.done = true;
+    } else {
+        if (R.betak == 0.0) {
+            R.t->ret = HDSDP_RETCODE_FAILED;
+            R.done = true;
+            return;
+        }
+        *R.t->maxStep = 1.0 / (valGamma + R.eigMin1);
+        if (R.kc != R.k) R.done = true;
+    }
+    R.k += 1;
+}
+}  // namespace
+
+void lanczos_small_batch(std::vector<LzTask> &tasks) {
+    if (tasks.empty()) return;
+    const double t0 = wall();
+    cudaStream_t s = tasks[0].lz->s;
+    Timers *tm = tasks[0].tm;
+    static std::atomic<unsigned long long> attr{0};
+    once_per_device(attr, [] {
+        const int bytes = (int) small_lanczos_smem(kSmallLanczosN, 30);
+        HB_CUDA(cudaFuncSetAttribute((const void *) lanczos_small_batch_kernel,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+        HB_CUDA(cudaFuncSetAttribute((const void *) lanczos_small_ritz_batch_kernel,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    });
+    for (LzTask &t : tasks) {
+        t.ret = HDSDP_RETCODE_OK;
+        compute_inverse_factor(s, *t.F);
+    }
+    if (tm) {
+        HB_CUDA(cudaStreamSynchronize(s));
+        tm->lz_inverse += wall() - t0;
+    }
+    int maxn = 0, maxdim = 0;
+    for (LzTask &t : tasks) {
+        maxn = std::max(maxn, t.lz->n);
+        maxdim = std::max(maxdim, t.lz->maxdim);
+    }
+    const size_t smem = small_lanczos_smem(maxn, maxdim);
+    for (size_t b0 = 0; b0 < tasks.size(); b0 += kLzBatch) {
+        const int nb = (int) std::min<size_t>(kLzBatch, tasks.size() - b0);
+        LzStepBatch B;
+        for (int q = 0; q < nb; ++q) {
+            LzTask &t = tasks[b0 + q];
+            Lanczos &L = *t.lz;
+            B.job[q] = LzStepJob{t.F->K, t.D, L.nComputed == 0 ? nullptr : L.warm,
+                                 L.nComputed == 0 ? L.init_vec : L.pert_vec, L.V, L.d_ab, t.F->ld, t.ldD, L.ld, L.n,
+                                 L.maxdim};
+        }
+        lanczos_small_batch_kernel<<<hb::counted(nb), 256, smem, s>>>(B);
+        HB_CUDA(cudaGetLastError());
+    }
+    for (LzTask &t : tasks) {
+        Lanczos &L = *t.lz;
+        HB_CUDA(cudaMemcpyAsync(L.h_ab, L.d_ab, sizeof(double) * (2 * L.maxdim + 2), cudaMemcpyDeviceToHost, s));
+        if (tm) tm->n_lanczos_mv += L.maxdim;
+    }
+    HB_CUDA(cudaStreamSynchronize(s));
+    std::vector<LzRun> runs(tasks.size());
+    std::vector<LzRun *> want;
+    for (size_t q = 0; q < tasks.size(); ++q) {
+        runs[q].t = &tasks[q];
+        if (lz_advance(runs[q])) want.push_back(&runs[q]);
+    }
+    while (!want.empty()) {
+        for (size_t b0 = 0; b0 < want.size(); b0 += kLzBatch) {
+            const int nb = (int) std::min<size_t>(kLzBatch, want.size() - b0);
+            LzRitzBatch B;
+            for (int q = 0; q < nb; ++q) {
+                LzRun &R = *want[b0 + q];
+                Lanczos &L = *R.t->lz;
+                B.job[q] = LzRitzJob{R.t->F->K, R.t->D, L.V, L.d_y, L.warm, L.d_scal, R.t->F->ld, R.t->ldD, L.ld,
+                                     R.eigMin1, L.n, R.kc + 1};
+            }
+            lanczos_small_ritz_batch_kernel<<<hb::counted(nb), 256, smem, s>>>(B);
+            HB_CUDA(cudaGetLastError());
+        }
+        for (LzRun *R : want) {
+            Lanczos &L = *R->t->lz;
+            HB_CUDA(cudaMemcpyAsync(L.h_scal, L.d_scal, sizeof(double) * 2, cudaMemcpyDeviceToHost, s));
+            if (tm) tm->n_lanczos_mv += 2;
+        }
+        HB_CUDA(cudaStreamSynchronize(s));
+        std::vector<LzRun *> next;
+        for (LzRun *R : want) {
+            lz_ritz_done(*R);
+            if (lz_advance(*R)) next.push_back(R);
+        }
+        want.swap(next);
+    }
+    for (LzTask &t : tasks)
+        if (t.ret == HDSDP_RETCODE_OK) t.lz->nComputed += 1;
+    if (tm) {
+        tm->lanczos += wall() - t0;
+        tm->n_lanczos += (long) tasks.size();
+    }
 }
 
 }  // namespace hb

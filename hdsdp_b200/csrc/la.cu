@@ -898,6 +898,27 @@ void factorize_async(cudaStream_t s, DenseFactor &F, const double *S, long ldS) 
     HB_CUDA(cudaGetLastError());
 }
 
+bool small_factor_batch_enqueue(cudaStream_t s, DenseFactor *const *F, const double *const *S, const long *ldS,
+                                int count);
+
+void factorize_small_batch(cudaStream_t s, DenseFactor *const *F, const double *const *S, const long *ldS, int count) {
+    if (count <= 0) return;
+    ensure_attrs();
+    if (!small_factor_batch_enqueue(s, F, S, ldS, count)) {
+        for (int q = 0; q < count; ++q) factorize_async(s, *F[q], S[q], ldS[q]);
+        return;
+    }
+    for (int q = 0; q < count; ++q) {
+        DenseFactor &G = *F[q];
+        G.k_valid = false;
+        G.k_pending = G.fuse_k && G.K && G.KT;
+        G.factored = true;
+        G.logdet_valid = false;
+        HB_CUDA(cudaMemcpyAsync(G.h_info, G.d_info, G.stat_logdet ? 2 * sizeof(double) : sizeof(int),
+                                cudaMemcpyDeviceToHost, s));
+    }
+}
+
 bool factor_status(cudaStream_t s, DenseFactor &F) {
     HB_CUDA(cudaStreamSynchronize(s));
     F.ok = (*F.h_info == 0);

@@ -86,6 +86,11 @@ bool factorize(cudaStream_t s, DenseFactor &F, const double *S, long ldS);
 // Enqueue the factorisation without synchronising; call factor_status() later.
 void factorize_async(cudaStream_t s, DenseFactor &F, const double *S, long ldS);
 bool factor_status(cudaStream_t s, DenseFactor &F);
+// Enqueue the factorisations of F[q] (order <= kSmallFactorMaxN) of S[q] (ldS[q]) for
+// q < count, one CTA each, in one launch per kSmallBatch of them: the arithmetic of
+// factorize_async for a single panel. Call factor_status() on each afterwards.
+constexpr int kSmallFactorMaxN = 64;
+void factorize_small_batch(cudaStream_t s, DenseFactor *const *F, const double *const *S, const long *ldS, int count);
 // K = L^-1 and KT = K^T (lower / upper triangular). Requires a successful factor.
 void compute_inverse_factor(cudaStream_t s, DenseFactor &F);
 // W = S^-1 = K^T K, full symmetric, into W (ldW).

@@ -353,8 +353,47 @@ void schur_precision(hdsdp *h) {
 }
 
 // ---- the cones in the user's order (interface/hdsdp_algo.c: every loop over HCones)
+//
+// With several SDP cones, the checks first bring every SDP cone's buffer up to date and
+// factor them together (factor_buffers: the small blocks in one launch, one wait), then
+// read the answers in the user's order with the reference's early exit. The cones after
+// the first failing one have then been factored too, which changes no result: every later
+// use of a buffer rebuilds it from its inputs.
+static std::vector<SdpCone *> sdp_cones(hdsdp *h) {
+    std::vector<SdpCone *> v;
+    for (ConeSlot &k : h->cones)
+        if (k.sdp) v.push_back(k.sdp);
+    return v;
+}
+
+static bool batched_cones(hdsdp *h) {
+    int nSdp = 0;
+    for (ConeSlot &k : h->cones) nSdp += k.sdp ? 1 : 0;
+    return nSdp > 1;
+}
+
+// the answers of the batched checks in the user's order: SDP cones from ok, LP cones by
+// their own check; stops at the first cone that is not interior
+template <class LpCheck>
+static int cones_first_failure(hdsdp *h, const std::vector<char> &ok, LpCheck lpCheck) {
+    size_t q = 0;
+    for (ConeSlot &k : h->cones) {
+        const int in = k.sdp ? (int) ok[q++] : lpCheck(*k.lp);
+        if (!in) return 0;
+    }
+    return 1;
+}
+
 hdsdp_retcode cones_interior(hdsdp *h, double tau, const double *y, int *interior) {
     *interior = 1;
+    if (batched_cones(h)) {
+        std::vector<SdpCone *> sc = sdp_cones(h);
+        for (SdpCone *c : sc) c->update(tau, y);
+        std::vector<char> ok;
+        factor_buffers(sc, BUFFER_DUALVAR, ok);
+        *interior = cones_first_failure(h, ok, [&](LpCone &lp) { return lp.interior_check(tau, y); });
+        return device_error_flag() ? HDSDP_RETCODE_FAILED : HDSDP_RETCODE_OK;
+    }
     for (ConeSlot &k : h->cones) {
         if (k.sdp) {
             hdsdp_retcode r = k.sdp->interior_check(tau, y, interior);
@@ -370,6 +409,15 @@ hdsdp_retcode cones_interior(hdsdp *h, double tau, const double *y, int *interio
 hdsdp_retcode cones_interior_expert(hdsdp *h, double dC, double dAs, const double *y, double dEye, int which,
                                     int *interior) {
     *interior = 1;
+    if (batched_cones(h)) {
+        std::vector<SdpCone *> sc = sdp_cones(h);
+        for (SdpCone *c : sc) c->update_buffer(dC, dAs, y, dEye, which);
+        std::vector<char> ok;
+        factor_buffers(sc, which == BUFFER_DUALVAR ? BUFFER_DUALVAR : BUFFER_DUALCHECK, ok);
+        *interior = cones_first_failure(
+            h, ok, [&](LpCone &lp) { return lp.interior_check_expert(dC, dAs, y, dEye, which); });
+        return device_error_flag() ? HDSDP_RETCODE_FAILED : HDSDP_RETCODE_OK;
+    }
     for (ConeSlot &k : h->cones) {
         if (k.sdp) {
             hdsdp_retcode r = k.sdp->interior_check_expert(dC, dAs, y, dEye, which, interior);
@@ -384,6 +432,31 @@ hdsdp_retcode cones_interior_expert(hdsdp *h, double dC, double dAs, const doubl
 
 // running minimum of the cones' step bounds
 hdsdp_retcode cones_ratio(hdsdp *h, double dtau, const double *dy, double ada, int which, double *mx) {
+    if (batched_cones(h)) {
+        // the small blocks' Lanczos bounds share their launches (lanczos_small_batch)
+        std::vector<double> st(h->cones.size(), HDSDP_INFINITY);
+        std::vector<LzTask> tasks;
+        size_t q = 0;
+        for (ConeSlot &k : h->cones) {
+            double *sq = &st[q++];
+            if (k.sdp && k.sdp->small_lanczos()) {
+                SdpCone &c = *k.sdp;
+                c.update_buffer(dtau, -1.0, dy, ada * c.dualResidual, BUFFER_DUALSTEP);
+                tasks.push_back(LzTask{&c.lz, which == BUFFER_DUALVAR ? &c.Fvar : &c.Fcheck, c.dS, c.ld, sq, c.tm,
+                                       HDSDP_RETCODE_OK});
+            } else if (k.sdp) {
+                hdsdp_retcode r = k.sdp->ratio_test(dtau, dy, ada, which, sq);
+                if (r != HDSDP_RETCODE_OK) return r;
+            } else {
+                *sq = k.lp->ratio_test(dtau, dy, ada, which);
+            }
+        }
+        lanczos_small_batch(tasks);
+        for (const LzTask &t : tasks)
+            if (t.ret != HDSDP_RETCODE_OK) return t.ret;
+        for (double v : st) *mx = std::min(*mx, v);
+        return HDSDP_RETCODE_OK;
+    }
     for (ConeSlot &k : h->cones) {
         double st = 0.0;
         if (k.sdp) {
@@ -399,6 +472,14 @@ hdsdp_retcode cones_ratio(hdsdp *h, double dtau, const double *dy, double ada, i
 
 hdsdp_retcode cones_add_step(hdsdp *h, double step, int which, int *interior) {
     *interior = 1;
+    if (batched_cones(h)) {
+        std::vector<SdpCone *> sc = sdp_cones(h);
+        for (SdpCone *c : sc) c->add_step(step, which);
+        std::vector<char> ok;
+        factor_buffers(sc, which == BUFFER_DUALVAR ? BUFFER_DUALVAR : BUFFER_DUALCHECK, ok);
+        *interior = cones_first_failure(h, ok, [&](LpCone &lp) { return lp.add_step_and_check(step, which); });
+        return device_error_flag() ? HDSDP_RETCODE_FAILED : HDSDP_RETCODE_OK;
+    }
     for (ConeSlot &k : h->cones) {
         if (k.sdp) {
             hdsdp_retcode r = k.sdp->add_step_and_check(step, which, interior);
@@ -421,6 +502,26 @@ void cones_set_start(hdsdp *h, double r) {
 // sum of the cones' log det (SDP) or sum log s (LP) at the buffer `which`
 hdsdp_retcode cones_barrier(hdsdp *h, double tau, const double *y, int which, double *sum) {
     *sum = 0.0;
+    if (y && batched_cones(h)) {
+        std::vector<SdpCone *> sc = sdp_cones(h);
+        for (SdpCone *c : sc) c->update(tau, y);
+        std::vector<char> ok;
+        factor_buffers(sc, BUFFER_DUALVAR, ok);
+        for (char o : ok)
+            if (!o) return HDSDP_RETCODE_FAILED;
+        // every factor is in place: the log dets are read without a new factorisation
+        for (ConeSlot &k : h->cones) {
+            if (k.sdp) {
+                double ld = 0.0;
+                hdsdp_retcode r = k.sdp->get_barrier(tau, nullptr, which, &ld);
+                if (r != HDSDP_RETCODE_OK) return r;
+                *sum += ld;
+            } else {
+                *sum += k.lp->get_barrier(tau, y, which);
+            }
+        }
+        return HDSDP_RETCODE_OK;
+    }
     for (ConeSlot &k : h->cones) {
         if (k.sdp) {
             double ld = 0.0;
@@ -437,6 +538,11 @@ hdsdp_retcode cones_barrier(hdsdp *h, double tau, const double *y, int which, do
 // HKKTBuildUp (interface/hdsdp_schur.c:256-268): clean, then every cone in order
 hdsdp_retcode build_kkt(hdsdp *h, int type) {
     h->kkt.clean(type);
+    if (batched_cones(h) && (type == KKT_TYPE_INFEASIBLE || type == KKT_TYPE_CORRECTOR)) {
+        bool lp = false;
+        for (ConeSlot &k : h->cones) lp = lp || (k.lp != nullptr);
+        if (!lp) return h->kkt.add_sdp_batch(sdp_cones(h), type);
+    }
     for (ConeSlot &k : h->cones) {
         if (k.sdp) {
             hdsdp_retcode r = h->kkt.add_sdp(*k.sdp, type);

@@ -66,6 +66,23 @@ struct Lanczos {
     hdsdp_retcode solve(DenseFactor &F, const double *D, long ldD, double *maxStep, Timers *tm);
 };
 
+// One cone's small-block Lanczos bound (order <= 96, dense factor) for lanczos_small_batch:
+// the operator I + alpha K (-D) K^T of its factor F and step matrix D, the bound into
+// *maxStep, the outcome in ret.
+struct LzTask {
+    Lanczos *lz;
+    DenseFactor *F;
+    const double *D;
+    long ldD;
+    double *maxStep;
+    Timers *tm;
+    hdsdp_retcode ret;
+};
+// The bounds of several tasks (one stream), the launches shared; each task's result is
+// the one Lanczos::solve gives.
+void lanczos_small_batch(std::vector<LzTask> &tasks);
+constexpr int kSmallLanczosMaxN = 96;
+
 // Inputs that produced a dual-slack buffer (dC*C + dAs*sum y_i A_i + dEye*I); a
 // factorisation of a buffer rebuilt from identical inputs is reused, which gives
 // bit-identical results because the factor kernels are deterministic.
@@ -124,11 +141,20 @@ struct SdpCone {
     }
     bool hybrid_factor(int which);
     bool ensure_dense(int which);
+    enum { FP_DONE = 0, FP_SMALL = 1, FP_ASYNC = 2 };
+    int factor_plan(int which, bool *ok);
+    bool factor_finish(int which);
+    // the step S += step * dS of add_step_and_check, without the factorisation
+    void add_step(double step, int which);
+    // ratio_test takes the small-block Lanczos path (order 2 .. kSmallLanczosMaxN, no
+    // sparse factor), which several cones can share (lanczos_small_batch)
+    bool small_lanczos() const { return n > 1 && n <= kSmallLanczosMaxN && !hy; }
     Lanczos lz;
     double dualResidual = 0.0, dualPerturb = 0.0;
     double *d_y = nullptr;       // device copy of the current coefficient vector
     double *d_vec = nullptr;     // device m scratch
     double *h_vec = nullptr;     // pinned m scratch
+    double *d_vec2 = nullptr, *h_vec2 = nullptr;   // second pair (batched Schur builds)
     double *d_scal = nullptr, *h_scal = nullptr;
     double objScal = 1.0;
     Timers *tm = nullptr;
@@ -162,6 +188,10 @@ struct SdpCone {
     void atimesx(const double *X, double *out);                                // host out (problem m), accumulated
     double trace_cx(const double *X);
 };
+
+// factor_buffer(which) of several cones (all on one stream), small dense factorisations
+// batched: ok[q] = positive definite
+void factor_buffers(const std::vector<SdpCone *> &cones, int which, std::vector<char> &ok);
 
 // Scalar dual box l <= y <= u (interface/hdsdp_conic_bound.c), host-side O(m).
 struct BoundCone {
@@ -268,6 +298,9 @@ struct KKT {
     void clean(int type);
     void open_m();
     hdsdp_retcode add_sdp(SdpCone &cone, int type);
+    // add_sdp for several SDP cones (types KKT_TYPE_INFEASIBLE and KKT_TYPE_CORRECTOR), one
+    // wait for all
+    hdsdp_retcode add_sdp_batch(const std::vector<SdpCone *> &cones, int type);
     hdsdp_retcode build(SdpCone &cone, int type) {  // a build with this single cone
         clean(type);
         return add_sdp(cone, type);
