@@ -623,9 +623,10 @@ struct SmallFactorJob {
     double *L, *Dinv, *K, *KT;
     long lds, ld;
     int *info;
+    double *hinfo;   // device address of the factor's pinned status words (written directly)
     int n, logdet;
 };
-constexpr int kSmallBatch = 40;
+constexpr int kSmallBatch = 36;
 struct SmallFactorBatch {
     SmallFactorJob job[kSmallBatch];
 };
@@ -662,13 +663,19 @@ __global__ void __launch_bounds__(COOP_THREADS, 1) potrf_small_batch_kernel(cons
     __syncthreads();
     const bool ok = (*(volatile int *) J.info == 0);
     if (ok && J.K) k_final_tile(J.Dinv, J.ld, J.K, J.KT, J.ld, n, 0, 0, sm);
+    double acc = 0.0;
     if (J.logdet) {
         __threadfence_block();
         __syncthreads();
-        double acc = 0.0;
         for (int i = threadIdx.x; i < n; i += blockDim.x) acc += log(J.L[(size_t) i + (size_t) i * J.ld]);
         acc = small_block_sum(acc);
         if (threadIdx.x == 0) reinterpret_cast<double *>(J.info)[1] = acc;
+    }
+    if (threadIdx.x == 0) {
+        // the status words straight into the host's pinned mirror
+        const int v = *(volatile int *) J.info;
+        reinterpret_cast<volatile int *>(J.hinfo)[0] = v;
+        if (J.logdet) J.hinfo[1] = acc;
     }
 }
 
@@ -996,7 +1003,9 @@ bool coop_factorize_enqueue(cudaStream_t s, DenseFactor &F, const double *S, lon
 }
 
 // The factorisations of F[0..count) (each n <= 64) of S[i] (ldS[i]) in launches of up to
-// kSmallBatch CTAs; returns false if a launch failed.
+// kSmallBatch CTAs, the status words written into each factor's pinned host mirror by the
+// kernel; returns false (nothing enqueued) if a mirror has no device address, or false
+// after a failed launch.
 bool small_factor_batch_enqueue(cudaStream_t s, DenseFactor *const *F, const double *const *S, const long *ldS,
                                 int count) {
     static std::atomic<unsigned long long> attr{0};
@@ -1009,8 +1018,13 @@ bool small_factor_batch_enqueue(cudaStream_t s, DenseFactor *const *F, const dou
         const int nb = std::min(kSmallBatch, count - b0);
         for (int q = 0; q < nb; ++q) {
             DenseFactor &G = *F[b0 + q];
+            double *hd = nullptr;
+            if (cudaHostGetDevicePointer((void **) &hd, G.h_info, 0) != cudaSuccess || !hd) {
+                cudaGetLastError();
+                return false;
+            }
             B.job[q] = SmallFactorJob{S[b0 + q], G.L, G.Dinv, G.fuse_k ? G.K : nullptr, G.fuse_k ? G.KT : nullptr,
-                                      ldS[b0 + q], G.ld, G.d_info, G.n, G.stat_logdet ? 1 : 0};
+                                      ldS[b0 + q], G.ld, G.d_info, hd, G.n, G.stat_logdet ? 1 : 0};
         }
         potrf_small_batch_kernel<<<hb::counted(nb), COOP_THREADS, SM_DOUBLES * sizeof(double), s>>>(B);
         if (cudaGetLastError() != cudaSuccess) return false;

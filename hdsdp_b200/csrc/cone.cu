@@ -551,10 +551,10 @@ int SdpCone::factor_plan(int which, bool *ok) {
     return FP_ASYNC;
 }
 
-bool SdpCone::factor_finish(int which) {
+bool SdpCone::factor_finish(int which, bool synced) {
     const bool var = (which == BUFFER_DUALVAR);
     DenseFactor &F = var ? Fvar : Fcheck;
-    const bool ok = factor_status(s, F);
+    const bool ok = synced ? factor_status_ready(F) : factor_status(s, F);
     (var ? hyVar : hyCheck) = false;
     (var ? facVar : facCheck) = var ? sigVar : sigCheck;
     (var ? facVarOk : facCheckOk) = ok;
@@ -586,8 +586,9 @@ void factor_buffers(const std::vector<SdpCone *> &cones, int which, std::vector<
         if (c.tm) tm = c.tm;
     }
     if (!F.empty()) factorize_small_batch(cones[0]->s, F.data(), S.data(), ldS.data(), (int) F.size());
+    HB_CUDA(cudaStreamSynchronize(cones[0]->s));
     for (size_t q = 0; q < cones.size(); ++q)
-        if (plan[q] != SdpCone::FP_DONE) ok[q] = cones[q]->factor_finish(which) ? 1 : 0;
+        if (plan[q] != SdpCone::FP_DONE) ok[q] = cones[q]->factor_finish(which, true) ? 1 : 0;
     if (tm) tm->s_factor += wall() - t0;
 }
 
@@ -1774,20 +1775,22 @@ __global__ void lanczos_small_ritz_kernel(int n, const double *K, long ldk, cons
 }
 
 // Several cones' small-block runs in one launch, one CTA each (the jobs by value).
+// hab / hout: device addresses of the host's pinned mirrors of ab / out, written directly
+// when set
 struct LzStepJob {
     const double *K, *D, *a, *b;
-    double *V, *ab;
+    double *V, *ab, *hab;
     long ldk, ldD, ldv;
     int n, maxdim;
 };
 struct LzRitzJob {
     const double *K, *D, *V, *y;
-    double *warm, *out;
+    double *warm, *out, *hout;
     long ldk, ldD, ldv;
     double lam;
     int n, kp1;
 };
-constexpr int kLzBatch = 36;
+constexpr int kLzBatch = 32;
 struct LzStepBatch {
     LzStepJob job[kLzBatch];
 };
@@ -1798,11 +1801,21 @@ struct LzRitzBatch {
 __global__ void lanczos_small_batch_kernel(const LzStepBatch B) {
     const LzStepJob &J = B.job[blockIdx.x];
     lanczos_small_body(J.n, J.K, J.ldk, J.D, J.ldD, J.a, J.b, J.V, J.ldv, J.ab, J.maxdim);
+    if (J.hab) {
+        __threadfence_block();
+        __syncthreads();
+        for (int e = threadIdx.x; e < 2 * J.maxdim + 2; e += blockDim.x) J.hab[e] = J.ab[e];
+    }
 }
 
 __global__ void lanczos_small_ritz_batch_kernel(const LzRitzBatch B) {
     const LzRitzJob &J = B.job[blockIdx.x];
     lanczos_small_ritz_body(J.n, J.K, J.ldk, J.D, J.ldD, J.V, J.ldv, J.kp1, J.y, J.lam, J.warm, J.out);
+    if (J.hout) {
+        __threadfence_block();
+        __syncthreads();
+        if (threadIdx.x < 2) J.hout[threadIdx.x] = J.out[threadIdx.x];
+    }
 }
 
 // All eigenpairs of the symmetric tridiagonal matrix with diagonal d[0..n) and
@@ -2230,6 +2243,21 @@ void lanczos_small_batch(std::vector<LzTask> &tasks) {
         maxdim = std::max(maxdim, t.lz->maxdim);
     }
     const size_t smem = small_lanczos_smem(maxn, maxdim);
+    // device addresses of the pinned mirrors (alpha / beta and the Ritz residuals), which
+    // the kernels write directly; a task without one gets copies
+    auto mapped = [](double *h) {
+        double *d = nullptr;
+        if (cudaHostGetDevicePointer((void **) &d, h, 0) != cudaSuccess) {
+            cudaGetLastError();
+            d = nullptr;
+        }
+        return d;
+    };
+    std::vector<double *> hab(tasks.size()), hsc(tasks.size());
+    for (size_t q = 0; q < tasks.size(); ++q) {
+        hab[q] = mapped(tasks[q].lz->h_ab);
+        hsc[q] = mapped(tasks[q].lz->h_scal);
+    }
     for (size_t b0 = 0; b0 < tasks.size(); b0 += kLzBatch) {
         const int nb = (int) std::min<size_t>(kLzBatch, tasks.size() - b0);
         LzStepBatch B;
@@ -2237,15 +2265,16 @@ void lanczos_small_batch(std::vector<LzTask> &tasks) {
             LzTask &t = tasks[b0 + q];
             Lanczos &L = *t.lz;
             B.job[q] = LzStepJob{t.F->K, t.D, L.nComputed == 0 ? nullptr : L.warm,
-                                 L.nComputed == 0 ? L.init_vec : L.pert_vec, L.V, L.d_ab, t.F->ld, t.ldD, L.ld, L.n,
-                                 L.maxdim};
+                                 L.nComputed == 0 ? L.init_vec : L.pert_vec, L.V, L.d_ab, hab[b0 + q], t.F->ld, t.ldD,
+                                 L.ld, L.n, L.maxdim};
         }
         lanczos_small_batch_kernel<<<hb::counted(nb), 256, smem, s>>>(B);
         HB_CUDA(cudaGetLastError());
     }
-    for (LzTask &t : tasks) {
-        Lanczos &L = *t.lz;
-        HB_CUDA(cudaMemcpyAsync(L.h_ab, L.d_ab, sizeof(double) * (2 * L.maxdim + 2), cudaMemcpyDeviceToHost, s));
+    for (size_t q = 0; q < tasks.size(); ++q) {
+        Lanczos &L = *tasks[q].lz;
+        if (!hab[q])
+            HB_CUDA(cudaMemcpyAsync(L.h_ab, L.d_ab, sizeof(double) * (2 * L.maxdim + 2), cudaMemcpyDeviceToHost, s));
         if (tm) tm->n_lanczos_mv += L.maxdim;
     }
     HB_CUDA(cudaStreamSynchronize(s));
@@ -2262,15 +2291,16 @@ void lanczos_small_batch(std::vector<LzTask> &tasks) {
             for (int q = 0; q < nb; ++q) {
                 LzRun &R = *want[b0 + q];
                 Lanczos &L = *R.t->lz;
-                B.job[q] = LzRitzJob{R.t->F->K, R.t->D, L.V, L.d_y, L.warm, L.d_scal, R.t->F->ld, R.t->ldD, L.ld,
-                                     R.eigMin1, L.n, R.kc + 1};
+                B.job[q] = LzRitzJob{R.t->F->K, R.t->D, L.V, L.d_y, L.warm, L.d_scal, hsc[R.t - tasks.data()],
+                                     R.t->F->ld, R.t->ldD, L.ld, R.eigMin1, L.n, R.kc + 1};
             }
             lanczos_small_ritz_batch_kernel<<<hb::counted(nb), 256, smem, s>>>(B);
             HB_CUDA(cudaGetLastError());
         }
         for (LzRun *R : want) {
             Lanczos &L = *R->t->lz;
-            HB_CUDA(cudaMemcpyAsync(L.h_scal, L.d_scal, sizeof(double) * 2, cudaMemcpyDeviceToHost, s));
+            if (!hsc[R->t - tasks.data()])
+                HB_CUDA(cudaMemcpyAsync(L.h_scal, L.d_scal, sizeof(double) * 2, cudaMemcpyDeviceToHost, s));
             if (tm) tm->n_lanczos_mv += 2;
         }
         HB_CUDA(cudaStreamSynchronize(s));

@@ -914,9 +914,16 @@ void factorize_small_batch(cudaStream_t s, DenseFactor *const *F, const double *
         G.k_pending = G.fuse_k && G.K && G.KT;
         G.factored = true;
         G.logdet_valid = false;
-        HB_CUDA(cudaMemcpyAsync(G.h_info, G.d_info, G.stat_logdet ? 2 * sizeof(double) : sizeof(int),
-                                cudaMemcpyDeviceToHost, s));
     }
+}
+
+bool factor_status_ready(DenseFactor &F) {
+    F.ok = (*(volatile int *) F.h_info == 0);
+    F.k_valid = F.ok && F.k_pending;
+    F.k_pending = false;
+    F.logdet_valid = F.ok && F.stat_logdet;
+    if (F.logdet_valid) F.logdet = 2.0 * reinterpret_cast<const volatile double *>(F.h_info)[1];
+    return F.ok;
 }
 
 bool factor_status(cudaStream_t s, DenseFactor &F) {

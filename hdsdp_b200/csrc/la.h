@@ -91,6 +91,9 @@ bool factor_status(cudaStream_t s, DenseFactor &F);
 // factorize_async for a single panel. Call factor_status() on each afterwards.
 constexpr int kSmallFactorMaxN = 64;
 void factorize_small_batch(cudaStream_t s, DenseFactor *const *F, const double *const *S, const long *ldS, int count);
+// factor_status() without its wait, for a caller that has synchronised the stream since
+// the factorisation was enqueued
+bool factor_status_ready(DenseFactor &F);
 // K = L^-1 and KT = K^T (lower / upper triangular). Requires a successful factor.
 void compute_inverse_factor(cudaStream_t s, DenseFactor &F);
 // W = S^-1 = K^T K, full symmetric, into W (ldW).

@@ -143,7 +143,7 @@ struct SdpCone {
     bool ensure_dense(int which);
     enum { FP_DONE = 0, FP_SMALL = 1, FP_ASYNC = 2 };
     int factor_plan(int which, bool *ok);
-    bool factor_finish(int which);
+    bool factor_finish(int which, bool synced = false);
     // the step S += step * dS of add_step_and_check, without the factorisation
     void add_step(double step, int which);
     // ratio_test takes the small-block Lanczos path (order 2 .. kSmallLanczosMaxN, no
