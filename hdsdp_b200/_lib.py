@@ -24,7 +24,7 @@ EXPORTS = [
     "hdsdpb_sparse_analyse",
     "hdsdpb_sparse_cholesky", "hdsdpb_sparse_congruence",
     "HDSDPGetIterLog", "HDSDPGetTimers", "HDSDPAdjoint",
-    "hdsdpb_schur_probe", "hdsdpb_ratio_probe", "hdsdpb_cholesky", "hdsdpb_cholesky_noalloc", "hdsdpb_inverse", "hdsdpb_gemm",
+    "hdsdpb_schur_probe", "hdsdpb_ratio_probe", "hdsdpb_cholesky", "hdsdpb_cholesky_batch", "hdsdpb_cholesky_noalloc", "hdsdpb_inverse", "hdsdpb_gemm",
     "hdsdpb_kernel_timing", "hdsdpb_gridsync_probe", "hdsdpb_launch_count", "hdsdpb_alloc_calls", "hdsdpb_release_cached_memory",
     "hdsdpb_kstat_enable", "hdsdpb_kstat_read", "hdsdpb_split_gemm", "hdsdpb_cholesky_solve", "HReadSDPA",
     # the conic callback interface and the KKT manager (include/hdsdp_conic.h)
@@ -87,6 +87,7 @@ def load():
         "hdsdpb_schur_probe": ([i, i, ip, ip, dp, dp, d, i, dp, dp, dp, dp], i),
         "hdsdpb_ratio_probe": ([i, i, ip, ip, dp, dp, d, dp, d, dp, dp], i),
         "hdsdpb_cholesky": ([i, dp, dp, dp], i),
+        "hdsdpb_cholesky_batch": ([i, i, i, dp, dp, dp, dp, ip], i),
         "hdsdpb_cholesky_noalloc": ([i, dp, dp, dp], i),
         "hdsdpb_inverse": ([i, dp, dp], i),
         "hdsdpb_cholesky_solve": ([i, dp, dp, dp], i),

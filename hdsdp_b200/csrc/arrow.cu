@@ -120,6 +120,7 @@ void apply_kt(cudaStream_t s, DenseFactor &F, const double *x, double *y) {
     coldot(s, F.n, F.n, F.K, F.ld, x, y, 1.0, 0.0, 1);
 }
 
+constexpr int kArrowBatchMaxN = 512;   // local blocks factored one CTA each up to this order
 constexpr int kColWarps = 8;      // columns per block of the batched column-dot kernel
 constexpr int kGemvRows = 128;    // rows per block of the batched gemv
 constexpr int kGemvCols = 256;    // columns per split of the batched gemv
@@ -228,12 +229,26 @@ void arrow_matvec(cudaStream_t s, ArrowSchur &A, const double *x, double *y) {
 // the factors of the current blocks (W_k and the coupling block's Schur complement)
 bool arrow_factor_once(cudaStream_t s, ArrowSchur &A) {
     const int nc = A.nc, K = A.ncone;
-    // every block's factorisation enqueued, then their statuses read together
-    for (int k = 0; k < K; ++k)
-        if (A.lk[k] > 0) factorize_async(s, A.Fk[k], A.Mkk[k], A.ldk[k]);
+    // every block's factorisation enqueued (blocks of order <= kArrowBatchMaxN one CTA each,
+    // in shared launches; larger ones on the whole GPU), then their statuses read together
+    std::vector<DenseFactor *> bF;
+    std::vector<const double *> bS;
+    std::vector<long> bld;
+    for (int k = 0; k < K; ++k) {
+        if (A.lk[k] == 0) continue;
+        if (K > 1 && A.lk[k] <= kArrowBatchMaxN) {
+            bF.push_back(&A.Fk[k]);
+            bS.push_back(A.Mkk[k]);
+            bld.push_back(A.ldk[k]);
+        } else {
+            factorize_async(s, A.Fk[k], A.Mkk[k], A.ldk[k]);
+        }
+    }
+    if (!bF.empty()) factorize_small_batch(s, bF.data(), bS.data(), bld.data(), (int) bF.size());
+    HB_CUDA(cudaStreamSynchronize(s));
     bool ok = true;
     for (int k = 0; k < K; ++k)
-        if (A.lk[k] > 0 && !factor_status(s, A.Fk[k])) ok = false;
+        if (A.lk[k] > 0 && !factor_status_ready(A.Fk[k])) ok = false;
     if (!ok) return false;
     for (int k = 0; k < K; ++k) {
         const int l = A.lk[k];

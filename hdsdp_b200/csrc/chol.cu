@@ -536,13 +536,16 @@ __device__ __forceinline__ void k_final_tile(const double *Dinv, long ldd, doubl
     }
 }
 
-__global__ void __launch_bounds__(COOP_THREADS, 1) potrf_coop_kernel(double *L, long ld, int n, double *Dinv,
-                                                                  long ldd, int *info, double *K, double *KT) {
-    cg::grid_group grid = cg::this_grid();
-    extern __shared__ double sm[];
+// The factorisation on a grid of ngrid blocks, this one being block bid; gsync() is the
+// grid-wide barrier. The cooperative kernel runs it on its grid; a batched launch runs it
+// with one block per matrix (bid 0, ngrid 1, gsync a block barrier). Every tile is computed
+// by the same operations whatever the grid, so the result does not depend on it.
+template <class GSync>
+__device__ void potrf_body(double *L, long ld, int n, double *Dinv, long ldd, int *info, double *K, double *KT,
+                           int bid, int ngrid, GSync gsync, double *sm) {
     const int nblk = (n + 63) / 64;
-    if (blockIdx.x == 0) potf2_dev(L, ld, 0, min(NB, n), Dinv, ldd, info, sm);
-    grid.sync();
+    if (bid == 0) potf2_dev(L, ld, 0, min(NB, n), Dinv, ldd, info, sm);
+    gsync();
     for (int j0 = 0; j0 < n; j0 += NB) {
         if (*(volatile int *) info) return;
         const int nb = min(NB, n - j0);
@@ -551,17 +554,17 @@ __global__ void __launch_bounds__(COOP_THREADS, 1) potrf_coop_kernel(double *L, 
         const int bj = j0 / 64;
         double *P = L + (size_t) (j0 + nb) + (size_t) j0 * ld;
         const int nchunk = (rows + 63) / 64;
-        const int pb = (j0 / 64) * 16 + (blockIdx.x == 1 ? 8 : 0);
+        const int pb = (j0 / 64) * 16 + (bid == 1 ? 8 : 0);
         (void) pb;
-        if (blockIdx.x <= 1) CHOL_STAMP(pb + 0);
+        if (bid <= 1) CHOL_STAMP(pb + 0);
         // panel solve; with K, the update of K's rows r >= bj by block row bj - 1
         const long nx = (K && bj >= 1) ? (long) (nblk - bj) * bj : 0;
         // block 0 stages the next diagonal block now (its updates by earlier panels are
         // complete) and keeps its own solved chunk 0, the rows that update that block
         const int nbn = min(NB, rows);
-        if (blockIdx.x == 0)
+        if (bid == 0)
             stage_tile(region(sm, R_T), L + (size_t) (j0 + nb) + (size_t) (j0 + nb) * ld, ld, nbn, nbn, 64);
-        for (long t = blockIdx.x; t < nchunk + nx; t += gridDim.x) {
+        for (long t = bid; t < nchunk + nx; t += ngrid) {
             if (t < nchunk) {
                 const int ch = (int) t;
                 const int mr = min(64, rows - ch * 64);
@@ -572,13 +575,13 @@ __global__ void __launch_bounds__(COOP_THREADS, 1) potrf_coop_kernel(double *L, 
                 k_update_tile(L, ld, K, n, bj + (int) (u / bj), (int) (u % bj), bj - 1, sm);
             }
         }
-        if (blockIdx.x <= 1) CHOL_STAMP(pb + 1);
-        grid.sync();
-        if (blockIdx.x <= 1) CHOL_STAMP(pb + 2);
+        if (bid <= 1) CHOL_STAMP(pb + 1);
+        gsync();
+        if (bid <= 1) CHOL_STAMP(pb + 2);
         const long ntile = (long) nchunk * (nchunk + 1) / 2;
         const long nk = K ? bj + 1 : 0;
         double *A22 = L + (size_t) (j0 + nb) + (size_t) (j0 + nb) * ld;
-        if (blockIdx.x == 0) {
+        if (bid == 0) {
             // tile (0, 0) is the next diagonal block: update it in shared memory and factor it
             CHOL_STAMP(pb + 3);
             potf2_dev(L, ld, j0 + nb, nbn, Dinv, ldd, info, sm, nullptr, 0, true);
@@ -586,8 +589,8 @@ __global__ void __launch_bounds__(COOP_THREADS, 1) potrf_coop_kernel(double *L, 
         }
         // remaining tiles (and K's block row bj), spread over the other blocks
         // (block 0 joins when the grid has one block)
-        const int nworker = (gridDim.x > 1) ? (int) gridDim.x - 1 : 1;
-        const int wid = (gridDim.x > 1) ? (int) blockIdx.x - 1 : 0;
+        const int nworker = (ngrid > 1) ? (int) ngrid - 1 : 1;
+        const int wid = (ngrid > 1) ? (int) bid - 1 : 0;
         if (wid >= 0) {
             auto trailing = [&](long t, TileJob &J) {
                 int ti, tj;
@@ -600,24 +603,31 @@ __global__ void __launch_bounds__(COOP_THREADS, 1) potrf_coop_kernel(double *L, 
             for (long t = 1 + wid; t < ntile + nk; t += nworker)
                 if (t >= ntile) k_final_tile(Dinv, ldd, K, KT, ld, n, bj, (int) (t - ntile), sm);
         }
-        if (blockIdx.x == 1) CHOL_STAMP(pb + 3);
-        grid.sync();
-        if (blockIdx.x <= 1) CHOL_STAMP(pb + 5);
+        if (bid == 1) CHOL_STAMP(pb + 3);
+        gsync();
+        if (bid <= 1) CHOL_STAMP(pb + 5);
     }
     if (!K || *(volatile int *) info) return;
     // the last block row of K: its update by block row nblk - 2, then its final form
     const int bj = nblk - 1;
     if (bj >= 1) {
-        for (int c = blockIdx.x; c < bj; c += gridDim.x) k_update_tile(L, ld, K, n, bj, c, bj - 1, sm);
-        grid.sync();
+        for (int c = bid; c < bj; c += ngrid) k_update_tile(L, ld, K, n, bj, c, bj - 1, sm);
+        gsync();
     }
-    for (int c = blockIdx.x; c <= bj; c += gridDim.x) k_final_tile(Dinv, ldd, K, KT, ld, n, bj, c, sm);
+    for (int c = bid; c <= bj; c += ngrid) k_final_tile(Dinv, ldd, K, KT, ld, n, bj, c, sm);
 }
 
-// Several factorisations of order <= 64 in one launch, one CTA each: the copy of the lower
-// triangle, the diagonal-block factorisation and inverse (potf2_dev), K = L^-1 and K^T from
-// the inverse block, and sum log L_ii next to the info word, each as the cooperative
-// kernel and the log-diagonal kernel do them for a single 64-column panel.
+__global__ void __launch_bounds__(COOP_THREADS, 1) potrf_coop_kernel(double *L, long ld, int n, double *Dinv,
+                                                                  long ldd, int *info, double *K, double *KT) {
+    cg::grid_group grid = cg::this_grid();
+    extern __shared__ double sm[];
+    potrf_body(L, ld, n, Dinv, ldd, info, K, KT, (int) blockIdx.x, (int) gridDim.x, [&]() { grid.sync(); }, sm);
+}
+
+// Several factorisations in one launch, one CTA each: the copy of the lower triangle, the
+// factorisation of the cooperative kernel on a grid of one block (with K = L^-1 and K^T for
+// a fused factor), and sum log L_ii next to the info word as the log-diagonal kernel forms
+// it; the results are those of the cooperative kernel on any grid.
 struct SmallFactorJob {
     const double *S;
     double *L, *Dinv, *K, *KT;
@@ -631,21 +641,30 @@ struct SmallFactorBatch {
     SmallFactorJob job[kSmallBatch];
 };
 
-__device__ double small_block_sum(double v) {
+// sum_i log L_ii (n <= 1024) summed as the log-diagonal kernel sums it with its 1024
+// threads (one term per thread, a shuffle tree per warp, then one over the 32 warp sums),
+// by COOP_THREADS threads each standing in for four: the same additions in the same order.
+__device__ double logdiag_1024(int n, const double *L, long ld) {
     __shared__ double red[32];
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    constexpr int kV = 1024 / COOP_THREADS;
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    if (lane == 0) red[w] = v;
-    __syncthreads();
-    const int nw = (blockDim.x + 31) >> 5;
-    v = (threadIdx.x < nw) ? red[threadIdx.x] : 0.0;
-    if (w == 0) {
+    for (int q = 0; q < kV; ++q) {
+        const int v = t + COOP_THREADS * q;
+        double x = (v < n) ? log(L[(size_t) v + (size_t) v * ld]) : 0.0;
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        if (lane == 0) red[w + (COOP_THREADS / 32) * q] = x;
     }
     __syncthreads();
-    return v;
+    double x = 0.0;
+    if (w == 0) {
+        x = red[lane];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    }
+    __syncthreads();
+    return x;
 }
 
 __global__ void __launch_bounds__(COOP_THREADS, 1) potrf_small_batch_kernel(const SmallFactorBatch B) {
@@ -659,16 +678,13 @@ __global__ void __launch_bounds__(COOP_THREADS, 1) potrf_small_batch_kernel(cons
     if (threadIdx.x == 0) *J.info = 0;
     __threadfence_block();
     __syncthreads();
-    potf2_dev(J.L, J.ld, 0, n, J.Dinv, J.ld, J.info, sm);
+    potrf_body(J.L, J.ld, n, J.Dinv, J.ld, J.info, J.K, J.KT, 0, 1, []() { __syncthreads(); }, sm);
     __syncthreads();
-    const bool ok = (*(volatile int *) J.info == 0);
-    if (ok && J.K) k_final_tile(J.Dinv, J.ld, J.K, J.KT, J.ld, n, 0, 0, sm);
     double acc = 0.0;
     if (J.logdet) {
         __threadfence_block();
         __syncthreads();
-        for (int i = threadIdx.x; i < n; i += blockDim.x) acc += log(J.L[(size_t) i + (size_t) i * J.ld]);
-        acc = small_block_sum(acc);
+        acc = logdiag_1024(n, J.L, J.ld);
         if (threadIdx.x == 0) reinterpret_cast<double *>(J.info)[1] = acc;
     }
     if (threadIdx.x == 0) {
@@ -1002,7 +1018,7 @@ bool coop_factorize_enqueue(cudaStream_t s, DenseFactor &F, const double *S, lon
     return true;
 }
 
-// The factorisations of F[0..count) (each n <= 64) of S[i] (ldS[i]) in launches of up to
+// The factorisations of F[0..count) (each n <= kSmallFactorMaxN) of S[i] (ldS[i]) in launches of up to
 // kSmallBatch CTAs, the status words written into each factor's pinned host mirror by the
 // kernel; returns false (nothing enqueued) if a mirror has no device address, or false
 // after a failed launch.

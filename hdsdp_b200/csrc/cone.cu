@@ -533,7 +533,7 @@ bool SdpCone::factor_buffer(int which) {
 
 // factor_buffer in two phases, for several cones at once: factor_plan() settles what
 // factor_buffer would do without waiting for the device. FP_DONE: the result is known
-// (*ok); FP_SMALL: a dense factorisation of order <= kSmallFactorMaxN, to be enqueued by
+// (*ok); FP_SMALL: a dense factorisation of order <= kBatchFactorMaxN, to be enqueued by
 // the caller with the other cones' (factorize_small_batch); FP_ASYNC: enqueued here.
 // factor_finish() then reads the status of an FP_SMALL or FP_ASYNC factorisation.
 int SdpCone::factor_plan(int which, bool *ok) {
@@ -546,7 +546,7 @@ int SdpCone::factor_plan(int which, bool *ok) {
         *ok = factor_buffer(which);   // reuse, copy or the hybrid factorisation
         return FP_DONE;
     }
-    if (n <= kSmallFactorMaxN) return FP_SMALL;
+    if (n <= kBatchFactorMaxN) return FP_SMALL;
     factorize_async(s, var ? Fvar : Fcheck, var ? Svar : Scheck, ld);
     return FP_ASYNC;
 }

@@ -213,6 +213,57 @@ int hdsdpb_cholesky(int n, const double *S, double *L, double *logdiag) {
     return ok ? 0 : 1;
 }
 
+// count factorisations of order n (S: count column-major n x n matrices, host), either one
+// CTA per matrix in shared launches (mode 0, factorize_small_batch) or each on the whole
+// GPU (mode 1, the cooperative kernel). Out (each may be null): L and K = L^-1 (lower,
+// count x n x n), logdiag = sum log L_ii, status (0 positive definite, 1 not).
+int hdsdpb_cholesky_batch(int count, int n, int mode, const double *S, double *L, double *K, double *logdiag,
+                          int *status) {
+    if (count < 0 || n <= 0 || n > kSmallFactorMaxN || !S || (mode != 0 && mode != 1)) return -1;
+    if (count == 0) return 0;
+    cudaStream_t s;
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return -1;
+    const long ld = pad_ld(n);
+    std::vector<DenseFactor> F(count);
+    std::vector<DenseFactor *> Fp(count);
+    std::vector<const double *> Sp(count);
+    std::vector<long> lds(count, ld);
+    double *dS = nullptr;
+    hb::cmalloc(&dS, sizeof(double) * ld * n * count);
+    for (int q = 0; q < count; ++q) {
+        cudaMemcpy2D(dS + (size_t) q * ld * n, sizeof(double) * ld, S + (size_t) q * n * n, sizeof(double) * n,
+                     sizeof(double) * n, n, cudaMemcpyHostToDevice);
+        F[q].alloc(n, 1);
+        Fp[q] = &F[q];
+        Sp[q] = dS + (size_t) q * ld * n;
+    }
+    legacy_fence();
+    if (mode == 0) {
+        factorize_small_batch(s, Fp.data(), Sp.data(), lds.data(), count);
+    } else {
+        for (int q = 0; q < count; ++q) factorize_async(s, F[q], Sp[q], ld);
+    }
+    HB_CUDA(cudaStreamSynchronize(s));
+    std::vector<double> h((size_t) ld * n);
+    for (int q = 0; q < count; ++q) {
+        const bool ok = factor_status_ready(F[q]);
+        if (status) status[q] = ok ? 0 : 1;
+        if (logdiag) logdiag[q] = ok ? 0.5 * F[q].logdet : 0.0;
+        for (int which = 0; which < 2; ++which) {
+            double *out = which ? K : L;
+            if (!out) continue;
+            cudaMemcpy(h.data(), which ? F[q].K : F[q].L, sizeof(double) * ld * n, cudaMemcpyDeviceToHost);
+            double *o = out + (size_t) q * n * n;
+            for (int j = 0; j < n; ++j)
+                for (int i = 0; i < n; ++i) o[(size_t) j * n + i] = (ok && i >= j) ? h[(size_t) j * ld + i] : 0.0;
+        }
+        F[q].release();
+    }
+    hb::cache_free(dS);
+    cudaStreamDestroy(s);
+    return device_error_flag() ? -1 : 0;
+}
+
 // The sparse factorisation of S (column-major n x n, host; its pattern given by the
 // nedge off-diagonal pairs) with degree cap `cap`, timed over `reps` calls after one
 // warm-up call, and the dense cooperative factorisation of the same S timed the same

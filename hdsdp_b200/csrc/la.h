@@ -87,9 +87,14 @@ bool factorize(cudaStream_t s, DenseFactor &F, const double *S, long ldS);
 void factorize_async(cudaStream_t s, DenseFactor &F, const double *S, long ldS);
 bool factor_status(cudaStream_t s, DenseFactor &F);
 // Enqueue the factorisations of F[q] (order <= kSmallFactorMaxN) of S[q] (ldS[q]) for
-// q < count, one CTA each, in one launch per kSmallBatch of them: the arithmetic of
-// factorize_async for a single panel. Call factor_status() on each afterwards.
-constexpr int kSmallFactorMaxN = 64;
+// q < count, one CTA each, in launches of up to 36 of them: the arithmetic of
+// factorize_async on a grid of one block, which gives the same factor on any grid. Call
+// factor_status() (or factor_status_ready() after a wait) on each afterwards. Worth it for
+// several matrices of moderate order: one CTA takes about as long for order 256 as the
+// whole-GPU kernel, and many run at once.
+constexpr int kSmallFactorMaxN = 1024;
+// the order up to which factor_buffers batches the cones' dense factorisations
+constexpr int kBatchFactorMaxN = 256;
 void factorize_small_batch(cudaStream_t s, DenseFactor *const *F, const double *const *S, const long *ldS, int count);
 // factor_status() without its wait, for a caller that has synchronised the stream since
 // the factorisation was enqueued

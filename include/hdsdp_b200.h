@@ -147,6 +147,14 @@ extern int hdsdpb_ratio_probe( int m, int n, const int *Ap, const int *Ai, const
    upper part zero) and sum(log L_ii). Returns 0 if positive definite, 1 if not. */
 extern int hdsdpb_cholesky( int n, const double *S, double *L, double *logdiag );
 
+/* count factorisations of order n <= 1024 (S: count column-major n x n matrices): mode 0 one
+   CTA per matrix in shared launches (the multi-cone path), mode 1 each on the whole GPU (the
+   cooperative kernel). L and K = L^-1 (lower), logdiag = sum log L_ii and status (0 positive
+   definite, 1 not) per matrix; any output may be NULL. Returns 0, or -1 on bad arguments or a
+   CUDA error. */
+extern int hdsdpb_cholesky_batch( int count, int n, int mode, const double *S, double *L, double *K,
+                                  double *logdiag, int *status );
+
 /* Solution of S x = b through the Cholesky factor of S by blocked forward and backward
    substitution with L (the reference's dpotrs use, linalg/hdsdp_linsolver.c:607-633; the
    solver uses it for Schur systems of order >= 6000). Returns 0 on success, 1 if S is

@@ -124,3 +124,43 @@ def test_cholesky_solve_indefinite(gpu_lib):
     S = _spd(100, 5)
     S[50, 50] = -1.0
     assert api.cholesky_solve(S, np.ones(100)) is None
+
+
+@pytest.mark.parametrize("n", [1, 37, 64, 65, 100, 128, 200, 333, 512, 1000])
+def test_cholesky_batch_matches_whole_gpu_kernel(gpu_lib, n):
+    """The one-CTA-per-matrix factorisation of the multi-cone path (mode 0) gives the
+    cooperative whole-GPU kernel's L, K = L^-1, log det and status to the bit (mode 1), and
+    matches NumPy; the third matrix is indefinite."""
+    import ctypes as C
+    from hdsdp_b200 import _lib
+    L = _lib.load()
+    rng = np.random.default_rng(n)
+    mats = []
+    for q in range(3):
+        G = rng.standard_normal((n, n))
+        S = G @ G.T / n + np.eye(n)
+        if q == 2:
+            S[n // 2, n // 2] = -1.0 - np.abs(S[n // 2]).sum()
+        mats.append(S)
+    Sall = np.ascontiguousarray(np.stack([np.asfortranarray(S).ravel(order="F") for S in mats]))
+    out = {}
+    dp = C.POINTER(C.c_double)
+    for mode in (0, 1):
+        Lo, Ko = np.zeros((3, n * n)), np.zeros((3, n * n))
+        ld, st = np.zeros(3), np.zeros(3, dtype=np.int32)
+        r = L.hdsdpb_cholesky_batch(3, n, mode, Sall.ctypes.data_as(dp), Lo.ctypes.data_as(dp),
+                                    Ko.ctypes.data_as(dp), ld.ctypes.data_as(dp),
+                                    st.ctypes.data_as(C.POINTER(C.c_int)))
+        assert r == 0
+        out[mode] = (Lo, Ko, ld, st)
+    for a, b in zip(out[0], out[1]):
+        assert np.array_equal(a, b)
+    Lo, Ko, ld, st = out[0]
+    assert list(st) == [0, 0, 1]
+    for q in range(2):
+        Lq = Lo[q].reshape(n, n, order="F")
+        Kq = Ko[q].reshape(n, n, order="F")
+        Lr = np.linalg.cholesky(mats[q])
+        assert np.abs(Lq - Lr).max() <= 1e-12 * max(1.0, np.abs(Lr).max())
+        assert np.abs(Kq @ Lq - np.eye(n)).max() <= 1e-10
+        assert ld[q] == pytest.approx(np.log(np.diag(Lr)).sum(), rel=1e-12, abs=1e-12)
