@@ -143,9 +143,10 @@ class Solver:
         self.L.HDSDPSetSparseSchur(self.h, int(mode))
 
     def sparse_schur_info(self) -> dict:
-        o = np.zeros(4)
+        o = np.zeros(6)
         self.L.HDSDPGetSparseSchurInfo(self.h, _dp(o))
-        return {"arrow": bool(o[0]), "coupling": int(o[1]), "cones": int(o[2]), "max_local": int(o[3])}
+        return {"arrow": bool(o[0]), "coupling": int(o[1]), "cones": int(o[2]), "max_local": int(o[3]),
+                "arrow_bytes": float(o[4]), "dense_bytes": float(o[5])}
 
     def optimize(self, d_only: int = 0) -> int:
         return self.L.HDSDPOptimize(self.h, int(d_only))

@@ -57,6 +57,7 @@ struct ArrowSchur {
     int maxl = 0, gsplit = 1;         // largest local block; column splits of the gemv
     double *U = nullptr;              // nc x (nopsB * gsplit) partial sums of the gemv
     long ldu = 0;
+    double bytes = 0.0;               // device memory of the blocks, their factors and scratch
 };
 
 namespace {
@@ -403,6 +404,19 @@ bool KKT::setup_arrow(const std::vector<SdpCone *> &cones) {
         }
     }
     HB_CUDA(cudaStreamSynchronize(s));
+    {
+        // device memory held: local blocks, their factors (L, K, K^T, diagonal-block inverses),
+        // B_k and W_k, the coupling block, its copy and factor, the solve's vectors and scratch
+        double b = 0.0;
+        for (int k = 0; k < A->ncone; ++k) {
+            const double l = A->lk[k], ldk = A->ldk[k];
+            if (l == 0) continue;
+            b += ldk * l * 4 + ldk * 64 + 2.0 * A->ldb * l;
+        }
+        if (A->nc > 0) b += 4.0 * A->ldc * A->nc + A->ldc * 64;
+        b += 6.0 * m + A->ldu * (double) A->nopsB * A->gsplit;
+        A->bytes = 8.0 * b;
+    }
     arrow = A;
     mOpen = false;
     return !device_error_flag();
@@ -513,9 +527,13 @@ bool KKT::arrow_solve(const double *rhs, double *lhs) {
     return ok;
 }
 
-void KKT::arrow_info(double out[4]) const {
+void KKT::arrow_info(double out[6]) const {
+    // the dense M and its factor (L and the diagonal-block inverses; K and K^T below
+    // kTriSolveMinM) for comparison
+    const double ld = (double) pad_ld(m);
+    out[5] = 8.0 * (ld * m * (m < kTriSolveMinM ? 4.0 : 2.0) + ld * 64);
     if (!arrow) {
-        out[0] = out[1] = out[2] = out[3] = 0.0;
+        out[0] = out[1] = out[2] = out[3] = out[4] = 0.0;
         return;
     }
     out[0] = 1.0;
@@ -524,6 +542,7 @@ void KKT::arrow_info(double out[4]) const {
     int mx = 0;
     for (int l : arrow->lk) mx = std::max(mx, l);
     out[3] = mx;
+    out[4] = arrow->bytes;
 }
 
 }  // namespace hb

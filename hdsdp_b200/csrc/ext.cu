@@ -18,7 +18,7 @@ void HDSDPSetPrimalRefinement(hdsdp *h, int on) { h->HIntParams[INT_PARAM_PSDP] 
 void HDSDPSetPrecision(hdsdp *h, int mode) { h->precision = mode; }
 void HDSDPSetSparseSlack(hdsdp *h, int mode) { h->sparseSlack = mode; }
 void HDSDPSetSparseSchur(hdsdp *h, int mode) { h->sparseSchur = mode; }
-void HDSDPGetSparseSchurInfo(hdsdp *h, double out[4]) { h->kkt.arrow_info(out); }
+void HDSDPGetSparseSchurInfo(hdsdp *h, double out[6]) { h->kkt.arrow_info(out); }
 
 // Host only (no device work): the ordering of the sparse factorisation of S for the
 // pattern of nedge off-diagonal pairs (ei[k], ej[k]) with degree cap `cap`.

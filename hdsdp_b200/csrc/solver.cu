@@ -1792,7 +1792,7 @@ hdsdp_retcode HDSDPOptimize(hdsdp *h, int dOptOnly) {
             goto exit_cleanup;
         }
         if (h->verbose && useArrow) {
-            double info[4];
+            double info[6];
             h->kkt.arrow_info(info);
             printf("  Schur complement: block arrow, %d cones (largest local block %d), %d coupling rows\n",
                    (int) info[2], (int) info[3], (int) info[1]);

@@ -293,8 +293,9 @@ struct KKT {
     void arrow_regularize(double reg);
     bool arrow_factorize();
     bool arrow_solve(const double *rhs, double *lhs);
-    // {engaged, coupling rows, cones, largest local block}
-    void arrow_info(double out[4]) const;
+    // {engaged, coupling rows, cones, largest local block, device bytes of the block arrow,
+    // device bytes the dense M and its factor take}
+    void arrow_info(double out[6]) const;
     void clean(int type);
     void open_m();
     hdsdp_retcode add_sdp(SdpCone &cone, int type);

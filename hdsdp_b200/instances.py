@@ -443,8 +443,20 @@ MULTIBLOCK_CASES = {
 }
 
 
+# Multi-block problems too large for the compiled reference (its sparse KKT goes through a
+# dense stand-in here) and for a dense Schur matrix on one GPU: 250 sparse cones of order 90
+# with 450 constraints each and 100 shared ones, m = 112,600, whose dense M and factor would
+# take 203 GB. The block arrow holds 250 blocks of 450 rows and 100 coupling rows.
+LARGE_ARROW_CASES = {
+    "mb250_m112k": dict(dims=[90] * 250, m_local=[450] * 250, m_couple=100, seed=17),
+    # the same family at 60 cones (m = 27,100), small enough for a dense M as well
+    "mb60_m27k": dict(dims=[90] * 60, m_local=[450] * 60, m_couple=100, seed=18),
+}
+
+
 def multiblock_case(name: str) -> ConicProblem:
-    return multiblock(name=name, **MULTIBLOCK_CASES[name])
+    spec = MULTIBLOCK_CASES.get(name) or LARGE_ARROW_CASES[name]
+    return multiblock(name=name, **spec)
 
 
 WORKLOADS = {

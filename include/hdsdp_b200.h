@@ -59,8 +59,10 @@ extern void HDSDPGetSparseSlackInfo( hdsdp *HSolver, double out[8] );
 extern void HDSDPSetSparseSchur( hdsdp *HSolver, int mode );
 
 /* out[0] = 1 if the last solve used the block arrow, out[1] = coupling rows, out[2] =
-   cones, out[3] = the largest cone's local rows. */
-extern void HDSDPGetSparseSchurInfo( hdsdp *HSolver, double out[4] );
+   cones, out[3] = the largest cone's local rows, out[4] = device bytes the block arrow
+   holds (blocks, factors, coupling block, scratch), out[5] = device bytes the dense M and
+   its factor would take. */
+extern void HDSDPGetSparseSchurInfo( hdsdp *HSolver, double out[6] );
 
 /* Per-iteration record of the last solve: elapsed seconds, primal and dual
    objective, barrier parameter, relative gap (p - d) / (1 + |p| + |d|) and
