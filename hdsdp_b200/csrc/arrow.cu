@@ -39,7 +39,10 @@ struct ArrowSchur {
     std::vector<int> perm;            // packed index -> problem row
     std::vector<const SdpCone *> cone;
     std::vector<int *> d_code;        // per cone, per row of its list: local index, or -(coupling index + 1)
-    std::vector<double *> Mkk, Bk, Wk;
+    std::vector<double *> Mkk, Bk, Wk;   // Bk / Wk: column blocks of Ball / Wall
+    double *Ball = nullptr, *Wall = nullptr;   // n_c x sum l_k: [B_1 ... B_K], [W_1 ... W_K]
+    GemmDesc *wdesc = nullptr;        // W_k = B_k K_k^T for the blocks with local rows
+    int nw = 0;
     std::vector<long> ldk;
     std::vector<DenseFactor> Fk;
     double *Mcc = nullptr, *Mcf = nullptr;
@@ -86,8 +89,9 @@ void zero_blocks(cudaStream_t s, ArrowSchur &A) {
     for (int k = 0; k < A.ncone; ++k) {
         if (A.lk[k] == 0) continue;
         HB_CUDA(cudaMemsetAsync(A.Mkk[k], 0, sizeof(double) * A.ldk[k] * A.lk[k], s));
-        if (A.nc > 0) HB_CUDA(cudaMemsetAsync(A.Bk[k], 0, sizeof(double) * A.ldb * A.lk[k], s));
     }
+    if (A.nc > 0 && A.off[A.ncone] > 0)
+        HB_CUDA(cudaMemsetAsync(A.Ball, 0, sizeof(double) * A.ldb * A.off[A.ncone], s));
     if (A.nc > 0) HB_CUDA(cudaMemsetAsync(A.Mcc, 0, sizeof(double) * A.ldc * A.nc, s));
 }
 
@@ -251,18 +255,15 @@ bool arrow_factor_once(cudaStream_t s, ArrowSchur &A) {
     for (int k = 0; k < K; ++k)
         if (A.lk[k] > 0 && !factor_status_ready(A.Fk[k])) ok = false;
     if (!ok) return false;
-    for (int k = 0; k < K; ++k) {
-        const int l = A.lk[k];
-        if (l == 0) continue;
-        compute_inverse_factor(s, A.Fk[k]);   // formed by the factorisation kernel already
-        if (nc > 0)   // W_k = B_k L_kk^-T = B_k K_k^T
-            gemm(s, nc, l, l, 1.0, A.Bk[k], A.ldb, 0, A.Fk[k].K, A.Fk[k].ld, 1, 0.0, A.Wk[k], A.ldb, GEMM_B_UPPER);
-    }
-    if (nc == 0) return true;
-    copy_matrix(s, nc, nc, A.Mcc, A.ldc, A.Mcf, A.ldc);
     for (int k = 0; k < K; ++k)
-        if (A.lk[k] > 0)
-            gemm(s, nc, nc, A.lk[k], -1.0, A.Wk[k], A.ldb, 0, A.Wk[k], A.ldb, 1, 1.0, A.Mcf, A.ldc, GEMM_C_LOWER);
+        if (A.lk[k] > 0) compute_inverse_factor(s, A.Fk[k]);   // formed by the factorisation kernel already
+    if (nc == 0) return true;
+    // W_k = B_k L_kk^-T = B_k K_k^T for every block in one launch, then
+    // M_cc - sum_k W_k W_k^T = M_cc - Wall Wall^T as one product
+    gemm_grouped(s, A.wdesc, A.nw, nc, A.maxl);
+    copy_matrix(s, nc, nc, A.Mcc, A.ldc, A.Mcf, A.ldc);
+    if (A.off[K] > 0)
+        gemm(s, nc, nc, A.off[K], -1.0, A.Wall, A.ldb, 0, A.Wall, A.ldb, 1, 1.0, A.Mcf, A.ldc, GEMM_C_LOWER);
     if (!hb::factorize(s, A.Fc, A.Mcf, A.ldc)) return false;
     if (A.Fc.fuse_k) compute_inverse_factor(s, A.Fc);
     return true;
@@ -349,10 +350,23 @@ bool KKT::setup_arrow(const std::vector<SdpCone *> &cones) {
         HB_CUDA(cmalloc(&A->Mkk[k], sizeof(double) * A->ldk[k] * l));
         A->Fk[k].alloc(l, 1);
         A->Fk[k].kfamily = KF_POTRF_SCHUR;
-        if (A->nc > 0) {
-            HB_CUDA(cmalloc(&A->Bk[k], sizeof(double) * A->ldb * l));
-            HB_CUDA(cmalloc(&A->Wk[k], sizeof(double) * A->ldb * l));
+    }
+    if (A->nc > 0 && A->off[A->ncone] > 0) {
+        const size_t cols = (size_t) A->off[A->ncone];
+        HB_CUDA(cmalloc(&A->Ball, sizeof(double) * A->ldb * cols));
+        HB_CUDA(cmalloc(&A->Wall, sizeof(double) * A->ldb * cols));
+        std::vector<GemmDesc> wd;
+        for (int k = 0; k < A->ncone; ++k) {
+            const int l = A->lk[k];
+            if (l == 0) continue;
+            A->Bk[k] = A->Ball + (size_t) A->off[k] * A->ldb;
+            A->Wk[k] = A->Wall + (size_t) A->off[k] * A->ldb;
+            wd.push_back(GemmDesc{A->nc, l, l, 1.0, 0.0, A->Bk[k], A->ldb, 0, A->Fk[k].K, A->Fk[k].ld, 1, A->Wk[k],
+                                  A->ldb, GEMM_B_UPPER, nullptr});
         }
+        A->nw = (int) wd.size();
+        HB_CUDA(cmalloc(&A->wdesc, sizeof(GemmDesc) * wd.size()));
+        HB_CUDA(cudaMemcpyAsync(A->wdesc, wd.data(), sizeof(GemmDesc) * wd.size(), cudaMemcpyHostToDevice, s));
     }
     if (A->nc > 0) {
         HB_CUDA(cmalloc(&A->Mcc, sizeof(double) * A->ldc * A->nc));
@@ -428,11 +442,12 @@ void KKT::release_arrow() {
     auto f = [](void *p) { if (p) cache_free(p); };
     for (int k = 0; k < A.ncone; ++k) {
         f(A.Mkk[k]);
-        f(A.Bk[k]);
-        f(A.Wk[k]);
         f(A.d_code[k]);
         A.Fk[k].release();
     }
+    f(A.Ball);
+    f(A.Wall);
+    f(A.wdesc);
     f(A.Mcc);
     f(A.Mcf);
     A.Fc.release();

@@ -248,20 +248,7 @@ int kstat_read(int family, long long *launches, double *ms, double *work) {
 namespace {
 constexpr int BM = 64, BN = 64, BK = 16, GT = 128;
 
-struct GemmP {
-    int M, N, K;
-    double alpha, beta;
-    const double *A;
-    long lda;
-    int ta;
-    const double *B;
-    long ldb;
-    int tb;
-    double *C;
-    long ldc;
-    int flags;
-    const int *abort_flag;
-};
+using GemmP = GemmDesc;
 
 __device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b) {
     asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
@@ -283,9 +270,10 @@ __device__ __forceinline__ double load_b(const GemmP &p, int k, int n) {
     return p.tb ? p.B[(size_t) n + (size_t) k * p.ldb] : p.B[(size_t) k + (size_t) n * p.ldb];
 }
 
-__global__ void __launch_bounds__(GT) gemm_kernel(GemmP p) {
-    const int m0 = blockIdx.x * BM;
-    const int n0 = blockIdx.y * BN;
+// one 64 x 64 tile (bx, by) of C
+__device__ __forceinline__ void gemm_tile(const GemmP &p, int bx, int by) {
+    const int m0 = bx * BM;
+    const int n0 = by * BN;
     if ((p.flags & GEMM_C_LOWER) && m0 + BM - 1 < n0) return;
     if (p.abort_flag && *p.abort_flag) return;
 
@@ -384,7 +372,25 @@ __global__ void __launch_bounds__(GT) gemm_kernel(GemmP p) {
         }
     }
 }
+
+__global__ void __launch_bounds__(GT) gemm_kernel(GemmP p) { gemm_tile(p, blockIdx.x, blockIdx.y); }
+
+// one GEMM of a group per blockIdx.z (tiles beyond its own M x N exit)
+__global__ void __launch_bounds__(GT) gemm_grouped_kernel(const GemmP *__restrict__ ps) {
+    const GemmP p = ps[blockIdx.z];
+    if ((int) blockIdx.x * BM >= p.M || (int) blockIdx.y * BN >= p.N) return;
+    gemm_tile(p, blockIdx.x, blockIdx.y);
+}
 }  // namespace
+
+void gemm_grouped(cudaStream_t s, const GemmDesc *d_desc, int count, int maxM, int maxN) {
+    if (count <= 0 || maxM <= 0 || maxN <= 0) return;
+    for (int z0 = 0; z0 < count; z0 += 65535) {
+        dim3 grid((maxM + BM - 1) / BM, (maxN + BN - 1) / BN, std::min(65535, count - z0));
+        gemm_grouped_kernel<<<hb::counted(grid), GT, 0, s>>>(d_desc + z0);
+        HB_CUDA(cudaGetLastError());
+    }
+}
 
 // ------------------------------------------------------------------------------------
 // Large-tile GEMM: 128 x 128 x 16 CTA tile, 8 warps (4 along M x 2 along N), warp tile

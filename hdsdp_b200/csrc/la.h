@@ -25,6 +25,25 @@ void gemm(cudaStream_t s, int M, int N, int K, double alpha, const double *A, lo
           const double *B, long ldb, int transB, double beta, double *C, long ldc, int flags = 0,
           const int *abort_flag = nullptr);
 
+// One GEMM of a group: C = alpha * op(A) * op(B) + beta * C with the flags above.
+struct GemmDesc {
+    int M, N, K;
+    double alpha, beta;
+    const double *A;
+    long lda;
+    int ta;
+    const double *B;
+    long ldb;
+    int tb;
+    double *C;
+    long ldc;
+    int flags;
+    const int *abort_flag;
+};
+// A group of independent GEMMs (device array of descriptors, none larger than maxM x maxN)
+// in one launch on the 64 x 64 DMMA tiles.
+void gemm_grouped(cudaStream_t s, const GemmDesc *d_desc, int count, int maxM, int maxN);
+
 // Column-dot matrix-vector product:
 //   out[i] = alpha * sum_{k in R(i)} A[k + i*lda] * x[k] + beta * out[i],  i < ncols
 // with R(i) = [0, nrows) (mode 0), [i, nrows) (mode 1), [0, i] (mode 2).
