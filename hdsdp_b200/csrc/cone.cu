@@ -1791,6 +1791,7 @@ struct LzRitzJob {
     int n, kp1;
 };
 constexpr int kLzBatch = 32;
+constexpr int kLzHostParallel = 8;   // cones from which the host replays run on several threads
 struct LzStepBatch {
     LzStepJob job[kLzBatch];
 };
@@ -2134,6 +2135,7 @@ struct LzRun {
     LzTask *t;
     int k = 0, lastChecked = -1;
     bool done = false;
+    double host_s = 0.0;   // seconds of host eigensolves (summed into the timers afterwards)
     // the Ritz evaluation asked for
     int kc = 0;
     double eigMin1 = 0, eigMin2 = 0, betak = 0;
@@ -2164,7 +2166,7 @@ bool lz_advance(LzRun &R) {
         std::vector<double> dd(L.h_ab, L.h_ab + kp1), ee(L.h_ab + maxdim, L.h_ab + maxdim + kp1);
         ee[kp1 - 1] = 0.0;
         tridiag_eig(kp1, dd, ee, R.ev, R.evec);
-        if (R.t->tm) R.t->tm->lz_host += wall() - th;
+        R.host_s += wall() - th;
         int i1 = 0, i2 = 0;
         for (int i = 1; i < kp1; ++i)
             if (R.ev[i] > R.ev[i1]) i1 = i;
@@ -2278,12 +2280,19 @@ void lanczos_small_batch(std::vector<LzTask> &tasks) {
         if (tm) tm->n_lanczos_mv += L.maxdim;
     }
     HB_CUDA(cudaStreamSynchronize(s));
+    // the host replays of the cones are independent: with many cones they run on several
+    // host threads (each cone's own steps stay in order, so every value is the same)
     std::vector<LzRun> runs(tasks.size());
     std::vector<LzRun *> want;
-    for (size_t q = 0; q < tasks.size(); ++q) {
-        runs[q].t = &tasks[q];
-        if (lz_advance(runs[q])) want.push_back(&runs[q]);
-    }
+    const int nrun = (int) runs.size();
+    std::vector<char> ask(nrun, 0);
+    for (int q = 0; q < nrun; ++q) runs[q].t = &tasks[q];
+    const bool par0 = nrun >= kLzHostParallel;
+    (void) par0;
+#pragma omp parallel for schedule(dynamic, 1) if (par0)
+    for (int q = 0; q < nrun; ++q) ask[q] = lz_advance(runs[q]) ? 1 : 0;
+    for (int q = 0; q < nrun; ++q)
+        if (ask[q]) want.push_back(&runs[q]);
     while (!want.empty()) {
         for (size_t b0 = 0; b0 < want.size(); b0 += kLzBatch) {
             const int nb = (int) std::min<size_t>(kLzBatch, want.size() - b0);
@@ -2304,16 +2313,24 @@ void lanczos_small_batch(std::vector<LzTask> &tasks) {
             if (tm) tm->n_lanczos_mv += 2;
         }
         HB_CUDA(cudaStreamSynchronize(s));
-        std::vector<LzRun *> next;
-        for (LzRun *R : want) {
-            lz_ritz_done(*R);
-            if (lz_advance(*R)) next.push_back(R);
+        const int nw = (int) want.size();
+        std::vector<char> again(nw, 0);
+        const bool par = nw >= kLzHostParallel;
+        (void) par;
+#pragma omp parallel for schedule(dynamic, 1) if (par)
+        for (int q = 0; q < nw; ++q) {
+            lz_ritz_done(*want[q]);
+            again[q] = lz_advance(*want[q]) ? 1 : 0;
         }
+        std::vector<LzRun *> next;
+        for (int q = 0; q < nw; ++q)
+            if (again[q]) next.push_back(want[q]);
         want.swap(next);
     }
     for (LzTask &t : tasks)
         if (t.ret == HDSDP_RETCODE_OK) t.lz->nComputed += 1;
     if (tm) {
+        for (const LzRun &R : runs) tm->lz_host += R.host_s;
         tm->lanczos += wall() - t0;
         tm->n_lanczos += (long) tasks.size();
     }
