@@ -8,7 +8,9 @@ the existing fixtures: "north_star" (MaxCut n=8000 and the theta layer n=200,
 primal refinement off; a few minutes), "stock" (the sparse-dual instances on
 the reference build with its own dual-storage rule), "hsd" (instances that end
 in the homogeneous self-dual embedding), "dense" (general dense coefficients),
-"multiblock" (multi-cone cases missing from the fixtures).
+"multiblock" (multi-cone cases missing from the fixtures), "large" (the 60-cone
+m = 27,100 block-arrow case; about half an hour on 8 cores, most of it the reference's
+dense stand-in for its sparse KKT factorisation).
 
 Writes tests/golden/golden.json (solver results and probe outputs) and
 tests/golden/golden_arrays.npz (Schur matrices, dual vectors). The inputs are
@@ -148,6 +150,22 @@ def add_groups(groups):
                 }
                 arrays["y/" + name] = r["y"]
                 print("multiblock", name, r["iters"], r["status_after_check"], r["pobj"], r["dobj"], flush=True)
+        elif g == "large":
+            # the large block-arrow case that the reference can still solve here (its sparse KKT
+            # through the dense stand-in: a 5.9 GB M and a dense factorisation per iteration)
+            out.setdefault("multiblock_solves", {})
+            for name in ("mb60_m27k",):
+                if name in out["multiblock_solves"]:
+                    continue
+                prob = instances.multiblock_case(name)
+                r = ref_api.solve_problem(prob)
+                out["multiblock_solves"][name] = {
+                    "m": prob.m, "cones": [[c[0], int(c[1])] for c in prob.cones], "retcode": r["retcode"],
+                    "iters": r["iters"], "status": r["status_after_check"], "pobj": r["pobj"], "dobj": r["dobj"],
+                    "errs": [float(e) for e in r["errs"]],
+                }
+                arrays["y/" + name] = r["y"]
+                print("large", name, r["iters"], r["status_after_check"], r["pobj"], r["dobj"], flush=True)
         elif g == "dense":
             out.setdefault("dense_solves", {})
             for name, make in DENSE.items():
