@@ -83,3 +83,23 @@ def test_arrow_where_the_dense_schur_matrix_cannot_fit(gpu_lib):
     assert r["status_after_check"] == 3
     assert max(abs(e) for e in r["errs"]) < 1e-7
     assert abs(r["pobj"] - r["dobj"]) <= 1e-7 * (1 + abs(r["pobj"]) + abs(r["dobj"]))
+
+
+@pytest.mark.slow
+def test_arrow_27k_rows_where_the_reference_stops(gpu_lib, golden):
+    """60 sparse cones of order 90, m = 27,100. Near the optimum the Schur matrix turns
+    numerically indefinite: the compiled reference, which factors its sparse KKT as positive
+    definite (Pardiso matrix type 2, linalg/hdsdp_linsolver.c:60), stops with
+    HDSDP_NUMERICAL after 26 iterations at a 3 % gap. This library retries such a
+    factorisation with a diagonal shift on the block arrow as on the dense M, and ends
+    optimal; the reference's last dual and primal objectives bracket the optimum found."""
+    ref = golden["multiblock_solves"]["mb60_m27k"]
+    assert ref["status"] == 10 and ref["iters"] == 26
+    prob = instances.multiblock_case("mb60_m27k")
+    r = api.solve_problem(prob)
+    info = r["sparse_schur"]
+    assert info["arrow"] and info["cones"] == 60 and info["coupling"] == 100
+    assert r["status_after_check"] == 3
+    assert max(abs(e) for e in r["errs"]) < 1e-7
+    assert ref["dobj"] <= r["dobj"] + 1e-6 * abs(r["dobj"])
+    assert r["pobj"] <= ref["pobj"] + 1e-6 * abs(r["pobj"])

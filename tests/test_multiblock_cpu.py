@@ -107,3 +107,14 @@ def test_cone_choice_at_the_threshold(m, nz):
     a = _choose(ours, "sdp", m, n, Ap, Ai, Ax)
     assert a == _choose(ref, "sdp", m, n, Ap, Ai, Ax)
     assert a == (DENSE_SDP if nz > 0.3 * m else SPARSE_SDP)
+
+
+def test_reference_stops_on_the_27k_row_arrow_case(golden):
+    """The compiled reference's record of mb60_m27k (instances.LARGE_ARROW_CASES): it ends
+    HDSDP_NUMERICAL after 26 iterations (its positive-definite sparse KKT factorisation fails
+    near the optimum), with its dual objective below its primal bound."""
+    g = golden["multiblock_solves"]["mb60_m27k"]
+    prob = instances.multiblock_case("mb60_m27k")
+    assert g["m"] == prob.m == 27100 and len(g["cones"]) == 60
+    assert g["status"] == 10 and g["iters"] == 26
+    assert g["dobj"] < g["pobj"]
