@@ -438,28 +438,123 @@ void SdpCone::release() {
 
 // target = dC*C + dAs*sum_i y_i A_i + (dEye [+ perturbation])*I
 // (sdpDenseConeIUpdateBuffer, interface/hdsdp_conic_sdp.c:343-402)
+// The host part: the buffer `which` (*target) is to hold dC*C + dAs*sum y_i A_i + dEye*I,
+// dEye with the cone's perturbation for the slack buffers; false when it holds that already.
+// *ly: the cone's coefficient vector (y itself for a dense cone).
+bool SdpCone::buffer_plan(double dC, double dAs, const double *y, double &dEye, int which, double **target,
+                          const double **ly) {
+    y = local(y);
+    *ly = y;
+    *target = (which == BUFFER_DUALVAR) ? Svar : (which == BUFFER_DUALCHECK) ? Scheck : dS;
+    if (which == BUFFER_DUALSTEP) return true;
+    dEye += dualPerturb;
+    SlackSig &sig = (which == BUFFER_DUALVAR) ? sigVar : sigCheck;
+    SlackSig next;
+    next.valid = true;
+    next.dC = dC;
+    next.dAs = dAs;
+    next.dEye = dEye;
+    next.y.assign(y, y + m);
+    if (sig.same(next)) return false;  // the buffer already holds exactly this matrix
+    sig = std::move(next);
+    return true;
+}
+
 void SdpCone::update_buffer(double dC, double dAs, const double *y, double dEye, int which) {
     double t0 = wall();
-    y = local(y);
-    double *target = (which == BUFFER_DUALVAR) ? Svar : (which == BUFFER_DUALCHECK) ? Scheck : dS;
-    if (which != BUFFER_DUALSTEP) dEye += dualPerturb;
-    if (which != BUFFER_DUALSTEP) {
-        SlackSig &sig = (which == BUFFER_DUALVAR) ? sigVar : sigCheck;
-        SlackSig next;
-        next.valid = true;
-        next.dC = dC;
-        next.dAs = dAs;
-        next.dEye = dEye;
-        next.y.assign(y, y + m);
-        if (sig.same(next)) {
-            if (tm) tm->assemble += wall() - t0;
-            return;  // the buffer already holds exactly this matrix
-        }
-        sig = std::move(next);
+    double *target = nullptr;
+    const double *ly = nullptr;
+    if (buffer_plan(dC, dAs, y, dEye, which, &target, &ly)) {
+        std::memcpy(h_vec, ly, sizeof(double) * m);
+        HB_CUDA(cudaMemcpyAsync(d_y, h_vec, sizeof(double) * m, cudaMemcpyHostToDevice, s));
+        dev.assemble(dC, dAs, d_y, dEye, target, ld);
     }
-    std::memcpy(h_vec, y, sizeof(double) * m);
-    HB_CUDA(cudaMemcpyAsync(d_y, h_vec, sizeof(double) * m, cudaMemcpyHostToDevice, s));
-    dev.assemble(dC, dAs, d_y, dEye, target, ld);
+    if (tm) tm->assemble += wall() - t0;
+}
+
+namespace {
+// S assembly of several small cones whose coefficients all sit in the gather map (no dense
+// rank-one or dense class), one CTA each: s_init_kernel's and s_gather_kernel's arithmetic
+// in one launch, the coefficients read from the problem's vector through the cone's rows.
+struct AsmJob {
+    const double *C;
+    double *S;
+    const int *pr, *pc, *ptr, *ej, *rows;
+    const double *ev;
+    long ldc, lds;
+    double dEye;
+    int n, npos;
+};
+constexpr int kAsmBatch = 32;
+constexpr int kAsmBatchMaxN = 128;
+struct AsmBatch {
+    AsmJob job[kAsmBatch];
+};
+
+__global__ void s_assemble_batch_kernel(const AsmBatch B, const double *__restrict__ y, double dC, double dA) {
+    const AsmJob &J = B.job[blockIdx.x];
+    const int n = J.n;
+    const long total = (long) n * n;
+    for (long idx = threadIdx.x; idx < total; idx += blockDim.x) {
+        const int r = (int) (idx % n), c = (int) (idx / n);
+        double v = (dC != 0.0) ? dC * J.C[(size_t) r + (size_t) c * J.ldc] : 0.0;
+        if (r == c) v += J.dEye;
+        J.S[(size_t) r + (size_t) c * J.lds] = v;
+    }
+    if (dA == 0.0) return;
+    __syncthreads();
+    for (int p = threadIdx.x; p < J.npos; p += blockDim.x) {
+        double acc = 0.0;
+        for (int e = J.ptr[p]; e < J.ptr[p + 1]; ++e) {
+            const int j = J.ej[e];
+            acc += J.ev[e] * y[J.rows ? J.rows[j] : j];
+        }
+        acc *= dA;
+        const int r = J.pr[p], c = J.pc[p];
+        J.S[(size_t) r + (size_t) c * J.lds] += acc;
+        if (r != c) J.S[(size_t) c + (size_t) r * J.lds] += acc;
+    }
+}
+}  // namespace
+
+// update_buffer for several cones (one stream): one upload of y (problem order, mAll) into
+// d_yall (device, pinned staging h_yall), the small gather-map cones assembled in shared
+// launches, the others one by one; every buffer gets the values update_buffer gives it.
+void assemble_buffers(const std::vector<SdpCone *> &cones, double dC, double dAs, const double *y,
+                      const std::vector<double> &dEye, int which, double *d_yall, double *h_yall) {
+    if (cones.empty()) return;
+    const double t0 = wall();
+    cudaStream_t s = cones[0]->s;
+    Timers *tm = cones[0]->tm;
+    std::vector<AsmJob> jobs;
+    bool uploaded = false;
+    for (size_t q = 0; q < cones.size(); ++q) {
+        SdpCone *c = cones[q];
+        double e = dEye[q], *target = nullptr;
+        const double *ly = nullptr;
+        if (!c->buffer_plan(dC, dAs, y, e, which, &target, &ly)) continue;
+        const SdpDevice &d = c->dev;
+        if (c->n <= kAsmBatchMaxN && (dAs == 0.0 || (d.nr1d == 0 && d.ndr == 0))) {
+            if (!uploaded) {
+                std::memcpy(h_yall, y, sizeof(double) * c->mAll);
+                HB_CUDA(cudaMemcpyAsync(d_yall, h_yall, sizeof(double) * c->mAll, cudaMemcpyHostToDevice, s));
+                uploaded = true;
+            }
+            jobs.push_back(AsmJob{d.Cfull, target, d.pos_r, d.pos_c, d.pos_ptr, d.ent_j, c->sparse ? c->d_rows : nullptr,
+                                  d.ent_v, d.ld, c->ld, e, c->n, d.npos});
+        } else {
+            std::memcpy(c->h_vec, ly, sizeof(double) * c->m);
+            HB_CUDA(cudaMemcpyAsync(c->d_y, c->h_vec, sizeof(double) * c->m, cudaMemcpyHostToDevice, s));
+            c->dev.assemble(dC, dAs, c->d_y, e, target, c->ld);
+        }
+    }
+    for (size_t b0 = 0; b0 < jobs.size(); b0 += kAsmBatch) {
+        const int nb = (int) std::min<size_t>(kAsmBatch, jobs.size() - b0);
+        AsmBatch B;
+        for (int q = 0; q < nb; ++q) B.job[q] = jobs[b0 + q];
+        s_assemble_batch_kernel<<<counted(nb), 256, 0, s>>>(B, d_yall, dC, dAs);
+        HB_CUDA(cudaGetLastError());
+    }
     if (tm) tm->assemble += wall() - t0;
 }
 

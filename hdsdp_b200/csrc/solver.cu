@@ -366,6 +366,13 @@ static std::vector<SdpCone *> sdp_cones(hdsdp *h) {
     return v;
 }
 
+// SdpCone::update(tau, y) of every cone of sc, batched
+static void update_cones(hdsdp *h, const std::vector<SdpCone *> &sc, double tau, const double *y) {
+    std::vector<double> eye;
+    for (SdpCone *c : sc) eye.push_back(-c->dualResidual);
+    assemble_buffers(sc, tau, -1.0, y, eye, BUFFER_DUALVAR, h->d_yall, h->h_yall);
+}
+
 static bool batched_cones(hdsdp *h) {
     int nSdp = 0;
     for (ConeSlot &k : h->cones) nSdp += k.sdp ? 1 : 0;
@@ -388,7 +395,7 @@ hdsdp_retcode cones_interior(hdsdp *h, double tau, const double *y, int *interio
     *interior = 1;
     if (batched_cones(h)) {
         std::vector<SdpCone *> sc = sdp_cones(h);
-        for (SdpCone *c : sc) c->update(tau, y);
+        update_cones(h, sc, tau, y);
         std::vector<char> ok;
         factor_buffers(sc, BUFFER_DUALVAR, ok);
         *interior = cones_first_failure(h, ok, [&](LpCone &lp) { return lp.interior_check(tau, y); });
@@ -411,7 +418,7 @@ hdsdp_retcode cones_interior_expert(hdsdp *h, double dC, double dAs, const doubl
     *interior = 1;
     if (batched_cones(h)) {
         std::vector<SdpCone *> sc = sdp_cones(h);
-        for (SdpCone *c : sc) c->update_buffer(dC, dAs, y, dEye, which);
+        assemble_buffers(sc, dC, dAs, y, std::vector<double>(sc.size(), dEye), which, h->d_yall, h->h_yall);
         std::vector<char> ok;
         factor_buffers(sc, which == BUFFER_DUALVAR ? BUFFER_DUALVAR : BUFFER_DUALCHECK, ok);
         *interior = cones_first_failure(
@@ -436,12 +443,13 @@ hdsdp_retcode cones_ratio(hdsdp *h, double dtau, const double *dy, double ada, i
         // the small blocks' Lanczos bounds share their launches (lanczos_small_batch)
         std::vector<double> st(h->cones.size(), HDSDP_INFINITY);
         std::vector<LzTask> tasks;
+        std::vector<SdpCone *> small;
         size_t q = 0;
         for (ConeSlot &k : h->cones) {
             double *sq = &st[q++];
             if (k.sdp && k.sdp->small_lanczos()) {
                 SdpCone &c = *k.sdp;
-                c.update_buffer(dtau, -1.0, dy, ada * c.dualResidual, BUFFER_DUALSTEP);
+                small.push_back(&c);
                 tasks.push_back(LzTask{&c.lz, which == BUFFER_DUALVAR ? &c.Fvar : &c.Fcheck, c.dS, c.ld, sq, c.tm,
                                        HDSDP_RETCODE_OK});
             } else if (k.sdp) {
@@ -450,6 +458,11 @@ hdsdp_retcode cones_ratio(hdsdp *h, double dtau, const double *dy, double ada, i
             } else {
                 *sq = k.lp->ratio_test(dtau, dy, ada, which);
             }
+        }
+        {
+            std::vector<double> eye;
+            for (SdpCone *c : small) eye.push_back(ada * c->dualResidual);
+            assemble_buffers(small, dtau, -1.0, dy, eye, BUFFER_DUALSTEP, h->d_yall, h->h_yall);
         }
         lanczos_small_batch(tasks);
         for (const LzTask &t : tasks)
@@ -504,7 +517,7 @@ hdsdp_retcode cones_barrier(hdsdp *h, double tau, const double *y, int which, do
     *sum = 0.0;
     if (y && batched_cones(h)) {
         std::vector<SdpCone *> sc = sdp_cones(h);
-        for (SdpCone *c : sc) c->update(tau, y);
+        update_cones(h, sc, tau, y);
         std::vector<char> ok;
         factor_buffers(sc, BUFFER_DUALVAR, ok);
         for (char o : ok)
@@ -1498,6 +1511,9 @@ double min_eig_estimate(SdpCone &c, double *X) {
 }
 
 void release_cones(hdsdp *h) {
+    if (h->d_yall) hb::cache_free(h->d_yall);
+    if (h->h_yall) hb::cache_free_host(h->h_yall);
+    h->d_yall = h->h_yall = nullptr;
     for (ConeSlot &k : h->cones) {
         if (k.sdp) {
             k.sdp->release();
@@ -1784,6 +1800,11 @@ hdsdp_retcode HDSDPOptimize(hdsdp *h, int dOptOnly) {
         for (ConeSlot &k : h->cones) {
             if (k.sdp && k.sdp->sparse) sp.push_back(k.sdp);
             else allSparse = false;
+        }
+        // the vector of the batched cone updates (several SDP cones)
+        if (batched_cones(h)) {
+            HB_CUDA(hb::cmalloc(&h->d_yall, sizeof(double) * std::max(h->nRows, 1)));
+            HB_CUDA(hb::cmalloc_host(&h->h_yall, sizeof(double) * std::max(h->nRows, 1)));
         }
         const bool useArrow = allSparse && arrow_chosen(h->sparseSchur, h->nRows, sp);
         h->kkt.init(h->nRows, h->stream, &h->timers, !useArrow);

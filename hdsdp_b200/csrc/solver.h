@@ -174,6 +174,8 @@ struct SdpCone {
     void detect_feature(const double *rowRHS, int intF[20], double dblF[20]) const;
 
     void update_buffer(double dC, double dAs, const double *y, double dEye, int which);
+    bool buffer_plan(double dC, double dAs, const double *y, double &dEye, int which, double **target,
+                     const double **ly);
     void set_start(double r) { dualResidual = r; }
     void reduce_resi(double r) { dualResidual = r; }
     void set_perturb(double p) { dualPerturb = p; }
@@ -188,6 +190,12 @@ struct SdpCone {
     void atimesx(const double *X, double *out);                                // host out (problem m), accumulated
     double trace_cx(const double *X);
 };
+
+// update_buffer(dC, dAs, y, dEye[q], which) of several cones (all on one stream): y in problem
+// order, uploaded once into d_yall (mAll doubles, pinned staging h_yall); small cones whose
+// coefficients all sit in the gather map assembled in shared launches
+void assemble_buffers(const std::vector<SdpCone *> &cones, double dC, double dAs, const double *y,
+                      const std::vector<double> &dEye, int which, double *d_yall, double *h_yall);
 
 // factor_buffer(which) of several cones (all on one stream), small dense factorisations
 // batched: ok[q] = positive definite
@@ -373,4 +381,5 @@ struct hdsdp_solver_internal {
     std::vector<hb::IterRecord> log;
     std::string modelFeatures;
     hb::AdjointState *adj = nullptr;  // cached adjoint factors of the last solve
+    double *d_yall = nullptr, *h_yall = nullptr;   // y of the batched cone updates (device, pinned)
 };
