@@ -418,7 +418,8 @@ hdsdp_retcode SdpCone::setup_device(cudaStream_t stream, Timers *t) {
 void SdpCone::release() {
     dev.release();
     auto f = [](void *p) { if (p) hb::cache_free(p); };
-    f(Svar); f(Scheck); f(dS); f(W); f(d_y); f(d_vec); f(d_vec2); f(d_scal); f(d_rows);
+    f(Svar); f(Scheck); f(dS); f(W); f(d_y); f(d_vec); f(d_vec2); f(d_scal); f(d_rows); f(Mown);
+    Mown = nullptr;
     if (h_vec) hb::cache_free_host(h_vec);
     if (h_vec2) hb::cache_free_host(h_vec2);
     d_vec2 = h_vec2 = nullptr;
@@ -973,6 +974,11 @@ void KKT::init(int m_, cudaStream_t stream, Timers *t, bool denseM) {
 
 void KKT::release() {
     release_arrow();
+    if (d_wdesc) hb::cache_free(d_wdesc);
+    if (d_jobs) hb::cache_free(d_jobs);
+    d_wdesc = nullptr;
+    d_jobs = nullptr;
+    fusedCap = 0;
     if (M) hb::cache_free(M);
     M = nullptr;
     if (Msub) hb::cache_free(Msub);
@@ -1144,6 +1150,10 @@ hdsdp_retcode KKT::add_sdp(SdpCone &cone, int type) {
     return device_error_flag() ? HDSDP_RETCODE_FAILED : HDSDP_RETCODE_OK;
 }
 
+// cones whose Schur build runs in the fused per-cone kernel
+constexpr int kFusedBuildMaxN = 512;
+constexpr int kFusedBuildMaxM = 1024;
+
 // add_sdp for every cone of `cones` (a build of type KKT_TYPE_INFEASIBLE or
 // KKT_TYPE_CORRECTOR, the cones in the user's order): all device work is enqueued first,
 // each cone's vectors and trace come back into its own pinned buffers, and after one wait
@@ -1151,8 +1161,78 @@ hdsdp_retcode KKT::add_sdp(SdpCone &cone, int type) {
 // result is the same to the bit.
 hdsdp_retcode KKT::add_sdp_batch(const std::vector<SdpCone *> &cones, int type) {
     const double t0 = wall();
-    for (SdpCone *cp : cones) {
-        SdpCone &cone = *cp;
+    const bool corr = (type == KKT_TYPE_CORRECTOR);
+    // Cones of the sparse and sparse rank-one classes only (FP64, no sparse slack factor,
+    // moderate size) are built together: every W = K^T K in one grouped GEMM, then one CTA per
+    // cone forms its Schur block (into its own scratch), <A_i, W>, <A_i, W^2> and tr W, the
+    // vectors written straight into the cone's pinned host buffers.
+    std::vector<char> fused(cones.size(), 0);
+    {
+        std::vector<GemmDesc> wd;
+        std::vector<SchurBuildJob> jobs;
+        int maxn = 0;
+        auto mapped = [](void *h) {
+            void *d = nullptr;
+            if (cudaHostGetDevicePointer(&d, h, 0) != cudaSuccess) {
+                cudaGetLastError();
+                return (double *) nullptr;
+            }
+            return (double *) d;
+        };
+        for (size_t q = 0; q < cones.size(); ++q) {
+            SdpCone &c = *cones[q];
+            if (!c.dev.batchable() || c.hy || c.n > kFusedBuildMaxN || c.m > kFusedBuildMaxM || c.m == 0) continue;
+            if (c.dev.precision == 1 && c.n >= kSplitInverseMinN) continue;
+            double *hv = mapped(c.h_vec), *hv2 = mapped(c.h_vec2), *hs = mapped(c.h_scal);
+            if (!hv || !hv2 || !hs) continue;
+            const long ldk = pad_ld(c.m);
+            if (!corr && !c.Mown) HB_CUDA(hb::cmalloc(&c.Mown, sizeof(double) * ldk * c.m));
+            compute_inverse_factor(s, c.Fvar);   // formed by the factorisation kernel already
+            wd.push_back(GemmDesc{c.n, c.n, c.n, 1.0, 0.0, c.Fvar.K, c.Fvar.ld, 1, c.Fvar.K, c.Fvar.ld, 0, c.W, c.ld,
+                                  GEMM_C_LOWER | GEMM_A_UPPER | GEMM_B_LOWER, nullptr});
+            SchurBuildJob J = schur_build_job(c.dev, c.W, c.ld, corr ? nullptr : c.Mown, ldk);
+            const double r = c.dualResidual;
+            J.inner = hv;
+            J.innersq = (r != 0.0) ? hv2 : nullptr;
+            J.trace = (!corr && r != 0.0) ? hs : nullptr;
+            J.reuse_vt = corr ? 1 : 0;
+            jobs.push_back(J);
+            maxn = std::max(maxn, c.n);
+            fused[q] = 1;
+        }
+        if (!jobs.empty()) {
+            if (fusedCap < jobs.size()) {
+                HB_CUDA(cudaStreamSynchronize(s));
+                if (d_wdesc) hb::cache_free(d_wdesc);
+                if (d_jobs) hb::cache_free(d_jobs);
+                fusedCap = jobs.size();
+                HB_CUDA(hb::cmalloc(&d_wdesc, sizeof(GemmDesc) * fusedCap));
+                HB_CUDA(hb::cmalloc(&d_jobs, sizeof(SchurBuildJob) * fusedCap));
+            }
+            HB_CUDA(cudaMemcpyAsync(d_wdesc, wd.data(), sizeof(GemmDesc) * wd.size(), cudaMemcpyHostToDevice, s));
+            HB_CUDA(cudaMemcpyAsync(d_jobs, jobs.data(), sizeof(SchurBuildJob) * jobs.size(), cudaMemcpyHostToDevice, s));
+            gemm_grouped(s, d_wdesc, (int) wd.size(), maxn, maxn);
+            schur_build_batch(s, d_jobs, (int) jobs.size());
+        }
+    }
+    for (size_t q = 0; q < cones.size(); ++q) {
+        SdpCone &cone = *cones[q];
+        if (fused[q]) {
+            // the cone's Schur block into M, in the cones' order
+            if (!corr) {
+                const int mk = cone.m;
+                const long ldk = pad_ld(mk);
+                open_m();
+                if (arrow) {
+                    arrow_add(cone, cone.Mown, ldk);
+                } else {
+                    dim3 blk(32, 8), grd((mk + 31) / 32, std::min((mk + 7) / 8, 4096));
+                    scatter_lower_kernel<<<hb::counted(grd), blk, 0, s>>>(mk, cone.Mown, ldk, cone.d_rows, M, ldm);
+                    HB_CUDA(cudaGetLastError());
+                }
+            }
+            continue;
+        }
         const int n = cone.n;
         const long ld = cone.ld;
         const double r = cone.dualResidual;

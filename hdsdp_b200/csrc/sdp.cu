@@ -408,7 +408,189 @@ __global__ void innersq_r1s_kernel(int n, int k, const int *id, const int *ptr, 
     if (lane == 0) out[id[a]] = sg[a] * acc;
 }
 
+// sum over i < n of f(i) as a 1024-thread block forms it (one term per thread, a shuffle tree
+// per warp, then one over the 32 warp sums; n <= 1024), by a block of 256 threads
+template <class F>
+__device__ double sum_as_1024(int n, F f) {
+    __shared__ double red[32];
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int v = t + 256 * q;
+        double x = (v < n) ? f(v) : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        if (lane == 0) red[w + 8 * q] = x;
+    }
+    __syncthreads();
+    double x = 0.0;
+    if (w == 0) {
+        x = red[lane];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    }
+    __syncthreads();
+    return x;
+}
+
+__global__ void __launch_bounds__(256) schur_build_batch_kernel(const SchurBuildJob *__restrict__ jobs) {
+    const SchurBuildJob J = jobs[blockIdx.x];
+    const int n = J.n, tid = threadIdx.x, nt = blockDim.x;
+    double *W = J.W;
+    const long ldw = J.ldW;
+    // W(j, i) = W(i, j), i > j
+    for (long idx = tid; idx < (long) n * n; idx += nt) {
+        const int i = (int) (idx % n), j = (int) (idx / n);
+        if (i > j) W[(size_t) j + (size_t) i * ldw] = W[(size_t) i + (size_t) j * ldw];
+    }
+    __syncthreads();
+    if (J.trace) {
+        const double tr = sum_as_1024(n, [&](int i) { return W[(size_t) i + (size_t) i * ldw]; });
+        if (tid == 0) *J.trace = tr;
+    }
+    const int nsp = J.nsp, nr1s = J.nr1s;
+    if (J.M) {
+        double *M = J.M;
+        const long ldm = J.ldM;
+        for (long idx = tid; idx < ldm * J.m; idx += nt) M[idx] = 0.0;
+        __syncthreads();
+        for (long t = tid; t < (long) nsp * nsp; t += nt) {   // schur_spsp_kernel
+            const int a = (int) (t % nsp), b = (int) (t / nsp);
+            if (b > a) continue;
+            const int *ptr = J.sp_ptr, *rr = J.sp_r, *cc = J.sp_c;
+            const double *vv = J.sp_v;
+            double acc = 0.0;
+            for (int e = ptr[a]; e < ptr[a + 1]; ++e)
+                for (int f = ptr[b]; f < ptr[b + 1]; ++f)
+                    acc += vv[e] * vv[f] * pair_term(W, ldw, rr[e], cc[e], rr[f], cc[f]);
+            M[(size_t) J.sp_id[a] + (size_t) J.sp_id[b] * ldm] = acc;
+        }
+        for (long t = tid; t < (long) nr1s * nr1s; t += nt) {   // schur_r1s_kernel
+            const int a = (int) (t % nr1s), b = (int) (t / nr1s);
+            if (b > a) continue;
+            const int *ptr = J.r1s_ptr, *pp = J.r1s_p;
+            const double *aa = J.r1s_a;
+            double g = 0.0;
+            for (int u0 = ptr[a]; u0 < ptr[a + 1]; ++u0) {
+                double gt = 0.0;
+                for (int u = ptr[b]; u < ptr[b + 1]; ++u) gt += aa[u] * W[(size_t) pp[u0] + (size_t) pp[u] * ldw];
+                g += aa[u0] * gt;
+            }
+            M[(size_t) J.r1s_id[a] + (size_t) J.r1s_id[b] * ldm] = J.r1s_sign[a] * J.r1s_sign[b] * g * g;
+        }
+        if (nr1s > 0 && nsp > 0) {
+            for (long t = tid; t < (long) n * nr1s; t += nt) {   // r1s_build_v_kernel
+                const int k = (int) (t % n), b = (int) (t / n);
+                double acc = 0.0;
+                for (int u = J.r1s_ptr[b]; u < J.r1s_ptr[b + 1]; ++u)
+                    acc += J.r1s_a[u] * W[(size_t) k + (size_t) J.r1s_p[u] * ldw];
+                J.Vs[(size_t) k + (size_t) b * J.ldv] = acc;
+            }
+            __syncthreads();
+            for (long t = tid; t < (long) nsp * nr1s; t += nt) {   // schur_r1_sp_kernel
+                const int b = (int) (t % nsp), a = (int) (t / nsp);
+                const double *v = J.Vs + (size_t) a * J.ldv;
+                double acc = 0.0;
+                for (int f = J.sp_ptr[b]; f < J.sp_ptr[b + 1]; ++f) {
+                    const int r = J.sp_r[f], c = J.sp_c[f];
+                    acc += J.sp_v[f] * ((r != c) ? 2.0 * v[r] * v[c] : v[r] * v[r]);
+                }
+                const int i = J.r1s_id[a], j = J.sp_id[b];
+                const int hi = max(i, j), lo = min(i, j);
+                M[(size_t) hi + (size_t) lo * ldm] = J.r1s_sign[a] * acc;
+            }
+        }
+    }
+    // inner_all
+    if (nsp + nr1s < J.m)
+        for (int i = tid; i < J.m; i += nt) J.inner[i] = 0.0;
+    __syncthreads();
+    for (int a = tid; a < nsp; a += nt) {   // inner_sp_kernel
+        double acc = 0.0;
+        for (int e = J.sp_ptr[a]; e < J.sp_ptr[a + 1]; ++e) {
+            const int r = J.sp_r[e], c = J.sp_c[e];
+            const double z = W[(size_t) r + (size_t) c * ldw];
+            acc += J.sp_v[e] * ((r != c) ? 2.0 * z : z);
+        }
+        J.inner[J.sp_id[a]] = acc;
+    }
+    for (int a = tid; a < nr1s; a += nt) {   // inner_r1s_kernel
+        double acc = 0.0;
+        for (int u0 = J.r1s_ptr[a]; u0 < J.r1s_ptr[a + 1]; ++u0) {
+            double at = 0.0;
+            for (int u = J.r1s_ptr[a]; u < J.r1s_ptr[a + 1]; ++u)
+                at += J.r1s_a[u] * W[(size_t) J.r1s_p[u0] + (size_t) J.r1s_p[u] * ldw];
+            acc += J.r1s_a[u0] * at;
+        }
+        J.inner[J.r1s_id[a]] = J.r1s_sign[a] * acc;
+    }
+    if (!J.innersq) return;
+    // inner_all_sq: one warp per constraint, as innersq_sp_kernel / innersq_r1s_kernel
+    __syncthreads();
+    if (nsp + nr1s < J.m)
+        for (int i = tid; i < J.m; i += nt) J.innersq[i] = 0.0;
+    __syncthreads();
+    const int lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
+    for (int a = warp; a < nsp; a += nw) {
+        double acc = 0.0;
+        for (int e = J.sp_ptr[a]; e < J.sp_ptr[a + 1]; ++e) {
+            const int r = J.sp_r[e], c = J.sp_c[e];
+            const double *wr = W + (size_t) r * ldw;
+            const double *wc = W + (size_t) c * ldw;
+            double d = 0.0;
+            for (int k = lane; k < n; k += 32) d += wr[k] * wc[k];
+            acc += J.sp_v[e] * ((r != c) ? 2.0 : 1.0) * d;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (lane == 0) J.innersq[J.sp_id[a]] = acc;
+    }
+    for (int a = warp; a < nr1s; a += nw) {
+        double acc = 0.0;
+        for (int r = lane; r < n; r += 32) {
+            double v = 0.0;
+            for (int u = J.r1s_ptr[a]; u < J.r1s_ptr[a + 1]; ++u) v += J.r1s_a[u] * W[(size_t) r + (size_t) J.r1s_p[u] * ldw];
+            acc += v * v;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (lane == 0) J.innersq[J.r1s_id[a]] = J.r1s_sign[a] * acc;
+    }
+}
+
 }  // namespace
+
+void schur_build_batch(cudaStream_t s, const SchurBuildJob *d_jobs, int count) {
+    for (int b0 = 0; b0 < count; b0 += 65535) {
+        schur_build_batch_kernel<<<hb::counted(std::min(65535, count - b0)), 256, 0, s>>>(d_jobs + b0);
+        HB_CUDA(cudaGetLastError());
+    }
+}
+
+SchurBuildJob schur_build_job(const SdpDevice &d, double *W, long ldW, double *M, long ldM) {
+    SchurBuildJob J{};
+    J.W = W;
+    J.ldW = ldW;
+    J.n = d.n;
+    J.m = d.m;
+    J.M = M;
+    J.ldM = ldM;
+    J.nsp = d.nsp;
+    J.sp_id = d.sp_id;
+    J.sp_ptr = d.sp_ptr;
+    J.sp_r = d.sp_r;
+    J.sp_c = d.sp_c;
+    J.sp_v = d.sp_v;
+    J.nr1s = d.nr1s;
+    J.r1s_id = d.r1s_id;
+    J.r1s_ptr = d.r1s_ptr;
+    J.r1s_p = d.r1s_p;
+    J.r1s_a = d.r1s_a;
+    J.r1s_sign = d.r1s_sign;
+    J.Vs = d.Vs;
+    J.ldv = d.ld;
+    return J;
+}
 
 static double host_seconds() {
     return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();

@@ -136,6 +136,36 @@ struct SdpDevice {
     // precision for the blocks that read W (sparse, sparse rank-one and dense
     // coefficients). False if the tensor-core path is unavailable.
     bool split_inverse(const double *Kinv, double *W, long ldW);
+    // the Schur build of this cone can run in schur_build_batch (coefficients of the sparse
+    // and sparse rank-one classes only)
+    bool batchable() const { return nr1d == 0 && ndr == 0; }
 };
+
+// One cone's share of a batched Schur build: from W (lower triangle as the GEMM writes it;
+// mirrored here as symmetrize_lower does) the Schur block M (ldM x m, zeroed first; null:
+// none, as in a corrector build), <A_i, W> into inner, <A_i, W^2> into innersq and tr W into
+// trace (null: skipped). Output addresses may be mapped pinned host memory.
+struct SchurBuildJob {
+    double *W;
+    long ldW;
+    int n, m;
+    double *M;
+    long ldM;
+    int nsp;
+    const int *sp_id, *sp_ptr, *sp_r, *sp_c;
+    const double *sp_v;
+    int nr1s;
+    const int *r1s_id, *r1s_ptr, *r1s_p;
+    const double *r1s_a, *r1s_sign;
+    double *Vs;
+    long ldv;
+    double *inner, *innersq, *trace;
+    int reuse_vt;   // inner_all_sq's reuse_vt (no effect on these classes; kept for the record)
+};
+// The builds of jobs[0 .. count) (device array), one CTA each: the operations of
+// symmetrize_lower, trace, schur_matrix, inner_all and inner_all_sq for these classes, each
+// output entry formed by the same arithmetic as those kernels form it.
+void schur_build_batch(cudaStream_t s, const SchurBuildJob *d_jobs, int count);
+SchurBuildJob schur_build_job(const SdpDevice &d, double *W, long ldW, double *M, long ldM);
 
 }  // namespace hb

@@ -155,6 +155,7 @@ struct SdpCone {
     double *d_vec = nullptr;     // device m scratch
     double *h_vec = nullptr;     // pinned m scratch
     double *d_vec2 = nullptr, *h_vec2 = nullptr;   // second pair (batched Schur builds)
+    double *Mown = nullptr;      // the cone's own Schur-block scratch (batched Schur builds)
     double *d_scal = nullptr, *h_scal = nullptr;
     double objScal = 1.0;
     Timers *tm = nullptr;
@@ -286,6 +287,11 @@ struct KKT {
     bool mOpen = false;
     double *Msub = nullptr;           // Schur block of a cone added into M (sparse or not first)
     size_t msubCap = 0;
+    // descriptors of the batched Schur builds (add_sdp_batch): the grouped W = K^T K and the
+    // per-cone build jobs
+    GemmDesc *d_wdesc = nullptr;
+    SchurBuildJob *d_jobs = nullptr;
+    size_t fusedCap = 0;
     // dense M and F are allocated unless denseM is false (the block-arrow form is used)
     void init(int m_, cudaStream_t stream, Timers *t, bool denseM = true);
     void release();
