@@ -9,6 +9,7 @@
 //   <A, W B W>    = sum_e sum_f v_e u_f * pair(e, f)       (pair below)
 #include "sdp.h"
 #include <cub/device/device_scan.cuh>
+#include <cub/device/device_radix_sort.cuh>
 #include <chrono>
 #include <unordered_map>
 #include <algorithm>
@@ -75,6 +76,23 @@ __global__ void r1map_place_kernel(int n, const int *__restrict__ cnt, const int
     pcnt[sl] = k;
 }
 
+// positions reordered by list length (perm[i] = the packed rank of the i-th): row, column and
+// count gathered to the new order, inv[perm[i]] = i
+__global__ void r1map_permute_kernel(int npos, const int *__restrict__ perm, const int *__restrict__ pr,
+                                     const int *__restrict__ pc, int *pr2, int *pc2, int *inv) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= npos) return;
+    const int p = perm[i];
+    pr2[i] = pr[p];
+    pc2[i] = pc[p];
+    inv[p] = i;
+}
+
+__global__ void iota_kernel(int n, int *x) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) x[i] = i;
+}
+
 // slices of 32 positions padded to their longest list: 32 * max count per slice
 __global__ void r1map_slice_kernel(int npos, int nslice, const int *__restrict__ pcnt, long long *len) {
     const int sl = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
@@ -91,9 +109,9 @@ __global__ void r1map_slice_kernel(int npos, int nslice, const int *__restrict__
 __global__ void r1map_fill_kernel(int n, const int *__restrict__ rptr, const int *__restrict__ rj,
                                   const double *__restrict__ ra, const double *__restrict__ sgn,
                                   const int *__restrict__ cnt, const int *__restrict__ slot,
-                                  const long long *__restrict__ sptr, int *ej, double *ev,
-                                  const int *__restrict__ lslot, const long long *__restrict__ lptr, int *lj,
-                                  double *lv) {
+                                  const int *__restrict__ inv, const long long *__restrict__ sptr, int *ej,
+                                  double *ev, const int *__restrict__ lslot, const long long *__restrict__ lptr,
+                                  int *lj, double *lv) {
     const int c = blockIdx.y, r = c + blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= n) return;
     const long long q = r1map_pos(n, r, c);
@@ -108,7 +126,7 @@ __global__ void r1map_fill_kernel(int n, const int *__restrict__ rptr, const int
         dj = lj;
         dv = lv;
     } else {
-        const int sl = slot[q];
+        const int sl = inv[slot[q]];
         at = sptr[sl >> 5] + (sl & 31);
         step = 32;
     }
@@ -815,6 +833,30 @@ void SdpDevice::upload(int n_, int m_, const HostCoeff &C, const std::vector<Hos
             exclusive_sum(s, d_llen, posL_ptr, (long long) nposL + 1);
             long long totalL = 0;
             HB_CUDA(cudaMemcpyAsync(&totalL, posL_ptr + nposL, sizeof(long long), cudaMemcpyDeviceToHost, s));
+            // the short positions ordered by list length (a stable sort: packed order within a
+            // length), so that the 32 positions of a slice have lists of about the same length
+            // and the slices carry little padding; each position's sum is unchanged
+            int *d_inv = nullptr;
+            HB_CUDA(hb::cmalloc(&d_inv, sizeof(int) * std::max(npos2, 1)));
+            if (npos2 > 0) {
+                int *d_iota = nullptr, *d_perm = nullptr, *d_cnt2 = nullptr, *d_r2 = nullptr, *d_c2 = nullptr;
+                for (int **p : {&d_iota, &d_perm, &d_cnt2, &d_r2, &d_c2}) HB_CUDA(hb::cmalloc(p, sizeof(int) * npos2));
+                iota_kernel<<<hb::counted((npos2 + 255) / 256), 256, 0, s>>>(npos2, d_iota);
+                size_t bytes = 0;
+                HB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, bytes, pos2_cnt, d_cnt2, d_iota, d_perm, npos2, 0,
+                                                        8, s));
+                void *tmp = nullptr;
+                HB_CUDA(hb::cmalloc(&tmp, bytes));
+                HB_CUDA(cub::DeviceRadixSort::SortPairs(tmp, bytes, pos2_cnt, d_cnt2, d_iota, d_perm, npos2, 0, 8, s));
+                r1map_permute_kernel<<<hb::counted((npos2 + 255) / 256), 256, 0, s>>>(npos2, d_perm, pos2_r, pos2_c,
+                                                                                     d_r2, d_c2, d_inv);
+                HB_CUDA(cudaMemcpyAsync(pos2_r, d_r2, sizeof(int) * npos2, cudaMemcpyDeviceToDevice, s));
+                HB_CUDA(cudaMemcpyAsync(pos2_c, d_c2, sizeof(int) * npos2, cudaMemcpyDeviceToDevice, s));
+                HB_CUDA(cudaMemcpyAsync(pos2_cnt, d_cnt2, sizeof(int) * npos2, cudaMemcpyDeviceToDevice, s));
+                HB_CUDA(cudaStreamSynchronize(s));
+                hb::cache_free(tmp);
+                for (int *p : {d_iota, d_perm, d_cnt2, d_r2, d_c2}) hb::cache_free(p);
+            }
             r1map_slice_kernel<<<hb::counted((int) ((32LL * (nslice + 1) + 255) / 256)), 256, 0, s>>>(
                 npos2, nslice, pos2_cnt, d_len);
             exclusive_sum(s, d_len, pos2_ptr, (long long) nslice + 1);
@@ -827,10 +869,12 @@ void SdpDevice::upload(int n_, int m_, const HostCoeff &C, const std::vector<Hos
             HB_CUDA(cudaMemsetAsync(ent2_v, 0, sizeof(double) * std::max(total, 1LL), s));
             HB_CUDA(hb::cmalloc(&entL_j, sizeof(int) * std::max(totalL, 1LL)));
             HB_CUDA(hb::cmalloc(&entL_v, sizeof(double) * std::max(totalL, 1LL)));
-            r1map_fill_kernel<<<hb::counted(pgrid), 256, 0, s>>>(n, d_rptr, d_rj, d_ra, d_sgn, d_cnt, d_slot, pos2_ptr,
-                                                                 ent2_j, ent2_v, d_lslot, posL_ptr, entL_j, entL_v);
+            r1map_fill_kernel<<<hb::counted(pgrid), 256, 0, s>>>(n, d_rptr, d_rj, d_ra, d_sgn, d_cnt, d_slot, d_inv,
+                                                                 pos2_ptr, ent2_j, ent2_v, d_lslot, posL_ptr, entL_j,
+                                                                 entL_v);
             HB_CUDA(cudaGetLastError());
             HB_CUDA(cudaStreamSynchronize(s));
+            hb::cache_free(d_inv);
             for (int *p : {d_rptr, d_rj, d_cnt, d_used, d_slot, d_long, d_lslot}) hb::cache_free(p);
             hb::cache_free(d_llen);
             hb::cache_free(d_ra);
