@@ -385,6 +385,7 @@ hdsdp_retcode SdpCone::setup_device(cudaStream_t stream, Timers *t) {
     HB_CUDA(cudaMemsetAsync(dS, 0, sizeof(double) * ld * n, s));
     Fvar.alloc(n);
     Fcheck.alloc(n);
+    facKeepOk = pinVar = false;
     lz.init(n, s);
     hyVar = hyCheck = false;
     if (sparseMode != 0 && (sparseMode == 1 || n >= kHybridMinN)) {
@@ -400,6 +401,7 @@ hdsdp_retcode SdpCone::setup_device(cudaStream_t stream, Timers *t) {
             }
         }
     }
+    if (!hy) Fkeep.alloc(n);   // the kept factor of the accepted point (dense factors only)
     HB_CUDA(hb::cmalloc(&d_y, sizeof(double) * std::max(m, 1)));
     HB_CUDA(hb::cmalloc(&d_vec, sizeof(double) * std::max(m, 1)));
     HB_CUDA(hb::cmalloc(&d_vec2, sizeof(double) * std::max(m, 1)));
@@ -428,6 +430,8 @@ void SdpCone::release() {
     d_rows = nullptr;
     Fvar.release();
     Fcheck.release();
+    Fkeep.release();
+    facKeepOk = pinVar = false;
     lz.release();
     if (hy) {
         hy->release();
@@ -591,6 +595,26 @@ static bool timed_factor(cudaStream_t s, DenseFactor &F, const double *S, long l
     return ok;
 }
 
+void SdpCone::keep_var() {
+    if (Fkeep.L && pinVar && facVarOk && facVar.valid) {
+        std::swap(Fvar, Fkeep);
+        facKeep = facVar;
+        facKeepOk = true;
+    }
+    pinVar = false;
+}
+
+bool SdpCone::restore_var() {
+    if (!Fkeep.L || !facKeepOk || !sigVar.same(facKeep)) return false;
+    std::swap(Fvar, Fkeep);
+    std::swap(facVar, facKeep);
+    std::swap(facVarOk, facKeepOk);
+    hyVar = false;
+    pinVar = true;
+    ++nFactorReuse;
+    return true;
+}
+
 bool SdpCone::factor_buffer(int which) {
     const bool var = (which == BUFFER_DUALVAR);
     DenseFactor &F = var ? Fvar : Fcheck;
@@ -603,6 +627,7 @@ bool SdpCone::factor_buffer(int which) {
         ++nFactorReuse;
         return fok;
     }
+    if (var && restore_var()) return facVarOk;
     if (sig.same(osig) && ook) {
         if (var ? hyCheck : hyVar) {
             // the other object holds a hybrid result for the same matrix
@@ -612,6 +637,7 @@ bool SdpCone::factor_buffer(int which) {
             F.factored = F.ok = true;
             F.k_valid = false;
         } else {
+            if (var) keep_var();
             copy_factor(s, F, var ? Fcheck : Fvar);
             (var ? hyVar : hyCheck) = false;
         }
@@ -620,6 +646,7 @@ bool SdpCone::factor_buffer(int which) {
         ++nFactorReuse;
         return true;
     }
+    if (var) keep_var();
     const bool ok = use_hybrid(which) ? hybrid_factor(which) : timed_factor(s, F, var ? Svar : Scheck, ld, tm);
     if (!use_hybrid(which)) (var ? hyVar : hyCheck) = false;
     fsig = sig;
@@ -638,10 +665,12 @@ int SdpCone::factor_plan(int which, bool *ok) {
     const SlackSig &fsig = var ? facVar : facCheck;
     const SlackSig &osig = var ? facCheck : facVar;
     const bool ook = var ? facCheckOk : facVarOk;
-    if (sig.same(fsig) || (sig.same(osig) && ook) || use_hybrid(which)) {
-        *ok = factor_buffer(which);   // reuse, copy or the hybrid factorisation
+    if (sig.same(fsig) || (var && Fkeep.L && facKeepOk && sig.same(facKeep)) || (sig.same(osig) && ook) ||
+        use_hybrid(which)) {
+        *ok = factor_buffer(which);   // reuse, the kept factor, copy or the hybrid factorisation
         return FP_DONE;
     }
+    if (var) keep_var();
     if (n <= kBatchFactorMaxN) return FP_SMALL;
     factorize_async(s, var ? Fvar : Fcheck, var ? Svar : Scheck, ld);
     return FP_ASYNC;
@@ -784,6 +813,7 @@ hdsdp_retcode SdpCone::get_barrier(double tau, const double *y, int which, doubl
 
 void SdpCone::add_step(double step, int which) {
     if (which == BUFFER_DUALVAR) {
+        keep_var();
         axpy(s, (int) (ld * n), step, dS, Svar);
         sigVar.valid = false;
         facVar.valid = false;
@@ -797,6 +827,7 @@ void SdpCone::add_step(double step, int which) {
 
 hdsdp_retcode SdpCone::add_step_and_check(double step, int which, int *interior) {
     if (which == BUFFER_DUALVAR) {
+        keep_var();
         axpy(s, (int) (ld * n), step, dS, Svar);
         sigVar.valid = false;
         facVar.valid = false;
@@ -1069,6 +1100,7 @@ hdsdp_retcode KKT::add_sdp(SdpCone &cone, int type) {
             tm->s_inverse += wall() - ti;
         }
         Wp = cone.W;
+        cone.pinVar = true;   // the accepted point's factor
     }
     SdpDevice &dev = cone.dev;
     if (type == KKT_TYPE_CORRECTOR) {
@@ -1190,6 +1222,7 @@ hdsdp_retcode KKT::add_sdp_batch(const std::vector<SdpCone *> &cones, int type) 
             compute_inverse_factor(s, c.Fvar);   // formed by the factorisation kernel already
             wd.push_back(GemmDesc{c.n, c.n, c.n, 1.0, 0.0, c.Fvar.K, c.Fvar.ld, 1, c.Fvar.K, c.Fvar.ld, 0, c.W, c.ld,
                                   GEMM_C_LOWER | GEMM_A_UPPER | GEMM_B_LOWER, nullptr});
+            c.pinVar = true;   // the accepted point's factor
             SchurBuildJob J = schur_build_job(c.dev, c.W, c.ld, corr ? nullptr : c.Mown, ldk);
             const double r = c.dualResidual;
             J.inner = hv;
@@ -1243,6 +1276,7 @@ hdsdp_retcode KKT::add_sdp_batch(const std::vector<SdpCone *> &cones, int type) 
             done = cone.dev.split_inverse(cone.Fvar.K, cone.W, ld);
         }
         if (!done) compute_inverse(s, cone.Fvar, cone.W, ld);
+        cone.pinVar = true;   // the accepted point's factor
         const double *Wp = cone.W;
         SdpDevice &dev = cone.dev;
         const int mk = cone.m;

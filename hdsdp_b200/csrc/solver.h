@@ -121,6 +121,16 @@ struct SdpCone {
     SlackSig facVar, facCheck;   // inputs of the matrices factored in Fvar / Fcheck
     bool facVarOk = false, facCheckOk = false;
     long nFactorReuse = 0;
+    // The factor of the slack at the point of the last Schur build (the accepted iterate) is
+    // set aside (Fkeep) when a trial point's factorisation is about to overwrite Fvar, and handed
+    // back when that point is factored again, as after a line search that found no better point.
+    // Dense factors only (no sparse slack factorisation on the cone).
+    DenseFactor Fkeep;
+    SlackSig facKeep;
+    bool facKeepOk = false;
+    bool pinVar = false;
+    void keep_var();       // before a factorisation into Fvar
+    bool restore_var();    // the kept factor is that of Svar's inputs: back into Fvar
     // Factor the buffer `which` (Svar into Fvar, Scheck into Fcheck), reusing a
     // factor of the same inputs held by either factor object.
     bool factor_buffer(int which);
