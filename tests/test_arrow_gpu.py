@@ -103,3 +103,23 @@ def test_arrow_27k_rows_where_the_reference_stops(gpu_lib, golden):
     assert max(abs(e) for e in r["errs"]) < 1e-7
     assert ref["dobj"] <= r["dobj"] + 1e-6 * abs(r["dobj"])
     assert r["pobj"] <= ref["pobj"] + 1e-6 * abs(r["pobj"])
+
+
+@pytest.mark.parametrize("name,spec,coupling", [
+    # no shared constraint: M is block diagonal, the block arrow has no coupling block
+    ("sep4", dict(dims=[8, 7, 6, 5], m_local=[6, 6, 6, 6], m_couple=0, seed=21), 0),
+    # one cone holds only shared constraints: it has no local block
+    ("zero_local", dict(dims=[6, 8, 8, 7, 6], m_local=[0, 8, 8, 8, 8], m_couple=2, seed=22), 2),
+])
+def test_arrow_edge_cases(gpu_lib, name, spec, coupling):
+    """The block arrow forced on against the dense M on the same data: the same status,
+    iterations within 2 and objectives to 1e-8."""
+    prob = instances.multiblock(name=name, **spec)
+    a = api.solve_problem(prob, sparse_schur=1)
+    d = api.solve_problem(prob, sparse_schur=0)
+    assert a["sparse_schur"]["arrow"] and a["sparse_schur"]["coupling"] == coupling
+    assert not d["sparse_schur"]["arrow"]
+    assert a["status_after_check"] == d["status_after_check"] == 3
+    assert abs(a["iters"] - d["iters"]) <= 2
+    assert a["dobj"] == pytest.approx(d["dobj"], rel=1e-8, abs=1e-10)
+    assert a["pobj"] == pytest.approx(d["pobj"], rel=1e-7, abs=1e-10)
