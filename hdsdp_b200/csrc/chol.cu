@@ -667,9 +667,7 @@ __device__ double logdiag_1024(int n, const double *L, long ld) {
     return x;
 }
 
-__global__ void __launch_bounds__(COOP_THREADS, 1) potrf_small_batch_kernel(const SmallFactorBatch B) {
-    extern __shared__ double sm[];
-    const SmallFactorJob &J = B.job[blockIdx.x];
+__device__ void small_factor_job(const SmallFactorJob &J, double *sm) {
     const int n = J.n;
     for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
         const int r = idx % n, c = idx / n;
@@ -693,6 +691,18 @@ __global__ void __launch_bounds__(COOP_THREADS, 1) potrf_small_batch_kernel(cons
         reinterpret_cast<volatile int *>(J.hinfo)[0] = v;
         if (J.logdet) J.hinfo[1] = acc;
     }
+}
+
+__global__ void __launch_bounds__(COOP_THREADS, 1) potrf_small_batch_kernel(const SmallFactorBatch B) {
+    extern __shared__ double sm[];
+    small_factor_job(B.job[blockIdx.x], sm);
+}
+
+// the same, the jobs in global memory (more than fit the parameters)
+__global__ void __launch_bounds__(COOP_THREADS, 1) potrf_batch_array_kernel(const SmallFactorJob *__restrict__ jobs) {
+    extern __shared__ double sm[];
+    const SmallFactorJob J = jobs[blockIdx.x];
+    small_factor_job(J, sm);
 }
 
 __global__ void __launch_bounds__(COOP_THREADS, 1) trtri_coop_kernel(const double *L, double *K, long ld, int n,
@@ -1028,24 +1038,47 @@ bool small_factor_batch_enqueue(cudaStream_t s, DenseFactor *const *F, const dou
     once_per_device(attr, [] {
         HB_CUDA(cudaFuncSetAttribute((const void *) potrf_small_batch_kernel,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, SM_DOUBLES * (int) sizeof(double)));
+        HB_CUDA(cudaFuncSetAttribute((const void *) potrf_batch_array_kernel,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, SM_DOUBLES * (int) sizeof(double)));
     });
-    for (int b0 = 0; b0 < count; b0 += kSmallBatch) {
-        SmallFactorBatch B;
-        const int nb = std::min(kSmallBatch, count - b0);
-        for (int q = 0; q < nb; ++q) {
-            DenseFactor &G = *F[b0 + q];
-            double *hd = nullptr;
-            if (cudaHostGetDevicePointer((void **) &hd, G.h_info, 0) != cudaSuccess || !hd) {
-                cudaGetLastError();
-                return false;
-            }
-            B.job[q] = SmallFactorJob{S[b0 + q], G.L, G.Dinv, G.fuse_k ? G.K : nullptr, G.fuse_k ? G.KT : nullptr,
-                                      ldS[b0 + q], G.ld, G.d_info, hd, G.n, G.stat_logdet ? 1 : 0};
+    std::vector<SmallFactorJob> jobs(count);
+    for (int q = 0; q < count; ++q) {
+        DenseFactor &G = *F[q];
+        double *hd = nullptr;
+        if (cudaHostGetDevicePointer((void **) &hd, G.h_info, 0) != cudaSuccess || !hd) {
+            cudaGetLastError();
+            return false;
         }
-        potrf_small_batch_kernel<<<hb::counted(nb), COOP_THREADS, SM_DOUBLES * sizeof(double), s>>>(B);
-        if (cudaGetLastError() != cudaSuccess) return false;
+        jobs[q] = SmallFactorJob{S[q], G.L, G.Dinv, G.fuse_k ? G.K : nullptr, G.fuse_k ? G.KT : nullptr, ldS[q], G.ld,
+                                 G.d_info, hd, G.n, G.stat_logdet ? 1 : 0};
     }
-    return true;
+    if (count <= kSmallBatch) {
+        SmallFactorBatch B;
+        for (int q = 0; q < count; ++q) B.job[q] = jobs[q];
+        potrf_small_batch_kernel<<<hb::counted(count), COOP_THREADS, SM_DOUBLES * sizeof(double), s>>>(B);
+        return cudaGetLastError() == cudaSuccess;
+    }
+    // more jobs than fit the parameters: one launch over a device copy of them, in a buffer kept
+    // per host thread and device (every caller waits for the launch before its thread enqueues
+    // another batch, so the buffer is free again by then)
+    struct JobBuf {
+        SmallFactorJob *p = nullptr;
+        size_t cap = 0;
+    };
+    thread_local JobBuf buf[kMaxDevices];
+    JobBuf &b = buf[current_device()];
+    if (b.cap < (size_t) count) {
+        if (b.p) hb::cache_free(b.p);
+        b.cap = (size_t) count;
+        if (hb::cmalloc(&b.p, sizeof(SmallFactorJob) * b.cap) != cudaSuccess) {
+            b.p = nullptr;
+            b.cap = 0;
+            return false;
+        }
+    }
+    HB_CUDA(cudaMemcpyAsync(b.p, jobs.data(), sizeof(SmallFactorJob) * count, cudaMemcpyHostToDevice, s));
+    potrf_batch_array_kernel<<<hb::counted(count), COOP_THREADS, SM_DOUBLES * sizeof(double), s>>>(b.p);
+    return cudaGetLastError() == cudaSuccess;
 }
 
 bool chol_solve(cudaStream_t s, DenseFactor &F, const double *b, double *x) {

@@ -108,9 +108,10 @@ bool factor_status(cudaStream_t s, DenseFactor &F);
 // Enqueue the factorisations of F[q] (order <= kSmallFactorMaxN) of S[q] (ldS[q]) for
 // q < count, one CTA each, in launches of up to 36 of them: the arithmetic of
 // factorize_async on a grid of one block, which gives the same factor on any grid. Call
-// factor_status() (or factor_status_ready() after a wait) on each afterwards. Worth it for
-// several matrices of moderate order: one CTA takes about as long for order 256 as the
-// whole-GPU kernel, and many run at once.
+// factor_status() (or factor_status_ready() after a wait) on each afterwards, and wait for
+// the stream before the same host thread enqueues another batch. Worth it for several
+// matrices of moderate order: one CTA takes about as long for order 256 as the whole-GPU
+// kernel, and many run at once.
 constexpr int kSmallFactorMaxN = 1024;
 // the order up to which factor_buffers batches the cones' dense factorisations
 constexpr int kBatchFactorMaxN = 256;
