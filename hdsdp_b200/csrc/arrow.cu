@@ -32,6 +32,14 @@ struct BlkOp {
     int rows, cols, xoff, yoff, mode;
 };
 
+// One square block of the arrow (a local block, or the coupling block last) for the batched
+// diagonal and mirror operations: order l, its rows at packed offset off.
+struct BlkDiag {
+    double *A;
+    long ld;
+    int l, off;
+};
+
 struct ArrowSchur {
     int m = 0, nc = 0, ncone = 0;
     std::vector<int> lk;              // local rows per cone
@@ -39,10 +47,19 @@ struct ArrowSchur {
     std::vector<int> perm;            // packed index -> problem row
     std::vector<const SdpCone *> cone;
     std::vector<int *> d_code;        // per cone, per row of its list: local index, or -(coupling index + 1)
-    std::vector<double *> Mkk, Bk, Wk;   // Bk / Wk: column blocks of Ball / Wall
+    std::vector<double *> Mkk, Bk, Wk;   // Mkk: blocks of Mall; Bk / Wk: column blocks of Ball / Wall
+    double *Mall = nullptr;           // every local block, one after the other
+    size_t mallSize = 0;
+    BlkDiag *dblk = nullptr;          // the local blocks and the coupling block, for the batched
+    int ndblk = 0, maxdl = 0;         // diagonal and mirror operations
     double *Ball = nullptr, *Wall = nullptr;   // n_c x sum l_k: [B_1 ... B_K], [W_1 ... W_K]
     GemmDesc *wdesc = nullptr;        // W_k = B_k K_k^T for the blocks with local rows
     int nw = 0;
+    // the coupling update Wall Wall^T split along its inner dimension when M_cc is too small to
+    // keep the GPU busy: nsplit partial products (column chunks of Wall) into P
+    GemmDesc *sdesc = nullptr;
+    double *P = nullptr;
+    int nsplit = 0;
     std::vector<long> ldk;
     std::vector<DenseFactor> Fk;
     double *Mcc = nullptr, *Mcf = nullptr;
@@ -86,33 +103,60 @@ __global__ void arrow_scatter_kernel(int mk, const double *__restrict__ Msub, lo
 }
 
 void zero_blocks(cudaStream_t s, ArrowSchur &A) {
-    for (int k = 0; k < A.ncone; ++k) {
-        if (A.lk[k] == 0) continue;
-        HB_CUDA(cudaMemsetAsync(A.Mkk[k], 0, sizeof(double) * A.ldk[k] * A.lk[k], s));
-    }
+    if (A.mallSize > 0) HB_CUDA(cudaMemsetAsync(A.Mall, 0, sizeof(double) * A.mallSize, s));
     if (A.nc > 0 && A.off[A.ncone] > 0)
         HB_CUDA(cudaMemsetAsync(A.Ball, 0, sizeof(double) * A.ldb * A.off[A.ncone], s));
     if (A.nc > 0) HB_CUDA(cudaMemsetAsync(A.Mcc, 0, sizeof(double) * A.ldc * A.nc, s));
 }
 
-// diag (packed order) added to the diagonals of the blocks
-void add_diag_packed(cudaStream_t s, ArrowSchur &A, const double *d) {
-    for (int k = 0; k < A.ncone; ++k)
-        if (A.lk[k] > 0) add_diag_vec(s, A.lk[k], A.Mkk[k], A.ldk[k], d + A.off[k]);
-    if (A.nc > 0) add_diag_vec(s, A.nc, A.Mcc, A.ldc, d + A.off[A.ncone]);
+// on the diagonal of every block (blockIdx.y): op 0 reads it into out[off + i], op 1 adds v,
+// op 2 adds d[off + i]
+__global__ void arrow_diag_kernel(const BlkDiag *__restrict__ b, int op, double v, const double *__restrict__ d,
+                                  double *out) {
+    const BlkDiag B = b[blockIdx.y];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < B.l; i += gridDim.x * blockDim.x) {
+        double *p = B.A + (size_t) i * (B.ld + 1);
+        if (op == 0) out[B.off + i] = *p;
+        else if (op == 1) *p += v;
+        else *p += d[B.off + i];
+    }
 }
 
-void add_diag_all(cudaStream_t s, ArrowSchur &A, double v) {
-    for (int k = 0; k < A.ncone; ++k)
-        if (A.lk[k] > 0) add_diag(s, A.lk[k], A.Mkk[k], A.ldk[k], v);
-    if (A.nc > 0) add_diag(s, A.nc, A.Mcc, A.ldc, v);
+// A(j, i) = A(i, j), i > j, in every block (blockIdx.z), 32 x 32 tiles
+__global__ void arrow_mirror_kernel(const BlkDiag *__restrict__ b) {
+    const BlkDiag B = b[blockIdx.z];
+    const int i0 = blockIdx.x * 32, j0 = blockIdx.y * 32;
+    if (i0 >= B.l || j0 >= B.l || i0 + 31 < j0) return;
+    for (int e = threadIdx.x; e < 32 * 32; e += blockDim.x) {
+        const int i = i0 + (e & 31), j = j0 + (e >> 5);
+        if (i < B.l && j < B.l && i > j) B.A[(size_t) j + (size_t) i * B.ld] = B.A[(size_t) i + (size_t) j * B.ld];
+    }
+}
+
+void arrow_diag(cudaStream_t s, ArrowSchur &A, int op, double v, const double *d, double *out) {
+    if (A.ndblk == 0) return;
+    dim3 grd((A.maxdl + 255) / 256, A.ndblk);
+    arrow_diag_kernel<<<counted(grd), 256, 0, s>>>(A.dblk, op, v, d, out);
+    HB_CUDA(cudaGetLastError());
+}
+
+// diag (packed order) added to the diagonals of the blocks
+void add_diag_packed(cudaStream_t s, ArrowSchur &A, const double *d) { arrow_diag(s, A, 2, 0.0, d, nullptr); }
+
+void add_diag_all(cudaStream_t s, ArrowSchur &A, double v) { arrow_diag(s, A, 1, v, nullptr, nullptr); }
+
+// every block's lower triangle mirrored into its upper one
+void mirror_blocks(cudaStream_t s, ArrowSchur &A) {
+    if (A.ndblk == 0) return;
+    const int t = (A.maxdl + 31) / 32;
+    dim3 grd(t, t, A.ndblk);
+    arrow_mirror_kernel<<<counted(grd), 256, 0, s>>>(A.dblk);
+    HB_CUDA(cudaGetLastError());
 }
 
 // the diagonals of all blocks, packed, on the host
 void diag_to_host(cudaStream_t s, ArrowSchur &A, double *h_buf) {
-    for (int k = 0; k < A.ncone; ++k)
-        if (A.lk[k] > 0) copy_matrix(s, 1, A.lk[k], A.Mkk[k], A.ldk[k] + 1, A.t + A.off[k], 1);
-    if (A.nc > 0) copy_matrix(s, 1, A.nc, A.Mcc, A.ldc + 1, A.t + A.off[A.ncone], 1);
+    arrow_diag(s, A, 0, 0.0, nullptr, A.t);
     HB_CUDA(cudaMemcpyAsync(h_buf, A.t, sizeof(double) * A.m, cudaMemcpyDeviceToHost, s));
     HB_CUDA(cudaStreamSynchronize(s));
 }
@@ -231,6 +275,20 @@ void arrow_matvec(cudaStream_t s, ArrowSchur &A, const double *x, double *y) {
     }
 }
 
+// Mcf = Mcc - sum_s P_s over the lower triangle (P_s: nc x nc partial products, pitch ld,
+// one after the other), the partials subtracted in order
+__global__ void arrow_split_sum_kernel(int nc, int ns, const double *__restrict__ P, long ld,
+                                       const double *__restrict__ Mcc, double *Mcf, long ldc) {
+    const long total = (long) nc * nc;
+    for (long idx = blockIdx.x * (long) blockDim.x + threadIdx.x; idx < total; idx += (long) gridDim.x * blockDim.x) {
+        const int i = (int) (idx % nc), j = (int) (idx / nc);
+        if (i < j) continue;
+        double v = Mcc[(size_t) i + (size_t) j * ldc];
+        for (int q = 0; q < ns; ++q) v -= P[(size_t) q * ld * nc + (size_t) i + (size_t) j * ld];
+        Mcf[(size_t) i + (size_t) j * ldc] = v;
+    }
+}
+
 // the factors of the current blocks (W_k and the coupling block's Schur complement)
 bool arrow_factor_once(cudaStream_t s, ArrowSchur &A) {
     const int nc = A.nc, K = A.ncone;
@@ -261,9 +319,20 @@ bool arrow_factor_once(cudaStream_t s, ArrowSchur &A) {
     // W_k = B_k L_kk^-T = B_k K_k^T for every block in one launch, then
     // M_cc - sum_k W_k W_k^T = M_cc - Wall Wall^T as one product
     gemm_grouped(s, A.wdesc, A.nw, nc, A.maxl);
-    copy_matrix(s, nc, nc, A.Mcc, A.ldc, A.Mcf, A.ldc);
-    if (A.off[K] > 0)
-        gemm(s, nc, nc, A.off[K], -1.0, A.Wall, A.ldb, 0, A.Wall, A.ldb, 1, 1.0, A.Mcf, A.ldc, GEMM_C_LOWER);
+    if (A.nsplit > 0) {
+        // few coupling rows and many local ones: the product split along its inner dimension
+        // (one grouped launch, a partial product per column chunk), the partials subtracted from
+        // M_cc in chunk order
+        gemm_grouped(s, A.sdesc, A.nsplit, nc, nc);
+        const long total = (long) nc * nc;
+        arrow_split_sum_kernel<<<counted((int) std::min<long>((total + 255) / 256, 4096)), 256, 0, s>>>(
+            nc, A.nsplit, A.P, A.ldc, A.Mcc, A.Mcf, A.ldc);
+        HB_CUDA(cudaGetLastError());
+    } else {
+        copy_matrix(s, nc, nc, A.Mcc, A.ldc, A.Mcf, A.ldc);
+        if (A.off[K] > 0)
+            gemm(s, nc, nc, A.off[K], -1.0, A.Wall, A.ldb, 0, A.Wall, A.ldb, 1, 1.0, A.Mcf, A.ldc, GEMM_C_LOWER);
+    }
     if (!hb::factorize(s, A.Fc, A.Mcf, A.ldc)) return false;
     if (A.Fc.fuse_k) compute_inverse_factor(s, A.Fc);
     return true;
@@ -347,9 +416,18 @@ bool KKT::setup_arrow(const std::vector<SdpCone *> &cones) {
         const int l = A->lk[k];
         if (l == 0) continue;
         A->ldk[k] = pad_ld(l);
-        HB_CUDA(cmalloc(&A->Mkk[k], sizeof(double) * A->ldk[k] * l));
+        A->mallSize += (size_t) A->ldk[k] * l;
         A->Fk[k].alloc(l, 1);
         A->Fk[k].kfamily = KF_POTRF_SCHUR;
+    }
+    if (A->mallSize > 0) {
+        HB_CUDA(cmalloc(&A->Mall, sizeof(double) * A->mallSize));
+        size_t at = 0;
+        for (int k = 0; k < A->ncone; ++k) {
+            if (A->lk[k] == 0) continue;
+            A->Mkk[k] = A->Mall + at;
+            at += (size_t) A->ldk[k] * A->lk[k];
+        }
     }
     if (A->nc > 0 && A->off[A->ncone] > 0) {
         const size_t cols = (size_t) A->off[A->ncone];
@@ -367,12 +445,48 @@ bool KKT::setup_arrow(const std::vector<SdpCone *> &cones) {
         A->nw = (int) wd.size();
         HB_CUDA(cmalloc(&A->wdesc, sizeof(GemmDesc) * wd.size()));
         HB_CUDA(cudaMemcpyAsync(A->wdesc, wd.data(), sizeof(GemmDesc) * wd.size(), cudaMemcpyHostToDevice, s));
+        // split the coupling update when its 64 x 64 output tiles are few against the SMs and its
+        // inner dimension long: chunks of at least 512 columns, the partials within 256 MB
+        const long tiles = (long) ((A->nc + 63) / 64) * ((A->nc + 63) / 64);
+        const long kk = (long) cols;
+        if (tiles < 4L * device_sm_count() && kk >= 4096) {
+            long ns = std::min<long>(4L * device_sm_count() / std::max(tiles, 1L), kk / 512);
+            const long cap = (256L << 20) / (8L * A->ldc * A->nc);
+            ns = std::max(1L, std::min(ns, cap));
+            if (ns > 1) {
+                A->nsplit = (int) ns;
+                HB_CUDA(cmalloc(&A->P, sizeof(double) * A->ldc * A->nc * ns));
+                std::vector<GemmDesc> sd;
+                const long chunk = (kk + ns - 1) / ns;
+                for (long q = 0; q < ns; ++q) {
+                    const long c0 = q * chunk, c1 = std::min(kk, c0 + chunk);
+                    double *Pq = A->P + (size_t) q * A->ldc * A->nc;
+                    const double *Wq = A->Wall + (size_t) c0 * A->ldb;
+                    sd.push_back(GemmDesc{A->nc, A->nc, (int) (c1 - c0), 1.0, 0.0, Wq, A->ldb, 0, Wq, A->ldb, 1, Pq,
+                                          A->ldc, GEMM_C_LOWER, nullptr});
+                }
+                HB_CUDA(cmalloc(&A->sdesc, sizeof(GemmDesc) * sd.size()));
+                HB_CUDA(cudaMemcpyAsync(A->sdesc, sd.data(), sizeof(GemmDesc) * sd.size(), cudaMemcpyHostToDevice, s));
+            }
+        }
     }
     if (A->nc > 0) {
         HB_CUDA(cmalloc(&A->Mcc, sizeof(double) * A->ldc * A->nc));
         HB_CUDA(cmalloc(&A->Mcf, sizeof(double) * A->ldc * A->nc));
         A->Fc.alloc(A->nc, A->nc < kTriSolveMinM ? 1 : 0);
         A->Fc.kfamily = KF_POTRF_SCHUR;
+    }
+    {
+        std::vector<BlkDiag> bd;
+        for (int k = 0; k < A->ncone; ++k)
+            if (A->lk[k] > 0) bd.push_back(BlkDiag{A->Mkk[k], A->ldk[k], A->lk[k], A->off[k]});
+        if (A->nc > 0) bd.push_back(BlkDiag{A->Mcc, A->ldc, A->nc, A->off[A->ncone]});
+        A->ndblk = (int) bd.size();
+        for (const BlkDiag &b : bd) A->maxdl = std::max(A->maxdl, b.l);
+        if (!bd.empty()) {
+            HB_CUDA(cmalloc(&A->dblk, sizeof(BlkDiag) * bd.size()));
+            HB_CUDA(cudaMemcpyAsync(A->dblk, bd.data(), sizeof(BlkDiag) * bd.size(), cudaMemcpyHostToDevice, s));
+        }
     }
     for (double **p : {&A->b, &A->x, &A->r, &A->z, &A->t, &A->d_diag}) HB_CUDA(cmalloc(p, sizeof(double) * m));
     HB_CUDA(cmalloc_host(&A->hb_, sizeof(double) * m));
@@ -441,10 +555,13 @@ void KKT::release_arrow() {
     ArrowSchur &A = *arrow;
     auto f = [](void *p) { if (p) cache_free(p); };
     for (int k = 0; k < A.ncone; ++k) {
-        f(A.Mkk[k]);
         f(A.d_code[k]);
         A.Fk[k].release();
     }
+    f(A.Mall);
+    f(A.dblk);
+    f(A.sdesc);
+    f(A.P);
     f(A.Ball);
     f(A.Wall);
     f(A.wdesc);
@@ -503,9 +620,7 @@ void KKT::arrow_regularize(double reg) {
 
 bool KKT::arrow_factorize() {
     ArrowSchur &A = *arrow;
-    for (int k = 0; k < A.ncone; ++k)
-        if (A.lk[k] > 0) symmetrize_lower(s, A.lk[k], A.Mkk[k], A.ldk[k]);
-    if (A.nc > 0) symmetrize_lower(s, A.nc, A.Mcc, A.ldc);
+    mirror_blocks(s, A);
     A.shift = 0.0;
     bool ok = arrow_factor_once(s, A);
     if (!ok) {
