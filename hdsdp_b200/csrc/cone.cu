@@ -2094,6 +2094,18 @@ void Lanczos::init(int n_, cudaStream_t s_) {
     HB_CUDA(hb::cmalloc(&d_y, sizeof(double) * 2 * (maxdim + 1)));
     HB_CUDA(hb::cmalloc(&d_scal, sizeof(double) * 4));
     HB_CUDA(hb::cmalloc_host(&h_scal, sizeof(double) * 4));
+    HB_CUDA(hb::cmalloc_host(&h_yv, sizeof(double) * 2 * (maxdim + 1)));
+    auto mapped = [](double *h) {
+        double *d = nullptr;
+        if (cudaHostGetDevicePointer((void **) &d, h, 0) != cudaSuccess) {
+            cudaGetLastError();
+            d = nullptr;
+        }
+        return d;
+    };
+    dm_ab = mapped(h_ab);
+    dm_scal = mapped(h_scal);
+    dm_yv = mapped(h_yv);
     // Deterministic start and perturbation vectors: srand(n) then, per entry,
     // srand(rand()) and sqrt(sqrt(rand() % 1627)) * (rand() % 2 - 0.5)
     // (HLanczosIPrepare / HLanczosIPerturb, linalg/hdsdp_lanczos.c:33-53).
@@ -2126,6 +2138,8 @@ void Lanczos::release() {
     if (h_ab) hb::cache_free_host(h_ab);
     if (h_scal) hb::cache_free_host(h_scal);
     h_ab = h_scal = nullptr;
+    if (h_yv) hb::cache_free_host(h_yv);
+    h_yv = dm_ab = dm_scal = dm_yv = nullptr;
 }
 
 hdsdp_retcode Lanczos::solve(DenseFactor &F, const double *D, long ldD, double *maxStep, Timers *tm) {
@@ -2397,7 +2411,8 @@ bool lz_advance(LzRun &R) {
             yy[i] = R.evec[(size_t) i + (size_t) i1 * kp1];
             yy[kp1 + i] = R.evec[(size_t) i + (size_t) i2 * kp1];
         }
-        HB_CUDA(cudaMemcpyAsync(L.d_y, yy.data(), sizeof(double) * 2 * kp1, cudaMemcpyHostToDevice, L.s));
+        if (L.dm_yv) std::memcpy(L.h_yv, yy.data(), sizeof(double) * 2 * kp1);   // read by the kernel in place
+        else HB_CUDA(cudaMemcpyAsync(L.d_y, yy.data(), sizeof(double) * 2 * kp1, cudaMemcpyHostToDevice, L.s));
         return true;
     }
     return false;
@@ -2456,18 +2471,10 @@ void lanczos_small_batch(std::vector<LzTask> &tasks) {
     const size_t smem = small_lanczos_smem(maxn, maxdim);
     // device addresses of the pinned mirrors (alpha / beta and the Ritz residuals), which
     // the kernels write directly; a task without one gets copies
-    auto mapped = [](double *h) {
-        double *d = nullptr;
-        if (cudaHostGetDevicePointer((void **) &d, h, 0) != cudaSuccess) {
-            cudaGetLastError();
-            d = nullptr;
-        }
-        return d;
-    };
     std::vector<double *> hab(tasks.size()), hsc(tasks.size());
     for (size_t q = 0; q < tasks.size(); ++q) {
-        hab[q] = mapped(tasks[q].lz->h_ab);
-        hsc[q] = mapped(tasks[q].lz->h_scal);
+        hab[q] = tasks[q].lz->dm_ab;
+        hsc[q] = tasks[q].lz->dm_scal;
     }
     for (size_t b0 = 0; b0 < tasks.size(); b0 += kLzBatch) {
         const int nb = (int) std::min<size_t>(kLzBatch, tasks.size() - b0);
@@ -2509,7 +2516,8 @@ void lanczos_small_batch(std::vector<LzTask> &tasks) {
             for (int q = 0; q < nb; ++q) {
                 LzRun &R = *want[b0 + q];
                 Lanczos &L = *R.t->lz;
-                B.job[q] = LzRitzJob{R.t->F->K, R.t->D, L.V, L.d_y, L.warm, L.d_scal, hsc[R.t - tasks.data()],
+                B.job[q] = LzRitzJob{R.t->F->K, R.t->D, L.V, L.dm_yv ? L.dm_yv : L.d_y, L.warm, L.d_scal,
+                                     hsc[R.t - tasks.data()],
                                      R.t->F->ld, R.t->ldD, L.ld, R.eigMin1, L.n, R.kc + 1};
             }
             lanczos_small_ritz_batch_kernel<<<hb::counted(nb), 256, smem, s>>>(B);

@@ -57,6 +57,10 @@ struct Lanczos {
     double *d_scal = nullptr, *h_scal = nullptr;
     double *init_vec = nullptr, *pert_vec = nullptr;  // device, deterministic per n
     double *part = nullptr;   // per-block partial sums of the fused steps (2 x kLanczosMaxBlocks)
+    // pinned Ritz coefficients, and the device addresses of the pinned h_ab, h_scal and h_yv
+    // (null where the memory is not mapped), for the batched small-block runs
+    double *h_yv = nullptr;
+    double *dm_ab = nullptr, *dm_scal = nullptr, *dm_yv = nullptr;
     int nComputed = 0;
     // when set, the operator is built from this sparse factor of S instead of F
     HybridFactor *hyOp = nullptr;
