@@ -76,6 +76,7 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-precision-legs", action="store_true", help="skip the other-precision solves")
     ap.add_argument("--no-maxcut-leg", action="store_true", help="skip the MaxCut n=8000 leg")
+    ap.add_argument("--no-arrow-leg", action="store_true", help="skip the block-arrow multi-cone leg")
     ap.add_argument("--ref-budget", type=float, default=REF_BUDGET_S,
                     help="seconds of complete reference solves to time (--impl reference)")
     return ap.parse_args()
@@ -388,6 +389,25 @@ def maxcut_leg(api, instances, np):
     return out
 
 
+def arrow_leg(api, instances, np):
+    """The block-arrow Schur complement on problems made of sparse SDP cones: 60 cones of
+    order 90 (m = 27,100) and 250 cones (m = 112,600, whose dense Schur matrix and factor would
+    take 203 GB); one untimed solve, then two device-timed ones each."""
+    out = {}
+    for name in ("mb60_m27k", "mb250_m112k"):
+        prob = instances.multiblock_case(name)
+        api.solve_problem(prob)
+        rs = [api.solve_problem(prob) for _ in range(2)]
+        r = rs[-1]
+        info = r["sparse_schur"]
+        out[name] = {"m": prob.m, "cones": len(prob.cones), "unit": UNIT,
+                     "value": float(np.mean([x["timers"]["ipm_device"] for x in rs])),
+                     "iters": r["iters"], "status": r["status_after_check"], "pobj": r["pobj"], "dobj": r["dobj"],
+                     "dimacs_max": float(np.max(np.abs(r["errs"]))), "arrow": info["arrow"],
+                     "arrow_bytes": info["arrow_bytes"], "dense_bytes": info["dense_bytes"]}
+    return out
+
+
 def run_b200(args):
     rank, world, local_rank = dist_env()
     if world > 1 and "CUDA_VISIBLE_DEVICES" not in os.environ:
@@ -552,6 +572,9 @@ def run_b200(args):
     mc = None
     if rank == 0 and not args.no_maxcut_leg:
         mc = maxcut_leg(api, instances, np)
+    arrow = None
+    if rank == 0 and not args.no_arrow_leg:
+        arrow = arrow_leg(api, instances, np)
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -568,6 +591,7 @@ def run_b200(args):
                               "the library reads them on the host and uploads the presolved coefficients"},
         "roofline": roofline, "kernels": kernels, "cpu_baseline": cpu, "clocks": clk,
         "gpu_launches": launches, "wall_s": wall, "adjoint": adj, "precision_legs": legs, "maxcut_n8000": mc,
+        "block_arrow": arrow,
         "split_s": {k: t[k] for k in ("schur", "schur_factor", "schur_solve", "s_factor", "s_inverse",
                                       "lanczos", "assemble", "primal", "setup", "total")},
     }
