@@ -1983,7 +1983,7 @@ __global__ void lanczos_small_ritz_kernel(int n, const double *K, long ldk, cons
     lanczos_small_ritz_body(n, K, ldk, D, ldD, V, ldv, kp1, y, lam, warm, out);
 }
 
-// Several cones' small-block runs in one launch, one CTA each (the jobs by value).
+// Several cones' small-block runs in one launch, one CTA each.
 // hab / hout: device addresses of the host's pinned mirrors of ab / out, written directly
 // when set
 struct LzStepJob {
@@ -2001,15 +2001,12 @@ struct LzRitzJob {
 };
 constexpr int kLzBatch = 32;
 constexpr int kLzHostParallel = 8;   // cones from which the host replays run on several threads
-struct LzStepBatch {
-    LzStepJob job[kLzBatch];
+// the two small-block kernels over a job array in device memory (any number of cones) or
+// over at most kLzBatch jobs passed by value
+template <class Job> struct LzPack {
+    Job job[kLzBatch];
 };
-struct LzRitzBatch {
-    LzRitzJob job[kLzBatch];
-};
-
-__global__ void lanczos_small_batch_kernel(const LzStepBatch B) {
-    const LzStepJob &J = B.job[blockIdx.x];
+__device__ void lz_run(const LzStepJob &J) {
     lanczos_small_body(J.n, J.K, J.ldk, J.D, J.ldD, J.a, J.b, J.V, J.ldv, J.ab, J.maxdim);
     if (J.hab) {
         __threadfence_block();
@@ -2017,15 +2014,49 @@ __global__ void lanczos_small_batch_kernel(const LzStepBatch B) {
         for (int e = threadIdx.x; e < 2 * J.maxdim + 2; e += blockDim.x) J.hab[e] = J.ab[e];
     }
 }
-
-__global__ void lanczos_small_ritz_batch_kernel(const LzRitzBatch B) {
-    const LzRitzJob &J = B.job[blockIdx.x];
+__device__ void lz_run(const LzRitzJob &J) {
     lanczos_small_ritz_body(J.n, J.K, J.ldk, J.D, J.ldD, J.V, J.ldv, J.kp1, J.y, J.lam, J.warm, J.out);
     if (J.hout) {
         __threadfence_block();
         __syncthreads();
         if (threadIdx.x < 2) J.hout[threadIdx.x] = J.out[threadIdx.x];
     }
+}
+template <class Job> __global__ void lz_pack_kernel(const LzPack<Job> B) { lz_run(B.job[blockIdx.x]); }
+template <class Job> __global__ void lz_array_kernel(const Job *__restrict__ jobs) { lz_run(jobs[blockIdx.x]); }
+
+// one launch over every job: by value when they fit the parameters, else from a device copy
+// kept per host thread, device and job type (stream-ordered behind the launches before it)
+template <class Job> void lz_launch(cudaStream_t s, const std::vector<Job> &jobs, size_t smem) {
+    const int count = (int) jobs.size();
+    if (count == 0) return;
+    if (count <= kLzBatch) {
+        LzPack<Job> B;
+        for (int q = 0; q < count; ++q) B.job[q] = jobs[q];
+        lz_pack_kernel<Job><<<hb::counted(count), 256, smem, s>>>(B);
+        HB_CUDA(cudaGetLastError());
+        return;
+    }
+    struct Buf {
+        Job *p = nullptr;
+        size_t cap = 0;
+    };
+    thread_local Buf buf[kMaxDevices];
+    Buf &b = buf[current_device()];
+    if (b.cap < jobs.size()) {
+        if (b.p) hb::cache_free(b.p);
+        b.p = nullptr;
+        b.cap = 0;
+        HB_CUDA(hb::cmalloc(&b.p, sizeof(Job) * jobs.size()));
+        b.cap = jobs.size();
+    }
+    HB_CUDA(cudaMemcpyAsync(b.p, jobs.data(), sizeof(Job) * jobs.size(), cudaMemcpyHostToDevice, s));
+    lz_array_kernel<Job><<<hb::counted(count), 256, smem, s>>>(b.p);
+    HB_CUDA(cudaGetLastError());
+}
+template <class Job> void lz_allow_smem(int bytes) {
+    HB_CUDA(cudaFuncSetAttribute((const void *) lz_pack_kernel<Job>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    HB_CUDA(cudaFuncSetAttribute((const void *) lz_array_kernel<Job>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
 }
 
 // All eigenpairs of the symmetric tridiagonal matrix with diagonal d[0..n) and
@@ -2450,10 +2481,8 @@ void lanczos_small_batch(std::vector<LzTask> &tasks) {
     static std::atomic<unsigned long long> attr{0};
     once_per_device(attr, [] {
         const int bytes = (int) small_lanczos_smem(kSmallLanczosN, 30);
-        HB_CUDA(cudaFuncSetAttribute((const void *) lanczos_small_batch_kernel,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-        HB_CUDA(cudaFuncSetAttribute((const void *) lanczos_small_ritz_batch_kernel,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+        lz_allow_smem<LzStepJob>(bytes);
+        lz_allow_smem<LzRitzJob>(bytes);
     });
     for (LzTask &t : tasks) {
         t.ret = HDSDP_RETCODE_OK;
@@ -2472,23 +2501,17 @@ void lanczos_small_batch(std::vector<LzTask> &tasks) {
     // device addresses of the pinned mirrors (alpha / beta and the Ritz residuals), which
     // the kernels write directly; a task without one gets copies
     std::vector<double *> hab(tasks.size()), hsc(tasks.size());
+    std::vector<LzStepJob> steps(tasks.size());
     for (size_t q = 0; q < tasks.size(); ++q) {
-        hab[q] = tasks[q].lz->dm_ab;
-        hsc[q] = tasks[q].lz->dm_scal;
+        LzTask &t = tasks[q];
+        Lanczos &L = *t.lz;
+        hab[q] = L.dm_ab;
+        hsc[q] = L.dm_scal;
+        steps[q] = LzStepJob{t.F->K, t.D, L.nComputed == 0 ? nullptr : L.warm,
+                             L.nComputed == 0 ? L.init_vec : L.pert_vec, L.V, L.d_ab, hab[q], t.F->ld, t.ldD,
+                             L.ld, L.n, L.maxdim};
     }
-    for (size_t b0 = 0; b0 < tasks.size(); b0 += kLzBatch) {
-        const int nb = (int) std::min<size_t>(kLzBatch, tasks.size() - b0);
-        LzStepBatch B;
-        for (int q = 0; q < nb; ++q) {
-            LzTask &t = tasks[b0 + q];
-            Lanczos &L = *t.lz;
-            B.job[q] = LzStepJob{t.F->K, t.D, L.nComputed == 0 ? nullptr : L.warm,
-                                 L.nComputed == 0 ? L.init_vec : L.pert_vec, L.V, L.d_ab, hab[b0 + q], t.F->ld, t.ldD,
-                                 L.ld, L.n, L.maxdim};
-        }
-        lanczos_small_batch_kernel<<<hb::counted(nb), 256, smem, s>>>(B);
-        HB_CUDA(cudaGetLastError());
-    }
+    lz_launch(s, steps, smem);
     for (size_t q = 0; q < tasks.size(); ++q) {
         Lanczos &L = *tasks[q].lz;
         if (!hab[q])
@@ -2510,19 +2533,14 @@ void lanczos_small_batch(std::vector<LzTask> &tasks) {
     for (int q = 0; q < nrun; ++q)
         if (ask[q]) want.push_back(&runs[q]);
     while (!want.empty()) {
-        for (size_t b0 = 0; b0 < want.size(); b0 += kLzBatch) {
-            const int nb = (int) std::min<size_t>(kLzBatch, want.size() - b0);
-            LzRitzBatch B;
-            for (int q = 0; q < nb; ++q) {
-                LzRun &R = *want[b0 + q];
-                Lanczos &L = *R.t->lz;
-                B.job[q] = LzRitzJob{R.t->F->K, R.t->D, L.V, L.dm_yv ? L.dm_yv : L.d_y, L.warm, L.d_scal,
-                                     hsc[R.t - tasks.data()],
-                                     R.t->F->ld, R.t->ldD, L.ld, R.eigMin1, L.n, R.kc + 1};
-            }
-            lanczos_small_ritz_batch_kernel<<<hb::counted(nb), 256, smem, s>>>(B);
-            HB_CUDA(cudaGetLastError());
+        std::vector<LzRitzJob> ritz(want.size());
+        for (size_t q = 0; q < want.size(); ++q) {
+            LzRun &R = *want[q];
+            Lanczos &L = *R.t->lz;
+            ritz[q] = LzRitzJob{R.t->F->K, R.t->D, L.V, L.dm_yv ? L.dm_yv : L.d_y, L.warm, L.d_scal,
+                                hsc[R.t - tasks.data()], R.t->F->ld, R.t->ldD, L.ld, R.eigMin1, L.n, R.kc + 1};
         }
+        lz_launch(s, ritz, smem);
         for (LzRun *R : want) {
             Lanczos &L = *R->t->lz;
             if (!hsc[R->t - tasks.data()])
@@ -2544,10 +2562,11 @@ void lanczos_small_batch(std::vector<LzTask> &tasks) {
             if (again[q]) next.push_back(want[q]);
         want.swap(next);
     }
+    if (tm)
+        for (const LzRun &R : runs) tm->lz_host += R.host_s;
     for (LzTask &t : tasks)
         if (t.ret == HDSDP_RETCODE_OK) t.lz->nComputed += 1;
     if (tm) {
-        for (const LzRun &R : runs) tm->lz_host += R.host_s;
         tm->lanczos += wall() - t0;
         tm->n_lanczos += (long) tasks.size();
     }
