@@ -20,7 +20,7 @@ EXPORTS = [
     "HUserDataCreate", "HUserDataSetConeData", "HUserDataChooseCone", "HUserDataClear",
     "HUserDataDestroy",
     "HDSDPGetStatus", "HDSDPGetIterCount", "HDSDPSetPrimalRefinement", "HDSDPSetPrecision",
-    "HDSDPSetSparseSlack", "HDSDPGetSparseSlackInfo", "HDSDPSetSparseSchur", "HDSDPGetSparseSchurInfo",
+    "HDSDPSetSparseSlack", "HDSDPGetSparseSlackInfo", "HDSDPSetSparseSchur", "HDSDPGetSparseSchurInfo", "HDSDPSetSchurLDL", "hdsdpb_ldl_solve",
     "hdsdpb_sparse_analyse",
     "hdsdpb_sparse_cholesky", "hdsdpb_sparse_congruence",
     "HDSDPGetIterLog", "HDSDPGetTimers", "HDSDPAdjoint",
@@ -78,6 +78,8 @@ def load():
         "HDSDPGetSparseSlackInfo": ([vp, dp], None),
         "HDSDPSetSparseSchur": ([vp, i], None),
         "HDSDPGetSparseSchurInfo": ([vp, dp], None),
+        "HDSDPSetSchurLDL": ([vp, i], None),
+        "hdsdpb_ldl_solve": ([i, dp, dp, dp, ip], i),
         "hdsdpb_sparse_analyse": ([i, i, ip, ip, i, dp, ip], i),
         "hdsdpb_sparse_cholesky": ([i, i, ip, ip, dp, i, i, dp], i),
         "hdsdpb_sparse_congruence": ([i, i, ip, ip, dp, dp, dp, dp, dp], i),

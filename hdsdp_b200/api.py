@@ -142,6 +142,11 @@ class Solver:
         1 block arrow (per-cone local blocks and a coupling block)."""
         self.L.HDSDPSetSparseSchur(self.h, int(mode))
 
+    def set_schur_ldl(self, mode: int):
+        """Factorisation of the dense Schur complement: 0 Cholesky (LDL^T with Bunch-Kaufman
+        pivoting when the Cholesky fails even with diagonal shifts), 1 LDL^T always."""
+        self.L.HDSDPSetSchurLDL(self.h, int(mode))
+
     def sparse_schur_info(self) -> dict:
         o = np.zeros(6)
         self.L.HDSDPGetSparseSchurInfo(self.h, _dp(o))
@@ -229,7 +234,7 @@ class Solver:
 
 
 def solve(inst, want_x: bool = True, primal_refinement: bool = True, precision: int = 0,
-          params: dict | None = None, lp=None, sparse_slack: int = -1) -> dict:
+          params: dict | None = None, lp=None, sparse_slack: int = -1, schur_ldl: int = 0) -> dict:
     """Solve ``inst`` on the GPU (with the LP cone ``lp`` = (n_lp, Ap, Ai, Ax) as cone 1 when
     given); returns the oracle driver's fields plus the iteration log."""
     s = Solver()
@@ -243,6 +248,7 @@ def solve(inst, want_x: bool = True, primal_refinement: bool = True, precision: 
         s.set_primal_refinement(primal_refinement)
         s.set_precision(precision)
         s.set_sparse_slack(sparse_slack)
+        s.set_schur_ldl(schur_ldl)
         for k, v in (params or {}).items():
             if isinstance(v, int):
                 s.set_int_param(k, v)
@@ -268,7 +274,7 @@ def solve(inst, want_x: bool = True, primal_refinement: bool = True, precision: 
 
 
 def solve_problem(prob, primal_refinement: bool = True, precision: int = 0, params: dict | None = None,
-                  sparse_slack: int = -1, sparse_schur: int = -1) -> dict:
+                  sparse_slack: int = -1, sparse_schur: int = -1, schur_ldl: int = 0) -> dict:
     """Solve a multi-cone problem (instances.ConicProblem: SDP blocks and LP cones over one
     set of constraints) on the GPU; returns y, objectives, status, iterations, the iteration
     log, DIMACS errors and per cone (X, S) or (x, s)."""
@@ -283,6 +289,7 @@ def solve_problem(prob, primal_refinement: bool = True, precision: int = 0, para
         s.set_precision(precision)
         s.set_sparse_slack(sparse_slack)
         s.set_sparse_schur(sparse_schur)
+        s.set_schur_ldl(schur_ldl)
         for k, v in (params or {}).items():
             if isinstance(v, int):
                 s.set_int_param(k, v)

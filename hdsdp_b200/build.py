@@ -11,7 +11,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libhdsdp_b200.so")
-SOURCES = ["la.cu", "chol.cu", "sdp.cu", "split.cu", "cone.cu", "solver.cu", "ext.cu", "adjoint.cu", "noalloc.cu", "lp.cu", "conic.cu", "sparse_chol.cu", "arrow.cu", "file_io.cpp"]
+SOURCES = ["la.cu", "chol.cu", "sdp.cu", "split.cu", "cone.cu", "solver.cu", "ext.cu", "adjoint.cu", "noalloc.cu", "lp.cu", "conic.cu", "sparse_chol.cu", "arrow.cu", "ldl.cu", "file_io.cpp"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
               "-Xcompiler", "-fPIC", "-Xcompiler", "-fopenmp", "-shared", "-cudart", "static", "-diag-suppress", "550",
               "-lgomp"]

@@ -1016,6 +1016,8 @@ void KKT::release() {
     Msub = nullptr;
     msubCap = 0;
     F.release();
+    ldl.release();
+    ldlActive = false;
     for (double **p : {&d_rhs, &d_x, &d_r, &d_t, &d_diag}) {
         if (*p) hb::cache_free(*p);
         *p = nullptr;
@@ -1403,10 +1405,18 @@ hdsdp_retcode KKT::factorize() {
     }
     symmetrize_lower(s, m, M, ldm);
     shift = 0.0;
+    ldlActive = false;
+    if (ldlMode == 1) {
+        const bool ok = ldl_factorize(s, ldl, M, ldm, m);
+        ldlActive = ok;
+        if (tm) tm->schur_factor += wall() - t0;
+        return ok && !device_error_flag() ? HDSDP_RETCODE_OK : HDSDP_RETCODE_FAILED;
+    }
     bool ok = hb::factorize(s, F, M, ldm);
     if (!ok) {
         // The reference switches to an LDL^T factorisation here (linsolver.c:1373-1377);
-        // this library retries the Cholesky with a small diagonal shift instead.
+        // this library first retries the Cholesky with a small diagonal shift, and takes
+        // the LDL^T factor of the unshifted M when every shift fails.
         copy_matrix(s, 1, m, M, ldm + 1, d_t, 1);
         HB_CUDA(cudaMemcpyAsync(h_buf, d_t, sizeof(double) * m, cudaMemcpyDeviceToHost, s));
         HB_CUDA(cudaStreamSynchronize(s));
@@ -1417,7 +1427,17 @@ hdsdp_retcode KKT::factorize() {
             shift += eps * std::max(mx, 1.0);
             ok = hb::factorize(s, F, M, ldm);
         }
-        if (ok) printf("KKT system is almost indefinite. Using a shifted Cholesky factor. \n");
+        if (ok) {
+            printf("KKT system is almost indefinite. Using a shifted Cholesky factor. \n");
+        } else {
+            copy_matrix(s, 1, m, d_t, 1, M, ldm + 1);   // the unshifted diagonal back
+            shift = 0.0;
+            ok = ldl_factorize(s, ldl, M, ldm, m);
+            ldlActive = ok;
+            if (ok) printf("KKT system is almost indefinite. Switch to LDL. \n");
+            if (tm) tm->schur_factor += wall() - t0;
+            return ok && !device_error_flag() ? HDSDP_RETCODE_OK : HDSDP_RETCODE_FAILED;
+        }
     }
     if (ok && F.fuse_k) compute_inverse_factor(s, F);
     HB_CUDA(cudaStreamSynchronize(s));
@@ -1438,6 +1458,21 @@ hdsdp_retcode KKT::solve(const double *rhs, double *lhs) {
     }
     std::memcpy(h_buf, rhs, sizeof(double) * m);
     HB_CUDA(cudaMemcpyAsync(d_rhs, h_buf, sizeof(double) * m, cudaMemcpyHostToDevice, s));
+    if (ldlActive) {
+        ldl_solve(s, ldl, d_rhs, d_x);
+        HB_CUDA(cudaMemcpyAsync(d_r, d_rhs, sizeof(double) * m, cudaMemcpyDeviceToDevice, s));
+        coldot(s, m, m, M, ldm, d_x, d_r, -1.0, 1.0, 0);   // r = b - M x
+        ldl_solve(s, ldl, d_r, d_r);
+        axpy(s, m, 1.0, d_r, d_x);
+        HB_CUDA(cudaMemcpyAsync(h_buf, d_x, sizeof(double) * m, cudaMemcpyDeviceToHost, s));
+        HB_CUDA(cudaStreamSynchronize(s));
+        std::memcpy(lhs, h_buf, sizeof(double) * m);
+        if (tm) {
+            tm->schur_solve += wall() - t0;
+            tm->n_schur_solve += 1;
+        }
+        return device_error_flag() ? HDSDP_RETCODE_FAILED : HDSDP_RETCODE_OK;
+    }
     bool ok = true;
     if (F.fuse_k) {
         coldot(s, m, m, F.KT, F.ld, d_rhs, d_t, 1.0, 0.0, 2);   // t = K b

@@ -19,6 +19,7 @@ void HDSDPSetPrecision(hdsdp *h, int mode) { h->precision = mode; }
 void HDSDPSetSparseSlack(hdsdp *h, int mode) { h->sparseSlack = mode; }
 void HDSDPSetSparseSchur(hdsdp *h, int mode) { h->sparseSchur = mode; }
 void HDSDPGetSparseSchurInfo(hdsdp *h, double out[6]) { h->kkt.arrow_info(out); }
+void HDSDPSetSchurLDL(hdsdp *h, int mode) { h->schurLdl = (mode == 1) ? 1 : 0; }
 
 // Host only (no device work): the ordering of the sparse factorisation of S for the
 // pattern of nedge off-diagonal pairs (ei[k], ej[k]) with degree cap `cap`.
@@ -377,6 +378,62 @@ int hdsdpb_sparse_congruence(int n, int nedge, const int *ei, const int *ej, con
     cudaStreamDestroy(s);
     if (device_error_flag()) return -1;
     return ok ? 0 : 1;
+}
+
+int hdsdpb_ldl_solve(int n, const double *S, const double *b, double *x, int out[3]) {
+    if (n < 0 || (n > 0 && (!S || !b || !x))) return -1;
+    if (out) out[0] = out[1] = out[2] = 0;
+    if (n == 0) return 0;
+    cudaStream_t s;
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return -1;
+    const long ld = pad_ld(n);
+    double *dS = nullptr, *dx = nullptr;
+    hb::cmalloc(&dS, sizeof(double) * ld * n);
+    hb::cmalloc(&dx, sizeof(double) * n);
+    cudaMemcpy2D(dS, sizeof(double) * ld, S, sizeof(double) * n, sizeof(double) * n, n, cudaMemcpyHostToDevice);
+    cudaMemcpy(dx, b, sizeof(double) * n, cudaMemcpyHostToDevice);
+    legacy_fence();
+    LdlFactor F;
+    const bool ok = ldl_factorize(s, F, dS, ld, n);
+    int ret = ok ? 0 : (F.h_info ? reinterpret_cast<int *>(F.h_info)[0] : -1);
+    if (!ok && ret <= 0) ret = -1;
+    if (ok) {
+        ldl_solve(s, F, dx, dx);
+        cudaMemcpyAsync(x, dx, sizeof(double) * n, cudaMemcpyDeviceToHost, s);
+        if (out) {
+            // the inertia of S from the blocks of D
+            std::vector<int> piv(n);
+            std::vector<double> dg(n), sub(n, 0.0);
+            cudaMemcpyAsync(piv.data(), F.piv, sizeof(int) * n, cudaMemcpyDeviceToHost, s);
+            cudaMemcpy2DAsync(dg.data(), sizeof(double), F.A, sizeof(double) * (F.ld + 1), sizeof(double), n,
+                              cudaMemcpyDeviceToHost, s);
+            if (n > 1)
+                cudaMemcpy2DAsync(sub.data(), sizeof(double), F.A + 1, sizeof(double) * (F.ld + 1), sizeof(double),
+                                  n - 1, cudaMemcpyDeviceToHost, s);
+            cudaStreamSynchronize(s);
+            for (int i = 0; i < n; ++i) {
+                if (piv[i] == 1) {
+                    (dg[i] < 0.0 ? out[1] : out[2]) += 1;
+                } else if (piv[i] == 2 && i + 1 < n) {
+                    out[0] += 1;
+                    const double det = dg[i] * dg[i + 1] - sub[i] * sub[i];
+                    if (det < 0.0) {
+                        out[1] += 1;
+                        out[2] += 1;
+                    } else {
+                        (dg[i] + dg[i + 1] < 0.0 ? out[1] : out[2]) += 2;
+                    }
+                }
+            }
+        }
+    }
+    cudaStreamSynchronize(s);
+    F.release();
+    hb::cache_free(dS);
+    hb::cache_free(dx);
+    cudaStreamDestroy(s);
+    if (device_error_flag()) return -1;
+    return ret;
 }
 
 int hdsdpb_cholesky_solve(int n, const double *S, const double *b, double *x) {

@@ -50,6 +50,27 @@ void gemm_grouped(cudaStream_t s, const GemmDesc *d_desc, int count, int maxM, i
 void coldot(cudaStream_t s, int nrows, int ncols, const double *A, long lda, const double *x,
             double *out, double alpha, double beta, int mode);
 
+// Symmetric indefinite factorisation P S P^T = L D L^T (Bunch-Kaufman pivoting, ldl.cu).
+// A holds D's 1 x 1 and 2 x 2 blocks on and below the diagonal and L^T strictly above it;
+// perm the symmetric permutation, piv the pivot size at the first index of each block
+// (1 or 2; -1 at the second index of a 2 x 2 block).
+constexpr int kMaxLdlGrid = 1024;
+struct LdlFactor {
+    int n = 0;
+    long ld = 0;
+    double *A = nullptr;
+    int *perm = nullptr, *piv = nullptr, *d_info = nullptr;
+    double *cm = nullptr, *part = nullptr, *w = nullptr;
+    double *h_info = nullptr;   // pinned: the info word (0, or the step whose pivot column is zero or NaN)
+    bool ok = false;
+    void release();
+};
+// Factor the full symmetric n x n matrix S (leading dimension ldS; only its lower triangle
+// is read); waits for the stream. False for an exactly singular or non-finite pivot.
+bool ldl_factorize(cudaStream_t s, LdlFactor &F, const double *S, long ldS, int n);
+// x = S^-1 b (device vectors; x may alias b), enqueued on s.
+void ldl_solve(cudaStream_t s, LdlFactor &F, const double *b, double *x);
+
 // Factor object for an n x n symmetric positive definite matrix.
 // L holds the lower Cholesky factor, Dinv the inverses of its 64 x 64
 // diagonal blocks, K = L^-1 and KT = L^-T (computed on demand).

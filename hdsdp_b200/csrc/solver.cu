@@ -1806,8 +1806,10 @@ hdsdp_retcode HDSDPOptimize(hdsdp *h, int dOptOnly) {
             HB_CUDA(hb::cmalloc(&h->d_yall, sizeof(double) * std::max(h->nRows, 1)));
             HB_CUDA(hb::cmalloc_host(&h->h_yall, sizeof(double) * std::max(h->nRows, 1)));
         }
-        const bool useArrow = allSparse && arrow_chosen(h->sparseSchur, h->nRows, sp);
+        // (an LDL^T factorisation asked for applies to the dense M)
+        const bool useArrow = allSparse && h->schurLdl != 1 && arrow_chosen(h->sparseSchur, h->nRows, sp);
         h->kkt.init(h->nRows, h->stream, &h->timers, !useArrow);
+        h->kkt.ldlMode = h->schurLdl;
         if (useArrow && !h->kkt.setup_arrow(sp)) {
             retcode = HDSDP_RETCODE_MEMORY;
             goto exit_cleanup;

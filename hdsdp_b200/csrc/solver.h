@@ -294,6 +294,12 @@ struct KKT {
     double *h_buf = nullptr;
     std::vector<double> diag_add;     // bound-cone diagonal accumulated before factorisation
     double shift = 0.0;               // diagonal shift applied if the Cholesky of M failed
+    // LDL^T (Bunch-Kaufman) factor of M: taken when the Cholesky fails even with the shift
+    // retries (ldlMode 0) or for every factorisation (ldlMode 1); ldlActive while the current
+    // factor is this one
+    LdlFactor ldl;
+    int ldlMode = 0;
+    bool ldlActive = false;
     const double *primalX = nullptr;  // device X for KKT_TYPE_PRIMAL
     Timers *tm = nullptr;
     // M holds a partial sum of the current build (false after clean: the first dense SDP
@@ -397,6 +403,7 @@ struct hdsdp_solver_internal {
     int precision = 0;
     int sparseSlack = -1;          // factorisation of S in PSD checks: -1 trial points sparse (automatic), 0 dense, 1 sparse
     int sparseSchur = -1;          // Schur complement form: -1 automatic, 0 dense, 1 block arrow when every cone is a sparse SDP cone
+    int schurLdl = 0;              // Schur factorisation: 0 Cholesky (LDL^T when it fails), 1 LDL^T
     int verbose = 0;
     std::vector<hb::IterRecord> log;
     std::string modelFeatures;

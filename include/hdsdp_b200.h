@@ -64,6 +64,14 @@ extern void HDSDPSetSparseSchur( hdsdp *HSolver, int mode );
    its factor would take. */
 extern void HDSDPGetSparseSchurInfo( hdsdp *HSolver, double out[6] );
 
+/* Factorisation of the dense Schur complement M. 0 (default) = Cholesky; when it fails,
+   retried with diagonal shifts up to 1e-6 of the largest diagonal entry, and when every
+   shift fails, the LDL^T factorisation with Bunch-Kaufman pivoting of the unshifted M (the
+   indefinite solver the reference switches to, linalg/hdsdp_linsolver.c:1367-1380). 1 =
+   LDL^T for every factorisation of M (the block-arrow form is then not used). Takes effect
+   at the next HDSDPOptimize. */
+extern void HDSDPSetSchurLDL( hdsdp *HSolver, int mode );
+
 /* Per-iteration record of the last solve: elapsed seconds, primal and dual
    objective, barrier parameter, relative gap (p - d) / (1 + |p| + |d|) and
    phase (0 infeasible, 1 embedding, 2 potential reduction, 3 refinement),
@@ -162,6 +170,14 @@ extern int hdsdpb_cholesky_batch( int count, int n, int mode, const double *S, d
    solver uses it for Schur systems of order >= 6000). Returns 0 on success, 1 if S is
    not positive definite, -1 on error. */
 extern int hdsdpb_cholesky_solve( int n, const double *S, const double *b, double *x );
+
+/* Solution of S x = b for a symmetric, possibly indefinite S (n x n, column-major, only
+   its lower triangle read) through P S P^T = L D L^T with Bunch-Kaufman pivoting (the
+   reference's dsytrf / dsytrs use, linalg/hdsdp_linsolver.c:1118-1190). out (may be NULL):
+   {2 x 2 pivots, negative eigenvalues, positive eigenvalues} of D, the inertia of S.
+   Returns 0 on success, k > 0 if the pivot column of step k is zero (S singular) or not
+   finite, -1 on error. */
+extern int hdsdpb_ldl_solve( int n, const double *S, const double *b, double *x, int out[3] );
 
 /* Allocation-free variant of hdsdpb_cholesky (no reference counterpart), for callers
    that cannot call cudaMalloc on their call path (a host framework whose allocator
