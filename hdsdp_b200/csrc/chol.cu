@@ -15,6 +15,7 @@
 #include <mutex>
 #include <algorithm>
 #include <vector>
+#include <utility>
 
 namespace cg = cooperative_groups;
 
@@ -537,12 +538,13 @@ __device__ __forceinline__ void k_final_tile(const double *Dinv, long ldd, doubl
 }
 
 // The factorisation on a grid of ngrid blocks, this one being block bid; gsync() is the
-// grid-wide barrier. The cooperative kernel runs it on its grid; a batched launch runs it
-// with one block per matrix (bid 0, ngrid 1, gsync a block barrier). Every tile is computed
-// by the same operations whatever the grid, so the result does not depend on it.
-template <class GSync>
+// grid-wide barrier, garrive() / gwait(token) its two halves. The cooperative kernel runs it
+// on its grid; a batched launch runs it with one block per matrix (bid 0, ngrid 1, gsync a
+// block barrier). Every tile is computed by the same operations whatever the grid, so the
+// result does not depend on it.
+template <class GSync, class GArrive, class GWait>
 __device__ void potrf_body(double *L, long ld, int n, double *Dinv, long ldd, int *info, double *K, double *KT,
-                           int bid, int ngrid, GSync gsync, double *sm) {
+                           int bid, int ngrid, GSync gsync, GArrive garrive, GWait gwait, double *sm) {
     const int nblk = (n + 63) / 64;
     if (bid == 0) potf2_dev(L, ld, 0, min(NB, n), Dinv, ldd, info, sm);
     gsync();
@@ -576,7 +578,13 @@ __device__ void potrf_body(double *L, long ld, int n, double *Dinv, long ldd, in
             }
         }
         if (bid <= 1) CHOL_STAMP(pb + 1);
-        gsync();
+        // block 0 goes on to the next diagonal block, which needs only what it holds itself
+        // (its solved chunk 0 and the staged block): it arrives at the barrier without waiting,
+        // and waits for it only after that factorisation
+        const bool early = (bid == 0 && ngrid > 1);
+        unsigned int tok = 0;
+        if (early) tok = garrive();
+        else gsync();
         if (bid <= 1) CHOL_STAMP(pb + 2);
         const long ntile = (long) nchunk * (nchunk + 1) / 2;
         const long nk = K ? bj + 1 : 0;
@@ -587,6 +595,7 @@ __device__ void potrf_body(double *L, long ld, int n, double *Dinv, long ldd, in
             potf2_dev(L, ld, j0 + nb, nbn, Dinv, ldd, info, sm, nullptr, 0, true);
             CHOL_STAMP(pb + 4);
         }
+        if (early) gwait(tok);
         // remaining tiles (and K's block row bj), spread over the other blocks
         // (block 0 joins when the grid has one block)
         const int nworker = (ngrid > 1) ? (int) ngrid - 1 : 1;
@@ -621,7 +630,9 @@ __global__ void __launch_bounds__(COOP_THREADS, 1) potrf_coop_kernel(double *L, 
                                                                   long ldd, int *info, double *K, double *KT) {
     cg::grid_group grid = cg::this_grid();
     extern __shared__ double sm[];
-    potrf_body(L, ld, n, Dinv, ldd, info, K, KT, (int) blockIdx.x, (int) gridDim.x, [&]() { grid.sync(); }, sm);
+    potrf_body(
+        L, ld, n, Dinv, ldd, info, K, KT, (int) blockIdx.x, (int) gridDim.x, [&]() { grid.sync(); },
+        [&]() { return grid.barrier_arrive(); }, [&](unsigned int t) { grid.barrier_wait(std::move(t)); }, sm);
 }
 
 // Several factorisations in one launch, one CTA each: the copy of the lower triangle, the
@@ -676,7 +687,13 @@ __device__ void small_factor_job(const SmallFactorJob &J, double *sm) {
     if (threadIdx.x == 0) *J.info = 0;
     __threadfence_block();
     __syncthreads();
-    potrf_body(J.L, J.ld, n, J.Dinv, J.ld, J.info, J.K, J.KT, 0, 1, []() { __syncthreads(); }, sm);
+    potrf_body(
+        J.L, J.ld, n, J.Dinv, J.ld, J.info, J.K, J.KT, 0, 1, []() { __syncthreads(); },
+        []() {
+            __syncthreads();
+            return 0u;
+        },
+        [](unsigned int) {}, sm);
     __syncthreads();
     double acc = 0.0;
     if (J.logdet) {
