@@ -4,7 +4,7 @@
     python tests/golden/make_golden.py --add GROUP [GROUP ...]
 
 --add runs only the named groups (EXTRA below) and merges their results into
-the existing fixtures: "north_star" (MaxCut n=8000 and the theta layer n=200,
+the existing fixtures: "maxcut_theta" (MaxCut n=8000 and the theta layer n=200,
 primal refinement off; a few minutes), "stock" (the sparse-dual instances on
 the reference build with its own dual-storage rule), "hsd" (instances that end
 in the homogeneous self-dual embedding), "dense" (general dense coefficients),
@@ -63,7 +63,7 @@ FULL = {
 
 
 # Groups generated on demand (--add) and merged into the fixtures.
-NORTH_STAR = {
+MAXCUT_THETA = {
     "maxcut_n8000": lambda: instances.WORKLOADS["maxcut_n8000"](),
     "theta_adjoint_n200": lambda: instances.WORKLOADS["theta_adjoint_n200"](),
 }
@@ -71,8 +71,8 @@ STOCK = {
     "maxcut60": SMALL["maxcut60"],
     "maxcut200": SMALL["maxcut200"],
     "theta_adj40": SMALL["theta_adj40"],
-    "theta_adjoint_n200": NORTH_STAR["theta_adjoint_n200"],
-    "maxcut_n8000": NORTH_STAR["maxcut_n8000"],
+    "theta_adjoint_n200": MAXCUT_THETA["theta_adjoint_n200"],
+    "maxcut_n8000": MAXCUT_THETA["maxcut_n8000"],
 }
 HSD = {
     "dinf8": lambda: instances.dual_infeasible(8, seed=1),
@@ -98,8 +98,8 @@ def add_groups(groups):
     out = json.load(open(gpath))
     arrays = dict(np.load(apath))
     for g in groups:
-        if g == "north_star":
-            for name, make in NORTH_STAR.items():
+        if g == "maxcut_theta":
+            for name, make in MAXCUT_THETA.items():
                 inst = make()
                 r = ref_api.solve(inst, want_x=False, params={4: 0})
                 key = "%s/psdp0" % name

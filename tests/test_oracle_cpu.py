@@ -138,7 +138,7 @@ def test_hsd_fixtures_end_in_the_embedding(golden):
         assert sol["iters"] > 20, key
 
 
-def test_north_star_reference_results(golden):
+def test_maxcut_and_theta_layer_reference_results(golden):
     """Full reference solves of MaxCut n=8000 and the theta layer n=200 (primal refinement
     off), with both dual-storage rules: optimal, and the two storage rules agree."""
     for name in ("maxcut_n8000", "theta_adjoint_n200"):

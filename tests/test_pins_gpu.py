@@ -20,7 +20,7 @@ import numpy as np
 import pytest
 
 from hdsdp_b200 import api, instances
-from make_golden import DENSE, HSD, NORTH_STAR, STOCK, probe_point
+from make_golden import DENSE, HSD, MAXCUT_THETA, STOCK, probe_point
 from test_solve_gpu import OPTIMAL, check_parity
 
 pytestmark = pytest.mark.gpu
@@ -35,7 +35,7 @@ def _y_close(r, y_ref):
 def test_maxcut_n8000_parity(gpu_lib, sparse_slack, golden, golden_arrays):
     """MaxCut n=8000 with the sparse dual-slack factorisation on trial points (default) and
     with dense factorisations only, against the reference's dense-storage solve."""
-    inst = NORTH_STAR["maxcut_n8000"]()
+    inst = MAXCUT_THETA["maxcut_n8000"]()
     r = api.solve(inst, want_x=False, primal_refinement=False, sparse_slack=sparse_slack)
     ref = golden["solves"]["maxcut_n8000/psdp0"]
     check_parity(r, ref)
@@ -46,14 +46,14 @@ def test_maxcut_n8000_parity(gpu_lib, sparse_slack, golden, golden_arrays):
 def test_maxcut_n8000_stock_parity(gpu_lib, golden, golden_arrays):
     """The default solve against the reference on its own path: sparse dual storage,
     factored through the Pardiso interface (linalg/hdsdp_linsolver.c:47-450)."""
-    inst = NORTH_STAR["maxcut_n8000"]()
+    inst = MAXCUT_THETA["maxcut_n8000"]()
     r = api.solve(inst, want_x=False, primal_refinement=False)
     check_parity(r, golden["solves_stock"]["maxcut_n8000/psdp0"])
     _y_close(r, golden_arrays["y_stock/maxcut_n8000/psdp0"])
 
 
 def test_theta_adjoint_n200_parity(gpu_lib, golden, golden_arrays):
-    inst = NORTH_STAR["theta_adjoint_n200"]()
+    inst = MAXCUT_THETA["theta_adjoint_n200"]()
     r = api.solve(inst, want_x=False, primal_refinement=False)
     check_parity(r, golden["solves"]["theta_adjoint_n200/psdp0"])
     _y_close(r, golden_arrays["y/theta_adjoint_n200/psdp0"])
