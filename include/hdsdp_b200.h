@@ -85,7 +85,7 @@ extern int HDSDPGetIterLog( hdsdp *HSolver, int maxLen, double *t, double *pObj,
    [4] S inverse       [5] Lanczos              [6] S assembly    [7] primal recovery
    [8] total           [9] #Schur builds       [10] #S factorisations
    [11] #Lanczos runs  [12] #Lanczos matvecs    [13] #Schur solves
-   [14] Lanczos: L^-1  [15] Lanczos: host eigen [16] Lanczos: device wait
+   [14] Lanczos: L^-1 (host time to enqueue it)  [15] Lanczos: host eigen [16] Lanczos: device wait
    [17] Schur: matrix  [18] Schur: <A_i, W>     [19] Schur: <A_i, W^2>
    [20] presolve + upload of the data (host wall clock)
    [21] iterations + final DIMACS check, CUDA events on the solver stream
