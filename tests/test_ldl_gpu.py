@@ -11,6 +11,7 @@ import pytest
 
 from hdsdp_b200 import api, instances
 from make_golden import FULL, SMALL
+from oracle import ldl_ref as R
 from test_solve_gpu import check_parity
 
 pytestmark = pytest.mark.gpu
@@ -64,6 +65,30 @@ def test_ldl_solve_against_numpy(gpu_lib, n):
         xr = np.linalg.solve(S, b)
         cond = np.linalg.cond(S)
         assert np.linalg.norm(x - xr) <= 1e-13 * cond * np.linalg.norm(xr) + 1e-300, kind
+
+
+# one-block and cooperative-grid orders
+@pytest.mark.parametrize("n", [40, 200, 385, 700])
+def test_ldl_pivots_match_lapack_restatement(gpu_lib, n):
+    """The device factorisation takes the pivots of the restatement of LAPACK's Bunch-Kaufman
+    (oracle/ldl_ref.py, itself checked against scipy.linalg.ldl): the same number of 2 x 2
+    blocks and the same inertia, and the same solution."""
+    rng = np.random.default_rng(500 + n)
+    for kind in ("random", "zero_diagonal", "small_diagonal"):
+        B = rng.standard_normal((n, n))
+        S = (B + B.T) / 2
+        if kind == "zero_diagonal":
+            np.fill_diagonal(S, 0.0)
+        elif kind == "small_diagonal":
+            S[np.diag_indices(n)] *= 0.1
+        b = rng.standard_normal(n)
+        F = R.bunch_kaufman(S)
+        r, x, out = ldl_solve(gpu_lib, S, b)
+        assert r == 0, kind
+        assert tuple(out) == R.inertia(F), kind
+        xr = R.solve(F, b)
+        cond = np.linalg.cond(S)
+        assert np.linalg.norm(x - xr) <= 1e-13 * cond * np.linalg.norm(xr), kind
 
 
 def test_ldl_edge_cases(gpu_lib):
