@@ -24,7 +24,7 @@ EXPORTS = [
     "hdsdpb_sparse_analyse",
     "hdsdpb_sparse_cholesky", "hdsdpb_sparse_congruence",
     "HDSDPGetIterLog", "HDSDPGetTimers", "HDSDPAdjoint",
-    "hdsdpb_schur_probe", "hdsdpb_ratio_probe", "hdsdpb_cholesky", "hdsdpb_cholesky_batch", "hdsdpb_cholesky_noalloc", "hdsdpb_inverse", "hdsdpb_gemm",
+    "hdsdpb_schur_probe", "hdsdpb_ratio_probe", "hdsdpb_cholesky", "hdsdpb_cholesky_batch", "hdsdpb_cholesky_noalloc", "hdsdpb_cholesky_inverse_factor", "hdsdpb_inverse", "hdsdpb_gemm",
     "hdsdpb_kernel_timing", "hdsdpb_gridsync_probe", "hdsdpb_launch_count", "hdsdpb_alloc_calls", "hdsdpb_release_cached_memory",
     "hdsdpb_kstat_enable", "hdsdpb_kstat_read", "hdsdpb_split_gemm", "hdsdpb_cholesky_solve", "HReadSDPA",
     # the conic callback interface and the KKT manager (include/hdsdp_conic.h)
@@ -92,6 +92,7 @@ def load():
         "hdsdpb_cholesky_batch": ([i, i, i, dp, dp, dp, dp, ip], i),
         "hdsdpb_cholesky_noalloc": ([i, dp, dp, dp], i),
         "hdsdpb_inverse": ([i, dp, dp], i),
+        "hdsdpb_cholesky_inverse_factor": ([i, dp, dp, dp], i),
         "hdsdpb_cholesky_solve": ([i, dp, dp, dp], i),
         "HReadSDPA": ([C.c_char_p] + [vp] * 13, i),
         "hdsdpb_gemm": ([i, i, i, d, dp, i, i, dp, i, i, d, dp, i], i),

@@ -1045,6 +1045,101 @@ bool coop_factorize_enqueue(cudaStream_t s, DenseFactor &F, const double *S, lon
     return true;
 }
 
+// ---- recursive blocked form (orders above kRecLeafMaxN, with K = L^-1) ----------------
+//   L11 L11^T = A11 (recursively; a block of at most kRecLeafMaxN rows on the cooperative
+//   kernel, which also forms its K and K^T), L21 = A21 K11^T, A22 -= L21 L21^T,
+//   L22 L22^T = A22 (recursively), K21 = -K22 (L21 K11), KT12 = K21^T.
+// The split falls on a 64-row boundary, so every diagonal block's 64 x 64 inverses land in
+// Dinv where the one-launch factorisation puts them. Each diagonal block reports its status
+// in a word of its own; the first failure (with its global pivot index) becomes the
+// factor's status.
+namespace {
+constexpr int kRecMaxLeaves = 16;
+struct RecLeaves {
+    int off[kRecMaxLeaves];
+    int count;
+};
+
+__global__ void rec_info_kernel(const RecLeaves R, const int *leaf_info, int *info) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    int v = 0;
+    for (int q = 0; q < R.count && v == 0; ++q)
+        if (leaf_info[q] != 0) v = leaf_info[q] + R.off[q];
+    *info = v;
+}
+
+// B (cols x rows) = A^T for A rows x cols
+__global__ void transpose_rect_kernel(int rows, int cols, const double *A, long lda, double *B, long ldb) {
+    __shared__ double tile[32][33];
+    const int bx = blockIdx.x * 32, by = blockIdx.y * 32;
+    for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+        const int r = bx + threadIdx.x, c = by + j;
+        if (r < rows && c < cols) tile[j][threadIdx.x] = A[(size_t) r + (size_t) c * lda];
+    }
+    __syncthreads();
+    for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+        const int r = by + threadIdx.x, c = bx + j;   // B(r, c) = A(c, r)
+        if (r < cols && c < rows) B[(size_t) r + (size_t) c * ldb] = tile[threadIdx.x][j];
+    }
+}
+
+bool rec_factor(cudaStream_t s, DenseFactor &F, int off, int n, RecLeaves &R) {
+    const long ld = F.ld;
+    if (n <= kRecLeafMaxN) {
+        if (R.count >= kRecMaxLeaves) return false;
+        DenseFactor V;   // a view of the diagonal block in F's buffers (never released)
+        V.n = n;
+        V.ld = ld;
+        V.L = F.L + off + (size_t) off * ld;
+        V.Dinv = F.Dinv + off;
+        V.K = F.K + off + (size_t) off * ld;
+        V.KT = F.KT + off + (size_t) off * ld;
+        V.d_info = F.d_rec_info + R.count;
+        V.fuse_k = true;
+        V.kfamily = F.kfamily;
+        R.off[R.count++] = off;
+        return coop_factorize_enqueue(s, V, V.L, ld);
+    }
+    const int n1 = ((n / 2) / 64) * 64, n2 = n - n1;
+    if (!rec_factor(s, F, off, n1, R)) return false;
+    double *L21 = F.L + (off + n1) + (size_t) off * ld;
+    double *A22 = F.L + (off + n1) + (size_t) (off + n1) * ld;
+    const double *K11 = F.K + off + (size_t) off * ld, *KT11 = F.KT + off + (size_t) off * ld;
+    const double *K22 = F.K + (off + n1) + (size_t) (off + n1) * ld;
+    double *K21 = F.K + (off + n1) + (size_t) off * ld, *KT12 = F.KT + off + (size_t) (off + n1) * ld;
+    double *W = F.d_rec_w;   // n2 x n1, leading dimension ld
+    gemm(s, n2, n1, n1, 1.0, L21, ld, 0, KT11, ld, 0, 0.0, W, ld, GEMM_B_UPPER);      // A21 K11^T
+    copy_matrix(s, n2, n1, W, ld, L21, ld);
+    gemm(s, n2, n2, n1, -1.0, L21, ld, 0, L21, ld, 1, 1.0, A22, ld, GEMM_C_LOWER);    // A22 -= L21 L21^T
+    if (!rec_factor(s, F, off + n1, n2, R)) return false;
+    gemm(s, n2, n1, n1, 1.0, L21, ld, 0, K11, ld, 0, 0.0, W, ld, GEMM_B_LOWER);       // L21 K11
+    gemm(s, n2, n1, n2, -1.0, K22, ld, 0, W, ld, 0, 0.0, K21, ld, GEMM_A_LOWER);      // -K22 (L21 K11)
+    dim3 grid((n2 + 31) / 32, (n1 + 31) / 32), block(32, 8);
+    transpose_rect_kernel<<<hb::counted(grid), block, 0, s>>>(n2, n1, K21, ld, KT12, ld);
+    return cudaGetLastError() == cudaSuccess;
+}
+}  // namespace
+
+bool rec_factorize_enqueue(cudaStream_t s, DenseFactor &F, const double *S, long ldS) {
+    const int n = F.n;
+    if (!F.d_rec_info && hb::cmalloc(&F.d_rec_info, sizeof(int) * kRecMaxLeaves) != cudaSuccess) {
+        F.d_rec_info = nullptr;
+        return false;
+    }
+    if (!F.d_rec_w && hb::cmalloc(&F.d_rec_w, sizeof(double) * F.ld * ((n + 1) / 2)) != cudaSuccess) {
+        F.d_rec_w = nullptr;
+        return false;
+    }
+    HB_CUDA(cudaMemsetAsync(F.d_rec_info, 0, sizeof(int) * kRecMaxLeaves, s));
+    copy_lower_k<<<hb::counted(grid_for_n((long) n * n)), 256, 0, s>>>(n, S, ldS, F.L, F.ld);
+    RecLeaves R;
+    R.count = 0;
+    const bool ok = rec_factor(s, F, 0, n, R);
+    rec_info_kernel<<<hb::counted(1), 32, 0, s>>>(R, F.d_rec_info, F.d_info);
+    if (!ok) device_error_flag() = 1;
+    return ok && cudaGetLastError() == cudaSuccess;
+}
+
 // The factorisations of F[0..count) (each n <= kSmallFactorMaxN) of S[i] (ldS[i]) in launches of up to
 // kSmallBatch CTAs, the status words written into each factor's pinned host mirror by the
 // kernel; returns false (nothing enqueued) if a mirror has no device address, or false

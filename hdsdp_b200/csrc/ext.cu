@@ -494,6 +494,39 @@ int hdsdpb_inverse(int n, const double *S, double *Sinv) {
     return ok ? 0 : 1;
 }
 
+int hdsdpb_cholesky_inverse_factor(int n, const double *S, double *L, double *K) {
+    if (n < 0 || (n > 0 && (!S || !L || !K))) return -1;
+    if (n == 0) return 0;
+    cudaStream_t s;
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return -1;
+    const long ld = pad_ld(n);
+    double *dS = nullptr;
+    hb::cmalloc(&dS, sizeof(double) * ld * n);
+    cudaMemcpy2D(dS, sizeof(double) * ld, S, sizeof(double) * n, sizeof(double) * n, n, cudaMemcpyHostToDevice);
+    legacy_fence();
+    DenseFactor F;
+    F.alloc(n, 1);
+    const bool ok = factorize(s, F, dS, ld);
+    if (ok) {
+        compute_inverse_factor(s, F);   // no work when the factorisation formed K
+        std::vector<double> h((size_t) ld * n);
+        cudaMemcpyAsync(h.data(), F.L, sizeof(double) * ld * n, cudaMemcpyDeviceToHost, s);
+        cudaStreamSynchronize(s);
+        for (int j = 0; j < n; ++j)
+            for (int i = 0; i < n; ++i) L[(size_t) j * n + i] = (i >= j) ? h[(size_t) j * ld + i] : 0.0;
+        cudaMemcpyAsync(h.data(), F.K, sizeof(double) * ld * n, cudaMemcpyDeviceToHost, s);
+        cudaStreamSynchronize(s);
+        for (int j = 0; j < n; ++j)
+            for (int i = 0; i < n; ++i) K[(size_t) j * n + i] = (i >= j) ? h[(size_t) j * ld + i] : 0.0;
+    }
+    cudaStreamSynchronize(s);
+    F.release();
+    hb::cache_free(dS);
+    cudaStreamDestroy(s);
+    if (device_error_flag()) return -1;
+    return ok ? 0 : 1;
+}
+
 int hdsdpb_gemm(int M, int N, int K, double alpha, const double *A, int lda, int transA, const double *B, int ldb,
                 int transB, double beta, double *C, int ldc) {
     const int ar = transA ? K : M, ac = transA ? M : K;
@@ -598,7 +631,8 @@ extern "C" int hdsdpb_kernel_timing(int which, int n, int reps, double *ms) {
     fill_spd_kernel<<<hb::counted(1024), 256, 0, s>>>(n, B, ld, 7u);
     fill(s, x, 1.0, n);
     DenseFactor F;
-    F.alloc(n, which == 7 ? 1 : ((which == 8 || which == 9) ? 0 : -1));
+    F.alloc(n, (which == 7 || which == 10) ? 1 : ((which == 8 || which == 9) ? 0 : -1));
+    F.no_rec = (which == 10);
     Lanczos lz;
     if (which == 5) lz.init(n, s);
     cudaEvent_t e0, e1;
@@ -614,7 +648,8 @@ extern "C" int hdsdpb_kernel_timing(int which, int n, int reps, double *ms) {
             case 5: { double st; lz.solve(F, B, ld, &st, nullptr); } break;
             case 6: gemm(s, n, n, 64, -1.0, A, ld, 0, B, ld, 1, 1.0, Cm, ld, GEMM_C_LOWER); break;
             case 7:
-            case 8: factorize_async(s, F, A, ld); break;
+            case 8:
+            case 10: factorize_async(s, F, A, ld); break;
             case 9: chol_solve(s, F, x, y); break;
         }
     };

@@ -804,8 +804,10 @@ void DenseFactor::alloc(int n_, int fuse_inverse) {
     // the solve scratch is sized for n: drop any from an earlier size
     if (d_flags) hb::cache_free(d_flags);
     if (d_tmp) hb::cache_free(d_tmp);
+    if (d_rec_w) hb::cache_free(d_rec_w);
     d_flags = nullptr;
     d_tmp = nullptr;
+    d_rec_w = nullptr;
     epoch = 0;
     n = n_;
     ld = pad_ld(n);
@@ -837,8 +839,12 @@ void DenseFactor::release() {
     if (d_info) hb::cache_free(d_info);
     if (d_flags) hb::cache_free(d_flags);
     if (d_tmp) hb::cache_free(d_tmp);
+    if (d_rec_info) hb::cache_free(d_rec_info);
+    if (d_rec_w) hb::cache_free(d_rec_w);
     d_flags = nullptr;
     d_tmp = nullptr;
+    d_rec_info = nullptr;
+    d_rec_w = nullptr;
     epoch = 0;
     if (h_info) hb::cache_free_host(h_info);
     L = Dinv = K = KT = nullptr;
@@ -863,6 +869,7 @@ static void ensure_attrs() {
 }
 
 bool coop_factorize_enqueue(cudaStream_t s, DenseFactor &F, const double *S, long ldS);
+bool rec_factorize_enqueue(cudaStream_t s, DenseFactor &F, const double *S, long ldS);
 bool coop_inverse_enqueue(cudaStream_t s, DenseFactor &F);
 
 void factorize_async(cudaStream_t s, DenseFactor &F, const double *S, long ldS) {
@@ -881,6 +888,11 @@ void factorize_async(cudaStream_t s, DenseFactor &F, const double *S, long ldS) 
             HB_CUDA(cudaMemcpyAsync(F.h_info, F.d_info, sizeof(int), cudaMemcpyDeviceToHost, s));
         }
     };
+    if (F.fuse_k && F.K && F.KT && !F.no_rec && n > kRecMinN && rec_factorize_enqueue(s, F, S, ldS)) {
+        F.k_pending = true;
+        status_copy();
+        return;
+    }
     if (coop_factorize_enqueue(s, F, S, ldS)) {
         F.k_pending = F.fuse_k && F.K && F.KT;
         status_copy();

@@ -198,6 +198,13 @@ extern int hdsdpb_cholesky_noalloc( int n, const double *S, double *L, double *l
    Returns 0 on success, 1 if not positive definite. */
 extern int hdsdpb_inverse( int n, const double *S, double *Sinv );
 
+/* The Cholesky factor L of a symmetric positive definite n x n matrix together with its
+   inverse K = L^-1, as the solver forms them for its Schur matrix below 6000 rows (K in the
+   factorisation's own launch; above order 3840 the recursive blocked form). Column-major
+   host buffers; L and K are written with zeros above the diagonal. Returns 0 on success, 1
+   if not positive definite, -1 on error. */
+extern int hdsdpb_cholesky_inverse_factor( int n, const double *S, double *L, double *K );
+
 /* FP64 GEMM on the tensor-core path: C = alpha op(A) op(B) + beta C with
    column-major host buffers (op = transpose when trans != 0). */
 extern int hdsdpb_gemm( int M, int N, int K, double alpha, const double *A, int lda, int transA,
@@ -215,8 +222,9 @@ extern int hdsdpb_split_gemm( int M, int N, int K, const double *A, int lda, int
    on the launching stream, 2 warm-up calls): 0 GEMM NN, 1 GEMM TN lower,
    2 Cholesky, 3 triangular inverse L^-1, 4 matrix-vector product,
    5 Lanczos step bound, 6 rank-64 SYRK update, 7 Cholesky that also forms L^-1,
-   8 Cholesky without it, 9 solve with the factor (forward and backward substitution).
-   Writes milliseconds per call. */
+   8 Cholesky without it, 9 solve with the factor (forward and backward substitution),
+   10 as 7 on the one-launch kernel at every order (7 takes the recursive blocked form
+   above order 3840). Writes milliseconds per call. */
 extern int hdsdpb_kernel_timing( int which, int n, int reps, double *ms );
 
 /* Host only (no device work): the ordering of the sparse factorisation of S for the

@@ -74,6 +74,23 @@ def test_cholesky_and_inverse(gpu_lib, n):
     assert np.abs(Si @ S - np.eye(n)).max() <= 1e-9
 
 
+# the one-launch kernel with K (up to 3840), just above the crossover to the recursive form
+# (one split), and an order whose halves split again
+@pytest.mark.parametrize("n", [700, 2100, 3840, 3904, 4577, 5999])
+def test_cholesky_with_inverse_factor(gpu_lib, n):
+    import ctypes as C
+    S = np.asfortranarray(_spd(n, 3 * n))
+    L = np.zeros((n, n), order="F")
+    K = np.zeros((n, n), order="F")
+    dp = C.POINTER(C.c_double)
+    r = gpu_lib.hdsdpb_cholesky_inverse_factor(n, S.ctypes.data_as(dp), L.ctypes.data_as(dp), K.ctypes.data_as(dp))
+    assert r == 0
+    Lref = np.linalg.cholesky(S)
+    assert np.abs(L - Lref).max() <= 1e-11 * np.abs(Lref).max()
+    assert np.abs(np.triu(K, 1)).max() == 0.0
+    assert np.abs(K @ Lref - np.eye(n)).max() <= 1e-10
+
+
 @pytest.mark.parametrize("n", [5, 64, 300])
 def test_cholesky_detects_indefinite(gpu_lib, n):
     S = _spd(n, 3)
