@@ -1054,7 +1054,7 @@ bool coop_factorize_enqueue(cudaStream_t s, DenseFactor &F, const double *S, lon
 // in a word of its own; the first failure (with its global pivot index) becomes the
 // factor's status.
 namespace {
-constexpr int kRecMaxLeaves = 16;
+constexpr int kRecMaxLeaves = 128;
 struct RecLeaves {
     int off[kRecMaxLeaves];
     int count;
@@ -1083,24 +1083,31 @@ __global__ void transpose_rect_kernel(int rows, int cols, const double *A, long 
     }
 }
 
+int rec_split(int n) { return ((n / 2) / 64) * 64; }
+
+// the diagonal block [off, off + n) of F on the cooperative kernel, its K and K^T into Kp / KTp
+// (leading dimension F.ld)
+bool rec_leaf(cudaStream_t s, DenseFactor &F, int off, int n, double *Kp, double *KTp, RecLeaves &R) {
+    if (R.count >= kRecMaxLeaves) return false;
+    DenseFactor V;   // a view of the diagonal block in F's buffers (never released)
+    V.n = n;
+    V.ld = F.ld;
+    V.L = F.L + off + (size_t) off * F.ld;
+    V.Dinv = F.Dinv + off;
+    V.K = Kp;
+    V.KT = KTp;
+    V.d_info = F.d_rec_info + R.count;
+    V.fuse_k = true;
+    V.kfamily = F.kfamily;
+    R.off[R.count++] = off;
+    return coop_factorize_enqueue(s, V, V.L, F.ld);
+}
+
 bool rec_factor(cudaStream_t s, DenseFactor &F, int off, int n, RecLeaves &R) {
     const long ld = F.ld;
-    if (n <= kRecLeafMaxN) {
-        if (R.count >= kRecMaxLeaves) return false;
-        DenseFactor V;   // a view of the diagonal block in F's buffers (never released)
-        V.n = n;
-        V.ld = ld;
-        V.L = F.L + off + (size_t) off * ld;
-        V.Dinv = F.Dinv + off;
-        V.K = F.K + off + (size_t) off * ld;
-        V.KT = F.KT + off + (size_t) off * ld;
-        V.d_info = F.d_rec_info + R.count;
-        V.fuse_k = true;
-        V.kfamily = F.kfamily;
-        R.off[R.count++] = off;
-        return coop_factorize_enqueue(s, V, V.L, ld);
-    }
-    const int n1 = ((n / 2) / 64) * 64, n2 = n - n1;
+    if (n <= kRecLeafMaxN)
+        return rec_leaf(s, F, off, n, F.K + off + (size_t) off * ld, F.KT + off + (size_t) off * ld, R);
+    const int n1 = rec_split(n), n2 = n - n1;
     if (!rec_factor(s, F, off, n1, R)) return false;
     double *L21 = F.L + (off + n1) + (size_t) off * ld;
     double *A22 = F.L + (off + n1) + (size_t) (off + n1) * ld;
@@ -1117,6 +1124,36 @@ bool rec_factor(cudaStream_t s, DenseFactor &F, int off, int n, RecLeaves &R) {
     dim3 grid((n2 + 31) / 32, (n1 + 31) / 32), block(32, 8);
     transpose_rect_kernel<<<hb::counted(grid), block, 0, s>>>(n2, n1, K21, ld, KT12, ld);
     return cudaGetLastError() == cudaSuccess;
+}
+
+// X (rows x nL, leading dimension ldx) <- X L^-T for the diagonal block L of F at [Loff, Loff +
+// nL), split as the factorisation split it: a leaf is one GEMM with that block's K^T (kept in
+// the strip), otherwise Xa <- Xa La^-T, Xc -= Xa Lb^T, Xc <- Xc Lc^-T
+bool rec_trsm(cudaStream_t s, DenseFactor &F, double *X, long ldx, int rows, int Loff, int nL) {
+    const long ld = F.ld;
+    if (nL <= kRecLeafMaxN) {
+        gemm(s, rows, nL, nL, 1.0, X, ldx, 0, F.d_rec_kts + Loff, ld, 0, 0.0, F.d_rec_w, ld, GEMM_B_UPPER);
+        copy_matrix(s, rows, nL, F.d_rec_w, ld, X, ldx);
+        return true;
+    }
+    const int n1 = rec_split(nL), nc = nL - n1;
+    if (!rec_trsm(s, F, X, ldx, rows, Loff, n1)) return false;
+    gemm(s, rows, nc, n1, -1.0, X, ldx, 0, F.L + (Loff + n1) + (size_t) Loff * ld, ld, 1, 1.0, X + (size_t) n1 * ldx,
+         ldx, 0);
+    return rec_trsm(s, F, X + (size_t) n1 * ldx, ldx, rows, Loff + n1, nc);
+}
+
+// the recursive form without K: the diagonal blocks' K (and K^T) go to the strips
+bool rec_factor_nok(cudaStream_t s, DenseFactor &F, int off, int n, RecLeaves &R) {
+    const long ld = F.ld;
+    if (n <= kRecLeafMaxN) return rec_leaf(s, F, off, n, F.d_rec_ks + off, F.d_rec_kts + off, R);
+    const int n1 = rec_split(n), n2 = n - n1;
+    if (!rec_factor_nok(s, F, off, n1, R)) return false;
+    double *L21 = F.L + (off + n1) + (size_t) off * ld;
+    double *A22 = F.L + (off + n1) + (size_t) (off + n1) * ld;
+    if (!rec_trsm(s, F, L21, ld, n2, off, n1)) return false;                            // A21 L11^-T
+    gemm(s, n2, n2, n1, -1.0, L21, ld, 0, L21, ld, 1, 1.0, A22, ld, GEMM_C_LOWER);    // A22 -= L21 L21^T
+    return rec_factor_nok(s, F, off + n1, n2, R);
 }
 }  // namespace
 
@@ -1135,6 +1172,39 @@ bool rec_factorize_enqueue(cudaStream_t s, DenseFactor &F, const double *S, long
     RecLeaves R;
     R.count = 0;
     const bool ok = rec_factor(s, F, 0, n, R);
+    rec_info_kernel<<<hb::counted(1), 32, 0, s>>>(R, F.d_rec_info, F.d_info);
+    if (!ok) device_error_flag() = 1;
+    return ok && cudaGetLastError() == cudaSuccess;
+}
+
+bool rec_factorize_nok_enqueue(cudaStream_t s, DenseFactor &F, const double *S, long ldS) {
+    const int n = F.n;
+    const size_t strip = (size_t) F.ld * kRecLeafMaxN;
+    if (!F.d_rec_info && hb::cmalloc(&F.d_rec_info, sizeof(int) * kRecMaxLeaves) != cudaSuccess) {
+        F.d_rec_info = nullptr;
+        return false;
+    }
+    if (!F.d_rec_w && hb::cmalloc(&F.d_rec_w, sizeof(double) * F.ld * std::max((n + 1) / 2, kRecLeafMaxN)) !=
+                          cudaSuccess) {
+        F.d_rec_w = nullptr;
+        return false;
+    }
+    if (!F.d_rec_ks) {
+        // zero outside the blocks' triangles, which the cooperative kernel never writes
+        if (hb::cmalloc(&F.d_rec_ks, sizeof(double) * strip) != cudaSuccess ||
+            hb::cmalloc(&F.d_rec_kts, sizeof(double) * strip) != cudaSuccess) {
+            if (F.d_rec_ks) hb::cache_free(F.d_rec_ks);
+            F.d_rec_ks = F.d_rec_kts = nullptr;
+            return false;
+        }
+        HB_CUDA(cudaMemsetAsync(F.d_rec_ks, 0, sizeof(double) * strip, s));
+        HB_CUDA(cudaMemsetAsync(F.d_rec_kts, 0, sizeof(double) * strip, s));
+    }
+    HB_CUDA(cudaMemsetAsync(F.d_rec_info, 0, sizeof(int) * kRecMaxLeaves, s));
+    copy_lower_k<<<hb::counted(grid_for_n((long) n * n)), 256, 0, s>>>(n, S, ldS, F.L, F.ld);
+    RecLeaves R;
+    R.count = 0;
+    const bool ok = rec_factor_nok(s, F, 0, n, R);
     rec_info_kernel<<<hb::counted(1), 32, 0, s>>>(R, F.d_rec_info, F.d_info);
     if (!ok) device_error_flag() = 1;
     return ok && cudaGetLastError() == cudaSuccess;

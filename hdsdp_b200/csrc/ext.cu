@@ -631,8 +631,8 @@ extern "C" int hdsdpb_kernel_timing(int which, int n, int reps, double *ms) {
     fill_spd_kernel<<<hb::counted(1024), 256, 0, s>>>(n, B, ld, 7u);
     fill(s, x, 1.0, n);
     DenseFactor F;
-    F.alloc(n, (which == 7 || which == 10) ? 1 : ((which == 8 || which == 9) ? 0 : -1));
-    F.no_rec = (which == 10);
+    F.alloc(n, (which == 7 || which == 10) ? 1 : ((which == 8 || which == 9 || which == 11) ? 0 : -1));
+    F.no_rec = (which == 10 || which == 11);
     Lanczos lz;
     if (which == 5) lz.init(n, s);
     cudaEvent_t e0, e1;
@@ -649,7 +649,8 @@ extern "C" int hdsdpb_kernel_timing(int which, int n, int reps, double *ms) {
             case 6: gemm(s, n, n, 64, -1.0, A, ld, 0, B, ld, 1, 1.0, Cm, ld, GEMM_C_LOWER); break;
             case 7:
             case 8:
-            case 10: factorize_async(s, F, A, ld); break;
+            case 10:
+            case 11: factorize_async(s, F, A, ld); break;
             case 9: chol_solve(s, F, x, y); break;
         }
     };

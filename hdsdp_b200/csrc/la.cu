@@ -805,9 +805,12 @@ void DenseFactor::alloc(int n_, int fuse_inverse) {
     if (d_flags) hb::cache_free(d_flags);
     if (d_tmp) hb::cache_free(d_tmp);
     if (d_rec_w) hb::cache_free(d_rec_w);
+    if (d_rec_ks) hb::cache_free(d_rec_ks);
+    if (d_rec_kts) hb::cache_free(d_rec_kts);
     d_flags = nullptr;
     d_tmp = nullptr;
     d_rec_w = nullptr;
+    d_rec_ks = d_rec_kts = nullptr;
     epoch = 0;
     n = n_;
     ld = pad_ld(n);
@@ -841,10 +844,13 @@ void DenseFactor::release() {
     if (d_tmp) hb::cache_free(d_tmp);
     if (d_rec_info) hb::cache_free(d_rec_info);
     if (d_rec_w) hb::cache_free(d_rec_w);
+    if (d_rec_ks) hb::cache_free(d_rec_ks);
+    if (d_rec_kts) hb::cache_free(d_rec_kts);
     d_flags = nullptr;
     d_tmp = nullptr;
     d_rec_info = nullptr;
     d_rec_w = nullptr;
+    d_rec_ks = d_rec_kts = nullptr;
     epoch = 0;
     if (h_info) hb::cache_free_host(h_info);
     L = Dinv = K = KT = nullptr;
@@ -870,6 +876,7 @@ static void ensure_attrs() {
 
 bool coop_factorize_enqueue(cudaStream_t s, DenseFactor &F, const double *S, long ldS);
 bool rec_factorize_enqueue(cudaStream_t s, DenseFactor &F, const double *S, long ldS);
+bool rec_factorize_nok_enqueue(cudaStream_t s, DenseFactor &F, const double *S, long ldS);
 bool coop_inverse_enqueue(cudaStream_t s, DenseFactor &F);
 
 void factorize_async(cudaStream_t s, DenseFactor &F, const double *S, long ldS) {
@@ -890,6 +897,11 @@ void factorize_async(cudaStream_t s, DenseFactor &F, const double *S, long ldS) 
     };
     if (F.fuse_k && F.K && F.KT && !F.no_rec && n > kRecMinN && rec_factorize_enqueue(s, F, S, ldS)) {
         F.k_pending = true;
+        status_copy();
+        return;
+    }
+    if (!F.fuse_k && !F.no_rec && n > kRecNoKMinN && rec_factorize_nok_enqueue(s, F, S, ldS)) {
+        F.k_pending = false;
         status_copy();
         return;
     }

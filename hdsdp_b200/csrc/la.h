@@ -82,6 +82,11 @@ constexpr int kFuseInverseMax = 2048;
 // against 3.22 recursive, 4096 4.25 / 3.79, 5120 7.48 / 6.36, 5999 11.6 / 9.98.
 constexpr int kRecMinN = 3840;
 constexpr int kRecLeafMaxN = 2560;
+// Above kRecNoKMinN a factorisation without K takes the recursive form too: L21 = A21 L11^-T
+// by a recursive triangular solve whose leaves are GEMMs with the diagonal blocks' own K
+// (kept in an n x kRecLeafMaxN strip). Measured on B200 (factor only, ms, one launch against
+// recursive): order 6016 5.62 / 6.67, 8000 11.8 / 11.7, 12000 36.8 / 31.2, 16000 83.9 / 64.4.
+constexpr int kRecNoKMinN = 8192;
 
 struct DenseFactor {
     int n = 0;
@@ -117,6 +122,7 @@ struct DenseFactor {
     // (allocated on first use): the diagonal blocks' status words and an n x n/2 product
     int *d_rec_info = nullptr;
     double *d_rec_w = nullptr;
+    double *d_rec_ks = nullptr, *d_rec_kts = nullptr;   // the diagonal blocks' K and K^T (no-K form)
     bool no_rec = false;      // keep the one-launch factorisation at every order (timing)
     int kfamily = KF_POTRF;   // kernel-timing family of this factor's factorisations
     void alloc(int n_, int fuse_inverse = -1);

@@ -224,7 +224,8 @@ extern int hdsdpb_split_gemm( int M, int N, int K, const double *A, int lda, int
    5 Lanczos step bound, 6 rank-64 SYRK update, 7 Cholesky that also forms L^-1,
    8 Cholesky without it, 9 solve with the factor (forward and backward substitution),
    10 as 7 on the one-launch kernel at every order (7 takes the recursive blocked form
-   above order 3840). Writes milliseconds per call. */
+   above order 3840), 11 as 8 on the one-launch kernel at every order (8 takes the
+   recursive form above order 8192). Writes milliseconds per call. */
 extern int hdsdpb_kernel_timing( int which, int n, int reps, double *ms );
 
 /* Host only (no device work): the ordering of the sparse factorisation of S for the

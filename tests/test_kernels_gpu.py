@@ -62,7 +62,8 @@ def _spd(n, seed, cond=1e3):
     return (Q * ev) @ Q.T
 
 
-@pytest.mark.parametrize("n", [1, 2, 31, 64, 65, 127, 200, 513, 1000, 2100])
+# up to 2100 the one-launch kernel; 8300 the recursive form without K
+@pytest.mark.parametrize("n", [1, 2, 31, 64, 65, 127, 200, 513, 1000, 2100, 8300])
 def test_cholesky_and_inverse(gpu_lib, n):
     S = _spd(n, n)
     L, logdiag, pd = api.cholesky(S)
